@@ -1,0 +1,316 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 dense plane sweep: samples·planes·views per second.
+
+Workload (one step): the full native clip — 640x360, 120 keyframes on a 40°
+arc with ±2° seeded jitter, 4-octave value-noise planes, noise σ=0.01 — where
+every keyframe is a reference against its 8 nearest source views, with 128
+inverse-depth hypotheses and a 7x7 ZNCC window at grid stride 2, followed by
+the reciprocal check, fusion and both surface-completion passes.  One step is
+one call of v3d_reconstruct_reference_patches over all 120 references.
+
+  value  units / device time of the whole batch, frames already in HBM
+         (CUDA events on the library's stream: sweep through completion)
+  e2e    units / wall time of the C-ABI call with pinned host frames
+         (host->device upload, planning, kernels, device->host results)
+
+A unit is one window cost between a grid site and one source view at one
+hypothesis (every grid site counts; the contrast gate is reported apart).
+With --gpus N each rank runs its own clip (seed + rank): weak scaling, no
+collective on the data path.  `--impl reference` times the CPU restatement of
+the reference pass on a bounded band of grid rows with all host threads.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "video-to-3d_b200"))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "plane-sweep samples·planes·views/s"
+UNIT = "samples·planes·views/s"
+WIDTH, HEIGHT, FRAMES = 640, 360, 120
+RADIUS, PLANES, SOURCES, STRIDE = 3, 128, 8, 2
+
+
+def parse():
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--storage", choices=["f32", "f16", "bf16"], default="f32")
+    ap.add_argument("--frames", type=int, default=FRAMES)
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def workload(args):
+    return {"workload": "full native clip %dx%d, %d keyframes, every keyframe vs its %d nearest "
+                        "views, %d planes, %dx%d ZNCC, stride %d, reciprocal+fusion+completion, "
+                        "%s images" % (WIDTH, HEIGHT, args.frames, SOURCES, PLANES,
+                                       2 * RADIUS + 1, 2 * RADIUS + 1, STRIDE, args.storage),
+            "width": WIDTH, "height": HEIGHT, "keyframes": args.frames, "source_views": SOURCES,
+            "planes": PLANES, "window": 2 * RADIUS + 1, "grid_stride": STRIDE,
+            "storage": args.storage, "cost": "1-ZNCC",
+            "l2": "flushed between timed steps (256 MiB write)",
+            "parallelism": "weak: one clip per GPU, no collective on the data path"}
+
+
+def load_clip(seed, frames):
+    """The seeded clip, cached under the system temp directory between runs."""
+    from v3d import synth
+    path = os.path.join(tempfile.gettempdir(), "v3d_clip_%d_%d_%d_%d.npz" %
+                        (seed, WIDTH, HEIGHT, frames))
+    if os.path.exists(path):
+        z = np.load(path)
+        from v3d.types import RegisteredCamera
+        cams = [RegisteredCamera(i, z["R"][i], z["t"][i]) for i in range(frames)]
+        return synth.Clip(WIDTH, HEIGHT, float(z["focal"]), cams, list(z["images"]), [], z["sparse"])
+    clip = synth.full_clip(seed=seed, width=WIDTH, height=HEIGHT, n_frames=frames)
+    np.savez(path, images=np.stack(clip.images), R=np.stack([c.rotation for c in clip.cameras]),
+             t=np.stack([c.translation for c in clip.cameras]), sparse=clip.sparse,
+             focal=clip.focal)
+    return clip
+
+
+class Clocks:
+    """nvidia-smi SM clock and throttle-reason samples during the timed region."""
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(tempfile.gettempdir(), "v3d_clocks_%d.csv" % os.getpid())
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.QUERY,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(clip, frames, prof, threads, rows_per_thread=1):
+    """The CPU oracle (restated reference pass) on a band of grid rows of reference 60."""
+    from tests.oracle_ffi import Oracle
+    import ctypes as C
+    from v3d import types
+    o = Oracle()
+    ny = (HEIGHT - 2 * (RADIUS + 2) + STRIDE - 1) // STRIDE
+    rows = min(ny, threads * rows_per_thread)
+    start = (ny - rows) // 2
+    inp = types.Inputs(frames, clip.cameras, clip.sparse)
+    L = o.lib
+    L.v3do_time_rows.argtypes = [C.POINTER(type(inp.frames[0])), C.c_uint64,
+                                 C.POINTER(type(inp.cameras[0])), C.c_uint64,
+                                 C.POINTER(C.c_double), C.c_uint64, C.c_double,
+                                 C.c_void_p, C.c_uint64, C.c_uint32, C.c_uint32, C.c_int32,
+                                 C.POINTER(C.c_double), C.POINTER(C.c_uint64)]
+    L.v3do_time_rows.restype = C.c_int32
+    secs, units = C.c_double(), C.c_uint64()
+    ref = len(clip.cameras) // 2
+    L.v3do_time_rows(inp.frames, inp.n_frames, inp.cameras, inp.n_cameras, inp.sparse,
+                     inp.n_sparse, clip.focal, C.addressof(prof), ref, start, start + rows,
+                     threads, C.byref(secs), C.byref(units))
+    return units.value / secs.value, {
+        "cores": threads, "kind": "port",
+        "sample": "reference %d, grid rows %d..%d of %d (%d sites x %d planes x %d views), "
+                  "sweep+reciprocal+fusion, %d threads, completion not included" % (
+                      ref, start, start + rows, ny, units.value // (PLANES * SOURCES), PLANES,
+                      SOURCES, threads),
+        "seconds": secs.value}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    from v3d import profiles
+    clip = load_clip(2, args.frames)
+    frames = clip.frames(args.storage)
+    prof = profiles.zncc(RADIUS, PLANES, SOURCES, STRIDE)
+    threads = os.cpu_count() or 1
+    vals = []
+    for i in range(args.warmup + args.steps):
+        v, info = cpu_baseline(clip, frames, prof, threads)
+        if i >= args.warmup:
+            vals.append(v)
+    value = float(np.mean(vals))
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": info["seconds"] * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded value-noise planes)", "config": workload(args),
+            "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": info["cores"],
+                             "kind": "port", "sample": info["sample"]},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, local):
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from v3d import dense, profiles
+    from v3d.types import FrameInput
+    clip = load_clip(2 + rank, args.frames)
+    # frames in pinned host memory, as a caller hands them over
+    pinned = []
+    for fi in clip.frames(args.storage):
+        t = torch.empty(fi.pixels.shape, dtype={np.dtype(np.float32): torch.float32,
+                                                np.dtype(np.float16): torch.float16,
+                                                np.dtype(np.uint16): torch.int16}[fi.pixels.dtype],
+                        pin_memory=True)
+        t.numpy()[...] = fi.pixels.view(t.numpy().dtype)
+        pinned.append((t, FrameInput(t.numpy().view(fi.pixels.dtype), bf16=fi.bf16)))
+    frames = [p[1] for p in pinned]
+    h2d = sum(f.pixels.nbytes for f in frames)
+    prof = profiles.zncc(RADIUS, PLANES, SOURCES, STRIDE)
+    ctx = dense.Context(local)
+    refs = list(range(args.frames))
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def step():
+        t0 = time.perf_counter()
+        res = ctx.reconstruct_reference_patches(frames, clip.cameras, clip.sparse, clip.focal,
+                                                refs, profile=prof)
+        return time.perf_counter() - t0, res, ctx.last_run_info()
+
+    for _ in range(args.warmup):
+        step()
+    clocks = Clocks(local)
+    clocks.start()
+    dev_ms, wall, infos, points = [], [], [], 0
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        w, res, info = step()
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        dev_ms.append(info["device_ms"])
+        wall.append(w)
+        infos.append(info)
+        points = sum(len(r.points) for r in res if r is not None)
+    clk = clocks.stop()
+    units = infos[-1]["plane_view_units"]
+    dev_s = float(np.mean(dev_ms)) / 1e3
+    wall_s = float(np.mean(wall))
+    if dist:
+        t = torch.tensor([dev_s, wall_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dev_s, wall_s = float(t[0]), float(t[1])
+        u = torch.tensor([units], device="cuda", dtype=torch.float64)
+        dist.all_reduce(u, op=dist.ReduceOp.SUM)
+        total_units = float(u[0])
+    else:
+        total_units = float(units)
+    sweep_ms = float(np.mean([i["sweep_ms"] for i in infos]))
+    recip_ms = float(np.mean([i["reciprocal_ms"] for i in infos]))
+    comp_ms = float(np.mean([i["completion_ms"] for i in infos]))
+    line = None
+    if rank == 0:
+        peaks = {}
+        try:
+            peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        except OSError:
+            pass
+        hbm = peaks.get("hbm_gbs", 6650.0)
+        # the dominant stage and its algorithmic bytes per launch
+        b = {"f32": 4, "f16": 2, "bf16": 2}[args.storage]
+        taps = (2 * RADIUS + 1) ** 2
+        stages = {"sweep": sweep_ms, "reciprocal": recip_ms}
+        dominant = max(stages, key=stages.get)
+        if dominant == "sweep":
+            alg_bytes = units * 4 * taps * b
+            kernel = "k_sweep_tiled (depth sweep, box-filtered ZNCC)"
+        else:
+            alg_bytes = infos[-1]["reciprocal_plane_evaluations"] * 4 * taps * b
+            kernel = "k_reciprocal (single-view reciprocal sweep)"
+        achieved = alg_bytes / (stages[dominant] / 1e3) / 1e9
+        line = {
+            "metric": METRIC, "value": total_units / dev_s, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_s * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded value-noise planes, ray-cast)", "config": workload(args),
+            "clocks": clk,
+            "e2e": {"value": total_units / wall_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": points * 72, "ms_per_step": wall_s * 1e3},
+            "gpu_launches": infos[-1]["kernel_launches"],
+            "stages_ms": {"sweep": sweep_ms, "reciprocal_primary": recip_ms,
+                          "completion": comp_ms, "total": dev_s * 1e3},
+            "roofline": {"bound": "hbm", "kernel": kernel, "achieved": achieved, "peak": hbm,
+                         "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
+                         "note": "achieved = bilinear-footprint bytes 4*W^2*b per window "
+                                 "evaluation / kernel time, against the measured HBM copy peak "
+                                 "(of measured); the gathers are served by L1/L2"},
+            "points_per_step": points,
+        }
+        if world == 1:
+            v, info = cpu_baseline(clip, frames, prof, os.cpu_count() or 1)
+            line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": info["cores"],
+                                    "kind": "port", "sample": info["sample"]}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_ours(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

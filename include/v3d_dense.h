@@ -1,0 +1,455 @@
+/*
+ * v3d_dense.h — C ABI of the B200 dense plane-sweep depth pass.
+ *
+ * This library replaces the per-reference dense pass of video-to-3d-core
+ * (crates/video-to-3d-core/src/dense_legacy.rs) and the multi-reference
+ * driver around it (crates/video-to-3d-core/src/dense.rs), plus the
+ * reference-grid triangle gates of crates/video-to-3d-core/src/mesh_legacy.rs
+ * and mesh.rs, with CUDA kernels written for sm_100a.  Every entry point takes
+ * plain host pointers and sizes; results are returned in library-owned
+ * host arrays that the caller releases with the matching *_free function.
+ *
+ * Reference interfaces replaced (file:line inside crates/video-to-3d-core/src):
+ *   v3d_estimate_depth_points_with_control  dense_legacy.rs:149-470
+ *   v3d_reconstruct_reference_patches       dense.rs:674-747 (one call per camera, batched)
+ *   v3d_estimate_depth_points_limited       dense.rs:250-330
+ *   v3d_has_distributed_landmarks           dense.rs:165-213
+ *   v3d_grid_stride                         dense.rs:215-218
+ *   v3d_reconstruct_dense_mesh_samples      mesh_legacy.rs:150-358
+ *   v3d_reconstruct_dense_mesh_with_control mesh.rs:74-220
+ *
+ * Data contract (mirrors the Rust types bit for bit where a layout exists):
+ *   FrameInput  (reconstruction/types.rs:17-21)  -> v3d_frame (RGBA8, tightly packed)
+ *   RegisteredCamera (multi_view.rs:85-89)       -> v3d_camera (world->camera R,t;
+ *                                                   R stored ROW-major here)
+ *   Point3 (reconstruction/types.rs:69-77)       -> v3d_point (20 bytes)
+ *   DenseGridSite (dense.rs:57-60)               -> v3d_grid_site
+ *   EvidencePointAttributes
+ *     (reconstruction_evidence.rs:108-115)       -> v3d_point_attributes
+ *   MeshTriangle (mesh_legacy.rs:18-23)          -> v3d_mesh_triangle
+ *
+ * Errors: the reference never fails, it "skips" with an English reason
+ * (dense_legacy.rs:157-236).  A skip is V3D_SKIPPED with stats.skip_code and
+ * stats.skip_reason set to the exact reference string.  Negative statuses are
+ * errors of this library (bad arguments, CUDA failures) and leave the result
+ * zeroed.
+ *
+ * Threading: a v3d_context owns one CUDA stream and its device buffers; calls
+ * on one context are serialised by an internal mutex.  Use one context per
+ * host thread for concurrency.
+ */
+#ifndef V3D_DENSE_H
+#define V3D_DENSE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define V3D_ABI_VERSION 1
+#define V3D_SKIP_REASON_BYTES 320
+#define V3D_MAX_PATCH_RADIUS 4       /* windows up to 9x9 */
+#define V3D_MAX_SOURCE_VIEWS 16
+#define V3D_MAX_DEPTH_HYPOTHESES 256
+
+typedef enum v3d_status {
+    V3D_OK = 0,
+    V3D_SKIPPED = 1,                 /* the pass did not run; see stats.skip_code */
+    V3D_ERR_INVALID_ARGUMENT = -1,
+    V3D_ERR_CUDA = -2,
+    V3D_ERR_OUT_OF_MEMORY = -3,
+    V3D_ERR_NO_DEVICE = -4,
+    V3D_ERR_INTERNAL = -5
+} v3d_status;
+
+/* Skip reasons of dense_legacy.rs:157-236 and dense.rs, in the order the
+ * reference tests them.  v3d_skip_reason_text() returns the exact string. */
+typedef enum v3d_skip_code {
+    V3D_SKIP_NONE = 0,
+    V3D_SKIP_NO_FRAMES = 1,              /* dense_legacy.rs:158 */
+    V3D_SKIP_FEWER_THAN_TWO_CAMERAS = 2, /* dense_legacy.rs:161 */
+    V3D_SKIP_FEW_SPARSE_LANDMARKS = 3,   /* dense_legacy.rs:164-166 */
+    V3D_SKIP_FRAMES_TOO_SMALL = 4,       /* dense_legacy.rs:172 */
+    V3D_SKIP_NO_REFERENCE_CAMERA = 5,    /* dense_legacy.rs:188-190 */
+    V3D_SKIP_NO_DEPTH_ENVELOPE = 6,      /* dense_legacy.rs:197-199 */
+    V3D_SKIP_REFERENCE_FRAME_MISSING = 7,/* dense_legacy.rs:206 */
+    V3D_SKIP_NO_SOURCE_VIEW = 8,         /* dense_legacy.rs:233-235 */
+    V3D_SKIP_CANCELED = 9                /* dense_legacy.rs:274 */
+} v3d_skip_code;
+
+typedef enum v3d_pixel_format {
+    V3D_PIXEL_RGBA8 = 0,      /* width*height*4 bytes; luma = (77R+150G+29B)>>8 (dense_legacy.rs:1147-1157) */
+    V3D_PIXEL_GRAY_F32 = 1,   /* width*height floats in [0,1] */
+    V3D_PIXEL_GRAY_F16 = 2,   /* width*height IEEE binary16 */
+    V3D_PIXEL_GRAY_BF16 = 3   /* width*height bfloat16 */
+} v3d_pixel_format;
+
+typedef struct v3d_frame {
+    uint32_t width;
+    uint32_t height;
+    int32_t format;           /* v3d_pixel_format */
+    int32_t reserved;
+    const void* data;         /* host pointer, tightly packed rows */
+} v3d_frame;
+
+typedef struct v3d_camera {
+    uint64_t frame_index;     /* index into the frames array */
+    double rotation[9];       /* world->camera rotation, row-major R[row*3+col] */
+    double translation[3];    /* world->camera translation t: x_cam = R x_world + t */
+} v3d_camera;
+
+typedef enum v3d_cost {
+    V3D_COST_ZSAD = 0,        /* mean |(r-mean r)-(s-mean s)| (dense_legacy.rs:1032-1095) */
+    V3D_COST_ZNCC = 1         /* 1 - zero-mean normalised cross-correlation */
+} v3d_cost;
+
+typedef enum v3d_precision {
+    V3D_PRECISION_EXACT64 = 0,/* every tap in f64 with the reference's unproject/project formulas */
+    V3D_PRECISION_FAST32 = 1  /* per-plane homographies composed in f64, taps and sums in f32 */
+} v3d_precision;
+
+/* Hot-path constants.  v3d_profile_reference() fills dense_legacy.rs:6-21;
+ * every other value is a project-defined profile (see the docs). */
+typedef struct v3d_profile {
+    int32_t cost;                     /* v3d_cost */
+    int32_t patch_radius;             /* PATCH_RADIUS, window = 2r+1, 1..V3D_MAX_PATCH_RADIUS */
+    int32_t depth_hypotheses;         /* DEPTH_HYPOTHESES, 2..V3D_MAX_DEPTH_HYPOTHESES */
+    int32_t max_source_views;         /* MAX_SOURCE_VIEWS, 1..V3D_MAX_SOURCE_VIEWS */
+    int32_t grid_stride;              /* 0: the reference grid_stride() rule; >0: fixed stride */
+    int32_t precision;                /* v3d_precision */
+    double min_reference_contrast;    /* MIN_REFERENCE_CONTRAST, image units */
+    double max_photometric_error;     /* MAX_PHOTOMETRIC_ERROR, cost units */
+    double min_ambiguity_margin;      /* MIN_AMBIGUITY_MARGIN, cost units */
+    double depth_margin_saturation;   /* DEPTH_MARGIN_SATURATION, cost units */
+    double error_confidence_scale;    /* 8.0 in 1/(1+error/8) (dense_legacy.rs:390) */
+    double min_window_variance;       /* ZNCC: per-pixel variance floor of both windows */
+} v3d_profile;
+
+/* Output records, laid out like the Rust structs. */
+typedef struct v3d_point {
+    float x, y, z, confidence;
+    uint8_t r, g, b, pad;
+} v3d_point;
+
+typedef struct v3d_grid_site {
+    uint32_t x, y;
+} v3d_grid_site;
+
+typedef struct v3d_point_attributes {
+    float reciprocal_consistency;
+    float depth_margin;
+} v3d_point_attributes;
+
+/* DenseStats (dense_legacy.rs:23-53; dense.rs:99-139 adds the fields after
+ * search_max_depth).  Option<T> fields carry a has_* flag. */
+typedef struct v3d_dense_stats {
+    int32_t attempted;
+    int32_t skip_code;                        /* v3d_skip_code, or -1 for a reason with no code */
+    char skip_reason[V3D_SKIP_REASON_BYTES];  /* "" when none */
+    int32_t has_skip_reason;
+    int32_t has_reference_frame;
+    uint64_t reference_frame;
+    uint64_t source_views;
+    uint64_t sampled_pixels;
+    uint64_t depth_hypotheses;
+    uint64_t accepted_points;
+    uint64_t surface_completion_proposals;
+    uint64_t surface_completed_points;
+    uint64_t surface_completion_rejected_texture;
+    uint64_t surface_completion_rejected_cross_view;
+    uint64_t surface_completion_rejected_reciprocal;
+    uint64_t surface_completion_rejected_fusion;
+    uint64_t surface_completion_rejected_footprint;
+    uint64_t grid_stride;
+    uint32_t grid_border;
+    uint32_t pad0;
+    uint64_t reciprocal_checked_points;
+    uint64_t reciprocal_rejected_points;
+    uint64_t reciprocal_consistent_points;
+    uint64_t fusion_input_observations;
+    uint64_t fusion_rejected_observations;
+    uint64_t fusion_rejected_points;
+    int32_t has_median_fusion_observations;
+    float median_fusion_observations;
+    int32_t has_median_supporting_views;
+    float median_supporting_views;
+    int32_t has_median_photometric_error;
+    float median_photometric_error;
+    int32_t has_search_min_depth;
+    float search_min_depth;
+    int32_t has_search_max_depth;
+    float search_max_depth;
+    /* dense.rs:136-138 (reference_view_limit is decided by the Rust budget plan) */
+    int32_t has_reference_view_limit;
+    int32_t pad1;
+    uint64_t reference_view_limit;
+} v3d_dense_stats;
+
+/* DenseReferenceAttemptStats (dense.rs:63-80). */
+typedef struct v3d_reference_attempt {
+    uint64_t reference_frame;
+    int32_t attempted;
+    int32_t accepted;
+    int32_t has_skip_reason;
+    int32_t pad0;
+    char skip_reason[V3D_SKIP_REASON_BYTES];
+    uint64_t sampled_pixels;
+    uint64_t accepted_points;
+    uint64_t reciprocal_checked_points;
+    uint64_t reciprocal_rejected_points;
+    uint64_t reciprocal_consistent_points;
+    uint64_t surface_completion_proposals;
+    uint64_t surface_completed_points;
+    uint64_t surface_completion_rejected_texture;
+    uint64_t surface_completion_rejected_cross_view;
+    uint64_t surface_completion_rejected_reciprocal;
+    uint64_t surface_completion_rejected_fusion;
+    uint64_t surface_completion_rejected_footprint;
+} v3d_reference_attempt;
+
+/* DenseReferencePatchStats (dense.rs:83-97). */
+typedef struct v3d_reference_patch {
+    uint64_t reference_frame;
+    uint64_t n_source_frames;
+    const uint64_t* source_frames;
+    uint64_t primary_start;
+    uint64_t primary_points;
+    uint64_t completion_start;
+    uint64_t completed_points;
+    uint64_t sampled_pixels;
+    uint64_t accepted_points;
+    uint64_t reciprocal_consistent_points;
+    uint64_t grid_stride;
+    uint32_t grid_border;
+    int32_t has_search_min_depth;
+    float search_min_depth;
+    int32_t has_search_max_depth;
+    float search_max_depth;
+    int32_t pad0;
+} v3d_reference_patch;
+
+/* DenseAnalysis (dense_legacy.rs:62-68; dense.rs:142-148).  All arrays are
+ * owned by the library; release with v3d_dense_result_free(). */
+typedef struct v3d_dense_result {
+    v3d_dense_stats stats;
+    uint64_t n_source_frames;
+    uint64_t* source_frames;
+    uint64_t n_points;
+    v3d_point* points;
+    v3d_grid_site* grid_sites;
+    v3d_point_attributes* point_attributes;
+    /* Multi-reference fields of dense.rs (empty for the per-reference pass). */
+    uint64_t n_reference_frames;
+    uint64_t* reference_frames;
+    uint64_t n_attempts;
+    v3d_reference_attempt* attempts;
+    uint64_t n_patches;
+    v3d_reference_patch* patches;
+    void* internal;
+} v3d_dense_result;
+
+/* MeshTriangle (mesh_legacy.rs:18-23). */
+typedef struct v3d_mesh_triangle {
+    uint64_t a, b, c;
+    float confidence;
+    uint32_t pad;
+} v3d_mesh_triangle;
+
+/* MeshStats (mesh_legacy.rs:26-37) and MeshReferencePatchStats (mesh.rs:15-27). */
+typedef struct v3d_mesh_stats {
+    int32_t attempted;
+    int32_t has_skip_reason;
+    char skip_reason[V3D_SKIP_REASON_BYTES];
+    int32_t has_reference_frame;
+    int32_t pad0;
+    uint64_t reference_frame;
+    uint64_t point_count;             /* mesh.rs patch stats only */
+    uint64_t grid_vertices;
+    uint64_t rejected_grid_vertices;
+    uint64_t candidate_cells;
+    uint64_t candidate_triangles;
+    uint64_t accepted_triangles;
+    uint64_t rejected_discontinuities;
+    uint64_t rejected_degenerate;
+} v3d_mesh_stats;
+
+typedef struct v3d_mesh_result {
+    v3d_mesh_stats stats;
+    uint64_t n_triangles;
+    v3d_mesh_triangle* triangles;
+    uint64_t n_reference_frames;
+    uint64_t* reference_frames;
+    uint64_t n_patches;
+    v3d_mesh_stats* patches;
+    void* internal;
+} v3d_mesh_result;
+
+/* The subset of DenseStats the mesh stage reads (mesh_legacy.rs:160-199;
+ * mesh.rs:84-144). */
+typedef struct v3d_mesh_dense_input {
+    int32_t attempted;
+    int32_t has_reference_frame;
+    uint64_t reference_frame;
+    uint64_t grid_stride;
+    uint32_t grid_border;
+    uint32_t pad0;
+    uint64_t n_patches;                  /* 0: single legacy call (mesh.rs:84-99) */
+    const v3d_reference_patch* patches;  /* reference patches of a multi-reference run */
+} v3d_mesh_dense_input;
+
+/* Cooperative cancellation (reconstruction/control.rs:35-57): polled where the
+ * reference polls; nonzero means canceled, and cancellation is sticky. */
+typedef int32_t (*v3d_cancel_fn)(void* user_data);
+
+typedef struct v3d_context v3d_context;
+
+/* ---- library / context ------------------------------------------------- */
+int32_t v3d_abi_version(void);
+const char* v3d_status_text(int32_t status);
+const char* v3d_skip_reason_text(int32_t skip_code);
+const char* v3d_last_error(const v3d_context* ctx);
+
+/* Create a context on CUDA device `device`: one stream plus growable device
+ * arenas sized on first use.  Returns V3D_ERR_NO_DEVICE without a GPU (there
+ * is no CPU fallback). */
+int32_t v3d_context_create(int32_t device, v3d_context** out);
+void v3d_context_destroy(v3d_context* ctx);
+
+/* Profile presets: the reference constants (dense_legacy.rs:6-21), and the
+ * project-defined ZNCC profile for the given window radius, plane count,
+ * source-view cap and fixed grid stride. */
+void v3d_profile_reference(v3d_profile* out);
+void v3d_profile_zncc(v3d_profile* out, int32_t patch_radius, int32_t depth_hypotheses,
+                      int32_t max_source_views, int32_t grid_stride);
+
+/* grid_stride (dense.rs:215-218). */
+uint64_t v3d_grid_stride(uint32_t width, uint32_t height, int32_t fine_grid);
+
+/* ---- dense pass ---------------------------------------------------------- */
+
+/* legacy::estimate_depth_points_with_control (dense_legacy.rs:149-470):
+ * one reference pass — reference and source selection, the depth sweep with
+ * photometric and ambiguity gates, the reciprocal source-view check, fusion,
+ * confidence and two surface-completion passes.  `sparse_xyz` holds
+ * n_sparse world points as x,y,z doubles. */
+int32_t v3d_estimate_depth_points_with_control(
+    v3d_context* ctx,
+    const v3d_frame* frames, uint64_t n_frames,
+    const v3d_camera* cameras, uint64_t n_cameras,
+    const double* sparse_xyz, uint64_t n_sparse,
+    double focal, int32_t fine_grid,
+    const v3d_profile* profile,
+    v3d_cancel_fn cancel, void* cancel_user,
+    v3d_dense_result* out);
+
+/* reconstruct_reference_patch (dense.rs:674-747) for each camera index in
+ * `camera_indices`, batched on the device.  out[i] receives the remapped
+ * pass of camera_indices[i]; `present[i]` is set to 0 where the reference
+ * returns None (fewer than 8 landmarks visible in that camera), else 1.
+ * Frames are uploaded once per call and shared by every reference. */
+int32_t v3d_reconstruct_reference_patches(
+    v3d_context* ctx,
+    const v3d_frame* frames, uint64_t n_frames,
+    const v3d_camera* cameras, uint64_t n_cameras,
+    const double* sparse_xyz, uint64_t n_sparse,
+    double focal, int32_t fine_grid,
+    const v3d_profile* profile,
+    const uint64_t* camera_indices, uint64_t n_references,
+    v3d_cancel_fn cancel, void* cancel_user,
+    v3d_dense_result* out, int32_t* present);
+
+/* estimate_depth_points_limited (dense.rs:250-330): the multi-reference plan
+ * (at most 6 attempts, `reference_views` accepted patches), the legacy
+ * fallback, attempt merging and patch concatenation.  `omitted_references`
+ * receives the second tuple element (a further candidate remained). */
+int32_t v3d_estimate_depth_points_limited(
+    v3d_context* ctx,
+    const v3d_frame* frames, uint64_t n_frames,
+    const v3d_camera* cameras, uint64_t n_cameras,
+    const double* sparse_xyz, uint64_t n_sparse,
+    double focal, uint64_t reference_views, int32_t fine_grid,
+    const v3d_profile* profile,
+    v3d_cancel_fn cancel, void* cancel_user,
+    v3d_dense_result* out, int32_t* omitted_references);
+
+/* has_distributed_landmarks (dense.rs:165-213), polling `cancel` once per
+ * 256-landmark chunk like the reference. */
+int32_t v3d_has_distributed_landmarks(
+    const v3d_frame* frames, uint64_t n_frames,
+    const v3d_camera* cameras, uint64_t n_cameras,
+    const double* sparse_xyz, uint64_t n_sparse,
+    double focal, v3d_cancel_fn cancel, void* cancel_user);
+
+void v3d_dense_result_free(v3d_dense_result* result);
+
+/* ---- diagnostics ----------------------------------------------------------- */
+
+/* Device-side account of the last dense call on `ctx`: the CUDA-event time of
+ * its kernels (uploads and read-back excluded) and how many kernels it
+ * launched.  No counterpart in the reference. */
+typedef struct v3d_run_info {
+    double device_ms;
+    uint64_t kernel_launches;
+    uint64_t grid_sites;      /* all grid sites of the references that ran */
+    uint64_t plane_view_units;/* sum over references of sites x planes x source views */
+    double sweep_ms;          /* depth sweep kernel */
+    double reciprocal_ms;     /* the primary reciprocal-check launch */
+    double completion_ms;     /* both surface-completion passes, reciprocal included */
+    uint64_t reciprocal_plane_evaluations; /* single-view hypotheses evaluated, all passes */
+    uint64_t candidates;      /* primary + completion candidates checked */
+} v3d_run_info;
+
+int32_t v3d_last_run_info(const v3d_context* ctx, v3d_run_info* out);
+
+/* Per-site outcome of the depth sweep (dense_legacy.rs:272-362) before the
+ * reciprocal check: status 1 = below the contrast gate, 2 = no hypothesis had
+ * a passing source view, 3 = photometric or ambiguity gate rejected,
+ * 4 = accepted; plane is the chosen hypothesis index. */
+typedef struct v3d_site_record {
+    uint32_t x, y;
+    int32_t status;
+    int32_t plane;
+    int32_t support;
+    int32_t pad;
+    double error;
+    double margin;
+} v3d_site_record;
+
+/* Runs the planning and the depth sweep of
+ * v3d_estimate_depth_points_with_control and returns the per-site records in
+ * raster order (capacity >= rows * columns of the grid, *n_sites receives the
+ * count; with out == NULL only the count is returned).  A diagnostic for parity measurements; it has no counterpart in the
+ * reference, whose sweep keeps these values internal. */
+int32_t v3d_debug_sweep(
+    v3d_context* ctx,
+    const v3d_frame* frames, uint64_t n_frames,
+    const v3d_camera* cameras, uint64_t n_cameras,
+    const double* sparse_xyz, uint64_t n_sparse,
+    double focal, int32_t fine_grid,
+    const v3d_profile* profile,
+    v3d_site_record* out, uint64_t capacity, uint64_t* n_sites);
+
+/* ---- reference-grid triangle gates -------------------------------------- */
+
+/* mesh::reconstruct_dense_mesh_with_control (mesh.rs:74-220); with
+ * dense->n_patches == 0 this is legacy::reconstruct_dense_mesh_samples
+ * (mesh_legacy.rs:150-358) over all points. */
+int32_t v3d_reconstruct_dense_mesh_with_control(
+    v3d_context* ctx,
+    const v3d_point* points, uint64_t n_points,
+    const v3d_grid_site* grid_sites, uint64_t n_grid_sites,
+    const v3d_mesh_dense_input* dense,
+    const v3d_camera* cameras, uint64_t n_cameras,
+    uint32_t width, uint32_t height, double focal,
+    v3d_cancel_fn cancel, void* cancel_user,
+    v3d_mesh_result* out);
+
+void v3d_mesh_result_free(v3d_mesh_result* result);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* V3D_DENSE_H */

@@ -1,0 +1,159 @@
+"""ctypes wrapper of the CPU oracle (oracle/_build/liboracle_v3d.so).
+
+Test infrastructure only: the parity tests use it as the checker, bench.py
+uses it as the timed CPU baseline.  Its functions take the same Python inputs
+as ``v3d.dense`` and return the same result objects.
+"""
+import ctypes as C
+import os
+
+from v3d import abi, types
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB = os.path.join(ROOT, "oracle", "_build", "liboracle_v3d.so")
+
+_P = C.POINTER
+
+
+class Oracle:
+    def __init__(self, path=LIB):
+        self.lib = C.CDLL(path)
+        L = self.lib
+        frames_args = [_P(abi.Frame), C.c_uint64, _P(abi.Camera), C.c_uint64,
+                       _P(C.c_double), C.c_uint64, C.c_double]
+        L.v3do_estimate_depth_points_with_control.argtypes = frames_args + [
+            C.c_int32, _P(abi.Profile), abi.CANCEL_FN, C.c_void_p, _P(abi.DenseResult)]
+        L.v3do_estimate_depth_points_with_control.restype = C.c_int32
+        L.v3do_reconstruct_reference_patches.argtypes = frames_args + [
+            C.c_int32, _P(abi.Profile), _P(C.c_uint64), C.c_uint64, C.c_int32,
+            _P(abi.DenseResult), _P(C.c_int32)]
+        L.v3do_reconstruct_reference_patches.restype = C.c_int32
+        L.v3do_estimate_depth_points_limited.argtypes = frames_args + [
+            C.c_uint64, C.c_int32, _P(abi.Profile), abi.CANCEL_FN, C.c_void_p,
+            _P(abi.DenseResult), _P(C.c_int32)]
+        L.v3do_estimate_depth_points_limited.restype = C.c_int32
+        L.v3do_has_distributed_landmarks.argtypes = frames_args + [abi.CANCEL_FN, C.c_void_p]
+        L.v3do_has_distributed_landmarks.restype = C.c_int32
+        L.v3do_reconstruct_dense_mesh_with_control.argtypes = [
+            _P(abi.Point), C.c_uint64, _P(abi.GridSite), C.c_uint64, _P(abi.MeshDenseInput),
+            _P(abi.Camera), C.c_uint64, C.c_uint32, C.c_uint32, C.c_double, abi.CANCEL_FN,
+            C.c_void_p, _P(abi.MeshResult)]
+        L.v3do_reconstruct_dense_mesh_with_control.restype = C.c_int32
+        L.v3do_dense_result_free.argtypes = [_P(abi.DenseResult)]
+        L.v3do_mesh_result_free.argtypes = [_P(abi.MeshResult)]
+        L.v3do_selftest.argtypes = [C.c_char_p, C.c_uint64, _P(C.c_int32)]
+        L.v3do_selftest.restype = C.c_int32
+        L.v3do_patch_error.argtypes = [_P(abi.Profile), _P(abi.Camera), _P(abi.Camera),
+                                       _P(abi.Frame), _P(abi.Frame), C.c_double, C.c_double,
+                                       C.c_double, C.c_double, _P(C.c_double)]
+        L.v3do_patch_error.restype = C.c_int32
+        L.v3do_grid_stride.argtypes = [C.c_uint32, C.c_uint32, C.c_int32]
+        L.v3do_grid_stride.restype = C.c_uint64
+        L.v3do_max_threads.restype = C.c_int32
+        L.v3do_debug_sweep.argtypes = frames_args + [C.c_int32, _P(abi.Profile),
+                                                     _P(abi.SiteRecord), C.c_uint64,
+                                                     _P(C.c_uint64)]
+        L.v3do_debug_sweep.restype = C.c_int32
+
+    def selftest(self):
+        buf = C.create_string_buffer(1 << 16)
+        checks = C.c_int32()
+        failures = self.lib.v3do_selftest(buf, len(buf), C.byref(checks))
+        return failures, checks.value, buf.value.decode()
+
+    def max_threads(self):
+        return self.lib.v3do_max_threads()
+
+    def estimate_depth_points_with_control(self, frames, cameras, sparse_points, focal,
+                                           fine_grid=False, control=None, profile=None):
+        inp = types.Inputs(frames, cameras, sparse_points)
+        fn, _keep = types.cancel_callback(control)
+        out = abi.DenseResult()
+        st = self.lib.v3do_estimate_depth_points_with_control(
+            inp.frames, inp.n_frames, inp.cameras, inp.n_cameras, inp.sparse, inp.n_sparse,
+            float(focal), int(fine_grid), C.byref(profile), fn, None, C.byref(out))
+        if st < 0:
+            raise ValueError("oracle rejected the inputs (status %d)" % st)
+        try:
+            return types.dense_from_result(out, st)
+        finally:
+            self.lib.v3do_dense_result_free(C.byref(out))
+
+    def reconstruct_reference_patches(self, frames, cameras, sparse_points, focal,
+                                      camera_indices, profile, fine_grid=False, threads=1):
+        inp = types.Inputs(frames, cameras, sparse_points)
+        n = len(camera_indices)
+        idx = (C.c_uint64 * max(n, 1))(*camera_indices)
+        outs = (abi.DenseResult * max(n, 1))()
+        present = (C.c_int32 * max(n, 1))()
+        st = self.lib.v3do_reconstruct_reference_patches(
+            inp.frames, inp.n_frames, inp.cameras, inp.n_cameras, inp.sparse, inp.n_sparse,
+            float(focal), int(fine_grid), C.byref(profile), idx, n, int(threads), outs, present)
+        if st < 0:
+            raise ValueError("oracle rejected the inputs (status %d)" % st)
+        res = []
+        for i in range(n):
+            res.append(types.dense_from_result(outs[i]) if present[i] else None)
+            self.lib.v3do_dense_result_free(C.byref(outs[i]))
+        return res
+
+    def estimate_depth_points_limited(self, frames, cameras, sparse_points, focal,
+                                      reference_views, fine_grid, profile, control=None):
+        inp = types.Inputs(frames, cameras, sparse_points)
+        fn, _keep = types.cancel_callback(control)
+        out = abi.DenseResult()
+        omitted = C.c_int32()
+        st = self.lib.v3do_estimate_depth_points_limited(
+            inp.frames, inp.n_frames, inp.cameras, inp.n_cameras, inp.sparse, inp.n_sparse,
+            float(focal), int(reference_views), int(fine_grid), C.byref(profile), fn, None,
+            C.byref(out), C.byref(omitted))
+        if st < 0:
+            raise ValueError("oracle rejected the inputs (status %d)" % st)
+        try:
+            return types.dense_from_result(out, st), bool(omitted.value)
+        finally:
+            self.lib.v3do_dense_result_free(C.byref(out))
+
+    def has_distributed_landmarks(self, frames, cameras, sparse_points, focal, control=None):
+        inp = types.Inputs(frames, cameras, sparse_points)
+        fn, _keep = types.cancel_callback(control)
+        return bool(self.lib.v3do_has_distributed_landmarks(
+            inp.frames, inp.n_frames, inp.cameras, inp.n_cameras, inp.sparse, inp.n_sparse,
+            float(focal), fn, None))
+
+    def reconstruct_dense_mesh_with_control(self, points, grid_sites, stats, cameras, width,
+                                            height, focal, control=None):
+        mi = types.MeshInputs(points, grid_sites, stats)
+        cams = types.Inputs([], cameras, [])
+        fn, _keep = types.cancel_callback(control)
+        out = abi.MeshResult()
+        self.lib.v3do_reconstruct_dense_mesh_with_control(
+            *mi.args(), cams.cameras, cams.n_cameras, int(width), int(height), float(focal),
+            fn, None, C.byref(out))
+        try:
+            return types.mesh_from_result(out)
+        finally:
+            self.lib.v3do_mesh_result_free(C.byref(out))
+
+    def debug_sweep(self, frames, cameras, sparse_points, focal, fine_grid=False, profile=None):
+        inp = types.Inputs(frames, cameras, sparse_points)
+        n = C.c_uint64()
+        cap = 1 << 22
+        buf = (abi.SiteRecord * cap)()
+        st = self.lib.v3do_debug_sweep(inp.frames, inp.n_frames, inp.cameras, inp.n_cameras,
+                                       inp.sparse, inp.n_sparse, float(focal), int(fine_grid),
+                                       C.byref(profile), buf, cap, C.byref(n))
+        if st == abi.SKIPPED:
+            return None
+        if st < 0:
+            raise ValueError("oracle rejected the inputs (status %d)" % st)
+        return types.site_records(buf, n.value)
+
+    def patch_error(self, profile, ref_cam, src_cam, ref_frame, src_frame, x, y, depth, focal):
+        inp = types.Inputs([ref_frame, src_frame], [ref_cam, src_cam], [])
+        cost = C.c_double()
+        st = self.lib.v3do_patch_error(C.byref(profile), C.byref(inp.cameras[0]),
+                                       C.byref(inp.cameras[1]), C.byref(inp.frames[0]),
+                                       C.byref(inp.frames[1]), x, y, depth, focal,
+                                       C.byref(cost))
+        return cost.value if st == 0 else None

@@ -1,0 +1,134 @@
+// Host-side planning and batch execution of the dense pass.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/v3d_dense.h"
+
+namespace v3d {
+
+struct HVec3 {
+    double x, y, z;
+};
+
+struct HCamera {
+    size_t frame_index;
+    double R[9];  // row-major world->camera
+    double t[3];
+};
+
+// Planned inputs of one per-reference pass (dense_legacy.rs:157-256).
+struct RefPlan {
+    bool skipped = false;
+    int skip_code = 0;
+    std::string skip_reason;
+    bool have_reference = false;
+    size_t reference_frame = 0;           // caller-visible frame index
+    std::vector<size_t> source_frames;    // caller-visible frame indices
+    size_t ref_slot = 0;                  // index into the call's frame array
+    std::vector<size_t> src_slots;
+    HCamera ref_cam{};
+    std::vector<HCamera> src_cams;
+    std::vector<double> src_min, src_max;
+    double search_min = 0, search_max = 0;
+    uint32_t width = 0, height = 0, stride = 0, border = 0, nx = 0, ny = 0;
+};
+
+// One pass's output (dense_legacy.rs:62-68 DenseAnalysis with DenseStats).
+struct PassResult {
+    RefPlan plan;
+    std::vector<v3d_point> points;
+    std::vector<v3d_grid_site> sites;
+    std::vector<v3d_point_attributes> attrs;
+    v3d_dense_stats stats{};
+};
+
+struct Inputs {
+    const v3d_frame* frames = nullptr;
+    size_t n_frames = 0;
+    std::vector<HCamera> cameras;
+    std::vector<HVec3> sparse;
+    double focal = 0;
+};
+
+struct CancelPoll {
+    v3d_cancel_fn fn = nullptr;
+    void* user = nullptr;
+    bool canceled = false;
+    bool poll() {
+        if (!canceled && fn && fn(user)) canceled = true;
+        return canceled;
+    }
+};
+
+// ---- planning (host_plan.cpp) ----
+uint32_t reference_grid_stride(uint32_t w, uint32_t h, bool fine);
+HVec3 camera_center(const HCamera& c);
+bool project_h(const HCamera& c, HVec3 p, uint32_t w, uint32_t h, double focal, HVec3& out);
+HVec3 unproject_h(const HCamera& c, double x, double y, double depth, uint32_t w, uint32_t h,
+                  double focal);
+bool in_image_bounds_h(double x, double y, uint32_t w, uint32_t h);
+
+// dense_legacy.rs:157-256 on an explicit view list: `cams[i]` with frame slots
+// `slot_of_frame_index(cams[i].frame_index)`.
+RefPlan plan_legacy(const v3d_profile& prof, const v3d_frame* frames, size_t n_frames,
+                    const std::vector<HCamera>& cams, const std::vector<HVec3>& sparse,
+                    double focal, bool fine_grid, const std::vector<size_t>* slot_map);
+
+// dense.rs:674-747: remap so the reference comes first; `present` is false
+// where the reference returns None.
+RefPlan plan_reference_patch(const v3d_profile& prof, const Inputs& in, size_t camera_index,
+                             bool fine_grid, bool& present);
+
+std::vector<size_t> reference_candidate_order(const Inputs& in);
+bool has_distributed_landmarks(const Inputs& in, CancelPoll& cancel);
+
+void skip_result(PassResult& r, int code, const std::string& reason);
+
+}  // namespace v3d
+
+struct v3d_context {
+    int device = 0;
+    void* stream = nullptr;  // cudaStream_t
+    std::mutex mu;
+    std::string last_error;
+    // growable device arena
+    void* arena = nullptr;
+    size_t arena_bytes = 0;
+    // pinned host staging for results
+    void* pinned = nullptr;
+    size_t pinned_bytes = 0;
+    // account of the last run_batch (v3d_last_run_info)
+    float last_ms = 0.f;
+    uint64_t last_launches = 0;
+    uint64_t last_sites = 0;
+    uint64_t last_units = 0;
+    float last_sweep_ms = 0.f, last_recip_ms = 0.f, last_completion_ms = 0.f;
+    uint64_t last_recip_evals = 0, last_candidates = 0;
+};
+
+namespace v3d {
+// ---- execution (pipeline.cpp) ----
+// Runs every non-skipped plan of `plans` as one device batch and fills
+// `results` (same order).  Returns a v3d_status.
+int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* frames,
+                  size_t n_frames, double focal, const std::vector<RefPlan>& plans,
+                  std::vector<PassResult>& results);
+
+// The sweep of one planned pass alone, as per-site records (v3d_debug_sweep).
+int32_t run_sweep_records(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* frames,
+                          size_t n_frames, double focal, const RefPlan& plan,
+                          std::vector<v3d_site_record>& out);
+
+// One legacy mesh pass (mesh_legacy.rs:200-358) over points[map[i]] (every
+// point when `map` is empty); triangle indices refer to the mapped list.
+int32_t run_mesh_patch(v3d_context* ctx, const v3d_point* points, const v3d_grid_site* sites,
+                       const std::vector<uint32_t>& map, size_t n_points, const HCamera& cam,
+                       uint32_t width, uint32_t height, uint32_t border, uint32_t stride,
+                       double focal, CancelPoll& cancel, v3d_mesh_stats& stats,
+                       std::vector<v3d_mesh_triangle>& tris, bool& canceled);
+}  // namespace v3d

@@ -1,0 +1,584 @@
+// Batched execution of planned reference passes on one CUDA stream.
+//
+// HBM layout of a batch (one arena, 256-byte aligned sub-buffers):
+//   frames      the caller's frames as handed in (RGBA8 or gray f32/f16/bf16),
+//               plus a u8 luma plane per RGBA8 frame; every source of every
+//               reference reads these shared copies
+//   refs        DevReference per reference (cameras, envelopes, homography parts)
+//   per site    SiteRank, status, occupancy and proposal records, flat over
+//               all references (site_off gives each reference's range)
+//   per cand    candidates, 16 reciprocal slots, fused output, status
+//   pool        accepted points: primaries, then completion pass 1, then pass 2,
+//               each segment in (reference, raster) order
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <stdexcept>
+
+#include "host.hpp"
+#include "pass_kernels.cuh"
+
+namespace v3d {
+
+namespace {
+
+struct Carver {
+    size_t off = 0;
+    template <class T>
+    size_t take(size_t count) {
+        off = (off + 255) & ~size_t(255);
+        size_t at = off;
+        off += count * sizeof(T);
+        return at;
+    }
+};
+
+int storage_of(int format) {
+    switch (format) {
+        case V3D_PIXEL_RGBA8: return kU8;
+        case V3D_PIXEL_GRAY_F32: return kF32;
+        case V3D_PIXEL_GRAY_F16: return kF16;
+        case V3D_PIXEL_GRAY_BF16: return kBF16;
+    }
+    return -1;
+}
+
+size_t bytes_per_pixel(int format) {
+    return format == V3D_PIXEL_RGBA8 || format == V3D_PIXEL_GRAY_F32 ? 4 : 2;
+}
+
+// 3x3 products in f64 for the fast policy's homography parts.
+void mat_mul(const double* a, const double* b, double* out) {
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            double s = 0;
+            for (int k = 0; k < 3; ++k) s += a[i * 3 + k] * b[k * 3 + j];
+            out[i * 3 + j] = s;
+        }
+}
+
+// Parts of the homography that maps pixel p of camera `from` at depth d along
+// `from`'s optical axis to camera `to`:  A p + (1/d) b  (homogeneous pixel).
+void homography_parts(const HCamera& from, uint32_t fw, uint32_t fh, const HCamera& to,
+                      uint32_t tw, uint32_t th, double f, float* A_out, float* b_out) {
+    double Rt[9];  // from.R^T
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) Rt[i * 3 + j] = from.R[j * 3 + i];
+    double M[9];
+    mat_mul(to.R, Rt, M);
+    double c[3];
+    for (int i = 0; i < 3; ++i)
+        c[i] = to.t[i] - (M[i * 3] * from.t[0] + M[i * 3 + 1] * from.t[1] + M[i * 3 + 2] * from.t[2]);
+    const double Kinv[9] = {1.0 / f, 0, -(fw * 0.5) / f, 0, 1.0 / f, -(fh * 0.5) / f, 0, 0, 1};
+    const double K[9] = {f, 0, tw * 0.5, 0, f, th * 0.5, 0, 0, 1};
+    double MK[9], A[9];
+    mat_mul(M, Kinv, MK);
+    mat_mul(K, MK, A);
+    for (int i = 0; i < 9; ++i) A_out[i] = static_cast<float>(A[i]);
+    for (int i = 0; i < 3; ++i)
+        b_out[i] = static_cast<float>(K[i * 3] * c[0] + K[i * 3 + 1] * c[1] + K[i * 3 + 2] * c[2]);
+}
+
+void set_cam(DevCamera& d, const HCamera& h) {
+    std::memcpy(d.R, h.R, sizeof(d.R));
+    std::memcpy(d.t, h.t, sizeof(d.t));
+}
+
+bool grow(void** ptr, size_t* have, size_t need, bool pinned) {
+    if (*have >= need) return true;
+    size_t cap = std::max(need, *have + *have / 2);
+    if (*ptr) {
+        if (pinned)
+            cudaFreeHost(*ptr);
+        else
+            cudaFree(*ptr);
+        *ptr = nullptr;
+        *have = 0;
+    }
+    cudaError_t e = pinned ? cudaMallocHost(ptr, cap) : cudaMalloc(ptr, cap);
+    if (e != cudaSuccess) {
+        *ptr = nullptr;
+        cudaGetLastError();
+        return false;
+    }
+    *have = cap;
+    return true;
+}
+
+struct Seg {
+    uint32_t begin, end;
+};
+
+double median_of(std::vector<double>& v) {
+    size_t k = v.size() / 2;  // round((n - 1) * 0.5)
+    std::nth_element(v.begin(), v.begin() + k, v.end());
+    return v[k];
+}
+
+}  // namespace
+
+#define V3D_CK(call)                                              \
+    do {                                                          \
+        cudaError_t e_ = (call);                                  \
+        if (e_ != cudaSuccess) {                                  \
+            ctx->last_error = std::string(#call) + ": " + cudaGetErrorString(e_); \
+            return e_ == cudaErrorMemoryAllocation ? V3D_ERR_OUT_OF_MEMORY : V3D_ERR_CUDA; \
+        }                                                         \
+    } while (0)
+
+namespace {
+
+// Device state of one batch after upload: the arena carve-out, the
+// DevReference array and the kernel-facing BatchDev.
+struct Prepared {
+    std::vector<size_t> active;
+    size_t n_active = 0;
+    uint64_t total = 0, cap = 1;
+    uint32_t max_nx = 0, max_ny = 0, stride0 = 0;
+    bool tiled = false;
+    BatchDev b{};
+    uint32_t* d_siteref = nullptr;
+    SiteRank* d_rank = nullptr;
+    uint8_t* d_status = nullptr;
+    RefCounters* d_ctr = nullptr;
+    void* d_scratch = nullptr;
+    uint32_t* d_idx = nullptr;
+    Cand* d_cands = nullptr;
+    uint8_t* d_cstat = nullptr;
+    RecipObs* d_obs = nullptr;
+    OutPoint* d_fused = nullptr;
+    OutPoint* d_pool = nullptr;
+    int32_t* d_occ = nullptr;
+    uint8_t* d_pstat = nullptr;
+    Cand* d_prop = nullptr;
+    uint32_t* d_counts = nullptr;
+};
+
+int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* frames,
+                size_t n_frames, double focal, const std::vector<RefPlan>& plans,
+                const std::vector<size_t>& active, bool sweep_only, Prepared& P) {
+    cudaStream_t stream = static_cast<cudaStream_t>(ctx->stream);
+    P.active = active;
+
+    // frames touched by the batch, all in one storage format
+    std::vector<int64_t> dev_of(n_frames, -1);
+    std::vector<size_t> used;
+    int format = -1;
+    auto use = [&](size_t slot) -> bool {
+        if (slot >= n_frames) return false;
+        if (dev_of[slot] < 0) {
+            dev_of[slot] = static_cast<int64_t>(used.size());
+            used.push_back(slot);
+        }
+        if (format < 0) format = frames[slot].format;
+        return frames[slot].format == format && frames[slot].data != nullptr;
+    };
+    for (size_t a : active) {
+        if (!use(plans[a].ref_slot)) {
+            ctx->last_error = "frames of one call must share a pixel format and carry data";
+            return V3D_ERR_INVALID_ARGUMENT;
+        }
+        for (size_t s : plans[a].src_slots)
+            if (!use(s)) {
+                ctx->last_error = "frames of one call must share a pixel format and carry data";
+                return V3D_ERR_INVALID_ARGUMENT;
+            }
+    }
+    const int storage = storage_of(format);
+    if (storage < 0) {
+        ctx->last_error = "unknown pixel format";
+        return V3D_ERR_INVALID_ARGUMENT;
+    }
+    const bool rgba = format == V3D_PIXEL_RGBA8;
+    const size_t n_active = active.size();
+    std::vector<uint64_t> site_off(n_active + 1, 0);
+    uint32_t max_nx = 0, max_ny = 0;
+    bool uniform_stride = true;
+    for (size_t k = 0; k < n_active; ++k) {
+        const RefPlan& p = plans[active[k]];
+        site_off[k + 1] = site_off[k] + static_cast<uint64_t>(p.nx) * p.ny;
+        max_nx = std::max(max_nx, p.nx);
+        max_ny = std::max(max_ny, p.ny);
+        uniform_stride = uniform_stride && p.stride == plans[active[0]].stride;
+    }
+    const uint64_t total = site_off[n_active];
+    const uint64_t cap = std::max<uint64_t>(total, 1);
+    P.n_active = n_active;
+    P.total = total;
+    P.cap = cap;
+    P.max_nx = max_nx;
+    P.max_ny = max_ny;
+
+    // ---- arena layout ----
+    Carver cv;
+    std::vector<size_t> raw_off(used.size()), luma_off(used.size());
+    for (size_t u = 0; u < used.size(); ++u) {
+        const v3d_frame& f = frames[used[u]];
+        size_t px = static_cast<size_t>(f.width) * f.height;
+        raw_off[u] = cv.take<uint8_t>(px * bytes_per_pixel(format));
+        luma_off[u] = rgba ? cv.take<uint8_t>(px) : raw_off[u];
+    }
+    const size_t o_refs = cv.take<DevReference>(n_active);
+    const size_t o_siteoff = cv.take<uint64_t>(n_active + 1);
+    const size_t o_siteref = cv.take<uint32_t>(cap);
+    const size_t o_rank = cv.take<SiteRank>(cap);
+    const size_t o_status = cv.take<uint8_t>(cap);
+    const size_t o_ctr = cv.take<RefCounters>(n_active);
+    const uint64_t pc = sweep_only ? 1 : cap;  // pass buffers are not needed for the sweep alone
+    const size_t o_scratch = cv.take<uint8_t>(compaction_scratch_bytes(pc));
+    const size_t o_idx = cv.take<uint32_t>(pc);
+    const size_t o_cands = cv.take<Cand>(pc);
+    const size_t o_cstat = cv.take<uint8_t>(pc);
+    const size_t o_obs = cv.take<RecipObs>(pc * kMaxSources);
+    const size_t o_fused = cv.take<OutPoint>(pc);
+    const size_t o_pool = cv.take<OutPoint>(pc);
+    const size_t o_occ = cv.take<int32_t>(pc);
+    const size_t o_pstat = cv.take<uint8_t>(pc);
+    const size_t o_prop = cv.take<Cand>(pc);
+    const size_t o_counts = cv.take<uint32_t>(16);
+    const size_t arena_need = cv.off + 256;
+    if (!grow(&ctx->arena, &ctx->arena_bytes, arena_need, false)) {
+        ctx->last_error = "device arena allocation failed";
+        return V3D_ERR_OUT_OF_MEMORY;
+    }
+    char* base = static_cast<char*>(ctx->arena);
+    auto at = [&](size_t off) { return base + off; };
+
+    // ---- uploads ----
+    for (size_t u = 0; u < used.size(); ++u) {
+        const v3d_frame& f = frames[used[u]];
+        size_t px = static_cast<size_t>(f.width) * f.height;
+        V3D_CK(cudaMemcpyAsync(at(raw_off[u]), f.data, px * bytes_per_pixel(format),
+                               cudaMemcpyHostToDevice, stream));
+        if (rgba)
+            V3D_CK(launch_luma(reinterpret_cast<const uint8_t*>(at(raw_off[u])),
+                               reinterpret_cast<uint8_t*>(at(luma_off[u])), px, stream));
+    }
+    const size_t staging = sizeof(DevReference) * n_active + sizeof(uint64_t) * (n_active + 1);
+    if (!grow(&ctx->pinned, &ctx->pinned_bytes, staging, true)) {
+        ctx->last_error = "pinned staging allocation failed";
+        return V3D_ERR_OUT_OF_MEMORY;
+    }
+    DevReference* hrefs = static_cast<DevReference*>(ctx->pinned);
+    std::memset(hrefs, 0, sizeof(DevReference) * n_active);
+    for (size_t k = 0; k < n_active; ++k) {
+        const RefPlan& p = plans[active[k]];
+        DevReference& d = hrefs[k];
+        set_cam(d.cam, p.ref_cam);
+        size_t ru = static_cast<size_t>(dev_of[p.ref_slot]);
+        d.img = DevImage{at(luma_off[ru]), frames[p.ref_slot].width, frames[p.ref_slot].height};
+        d.rgba = rgba ? reinterpret_cast<const uint8_t*>(at(raw_off[ru])) : nullptr;
+        d.focal = focal;
+        d.search_min = p.search_min;
+        d.search_max = p.search_max;
+        d.border = p.border;
+        d.stride = p.stride;
+        d.nx = p.nx;
+        d.ny = p.ny;
+        d.n_src = static_cast<int32_t>(p.src_slots.size());
+        for (size_t j = 0; j < p.src_slots.size(); ++j) {
+            DevSource& s = d.src[j];
+            size_t su = static_cast<size_t>(dev_of[p.src_slots[j]]);
+            const v3d_frame& sf = frames[p.src_slots[j]];
+            set_cam(s.cam, p.src_cams[j]);
+            s.img = DevImage{at(luma_off[su]), sf.width, sf.height};
+            s.search_min = p.src_min[j];
+            s.search_max = p.src_max[j];
+            homography_parts(p.ref_cam, d.img.width, d.img.height, p.src_cams[j], sf.width,
+                             sf.height, focal, s.fwd_A, s.fwd_b);
+            homography_parts(p.src_cams[j], sf.width, sf.height, p.ref_cam, d.img.width,
+                             d.img.height, focal, s.bwd_A, s.bwd_b);
+        }
+    }
+    uint64_t* hoff = reinterpret_cast<uint64_t*>(hrefs + n_active);
+    std::memcpy(hoff, site_off.data(), sizeof(uint64_t) * (n_active + 1));
+    V3D_CK(cudaMemcpyAsync(at(o_refs), hrefs, sizeof(DevReference) * n_active,
+                           cudaMemcpyHostToDevice, stream));
+    V3D_CK(cudaMemcpyAsync(at(o_siteoff), hoff, sizeof(uint64_t) * (n_active + 1),
+                           cudaMemcpyHostToDevice, stream));
+
+    auto* d_siteref = P.d_siteref = reinterpret_cast<uint32_t*>(at(o_siteref));
+    P.d_rank = reinterpret_cast<SiteRank*>(at(o_rank));
+    auto* d_status = P.d_status = reinterpret_cast<uint8_t*>(at(o_status));
+    auto* d_ctr = P.d_ctr = reinterpret_cast<RefCounters*>(at(o_ctr));
+    P.d_scratch = at(o_scratch);
+    P.d_idx = reinterpret_cast<uint32_t*>(at(o_idx));
+    P.d_cands = reinterpret_cast<Cand*>(at(o_cands));
+    P.d_cstat = reinterpret_cast<uint8_t*>(at(o_cstat));
+    P.d_obs = reinterpret_cast<RecipObs*>(at(o_obs));
+    P.d_fused = reinterpret_cast<OutPoint*>(at(o_fused));
+    P.d_pool = reinterpret_cast<OutPoint*>(at(o_pool));
+    P.d_occ = reinterpret_cast<int32_t*>(at(o_occ));
+    P.d_pstat = reinterpret_cast<uint8_t*>(at(o_pstat));
+    P.d_prop = reinterpret_cast<Cand*>(at(o_prop));
+    auto* d_counts = P.d_counts = reinterpret_cast<uint32_t*>(at(o_counts));
+
+    V3D_CK(cudaMemsetAsync(d_status, 0, cap, stream));
+    V3D_CK(cudaMemsetAsync(d_ctr, 0, sizeof(RefCounters) * n_active, stream));
+    V3D_CK(cudaMemsetAsync(d_counts, 0, sizeof(uint32_t) * 16, stream));
+    V3D_CK(launch_site_ref(reinterpret_cast<const uint64_t*>(at(o_siteoff)),
+                           static_cast<int32_t>(n_active), total, d_siteref, stream));
+
+    BatchDev& b = P.b;
+    b.refs = reinterpret_cast<const DevReference*>(at(o_refs));
+    b.site_off = reinterpret_cast<const uint64_t*>(at(o_siteoff));
+    b.n_refs = static_cast<int32_t>(n_active);
+    b.storage = storage;
+    b.prof.cost = prof.cost;
+    b.prof.radius = prof.patch_radius;
+    b.prof.planes = prof.depth_hypotheses;
+    b.prof.pad = 0;
+    b.prof.min_contrast = prof.min_reference_contrast;
+    b.prof.max_error = prof.max_photometric_error;
+    b.prof.min_margin = prof.min_ambiguity_margin;
+    b.prof.margin_saturation = prof.depth_margin_saturation;
+    b.prof.error_scale = prof.error_confidence_scale;
+    b.prof.min_variance = prof.min_window_variance;
+    b.exact = prof.precision == V3D_PRECISION_EXACT64;
+
+    const uint32_t stride0 = plans[active[0]].stride;
+    const int W = 2 * prof.patch_radius + 1;
+    P.stride0 = stride0;
+    P.tiled = !b.exact && prof.cost == V3D_COST_ZNCC && uniform_stride && stride0 >= 1 &&
+              stride0 <= 4 && static_cast<int>(stride0) < W;
+    return V3D_OK;
+}
+
+}  // namespace
+
+int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* frames,
+                  size_t n_frames, double focal, const std::vector<RefPlan>& plans,
+                  std::vector<PassResult>& results) {
+    cudaStream_t stream = static_cast<cudaStream_t>(ctx->stream);
+    results.assign(plans.size(), PassResult{});
+    std::vector<size_t> active;
+    for (size_t i = 0; i < plans.size(); ++i) {
+        results[i].plan = plans[i];
+        if (plans[i].skipped)
+            skip_result(results[i], plans[i].skip_code, plans[i].skip_reason);
+        else
+            active.push_back(i);
+    }
+    if (active.empty()) return V3D_OK;
+    Prepared P;
+    int32_t pst = prepare(ctx, prof, frames, n_frames, focal, plans, active, false, P);
+    if (pst != V3D_OK) return pst;
+    const size_t n_active = P.n_active;
+    const uint64_t total = P.total, cap = P.cap;
+    const BatchDev& b = P.b;
+    uint32_t* d_siteref = P.d_siteref;
+    SiteRank* d_rank = P.d_rank;
+    uint8_t* d_status = P.d_status;
+    RefCounters* d_ctr = P.d_ctr;
+    void* d_scratch = P.d_scratch;
+    uint32_t* d_idx = P.d_idx;
+    Cand* d_cands = P.d_cands;
+    uint8_t* d_cstat = P.d_cstat;
+    RecipObs* d_obs = P.d_obs;
+    OutPoint* d_fused = P.d_fused;
+    OutPoint* d_pool = P.d_pool;
+    int32_t* d_occ = P.d_occ;
+    uint8_t* d_pstat = P.d_pstat;
+    Cand* d_prop = P.d_prop;
+    uint32_t* c_cand = P.d_counts + 0;
+    uint32_t* c_acc = P.d_counts + 1;
+    uint32_t* c_pool = P.d_counts + 2;
+    uint32_t* c_seg = P.d_counts + 3;  // [3] segment ends
+    const uint32_t max_nx = P.max_nx, max_ny = P.max_ny, stride0 = P.stride0;
+    const bool tiled = P.tiled;
+
+    cudaEvent_t ev0, ev1;
+    cudaEventCreate(&ev0);
+    cudaEventCreate(&ev1);
+    cudaEventRecord(ev0, stream);
+    // kernel launches enqueued below: sweep, 2 x 3 compaction kernels,
+    // candidates, reciprocal, fuse, append (2), occupancy (2), then per
+    // completion pass propose, compaction (3), gather, reciprocal, fuse,
+    // compaction (3), append (2), occupancy
+    ctx->last_launches = 1 + 3 + 1 + 1 + 1 + 3 + 2 + 2 + 2 * (1 + 3 + 1 + 1 + 1 + 3 + 2 + 1);
+    ctx->last_sites = total;
+    ctx->last_units = 0;
+    for (size_t k = 0; k < n_active; ++k) {
+        const RefPlan& pl = plans[active[k]];
+        ctx->last_units += static_cast<uint64_t>(pl.nx) * pl.ny * prof.depth_hypotheses *
+                           pl.src_slots.size();
+    }
+
+    // stage events: sweep | primary reciprocal | completion passes
+    cudaEvent_t es[6];
+    for (auto& e : es) cudaEventCreate(&e);
+    // primary sweep, reciprocal check and fusion
+    cudaEventRecord(es[0], stream);
+    V3D_CK(launch_sweep_dispatch(b, d_siteref, total, max_nx, max_ny, stride0, tiled, d_rank,
+                                 d_status, d_ctr, stream));
+    cudaEventRecord(es[1], stream);
+    V3D_CK(launch_compact(d_status, kSiteAccepted, total, d_idx, c_cand, d_scratch, stream));
+    V3D_CK(launch_make_primary_cands(b, d_idx, c_cand, cap, d_siteref, d_rank, d_cands, stream));
+    cudaEventRecord(es[2], stream);
+    V3D_CK(launch_reciprocal(b, d_cands, c_cand, cap, d_obs, d_ctr, stream));
+    cudaEventRecord(es[3], stream);
+    V3D_CK(cudaMemsetAsync(d_cstat, 0, cap, stream));
+    V3D_CK(launch_fuse(b, d_cands, c_cand, cap, d_obs, false, 0, d_fused, d_cstat, d_ctr, stream));
+    V3D_CK(launch_compact(d_cstat, kCandAccepted, cap, d_idx, c_acc, d_scratch, stream));
+    V3D_CK(launch_append(d_idx, c_acc, cap, d_fused, d_pool, c_pool, c_seg + 0, stream));
+    V3D_CK(launch_occupancy_clear(d_occ, total, stream));
+    V3D_CK(launch_occupy(b, d_pool, nullptr, c_seg + 0, cap, d_occ, stream));
+
+    // two surface-completion passes (dense_legacy.rs:542-734)
+    cudaEventRecord(es[4], stream);
+    for (int pass = 0; pass < 2; ++pass) {
+        V3D_CK(launch_propose(b, pass, total, d_siteref, d_occ, d_pool, d_pstat, d_prop, d_ctr,
+                              stream));
+        V3D_CK(launch_compact(d_pstat, kPropCandidate, total, d_idx, c_cand, d_scratch, stream));
+        V3D_CK(launch_gather_cands(d_idx, c_cand, cap, d_prop, d_cands, stream));
+        V3D_CK(launch_reciprocal(b, d_cands, c_cand, cap, d_obs, d_ctr, stream));
+        V3D_CK(cudaMemsetAsync(d_cstat, 0, cap, stream));
+        V3D_CK(launch_fuse(b, d_cands, c_cand, cap, d_obs, true, pass, d_fused, d_cstat, d_ctr,
+                           stream));
+        V3D_CK(launch_compact(d_cstat, kCandAccepted, cap, d_idx, c_acc, d_scratch, stream));
+        V3D_CK(launch_append(d_idx, c_acc, cap, d_fused, d_pool, c_pool, c_seg + pass + 1, stream));
+        V3D_CK(launch_occupy(b, d_pool, c_seg + pass, c_seg + pass + 1, cap, d_occ, stream));
+    }
+    cudaEventRecord(es[5], stream);
+    cudaEventRecord(ev1, stream);
+
+    // ---- read back ----
+    std::vector<RefCounters> ctr(n_active);
+    uint32_t segs[3];
+    V3D_CK(cudaMemcpyAsync(ctr.data(), d_ctr, sizeof(RefCounters) * n_active,
+                           cudaMemcpyDeviceToHost, stream));
+    V3D_CK(cudaMemcpyAsync(segs, c_seg, sizeof(segs), cudaMemcpyDeviceToHost, stream));
+    V3D_CK(cudaStreamSynchronize(stream));
+    cudaEventElapsedTime(&ctx->last_ms, ev0, ev1);
+    cudaEventElapsedTime(&ctx->last_sweep_ms, es[0], es[1]);
+    cudaEventElapsedTime(&ctx->last_recip_ms, es[2], es[3]);
+    cudaEventElapsedTime(&ctx->last_completion_ms, es[4], es[5]);
+    cudaEventDestroy(ev0);
+    cudaEventDestroy(ev1);
+    for (auto& e : es) cudaEventDestroy(e);
+    ctx->last_recip_evals = 0;
+    ctx->last_candidates = 0;
+    for (const RefCounters& c : ctr) {
+        ctx->last_recip_evals += c.recip_evals;
+        ctx->last_candidates += c.candidates;
+    }
+    const size_t n_pool = segs[2];
+    std::vector<OutPoint> pool(n_pool);
+    if (n_pool) {
+        if (!grow(&ctx->pinned, &ctx->pinned_bytes, n_pool * sizeof(OutPoint), true)) {
+            ctx->last_error = "pinned staging allocation failed";
+            return V3D_ERR_OUT_OF_MEMORY;
+        }
+        V3D_CK(cudaMemcpyAsync(ctx->pinned, d_pool, n_pool * sizeof(OutPoint),
+                               cudaMemcpyDeviceToHost, stream));
+        V3D_CK(cudaStreamSynchronize(stream));
+        std::memcpy(pool.data(), ctx->pinned, n_pool * sizeof(OutPoint));
+    }
+
+    // ---- assemble per reference ----
+    const Seg seg[3] = {{0, segs[0]}, {segs[0], segs[1]}, {segs[1], segs[2]}};
+    std::vector<size_t> cursor = {seg[0].begin, seg[1].begin, seg[2].begin};
+    for (size_t k = 0; k < n_active; ++k) {
+        PassResult& r = results[active[k]];
+        const RefPlan& p = plans[active[k]];
+        const RefCounters& c = ctr[k];
+        std::vector<double> errors, supports, observations;
+        for (int sgi = 0; sgi < 3; ++sgi) {
+            size_t& i = cursor[sgi];
+            while (i < seg[sgi].end && pool[i].ref == k) {
+                const OutPoint& o = pool[i];
+                r.points.push_back(o.p);
+                r.sites.push_back(o.s);
+                r.attrs.push_back(o.a);
+                errors.push_back(o.error);
+                supports.push_back(o.support);
+                if (sgi == 0) observations.push_back(o.observations);
+                ++i;
+            }
+        }
+        v3d_dense_stats& s = r.stats;
+        std::memset(&s, 0, sizeof(s));
+        s.attempted = 1;
+        s.has_reference_frame = p.have_reference;
+        s.reference_frame = p.reference_frame;
+        s.source_views = p.src_slots.size();
+        s.sampled_pixels = c.sampled;
+        s.depth_hypotheses = static_cast<uint64_t>(prof.depth_hypotheses);
+        s.accepted_points = r.points.size();
+        s.surface_completion_proposals = c.proposals;
+        s.surface_completed_points = c.completed;
+        s.surface_completion_rejected_texture = c.rej_texture;
+        s.surface_completion_rejected_cross_view = c.rej_cross;
+        s.surface_completion_rejected_reciprocal = c.rej_recip;
+        s.surface_completion_rejected_fusion = c.rej_fusion;
+        s.surface_completion_rejected_footprint = c.rej_footprint;
+        s.grid_stride = p.stride;
+        s.grid_border = p.border;
+        s.reciprocal_checked_points = c.checked;
+        s.reciprocal_rejected_points = c.recip_rejected;
+        s.reciprocal_consistent_points = c.consistent;
+        s.fusion_input_observations = c.fusion_input;
+        s.fusion_rejected_observations = c.fusion_rejected_obs;
+        s.fusion_rejected_points = c.fusion_rejected_pts;
+        if (!observations.empty()) {
+            s.has_median_fusion_observations = 1;
+            s.median_fusion_observations = static_cast<float>(median_of(observations));
+        }
+        if (!supports.empty()) {
+            s.has_median_supporting_views = 1;
+            s.median_supporting_views = static_cast<float>(median_of(supports));
+        }
+        if (!errors.empty()) {
+            s.has_median_photometric_error = 1;
+            s.median_photometric_error = static_cast<float>(median_of(errors));
+        }
+        s.has_search_min_depth = 1;
+        s.search_min_depth = static_cast<float>(p.search_min);
+        s.has_search_max_depth = 1;
+        s.search_max_depth = static_cast<float>(p.search_max);
+    }
+    return V3D_OK;
+}
+
+int32_t run_sweep_records(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* frames,
+                          size_t n_frames, double focal, const RefPlan& plan,
+                          std::vector<v3d_site_record>& out) {
+    out.clear();
+    if (plan.skipped) return V3D_OK;
+    cudaStream_t stream = static_cast<cudaStream_t>(ctx->stream);
+    std::vector<RefPlan> plans{plan};
+    Prepared P;
+    int32_t pst = prepare(ctx, prof, frames, n_frames, focal, plans, {0}, true, P);
+    if (pst != V3D_OK) return pst;
+    V3D_CK(launch_sweep_dispatch(P.b, P.d_siteref, P.total, P.max_nx, P.max_ny, P.stride0, P.tiled,
+                                 P.d_rank, P.d_status, P.d_ctr, stream));
+    std::vector<SiteRank> rank(P.total);
+    std::vector<uint8_t> status(P.total);
+    if (P.total) {
+        V3D_CK(cudaMemcpyAsync(rank.data(), P.d_rank, sizeof(SiteRank) * P.total,
+                               cudaMemcpyDeviceToHost, stream));
+        V3D_CK(cudaMemcpyAsync(status.data(), P.d_status, P.total, cudaMemcpyDeviceToHost, stream));
+    }
+    V3D_CK(cudaStreamSynchronize(stream));
+    out.resize(P.total);
+    for (uint64_t i = 0; i < P.total; ++i) {
+        v3d_site_record& r = out[i];
+        std::memset(&r, 0, sizeof(r));
+        uint32_t gy = static_cast<uint32_t>(i / plan.nx), gx = static_cast<uint32_t>(i % plan.nx);
+        r.x = plan.border + gx * plan.stride;
+        r.y = plan.border + gy * plan.stride;
+        r.status = status[i];
+        if (status[i] >= kSiteGateRejected) {
+            r.plane = rank[i].plane;
+            r.support = rank[i].support;
+            r.error = rank[i].error;
+            r.margin = rank[i].margin;
+        } else {
+            r.plane = -1;
+        }
+    }
+    return V3D_OK;
+}
+
+}  // namespace v3d

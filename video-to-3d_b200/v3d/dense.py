@@ -1,0 +1,208 @@
+"""Python mirror of video-to-3d-core's dense and mesh API over the CUDA library.
+
+Function names and argument meaning follow crates/video-to-3d-core/src:
+``estimate_depth_points_with_control`` (dense_legacy.rs:149-156),
+``reconstruct_reference_patches`` (dense.rs:674-747, batched),
+``estimate_depth_points_limited`` (dense.rs:250-330),
+``has_distributed_landmarks`` (dense.rs:165-213), ``grid_stride``
+(dense.rs:215-218) and ``reconstruct_dense_mesh_with_control``
+(mesh.rs:74-220).  Every compute call runs on the GPU through
+libv3d_dense.so; there is no CPU fallback, and a missing library or device
+raises.
+"""
+import ctypes as C
+import os
+
+from . import abi, profiles, types
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(HERE), "lib", "libv3d_dense.so")
+_P = C.POINTER
+_lib = None
+
+
+class V3DError(RuntimeError):
+    def __init__(self, status, message=""):
+        self.status = status
+        super().__init__("v3d status %d%s" % (status, (": " + message) if message else ""))
+
+
+def library():
+    """Load libv3d_dense.so (built by video-to-3d_b200/build.py)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise FileNotFoundError("%s is missing; run video-to-3d_b200/build.py" % LIB_PATH)
+    L = C.CDLL(LIB_PATH)
+    frames_args = [_P(abi.Frame), C.c_uint64, _P(abi.Camera), C.c_uint64, _P(C.c_double),
+                   C.c_uint64, C.c_double]
+    L.v3d_abi_version.restype = C.c_int32
+    L.v3d_status_text.argtypes = [C.c_int32]
+    L.v3d_status_text.restype = C.c_char_p
+    L.v3d_skip_reason_text.argtypes = [C.c_int32]
+    L.v3d_skip_reason_text.restype = C.c_char_p
+    L.v3d_last_error.argtypes = [C.c_void_p]
+    L.v3d_last_error.restype = C.c_char_p
+    L.v3d_context_create.argtypes = [C.c_int32, _P(C.c_void_p)]
+    L.v3d_context_create.restype = C.c_int32
+    L.v3d_context_destroy.argtypes = [C.c_void_p]
+    L.v3d_context_destroy.restype = None
+    L.v3d_profile_reference.argtypes = [_P(abi.Profile)]
+    L.v3d_profile_zncc.argtypes = [_P(abi.Profile), C.c_int32, C.c_int32, C.c_int32, C.c_int32]
+    L.v3d_grid_stride.argtypes = [C.c_uint32, C.c_uint32, C.c_int32]
+    L.v3d_grid_stride.restype = C.c_uint64
+    L.v3d_estimate_depth_points_with_control.argtypes = [C.c_void_p] + frames_args + [
+        C.c_int32, _P(abi.Profile), abi.CANCEL_FN, C.c_void_p, _P(abi.DenseResult)]
+    L.v3d_estimate_depth_points_with_control.restype = C.c_int32
+    L.v3d_reconstruct_reference_patches.argtypes = [C.c_void_p] + frames_args + [
+        C.c_int32, _P(abi.Profile), _P(C.c_uint64), C.c_uint64, abi.CANCEL_FN, C.c_void_p,
+        _P(abi.DenseResult), _P(C.c_int32)]
+    L.v3d_reconstruct_reference_patches.restype = C.c_int32
+    L.v3d_estimate_depth_points_limited.argtypes = [C.c_void_p] + frames_args + [
+        C.c_uint64, C.c_int32, _P(abi.Profile), abi.CANCEL_FN, C.c_void_p, _P(abi.DenseResult),
+        _P(C.c_int32)]
+    L.v3d_estimate_depth_points_limited.restype = C.c_int32
+    L.v3d_has_distributed_landmarks.argtypes = frames_args + [abi.CANCEL_FN, C.c_void_p]
+    L.v3d_has_distributed_landmarks.restype = C.c_int32
+    L.v3d_dense_result_free.argtypes = [_P(abi.DenseResult)]
+    L.v3d_dense_result_free.restype = None
+    L.v3d_reconstruct_dense_mesh_with_control.argtypes = [
+        C.c_void_p, _P(abi.Point), C.c_uint64, _P(abi.GridSite), C.c_uint64,
+        _P(abi.MeshDenseInput), _P(abi.Camera), C.c_uint64, C.c_uint32, C.c_uint32,
+        C.c_double, abi.CANCEL_FN, C.c_void_p, _P(abi.MeshResult)]
+    L.v3d_reconstruct_dense_mesh_with_control.restype = C.c_int32
+    L.v3d_mesh_result_free.argtypes = [_P(abi.MeshResult)]
+    L.v3d_mesh_result_free.restype = None
+    L.v3d_debug_sweep.argtypes = [C.c_void_p] + frames_args + [
+        C.c_int32, _P(abi.Profile), _P(abi.SiteRecord), C.c_uint64, _P(C.c_uint64)]
+    L.v3d_debug_sweep.restype = C.c_int32
+    L.v3d_last_run_info.argtypes = [C.c_void_p, _P(abi.RunInfo)]
+    L.v3d_last_run_info.restype = C.c_int32
+    _lib = L
+    return L
+
+
+class Context:
+    """A CUDA stream plus device buffers on one GPU (v3d_context)."""
+
+    def __init__(self, device=0):
+        self.lib = library()
+        self.handle = C.c_void_p()
+        st = self.lib.v3d_context_create(int(device), C.byref(self.handle))
+        if st != abi.OK:
+            raise V3DError(st, self.lib.v3d_status_text(st).decode())
+
+    def close(self):
+        if self.handle:
+            self.lib.v3d_context_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st):
+        if st < 0:
+            raise V3DError(st, self.lib.v3d_last_error(self.handle).decode())
+        return st
+
+    def estimate_depth_points_with_control(self, frames, cameras, sparse_points, focal,
+                                           fine_grid=False, control=None, profile=None):
+        prof = profile if profile is not None else profiles.reference()
+        inp = types.Inputs(frames, cameras, sparse_points)
+        fn, _keep = types.cancel_callback(control)
+        out = abi.DenseResult()
+        st = self._check(self.lib.v3d_estimate_depth_points_with_control(
+            self.handle, inp.frames, inp.n_frames, inp.cameras, inp.n_cameras, inp.sparse,
+            inp.n_sparse, float(focal), int(fine_grid), C.byref(prof), fn, None, C.byref(out)))
+        try:
+            return types.dense_from_result(out, st)
+        finally:
+            self.lib.v3d_dense_result_free(C.byref(out))
+
+    def reconstruct_reference_patches(self, frames, cameras, sparse_points, focal,
+                                      camera_indices, profile=None, fine_grid=False,
+                                      control=None):
+        prof = profile if profile is not None else profiles.reference()
+        inp = types.Inputs(frames, cameras, sparse_points)
+        fn, _keep = types.cancel_callback(control)
+        n = len(camera_indices)
+        idx = (C.c_uint64 * max(n, 1))(*camera_indices)
+        outs = (abi.DenseResult * max(n, 1))()
+        present = (C.c_int32 * max(n, 1))()
+        self._check(self.lib.v3d_reconstruct_reference_patches(
+            self.handle, inp.frames, inp.n_frames, inp.cameras, inp.n_cameras, inp.sparse,
+            inp.n_sparse, float(focal), int(fine_grid), C.byref(prof), idx, n, fn, None, outs,
+            present))
+        res = []
+        for i in range(n):
+            res.append(types.dense_from_result(outs[i]) if present[i] else None)
+            self.lib.v3d_dense_result_free(C.byref(outs[i]))
+        return res
+
+    def estimate_depth_points_limited(self, frames, cameras, sparse_points, focal,
+                                      reference_views, fine_grid, profile=None, control=None):
+        prof = profile if profile is not None else profiles.reference()
+        inp = types.Inputs(frames, cameras, sparse_points)
+        fn, _keep = types.cancel_callback(control)
+        out = abi.DenseResult()
+        omitted = C.c_int32()
+        st = self._check(self.lib.v3d_estimate_depth_points_limited(
+            self.handle, inp.frames, inp.n_frames, inp.cameras, inp.n_cameras, inp.sparse,
+            inp.n_sparse, float(focal), int(reference_views), int(fine_grid), C.byref(prof), fn,
+            None, C.byref(out), C.byref(omitted)))
+        try:
+            return types.dense_from_result(out, st), bool(omitted.value)
+        finally:
+            self.lib.v3d_dense_result_free(C.byref(out))
+
+    def last_run_info(self):
+        """Device time, kernel launches and work units of the last dense call."""
+        info = abi.RunInfo()
+        self._check(self.lib.v3d_last_run_info(self.handle, C.byref(info)))
+        return {name: getattr(info, name) for name, _ in abi.RunInfo._fields_}
+
+    def debug_sweep(self, frames, cameras, sparse_points, focal, fine_grid=False, profile=None):
+        """Per-site sweep records (status, plane, support, error, margin) in raster order."""
+        prof = profile if profile is not None else profiles.reference()
+        inp = types.Inputs(frames, cameras, sparse_points)
+        n = C.c_uint64()
+        st = self._check(self.lib.v3d_debug_sweep(
+            self.handle, inp.frames, inp.n_frames, inp.cameras, inp.n_cameras, inp.sparse,
+            inp.n_sparse, float(focal), int(fine_grid), C.byref(prof), None, 0, C.byref(n)))
+        if st == abi.SKIPPED:
+            return None
+        buf = (abi.SiteRecord * max(n.value, 1))()
+        self._check(self.lib.v3d_debug_sweep(
+            self.handle, inp.frames, inp.n_frames, inp.cameras, inp.n_cameras, inp.sparse,
+            inp.n_sparse, float(focal), int(fine_grid), C.byref(prof), buf, n.value, C.byref(n)))
+        return types.site_records(buf, n.value)
+
+    def reconstruct_dense_mesh_with_control(self, points, grid_sites, stats, cameras, width,
+                                            height, focal, control=None):
+        mi = types.MeshInputs(points, grid_sites, stats)
+        cams = types.Inputs([], cameras, [])
+        fn, _keep = types.cancel_callback(control)
+        out = abi.MeshResult()
+        self._check(self.lib.v3d_reconstruct_dense_mesh_with_control(
+            self.handle, *mi.args(), cams.cameras, cams.n_cameras, int(width), int(height),
+            float(focal), fn, None, C.byref(out)))
+        try:
+            return types.mesh_from_result(out)
+        finally:
+            self.lib.v3d_mesh_result_free(C.byref(out))
+
+
+def has_distributed_landmarks(frames, cameras, sparse_points, focal, control=None):
+    inp = types.Inputs(frames, cameras, sparse_points)
+    fn, _keep = types.cancel_callback(control)
+    return bool(library().v3d_has_distributed_landmarks(
+        inp.frames, inp.n_frames, inp.cameras, inp.n_cameras, inp.sparse, inp.n_sparse,
+        float(focal), fn, None))
+
+
+def grid_stride(width, height, fine_grid):
+    return int(library().v3d_grid_stride(int(width), int(height), int(fine_grid)))
