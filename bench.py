@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--storage", choices=["f32", "f16", "bf16"], default="f32")
     ap.add_argument("--frames", type=int, default=FRAMES)
+    ap.add_argument("--no-cpu-baseline", action="store_true",
+                    help="skip the CPU baseline leg (profiling runs)")
     return ap.parse_args()
 
 
@@ -251,6 +253,8 @@ def run_ours(args, rank, world, local):
         total_units = float(u[0])
     else:
         total_units = float(units)
+    host = {k: float(np.mean([i[k] for i in infos]))
+            for k in ("host_plan_ms", "host_upload_ms", "host_wait_ms", "host_assemble_ms")}
     sweep_ms = float(np.mean([i["sweep_ms"] for i in infos]))
     recip_ms = float(np.mean([i["reciprocal_ms"] for i in infos]))
     comp_ms = float(np.mean([i["completion_ms"] for i in infos]))
@@ -284,7 +288,7 @@ def run_ours(args, rank, world, local):
                     "d2h_bytes_per_step": points * 72, "ms_per_step": wall_s * 1e3},
             "gpu_launches": infos[-1]["kernel_launches"],
             "stages_ms": {"sweep": sweep_ms, "reciprocal_primary": recip_ms,
-                          "completion": comp_ms, "total": dev_s * 1e3},
+                          "completion": comp_ms, "total": dev_s * 1e3, **host},
             "roofline": {"bound": "hbm", "kernel": kernel, "achieved": achieved, "peak": hbm,
                          "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
                          "note": "achieved = bilinear-footprint bytes 4*W^2*b per window "
@@ -292,7 +296,7 @@ def run_ours(args, rank, world, local):
                                  "(of measured); the gathers are served by L1/L2"},
             "points_per_step": points,
         }
-        if world == 1:
+        if world == 1 and not args.no_cpu_baseline:
             v, info = cpu_baseline(clip, frames, prof, os.cpu_count() or 1)
             line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": info["cores"],
                                     "kind": "port", "sample": info["sample"]}

@@ -399,6 +399,10 @@ typedef struct v3d_run_info {
     double completion_ms;     /* both surface-completion passes, reciprocal included */
     uint64_t reciprocal_plane_evaluations; /* single-view hypotheses evaluated, all passes */
     uint64_t candidates;      /* primary + completion candidates checked */
+    double host_plan_ms;      /* host planning of every reference */
+    double host_upload_ms;    /* staging and enqueueing uploads and kernels */
+    double host_wait_ms;      /* waiting for the device, read-back included */
+    double host_assemble_ms;  /* splitting the point pool per reference, medians */
 } v3d_run_info;
 
 int32_t v3d_last_run_info(const v3d_context* ctx, v3d_run_info* out);

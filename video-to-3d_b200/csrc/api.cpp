@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cstdlib>
 #include <cstring>
 #include <memory>
@@ -240,6 +241,10 @@ int32_t v3d_last_run_info(const v3d_context* ctx, v3d_run_info* out) {
     out->completion_ms = ctx->last_completion_ms;
     out->reciprocal_plane_evaluations = ctx->last_recip_evals;
     out->candidates = ctx->last_candidates;
+    out->host_plan_ms = ctx->last_plan_ms;
+    out->host_upload_ms = ctx->last_upload_ms;
+    out->host_wait_ms = ctx->last_wait_ms;
+    out->host_assemble_ms = ctx->last_assemble_ms;
     return V3D_OK;
 }
 
@@ -381,14 +386,20 @@ int32_t v3d_reconstruct_reference_patches(v3d_context* ctx, const v3d_frame* fra
         return V3D_ERR_INVALID_ARGUMENT;
     std::lock_guard<std::mutex> lock(ctx->mu);
     cudaSetDevice(ctx->device);
+    const auto t_plan = std::chrono::steady_clock::now();
     Inputs in = load_inputs(frames, n_frames, cameras, n_cameras, sparse_xyz, n_sparse, focal);
     std::vector<RefPlan> plans(n_refs);
     std::vector<bool> pres(n_refs);
     CancelPoll cp{cancel, cancel_user};
     std::vector<uint8_t> canceled(n_refs, 0);
-    for (uint64_t i = 0; i < n_refs; ++i) {
+    std::vector<uint8_t> pres8(n_refs, 0);
+    parallel_for(n_refs, [&](size_t i) {
         bool p = false;
         plans[i] = plan_reference_patch(*profile, in, camera_indices[i], fine_grid != 0, p);
+        pres8[i] = p;
+    });
+    for (uint64_t i = 0; i < n_refs; ++i) {
+        const bool p = pres8[i] != 0;
         pres[i] = p;
         if (!p) {
             plans[i].skipped = true;
@@ -403,8 +414,11 @@ int32_t v3d_reconstruct_reference_patches(v3d_context* ctx, const v3d_frame* fra
             plans[i].skipped = true;
         }
     }
+    const double plan_ms = std::chrono::duration<double, std::milli>(
+                               std::chrono::steady_clock::now() - t_plan).count();
     std::vector<PassResult> res;
     int32_t st = run_batch(ctx, *profile, frames, n_frames, focal, plans, res);
+    ctx->last_plan_ms = plan_ms;
     if (st < 0) return st;
     for (uint64_t i = 0; i < n_refs; ++i) {
         present[i] = pres[i] ? 1 : 0;

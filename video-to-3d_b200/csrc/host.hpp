@@ -3,6 +3,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <functional>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -75,9 +76,16 @@ bool in_image_bounds_h(double x, double y, uint32_t w, uint32_t h);
 
 // dense_legacy.rs:157-256 on an explicit view list: `cams[i]` with frame slots
 // `slot_of_frame_index(cams[i].frame_index)`.
+// `first_camera_sees_all`: the caller guarantees every landmark is visible in
+// cams[0] at frame 0's size (the remapped per-reference call), which lets the
+// reference selection skip scanning the other cameras.
 RefPlan plan_legacy(const v3d_profile& prof, const v3d_frame* frames, size_t n_frames,
                     const std::vector<HCamera>& cams, const std::vector<HVec3>& sparse,
-                    double focal, bool fine_grid, const std::vector<size_t>* slot_map);
+                    double focal, bool fine_grid, const std::vector<size_t>* slot_map,
+                    bool first_camera_sees_all = false);
+
+// Runs fn(i) for i in [0, n) on the host's hardware threads.
+void parallel_for(size_t n, const std::function<void(size_t)>& fn);
 
 // dense.rs:674-747: remap so the reference comes first; `present` is false
 // where the reference returns None.
@@ -109,6 +117,7 @@ struct v3d_context {
     uint64_t last_units = 0;
     float last_sweep_ms = 0.f, last_recip_ms = 0.f, last_completion_ms = 0.f;
     uint64_t last_recip_evals = 0, last_candidates = 0;
+    double last_plan_ms = 0, last_upload_ms = 0, last_wait_ms = 0, last_assemble_ms = 0;
 };
 
 namespace v3d {

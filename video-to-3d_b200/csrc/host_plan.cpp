@@ -6,8 +6,10 @@
 // device.  Built with -ffp-contract=off so its f64 results (the hypothesis
 // envelope above all) are the reference's to the bit.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
+#include <thread>
 
 #include "host.hpp"
 
@@ -96,7 +98,8 @@ bool in_image_bounds_h(double x, double y, uint32_t w, uint32_t h) {
 
 RefPlan plan_legacy(const v3d_profile& prof, const v3d_frame* frames, size_t n_frames,
                     const std::vector<HCamera>& cams, const std::vector<HVec3>& sparse,
-                    double focal, bool fine_grid, const std::vector<size_t>* slot_map) {
+                    double focal, bool fine_grid, const std::vector<size_t>* slot_map,
+                    bool first_camera_sees_all) {
     // `cams[i].frame_index` indexes the (possibly remapped) frame list whose
     // entry k lives in frames[slot_map ? (*slot_map)[k] : k].
     RefPlan p;
@@ -125,7 +128,20 @@ RefPlan plan_legacy(const v3d_profile& prof, const v3d_frame* frames, size_t n_f
     // reference: most visible landmarks, ties to the smallest frame index (last maximum)
     const HCamera* reference = nullptr;
     std::vector<double> ref_depths;
-    for (const HCamera& c : cams) {
+    bool fast = false;
+    if (first_camera_sees_all && cams[0].frame_index == 0) {
+        // Every landmark lies inside cams[0]'s view at frame 0's size, so no
+        // camera sees more and ties go to the smallest frame index: the scan
+        // below would select cams[0].
+        auto d = visible_depths(cams[0], sparse, width, height, focal);
+        if (d.size() >= kMinVisibleSparsePoints && d.size() == sparse.size()) {
+            reference = &cams[0];
+            ref_depths = std::move(d);
+            fast = true;
+        }
+    }
+    for (size_t ci = 0; !fast && ci < cams.size(); ++ci) {
+        const HCamera& c = cams[ci];
         auto d = visible_depths(c, sparse, width, height, focal);
         if (d.size() < kMinVisibleSparsePoints) continue;
         bool take = !reference || d.size() > ref_depths.size() ||
@@ -264,7 +280,8 @@ RefPlan plan_reference_patch(const v3d_profile& prof, const Inputs& in, size_t c
         rcams.push_back(m);
     }
     present = true;
-    RefPlan p = plan_legacy(prof, in.frames, in.n_frames, rcams, visible, in.focal, fine_grid, &slots);
+    RefPlan p = plan_legacy(prof, in.frames, in.n_frames, rcams, visible, in.focal, fine_grid, &slots,
+                            true);
     // report frames in the caller's index space (dense.rs:734-745)
     p.have_reference = true;
     p.reference_frame = rc.frame_index;
@@ -341,6 +358,22 @@ bool has_distributed_landmarks(const Inputs& in, CancelPoll& cancel) {
         }
     }
     return false;
+}
+
+void parallel_for(size_t n, const std::function<void(size_t)>& fn) {
+    size_t workers = std::min<size_t>(n, std::max(1u, std::thread::hardware_concurrency()));
+    if (workers <= 1) {
+        for (size_t i = 0; i < n; ++i) fn(i);
+        return;
+    }
+    std::atomic<size_t> next{0};
+    std::vector<std::thread> pool;
+    pool.reserve(workers);
+    for (size_t w = 0; w < workers; ++w)
+        pool.emplace_back([&]() {
+            for (size_t i = next++; i < n; i = next++) fn(i);
+        });
+    for (auto& t : pool) t.join();
 }
 
 void skip_result(PassResult& r, int code, const std::string& reason) {

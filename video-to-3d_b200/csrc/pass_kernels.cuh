@@ -87,7 +87,9 @@ enum PropStatus : uint8_t {
 struct BatchDev {
     const DevReference* refs;   // [n_refs]
     const uint64_t* site_off;   // [n_refs + 1] flat site offsets
+    const float* src_inv;       // [n_refs][kMaxSources][planes] 1/depth of each source hypothesis
     int32_t n_refs;
+    int32_t max_src;            // largest source count of the batch
     int32_t storage;            // StorageFormat
     DevProfile prof;
     bool exact;

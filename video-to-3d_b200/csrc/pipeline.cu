@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cstring>
 #include <stdexcept>
 
@@ -220,6 +221,8 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
         luma_off[u] = rgba ? cv.take<uint8_t>(px) : raw_off[u];
     }
     const size_t o_refs = cv.take<DevReference>(n_active);
+    const size_t inv_count = n_active * kMaxSources * static_cast<size_t>(prof.depth_hypotheses);
+    const size_t o_srcinv = cv.take<float>(inv_count);
     const size_t o_siteoff = cv.take<uint64_t>(n_active + 1);
     const size_t o_siteref = cv.take<uint32_t>(cap);
     const size_t o_rank = cv.take<SiteRank>(cap);
@@ -255,7 +258,8 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
             V3D_CK(launch_luma(reinterpret_cast<const uint8_t*>(at(raw_off[u])),
                                reinterpret_cast<uint8_t*>(at(luma_off[u])), px, stream));
     }
-    const size_t staging = sizeof(DevReference) * n_active + sizeof(uint64_t) * (n_active + 1);
+    const size_t staging = sizeof(DevReference) * n_active + sizeof(uint64_t) * (n_active + 1) +
+                           sizeof(float) * inv_count;
     if (!grow(&ctx->pinned, &ctx->pinned_bytes, staging, true)) {
         ctx->last_error = "pinned staging allocation failed";
         return V3D_ERR_OUT_OF_MEMORY;
@@ -293,10 +297,27 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
     }
     uint64_t* hoff = reinterpret_cast<uint64_t*>(hrefs + n_active);
     std::memcpy(hoff, site_off.data(), sizeof(uint64_t) * (n_active + 1));
+    // 1/depth of every source hypothesis, from the f64 hypothesis formula
+    // (dense_legacy.rs:286-293, 908-916) rounded once to f32
+    float* hinv = reinterpret_cast<float*>(hoff + n_active + 1);
+    std::memset(hinv, 0, sizeof(float) * inv_count);
+    const int n_hyp = prof.depth_hypotheses;
+    for (size_t k = 0; k < n_active; ++k) {
+        const RefPlan& pl = plans[active[k]];
+        for (size_t j = 0; j < pl.src_slots.size(); ++j)
+            for (int q = 0; q < n_hyp; ++q) {
+                double t = n_hyp == 1 ? 0.0 : static_cast<double>(q) / static_cast<double>(n_hyp - 1);
+                double inv = (1.0 / pl.src_min[j]) * (1.0 - t) + (1.0 / pl.src_max[j]) * t;
+                double depth = 1.0 / inv;
+                hinv[(k * kMaxSources + j) * n_hyp + q] = static_cast<float>(1.0 / depth);
+            }
+    }
     V3D_CK(cudaMemcpyAsync(at(o_refs), hrefs, sizeof(DevReference) * n_active,
                            cudaMemcpyHostToDevice, stream));
     V3D_CK(cudaMemcpyAsync(at(o_siteoff), hoff, sizeof(uint64_t) * (n_active + 1),
                            cudaMemcpyHostToDevice, stream));
+    V3D_CK(cudaMemcpyAsync(at(o_srcinv), hinv, sizeof(float) * inv_count, cudaMemcpyHostToDevice,
+                           stream));
 
     auto* d_siteref = P.d_siteref = reinterpret_cast<uint32_t*>(at(o_siteref));
     P.d_rank = reinterpret_cast<SiteRank*>(at(o_rank));
@@ -323,7 +344,11 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
     BatchDev& b = P.b;
     b.refs = reinterpret_cast<const DevReference*>(at(o_refs));
     b.site_off = reinterpret_cast<const uint64_t*>(at(o_siteoff));
+    b.src_inv = reinterpret_cast<const float*>(at(o_srcinv));
     b.n_refs = static_cast<int32_t>(n_active);
+    b.max_src = 1;
+    for (size_t k = 0; k < n_active; ++k)
+        b.max_src = std::max<int32_t>(b.max_src, static_cast<int32_t>(plans[active[k]].src_slots.size()));
     b.storage = storage;
     b.prof.cost = prof.cost;
     b.prof.radius = prof.patch_radius;
@@ -361,6 +386,11 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
             active.push_back(i);
     }
     if (active.empty()) return V3D_OK;
+    using clk = std::chrono::steady_clock;
+    auto ms_since = [](clk::time_point t) {
+        return std::chrono::duration<double, std::milli>(clk::now() - t).count();
+    };
+    const clk::time_point t_upload = clk::now();
     Prepared P;
     int32_t pst = prepare(ctx, prof, frames, n_frames, focal, plans, active, false, P);
     if (pst != V3D_OK) return pst;
@@ -444,6 +474,8 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
     cudaEventRecord(ev1, stream);
 
     // ---- read back ----
+    ctx->last_upload_ms = ms_since(t_upload);
+    const clk::time_point t_wait = clk::now();
     std::vector<RefCounters> ctr(n_active);
     uint32_t segs[3];
     V3D_CK(cudaMemcpyAsync(ctr.data(), d_ctr, sizeof(RefCounters) * n_active,
@@ -464,7 +496,6 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
         ctx->last_candidates += c.candidates;
     }
     const size_t n_pool = segs[2];
-    std::vector<OutPoint> pool(n_pool);
     if (n_pool) {
         if (!grow(&ctx->pinned, &ctx->pinned_bytes, n_pool * sizeof(OutPoint), true)) {
             ctx->last_error = "pinned staging allocation failed";
@@ -473,28 +504,44 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
         V3D_CK(cudaMemcpyAsync(ctx->pinned, d_pool, n_pool * sizeof(OutPoint),
                                cudaMemcpyDeviceToHost, stream));
         V3D_CK(cudaStreamSynchronize(stream));
-        std::memcpy(pool.data(), ctx->pinned, n_pool * sizeof(OutPoint));
     }
+    const OutPoint* pool = static_cast<const OutPoint*>(ctx->pinned);
 
+    ctx->last_wait_ms = ms_since(t_wait);
+    const clk::time_point t_assemble = clk::now();
     // ---- assemble per reference ----
-    const Seg seg[3] = {{0, segs[0]}, {segs[0], segs[1]}, {segs[1], segs[2]}};
-    std::vector<size_t> cursor = {seg[0].begin, seg[1].begin, seg[2].begin};
-    for (size_t k = 0; k < n_active; ++k) {
+    // each pool segment is ordered by reference: find every reference's range
+    const uint32_t seg_begin[3] = {0, segs[0], segs[1]}, seg_end[3] = {segs[0], segs[1], segs[2]};
+    std::vector<uint32_t> range(3 * (n_active + 1));
+    for (int sgi = 0; sgi < 3; ++sgi) {
+        uint32_t i = seg_begin[sgi];
+        for (size_t k = 0; k <= n_active; ++k) {
+            while (i < seg_end[sgi] && pool[i].ref < k) ++i;
+            range[sgi * (n_active + 1) + k] = i;
+        }
+    }
+    parallel_for(n_active, [&](size_t k) {
         PassResult& r = results[active[k]];
         const RefPlan& p = plans[active[k]];
         const RefCounters& c = ctr[k];
-        std::vector<double> errors, supports, observations;
+        size_t n = 0;
+        for (int sgi = 0; sgi < 3; ++sgi)
+            n += range[sgi * (n_active + 1) + k + 1] - range[sgi * (n_active + 1) + k];
+        r.points.resize(n);
+        r.sites.resize(n);
+        r.attrs.resize(n);
+        std::vector<double> errors(n), supports(n), observations;
+        size_t o = 0;
         for (int sgi = 0; sgi < 3; ++sgi) {
-            size_t& i = cursor[sgi];
-            while (i < seg[sgi].end && pool[i].ref == k) {
-                const OutPoint& o = pool[i];
-                r.points.push_back(o.p);
-                r.sites.push_back(o.s);
-                r.attrs.push_back(o.a);
-                errors.push_back(o.error);
-                supports.push_back(o.support);
-                if (sgi == 0) observations.push_back(o.observations);
-                ++i;
+            const uint32_t b0 = range[sgi * (n_active + 1) + k], b1 = range[sgi * (n_active + 1) + k + 1];
+            for (uint32_t i = b0; i < b1; ++i, ++o) {
+                const OutPoint& q = pool[i];
+                r.points[o] = q.p;
+                r.sites[o] = q.s;
+                r.attrs[o] = q.a;
+                errors[o] = q.error;
+                supports[o] = q.support;
+                if (sgi == 0) observations.push_back(q.observations);
             }
         }
         v3d_dense_stats& s = r.stats;
@@ -505,7 +552,7 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
         s.source_views = p.src_slots.size();
         s.sampled_pixels = c.sampled;
         s.depth_hypotheses = static_cast<uint64_t>(prof.depth_hypotheses);
-        s.accepted_points = r.points.size();
+        s.accepted_points = n;
         s.surface_completion_proposals = c.proposals;
         s.surface_completed_points = c.completed;
         s.surface_completion_rejected_texture = c.rej_texture;
@@ -525,11 +572,9 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
             s.has_median_fusion_observations = 1;
             s.median_fusion_observations = static_cast<float>(median_of(observations));
         }
-        if (!supports.empty()) {
+        if (n) {
             s.has_median_supporting_views = 1;
             s.median_supporting_views = static_cast<float>(median_of(supports));
-        }
-        if (!errors.empty()) {
             s.has_median_photometric_error = 1;
             s.median_photometric_error = static_cast<float>(median_of(errors));
         }
@@ -537,7 +582,8 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
         s.search_min_depth = static_cast<float>(p.search_min);
         s.has_search_max_depth = 1;
         s.search_max_depth = static_cast<float>(p.search_max);
-    }
+    });
+    ctx->last_assemble_ms = ms_since(t_assemble);
     return V3D_OK;
 }
 

@@ -1,0 +1,1065 @@
+// Storage-typed kernels of the dense pass: the depth sweeps, the reciprocal
+// check and the completion proposals, templated on the pixel storage type T,
+// the exactness policy, the window radius R and (fast policy) the cost.
+// typed_<type>.cu instantiate one storage type each so the kernels compile in
+// parallel; pass_kernels.cu dispatches to them.
+#pragma once
+
+#include "pass_kernels.cuh"
+#include "typed.cuh"
+
+namespace v3d {
+namespace typed_detail {
+
+constexpr int kTileX = 32;
+constexpr int kTileY = 8;
+constexpr double kInf = __builtin_huge_val();
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+__device__ __forceinline__ void site_xy(const DevReference& ref, uint32_t local, uint32_t& x,
+                                        uint32_t& y) {
+    uint32_t gy = local / ref.nx, gx = local - gy * ref.nx;
+    x = ref.border + gx * ref.stride;
+    y = ref.border + gy * ref.stride;
+}
+
+// ---- fast window cost --------------------------------------------------------
+// Window cost between fixed values pv (taps of the first image, row-major) and
+// samples of `img` at H (x + dx, y + dy, 1); false where the reference's
+// patch_error returns None (a tap behind the camera or outside the bilinear
+// bounds, or a ZNCC window under the variance floor).
+template <class T, int R, int COST>
+__device__ __forceinline__ bool window_cost_fast(const DevProfile& prof, const float* pv,
+                                                 float pmean, float pvar, const float* H,
+                                                 float zmin, const DevImage& img, float x, float y,
+                                                 float& cost) {
+    constexpr int W = 2 * R + 1;
+    constexpr int N = W * W;
+    const T* data = static_cast<const T*>(img.data);
+    const uint32_t w = img.width, h = img.height;
+    if (COST == 1) {
+        float ss = 0.f, sss = 0.f, sps = 0.f;
+#pragma unroll
+        for (int dy = 0; dy < W; ++dy) {
+            float Y = y + (float)(dy - R);
+#pragma unroll
+            for (int dx = 0; dx < W; ++dx) {
+                float X = x + (float)(dx - R);
+                float h2 = fmaf(H[6], X, fmaf(H[7], Y, H[8]));
+                if (!(h2 > zmin)) return false;
+                float inv = __frcp_rn(h2);
+                float u = fmaf(H[0], X, fmaf(H[1], Y, H[2])) * inv;
+                float v = fmaf(H[3], X, fmaf(H[4], Y, H[5])) * inv;
+                if (!in_bounds_fast(u, v, w, h)) return false;
+                float s = sample_fast<T>(data, w, u, v) - pmean;
+                ss += s;
+                sss = fmaf(s, s, sss);
+                sps = fmaf(pv[dy * W + dx] - pmean, s, sps);
+            }
+        }
+        const float n = (float)N;
+        float vs = sss - ss * ss / n;
+        float cov = sps;  // sum of (p - mean p) equals zero up to rounding
+        if (!(pvar > 0.f) || !(vs > 0.f) || pvar / n < (float)prof.min_variance ||
+            vs / n < (float)prof.min_variance)
+            return false;
+        cost = 1.0f - cov * rsqrtf(pvar * vs);
+        return true;
+    }
+    float sv[N];
+    float ss = 0.f;
+#pragma unroll
+    for (int dy = 0; dy < W; ++dy) {
+        float Y = y + (float)(dy - R);
+#pragma unroll
+        for (int dx = 0; dx < W; ++dx) {
+            float X = x + (float)(dx - R);
+            float h2 = fmaf(H[6], X, fmaf(H[7], Y, H[8]));
+            if (!(h2 > zmin)) return false;
+            float inv = __frcp_rn(h2);
+            float u = fmaf(H[0], X, fmaf(H[1], Y, H[2])) * inv;
+            float v = fmaf(H[3], X, fmaf(H[4], Y, H[5])) * inv;
+            if (!in_bounds_fast(u, v, w, h)) return false;
+            float s = sample_fast<T>(data, w, u, v);
+            sv[dy * W + dx] = s;
+            ss += s;
+        }
+    }
+    float ms = ss / (float)N;
+    float acc = 0.f;
+#pragma unroll
+    for (int i = 0; i < N; ++i) acc += fabsf((pv[i] - pmean) - (sv[i] - ms));
+    cost = acc / (float)N;
+    return true;
+}
+
+// Fixed-window statistics for window_cost_fast: mean and sum of squared deviations.
+template <int R>
+__device__ __forceinline__ void window_stats(const float* pv, float& mean, float& var) {
+    constexpr int N = (2 * R + 1) * (2 * R + 1);
+    float s = 0.f;
+#pragma unroll
+    for (int i = 0; i < N; ++i) s += pv[i];
+    mean = s / (float)N;
+    float v = 0.f;
+#pragma unroll
+    for (int i = 0; i < N; ++i) v = fmaf(pv[i] - mean, pv[i] - mean, v);
+    var = v;
+}
+
+// Homography ref->src (or src->ref) at inverse depth `inv`: A + inv * b e3^T.
+__device__ __forceinline__ void plane_h(const float* A, const float* b, float inv, float* H) {
+#pragma unroll
+    for (int i = 0; i < 9; ++i) H[i] = A[i];
+    H[2] = fmaf(inv, b[0], A[2]);
+    H[5] = fmaf(inv, b[1], A[5]);
+    H[8] = fmaf(inv, b[2], A[8]);
+}
+
+// f32 bilinear taps of a window at fractional centre (x, y); false if out of bounds.
+template <class T, int R>
+__device__ __forceinline__ bool load_window(const DevImage& img, float x, float y, float* pv) {
+    constexpr int W = 2 * R + 1;
+    const T* data = static_cast<const T*>(img.data);
+#pragma unroll
+    for (int dy = 0; dy < W; ++dy)
+#pragma unroll
+        for (int dx = 0; dx < W; ++dx) {
+            float X = x + (float)(dx - R), Y = y + (float)(dy - R);
+            if (!in_bounds_fast(X, Y, img.width, img.height)) return false;
+            pv[dy * W + dx] = sample_fast<T>(data, img.width, X, Y);
+        }
+    return true;
+}
+
+// Integer-position window (exact pixel values).
+template <class T, int R>
+__device__ __forceinline__ void load_window_int(const DevImage& img, uint32_t x, uint32_t y,
+                                                float* pv) {
+    constexpr int W = 2 * R + 1;
+    const T* data = static_cast<const T*>(img.data);
+#pragma unroll
+    for (int dy = 0; dy < W; ++dy)
+#pragma unroll
+        for (int dx = 0; dx < W; ++dx)
+            pv[dy * W + dx] = pix<T>(data, (size_t)(y + dy - R) * img.width + (x + dx - R));
+}
+
+__device__ __forceinline__ float zmin_of(double inv_depth) { return (float)(1.0e-4 * inv_depth); }
+
+
+// ---- sweep, warp per site ----------------------------------------------------
+// Lanes take hypotheses lane, lane+32, ...; each lane keeps the running
+// best/second state, and a warp merge reproduces the reference's sort.
+template <class T, bool EXACT, int R, int COST>
+__global__ void __launch_bounds__(256) k_sweep_site(BatchDev b, const uint32_t* __restrict__ site_ref,
+                                                    uint64_t total, SiteRank* __restrict__ rank,
+                                                    uint8_t* __restrict__ status,
+                                                    RefCounters* __restrict__ ctr) {
+    constexpr int W = 2 * R + 1;
+    const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint32_t lane = lane_id();
+    if (gw >= total) return;
+    const uint32_t r = site_ref[gw];
+    const DevReference& ref = b.refs[r];
+    const uint32_t local = (uint32_t)(gw - b.site_off[r]);
+    uint32_t x, y;
+    site_xy(ref, local, x, y);
+    const DevProfile& prof = b.prof;
+    double contrast = 0.0;
+    if (lane == 0) contrast = patch_contrast_exact<T>(ref.img, (double)x, (double)y, R);
+    contrast = __shfl_sync(0xffffffffu, contrast, 0);
+    if (contrast < prof.min_contrast) {
+        if (lane == 0) status[gw] = kSiteLowContrast;
+        return;
+    }
+    if (lane == 0) atomicAdd(&ctr[r].sampled, 1ull);
+    float pv[W * W];
+    float pmean = 0.f, pvar = 0.f;
+    if (!EXACT) {
+        load_window_int<T, R>(ref.img, x, y, pv);
+        window_stats<R>(pv, pmean, pvar);
+    }
+    Rank st = rank_empty();
+    const int n_src = ref.n_src;
+    for (int k = lane; k < prof.planes; k += 32) {
+        const double depth = hypothesis_depth(k, prof.planes, ref.search_min, ref.search_max);
+        const double inv = ddiv(1.0, depth);
+        double errs[kMaxSources];
+        int n = 0;
+        for (int s = 0; s < n_src; ++s) {
+            const DevSource& src = ref.src[s];
+            double e;
+            bool ok;
+            if (EXACT) {
+                ok = patch_error_exact<T>(prof, ref.cam, ref.img, src.cam, src.img, ref.focal,
+                                          (double)x, (double)y, depth, e);
+            } else {
+                float H[9];
+                plane_h(src.fwd_A, src.fwd_b, (float)inv, H);
+                float c;
+                ok = window_cost_fast<T, R, COST>(prof, pv, pmean, pvar, H, zmin_of(inv), src.img,
+                                                  (float)x, (float)y, c);
+                e = c;
+            }
+            if (ok && e <= prof.max_error) errs[n++] = e;
+        }
+        if (n > 0) {
+            Rank c;
+            c.support = n;
+            c.plane = k;
+            c.error = median_of(errs, n);
+            c.second = kInf;
+            st = rank_merge(st, c);
+        }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) st = rank_shfl_merge(st, off);
+    if (lane != 0) return;
+    SiteRank out;
+    out.support = st.support;
+    out.plane = st.plane;
+    out.error = st.error;
+    out.margin = isinf(st.second) ? kInf : dsub(st.second, st.error);
+    uint8_t code;
+    if (st.support < 0)
+        code = kSiteNoCandidate;
+    else if (st.error > prof.max_error || out.margin < prof.min_margin)
+        code = kSiteGateRejected;
+    else
+        code = kSiteAccepted;
+    rank[gw] = out;
+    status[gw] = code;
+}
+
+// ---- sweep, tiled ZNCC (fast policy) -----------------------------------------
+// A CTA owns a 32x8 block of grid sites.  For every (plane, source) it warps
+// the block's pixel footprint into the source once (f32 homography and f32
+// bilinear), then forms the window sums of s, s^2 and r*s with separable box
+// filters, so overlapping windows (stride < window) share every bilinear
+// sample.  Products and sums are formed in f64: s^2 - (sum s)^2/n cancels
+// badly in f32 on low-variance windows.  Invalid taps are NaN and poison
+// their windows, which reproduces the reference's all-taps-valid rule.
+template <class T, int R>
+__global__ void __launch_bounds__(256) k_sweep_tiled(BatchDev b, uint64_t total_sites_unused,
+                                                     SiteRank* __restrict__ rank,
+                                                     uint8_t* __restrict__ status,
+                                                     RefCounters* __restrict__ ctr) {
+    constexpr int W = 2 * R + 1;
+    constexpr int N = W * W;
+    extern __shared__ double smem_d[];
+    const uint32_t r = blockIdx.z;
+    const DevReference& ref = b.refs[r];
+    const DevProfile& prof = b.prof;
+    const uint32_t gx0 = blockIdx.x * kTileX, gy0 = blockIdx.y * kTileY;
+    if (gx0 >= ref.nx || gy0 >= ref.ny) return;
+    const int s = (int)ref.stride;
+    const int PX = (kTileX - 1) * s + W, PY = (kTileY - 1) * s + W;
+    const int npx = PX * PY;
+    double* hs = smem_d;                     // [PY][32] row sums of s
+    double* hss = hs + PY * kTileX;          // [PY][32] row sums of s^2
+    double* hrs = hss + PY * kTileX;         // [PY][32] row sums of r*s
+    float* refv = reinterpret_cast<float*>(hrs + PY * kTileX);  // [PY][PX] reference values
+    float* samp = refv + npx;                // [PY][PX] source samples (NaN = invalid)
+    float* costs = samp + npx;               // [n_src][256]
+    float* hA = costs + kMaxSources * 256;   // [n_src][12] homography parts
+    float* pinv = hA + kMaxSources * 12;     // [planes] inverse depths
+    const int tid = threadIdx.x;
+    const T* rdata = static_cast<const T*>(ref.img.data);
+    const int px0 = (int)(ref.border + gx0 * s) - R, py0 = (int)(ref.border + gy0 * s) - R;
+    for (int i = tid; i < npx; i += 256) {
+        int yy = i / PX, xx = i - yy * PX;
+        int X = px0 + xx, Y = py0 + yy;
+        float v = __int_as_float(0x7fc00000);
+        if (X >= 0 && Y >= 0 && X < (int)ref.img.width && Y < (int)ref.img.height)
+            v = pix<T>(rdata, (size_t)Y * ref.img.width + X);
+        refv[i] = v;
+    }
+    const int n_src = ref.n_src;
+    for (int i = tid; i < n_src * 12; i += 256) {
+        int j = i / 12, c = i - j * 12;
+        hA[i] = c < 9 ? ref.src[j].fwd_A[c] : ref.src[j].fwd_b[c - 9];
+    }
+    for (int k = tid; k < prof.planes; k += 256)
+        pinv[k] = (float)ddiv(1.0, hypothesis_depth(k, prof.planes, ref.search_min, ref.search_max));
+    __syncthreads();
+
+    const int tx = tid & 31, ty = tid >> 5;
+    const uint32_t gx = gx0 + tx, gy = gy0 + ty;
+    const bool active = gx < ref.nx && gy < ref.ny;
+    const uint64_t gsite = b.site_off[r] + (uint64_t)gy * ref.nx + gx;
+    // reference window statistics and the contrast gate on exact pixel values
+    double sr = 0.0, srr = 0.0;
+    bool sampled = false;
+    if (active) {
+        float mn = 3.0e38f, mx = -3.0e38f;
+        for (int dy = 0; dy < W; ++dy)
+            for (int dx = 0; dx < W; ++dx) {
+                float v = refv[(ty * s + dy) * PX + tx * s + dx];
+                mn = fminf(mn, v);
+                mx = fmaxf(mx, v);
+                sr += (double)v;
+                srr = fma((double)v, (double)v, srr);
+            }
+        double contrast = (double)mx - (double)mn;
+        sampled = contrast >= prof.min_contrast;
+        if (!sampled) status[gsite] = kSiteLowContrast;
+        else atomicAdd(&ctr[r].sampled, 1ull);
+    }
+    const double n = (double)N;
+    const double vr = srr - sr * sr / n;
+    const double minvar_n = prof.min_variance * n;
+    Rank st = rank_empty();
+    for (int k = 0; k < prof.planes; ++k) {
+        const float inv = pinv[k];
+        const float zmin = 1.0e-4f * inv;
+        for (int j = 0; j < n_src; ++j) {
+            const float* A = hA + j * 12;
+            const float H2 = fmaf(inv, A[9], A[2]);
+            const float H5 = fmaf(inv, A[10], A[5]);
+            const float H8 = fmaf(inv, A[11], A[8]);
+            const DevImage si = ref.src[j].img;
+            const T* sdata = static_cast<const T*>(si.data);
+            const float wl = (float)(si.width - 1), hl = (float)(si.height - 1);
+            for (int i = tid; i < npx; i += 256) {
+                int yy = i / PX, xx = i - yy * PX;
+                float X = (float)(px0 + xx), Y = (float)(py0 + yy);
+                float h2 = fmaf(A[6], X, fmaf(A[7], Y, H8));
+                float v = __int_as_float(0x7fc00000);
+                if (h2 > zmin) {
+                    float iv = __frcp_rn(h2);
+                    float u = fmaf(A[0], X, fmaf(A[1], Y, H2)) * iv;
+                    float q = fmaf(A[3], X, fmaf(A[4], Y, H5)) * iv;
+                    if (u >= 0.f && q >= 0.f && u < wl && q < hl)
+                        v = sample_fast<T>(sdata, si.width, u, q);
+                }
+                samp[i] = v;
+            }
+            __syncthreads();
+            for (int i = tid; i < PY * kTileX; i += 256) {
+                int row = i >> 5, col = i & 31;
+                const float* sp = samp + row * PX + col * s;
+                const float* rp = refv + row * PX + col * s;
+                double a = 0.0, bb = 0.0, c = 0.0;
+#pragma unroll
+                for (int dx = 0; dx < W; ++dx) {
+                    double v = (double)sp[dx];
+                    a += v;
+                    bb = fma(v, v, bb);
+                    c = fma((double)rp[dx], v, c);
+                }
+                hs[i] = a;
+                hss[i] = bb;
+                hrs[i] = c;
+            }
+            __syncthreads();
+            if (sampled) {
+                double a = 0.0, bb = 0.0, c = 0.0;
+#pragma unroll
+                for (int dy = 0; dy < W; ++dy) {
+                    int i = (ty * s + dy) * kTileX + tx;
+                    a += hs[i];
+                    bb += hss[i];
+                    c += hrs[i];
+                }
+                double vs = bb - a * a / n;
+                double cov = c - sr * a / n;
+                float cost = __int_as_float(0x7fc00000);
+                if (vs > 0.0 && vr > 0.0 && vs >= minvar_n && vr >= minvar_n)
+                    cost = (float)(1.0 - cov / sqrt(vr * vs));
+                costs[j * 256 + tid] = cost;  // NaN when invalid
+            }
+        }
+        if (sampled) {
+            double errs[kMaxSources];
+            int cnt = 0;
+            for (int j = 0; j < n_src; ++j) {
+                float c = costs[j * 256 + tid];
+                if ((double)c <= prof.max_error) errs[cnt++] = c;
+            }
+            if (cnt > 0) {
+                Rank c;
+                c.support = cnt;
+                c.plane = k;
+                c.error = median_of(errs, cnt);
+                c.second = kInf;
+                st = rank_merge(st, c);
+            }
+        }
+    }
+    if (!sampled) return;
+    SiteRank out;
+    out.support = st.support;
+    out.plane = st.plane;
+    out.error = st.error;
+    out.margin = isinf(st.second) ? kInf : dsub(st.second, st.error);
+    uint8_t code;
+    if (st.support < 0)
+        code = kSiteNoCandidate;
+    else if (st.error > prof.max_error || out.margin < prof.min_margin)
+        code = kSiteGateRejected;
+    else
+        code = kSiteAccepted;
+    rank[gsite] = out;
+    status[gsite] = code;
+}
+
+
+// ---- reciprocal check, warp per (candidate, source) ----------------------------
+// reciprocal_depth_observations (dense_legacy.rs:777-857) for one source:
+// direct cost at the re-projected reference position, projection into the
+// source, then estimate_single_view_depth (dense_legacy.rs:887-949) with lanes
+// over the source's hypotheses, and the reciprocal agreement test.
+template <class T, int R>
+__global__ void __launch_bounds__(256) k_reciprocal_exact(BatchDev b, const Cand* __restrict__ cands,
+                                                    const uint32_t* __restrict__ count,
+                                                    RecipObs* __restrict__ obs,
+                                                    RefCounters* __restrict__ ctr) {
+    const uint32_t lane = lane_id();
+    const uint64_t items = (uint64_t)(*count) * kMaxSources;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    const DevProfile& prof = b.prof;
+    for (uint64_t it = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; it < items;
+         it += nwarps) {
+        const uint32_t ci = (uint32_t)(it / kMaxSources);
+        const int si = (int)(it - (uint64_t)ci * kMaxSources);
+        const Cand cd = cands[ci];
+        const DevReference& ref = b.refs[cd.ref];
+        RecipObs res;
+        res.valid = 0;
+        res.pad = 0;
+        res.pos = D3{0, 0, 0};
+        bool ok = si < ref.n_src;
+        const DevSource& src = ref.src[ok ? si : 0];
+        D3 rp, sp;
+        if (ok) ok = project_exact(ref.cam, cd.pos, ref.img.width, ref.img.height, ref.focal, rp);
+        // direct cost of the reference window at (rp.x, rp.y), depth rp.z
+        if (ok) {
+            bool dok = false;
+            double de = 0.0;
+            if (lane == 0)
+                dok = patch_error_exact<T>(prof, ref.cam, ref.img, src.cam, src.img, ref.focal,
+                                           rp.x, rp.y, rp.z, de);
+            dok = __shfl_sync(0xffffffffu, dok, 0);
+            de = __shfl_sync(0xffffffffu, de, 0);
+            ok = dok && !(de > prof.max_error);
+        }
+        if (ok) ok = project_exact(src.cam, cd.pos, src.img.width, src.img.height, ref.focal, sp);
+        if (ok) {
+            double contrast = 0.0;
+            if (lane == 0) contrast = patch_contrast_exact<T>(src.img, sp.x, sp.y, R);
+            contrast = __shfl_sync(0xffffffffu, contrast, 0);
+            ok = !(contrast < prof.min_contrast);
+        }
+        if (ok) {
+            double be = kInf;
+            int bk = 0x7fffffff;
+            if (ok && lane == 0) atomicAdd(&ctr[cd.ref].recip_evals, (unsigned long long)prof.planes);
+            for (int k = lane; ok && k < prof.planes; k += 32) {
+                double d = hypothesis_depth(k, prof.planes, src.search_min, src.search_max);
+                double e;
+                const bool eok = patch_error_exact<T>(prof, src.cam, src.img, ref.cam, ref.img,
+                                                      ref.focal, sp.x, sp.y, d, e);
+                if (eok && e <= prof.max_error && e < be) {
+                    be = e;
+                    bk = k;
+                }
+            }
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                double oe = __shfl_down_sync(0xffffffffu, be, off);
+                int ok2 = __shfl_down_sync(0xffffffffu, bk, off);
+                if (oe < be || (oe == be && ok2 < bk)) {
+                    be = oe;
+                    bk = ok2;
+                }
+            }
+            bk = __shfl_sync(0xffffffffu, bk, 0);
+            if (bk == 0x7fffffff) {
+                ok = false;
+            } else {
+                double rd = hypothesis_depth(bk, prof.planes, src.search_min, src.search_max);
+                // reciprocal_depth_agrees (dense_legacy.rs:951-957)
+                double ex = sp.z;
+                bool agree = isfinite(ex) && isfinite(rd) && ex > 0.0 && rd > 0.0;
+                if (agree) {
+                    double scale = fmax(fmax(ex, rd), 1.0e-9);
+                    agree = ddiv(fabs(dsub(ex, rd)), scale) <= kMaxReciprocalRelativeDepthError;
+                }
+                if (agree) {
+                    res.pos = unproject_exact(src.cam, sp.x, sp.y, rd, src.img.width,
+                                              src.img.height, ref.focal);
+                    res.valid = finite3(res.pos) ? 1 : 0;
+                }
+            }
+        }
+        if (lane == 0) obs[it] = res;
+    }
+}
+
+// ---- reciprocal check, fast policy ---------------------------------------------
+// Same contract as k_reciprocal for the fast policy, organised for the
+// memory system: one warp per (candidate, source);
+//  * the direct cost and the exact-f64 source contrast run lane-parallel over
+//    the window taps with warp reductions (max/min are order-free, so the
+//    contrast gate stays exact);
+//  * the single-view sweep moves every window tap monotonically along its
+//    epipolar line as the inverse depth varies (a 1-D projective map), so the
+//    reference texels of all hypotheses lie in the bounding box of the 4 window
+//    corners mapped at the first and last hypothesis.  That band is staged
+//    into shared memory with coalesced loads and every bilinear tap of every
+//    hypothesis reads it from there; a band too large for the buffer falls
+//    back to global loads.
+constexpr int kBandCap = 1344;  // texels staged per warp (8 warps x 5.25 KB static smem)
+
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ float warp_minf(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ float warp_maxf(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+struct BandView {
+    const float* band;
+    int bx0, by0, bw, bh;
+};
+
+// Window cost against the fixed window pv (mean pm, squared deviation pvar),
+// sampling through H at taps (x + dx, y + dy).  The window rows run as a
+// rolled loop with the taps of a row unrolled: a fully unrolled 7x7 or 9x9
+// body, once per sampling path, outgrows the instruction cache.
+// Sampler: the staged band (BandSampler) or the image in global memory.
+struct BandSampler {
+    const float* band;
+    int bx0, by0, bw, bh;
+    __device__ __forceinline__ float operator()(float u, float v) const {
+        const float fu = floorf(u), fv = floorf(v);
+        int ix = (int)fu - bx0, iy = (int)fv - by0;
+        ix = min(max(ix, 0), bw - 2);
+        iy = min(max(iy, 0), bh - 2);
+        const float* q = band + iy * bw + ix;
+        const float tx = u - fu, ty = v - fv;
+        const float top = fmaf(q[1] - q[0], tx, q[0]);
+        const float bot = fmaf(q[bw + 1] - q[bw], tx, q[bw]);
+        return fmaf(bot - top, ty, top);
+    }
+};
+
+template <class T>
+struct GlobalSampler {
+    const T* data;
+    uint32_t width;
+    __device__ __forceinline__ float operator()(float u, float v) const {
+        return sample_fast<T>(data, width, u, v);
+    }
+};
+
+template <int R, int COST, class S>
+__device__ __forceinline__ bool window_cost_sampled(const float* pv, float pm, float pvar,
+                                                    const float* H, float zmin, float wl, float hl,
+                                                    float minvar, const S& sample, float x,
+                                                    float y, float& cost) {
+    constexpr int W = 2 * R + 1;
+    constexpr int N = W * W;
+    float sv[COST == 1 ? 1 : N];
+    float ss = 0.f, sss = 0.f, sps = 0.f;
+#pragma unroll 1
+    for (int dy = 0; dy < W; ++dy) {
+        const float Y = y + (float)(dy - R);
+        const float hx = fmaf(H[1], Y, H[2]), hy = fmaf(H[4], Y, H[5]), hz = fmaf(H[7], Y, H[8]);
+        const float* prow = pv + dy * W;
+#pragma unroll
+        for (int dx = 0; dx < W; ++dx) {
+            const float X = x + (float)(dx - R);
+            const float h2 = fmaf(H[6], X, hz);
+            if (!(h2 > zmin)) return false;
+            const float iv = __frcp_rn(h2);
+            const float u = fmaf(H[0], X, hx) * iv;
+            const float v = fmaf(H[3], X, hy) * iv;
+            if (!(u >= 0.f && v >= 0.f && u < wl && v < hl)) return false;
+            const float smp = sample(u, v);
+            if (COST == 1) {
+                const float s = smp - pm;
+                ss += s;
+                sss = fmaf(s, s, sss);
+                sps = fmaf(prow[dx] - pm, s, sps);
+            } else {
+                sv[dy * W + dx] = smp;
+                ss += smp;
+            }
+        }
+    }
+    if (COST == 1) {
+        const float n = (float)N;
+        const float vs = sss - ss * ss / n;
+        if (!(pvar > 0.f) || !(vs > 0.f) || pvar / n < minvar || vs / n < minvar) return false;
+        cost = 1.0f - sps * rsqrtf(pvar * vs);
+        return true;
+    }
+    const float ms = ss / (float)N;
+    float acc = 0.f;
+#pragma unroll
+    for (int i = 0; i < N; ++i) acc += fabsf((pv[i] - pm) - (sv[i] - ms));
+    cost = acc / (float)N;
+    return true;
+}
+
+// Best (lowest cost, then lowest index) hypothesis of this lane's share.
+template <int R, int COST, class S>
+__device__ __forceinline__ void sweep_lane(const DevProfile& prof, const DevSource& src,
+                                           const float* inv_tab, const float* pv, float pm,
+                                           float pvar, float wl, float hl, const S& sample,
+                                           float x0, float y0, uint32_t lane, float& be,
+                                           int& bk) {
+    const float minvar = (float)prof.min_variance;
+    for (int k = lane; k < prof.planes; k += 32) {
+        const float inv = inv_tab[k];
+        float H[9];
+        plane_h(src.bwd_A, src.bwd_b, inv, H);
+        float e;
+        if (window_cost_sampled<R, COST>(pv, pm, pvar, H, 1.0e-4f * inv, wl, hl, minvar, sample,
+                                         x0, y0, e) &&
+            (double)e <= prof.max_error && e < be) {
+            be = e;
+            bk = k;
+        }
+    }
+}
+
+template <class T, int R, int COST>
+__global__ void __launch_bounds__(256, 2) k_reciprocal_fast(BatchDev b, const Cand* __restrict__ cands,
+                                                         const uint32_t* __restrict__ count,
+                                                         RecipObs* __restrict__ obs,
+                                                         RefCounters* __restrict__ ctr) {
+    constexpr int W = 2 * R + 1;
+    constexpr int N = W * W;
+    __shared__ float band_all[8][kBandCap];
+    __shared__ float pv_all[8][N];
+    const uint32_t lane = lane_id(), wid = threadIdx.x >> 5;
+    float* band = band_all[wid];
+    float* pv = pv_all[wid];
+    const uint32_t ms = (uint32_t)b.max_src;
+    const uint64_t items = (uint64_t)(*count) * ms;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    const DevProfile& prof = b.prof;
+    for (uint64_t item = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; item < items;
+         item += nwarps) {
+        const uint32_t ci = (uint32_t)(item / ms);
+        const int si = (int)(item - (uint64_t)ci * ms);
+        const uint64_t it = (uint64_t)ci * kMaxSources + si;
+        const Cand cd = cands[ci];
+        const DevReference& ref = b.refs[cd.ref];
+        RecipObs res;
+        res.valid = 0;
+        res.pad = 0;
+        res.pos = D3{0, 0, 0};
+        bool ok = si < ref.n_src;
+        const DevSource& src = ref.src[ok ? si : 0];
+        const float* inv_tab = b.src_inv + ((size_t)cd.ref * kMaxSources + (ok ? si : 0)) * prof.planes;
+        D3 rp, sp;
+        if (ok) ok = project_exact(ref.cam, cd.pos, ref.img.width, ref.img.height, ref.focal, rp);
+        // direct cost of the reference window at (rp.x, rp.y), depth rp.z; lanes over taps
+        if (ok) {
+            const double inv = ddiv(1.0, rp.z);
+            float H[9];
+            plane_h(src.fwd_A, src.fwd_b, (float)inv, H);
+            const float zmin = zmin_of(inv);
+            const T* rdata = static_cast<const T*>(ref.img.data);
+            const T* sdata = static_cast<const T*>(src.img.data);
+            float rv[2] = {0.f, 0.f}, sv2[2] = {0.f, 0.f};
+            bool tv = true;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int t = lane + 32 * h;
+                if (t >= N) continue;
+                const float X = (float)rp.x + (float)(t % W - R);
+                const float Y = (float)rp.y + (float)(t / W - R);
+                if (!in_bounds_fast(X, Y, ref.img.width, ref.img.height)) {
+                    tv = false;
+                    continue;
+                }
+                rv[h] = sample_fast<T>(rdata, ref.img.width, X, Y);
+                const float h2 = fmaf(H[6], X, fmaf(H[7], Y, H[8]));
+                if (!(h2 > zmin)) {
+                    tv = false;
+                    continue;
+                }
+                const float iv = __frcp_rn(h2);
+                const float u = fmaf(H[0], X, fmaf(H[1], Y, H[2])) * iv;
+                const float v = fmaf(H[3], X, fmaf(H[4], Y, H[5])) * iv;
+                if (!in_bounds_fast(u, v, src.img.width, src.img.height)) {
+                    tv = false;
+                    continue;
+                }
+                sv2[h] = sample_fast<T>(sdata, src.img.width, u, v);
+            }
+            ok = __all_sync(0xffffffffu, tv);
+            if (ok) {
+                const float n = (float)N;
+                const bool h1 = lane + 32 < N;
+                const float mr = warp_sum(rv[0] + (h1 ? rv[1] : 0.f)) / n;
+                const float ms = warp_sum(sv2[0] + (h1 ? sv2[1] : 0.f)) / n;
+                const float dr0 = rv[0] - mr, ds0 = sv2[0] - ms;
+                const float dr1 = h1 ? rv[1] - mr : 0.f, ds1 = h1 ? sv2[1] - ms : 0.f;
+                float cost;
+                if (COST == 1) {
+                    const float cov = warp_sum(dr0 * ds0 + dr1 * ds1);
+                    const float vr = warp_sum(dr0 * dr0 + dr1 * dr1);
+                    const float vs = warp_sum(ds0 * ds0 + ds1 * ds1);
+                    if (!(vr > 0.f) || !(vs > 0.f) || vr / n < (float)prof.min_variance ||
+                        vs / n < (float)prof.min_variance)
+                        ok = false;
+                    cost = 1.0f - cov * rsqrtf(vr * vs);
+                } else {
+                    cost = warp_sum(fabsf(dr0 - ds0) + (h1 ? fabsf(dr1 - ds1) : 0.f)) / n;
+                }
+                ok = ok && !((double)cost > prof.max_error);
+            }
+        }
+        if (ok) ok = project_exact(src.cam, cd.pos, src.img.width, src.img.height, ref.focal, sp);
+        // exact patch_contrast of the source window at (sp.x, sp.y), lanes over taps
+        float pm = 0.f, pvar = 0.f;
+        if (ok) {
+            double mn = kInf, mx = -kInf;
+            bool inb = true;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int t = lane + 32 * h;
+                if (t >= N) continue;
+                double v;
+                if (!sample_exact<T>(src.img, dadd(sp.x, (double)(t % W - R)),
+                                     dadd(sp.y, (double)(t / W - R)), v)) {
+                    inb = false;
+                    continue;
+                }
+                mn = fmin(mn, v);
+                mx = fmax(mx, v);
+                pv[t] = (float)v;
+            }
+            ok = __all_sync(0xffffffffu, inb);
+            if (ok) {
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+                    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+                }
+                ok = !(dsub(mx, mn) < prof.min_contrast);
+            }
+            __syncwarp();
+            if (ok) {
+                const bool h1 = lane + 32 < N;
+                const float p0 = pv[lane < N ? lane : 0], p1 = h1 ? pv[lane + 32] : 0.f;
+                pm = warp_sum((lane < N ? p0 : 0.f) + p1) / (float)N;
+                const float d0 = lane < N ? p0 - pm : 0.f, d1 = h1 ? p1 - pm : 0.f;
+                pvar = warp_sum(d0 * d0 + d1 * d1);
+            }
+        }
+        if (ok) {
+            // band of the reference texels that every hypothesis can reach
+            BandView bv{nullptr, 0, 0, 0, 0};
+            {
+                const int k = (lane & 1) ? prof.planes - 1 : 0;
+                const float cx = (float)sp.x + ((lane & 2) ? (float)R : -(float)R);
+                const float cy = (float)sp.y + ((lane & 4) ? (float)R : -(float)R);
+                float H[9];
+                plane_h(src.bwd_A, src.bwd_b, inv_tab[k], H);
+                const float h2 = fmaf(H[6], cx, fmaf(H[7], cy, H[8]));
+                float u = fmaf(H[0], cx, fmaf(H[1], cy, H[2])) / h2;
+                float v = fmaf(H[3], cx, fmaf(H[4], cy, H[5])) / h2;
+                bool good = lane >= 8 || (h2 > 0.f && isfinite(u) && isfinite(v));
+                good = __all_sync(0xffffffffu, good);
+                float umin = warp_minf(lane < 8 ? u : 3.0e38f), umax = warp_maxf(lane < 8 ? u : -3.0e38f);
+                float vmin = warp_minf(lane < 8 ? v : 3.0e38f), vmax = warp_maxf(lane < 8 ? v : -3.0e38f);
+                if (good) {
+                    const float wl = (float)(ref.img.width - 1), hl = (float)(ref.img.height - 1);
+                    umin = fmaxf(umin, 0.f);
+                    vmin = fmaxf(vmin, 0.f);
+                    umax = fminf(umax, wl);
+                    vmax = fminf(vmax, hl);
+                    if (umin <= umax && vmin <= vmax) {
+                        const int bx0 = max((int)floorf(umin) - 1, 0);
+                        const int by0 = max((int)floorf(vmin) - 1, 0);
+                        const int bx1 = min((int)floorf(umax) + 2, (int)ref.img.width - 1);
+                        const int by1 = min((int)floorf(vmax) + 2, (int)ref.img.height - 1);
+                        const int bw = bx1 - bx0 + 1, bh = by1 - by0 + 1;
+                        if (bw >= 2 && bh >= 2 && bw * bh <= kBandCap) {
+                            const T* rdata = static_cast<const T*>(ref.img.data);
+                            for (int i = lane; i < bw * bh; i += 32) {
+                                const int yy = i / bw, xx = i - yy * bw;
+                                band[i] = pix<T>(rdata, (size_t)(by0 + yy) * ref.img.width + bx0 + xx);
+                            }
+                            bv = BandView{band, bx0, by0, bw, bh};
+                        }
+                    }
+                }
+            }
+            __syncwarp();
+            if (lane == 0) atomicAdd(&ctr[cd.ref].recip_evals, (unsigned long long)prof.planes);
+            float be = 3.0e38f;
+            int bk = 0x7fffffff;
+            const float x0 = (float)sp.x, y0 = (float)sp.y;
+            const float wl = (float)(ref.img.width - 1), hl = (float)(ref.img.height - 1);
+            if (bv.band)
+                sweep_lane<R, COST>(prof, src, inv_tab, pv, pm, pvar, wl, hl,
+                                    BandSampler{bv.band, bv.bx0, bv.by0, bv.bw, bv.bh}, x0, y0,
+                                    lane, be, bk);
+            else
+                sweep_lane<R, COST>(prof, src, inv_tab, pv, pm, pvar, wl, hl,
+                                    GlobalSampler<T>{static_cast<const T*>(ref.img.data),
+                                                     ref.img.width},
+                                    x0, y0, lane, be, bk);
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                const float oe = __shfl_down_sync(0xffffffffu, be, off);
+                const int ok2 = __shfl_down_sync(0xffffffffu, bk, off);
+                if (oe < be || (oe == be && ok2 < bk)) {
+                    be = oe;
+                    bk = ok2;
+                }
+            }
+            bk = __shfl_sync(0xffffffffu, bk, 0);
+            if (bk == 0x7fffffff) {
+                ok = false;
+            } else {
+                const double rd = hypothesis_depth(bk, prof.planes, src.search_min, src.search_max);
+                const double ex = sp.z;
+                bool agree = isfinite(ex) && isfinite(rd) && ex > 0.0 && rd > 0.0;
+                if (agree) {
+                    const double scale = fmax(fmax(ex, rd), 1.0e-9);
+                    agree = ddiv(fabs(dsub(ex, rd)), scale) <= kMaxReciprocalRelativeDepthError;
+                }
+                if (agree) {
+                    res.pos = unproject_exact(src.cam, sp.x, sp.y, rd, src.img.width,
+                                              src.img.height, ref.focal);
+                    res.valid = finite3(res.pos) ? 1 : 0;
+                }
+            }
+        }
+        __syncwarp();
+        if (lane == 0 && si < ref.n_src) obs[it] = res;
+    }
+}
+
+
+// ---- surface completion proposals (dense_legacy.rs:542-650) ------------------
+template <class T, bool EXACT, int R, int COST>
+__global__ void __launch_bounds__(128) k_propose(BatchDev b, int pass, uint64_t total,
+                                                 const uint32_t* __restrict__ site_ref,
+                                                 const int32_t* __restrict__ occ,
+                                                 const OutPoint* __restrict__ pool,
+                                                 uint8_t* __restrict__ prop_status,
+                                                 Cand* __restrict__ prop, RefCounters* __restrict__ ctr) {
+    constexpr int W = 2 * R + 1;
+    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < total;
+         g += (uint64_t)gridDim.x * blockDim.x) {
+        prop_status[g] = kPropNone;
+        const uint32_t r = site_ref[g];
+        const DevReference& ref = b.refs[r];
+        if (ref.n_src == 0 || ref.stride == 0) continue;
+        if (pass > 0 && ctr[r].pass_additions[pass - 1] == 0) continue;
+        if (occ[g] >= 0) continue;
+        const uint32_t local = (uint32_t)(g - b.site_off[r]);
+        const uint32_t gy = local / ref.nx, gx = local - gy * ref.nx;
+        const uint32_t x = ref.border + gx * ref.stride, y = ref.border + gy * ref.stride;
+        double depths[8], confs[8], margins[8];
+        int n = 0;
+        for (int oy = -1; oy <= 1; ++oy)
+            for (int ox = -1; ox <= 1; ++ox) {
+                if (ox == 0 && oy == 0) continue;
+                int ngx = (int)gx + ox, ngy = (int)gy + oy;
+                if (ngx < 0 || ngy < 0 || ngx >= (int)ref.nx || ngy >= (int)ref.ny) continue;
+                int32_t pi = occ[b.site_off[r] + (uint64_t)ngy * ref.nx + ngx];
+                if (pi < 0) continue;
+                const OutPoint& pt = pool[pi];
+                D3 pos{(double)pt.p.x, (double)pt.p.y, (double)pt.p.z};
+                D3 q;
+                if (!project_exact(ref.cam, pos, ref.img.width, ref.img.height, ref.focal, q))
+                    continue;
+                depths[n] = q.z;
+                confs[n] = (double)pt.p.confidence;
+                margins[n] = (double)pt.a.depth_margin;
+                ++n;
+            }
+        // surface_depth_prediction (dense_legacy.rs:739-753)
+        if (n < kMinSurfaceNeighbors) continue;
+        double sorted[8];
+        for (int i = 0; i < n; ++i) sorted[i] = depths[i];
+        double predicted = median_of(sorted, n);
+        double mn = sorted[0], mx = sorted[n - 1];
+        if (!isfinite(mn) || !isfinite(mx) || mn <= 0.0 || mx <= 0.0) continue;
+        if (ddiv(dsub(mx, mn), mx) > kMaxSurfaceNeighborSpread) continue;
+        RefCounters& c = ctr[r];
+        atomicAdd(&c.proposals, 1ull);
+        if (patch_contrast_exact<T>(ref.img, (double)x, (double)y, R) < b.prof.min_contrast) {
+            atomicAdd(&c.rej_texture, 1ull);
+            prop_status[g] = kPropTexture;
+            continue;
+        }
+        D3 ppos = unproject_exact(ref.cam, (double)x, (double)y, predicted, ref.img.width,
+                                  ref.img.height, ref.focal);
+        double errs[kMaxSources];
+        int ne = 0;
+        float pv[W * W];
+        float pm = 0.f, pvv = 0.f;
+        double inv = ddiv(1.0, predicted);
+        if (!EXACT) {
+            load_window_int<T, R>(ref.img, x, y, pv);
+            window_stats<R>(pv, pm, pvv);
+        }
+        for (int s = 0; s < ref.n_src; ++s) {
+            const DevSource& src = ref.src[s];
+            double e;
+            bool ok;
+            if (EXACT) {
+                ok = patch_error_exact<T>(b.prof, ref.cam, ref.img, src.cam, src.img, ref.focal,
+                                          (double)x, (double)y, predicted, e);
+            } else {
+                float H[9];
+                plane_h(src.fwd_A, src.fwd_b, (float)inv, H);
+                float cst;
+                ok = window_cost_fast<T, R, COST>(b.prof, pv, pm, pvv, H, zmin_of(inv), src.img,
+                                                  (float)x, (float)y, cst);
+                e = cst;
+            }
+            if (ok && e <= b.prof.max_error) errs[ne++] = e;
+        }
+        if (ne == 0) {
+            atomicAdd(&c.rej_cross, 1ull);
+            prop_status[g] = kPropCrossView;
+            continue;
+        }
+        double direct_error = median_of(errs, ne);
+        double csum = 0.0, msum = 0.0;
+        for (int i = 0; i < n; ++i) csum = dadd(csum, confs[i]);
+        for (int i = 0; i < n; ++i) msum = dadd(msum, margins[i]);
+        Cand cd;
+        cd.ref = r;
+        cd.site = local;
+        cd.x = x;
+        cd.y = y;
+        cd.pos = ppos;
+        cd.depth = predicted;
+        cd.error = direct_error;
+        cd.margin = ddiv(msum, (double)n);
+        cd.nconf = ddiv(csum, (double)n);
+        cd.support = ne;
+        cd.pad = 0;
+        prop[g] = cd;
+        prop_status[g] = kPropCandidate;
+    }
+}
+
+
+inline int sm_count() {
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+    }
+    return sms;
+}
+
+// Dispatch helpers over (storage type, exactness, radius).
+
+}  // namespace typed_detail
+
+template <class T>
+cudaError_t Typed<T>::sweep_site(const BatchDev& b, const uint32_t* site_ref, uint64_t total,
+                                 SiteRank* rank, uint8_t* status, RefCounters* ctr,
+                                 cudaStream_t st) {
+    using namespace typed_detail;
+    const unsigned blocks = (unsigned)((total * 32 + 255) / 256);
+#define V3D_SITE(E, RR, C)                                                                   \
+    if (b.exact == E && b.prof.radius == RR && (E || b.prof.cost == C)) {                     \
+        k_sweep_site<T, E, RR, C><<<blocks, 256, 0, st>>>(b, site_ref, total, rank, status, ctr); \
+        return cudaGetLastError();                                                           \
+    }
+#define V3D_SITE_R(RR) V3D_SITE(true, RR, 0) V3D_SITE(false, RR, 0) V3D_SITE(false, RR, 1)
+    V3D_SITE_R(1) V3D_SITE_R(2) V3D_SITE_R(3) V3D_SITE_R(4)
+#undef V3D_SITE_R
+#undef V3D_SITE
+    return cudaErrorInvalidValue;
+}
+
+template <class T>
+cudaError_t Typed<T>::sweep_tiled(const BatchDev& b, uint32_t max_nx, uint32_t max_ny,
+                                  uint32_t stride, SiteRank* rank, uint8_t* status,
+                                  RefCounters* ctr, cudaStream_t st) {
+    using namespace typed_detail;
+    auto run = [&](auto kern, int W) -> cudaError_t {
+        const int PX = (kTileX - 1) * (int)stride + W, PY = (kTileY - 1) * (int)stride + W;
+        const size_t smem = sizeof(double) * 3 * (size_t)PY * kTileX +
+                            sizeof(float) * (2 * (size_t)PX * PY + kMaxSources * 256 +
+                                             kMaxSources * 12 + kMaxPlanes);
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) return e;
+        dim3 grid((max_nx + kTileX - 1) / kTileX, (max_ny + kTileY - 1) / kTileY, b.n_refs);
+        kern<<<grid, 256, smem, st>>>(b, 0, rank, status, ctr);
+        return cudaGetLastError();
+    };
+    switch (b.prof.radius) {
+        case 1: return run(k_sweep_tiled<T, 1>, 3);
+        case 2: return run(k_sweep_tiled<T, 2>, 5);
+        case 3: return run(k_sweep_tiled<T, 3>, 7);
+        case 4: return run(k_sweep_tiled<T, 4>, 9);
+    }
+    return cudaErrorInvalidValue;
+}
+
+template <class T>
+cudaError_t Typed<T>::reciprocal(const BatchDev& b, const Cand* cands, const uint32_t* count,
+                                 RecipObs* obs, RefCounters* ctr, cudaStream_t st) {
+    using namespace typed_detail;
+    const unsigned blocks = (unsigned)sm_count() * 8;
+#define V3D_REC(RR)                                                                            \
+    if (b.prof.radius == RR) {                                                                 \
+        if (b.exact)                                                                           \
+            k_reciprocal_exact<T, RR><<<blocks, 256, 0, st>>>(b, cands, count, obs, ctr);      \
+        else if (b.prof.cost == 1)                                                             \
+            k_reciprocal_fast<T, RR, 1><<<blocks, 256, 0, st>>>(b, cands, count, obs, ctr);    \
+        else                                                                                   \
+            k_reciprocal_fast<T, RR, 0><<<blocks, 256, 0, st>>>(b, cands, count, obs, ctr);    \
+        return cudaGetLastError();                                                             \
+    }
+    V3D_REC(1) V3D_REC(2) V3D_REC(3) V3D_REC(4)
+#undef V3D_REC
+    return cudaErrorInvalidValue;
+}
+
+template <class T>
+cudaError_t Typed<T>::propose(const BatchDev& b, int pass, uint64_t total,
+                              const uint32_t* site_ref, const int32_t* occ, const OutPoint* pool,
+                              uint8_t* prop_status, Cand* prop, RefCounters* ctr,
+                              cudaStream_t st) {
+    using namespace typed_detail;
+    uint64_t blocks = (total + 127) / 128;
+    if (blocks > (uint64_t)sm_count() * 64) blocks = (uint64_t)sm_count() * 64;
+    if (blocks == 0) blocks = 1;
+#define V3D_PROP(E, RR, C)                                                                \
+    if (b.exact == E && b.prof.radius == RR && (E || b.prof.cost == C)) {                  \
+        k_propose<T, E, RR, C><<<(unsigned)blocks, 128, 0, st>>>(b, pass, total, site_ref, \
+                                                                 occ, pool, prop_status,   \
+                                                                 prop, ctr);               \
+        return cudaGetLastError();                                                        \
+    }
+#define V3D_PROP_R(RR) V3D_PROP(true, RR, 0) V3D_PROP(false, RR, 0) V3D_PROP(false, RR, 1)
+    V3D_PROP_R(1) V3D_PROP_R(2) V3D_PROP_R(3) V3D_PROP_R(4)
+#undef V3D_PROP_R
+#undef V3D_PROP
+    return cudaErrorInvalidValue;
+}
+
+}  // namespace v3d

@@ -183,7 +183,9 @@ class RunInfo(C.Structure):
                 ("grid_sites", C.c_uint64), ("plane_view_units", C.c_uint64),
                 ("sweep_ms", C.c_double), ("reciprocal_ms", C.c_double),
                 ("completion_ms", C.c_double), ("reciprocal_plane_evaluations", C.c_uint64),
-                ("candidates", C.c_uint64)]
+                ("candidates", C.c_uint64), ("host_plan_ms", C.c_double),
+                ("host_upload_ms", C.c_double), ("host_wait_ms", C.c_double),
+                ("host_assemble_ms", C.c_double)]
 
 
 CANCEL_FN = C.CFUNCTYPE(C.c_int32, C.c_void_p)

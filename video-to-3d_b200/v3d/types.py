@@ -128,8 +128,8 @@ def _opt(has, value):
 def _array(ptr, n, dtype):
     if n == 0 or not ptr:
         return np.zeros(0, dtype=dtype)
-    buf = C.cast(ptr, C.POINTER(C.c_uint8 * (n * dtype.itemsize))).contents
-    return np.frombuffer(bytes(buf), dtype=dtype).copy()
+    raw = np.ctypeslib.as_array(C.cast(ptr, C.POINTER(C.c_uint8)), shape=(n * dtype.itemsize,))
+    return raw.view(dtype).copy()
 
 
 def stats_dict(s):
