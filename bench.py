@@ -5,11 +5,12 @@ Workload (one step): the full native clip — 640x360, 120 keyframes on a 40°
 arc with ±2° seeded jitter, 4-octave value-noise planes, noise σ=0.01 — where
 every keyframe is a reference against its 8 nearest source views, with 128
 inverse-depth hypotheses and a 7x7 ZNCC window at grid stride 2, followed by
-the reciprocal check, fusion and both surface-completion passes.  One step is
-one call of v3d_reconstruct_reference_patches over all 120 references.
+the reciprocal check, fusion, both surface-completion passes and the
+reference-grid triangle gates of every patch.  One step is one call of
+v3d_reconstruct_reference_patches_meshed over all 120 references.
 
   value  units / device time of the whole batch, frames already in HBM
-         (CUDA events on the library's stream: sweep through completion)
+         (CUDA events on the library's stream: sweep through the mesh gates)
   e2e    units / wall time of the C-ABI call with pinned host frames
          (host->device upload, planning, kernels, device->host results)
 
@@ -62,7 +63,8 @@ def dist_env():
 
 def workload(args):
     return {"workload": "full native clip %dx%d, %d keyframes, every keyframe vs its %d nearest "
-                        "views, %d planes, %dx%d ZNCC, stride %d, reciprocal+fusion+completion, "
+                        "views, %d planes, %dx%d ZNCC, stride %d, reciprocal+fusion+completion+"
+                        "grid-mesh gates, "
                         "%s images" % (WIDTH, HEIGHT, args.frames, SOURCES, PLANES,
                                        2 * RADIUS + 1, 2 * RADIUS + 1, STRIDE, args.storage),
             "width": WIDTH, "height": HEIGHT, "keyframes": args.frames, "source_views": SOURCES,
@@ -218,15 +220,15 @@ def run_ours(args, rank, world, local):
 
     def step():
         t0 = time.perf_counter()
-        res = ctx.reconstruct_reference_patches(frames, clip.cameras, clip.sparse, clip.focal,
-                                                refs, profile=prof)
+        res = ctx.reconstruct_reference_patches_meshed(frames, clip.cameras, clip.sparse,
+                                                       clip.focal, refs, profile=prof)
         return time.perf_counter() - t0, res, ctx.last_run_info()
 
     for _ in range(args.warmup):
         step()
     clocks = Clocks(local)
     clocks.start()
-    dev_ms, wall, infos, points = [], [], [], 0
+    dev_ms, wall, infos, points, triangles = [], [], [], 0, 0
     for _ in range(args.steps):
         flush.zero_()
         torch.cuda.synchronize()
@@ -239,7 +241,8 @@ def run_ours(args, rank, world, local):
         dev_ms.append(info["device_ms"])
         wall.append(w)
         infos.append(info)
-        points = sum(len(r.points) for r in res if r is not None)
+        points = sum(len(r[0].points) for r in res if r is not None)
+        triangles = sum(len(r[1].triangles) for r in res if r is not None)
     clk = clocks.stop()
     units = infos[-1]["plane_view_units"]
     dev_s = float(np.mean(dev_ms)) / 1e3
@@ -258,6 +261,7 @@ def run_ours(args, rank, world, local):
     sweep_ms = float(np.mean([i["sweep_ms"] for i in infos]))
     recip_ms = float(np.mean([i["reciprocal_ms"] for i in infos]))
     comp_ms = float(np.mean([i["completion_ms"] for i in infos]))
+    mesh_ms = float(np.mean([i["mesh_ms"] for i in infos]))
     line = None
     if rank == 0:
         peaks = {}
@@ -285,16 +289,19 @@ def run_ours(args, rank, world, local):
             "data": "synthetic (seeded value-noise planes, ray-cast)", "config": workload(args),
             "clocks": clk,
             "e2e": {"value": total_units / wall_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": points * 72, "ms_per_step": wall_s * 1e3},
+                    "d2h_bytes_per_step": points * 72 + triangles * 32,
+                    "ms_per_step": wall_s * 1e3},
             "gpu_launches": infos[-1]["kernel_launches"],
             "stages_ms": {"sweep": sweep_ms, "reciprocal_primary": recip_ms,
-                          "completion": comp_ms, "total": dev_s * 1e3, **host},
+                          "completion": comp_ms, "mesh": mesh_ms, "total": dev_s * 1e3,
+                          **host},
             "roofline": {"bound": "hbm", "kernel": kernel, "achieved": achieved, "peak": hbm,
                          "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
                          "note": "achieved = bilinear-footprint bytes 4*W^2*b per window "
                                  "evaluation / kernel time, against the measured HBM copy peak "
                                  "(of measured); the gathers are served by L1/L2"},
             "points_per_step": points,
+            "triangles_per_step": triangles,
         }
         if world == 1 and not args.no_cpu_baseline:
             v, info = cpu_baseline(clip, frames, prof, os.cpu_count() or 1)

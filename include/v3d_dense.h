@@ -360,6 +360,23 @@ int32_t v3d_reconstruct_reference_patches(
     v3d_cancel_fn cancel, void* cancel_user,
     v3d_dense_result* out, int32_t* present);
 
+/* v3d_reconstruct_reference_patches followed, on the device and in the same
+ * batch, by the reference-grid triangle gates of every patch
+ * (mesh_legacy.rs:150-358 over the patch's points with its reference camera,
+ * as mesh.rs:100-207 runs them per patch).  mesh_out[i] holds patch i's
+ * triangles (indices into out[i].points) and statistics; width and height are
+ * the reference frame's. */
+int32_t v3d_reconstruct_reference_patches_meshed(
+    v3d_context* ctx,
+    const v3d_frame* frames, uint64_t n_frames,
+    const v3d_camera* cameras, uint64_t n_cameras,
+    const double* sparse_xyz, uint64_t n_sparse,
+    double focal, int32_t fine_grid,
+    const v3d_profile* profile,
+    const uint64_t* camera_indices, uint64_t n_references,
+    v3d_cancel_fn cancel, void* cancel_user,
+    v3d_dense_result* out, v3d_mesh_result* mesh_out, int32_t* present);
+
 /* estimate_depth_points_limited (dense.rs:250-330): the multi-reference plan
  * (at most 6 attempts, `reference_views` accepted patches), the legacy
  * fallback, attempt merging and patch concatenation.  `omitted_references`
@@ -403,6 +420,8 @@ typedef struct v3d_run_info {
     double host_upload_ms;    /* staging and enqueueing uploads and kernels */
     double host_wait_ms;      /* waiting for the device, read-back included */
     double host_assemble_ms;  /* splitting the point pool per reference, medians */
+    double mesh_ms;           /* device mesh stage of the _meshed call */
+    uint64_t triangles;       /* accepted triangles of the _meshed call */
 } v3d_run_info;
 
 int32_t v3d_last_run_info(const v3d_context* ctx, v3d_run_info* out);

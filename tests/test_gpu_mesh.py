@@ -76,3 +76,32 @@ def test_mesh_of_dense_patches(ctx, oracle):
                                                    clip.width, clip.height, clip.focal)
     same_mesh(g, o)
     assert g.stats["accepted_triangles"] > 0
+
+
+@pytest.mark.parametrize("storage,exact", [("rgba8", True), ("f32", True), ("f32", False)])
+def test_meshed_reference_patches_match_per_patch_mesh(ctx, oracle, storage, exact):
+    """Device mesh of every patch in the batch == the legacy mesh of that patch."""
+    from v3d import abi
+    clip = synth.make_clip(192, 112, 7, 20.0, 1.5, seed=21, noise_sigma=0.01,
+                           landmark_cameras=[1, 3, 5], landmarks_per_camera=300)
+    frames = clip.frames(storage)
+    if storage == "rgba8":
+        prof = profiles.reference()
+    else:
+        prof = profiles.zncc(2, 32, 4, 2, precision=abi.PRECISION_EXACT64 if exact
+                             else abi.PRECISION_FAST32)
+    refs = [0, 3, 6]
+    got = ctx.reconstruct_reference_patches_meshed(frames, clip.cameras, clip.sparse, clip.focal,
+                                                   refs, profile=prof)
+    plain = ctx.reconstruct_reference_patches(frames, clip.cameras, clip.sparse, clip.focal, refs,
+                                              profile=prof)
+    total = 0
+    for (d, m), p in zip(got, plain):
+        # the dense half is the plain call's result
+        assert d.stats == p.stats and d.points.tobytes() == p.points.tobytes()
+        o = oracle.reconstruct_dense_mesh_with_control(d.points, d.grid_sites, d.stats,
+                                                       clip.cameras, clip.width, clip.height,
+                                                       clip.focal)
+        same_mesh(m, o)
+        total += len(m.triangles)
+    assert total > 0

@@ -245,6 +245,8 @@ int32_t v3d_last_run_info(const v3d_context* ctx, v3d_run_info* out) {
     out->host_upload_ms = ctx->last_upload_ms;
     out->host_wait_ms = ctx->last_wait_ms;
     out->host_assemble_ms = ctx->last_assemble_ms;
+    out->mesh_ms = ctx->last_mesh_ms;
+    out->triangles = ctx->last_triangles;
     return V3D_OK;
 }
 
@@ -367,17 +369,38 @@ int32_t v3d_estimate_depth_points_with_control(v3d_context* ctx, const v3d_frame
     return status_of(res[0]);
 }
 
-int32_t v3d_reconstruct_reference_patches(v3d_context* ctx, const v3d_frame* frames,
-                                          uint64_t n_frames, const v3d_camera* cameras,
-                                          uint64_t n_cameras, const double* sparse_xyz,
-                                          uint64_t n_sparse, double focal, int32_t fine_grid,
-                                          const v3d_profile* profile,
-                                          const uint64_t* camera_indices, uint64_t n_refs,
-                                          v3d_cancel_fn cancel, void* cancel_user,
-                                          v3d_dense_result* out, int32_t* present) {
+}  // extern "C"
+
+namespace {
+
+// mesh.rs from_legacy (mesh.rs:244-281) of one patch's legacy mesh.
+void fill_mesh(v3d_mesh_result* out, const MeshOut& m) {
+    std::memset(out, 0, sizeof(*out));
+    out->stats = m.stats;
+    out->n_triangles = m.tris.size();
+    out->triangles = dup(m.tris);
+    if (m.stats.has_reference_frame) {
+        std::vector<uint64_t> rf{m.stats.reference_frame};
+        out->n_reference_frames = 1;
+        out->reference_frames = dup(rf);
+        v3d_mesh_stats p = m.stats;
+        p.point_count = m.stats.grid_vertices + m.stats.rejected_grid_vertices;
+        std::vector<v3d_mesh_stats> ps{p};
+        out->n_patches = 1;
+        out->patches = dup(ps);
+    }
+}
+
+int32_t reference_patches(v3d_context* ctx, const v3d_frame* frames, uint64_t n_frames,
+                          const v3d_camera* cameras, uint64_t n_cameras, const double* sparse_xyz,
+                          uint64_t n_sparse, double focal, int32_t fine_grid,
+                          const v3d_profile* profile, const uint64_t* camera_indices,
+                          uint64_t n_refs, v3d_cancel_fn cancel, void* cancel_user,
+                          v3d_dense_result* out, v3d_mesh_result* mesh_out, int32_t* present) {
     if (!out || !present || (n_refs && !camera_indices)) return V3D_ERR_INVALID_ARGUMENT;
     for (uint64_t i = 0; i < n_refs; ++i) {
         std::memset(&out[i], 0, sizeof(out[i]));
+        if (mesh_out) std::memset(&mesh_out[i], 0, sizeof(mesh_out[i]));
         present[i] = 0;
     }
     if (!ensure_device(ctx)) return V3D_ERR_NO_DEVICE;
@@ -417,9 +440,22 @@ int32_t v3d_reconstruct_reference_patches(v3d_context* ctx, const v3d_frame* fra
     const double plan_ms = std::chrono::duration<double, std::milli>(
                                std::chrono::steady_clock::now() - t_plan).count();
     std::vector<PassResult> res;
-    int32_t st = run_batch(ctx, *profile, frames, n_frames, focal, plans, res);
+    std::vector<MeshOut> meshes;
+    int32_t st = run_batch(ctx, *profile, frames, n_frames, focal, plans, res,
+                           mesh_out ? &meshes : nullptr);
     ctx->last_plan_ms = plan_ms;
     if (st < 0) return st;
+    if (mesh_out && meshes.size() != n_refs) {
+        meshes.assign(n_refs, MeshOut{});
+        for (uint64_t i = 0; i < n_refs; ++i) {
+            v3d_mesh_stats& s = meshes[i].stats;
+            s.has_reference_frame = plans[i].have_reference;
+            s.reference_frame = plans[i].reference_frame;
+            s.has_skip_reason = 1;
+            std::strncpy(s.skip_reason, "dense reconstruction was not attempted",
+                         V3D_SKIP_REASON_BYTES - 1);
+        }
+    }
     for (uint64_t i = 0; i < n_refs; ++i) {
         present[i] = pres[i] ? 1 : 0;
         if (!pres[i]) continue;
@@ -428,8 +464,50 @@ int32_t v3d_reconstruct_reference_patches(v3d_context* ctx, const v3d_frame* fra
         res[i].stats.has_reference_frame = 1;
         res[i].stats.reference_frame = in.cameras[camera_indices[i]].frame_index;
         fill_pass(&out[i], res[i]);
+        if (mesh_out) {
+            if (canceled[i] || !res[i].stats.attempted) {
+                v3d_mesh_stats& s = meshes[i].stats;
+                std::memset(&s, 0, sizeof(s));
+                meshes[i].tris.clear();
+                s.has_reference_frame = 1;
+                s.reference_frame = res[i].stats.reference_frame;
+                s.has_skip_reason = 1;
+                std::strncpy(s.skip_reason, "dense reconstruction was not attempted",
+                             V3D_SKIP_REASON_BYTES - 1);
+            }
+            fill_mesh(&mesh_out[i], meshes[i]);
+        }
     }
     return V3D_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t v3d_reconstruct_reference_patches(v3d_context* ctx, const v3d_frame* frames,
+                                          uint64_t n_frames, const v3d_camera* cameras,
+                                          uint64_t n_cameras, const double* sparse_xyz,
+                                          uint64_t n_sparse, double focal, int32_t fine_grid,
+                                          const v3d_profile* profile,
+                                          const uint64_t* camera_indices, uint64_t n_refs,
+                                          v3d_cancel_fn cancel, void* cancel_user,
+                                          v3d_dense_result* out, int32_t* present) {
+    return reference_patches(ctx, frames, n_frames, cameras, n_cameras, sparse_xyz, n_sparse,
+                             focal, fine_grid, profile, camera_indices, n_refs, cancel,
+                             cancel_user, out, nullptr, present);
+}
+
+int32_t v3d_reconstruct_reference_patches_meshed(
+    v3d_context* ctx, const v3d_frame* frames, uint64_t n_frames, const v3d_camera* cameras,
+    uint64_t n_cameras, const double* sparse_xyz, uint64_t n_sparse, double focal,
+    int32_t fine_grid, const v3d_profile* profile, const uint64_t* camera_indices,
+    uint64_t n_refs, v3d_cancel_fn cancel, void* cancel_user, v3d_dense_result* out,
+    v3d_mesh_result* mesh_out, int32_t* present) {
+    if (!mesh_out) return V3D_ERR_INVALID_ARGUMENT;
+    return reference_patches(ctx, frames, n_frames, cameras, n_cameras, sparse_xyz, n_sparse,
+                             focal, fine_grid, profile, camera_indices, n_refs, cancel,
+                             cancel_user, out, mesh_out, present);
 }
 
 int32_t v3d_has_distributed_landmarks(const v3d_frame* frames, uint64_t n_frames,

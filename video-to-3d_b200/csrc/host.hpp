@@ -39,6 +39,12 @@ struct RefPlan {
     uint32_t width = 0, height = 0, stride = 0, border = 0, nx = 0, ny = 0;
 };
 
+// One patch's reference-grid triangles (mesh_legacy.rs:40-43).
+struct MeshOut {
+    v3d_mesh_stats stats{};
+    std::vector<v3d_mesh_triangle> tris;
+};
+
 // One pass's output (dense_legacy.rs:62-68 DenseAnalysis with DenseStats).
 struct PassResult {
     RefPlan plan;
@@ -118,15 +124,19 @@ struct v3d_context {
     float last_sweep_ms = 0.f, last_recip_ms = 0.f, last_completion_ms = 0.f;
     uint64_t last_recip_evals = 0, last_candidates = 0;
     double last_plan_ms = 0, last_upload_ms = 0, last_wait_ms = 0, last_assemble_ms = 0;
+    float last_mesh_ms = 0.f;
+    uint64_t last_triangles = 0;
 };
 
 namespace v3d {
 // ---- execution (pipeline.cpp) ----
 // Runs every non-skipped plan of `plans` as one device batch and fills
 // `results` (same order).  Returns a v3d_status.
+// With `mesh` set, the reference-grid triangle gates of every patch run on
+// the device after completion and (*mesh)[i] receives plan i's mesh.
 int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* frames,
                   size_t n_frames, double focal, const std::vector<RefPlan>& plans,
-                  std::vector<PassResult>& results);
+                  std::vector<PassResult>& results, std::vector<MeshOut>* mesh = nullptr);
 
 // The sweep of one planned pass alone, as per-site records (v3d_debug_sweep).
 int32_t run_sweep_records(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* frames,

@@ -18,6 +18,7 @@
 #include <stdexcept>
 
 #include "host.hpp"
+#include "mesh_batch.cuh"
 #include "pass_kernels.cuh"
 
 namespace v3d {
@@ -154,11 +155,22 @@ struct Prepared {
     uint8_t* d_pstat = nullptr;
     Cand* d_prop = nullptr;
     uint32_t* d_counts = nullptr;
+    // mesh stage
+    uint64_t total_slots = 0;
+    v3d_point* m_pts = nullptr;
+    v3d_grid_site* m_sites = nullptr;
+    uint32_t* m_patch = nullptr;
+    uint32_t* m_local = nullptr;
+    uint32_t* m_range = nullptr;
+    v3d_mesh_triangle* m_tris = nullptr;
+    uint32_t* m_tpatch = nullptr;
+    MeshScratch mesh{};
 };
 
 int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* frames,
                 size_t n_frames, double focal, const std::vector<RefPlan>& plans,
-                const std::vector<size_t>& active, bool sweep_only, Prepared& P) {
+                const std::vector<size_t>& active, bool sweep_only, Prepared& P,
+                bool with_mesh = false) {
     cudaStream_t stream = static_cast<cudaStream_t>(ctx->stream);
     P.active = active;
 
@@ -240,6 +252,24 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
     const size_t o_pstat = cv.take<uint8_t>(pc);
     const size_t o_prop = cv.take<Cand>(pc);
     const size_t o_counts = cv.take<uint32_t>(16);
+    // mesh stage: pool as mesh input, per-(segment, reference) ranges, scratch, triangles
+    uint64_t total_slots = 0;
+    for (size_t k = 0; k < n_active; ++k)
+        total_slots += mesh_slots(plans[active[k]].nx, plans[active[k]].ny);
+    P.total_slots = with_mesh ? total_slots : 0;
+    const uint64_t mc = with_mesh ? cap : 1;
+    const size_t o_mpts = cv.take<v3d_point>(mc);
+    const size_t o_msites = cv.take<v3d_grid_site>(mc);
+    const size_t o_mpatch = cv.take<uint32_t>(mc);
+    const size_t o_mlocal = cv.take<uint32_t>(mc);
+    const size_t o_mrange = cv.take<uint32_t>(6 * n_active);
+    const size_t mesh_bytes =
+        with_mesh ? mesh_scratch_layout(nullptr, static_cast<uint32_t>(n_active), cap, total,
+                                        total_slots, nullptr)
+                  : 0;
+    const size_t o_mscratch = cv.take<uint8_t>(mesh_bytes + 256);
+    const size_t o_mtris = cv.take<v3d_mesh_triangle>(with_mesh ? std::max<uint64_t>(total_slots, 1) : 1);
+    const size_t o_mtpatch = cv.take<uint32_t>(with_mesh ? std::max<uint64_t>(total_slots, 1) : 1);
     const size_t arena_need = cv.off + 256;
     if (!grow(&ctx->arena, &ctx->arena_bytes, arena_need, false)) {
         ctx->last_error = "device arena allocation failed";
@@ -334,6 +364,16 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
     P.d_pstat = reinterpret_cast<uint8_t*>(at(o_pstat));
     P.d_prop = reinterpret_cast<Cand*>(at(o_prop));
     auto* d_counts = P.d_counts = reinterpret_cast<uint32_t*>(at(o_counts));
+    P.m_pts = reinterpret_cast<v3d_point*>(at(o_mpts));
+    P.m_sites = reinterpret_cast<v3d_grid_site*>(at(o_msites));
+    P.m_patch = reinterpret_cast<uint32_t*>(at(o_mpatch));
+    P.m_local = reinterpret_cast<uint32_t*>(at(o_mlocal));
+    P.m_range = reinterpret_cast<uint32_t*>(at(o_mrange));
+    P.m_tris = reinterpret_cast<v3d_mesh_triangle*>(at(o_mtris));
+    P.m_tpatch = reinterpret_cast<uint32_t*>(at(o_mtpatch));
+    if (with_mesh)
+        mesh_scratch_layout(at(o_mscratch), static_cast<uint32_t>(n_active), cap, total,
+                            total_slots, &P.mesh);
 
     V3D_CK(cudaMemsetAsync(d_status, 0, cap, stream));
     V3D_CK(cudaMemsetAsync(d_ctr, 0, sizeof(RefCounters) * n_active, stream));
@@ -372,9 +412,51 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
 
 }  // namespace
 
+namespace {
+
+// Per-(segment, reference) ranges of the point pool: every segment is ordered
+// by reference.  range[s][k] = first pool index of reference k in segment s,
+// range_end likewise; empty ranges stay [0, 0).
+__global__ void k_pool_ranges(const OutPoint* __restrict__ pool, const uint32_t* __restrict__ seg,
+                              uint32_t n_refs, uint32_t* __restrict__ start,
+                              uint32_t* __restrict__ end) {
+    const uint32_t n = seg[2];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t s = i < seg[0] ? 0 : (i < seg[1] ? 1 : 2);
+        const uint32_t b = s == 0 ? 0 : seg[s - 1], e = seg[s];
+        const uint32_t k = pool[i].ref;
+        if (i == b || pool[i - 1].ref != k) start[s * n_refs + k] = i;
+        if (i + 1 == e || pool[i + 1].ref != k) end[s * n_refs + k] = i + 1;
+    }
+}
+
+// The pool as mesh input: points, sites, patch (= reference) and the index of
+// each point inside its reference's output (primaries, then completions).
+__global__ void k_pool_mesh_input(const OutPoint* __restrict__ pool,
+                                  const uint32_t* __restrict__ seg, uint32_t n_refs,
+                                  const uint32_t* __restrict__ start,
+                                  const uint32_t* __restrict__ end, v3d_point* __restrict__ pts,
+                                  v3d_grid_site* __restrict__ sites, uint32_t* __restrict__ patch,
+                                  uint32_t* __restrict__ local) {
+    const uint32_t n = seg[2];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t s = i < seg[0] ? 0 : (i < seg[1] ? 1 : 2);
+        const OutPoint& q = pool[i];
+        const uint32_t k = q.ref;
+        uint32_t l = i - start[s * n_refs + k];
+        for (uint32_t t = 0; t < s; ++t) l += end[t * n_refs + k] - start[t * n_refs + k];
+        pts[i] = q.p;
+        sites[i] = q.s;
+        patch[i] = k;
+        local[i] = l;
+    }
+}
+
+}  // namespace
+
 int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* frames,
                   size_t n_frames, double focal, const std::vector<RefPlan>& plans,
-                  std::vector<PassResult>& results) {
+                  std::vector<PassResult>& results, std::vector<MeshOut>* mesh) {
     cudaStream_t stream = static_cast<cudaStream_t>(ctx->stream);
     results.assign(plans.size(), PassResult{});
     std::vector<size_t> active;
@@ -392,7 +474,8 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
     };
     const clk::time_point t_upload = clk::now();
     Prepared P;
-    int32_t pst = prepare(ctx, prof, frames, n_frames, focal, plans, active, false, P);
+    int32_t pst = prepare(ctx, prof, frames, n_frames, focal, plans, active, false, P,
+                          mesh != nullptr);
     if (pst != V3D_OK) return pst;
     const size_t n_active = P.n_active;
     const uint64_t total = P.total, cap = P.cap;
@@ -436,7 +519,7 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
     }
 
     // stage events: sweep | primary reciprocal | completion passes
-    cudaEvent_t es[6];
+    cudaEvent_t es[8];
     for (auto& e : es) cudaEventCreate(&e);
     // primary sweep, reciprocal check and fusion
     cudaEventRecord(es[0], stream);
@@ -471,6 +554,56 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
         V3D_CK(launch_occupy(b, d_pool, c_seg + pass, c_seg + pass + 1, cap, d_occ, stream));
     }
     cudaEventRecord(es[5], stream);
+    std::vector<MeshPatchDev> mp;
+    if (mesh) {
+        // patch descriptors need the per-reference point counts: one read of the counters
+        std::vector<RefCounters> c0(n_active);
+        V3D_CK(cudaMemcpyAsync(c0.data(), d_ctr, sizeof(RefCounters) * n_active,
+                               cudaMemcpyDeviceToHost, stream));
+        V3D_CK(cudaStreamSynchronize(stream));
+        mp.resize(n_active);
+        uint64_t slot_off = 0;
+        for (size_t k = 0; k < n_active; ++k) {
+            const RefPlan& pl = plans[active[k]];
+            MeshPatchDev& m = mp[k];
+            std::memset(&m, 0, sizeof(m));
+            set_cam(m.cam, pl.ref_cam);
+            m.focal = focal;
+            m.width = frames[pl.ref_slot].width;
+            m.height = frames[pl.ref_slot].height;
+            m.border = pl.border;
+            m.stride = pl.stride;
+            m.gw = pl.nx;
+            m.gh = pl.ny;
+            m.slot_off = slot_off;
+            m.n_points = c0[k].primary_points + c0[k].completed;
+            slot_off += mesh_slots(pl.nx, pl.ny);
+        }
+        uint64_t go = 0;
+        for (size_t k = 0; k < n_active; ++k) {
+            mp[k].grid_off = go;
+            go += static_cast<uint64_t>(mp[k].gw) * mp[k].gh;
+        }
+        V3D_CK(cudaMemcpyAsync(P.mesh.patches, mp.data(), sizeof(MeshPatchDev) * n_active,
+                               cudaMemcpyHostToDevice, stream));
+        cudaEventRecord(es[6], stream);
+        V3D_CK(cudaMemsetAsync(P.m_range, 0, sizeof(uint32_t) * 6 * n_active, stream));
+        const unsigned gb = static_cast<unsigned>(std::min<uint64_t>((cap + 255) / 256, 148 * 16));
+        k_pool_ranges<<<gb, 256, 0, stream>>>(d_pool, c_seg, static_cast<uint32_t>(n_active),
+                                              P.m_range, P.m_range + 3 * n_active);
+        k_pool_mesh_input<<<gb, 256, 0, stream>>>(d_pool, c_seg, static_cast<uint32_t>(n_active),
+                                                  P.m_range, P.m_range + 3 * n_active, P.m_pts,
+                                                  P.m_sites, P.m_patch, P.m_local);
+        V3D_CK(cudaGetLastError());
+        // the pool's size bounds the loops; every point beyond it is unused
+        uint64_t n_points = 0;
+        for (size_t k = 0; k < n_active; ++k) n_points += mp[k].n_points;
+        V3D_CK(mesh_batch_enqueue(P.mesh, static_cast<uint32_t>(n_active), total, P.total_slots,
+                                  P.m_pts, P.m_sites, P.m_patch, P.m_local, n_points, P.m_tris,
+                                  P.m_tpatch, stream));
+        ctx->last_launches += 2 + 6;
+    }
+    cudaEventRecord(es[7], stream);
     cudaEventRecord(ev1, stream);
 
     // ---- read back ----
@@ -486,6 +619,8 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
     cudaEventElapsedTime(&ctx->last_sweep_ms, es[0], es[1]);
     cudaEventElapsedTime(&ctx->last_recip_ms, es[2], es[3]);
     cudaEventElapsedTime(&ctx->last_completion_ms, es[4], es[5]);
+    ctx->last_mesh_ms = 0.f;
+    if (mesh) cudaEventElapsedTime(&ctx->last_mesh_ms, es[6], es[7]);
     cudaEventDestroy(ev0);
     cudaEventDestroy(ev1);
     for (auto& e : es) cudaEventDestroy(e);
@@ -507,8 +642,74 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
     }
     const OutPoint* pool = static_cast<const OutPoint*>(ctx->pinned);
 
+    std::vector<MeshCounters> mcount;
+    std::vector<v3d_mesh_triangle> tris;
+    std::vector<uint32_t> tri_patch;
+    ctx->last_triangles = 0;
+    if (mesh) {
+        uint32_t n_tris = 0;
+        mcount.resize(n_active);
+        V3D_CK(cudaMemcpyAsync(&n_tris, P.mesh.count, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                               stream));
+        V3D_CK(cudaMemcpyAsync(mcount.data(), P.mesh.counters, sizeof(MeshCounters) * n_active,
+                               cudaMemcpyDeviceToHost, stream));
+        V3D_CK(cudaStreamSynchronize(stream));
+        tris.resize(n_tris);
+        if (n_tris) {
+            V3D_CK(cudaMemcpyAsync(tris.data(), P.m_tris, sizeof(v3d_mesh_triangle) * n_tris,
+                                   cudaMemcpyDeviceToHost, stream));
+            V3D_CK(cudaStreamSynchronize(stream));
+        }
+        ctx->last_triangles = n_tris;
+    }
     ctx->last_wait_ms = ms_since(t_wait);
     const clk::time_point t_assemble = clk::now();
+    if (mesh) {
+        // triangles are in patch order; accepted counts give each patch's range
+        mesh->assign(plans.size(), MeshOut{});
+        size_t t0 = 0;
+        for (size_t k = 0; k < n_active; ++k) {
+            MeshOut& m = (*mesh)[active[k]];
+            const MeshCounters& c = mcount[k];
+            const uint64_t npts = mp[k].n_points;
+            v3d_mesh_stats& s = m.stats;
+            std::memset(&s, 0, sizeof(s));
+            s.has_reference_frame = 1;
+            s.reference_frame = plans[active[k]].reference_frame;
+            auto reason = [&](const char* r) {
+                s.has_skip_reason = 1;
+                std::strncpy(s.skip_reason, r, V3D_SKIP_REASON_BYTES - 1);
+            };
+            if (npts < 3) {
+                reason("fewer than three accepted fused dense points are available");
+                continue;
+            }
+            s.attempted = 1;
+            s.grid_vertices = c.vertices;
+            s.rejected_grid_vertices = npts > c.vertices ? npts - c.vertices : 0;
+            if (c.vertices < 3) {
+                reason("fewer than three fused dense points align with the reference sampling grid");
+                continue;
+            }
+            s.candidate_cells = c.candidate_cells;
+            s.candidate_triangles = c.candidate_triangles;
+            s.accepted_triangles = c.accepted;
+            s.rejected_discontinuities = c.discontinuities;
+            s.rejected_degenerate = c.degenerate;
+            m.tris.assign(tris.begin() + t0, tris.begin() + t0 + c.accepted);
+            t0 += c.accepted;
+        }
+        for (size_t i = 0; i < plans.size(); ++i) {
+            if (!plans[i].skipped) continue;
+            MeshOut& m = (*mesh)[i];
+            std::memset(&m.stats, 0, sizeof(m.stats));
+            m.stats.has_reference_frame = plans[i].have_reference;
+            m.stats.reference_frame = plans[i].reference_frame;
+            m.stats.has_skip_reason = 1;
+            std::strncpy(m.stats.skip_reason, "dense reconstruction was not attempted",
+                         V3D_SKIP_REASON_BYTES - 1);
+        }
+    }
     // ---- assemble per reference ----
     // each pool segment is ordered by reference: find every reference's range
     const uint32_t seg_begin[3] = {0, segs[0], segs[1]}, seg_end[3] = {segs[0], segs[1], segs[2]};

@@ -185,7 +185,8 @@ class RunInfo(C.Structure):
                 ("completion_ms", C.c_double), ("reciprocal_plane_evaluations", C.c_uint64),
                 ("candidates", C.c_uint64), ("host_plan_ms", C.c_double),
                 ("host_upload_ms", C.c_double), ("host_wait_ms", C.c_double),
-                ("host_assemble_ms", C.c_double)]
+                ("host_assemble_ms", C.c_double), ("mesh_ms", C.c_double),
+                ("triangles", C.c_uint64)]
 
 
 CANCEL_FN = C.CFUNCTYPE(C.c_int32, C.c_void_p)

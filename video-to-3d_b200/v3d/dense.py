@@ -77,6 +77,10 @@ def library():
     L.v3d_debug_sweep.argtypes = [C.c_void_p] + frames_args + [
         C.c_int32, _P(abi.Profile), _P(abi.SiteRecord), C.c_uint64, _P(C.c_uint64)]
     L.v3d_debug_sweep.restype = C.c_int32
+    L.v3d_reconstruct_reference_patches_meshed.argtypes = [C.c_void_p] + frames_args + [
+        C.c_int32, _P(abi.Profile), _P(C.c_uint64), C.c_uint64, abi.CANCEL_FN, C.c_void_p,
+        _P(abi.DenseResult), _P(abi.MeshResult), _P(C.c_int32)]
+    L.v3d_reconstruct_reference_patches_meshed.restype = C.c_int32
     L.v3d_last_run_info.argtypes = [C.c_void_p, _P(abi.RunInfo)]
     L.v3d_last_run_info.restype = C.c_int32
     _lib = L
@@ -141,6 +145,31 @@ class Context:
         for i in range(n):
             res.append(types.dense_from_result(outs[i]) if present[i] else None)
             self.lib.v3d_dense_result_free(C.byref(outs[i]))
+        return res
+
+    def reconstruct_reference_patches_meshed(self, frames, cameras, sparse_points, focal,
+                                             camera_indices, profile=None, fine_grid=False,
+                                             control=None):
+        """Per-reference passes plus each patch's grid-mesh triangles, in one device batch.
+        Returns a list of (DenseAnalysis, MeshAnalysis) or None per camera index."""
+        prof = profile if profile is not None else profiles.reference()
+        inp = types.Inputs(frames, cameras, sparse_points)
+        fn, _keep = types.cancel_callback(control)
+        n = len(camera_indices)
+        idx = (C.c_uint64 * max(n, 1))(*camera_indices)
+        outs = (abi.DenseResult * max(n, 1))()
+        meshes = (abi.MeshResult * max(n, 1))()
+        present = (C.c_int32 * max(n, 1))()
+        self._check(self.lib.v3d_reconstruct_reference_patches_meshed(
+            self.handle, inp.frames, inp.n_frames, inp.cameras, inp.n_cameras, inp.sparse,
+            inp.n_sparse, float(focal), int(fine_grid), C.byref(prof), idx, n, fn, None, outs,
+            meshes, present))
+        res = []
+        for i in range(n):
+            res.append((types.dense_from_result(outs[i]), types.mesh_from_result(meshes[i]))
+                       if present[i] else None)
+            self.lib.v3d_dense_result_free(C.byref(outs[i]))
+            self.lib.v3d_mesh_result_free(C.byref(meshes[i]))
         return res
 
     def estimate_depth_points_limited(self, frames, cameras, sparse_points, focal,
