@@ -471,6 +471,57 @@ int32_t v3d_reconstruct_dense_mesh_with_control(
 
 void v3d_mesh_result_free(v3d_mesh_result* result);
 
+/* ---- allocation-free variant ---------------------------------------------- */
+
+/* Outcome counters of v3d_mesh_patch_device_noalloc, written to device memory. */
+typedef struct v3d_mesh_counts {
+    uint64_t grid_vertices;
+    uint64_t candidate_cells;
+    uint64_t candidate_triangles;
+    uint64_t accepted_triangles;
+    uint64_t rejected_discontinuities;
+    uint64_t rejected_degenerate;
+} v3d_mesh_counts;
+
+#define V3D_NOALLOC_SCRATCH_BYTES (32u << 20)
+
+/* Reference-grid triangle gates of one patch whose points already live in
+ * device memory, for callers that may not allocate GPU memory: a host that
+ * hands the library pointers into its own pre-allocated pool, a serving loop
+ * that must not call cudaMalloc (which can synchronise the device), or a
+ * plug-in running under an allocator it does not own.  No counterpart in the
+ * reference; it computes what v3d_reconstruct_dense_mesh_with_control does for
+ * a single patch (mesh_legacy.rs:200-358), triangle for triangle.
+ *
+ * Allocates nothing: no cudaMalloc, cudaFree or allocating library call.  All
+ * working memory comes from one file-scope device array of
+ * V3D_NOALLOC_SCRATCH_BYTES (32 MiB) that every GPU loading the library keeps
+ * until exit; a patch whose lattice, points and candidate slots need more is
+ * rejected with V3D_ERR_INVALID_ARGUMENT before anything is enqueued (about
+ * 1280x720 at grid stride 2 fits).  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress) with that device current, so
+ * make it before any stream capture.  Every call shares the array and leaves
+ * the last call's contents there; the call clears what must start at zero.
+ * Calls that overlap on the GPU (other streams, other host threads) race on
+ * the array: order them on one stream.
+ *
+ * Inputs: points_dev / sites_dev (device, n_points each), the reference camera
+ * and geometry on the host.  Outputs (device): triangles_dev receives the
+ * accepted triangles with indices into points_dev, *counts_dev the counters
+ * (accepted_triangles = number written).  triangles_dev must hold
+ * 2*(gw+1)*(gh+1) + (gw-2)*gh + gw*(gh-2) triangles, the number of candidate
+ * slots, where gw and gh are the grid columns and rows
+ * ceil((width - 2*border) / stride) and ceil((height - 2*border) / stride).
+ * Work is enqueued on `stream` (a cudaStream_t, NULL for the legacy stream);
+ * results are valid once the stream has reached them.  Fewer than 3 points
+ * yield no triangles (the reference skips such a patch before the grid). */
+int32_t v3d_mesh_patch_device_noalloc(
+    const v3d_point* points_dev, const v3d_grid_site* sites_dev, uint64_t n_points,
+    const v3d_camera* reference_camera,
+    uint32_t width, uint32_t height, uint32_t grid_border, uint64_t grid_stride, double focal,
+    v3d_mesh_triangle* triangles_dev, uint64_t triangle_capacity,
+    v3d_mesh_counts* counts_dev, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -178,6 +178,12 @@ class SiteRecord(C.Structure):
 SITE_RECORD_DTYPE = [("x", "<u4"), ("y", "<u4"), ("status", "<i4"), ("plane", "<i4"),
                      ("support", "<i4"), ("pad", "<i4"), ("error", "<f8"), ("margin", "<f8")]
 
+class MeshCounts(C.Structure):
+    _fields_ = [("grid_vertices", C.c_uint64), ("candidate_cells", C.c_uint64),
+                ("candidate_triangles", C.c_uint64), ("accepted_triangles", C.c_uint64),
+                ("rejected_discontinuities", C.c_uint64), ("rejected_degenerate", C.c_uint64)]
+
+
 class RunInfo(C.Structure):
     _fields_ = [("device_ms", C.c_double), ("kernel_launches", C.c_uint64),
                 ("grid_sites", C.c_uint64), ("plane_view_units", C.c_uint64),
@@ -198,5 +204,5 @@ STRUCTS = {
     "v3d_reference_patch": ReferencePatch, "v3d_dense_result": DenseResult,
     "v3d_mesh_triangle": MeshTriangle, "v3d_mesh_stats": MeshStats,
     "v3d_mesh_result": MeshResult, "v3d_mesh_dense_input": MeshDenseInput,
-    "v3d_site_record": SiteRecord, "v3d_run_info": RunInfo,
+    "v3d_site_record": SiteRecord, "v3d_run_info": RunInfo, "v3d_mesh_counts": MeshCounts,
 }
