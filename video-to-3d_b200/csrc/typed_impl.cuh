@@ -308,8 +308,11 @@ __global__ void __launch_bounds__(256) k_sweep_tiled(BatchDev b, uint64_t total_
         else atomicAdd(&ctr[r].sampled, 1ull);
     }
     const double n = (double)N;
+    const double inv_n = 1.0 / n;
     const double vr = srr - sr * sr / n;
     const double minvar_n = prof.min_variance * n;
+    const bool vr_ok = vr > 0.0 && vr >= minvar_n;
+    const float vr_f = (float)vr;
     Rank st = rank_empty();
     for (int k = 0; k < prof.planes; ++k) {
         const float inv = pinv[k];
@@ -322,19 +325,25 @@ __global__ void __launch_bounds__(256) k_sweep_tiled(BatchDev b, uint64_t total_
             const DevImage si = ref.src[j].img;
             const T* sdata = static_cast<const T*>(si.data);
             const float wl = (float)(si.width - 1), hl = (float)(si.height - 1);
-            for (int i = tid; i < npx; i += 256) {
-                int yy = i / PX, xx = i - yy * PX;
-                float X = (float)(px0 + xx), Y = (float)(py0 + yy);
-                float h2 = fmaf(A[6], X, fmaf(A[7], Y, H8));
-                float v = __int_as_float(0x7fc00000);
-                if (h2 > zmin) {
-                    float iv = __frcp_rn(h2);
-                    float u = fmaf(A[0], X, fmaf(A[1], Y, H2)) * iv;
-                    float q = fmaf(A[3], X, fmaf(A[4], Y, H5)) * iv;
-                    if (u >= 0.f && q >= 0.f && u < wl && q < hl)
-                        v = sample_fast<T>(sdata, si.width, u, q);
+            // warp rows, lanes columns: no index division, the homography
+            // folded per row, the reciprocal from the approximate unit
+            for (int yy = ty; yy < PY; yy += kTileY) {
+                const float Y = (float)(py0 + yy);
+                const float hx = fmaf(A[1], Y, H2), hy = fmaf(A[4], Y, H5), hz = fmaf(A[7], Y, H8);
+                float* row = samp + yy * PX;
+                for (int xx = tx; xx < PX; xx += kTileX) {
+                    const float X = (float)(px0 + xx);
+                    const float h2 = fmaf(A[6], X, hz);
+                    float v = __int_as_float(0x7fc00000);
+                    if (h2 > zmin) {
+                        const float iv = __fdividef(1.0f, h2);
+                        const float u = fmaf(A[0], X, hx) * iv;
+                        const float q = fmaf(A[3], X, hy) * iv;
+                        if (u >= 0.f && q >= 0.f && u < wl && q < hl)
+                            v = sample_fast<T>(sdata, si.width, u, q);
+                    }
+                    row[xx] = v;
                 }
-                samp[i] = v;
             }
             __syncthreads();
             for (int i = tid; i < PY * kTileX; i += 256) {
@@ -363,11 +372,12 @@ __global__ void __launch_bounds__(256) k_sweep_tiled(BatchDev b, uint64_t total_
                     bb += hss[i];
                     c += hrs[i];
                 }
-                double vs = bb - a * a / n;
-                double cov = c - sr * a / n;
+                // the cancelling differences in f64, the ratio in f32
+                const double vs = bb - a * a * inv_n;
+                const double cov = c - sr * a * inv_n;
                 float cost = __int_as_float(0x7fc00000);
-                if (vs > 0.0 && vr > 0.0 && vs >= minvar_n && vr >= minvar_n)
-                    cost = (float)(1.0 - cov / sqrt(vr * vs));
+                if (vs > 0.0 && vs >= minvar_n && vr_ok)
+                    cost = 1.0f - (float)cov * rsqrtf(vr_f * (float)vs);
                 costs[j * 256 + tid] = cost;  // NaN when invalid
             }
         }
