@@ -20,9 +20,18 @@ using namespace v3d;
 
 namespace {
 
+// What a C result holds besides its malloc'd arrays: the source-frame lists
+// of its patches and, when its points live in a batch's pinned block, a
+// reference to that block (the point arrays are then not freed one by one).
 struct ResultOwner {
     std::vector<std::vector<uint64_t>> patch_sources;
+    HostBlock block;
 };
+
+ResultOwner* owner_of(v3d_dense_result* out) {
+    if (!out->internal) out->internal = new ResultOwner;
+    return static_cast<ResultOwner*>(out->internal);
+}
 
 template <class T>
 T* dup(const std::vector<T>& v) {
@@ -83,9 +92,12 @@ void fill_pass(v3d_dense_result* out, const PassResult& r) {
         out->stats.source_views = sf.size();
     }
     out->n_points = r.points.size();
-    out->points = dup(r.points);
-    out->grid_sites = dup(r.sites);
-    out->point_attributes = dup(r.attrs);
+    if (!r.points.empty()) {
+        out->points = r.points.begin();
+        out->grid_sites = r.sites.begin();
+        out->point_attributes = r.attrs.begin();
+        owner_of(out)->block = r.block;
+    }
 }
 
 int32_t status_of(const PassResult& r) { return r.stats.attempted ? V3D_OK : V3D_SKIPPED; }
@@ -177,14 +189,13 @@ void fill_from_legacy(v3d_dense_result* out, const PassResult& r) {
     out->n_attempts = 1;
     out->attempts = dup(at);
     if (s.attempted) {
-        auto* owner = new ResultOwner;
+        ResultOwner* owner = owner_of(out);
         owner->patch_sources.emplace_back(r.plan.source_frames.begin(), r.plan.source_frames.end());
         std::vector<v3d_reference_patch> ps{patch_of(r, 0, primary, primary, completion)};
         ps[0].n_source_frames = owner->patch_sources[0].size();
         ps[0].source_frames = owner->patch_sources[0].data();
         out->n_patches = 1;
         out->patches = dup(ps);
-        out->internal = owner;
     }
 }
 
@@ -324,14 +335,17 @@ uint64_t v3d_grid_stride(uint32_t width, uint32_t height, int32_t fine_grid) {
 
 void v3d_dense_result_free(v3d_dense_result* r) {
     if (!r) return;
+    auto* owner = static_cast<ResultOwner*>(r->internal);
     std::free(r->source_frames);
-    std::free(r->points);
-    std::free(r->grid_sites);
-    std::free(r->point_attributes);
+    if (!owner || !owner->block) {
+        std::free(r->points);
+        std::free(r->grid_sites);
+        std::free(r->point_attributes);
+    }
     std::free(r->reference_frames);
     std::free(r->attempts);
     std::free(r->patches);
-    delete static_cast<ResultOwner*>(r->internal);
+    delete owner;
     std::memset(r, 0, sizeof(*r));
 }
 
@@ -378,7 +392,11 @@ void fill_mesh(v3d_mesh_result* out, const MeshOut& m) {
     std::memset(out, 0, sizeof(*out));
     out->stats = m.stats;
     out->n_triangles = m.tris.size();
-    out->triangles = dup(m.tris);
+    if (!m.tris.empty()) {
+        // the triangles stay in the batch's pinned block; `internal` holds it
+        out->triangles = m.tris.begin();
+        out->internal = new HostBlock(m.block);
+    }
     if (m.stats.has_reference_frame) {
         std::vector<uint64_t> rf{m.stats.reference_frame};
         out->n_reference_frames = 1;
@@ -468,7 +486,8 @@ int32_t reference_patches(v3d_context* ctx, const v3d_frame* frames, uint64_t n_
             if (canceled[i] || !res[i].stats.attempted) {
                 v3d_mesh_stats& s = meshes[i].stats;
                 std::memset(&s, 0, sizeof(s));
-                meshes[i].tris.clear();
+                meshes[i].tris = {};
+                meshes[i].block.reset();
                 s.has_reference_frame = 1;
                 s.reference_frame = res[i].stats.reference_frame;
                 s.has_skip_reason = 1;
@@ -740,7 +759,7 @@ int32_t v3d_estimate_depth_points_limited(v3d_context* ctx, const v3d_frame* fra
     out->grid_sites = dup(sites);
     out->point_attributes = dup(attrs);
     std::vector<uint64_t> rfs;
-    auto* owner = new ResultOwner;
+    ResultOwner* owner = owner_of(out);
     std::vector<v3d_reference_patch> ps;
     for (size_t i = 0; i < patches.size(); ++i) {
         const Patch& p = patches[i];
@@ -758,7 +777,6 @@ int32_t v3d_estimate_depth_points_limited(v3d_context* ctx, const v3d_frame* fra
     out->attempts = dup(attempts);
     out->n_patches = ps.size();
     out->patches = dup(ps);
-    out->internal = owner;
     *omitted_references = omitted ? 1 : 0;
     return V3D_OK;
 }

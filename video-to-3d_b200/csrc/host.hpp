@@ -4,6 +4,7 @@
 #include <cstddef>
 #include <cstdint>
 #include <functional>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -39,18 +40,37 @@ struct RefPlan {
     uint32_t width = 0, height = 0, stride = 0, border = 0, nx = 0, ny = 0;
 };
 
+// Page-locked host memory shared by the results of one batch
+// (host_block.cpp); the deleter returns it to a process-wide cache.
+using HostBlock = std::shared_ptr<uint8_t>;
+HostBlock host_block(size_t bytes);  // empty on allocation failure
+
+// A view of `size()` elements inside a HostBlock.
+template <class T>
+struct Span {
+    T* ptr = nullptr;
+    size_t len = 0;
+    size_t size() const { return len; }
+    bool empty() const { return len == 0; }
+    T* begin() const { return ptr; }
+    T* end() const { return ptr + len; }
+    T& operator[](size_t i) const { return ptr[i]; }
+};
+
 // One patch's reference-grid triangles (mesh_legacy.rs:40-43).
 struct MeshOut {
     v3d_mesh_stats stats{};
-    std::vector<v3d_mesh_triangle> tris;
+    Span<v3d_mesh_triangle> tris;
+    HostBlock block;  // holds `tris`
 };
 
 // One pass's output (dense_legacy.rs:62-68 DenseAnalysis with DenseStats).
 struct PassResult {
     RefPlan plan;
-    std::vector<v3d_point> points;
-    std::vector<v3d_grid_site> sites;
-    std::vector<v3d_point_attributes> attrs;
+    Span<v3d_point> points;
+    Span<v3d_grid_site> sites;
+    Span<v3d_point_attributes> attrs;
+    HostBlock block;  // holds the three arrays
     v3d_dense_stats stats{};
 };
 

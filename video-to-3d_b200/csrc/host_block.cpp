@@ -1,0 +1,78 @@
+// Pinned host blocks that result arrays live in.
+//
+// A batch's points, grid sites, attributes and triangles are copied from the
+// device straight into one page-locked block, and every per-reference result
+// of the batch points into it.  The block is reference counted (one count per
+// PassResult copy, per C result and per mesh result); when the last holder
+// lets go it returns to a small process-wide cache instead of being unpinned,
+// so a caller that drops the previous call's results before the next call
+// reuses the same two blocks without page faults or cudaHostAlloc.
+#include <cuda_runtime.h>
+
+#include <map>
+#include <mutex>
+
+#include "host.hpp"
+
+namespace v3d {
+namespace {
+
+constexpr size_t kBlockAlign = size_t{2} << 20;  // sizes rounded to 2 MiB
+constexpr size_t kCachedBlocks = 4;               // blocks kept for reuse
+
+struct BlockCache {
+    std::mutex mu;
+    std::multimap<size_t, void*> free;  // bytes -> block
+};
+
+// Never destroyed: holders may release blocks during static destruction.
+BlockCache& cache() {
+    static BlockCache* c = new BlockCache;
+    return *c;
+}
+
+void recycle(void* p, size_t bytes) {
+    BlockCache& c = cache();
+    void* drop = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(c.mu);
+        c.free.emplace(bytes, p);
+        if (c.free.size() > kCachedBlocks) {
+            // keep the largest blocks; unpin the smallest
+            auto it = c.free.begin();
+            drop = it->second;
+            c.free.erase(it);
+        }
+    }
+    if (drop) cudaFreeHost(drop);
+}
+
+}  // namespace
+
+HostBlock host_block(size_t bytes) {
+    bytes = (bytes + kBlockAlign - 1) / kBlockAlign * kBlockAlign;
+    if (bytes == 0) bytes = kBlockAlign;
+    BlockCache& c = cache();
+    void* p = nullptr;
+    size_t have = 0;
+    {
+        std::lock_guard<std::mutex> lock(c.mu);
+        // the smallest cached block that fits, unless it wastes more than 4x
+        auto it = c.free.lower_bound(bytes);
+        if (it != c.free.end() && it->first <= 4 * bytes) {
+            p = it->second;
+            have = it->first;
+            c.free.erase(it);
+        }
+    }
+    if (!p) {
+        if (cudaHostAlloc(&p, bytes, cudaHostAllocPortable) != cudaSuccess) {
+            cudaGetLastError();
+            return HostBlock();
+        }
+        have = bytes;
+    }
+    return HostBlock(static_cast<uint8_t*>(p), [have](uint8_t* q) { recycle(q, have); });
+}
+
+}  // namespace v3d

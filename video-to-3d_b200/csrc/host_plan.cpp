@@ -381,9 +381,10 @@ void skip_result(PassResult& r, int code, const std::string& reason) {
     r.stats.skip_code = code;
     r.stats.has_skip_reason = 1;
     std::strncpy(r.stats.skip_reason, reason.c_str(), V3D_SKIP_REASON_BYTES - 1);
-    r.points.clear();
-    r.sites.clear();
-    r.attrs.clear();
+    r.points = {};
+    r.sites = {};
+    r.attrs = {};
+    r.block.reset();
 }
 
 }  // namespace v3d

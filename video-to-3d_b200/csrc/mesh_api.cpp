@@ -97,7 +97,11 @@ extern "C" {
 
 void v3d_mesh_result_free(v3d_mesh_result* r) {
     if (!r) return;
-    std::free(r->triangles);
+    // a batch's triangles live in its pinned block, which `internal` holds
+    if (r->internal)
+        delete static_cast<v3d::HostBlock*>(r->internal);
+    else
+        std::free(r->triangles);
     std::free(r->reference_frames);
     std::free(r->patches);
     std::memset(r, 0, sizeof(*r));

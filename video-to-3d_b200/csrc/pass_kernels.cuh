@@ -58,6 +58,19 @@ struct OutPoint {
     double observations;
 };
 
+// What the per-reference medians (dense_legacy.rs:459-462) read of one output
+// point.  The photometric error is narrowed to f32 per point: the reference
+// takes the median in f64 and narrows the result, and narrowing is monotone,
+// so the order statistic is the same.  Support and fusion observations are
+// small counts; only primary points enter the observation median.
+struct MedianKey {
+    float error;
+    uint8_t support;
+    uint8_t observations;
+    uint8_t primary;
+    uint8_t pad;
+};
+
 // Per-reference counters, accumulated with integer atomics.
 struct RefCounters {
     unsigned long long sampled, checked, recip_rejected, consistent, fusion_input,

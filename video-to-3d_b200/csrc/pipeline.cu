@@ -12,6 +12,8 @@
 //               each segment in (reference, raster) order
 #include <cuda_runtime.h>
 
+#include <cub/block/block_scan.cuh>
+
 #include <algorithm>
 #include <chrono>
 #include <cstring>
@@ -112,12 +114,6 @@ struct Seg {
     uint32_t begin, end;
 };
 
-double median_of(std::vector<double>& v) {
-    size_t k = v.size() / 2;  // round((n - 1) * 0.5)
-    std::nth_element(v.begin(), v.begin() + k, v.end());
-    return v[k];
-}
-
 }  // namespace
 
 #define V3D_CK(call)                                              \
@@ -155,13 +151,17 @@ struct Prepared {
     uint8_t* d_pstat = nullptr;
     Cand* d_prop = nullptr;
     uint32_t* d_counts = nullptr;
+    // output: the pool in per-reference order (primaries, then completions)
+    v3d_point* o_pts = nullptr;
+    v3d_grid_site* o_sites = nullptr;
+    v3d_point_attributes* o_attrs = nullptr;
+    MedianKey* o_med = nullptr;
+    uint32_t* o_patch = nullptr;  // reference of each output point (mesh input)
+    uint32_t* o_local = nullptr;  // index inside its reference (mesh input)
+    uint32_t* o_base = nullptr;   // [n_active + 1] first output index per reference
+    uint32_t* m_range = nullptr;  // [2][3][n_active] per-(segment, reference) pool ranges
     // mesh stage
     uint64_t total_slots = 0;
-    v3d_point* m_pts = nullptr;
-    v3d_grid_site* m_sites = nullptr;
-    uint32_t* m_patch = nullptr;
-    uint32_t* m_local = nullptr;
-    uint32_t* m_range = nullptr;
     v3d_mesh_triangle* m_tris = nullptr;
     uint32_t* m_tpatch = nullptr;
     MeshScratch mesh{};
@@ -258,10 +258,13 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
         total_slots += mesh_slots(plans[active[k]].nx, plans[active[k]].ny);
     P.total_slots = with_mesh ? total_slots : 0;
     const uint64_t mc = with_mesh ? cap : 1;
-    const size_t o_mpts = cv.take<v3d_point>(mc);
-    const size_t o_msites = cv.take<v3d_grid_site>(mc);
-    const size_t o_mpatch = cv.take<uint32_t>(mc);
-    const size_t o_mlocal = cv.take<uint32_t>(mc);
+    const size_t o_opts = cv.take<v3d_point>(pc);
+    const size_t o_osites = cv.take<v3d_grid_site>(pc);
+    const size_t o_oattrs = cv.take<v3d_point_attributes>(pc);
+    const size_t o_omed = cv.take<MedianKey>(pc);
+    const size_t o_opatch = cv.take<uint32_t>(mc);
+    const size_t o_olocal = cv.take<uint32_t>(mc);
+    const size_t o_obase = cv.take<uint32_t>(n_active + 1);
     const size_t o_mrange = cv.take<uint32_t>(6 * n_active);
     const size_t mesh_bytes =
         with_mesh ? mesh_scratch_layout(nullptr, static_cast<uint32_t>(n_active), cap, total,
@@ -364,10 +367,13 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
     P.d_pstat = reinterpret_cast<uint8_t*>(at(o_pstat));
     P.d_prop = reinterpret_cast<Cand*>(at(o_prop));
     auto* d_counts = P.d_counts = reinterpret_cast<uint32_t*>(at(o_counts));
-    P.m_pts = reinterpret_cast<v3d_point*>(at(o_mpts));
-    P.m_sites = reinterpret_cast<v3d_grid_site*>(at(o_msites));
-    P.m_patch = reinterpret_cast<uint32_t*>(at(o_mpatch));
-    P.m_local = reinterpret_cast<uint32_t*>(at(o_mlocal));
+    P.o_pts = reinterpret_cast<v3d_point*>(at(o_opts));
+    P.o_sites = reinterpret_cast<v3d_grid_site*>(at(o_osites));
+    P.o_attrs = reinterpret_cast<v3d_point_attributes*>(at(o_oattrs));
+    P.o_med = reinterpret_cast<MedianKey*>(at(o_omed));
+    P.o_patch = with_mesh ? reinterpret_cast<uint32_t*>(at(o_opatch)) : nullptr;
+    P.o_local = with_mesh ? reinterpret_cast<uint32_t*>(at(o_olocal)) : nullptr;
+    P.o_base = reinterpret_cast<uint32_t*>(at(o_obase));
     P.m_range = reinterpret_cast<uint32_t*>(at(o_mrange));
     P.m_tris = reinterpret_cast<v3d_mesh_triangle*>(at(o_mtris));
     P.m_tpatch = reinterpret_cast<uint32_t*>(at(o_mtpatch));
@@ -430,14 +436,40 @@ __global__ void k_pool_ranges(const OutPoint* __restrict__ pool, const uint32_t*
     }
 }
 
-// The pool as mesh input: points, sites, patch (= reference) and the index of
-// each point inside its reference's output (primaries, then completions).
-__global__ void k_pool_mesh_input(const OutPoint* __restrict__ pool,
-                                  const uint32_t* __restrict__ seg, uint32_t n_refs,
-                                  const uint32_t* __restrict__ start,
-                                  const uint32_t* __restrict__ end, v3d_point* __restrict__ pts,
-                                  v3d_grid_site* __restrict__ sites, uint32_t* __restrict__ patch,
-                                  uint32_t* __restrict__ local) {
+// Exclusive prefix of the references' output sizes (their three segment
+// ranges): base[k] is reference k's first output index, base[n_refs] the total.
+__global__ void __launch_bounds__(1024) k_ref_bases(const uint32_t* __restrict__ start,
+                                                    const uint32_t* __restrict__ end,
+                                                    uint32_t n_refs, uint32_t* __restrict__ base) {
+    using Scan = cub::BlockScan<uint32_t, 1024>;
+    __shared__ typename Scan::TempStorage tmp;
+    uint32_t carry = 0;
+    for (uint32_t k0 = 0; k0 < n_refs; k0 += 1024) {
+        const uint32_t k = k0 + threadIdx.x;
+        uint32_t c = 0;
+        if (k < n_refs)
+            for (int s = 0; s < 3; ++s) c += end[s * n_refs + k] - start[s * n_refs + k];
+        uint32_t x, agg;
+        Scan(tmp).ExclusiveSum(c, x, agg);
+        if (k < n_refs) base[k] = carry + x;
+        carry += agg;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) base[n_refs] = carry;
+}
+
+// The pool in output order: reference by reference, each reference's
+// primaries then its completions of pass 1 and pass 2 (the order in which
+// dense_legacy.rs:397-412 and 727-733 push them), as the arrays the caller receives,
+// the median keys and, for the mesh stage, each point's reference and index
+// inside it.
+__global__ void k_pool_output(const OutPoint* __restrict__ pool, const uint32_t* __restrict__ seg,
+                              uint32_t n_refs, const uint32_t* __restrict__ start,
+                              const uint32_t* __restrict__ end, const uint32_t* __restrict__ base,
+                              v3d_point* __restrict__ pts, v3d_grid_site* __restrict__ sites,
+                              v3d_point_attributes* __restrict__ attrs,
+                              MedianKey* __restrict__ med, uint32_t* __restrict__ patch,
+                              uint32_t* __restrict__ local) {
     const uint32_t n = seg[2];
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint32_t s = i < seg[0] ? 0 : (i < seg[1] ? 1 : 2);
@@ -445,10 +477,21 @@ __global__ void k_pool_mesh_input(const OutPoint* __restrict__ pool,
         const uint32_t k = q.ref;
         uint32_t l = i - start[s * n_refs + k];
         for (uint32_t t = 0; t < s; ++t) l += end[t * n_refs + k] - start[t * n_refs + k];
-        pts[i] = q.p;
-        sites[i] = q.s;
-        patch[i] = k;
-        local[i] = l;
+        const uint32_t o = base[k] + l;
+        pts[o] = q.p;
+        sites[o] = q.s;
+        attrs[o] = q.a;
+        MedianKey m;
+        m.error = (float)q.error;
+        m.support = (uint8_t)fmin(fmax(q.support, 0.0), 255.0);
+        m.observations = (uint8_t)fmin(fmax(q.observations, 0.0), 255.0);
+        m.primary = s == 0;
+        m.pad = 0;
+        med[o] = m;
+        if (patch) {
+            patch[o] = k;
+            local[o] = l;
+        }
     }
 }
 
@@ -554,6 +597,21 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
         V3D_CK(launch_occupy(b, d_pool, c_seg + pass, c_seg + pass + 1, cap, d_occ, stream));
     }
     cudaEventRecord(es[5], stream);
+    // the pool in output order
+    {
+        const unsigned gb = static_cast<unsigned>(std::min<uint64_t>((cap + 255) / 256, 148 * 16));
+        V3D_CK(cudaMemsetAsync(P.m_range, 0, sizeof(uint32_t) * 6 * n_active, stream));
+        k_pool_ranges<<<gb, 256, 0, stream>>>(d_pool, c_seg, static_cast<uint32_t>(n_active),
+                                              P.m_range, P.m_range + 3 * n_active);
+        k_ref_bases<<<1, 1024, 0, stream>>>(P.m_range, P.m_range + 3 * n_active,
+                                           static_cast<uint32_t>(n_active), P.o_base);
+        k_pool_output<<<gb, 256, 0, stream>>>(d_pool, c_seg, static_cast<uint32_t>(n_active),
+                                              P.m_range, P.m_range + 3 * n_active, P.o_base,
+                                              P.o_pts, P.o_sites, P.o_attrs, P.o_med, P.o_patch,
+                                              P.o_local);
+        V3D_CK(cudaGetLastError());
+        ctx->last_launches += 3;
+    }
     std::vector<MeshPatchDev> mp;
     if (mesh) {
         // patch descriptors need the per-reference point counts: one read of the counters
@@ -587,21 +645,13 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
         V3D_CK(cudaMemcpyAsync(P.mesh.patches, mp.data(), sizeof(MeshPatchDev) * n_active,
                                cudaMemcpyHostToDevice, stream));
         cudaEventRecord(es[6], stream);
-        V3D_CK(cudaMemsetAsync(P.m_range, 0, sizeof(uint32_t) * 6 * n_active, stream));
-        const unsigned gb = static_cast<unsigned>(std::min<uint64_t>((cap + 255) / 256, 148 * 16));
-        k_pool_ranges<<<gb, 256, 0, stream>>>(d_pool, c_seg, static_cast<uint32_t>(n_active),
-                                              P.m_range, P.m_range + 3 * n_active);
-        k_pool_mesh_input<<<gb, 256, 0, stream>>>(d_pool, c_seg, static_cast<uint32_t>(n_active),
-                                                  P.m_range, P.m_range + 3 * n_active, P.m_pts,
-                                                  P.m_sites, P.m_patch, P.m_local);
-        V3D_CK(cudaGetLastError());
-        // the pool's size bounds the loops; every point beyond it is unused
+        // the output arrays bound the loops; every point beyond their size is unused
         uint64_t n_points = 0;
         for (size_t k = 0; k < n_active; ++k) n_points += mp[k].n_points;
         V3D_CK(mesh_batch_enqueue(P.mesh, static_cast<uint32_t>(n_active), total, P.total_slots,
-                                  P.m_pts, P.m_sites, P.m_patch, P.m_local, n_points, P.m_tris,
+                                  P.o_pts, P.o_sites, P.o_patch, P.o_local, n_points, P.m_tris,
                                   P.m_tpatch, stream));
-        ctx->last_launches += 2 + 6;
+        ctx->last_launches += 6;
     }
     cudaEventRecord(es[7], stream);
     cudaEventRecord(ev1, stream);
@@ -610,10 +660,19 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
     ctx->last_upload_ms = ms_since(t_upload);
     const clk::time_point t_wait = clk::now();
     std::vector<RefCounters> ctr(n_active);
-    uint32_t segs[3];
+    std::vector<uint32_t> base(n_active + 1);
+    std::vector<MeshCounters> mcount(mesh ? n_active : 0);
+    uint32_t n_tris = 0;
     V3D_CK(cudaMemcpyAsync(ctr.data(), d_ctr, sizeof(RefCounters) * n_active,
                            cudaMemcpyDeviceToHost, stream));
-    V3D_CK(cudaMemcpyAsync(segs, c_seg, sizeof(segs), cudaMemcpyDeviceToHost, stream));
+    V3D_CK(cudaMemcpyAsync(base.data(), P.o_base, sizeof(uint32_t) * (n_active + 1),
+                           cudaMemcpyDeviceToHost, stream));
+    if (mesh) {
+        V3D_CK(cudaMemcpyAsync(&n_tris, P.mesh.count, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                               stream));
+        V3D_CK(cudaMemcpyAsync(mcount.data(), P.mesh.counters, sizeof(MeshCounters) * n_active,
+                               cudaMemcpyDeviceToHost, stream));
+    }
     V3D_CK(cudaStreamSynchronize(stream));
     cudaEventElapsedTime(&ctx->last_ms, ev0, ev1);
     cudaEventElapsedTime(&ctx->last_sweep_ms, es[0], es[1]);
@@ -630,40 +689,54 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
         ctx->last_recip_evals += c.recip_evals;
         ctx->last_candidates += c.candidates;
     }
-    const size_t n_pool = segs[2];
-    if (n_pool) {
-        if (!grow(&ctx->pinned, &ctx->pinned_bytes, n_pool * sizeof(OutPoint), true)) {
-            ctx->last_error = "pinned staging allocation failed";
+    ctx->last_triangles = n_tris;
+    const size_t n_out = base[n_active];
+    if (mesh) {
+        uint64_t acc = 0;
+        for (const MeshCounters& c : mcount) acc += c.accepted;
+        if (acc != n_tris) {
+            ctx->last_error = "mesh triangle counts disagree";
+            return V3D_ERR_INTERNAL;
+        }
+    }
+    // one pinned block receives every array of the batch; the results point into it
+    Carver hl;
+    const size_t h_pts = hl.take<v3d_point>(n_out);
+    const size_t h_sites = hl.take<v3d_grid_site>(n_out);
+    const size_t h_attrs = hl.take<v3d_point_attributes>(n_out);
+    const size_t h_med = hl.take<MedianKey>(n_out);
+    const size_t h_tris = hl.take<v3d_mesh_triangle>(n_tris);
+    HostBlock block;
+    if (n_out || n_tris) {
+        block = host_block(hl.off);
+        if (!block) {
+            ctx->last_error = "pinned result block allocation failed";
             return V3D_ERR_OUT_OF_MEMORY;
         }
-        V3D_CK(cudaMemcpyAsync(ctx->pinned, d_pool, n_pool * sizeof(OutPoint),
-                               cudaMemcpyDeviceToHost, stream));
-        V3D_CK(cudaStreamSynchronize(stream));
-    }
-    const OutPoint* pool = static_cast<const OutPoint*>(ctx->pinned);
-
-    std::vector<MeshCounters> mcount;
-    std::vector<v3d_mesh_triangle> tris;
-    std::vector<uint32_t> tri_patch;
-    ctx->last_triangles = 0;
-    if (mesh) {
-        uint32_t n_tris = 0;
-        mcount.resize(n_active);
-        V3D_CK(cudaMemcpyAsync(&n_tris, P.mesh.count, sizeof(uint32_t), cudaMemcpyDeviceToHost,
-                               stream));
-        V3D_CK(cudaMemcpyAsync(mcount.data(), P.mesh.counters, sizeof(MeshCounters) * n_active,
-                               cudaMemcpyDeviceToHost, stream));
-        V3D_CK(cudaStreamSynchronize(stream));
-        tris.resize(n_tris);
-        if (n_tris) {
-            V3D_CK(cudaMemcpyAsync(tris.data(), P.m_tris, sizeof(v3d_mesh_triangle) * n_tris,
+        uint8_t* hb = block.get();
+        if (n_out) {
+            V3D_CK(cudaMemcpyAsync(hb + h_pts, P.o_pts, sizeof(v3d_point) * n_out,
                                    cudaMemcpyDeviceToHost, stream));
-            V3D_CK(cudaStreamSynchronize(stream));
+            V3D_CK(cudaMemcpyAsync(hb + h_sites, P.o_sites, sizeof(v3d_grid_site) * n_out,
+                                   cudaMemcpyDeviceToHost, stream));
+            V3D_CK(cudaMemcpyAsync(hb + h_attrs, P.o_attrs, sizeof(v3d_point_attributes) * n_out,
+                                   cudaMemcpyDeviceToHost, stream));
+            V3D_CK(cudaMemcpyAsync(hb + h_med, P.o_med, sizeof(MedianKey) * n_out,
+                                   cudaMemcpyDeviceToHost, stream));
         }
-        ctx->last_triangles = n_tris;
+        if (n_tris)
+            V3D_CK(cudaMemcpyAsync(hb + h_tris, P.m_tris, sizeof(v3d_mesh_triangle) * n_tris,
+                                   cudaMemcpyDeviceToHost, stream));
+        V3D_CK(cudaStreamSynchronize(stream));
     }
     ctx->last_wait_ms = ms_since(t_wait);
     const clk::time_point t_assemble = clk::now();
+    uint8_t* hb = block.get();
+    v3d_point* o_pts = reinterpret_cast<v3d_point*>(hb + h_pts);
+    v3d_grid_site* o_sites = reinterpret_cast<v3d_grid_site*>(hb + h_sites);
+    v3d_point_attributes* o_attrs = reinterpret_cast<v3d_point_attributes*>(hb + h_attrs);
+    const MedianKey* o_med = reinterpret_cast<const MedianKey*>(hb + h_med);
+    v3d_mesh_triangle* o_tris = reinterpret_cast<v3d_mesh_triangle*>(hb + h_tris);
     if (mesh) {
         // triangles are in patch order; accepted counts give each patch's range
         mesh->assign(plans.size(), MeshOut{});
@@ -680,6 +753,8 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
                 s.has_skip_reason = 1;
                 std::strncpy(s.skip_reason, r, V3D_SKIP_REASON_BYTES - 1);
             };
+            const size_t first = t0;
+            t0 += c.accepted;
             if (npts < 3) {
                 reason("fewer than three accepted fused dense points are available");
                 continue;
@@ -696,8 +771,10 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
             s.accepted_triangles = c.accepted;
             s.rejected_discontinuities = c.discontinuities;
             s.rejected_degenerate = c.degenerate;
-            m.tris.assign(tris.begin() + t0, tris.begin() + t0 + c.accepted);
-            t0 += c.accepted;
+            if (c.accepted) {
+                m.tris = Span<v3d_mesh_triangle>{o_tris + first, c.accepted};
+                m.block = block;
+            }
         }
         for (size_t i = 0; i < plans.size(); ++i) {
             if (!plans[i].skipped) continue;
@@ -711,40 +788,38 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
         }
     }
     // ---- assemble per reference ----
-    // each pool segment is ordered by reference: find every reference's range
-    const uint32_t seg_begin[3] = {0, segs[0], segs[1]}, seg_end[3] = {segs[0], segs[1], segs[2]};
-    std::vector<uint32_t> range(3 * (n_active + 1));
-    for (int sgi = 0; sgi < 3; ++sgi) {
-        uint32_t i = seg_begin[sgi];
-        for (size_t k = 0; k <= n_active; ++k) {
-            while (i < seg_end[sgi] && pool[i].ref < k) ++i;
-            range[sgi * (n_active + 1) + k] = i;
-        }
-    }
     parallel_for(n_active, [&](size_t k) {
         PassResult& r = results[active[k]];
         const RefPlan& p = plans[active[k]];
         const RefCounters& c = ctr[k];
-        size_t n = 0;
-        for (int sgi = 0; sgi < 3; ++sgi)
-            n += range[sgi * (n_active + 1) + k + 1] - range[sgi * (n_active + 1) + k];
-        r.points.resize(n);
-        r.sites.resize(n);
-        r.attrs.resize(n);
-        std::vector<double> errors(n), supports(n), observations;
-        size_t o = 0;
-        for (int sgi = 0; sgi < 3; ++sgi) {
-            const uint32_t b0 = range[sgi * (n_active + 1) + k], b1 = range[sgi * (n_active + 1) + k + 1];
-            for (uint32_t i = b0; i < b1; ++i, ++o) {
-                const OutPoint& q = pool[i];
-                r.points[o] = q.p;
-                r.sites[o] = q.s;
-                r.attrs[o] = q.a;
-                errors[o] = q.error;
-                supports[o] = q.support;
-                if (sgi == 0) observations.push_back(q.observations);
+        const size_t b0 = base[k], n = base[k + 1] - base[k];
+        if (n) {
+            r.points = Span<v3d_point>{o_pts + b0, n};
+            r.sites = Span<v3d_grid_site>{o_sites + b0, n};
+            r.attrs = Span<v3d_point_attributes>{o_attrs + b0, n};
+            r.block = block;
+        }
+        // medians: round((n - 1) * 0.5) = n / 2-th order statistic (dense_legacy.rs:1168-1182)
+        std::vector<float> errors(n);
+        uint64_t sup_hist[256] = {0}, obs_hist[256] = {0};
+        uint64_t n_obs = 0;
+        for (size_t i = 0; i < n; ++i) {
+            const MedianKey& m = o_med[b0 + i];
+            errors[i] = m.error;
+            ++sup_hist[m.support];
+            if (m.primary) {
+                ++obs_hist[m.observations];
+                ++n_obs;
             }
         }
+        auto hist_kth = [](const uint64_t* h, uint64_t kth) {
+            uint64_t acc = 0;
+            for (int v = 0; v < 256; ++v) {
+                acc += h[v];
+                if (acc > kth) return static_cast<double>(v);
+            }
+            return 255.0;
+        };
         v3d_dense_stats& s = r.stats;
         std::memset(&s, 0, sizeof(s));
         s.attempted = 1;
@@ -769,15 +844,16 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
         s.fusion_input_observations = c.fusion_input;
         s.fusion_rejected_observations = c.fusion_rejected_obs;
         s.fusion_rejected_points = c.fusion_rejected_pts;
-        if (!observations.empty()) {
+        if (n_obs) {
             s.has_median_fusion_observations = 1;
-            s.median_fusion_observations = static_cast<float>(median_of(observations));
+            s.median_fusion_observations = static_cast<float>(hist_kth(obs_hist, n_obs / 2));
         }
         if (n) {
             s.has_median_supporting_views = 1;
-            s.median_supporting_views = static_cast<float>(median_of(supports));
+            s.median_supporting_views = static_cast<float>(hist_kth(sup_hist, n / 2));
+            std::nth_element(errors.begin(), errors.begin() + n / 2, errors.end());
             s.has_median_photometric_error = 1;
-            s.median_photometric_error = static_cast<float>(median_of(errors));
+            s.median_photometric_error = errors[n / 2];
         }
         s.has_search_min_depth = 1;
         s.search_min_depth = static_cast<float>(p.search_min);

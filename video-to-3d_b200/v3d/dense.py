@@ -113,6 +113,15 @@ class Context:
             raise V3DError(st, self.lib.v3d_last_error(self.handle).decode())
         return st
 
+    # Results are wrapped without copying their arrays: the numpy views own the
+    # C result and free it when they are collected.
+    def _dense(self, out, st=abi.OK):
+        return types.dense_from_result(
+            out, st, types.ResultOwner(self.lib.v3d_dense_result_free, out))
+
+    def _mesh(self, out):
+        return types.mesh_from_result(out, types.ResultOwner(self.lib.v3d_mesh_result_free, out))
+
     def estimate_depth_points_with_control(self, frames, cameras, sparse_points, focal,
                                            fine_grid=False, control=None, profile=None):
         prof = profile if profile is not None else profiles.reference()
@@ -122,10 +131,7 @@ class Context:
         st = self._check(self.lib.v3d_estimate_depth_points_with_control(
             self.handle, inp.frames, inp.n_frames, inp.cameras, inp.n_cameras, inp.sparse,
             inp.n_sparse, float(focal), int(fine_grid), C.byref(prof), fn, None, C.byref(out)))
-        try:
-            return types.dense_from_result(out, st)
-        finally:
-            self.lib.v3d_dense_result_free(C.byref(out))
+        return self._dense(out, st)
 
     def reconstruct_reference_patches(self, frames, cameras, sparse_points, focal,
                                       camera_indices, profile=None, fine_grid=False,
@@ -141,11 +147,7 @@ class Context:
             self.handle, inp.frames, inp.n_frames, inp.cameras, inp.n_cameras, inp.sparse,
             inp.n_sparse, float(focal), int(fine_grid), C.byref(prof), idx, n, fn, None, outs,
             present))
-        res = []
-        for i in range(n):
-            res.append(types.dense_from_result(outs[i]) if present[i] else None)
-            self.lib.v3d_dense_result_free(C.byref(outs[i]))
-        return res
+        return [self._dense(outs[i]) if present[i] else None for i in range(n)]
 
     def reconstruct_reference_patches_meshed(self, frames, cameras, sparse_points, focal,
                                              camera_indices, profile=None, fine_grid=False,
@@ -166,10 +168,12 @@ class Context:
             meshes, present))
         res = []
         for i in range(n):
-            res.append((types.dense_from_result(outs[i]), types.mesh_from_result(meshes[i]))
-                       if present[i] else None)
-            self.lib.v3d_dense_result_free(C.byref(outs[i]))
-            self.lib.v3d_mesh_result_free(C.byref(meshes[i]))
+            if present[i]:
+                res.append((self._dense(outs[i]), self._mesh(meshes[i])))
+            else:
+                self.lib.v3d_dense_result_free(C.byref(outs[i]))
+                self.lib.v3d_mesh_result_free(C.byref(meshes[i]))
+                res.append(None)
         return res
 
     def estimate_depth_points_limited(self, frames, cameras, sparse_points, focal,
@@ -183,10 +187,7 @@ class Context:
             self.handle, inp.frames, inp.n_frames, inp.cameras, inp.n_cameras, inp.sparse,
             inp.n_sparse, float(focal), int(reference_views), int(fine_grid), C.byref(prof), fn,
             None, C.byref(out), C.byref(omitted)))
-        try:
-            return types.dense_from_result(out, st), bool(omitted.value)
-        finally:
-            self.lib.v3d_dense_result_free(C.byref(out))
+        return self._dense(out, st), bool(omitted.value)
 
     def last_run_info(self):
         """Device time, kernel launches and work units of the last dense call."""
@@ -219,10 +220,7 @@ class Context:
         self._check(self.lib.v3d_reconstruct_dense_mesh_with_control(
             self.handle, *mi.args(), cams.cameras, cams.n_cameras, int(width), int(height),
             float(focal), fn, None, C.byref(out)))
-        try:
-            return types.mesh_from_result(out)
-        finally:
-            self.lib.v3d_mesh_result_free(C.byref(out))
+        return self._mesh(out)
 
 
 def has_distributed_landmarks(frames, cameras, sparse_points, focal, control=None):

@@ -125,11 +125,34 @@ def _opt(has, value):
     return value if has else None
 
 
-def _array(ptr, n, dtype):
+class ResultOwner:
+    """Frees one C result when the last array viewing its memory is collected.
+
+    The device library hands results back in page-locked memory shared by a
+    whole batch; wrapping them without a copy keeps that memory alive exactly
+    as long as a numpy view of it exists."""
+
+    __slots__ = ("_free", "_ref")
+
+    def __init__(self, free, struct):
+        self._free = free
+        self._ref = C.pointer(struct)  # keeps the struct (and its array) alive
+
+    def __del__(self):
+        free, self._free = self._free, None
+        if free is not None:
+            free(self._ref)
+
+
+def _array(ptr, n, dtype, owner=None):
     if n == 0 or not ptr:
         return np.zeros(0, dtype=dtype)
-    raw = np.ctypeslib.as_array(C.cast(ptr, C.POINTER(C.c_uint8)), shape=(n * dtype.itemsize,))
-    return raw.view(dtype).copy()
+    addr = C.cast(ptr, C.c_void_p).value
+    buf = (C.c_char * (n * dtype.itemsize)).from_address(addr)
+    if owner is None:
+        return np.frombuffer(buf, dtype=dtype).copy()
+    buf._owner = owner
+    return np.frombuffer(buf, dtype=dtype)
 
 
 def stats_dict(s):
@@ -183,16 +206,18 @@ def _patch_dict(p):
     }
 
 
-def dense_from_result(r, status=abi.OK):
+def dense_from_result(r, status=abi.OK, owner=None):
+    """DenseAnalysis of a C result; with `owner` (a ResultOwner of r) the point
+    arrays are views of the result's memory, else copies."""
     stats = stats_dict(r.stats)
     stats["source_frames"] = [int(r.source_frames[i]) for i in range(r.n_source_frames)]
     stats["reference_frames"] = [int(r.reference_frames[i]) for i in range(r.n_reference_frames)]
     stats["reference_attempts"] = [_attempt_dict(r.attempts[i]) for i in range(r.n_attempts)]
     stats["reference_patches"] = [_patch_dict(r.patches[i]) for i in range(r.n_patches)]
     n = int(r.n_points)
-    return DenseAnalysis(stats=stats, points=_array(r.points, n, POINT_DTYPE),
-                         grid_sites=_array(r.grid_sites, n, SITE_DTYPE),
-                         point_attributes=_array(r.point_attributes, n, ATTR_DTYPE),
+    return DenseAnalysis(stats=stats, points=_array(r.points, n, POINT_DTYPE, owner),
+                         grid_sites=_array(r.grid_sites, n, SITE_DTYPE, owner),
+                         point_attributes=_array(r.point_attributes, n, ATTR_DTYPE, owner),
                          status=status)
 
 
@@ -207,10 +232,11 @@ def _mesh_stats_dict(s):
     return d
 
 
-def mesh_from_result(r):
+def mesh_from_result(r, owner=None):
+    """MeshAnalysis of a C mesh result; `owner` as for dense_from_result."""
     return MeshAnalysis(
         stats=_mesh_stats_dict(r.stats),
-        triangles=_array(r.triangles, int(r.n_triangles), TRIANGLE_DTYPE),
+        triangles=_array(r.triangles, int(r.n_triangles), TRIANGLE_DTYPE, owner),
         reference_frames=[int(r.reference_frames[i]) for i in range(r.n_reference_frames)],
         reference_patches=[_mesh_stats_dict(r.patches[i]) for i in range(r.n_patches)])
 
