@@ -205,10 +205,25 @@ def test_fast_zsad_sweep_agreement(ctx, oracle):
     assert cost_err < 1e-3, cost_err  # 0-255 units
 
 
-def test_fast_zncc_points(ctx, oracle):
+def _zsad(radius):
+    prof = profiles.reference(precision=abi.PRECISION_FAST32)
+    prof.patch_radius = radius
+    prof.depth_hypotheses = 48
+    prof.grid_stride = 2
+    return prof
+
+
+# radius 4 (9x9, 81 taps) needs three rounds of 32 lanes in the lane-parallel
+# direct cost and window reductions
+@pytest.mark.parametrize("prof_of,storage", [
+    (lambda: profiles.zncc(2, 64, 4, 2), "f32"),
+    (lambda: profiles.zncc(4, 64, 4, 2), "f32"),
+    (lambda: _zsad(4), "rgba8"),
+], ids=["zncc-r2", "zncc-r4", "zsad-r4"])
+def test_fast_points(ctx, oracle, prof_of, storage):
     clip = synth.plain_small_clip(seed=5, width=192, height=112)
-    frames = clip.frames("f32")
-    prof = profiles.zncc(2, 64, 4, 2)
+    frames = clip.frames(storage)
+    prof = prof_of()
     exact = profiles.with_precision(prof, abi.PRECISION_EXACT64)
     g = ctx.reconstruct_reference_patches(frames, clip.cameras, clip.sparse, clip.focal, [2],
                                           profile=prof)[0]

@@ -509,76 +509,99 @@ __global__ void __launch_bounds__(256) k_reciprocal_exact(BatchDev b, const Cand
 }
 
 // ---- reciprocal check, fast policy ---------------------------------------------
-// Same contract as k_reciprocal for the fast policy, organised for the
-// memory system: one warp per (candidate, source);
-//  * the direct cost and the exact-f64 source contrast run lane-parallel over
-//    the window taps with warp reductions (max/min are order-free, so the
-//    contrast gate stays exact);
-//  * the single-view sweep moves every window tap monotonically along its
-//    epipolar line as the inverse depth varies (a 1-D projective map), so the
-//    reference texels of all hypotheses lie in the bounding box of the 4 window
-//    corners mapped at the first and last hypothesis.  That band is staged
-//    into shared memory with coalesced loads and every bilinear tap of every
-//    hypothesis reads it from there; a band too large for the buffer falls
-//    back to global loads.
-constexpr int kBandCap = 1344;  // texels staged per warp (8 warps x 5.25 KB static smem)
+// Same contract as k_reciprocal_exact for the fast policy, split in two
+// kernels so that the single-view sweep, where the time goes, is not sized
+// by the registers of the exact-f64 prologue:
+//  * k_recip_prepare, one warp per (candidate, source): the direct cost and
+//    the exact-f64 source contrast, lane-parallel over the window taps with
+//    warp reductions (max/min are order-free, so the contrast gate stays
+//    exact).  A pair that passes parks its source pixel in its RecipObs slot
+//    with valid = kObsPending;
+//  * k_recip_sweep, one warp per pending pair, lanes over hypotheses:
+//    re-samples the source window (the same f64 taps, so the same f32
+//    values), sweeps every hypothesis and writes the final RecipObs.
+//    Per hypothesis the four window corners are mapped first; when they land
+//    inside the bilinear domain with a margin that covers f32 rounding, every
+//    tap does (the denominator is affine, so its minimum over the window is at
+//    a corner, and a projective map with a positive denominator keeps the
+//    window inside the hull of its mapped corners) and the taps skip their
+//    bounds tests.
+constexpr int32_t kObsPending = 2;
+// rounds of 32 lanes that cover the taps of the largest window (9x9)
+constexpr int kTapRounds = ((2 * V3D_MAX_PATCH_RADIUS + 1) * (2 * V3D_MAX_PATCH_RADIUS + 1) + 31) / 32;
 
 __device__ __forceinline__ float warp_sum(float v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
 }
-__device__ __forceinline__ float warp_minf(float v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
-    return v;
-}
-__device__ __forceinline__ float warp_maxf(float v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
-    return v;
-}
 
-struct BandView {
-    const float* band;
-    int bx0, by0, bw, bh;
-};
-
-// Window cost against the fixed window pv (mean pm, squared deviation pvar),
-// sampling through H at taps (x + dx, y + dy).  The window rows run as a
-// rolled loop with the taps of a row unrolled: a fully unrolled 7x7 or 9x9
-// body, once per sampling path, outgrows the instruction cache.
-// Sampler: the staged band (BandSampler) or the image in global memory.
-struct BandSampler {
-    const float* band;
-    int bx0, by0, bw, bh;
-    __device__ __forceinline__ float operator()(float u, float v) const {
-        const float fu = floorf(u), fv = floorf(v);
-        int ix = (int)fu - bx0, iy = (int)fv - by0;
-        ix = min(max(ix, 0), bw - 2);
-        iy = min(max(iy, 0), bh - 2);
-        const float* q = band + iy * bw + ix;
-        const float tx = u - fu, ty = v - fv;
-        const float top = fmaf(q[1] - q[0], tx, q[0]);
-        const float bot = fmaf(q[bw + 1] - q[bw], tx, q[bw]);
-        return fmaf(bot - top, ty, top);
-    }
-};
-
+// Bilinear sample at a non-negative coordinate below 2^22 (the caller checks
+// the domain).  floor() is one round-down add of 2^23, which leaves floor(u)
+// in the low mantissa bits: the same floor, integer and fraction as floorf.
 template <class T>
-struct GlobalSampler {
-    const T* data;
-    uint32_t width;
-    __device__ __forceinline__ float operator()(float u, float v) const {
-        return sample_fast<T>(data, width, u, v);
-    }
-};
+__device__ __forceinline__ float sample_nonneg(const T* __restrict__ p, uint32_t w, float u,
+                                               float v) {
+    constexpr float kShift = 8388608.0f;  // 2^23
+    const float tu = __fadd_rd(u, kShift), tv = __fadd_rd(v, kShift);
+    const float fu = tu - kShift, fv = tv - kShift;
+    const uint32_t ix = (uint32_t)(__float_as_int(tu) - __float_as_int(kShift));
+    const uint32_t iy = (uint32_t)(__float_as_int(tv) - __float_as_int(kShift));
+    const float tx = u - fu, ty = v - fv;
+    const size_t r0 = (size_t)iy * w + ix;
+    const float v00 = pix<T>(p, r0), v10 = pix<T>(p, r0 + 1);
+    const float v01 = pix<T>(p, r0 + w), v11 = pix<T>(p, r0 + w + 1);
+    const float top = fmaf(v10 - v00, tx, v00);
+    const float bot = fmaf(v11 - v01, tx, v01);
+    return fmaf(bot - top, ty, top);
+}
 
-template <int R, int COST, class S>
-__device__ __forceinline__ bool window_cost_sampled(const float* pv, float pm, float pvar,
-                                                    const float* H, float zmin, float wl, float hl,
-                                                    float minvar, const S& sample, float x,
-                                                    float y, float& cost) {
+// True when every tap (x + dx, y + dy), |dx|, |dy| <= R, maps through H to a
+// point with denominator above zmin and inside [0, wl) x [0, hl), as the f32
+// per-tap tests of window_cost would compute it.  The margins bound the f32
+// rounding of the corner and of any inner tap (a few ulp of the magnitudes
+// involved, taken at 2^-20 relative).
+template <int R>
+__device__ __forceinline__ bool window_inside(const float* H, float zmin, float wl, float hl,
+                                              float x, float y) {
+    const float ax = fabsf(x) + (float)R, ay = fabsf(y) + (float)R;
+    const float su = fmaf(fabsf(H[0]), ax, fmaf(fabsf(H[1]), ay, fabsf(H[2])));
+    const float sv = fmaf(fabsf(H[3]), ax, fmaf(fabsf(H[4]), ay, fabsf(H[5])));
+    const float sz = fmaf(fabsf(H[6]), ax, fmaf(fabsf(H[7]), ay, fabsf(H[8])));
+    constexpr float kRel = 9.5367431640625e-07f;  // 2^-20
+    float hmin = 3.0e38f, umin = 3.0e38f, vmin = 3.0e38f, umax = -3.0e38f, vmax = -3.0e38f;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const float X = x + ((c & 1) ? (float)R : -(float)R);
+        const float Y = y + ((c & 2) ? (float)R : -(float)R);
+        const float h2 = fmaf(H[6], X, fmaf(H[7], Y, H[8]));
+        const float iv = __fdividef(1.0f, h2);
+        const float u = fmaf(H[0], X, fmaf(H[1], Y, H[2])) * iv;
+        const float v = fmaf(H[3], X, fmaf(H[4], Y, H[5])) * iv;
+        hmin = fminf(hmin, h2);
+        umin = fminf(umin, u);
+        umax = fmaxf(umax, u);
+        vmin = fminf(vmin, v);
+        vmax = fmaxf(vmax, v);
+    }
+    if (!(hmin > zmin + kRel * sz) || !(hmin > 0.f)) return false;
+    const float m = 0.015625f + kRel * (fmaxf(su, sv) + fmaxf(wl, hl) * sz) / hmin;
+    // NaN fails every comparison
+    return umin >= m && vmin >= m && umax <= wl - m && vmax <= hl - m;
+}
+
+// Window cost against the window centred on its mean pm (pvc, squared
+// deviation pvar), sampling the image through H at taps (x + dx, y + dy);
+// the samples are shifted by pm too before their sums, as in the direct cost.  CHECK runs the
+// per-tap domain tests; without it the caller has established the domain
+// with window_inside.  The window rows run as a rolled loop with the taps of
+// a row unrolled: a fully unrolled 7x7 or 9x9 body outgrows the instruction
+// cache.
+template <class T, int R, int COST, bool CHECK>
+__device__ __forceinline__ bool window_cost(const float* pvc, float pm, float pvar, const float* H,
+                                            float zmin, float wl, float hl, float minvar,
+                                            const T* __restrict__ img, uint32_t w, float x,
+                                            float y, float& cost) {
     constexpr int W = 2 * R + 1;
     constexpr int N = W * W;
     float sv[COST == 1 ? 1 : N];
@@ -587,22 +610,22 @@ __device__ __forceinline__ bool window_cost_sampled(const float* pv, float pm, f
     for (int dy = 0; dy < W; ++dy) {
         const float Y = y + (float)(dy - R);
         const float hx = fmaf(H[1], Y, H[2]), hy = fmaf(H[4], Y, H[5]), hz = fmaf(H[7], Y, H[8]);
-        const float* prow = pv + dy * W;
+        const float* prow = pvc + dy * W;
 #pragma unroll
         for (int dx = 0; dx < W; ++dx) {
             const float X = x + (float)(dx - R);
             const float h2 = fmaf(H[6], X, hz);
-            if (!(h2 > zmin)) return false;
-            const float iv = __frcp_rn(h2);
+            if (CHECK && !(h2 > zmin)) return false;
+            const float iv = __fdividef(1.0f, h2);
             const float u = fmaf(H[0], X, hx) * iv;
             const float v = fmaf(H[3], X, hy) * iv;
-            if (!(u >= 0.f && v >= 0.f && u < wl && v < hl)) return false;
-            const float smp = sample(u, v);
+            if (CHECK && !(u >= 0.f && v >= 0.f && u < wl && v < hl)) return false;
+            const float smp = sample_nonneg<T>(img, w, u, v);
             if (COST == 1) {
                 const float s = smp - pm;
                 ss += s;
                 sss = fmaf(s, s, sss);
-                sps = fmaf(prow[dx] - pm, s, sps);
+                sps = fmaf(prow[dx], s, sps);
             } else {
                 sv[dy * W + dx] = smp;
                 ss += smp;
@@ -619,45 +642,19 @@ __device__ __forceinline__ bool window_cost_sampled(const float* pv, float pm, f
     const float ms = ss / (float)N;
     float acc = 0.f;
 #pragma unroll
-    for (int i = 0; i < N; ++i) acc += fabsf((pv[i] - pm) - (sv[i] - ms));
+    for (int i = 0; i < N; ++i) acc += fabsf(pvc[i] - (sv[i] - ms));
     cost = acc / (float)N;
     return true;
 }
 
-// Best (lowest cost, then lowest index) hypothesis of this lane's share.
-template <int R, int COST, class S>
-__device__ __forceinline__ void sweep_lane(const DevProfile& prof, const DevSource& src,
-                                           const float* inv_tab, const float* pv, float pm,
-                                           float pvar, float wl, float hl, const S& sample,
-                                           float x0, float y0, uint32_t lane, float& be,
-                                           int& bk) {
-    const float minvar = (float)prof.min_variance;
-    for (int k = lane; k < prof.planes; k += 32) {
-        const float inv = inv_tab[k];
-        float H[9];
-        plane_h(src.bwd_A, src.bwd_b, inv, H);
-        float e;
-        if (window_cost_sampled<R, COST>(pv, pm, pvar, H, 1.0e-4f * inv, wl, hl, minvar, sample,
-                                         x0, y0, e) &&
-            (double)e <= prof.max_error && e < be) {
-            be = e;
-            bk = k;
-        }
-    }
-}
-
 template <class T, int R, int COST>
-__global__ void __launch_bounds__(256, 2) k_reciprocal_fast(BatchDev b, const Cand* __restrict__ cands,
-                                                         const uint32_t* __restrict__ count,
-                                                         RecipObs* __restrict__ obs,
-                                                         RefCounters* __restrict__ ctr) {
+__global__ void __launch_bounds__(256) k_recip_prepare(BatchDev b, const Cand* __restrict__ cands,
+                                                       const uint32_t* __restrict__ count,
+                                                       RecipObs* __restrict__ obs,
+                                                       RefCounters* __restrict__ ctr) {
     constexpr int W = 2 * R + 1;
     constexpr int N = W * W;
-    __shared__ float band_all[8][kBandCap];
-    __shared__ float pv_all[8][N];
-    const uint32_t lane = lane_id(), wid = threadIdx.x >> 5;
-    float* band = band_all[wid];
-    float* pv = pv_all[wid];
+    const uint32_t lane = lane_id();
     const uint32_t ms = (uint32_t)b.max_src;
     const uint64_t items = (uint64_t)(*count) * ms;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
@@ -675,7 +672,6 @@ __global__ void __launch_bounds__(256, 2) k_reciprocal_fast(BatchDev b, const Ca
         res.pos = D3{0, 0, 0};
         bool ok = si < ref.n_src;
         const DevSource& src = ref.src[ok ? si : 0];
-        const float* inv_tab = b.src_inv + ((size_t)cd.ref * kMaxSources + (ok ? si : 0)) * prof.planes;
         D3 rp, sp;
         if (ok) ok = project_exact(ref.cam, cd.pos, ref.img.width, ref.img.height, ref.focal, rp);
         // direct cost of the reference window at (rp.x, rp.y), depth rp.z; lanes over taps
@@ -686,10 +682,12 @@ __global__ void __launch_bounds__(256, 2) k_reciprocal_fast(BatchDev b, const Ca
             const float zmin = zmin_of(inv);
             const T* rdata = static_cast<const T*>(ref.img.data);
             const T* sdata = static_cast<const T*>(src.img.data);
-            float rv[2] = {0.f, 0.f}, sv2[2] = {0.f, 0.f};
+            float rv[kTapRounds], sv2[kTapRounds];
             bool tv = true;
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
+            for (int h = 0; h < kTapRounds; ++h) {
+                rv[h] = 0.f;
+                sv2[h] = 0.f;
                 const int t = lane + 32 * h;
                 if (t >= N) continue;
                 const float X = (float)rp.x + (float)(t % W - R);
@@ -715,35 +713,55 @@ __global__ void __launch_bounds__(256, 2) k_reciprocal_fast(BatchDev b, const Ca
             }
             ok = __all_sync(0xffffffffu, tv);
             if (ok) {
+                // taps beyond N contribute exact zeros to every sum
                 const float n = (float)N;
-                const bool h1 = lane + 32 < N;
-                const float mr = warp_sum(rv[0] + (h1 ? rv[1] : 0.f)) / n;
-                const float ms = warp_sum(sv2[0] + (h1 ? sv2[1] : 0.f)) / n;
-                const float dr0 = rv[0] - mr, ds0 = sv2[0] - ms;
-                const float dr1 = h1 ? rv[1] - mr : 0.f, ds1 = h1 ? sv2[1] - ms : 0.f;
+                float sr = 0.f, ssv = 0.f;
+#pragma unroll
+                for (int h = 0; h < kTapRounds; ++h) {
+                    sr += rv[h];
+                    ssv += sv2[h];
+                }
+                const float mr = warp_sum(sr) / n;
+                const float mss = warp_sum(ssv) / n;
+                float dr[kTapRounds], ds[kTapRounds];
+#pragma unroll
+                for (int h = 0; h < kTapRounds; ++h) {
+                    const bool in = lane + 32 * h < N;
+                    dr[h] = in ? rv[h] - mr : 0.f;
+                    ds[h] = in ? sv2[h] - mss : 0.f;
+                }
                 float cost;
                 if (COST == 1) {
-                    const float cov = warp_sum(dr0 * ds0 + dr1 * ds1);
-                    const float vr = warp_sum(dr0 * dr0 + dr1 * dr1);
-                    const float vs = warp_sum(ds0 * ds0 + ds1 * ds1);
+                    float c = 0.f, r2 = 0.f, s2 = 0.f;
+#pragma unroll
+                    for (int h = 0; h < kTapRounds; ++h) {
+                        c += dr[h] * ds[h];
+                        r2 += dr[h] * dr[h];
+                        s2 += ds[h] * ds[h];
+                    }
+                    const float cov = warp_sum(c);
+                    const float vr = warp_sum(r2);
+                    const float vs = warp_sum(s2);
                     if (!(vr > 0.f) || !(vs > 0.f) || vr / n < (float)prof.min_variance ||
                         vs / n < (float)prof.min_variance)
                         ok = false;
                     cost = 1.0f - cov * rsqrtf(vr * vs);
                 } else {
-                    cost = warp_sum(fabsf(dr0 - ds0) + (h1 ? fabsf(dr1 - ds1) : 0.f)) / n;
+                    float a = 0.f;
+#pragma unroll
+                    for (int h = 0; h < kTapRounds; ++h) a += fabsf(dr[h] - ds[h]);
+                    cost = warp_sum(a) / n;
                 }
                 ok = ok && !((double)cost > prof.max_error);
             }
         }
         if (ok) ok = project_exact(src.cam, cd.pos, src.img.width, src.img.height, ref.focal, sp);
         // exact patch_contrast of the source window at (sp.x, sp.y), lanes over taps
-        float pm = 0.f, pvar = 0.f;
         if (ok) {
             double mn = kInf, mx = -kInf;
             bool inb = true;
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
+            for (int h = 0; h < kTapRounds; ++h) {
                 const int t = lane + 32 * h;
                 if (t >= N) continue;
                 double v;
@@ -754,7 +772,6 @@ __global__ void __launch_bounds__(256, 2) k_reciprocal_fast(BatchDev b, const Ca
                 }
                 mn = fmin(mn, v);
                 mx = fmax(mx, v);
-                pv[t] = (float)v;
             }
             ok = __all_sync(0xffffffffu, inb);
             if (ok) {
@@ -765,84 +782,107 @@ __global__ void __launch_bounds__(256, 2) k_reciprocal_fast(BatchDev b, const Ca
                 }
                 ok = !(dsub(mx, mn) < prof.min_contrast);
             }
-            __syncwarp();
-            if (ok) {
-                const bool h1 = lane + 32 < N;
-                const float p0 = pv[lane < N ? lane : 0], p1 = h1 ? pv[lane + 32] : 0.f;
-                pm = warp_sum((lane < N ? p0 : 0.f) + p1) / (float)N;
-                const float d0 = lane < N ? p0 - pm : 0.f, d1 = h1 ? p1 - pm : 0.f;
-                pvar = warp_sum(d0 * d0 + d1 * d1);
-            }
         }
         if (ok) {
-            // band of the reference texels that every hypothesis can reach
-            BandView bv{nullptr, 0, 0, 0, 0};
-            {
-                const int k = (lane & 1) ? prof.planes - 1 : 0;
-                const float cx = (float)sp.x + ((lane & 2) ? (float)R : -(float)R);
-                const float cy = (float)sp.y + ((lane & 4) ? (float)R : -(float)R);
-                float H[9];
-                plane_h(src.bwd_A, src.bwd_b, inv_tab[k], H);
-                const float h2 = fmaf(H[6], cx, fmaf(H[7], cy, H[8]));
-                float u = fmaf(H[0], cx, fmaf(H[1], cy, H[2])) / h2;
-                float v = fmaf(H[3], cx, fmaf(H[4], cy, H[5])) / h2;
-                bool good = lane >= 8 || (h2 > 0.f && isfinite(u) && isfinite(v));
-                good = __all_sync(0xffffffffu, good);
-                float umin = warp_minf(lane < 8 ? u : 3.0e38f), umax = warp_maxf(lane < 8 ? u : -3.0e38f);
-                float vmin = warp_minf(lane < 8 ? v : 3.0e38f), vmax = warp_maxf(lane < 8 ? v : -3.0e38f);
-                if (good) {
-                    const float wl = (float)(ref.img.width - 1), hl = (float)(ref.img.height - 1);
-                    umin = fmaxf(umin, 0.f);
-                    vmin = fmaxf(vmin, 0.f);
-                    umax = fminf(umax, wl);
-                    vmax = fminf(vmax, hl);
-                    if (umin <= umax && vmin <= vmax) {
-                        const int bx0 = max((int)floorf(umin) - 1, 0);
-                        const int by0 = max((int)floorf(vmin) - 1, 0);
-                        const int bx1 = min((int)floorf(umax) + 2, (int)ref.img.width - 1);
-                        const int by1 = min((int)floorf(vmax) + 2, (int)ref.img.height - 1);
-                        const int bw = bx1 - bx0 + 1, bh = by1 - by0 + 1;
-                        if (bw >= 2 && bh >= 2 && bw * bh <= kBandCap) {
-                            const T* rdata = static_cast<const T*>(ref.img.data);
-                            for (int i = lane; i < bw * bh; i += 32) {
-                                const int yy = i / bw, xx = i - yy * bw;
-                                band[i] = pix<T>(rdata, (size_t)(by0 + yy) * ref.img.width + bx0 + xx);
-                            }
-                            bv = BandView{band, bx0, by0, bw, bh};
-                        }
-                    }
-                }
-            }
-            __syncwarp();
+            res.pos = sp;
+            res.valid = kObsPending;
             if (lane == 0) atomicAdd(&ctr[cd.ref].recip_evals, (unsigned long long)prof.planes);
-            float be = 3.0e38f;
-            int bk = 0x7fffffff;
-            const float x0 = (float)sp.x, y0 = (float)sp.y;
-            const float wl = (float)(ref.img.width - 1), hl = (float)(ref.img.height - 1);
-            if (bv.band)
-                sweep_lane<R, COST>(prof, src, inv_tab, pv, pm, pvar, wl, hl,
-                                    BandSampler{bv.band, bv.bx0, bv.by0, bv.bw, bv.bh}, x0, y0,
-                                    lane, be, bk);
-            else
-                sweep_lane<R, COST>(prof, src, inv_tab, pv, pm, pvar, wl, hl,
-                                    GlobalSampler<T>{static_cast<const T*>(ref.img.data),
-                                                     ref.img.width},
-                                    x0, y0, lane, be, bk);
+        }
+        if (lane == 0 && si < ref.n_src) obs[it] = res;
+    }
+}
+
+template <class T, int R, int COST>
+__global__ void __launch_bounds__(256, 3) k_recip_sweep(BatchDev b, const Cand* __restrict__ cands,
+                                                     const uint32_t* __restrict__ count,
+                                                     RecipObs* __restrict__ obs) {
+    constexpr int W = 2 * R + 1;
+    constexpr int N = W * W;
+    __shared__ float pvc_all[8][N];
+    const uint32_t lane = lane_id(), wid = threadIdx.x >> 5;
+    float* pvc = pvc_all[wid];
+    const uint32_t ms = (uint32_t)b.max_src;
+    const uint64_t items = (uint64_t)(*count) * ms;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    const DevProfile& prof = b.prof;
+    for (uint64_t item = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; item < items;
+         item += nwarps) {
+        const uint32_t ci = (uint32_t)(item / ms);
+        const int si = (int)(item - (uint64_t)ci * ms);
+        const uint64_t it = (uint64_t)ci * kMaxSources + si;
+        const uint32_t r = cands[ci].ref;
+        const DevReference& ref = b.refs[r];
+        if (si >= ref.n_src || obs[it].valid != kObsPending) continue;
+        const D3 sp = obs[it].pos;
+        const DevSource& src = ref.src[si];
+        // the source window as the contrast gate sampled it, centred; taps
+        // beyond N contribute exact zeros to the sums
+        float p[kTapRounds];
+        float psum = 0.f;
 #pragma unroll
-            for (int off = 16; off > 0; off >>= 1) {
-                const float oe = __shfl_down_sync(0xffffffffu, be, off);
-                const int ok2 = __shfl_down_sync(0xffffffffu, bk, off);
-                if (oe < be || (oe == be && ok2 < bk)) {
-                    be = oe;
-                    bk = ok2;
-                }
+        for (int h = 0; h < kTapRounds; ++h) {
+            const int t = lane + 32 * h;
+            double v = 0.0;
+            if (t < N)
+                sample_exact<T>(src.img, dadd(sp.x, (double)(t % W - R)),
+                                dadd(sp.y, (double)(t / W - R)), v);
+            p[h] = (float)v;
+            psum += p[h];
+        }
+        const float pm = warp_sum(psum) / (float)N;
+        float dsq = 0.f;
+#pragma unroll
+        for (int h = 0; h < kTapRounds; ++h) {
+            const int t = lane + 32 * h;
+            const float d = t < N ? p[h] - pm : 0.f;
+            dsq += d * d;
+            if (t < N) pvc[t] = d;
+        }
+        const float pvar = warp_sum(dsq);
+        __syncwarp();
+        const float* inv_tab = b.src_inv + ((size_t)r * kMaxSources + si) * prof.planes;
+        const T* rimg = static_cast<const T*>(ref.img.data);
+        const uint32_t rw = ref.img.width;
+        const float wl = (float)(ref.img.width - 1), hl = (float)(ref.img.height - 1);
+        const float x0 = (float)sp.x, y0 = (float)sp.y;
+        const float minvar = (float)prof.min_variance;
+        float be = 3.0e38f;
+        int bk = 0x7fffffff;
+        for (int k = lane; k < prof.planes; k += 32) {
+            const float inv = inv_tab[k];
+            float H[9];
+            plane_h(src.bwd_A, src.bwd_b, inv, H);
+            const float zmin = 1.0e-4f * inv;
+            float e;
+            const bool ok =
+                window_inside<R>(H, zmin, wl, hl, x0, y0)
+                    ? window_cost<T, R, COST, false>(pvc, pm, pvar, H, zmin, wl, hl, minvar, rimg,
+                                                     rw, x0, y0, e)
+                    : window_cost<T, R, COST, true>(pvc, pm, pvar, H, zmin, wl, hl, minvar, rimg,
+                                                    rw, x0, y0, e);
+            if (ok && (double)e <= prof.max_error && e < be) {
+                be = e;
+                bk = k;
             }
-            bk = __shfl_sync(0xffffffffu, bk, 0);
-            if (bk == 0x7fffffff) {
-                ok = false;
-            } else {
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            const float oe = __shfl_down_sync(0xffffffffu, be, off);
+            const int ok2 = __shfl_down_sync(0xffffffffu, bk, off);
+            if (oe < be || (oe == be && ok2 < bk)) {
+                be = oe;
+                bk = ok2;
+            }
+        }
+        if (lane == 0) {
+            RecipObs res;
+            res.valid = 0;
+            res.pad = 0;
+            res.pos = D3{0, 0, 0};
+            if (bk != 0x7fffffff) {
                 const double rd = hypothesis_depth(bk, prof.planes, src.search_min, src.search_max);
                 const double ex = sp.z;
+                // reciprocal_depth_agrees (dense_legacy.rs:951-957)
                 bool agree = isfinite(ex) && isfinite(rd) && ex > 0.0 && rd > 0.0;
                 if (agree) {
                     const double scale = fmax(fmax(ex, rd), 1.0e-9);
@@ -854,9 +894,9 @@ __global__ void __launch_bounds__(256, 2) k_reciprocal_fast(BatchDev b, const Ca
                     res.valid = finite3(res.pos) ? 1 : 0;
                 }
             }
+            obs[it] = res;
         }
         __syncwarp();
-        if (lane == 0 && si < ref.n_src) obs[it] = res;
     }
 }
 
@@ -1038,10 +1078,13 @@ cudaError_t Typed<T>::reciprocal(const BatchDev& b, const Cand* cands, const uin
     if (b.prof.radius == RR) {                                                                 \
         if (b.exact)                                                                           \
             k_reciprocal_exact<T, RR><<<blocks, 256, 0, st>>>(b, cands, count, obs, ctr);      \
-        else if (b.prof.cost == 1)                                                             \
-            k_reciprocal_fast<T, RR, 1><<<blocks, 256, 0, st>>>(b, cands, count, obs, ctr);    \
-        else                                                                                   \
-            k_reciprocal_fast<T, RR, 0><<<blocks, 256, 0, st>>>(b, cands, count, obs, ctr);    \
+        else if (b.prof.cost == 1) {                                                           \
+            k_recip_prepare<T, RR, 1><<<blocks, 256, 0, st>>>(b, cands, count, obs, ctr);      \
+            k_recip_sweep<T, RR, 1><<<blocks, 256, 0, st>>>(b, cands, count, obs);             \
+        } else {                                                                               \
+            k_recip_prepare<T, RR, 0><<<blocks, 256, 0, st>>>(b, cands, count, obs, ctr);      \
+            k_recip_sweep<T, RR, 0><<<blocks, 256, 0, st>>>(b, cands, count, obs);             \
+        }                                                                                      \
         return cudaGetLastError();                                                             \
     }
     V3D_REC(1) V3D_REC(2) V3D_REC(3) V3D_REC(4)

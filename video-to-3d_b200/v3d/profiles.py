@@ -6,7 +6,8 @@ are in cost units of 1 - ZNCC (0 = identical windows, 1 = uncorrelated).
 """
 from . import abi
 
-# Project-defined ZNCC gate values (see DESIGN.md "ZNCC profile").
+# Project-defined ZNCC gate values (the reference has no ZNCC cost; these are
+# the gates of this build's 1 - ZNCC profile, mirrored in v3d_profile_zncc).
 ZNCC_MAX_COST = 0.5             # photometric gate: ZNCC >= 0.5
 ZNCC_MIN_MARGIN = 0.002         # ambiguity gate: comparable second must be this much worse
 ZNCC_MARGIN_SATURATION = 0.05   # depth_margin = margin / 0.05, clamped to [0, 1]
