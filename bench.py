@@ -257,7 +257,8 @@ def run_ours(args, rank, world, local):
     else:
         total_units = float(units)
     host = {k: float(np.mean([i[k] for i in infos]))
-            for k in ("host_plan_ms", "host_upload_ms", "host_wait_ms", "host_assemble_ms")}
+            for k in ("host_plan_ms", "host_upload_ms", "host_wait_ms", "host_block_ms",
+                      "host_readback_ms", "host_assemble_ms")}
     sweep_ms = float(np.mean([i["sweep_ms"] for i in infos]))
     recip_ms = float(np.mean([i["reciprocal_ms"] for i in infos]))
     comp_ms = float(np.mean([i["completion_ms"] for i in infos]))

@@ -422,6 +422,9 @@ typedef struct v3d_run_info {
     double host_assemble_ms;  /* splitting the point pool per reference, medians */
     double mesh_ms;           /* device mesh stage of the _meshed call */
     uint64_t triangles;       /* accepted triangles of the _meshed call */
+    double host_block_ms;     /* acquiring the pinned result block (within host_wait_ms) */
+    double host_readback_ms;  /* result copies into that block (within host_wait_ms) */
+    uint64_t result_bytes;    /* bytes of that block the results occupy */
 } v3d_run_info;
 
 int32_t v3d_last_run_info(const v3d_context* ctx, v3d_run_info* out);

@@ -258,6 +258,9 @@ int32_t v3d_last_run_info(const v3d_context* ctx, v3d_run_info* out) {
     out->host_assemble_ms = ctx->last_assemble_ms;
     out->mesh_ms = ctx->last_mesh_ms;
     out->triangles = ctx->last_triangles;
+    out->host_block_ms = ctx->last_block_ms;
+    out->host_readback_ms = ctx->last_readback_ms;
+    out->result_bytes = ctx->last_result_bytes;
     return V3D_OK;
 }
 

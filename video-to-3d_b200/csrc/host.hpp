@@ -44,6 +44,7 @@ struct RefPlan {
 // (host_block.cpp); the deleter returns it to a process-wide cache.
 using HostBlock = std::shared_ptr<uint8_t>;
 HostBlock host_block(size_t bytes);  // empty on allocation failure
+size_t host_block_bytes(const HostBlock& b);  // capacity of a block from host_block
 
 // A view of `size()` elements inside a HostBlock.
 template <class T>
@@ -146,6 +147,8 @@ struct v3d_context {
     double last_plan_ms = 0, last_upload_ms = 0, last_wait_ms = 0, last_assemble_ms = 0;
     float last_mesh_ms = 0.f;
     uint64_t last_triangles = 0;
+    double last_block_ms = 0, last_readback_ms = 0;
+    uint64_t last_result_bytes = 0;
 };
 
 namespace v3d {

@@ -47,6 +47,12 @@ void recycle(void* p, size_t bytes) {
     if (drop) cudaFreeHost(drop);
 }
 
+// Deleter of a block: back to the cache; carries the block's capacity.
+struct BlockRecycler {
+    size_t bytes;
+    void operator()(uint8_t* q) const { recycle(q, bytes); }
+};
+
 }  // namespace
 
 HostBlock host_block(size_t bytes) {
@@ -72,7 +78,12 @@ HostBlock host_block(size_t bytes) {
         }
         have = bytes;
     }
-    return HostBlock(static_cast<uint8_t*>(p), [have](uint8_t* q) { recycle(q, have); });
+    return HostBlock(static_cast<uint8_t*>(p), BlockRecycler{have});
+}
+
+size_t host_block_bytes(const HostBlock& b) {
+    const BlockRecycler* d = std::get_deleter<BlockRecycler>(b);
+    return d ? d->bytes : 0;
 }
 
 }  // namespace v3d

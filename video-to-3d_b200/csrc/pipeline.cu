@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cstring>
+#include <future>
 #include <stdexcept>
 
 #include "host.hpp"
@@ -612,6 +613,17 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
         V3D_CK(cudaGetLastError());
         ctx->last_launches += 3;
     }
+    // The result block, acquired on a helper thread while the device works,
+    // sized like the last call's results: a caller that still holds those
+    // needs a second block, and pinning one takes longer than the copies.
+    // Started only now, once every kernel before the read-back is enqueued:
+    // pinning can hold up this thread's CUDA calls while it runs.
+    std::future<HostBlock> early;
+    if (ctx->last_result_bytes)
+        early = std::async(std::launch::async, [dev = ctx->device, bytes = ctx->last_result_bytes] {
+            cudaSetDevice(dev);  // a new thread starts on device 0
+            return host_block(bytes);
+        });
     std::vector<MeshPatchDev> mp;
     if (mesh) {
         // patch descriptors need the per-reference point counts: one read of the counters
@@ -707,12 +719,18 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
     const size_t h_med = hl.take<MedianKey>(n_out);
     const size_t h_tris = hl.take<v3d_mesh_triangle>(n_tris);
     HostBlock block;
+    ctx->last_block_ms = ctx->last_readback_ms = 0;
+    ctx->last_result_bytes = n_out || n_tris ? hl.off : 0;
     if (n_out || n_tris) {
-        block = host_block(hl.off);
+        const clk::time_point t_block = clk::now();
+        if (early.valid()) block = early.get();
+        if (host_block_bytes(block) < hl.off) block = host_block(hl.off);
         if (!block) {
             ctx->last_error = "pinned result block allocation failed";
             return V3D_ERR_OUT_OF_MEMORY;
         }
+        ctx->last_block_ms = ms_since(t_block);
+        const clk::time_point t_copy = clk::now();
         uint8_t* hb = block.get();
         if (n_out) {
             V3D_CK(cudaMemcpyAsync(hb + h_pts, P.o_pts, sizeof(v3d_point) * n_out,
@@ -728,6 +746,7 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
             V3D_CK(cudaMemcpyAsync(hb + h_tris, P.m_tris, sizeof(v3d_mesh_triangle) * n_tris,
                                    cudaMemcpyDeviceToHost, stream));
         V3D_CK(cudaStreamSynchronize(stream));
+        ctx->last_readback_ms = ms_since(t_copy);
     }
     ctx->last_wait_ms = ms_since(t_wait);
     const clk::time_point t_assemble = clk::now();

@@ -148,6 +148,27 @@ __device__ __forceinline__ void load_window_int(const DevImage& img, uint32_t x,
 
 __device__ __forceinline__ float zmin_of(double inv_depth) { return (float)(1.0e-4 * inv_depth); }
 
+// Bilinear sample at a non-negative coordinate below 2^22 (the caller checks
+// the domain).  floor() is one round-down add of 2^23, which leaves floor(u)
+// in the low mantissa bits: the same floor, integer and fraction as floorf.
+template <class T>
+__device__ __forceinline__ float sample_nonneg(const T* __restrict__ p, uint32_t w, float u,
+                                               float v) {
+    constexpr float kShift = 8388608.0f;  // 2^23
+    const float tu = __fadd_rd(u, kShift), tv = __fadd_rd(v, kShift);
+    const float fu = tu - kShift, fv = tv - kShift;
+    const uint32_t ix = (uint32_t)(__float_as_int(tu) - __float_as_int(kShift));
+    const uint32_t iy = (uint32_t)(__float_as_int(tv) - __float_as_int(kShift));
+    const float tx = u - fu, ty = v - fv;
+    const size_t r0 = (size_t)iy * w + ix;
+    const float v00 = pix<T>(p, r0), v10 = pix<T>(p, r0 + 1);
+    const float v01 = pix<T>(p, r0 + w), v11 = pix<T>(p, r0 + w + 1);
+    const float top = fmaf(v10 - v00, tx, v00);
+    const float bot = fmaf(v11 - v01, tx, v01);
+    return fmaf(bot - top, ty, top);
+}
+
+
 
 // ---- sweep, warp per site ----------------------------------------------------
 // Lanes take hypotheses lane, lane+32, ...; each lane keeps the running
@@ -241,6 +262,12 @@ __global__ void __launch_bounds__(256) k_sweep_site(BatchDev b, const uint32_t* 
 // sample.  Products and sums are formed in f64: s^2 - (sum s)^2/n cancels
 // badly in f32 on low-variance windows.  Invalid taps are NaN and poison
 // their windows, which reproduces the reference's all-taps-valid rule.
+//
+// The footprint rows in shared memory keep their columns grouped by x mod
+// stride (column x at slot (x % s) * PXs + x / s), so the stride-s reads of
+// the horizontal box filter fall on consecutive words across the lanes; the
+// footprint's x coordinates come from a per-slot table, so the warp step
+// converts no integers.
 template <class T, int R>
 __global__ void __launch_bounds__(256) k_sweep_tiled(BatchDev b, uint64_t total_sites_unused,
                                                      SiteRank* __restrict__ rank,
@@ -256,23 +283,31 @@ __global__ void __launch_bounds__(256) k_sweep_tiled(BatchDev b, uint64_t total_
     if (gx0 >= ref.nx || gy0 >= ref.ny) return;
     const int s = (int)ref.stride;
     const int PX = (kTileX - 1) * s + W, PY = (kTileY - 1) * s + W;
-    const int npx = PX * PY;
+    const int PXs = (PX + s - 1) / s, PXp = PXs * s;  // columns per residue, padded row
+    const int np = PY * PXp;
+    const int ms = b.max_src;
     double* hs = smem_d;                     // [PY][32] row sums of s
     double* hss = hs + PY * kTileX;          // [PY][32] row sums of s^2
     double* hrs = hss + PY * kTileX;         // [PY][32] row sums of r*s
-    float* refv = reinterpret_cast<float*>(hrs + PY * kTileX);  // [PY][PX] reference values
-    float* samp = refv + npx;                // [PY][PX] source samples (NaN = invalid)
-    float* costs = samp + npx;               // [n_src][256]
-    float* hA = costs + kMaxSources * 256;   // [n_src][12] homography parts
-    float* pinv = hA + kMaxSources * 12;     // [planes] inverse depths
+    float* refv = reinterpret_cast<float*>(hrs + PY * kTileX);  // [PY][PXp] reference values
+    float* samp = refv + np;                 // [PY][PXp] source samples (NaN = invalid)
+    float* colx = samp + np;                 // [PXp] footprint x of each slot, NaN = padding
+    float* costs = colx + PXp;               // [max_src][256]
+    float* hA = costs + ms * 256;            // [max_src][12] homography parts
+    float* pinv = hA + ms * 12;              // [planes] inverse depths
     const int tid = threadIdx.x;
     const T* rdata = static_cast<const T*>(ref.img.data);
     const int px0 = (int)(ref.border + gx0 * s) - R, py0 = (int)(ref.border + gy0 * s) - R;
-    for (int i = tid; i < npx; i += 256) {
-        int yy = i / PX, xx = i - yy * PX;
-        int X = px0 + xx, Y = py0 + yy;
+    for (int t = tid; t < PXp; t += 256) {
+        const int x = (t % PXs) * s + t / PXs;
+        colx[t] = x < PX ? (float)(px0 + x) : __int_as_float(0x7fc00000);
+    }
+    for (int i = tid; i < np; i += 256) {
+        const int yy = i / PXp, t = i - yy * PXp;
+        const int x = (t % PXs) * s + t / PXs;
+        const int X = px0 + x, Y = py0 + yy;
         float v = __int_as_float(0x7fc00000);
-        if (X >= 0 && Y >= 0 && X < (int)ref.img.width && Y < (int)ref.img.height)
+        if (x < PX && X >= 0 && Y >= 0 && X < (int)ref.img.width && Y < (int)ref.img.height)
             v = pix<T>(rdata, (size_t)Y * ref.img.width + X);
         refv[i] = v;
     }
@@ -283,6 +318,10 @@ __global__ void __launch_bounds__(256) k_sweep_tiled(BatchDev b, uint64_t total_
     }
     for (int k = tid; k < prof.planes; k += 256)
         pinv[k] = (float)ddiv(1.0, hypothesis_depth(k, prof.planes, ref.search_min, ref.search_max));
+    // slot of tap dx of the window that starts at column 0 (add the window's start)
+    int toff[W];
+#pragma unroll
+    for (int dx = 0; dx < W; ++dx) toff[dx] = (dx % s) * PXs + dx / s;
     __syncthreads();
 
     const int tx = tid & 31, ty = tid >> 5;
@@ -295,8 +334,9 @@ __global__ void __launch_bounds__(256) k_sweep_tiled(BatchDev b, uint64_t total_
     if (active) {
         float mn = 3.0e38f, mx = -3.0e38f;
         for (int dy = 0; dy < W; ++dy)
+#pragma unroll
             for (int dx = 0; dx < W; ++dx) {
-                float v = refv[(ty * s + dy) * PX + tx * s + dx];
+                float v = refv[(ty * s + dy) * PXp + toff[dx] + tx];
                 mn = fminf(mn, v);
                 mx = fmaxf(mx, v);
                 sr += (double)v;
@@ -325,39 +365,40 @@ __global__ void __launch_bounds__(256) k_sweep_tiled(BatchDev b, uint64_t total_
             const DevImage si = ref.src[j].img;
             const T* sdata = static_cast<const T*>(si.data);
             const float wl = (float)(si.width - 1), hl = (float)(si.height - 1);
-            // warp rows, lanes columns: no index division, the homography
-            // folded per row, the reciprocal from the approximate unit
-            for (int yy = ty; yy < PY; yy += kTileY) {
-                const float Y = (float)(py0 + yy);
+            // warps over rows, lanes over column slots; the homography folded
+            // per row, the reciprocal from the approximate unit
+            float Y = (float)(py0 + ty);
+            for (int yy = ty; yy < PY; yy += kTileY, Y += (float)kTileY) {
                 const float hx = fmaf(A[1], Y, H2), hy = fmaf(A[4], Y, H5), hz = fmaf(A[7], Y, H8);
-                float* row = samp + yy * PX;
-                for (int xx = tx; xx < PX; xx += kTileX) {
-                    const float X = (float)(px0 + xx);
+                float* row = samp + yy * PXp;
+                for (int t = tx; t < PXp; t += kTileX) {
+                    const float X = colx[t];
                     const float h2 = fmaf(A[6], X, hz);
                     float v = __int_as_float(0x7fc00000);
-                    if (h2 > zmin) {
+                    if (h2 > zmin) {  // false for padding slots (X is NaN)
                         const float iv = __fdividef(1.0f, h2);
                         const float u = fmaf(A[0], X, hx) * iv;
                         const float q = fmaf(A[3], X, hy) * iv;
                         if (u >= 0.f && q >= 0.f && u < wl && q < hl)
-                            v = sample_fast<T>(sdata, si.width, u, q);
+                            v = sample_nonneg<T>(sdata, si.width, u, q);
                     }
-                    row[xx] = v;
+                    row[t] = v;
                 }
             }
             __syncthreads();
-            for (int i = tid; i < PY * kTileX; i += 256) {
-                int row = i >> 5, col = i & 31;
-                const float* sp = samp + row * PX + col * s;
-                const float* rp = refv + row * PX + col * s;
+            // horizontal box filter, one row per warp, the window of lane c at slot c
+            for (int yy = ty; yy < PY; yy += kTileY) {
+                const float* sp = samp + yy * PXp + tx;
+                const float* rp = refv + yy * PXp + tx;
                 double a = 0.0, bb = 0.0, c = 0.0;
 #pragma unroll
                 for (int dx = 0; dx < W; ++dx) {
-                    double v = (double)sp[dx];
+                    const double v = (double)sp[toff[dx]];
                     a += v;
                     bb = fma(v, v, bb);
-                    c = fma((double)rp[dx], v, c);
+                    c = fma((double)rp[toff[dx]], v, c);
                 }
+                const int i = yy * kTileX + tx;
                 hs[i] = a;
                 hss[i] = bb;
                 hrs[i] = c;
@@ -367,7 +408,7 @@ __global__ void __launch_bounds__(256) k_sweep_tiled(BatchDev b, uint64_t total_
                 double a = 0.0, bb = 0.0, c = 0.0;
 #pragma unroll
                 for (int dy = 0; dy < W; ++dy) {
-                    int i = (ty * s + dy) * kTileX + tx;
+                    const int i = (ty * s + dy) * kTileX + tx;
                     a += hs[i];
                     bb += hss[i];
                     c += hrs[i];
@@ -382,17 +423,27 @@ __global__ void __launch_bounds__(256) k_sweep_tiled(BatchDev b, uint64_t total_
             }
         }
         if (sampled) {
-            double errs[kMaxSources];
+            // the passing source costs, compacted and sorted in this thread's column
+            float* col = costs + tid;
             int cnt = 0;
             for (int j = 0; j < n_src; ++j) {
-                float c = costs[j * 256 + tid];
-                if ((double)c <= prof.max_error) errs[cnt++] = c;
+                const float c = col[j * 256];
+                if ((double)c <= prof.max_error) col[(cnt++) * 256] = c;
             }
             if (cnt > 0) {
+                for (int i = 1; i < cnt; ++i) {
+                    const float x = col[i * 256];
+                    int m = i - 1;
+                    while (m >= 0 && col[m * 256] > x) {
+                        col[(m + 1) * 256] = col[m * 256];
+                        --m;
+                    }
+                    col[(m + 1) * 256] = x;
+                }
                 Rank c;
                 c.support = cnt;
                 c.plane = k;
-                c.error = median_of(errs, cnt);
+                c.error = (double)col[(cnt / 2) * 256];
                 c.second = kInf;
                 st = rank_merge(st, c);
             }
@@ -414,7 +465,6 @@ __global__ void __launch_bounds__(256) k_sweep_tiled(BatchDev b, uint64_t total_
     rank[gsite] = out;
     status[gsite] = code;
 }
-
 
 // ---- reciprocal check, warp per (candidate, source) ----------------------------
 // reciprocal_depth_observations (dense_legacy.rs:777-857) for one source:
@@ -534,26 +584,6 @@ __device__ __forceinline__ float warp_sum(float v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
-}
-
-// Bilinear sample at a non-negative coordinate below 2^22 (the caller checks
-// the domain).  floor() is one round-down add of 2^23, which leaves floor(u)
-// in the low mantissa bits: the same floor, integer and fraction as floorf.
-template <class T>
-__device__ __forceinline__ float sample_nonneg(const T* __restrict__ p, uint32_t w, float u,
-                                               float v) {
-    constexpr float kShift = 8388608.0f;  // 2^23
-    const float tu = __fadd_rd(u, kShift), tv = __fadd_rd(v, kShift);
-    const float fu = tu - kShift, fv = tv - kShift;
-    const uint32_t ix = (uint32_t)(__float_as_int(tu) - __float_as_int(kShift));
-    const uint32_t iy = (uint32_t)(__float_as_int(tv) - __float_as_int(kShift));
-    const float tx = u - fu, ty = v - fv;
-    const size_t r0 = (size_t)iy * w + ix;
-    const float v00 = pix<T>(p, r0), v10 = pix<T>(p, r0 + 1);
-    const float v01 = pix<T>(p, r0 + w), v11 = pix<T>(p, r0 + w + 1);
-    const float top = fmaf(v10 - v00, tx, v00);
-    const float bot = fmaf(v11 - v01, tx, v01);
-    return fmaf(bot - top, ty, top);
 }
 
 // True when every tap (x + dx, y + dy), |dx|, |dy| <= R, maps through H to a
@@ -1049,10 +1079,12 @@ cudaError_t Typed<T>::sweep_tiled(const BatchDev& b, uint32_t max_nx, uint32_t m
                                   RefCounters* ctr, cudaStream_t st) {
     using namespace typed_detail;
     auto run = [&](auto kern, int W) -> cudaError_t {
-        const int PX = (kTileX - 1) * (int)stride + W, PY = (kTileY - 1) * (int)stride + W;
+        const int s = (int)stride;
+        const int PX = (kTileX - 1) * s + W, PY = (kTileY - 1) * s + W;
+        const size_t PXp = (size_t)((PX + s - 1) / s) * s, np = PXp * PY;
         const size_t smem = sizeof(double) * 3 * (size_t)PY * kTileX +
-                            sizeof(float) * (2 * (size_t)PX * PY + kMaxSources * 256 +
-                                             kMaxSources * 12 + kMaxPlanes);
+                            sizeof(float) * (2 * np + PXp + (size_t)b.max_src * (256 + 12) +
+                                             (size_t)b.prof.planes);
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);
         if (e != cudaSuccess) return e;
