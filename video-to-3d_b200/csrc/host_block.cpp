@@ -4,9 +4,10 @@
 // device straight into one page-locked block, and every per-reference result
 // of the batch points into it.  The block is reference counted (one count per
 // PassResult copy, per C result and per mesh result); when the last holder
-// lets go it returns to a small process-wide cache instead of being unpinned,
-// so a caller that drops the previous call's results before the next call
-// reuses the same two blocks without page faults or cudaHostAlloc.
+// lets go it returns to a small process-wide cache instead of being unpinned.
+// A fresh block is pinned together with a spare of its size, so a caller that
+// keeps one call's results while it makes the next alternates between two
+// blocks and never pins (or page-faults) again.
 #include <cuda_runtime.h>
 
 #include <map>
@@ -77,6 +78,14 @@ HostBlock host_block(size_t bytes) {
             return HostBlock();
         }
         have = bytes;
+        // Pin a spare of the same size as well: a caller that keeps one call's
+        // results while it makes the next needs two blocks, and pinning (which
+        // can stall the other CUDA calls of the process) then happens once.
+        void* spare = nullptr;
+        if (cudaHostAlloc(&spare, bytes, cudaHostAllocPortable) == cudaSuccess)
+            recycle(spare, bytes);
+        else
+            cudaGetLastError();
     }
     return HostBlock(static_cast<uint8_t*>(p), BlockRecycler{have});
 }
