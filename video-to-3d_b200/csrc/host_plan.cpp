@@ -18,15 +18,15 @@ namespace v3d {
 namespace {
 constexpr size_t kMinVisibleSparsePoints = 8;  // dense_legacy.rs:8
 
-double quantile_sorted(const std::vector<double>& v, double q) {
-    // dense_legacy.rs:1168-1174
+// quantile (dense_legacy.rs:1168-1174) of the sorted values: the element of
+// rank round((n - 1) q).  The depths are finite, so that order statistic is
+// selected in place instead of sorting (any permutation of v is left behind).
+double quantile_of(std::vector<double>& v, double q) {
     if (v.empty()) return std::nan("");
     double c = q < 0.0 ? 0.0 : (q > 1.0 ? 1.0 : q);
-    return v[static_cast<size_t>(std::round(static_cast<double>(v.size() - 1) * c))];
-}
-
-void sort_depths(std::vector<double>& v) {
-    std::stable_sort(v.begin(), v.end(), [](double a, double b) { return a < b; });
+    const size_t k = static_cast<size_t>(std::round(static_cast<double>(v.size() - 1) * c));
+    std::nth_element(v.begin(), v.begin() + k, v.end());
+    return v[k];
 }
 
 std::vector<double> visible_depths(const HCamera& c, const std::vector<HVec3>& sparse, uint32_t w,
@@ -41,12 +41,11 @@ std::vector<double> visible_depths(const HCamera& c, const std::vector<HVec3>& s
 }
 
 bool envelope(std::vector<double>& depths, double& mn, double& mx, double* median) {
-    sort_depths(depths);
-    double lower = quantile_sorted(depths, 0.10), upper = quantile_sorted(depths, 0.90);
+    double lower = quantile_of(depths, 0.10), upper = quantile_of(depths, 0.90);
     if (!std::isfinite(lower) || !std::isfinite(upper) || lower <= 0.0 || upper <= 0.0) return false;
     mn = std::fmax(lower * 0.8, 1.0e-4);
     mx = std::fmax(upper * 1.25, mn * 1.2);
-    if (median) *median = quantile_sorted(depths, 0.50);
+    if (median) *median = quantile_of(depths, 0.50);
     return true;
 }
 
