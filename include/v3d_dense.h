@@ -377,6 +377,38 @@ int32_t v3d_reconstruct_reference_patches_meshed(
     v3d_cancel_fn cancel, void* cancel_user,
     v3d_dense_result* out, v3d_mesh_result* mesh_out, int32_t* present);
 
+/* One clip of v3d_reconstruct_clips: its frames, cameras, landmarks and focal
+ * length, the cameras to reconstruct as references, and its own hypothesis
+ * count and source-view limit (0 takes the profile's). */
+typedef struct v3d_clip {
+    const v3d_frame* frames;
+    uint64_t n_frames;
+    const v3d_camera* cameras;
+    uint64_t n_cameras;
+    const double* sparse_xyz;
+    uint64_t n_sparse;
+    double focal;
+    const uint64_t* camera_indices;
+    uint64_t n_references;
+    int32_t depth_hypotheses;
+    int32_t max_source_views;
+} v3d_clip;
+
+/* reconstruct_reference_patch (dense.rs:674-747) for the references of many
+ * clips of uneven size, as one device batch: every kernel runs once over the
+ * references of all clips.  The reference has no multi-clip call; per clip
+ * the results equal v3d_reconstruct_reference_patches(_meshed) with that
+ * clip's inputs and profile.  out, present and (when not NULL) mesh_out hold
+ * the references clip by clip, in each clip's camera_indices order.  All
+ * frames of a call share one pixel format; the profile's cost, window,
+ * stride, precision and gates apply to every clip. */
+int32_t v3d_reconstruct_clips(
+    v3d_context* ctx,
+    const v3d_clip* clips, uint64_t n_clips,
+    int32_t fine_grid, const v3d_profile* profile,
+    v3d_cancel_fn cancel, void* cancel_user,
+    v3d_dense_result* out, v3d_mesh_result* mesh_out, int32_t* present);
+
 /* estimate_depth_points_limited (dense.rs:250-330): the multi-reference plan
  * (at most 6 attempts, `reference_views` accepted patches), the legacy
  * fallback, attempt merging and patch concatenation.  `omitted_references`

@@ -412,40 +412,43 @@ void fill_mesh(v3d_mesh_result* out, const MeshOut& m) {
     }
 }
 
-int32_t reference_patches(v3d_context* ctx, const v3d_frame* frames, uint64_t n_frames,
-                          const v3d_camera* cameras, uint64_t n_cameras, const double* sparse_xyz,
-                          uint64_t n_sparse, double focal, int32_t fine_grid,
-                          const v3d_profile* profile, const uint64_t* camera_indices,
-                          uint64_t n_refs, v3d_cancel_fn cancel, void* cancel_user,
-                          v3d_dense_result* out, v3d_mesh_result* mesh_out, int32_t* present) {
-    if (!out || !present || (n_refs && !camera_indices)) return V3D_ERR_INVALID_ARGUMENT;
-    for (uint64_t i = 0; i < n_refs; ++i) {
-        std::memset(&out[i], 0, sizeof(out[i]));
-        if (mesh_out) std::memset(&mesh_out[i], 0, sizeof(mesh_out[i]));
-        present[i] = 0;
-    }
-    if (!ensure_device(ctx)) return V3D_ERR_NO_DEVICE;
-    if (!valid_profile(profile) || !valid_frames(frames, n_frames) ||
-        (n_cameras && !cameras) || (n_sparse && !sparse_xyz))
-        return V3D_ERR_INVALID_ARGUMENT;
+// One clip of a device batch: its inputs, its profile and the cameras to use
+// as references.  Frame slots of its plans are local to the clip until the
+// batch concatenates the clips' frames.
+struct ClipJob {
+    Inputs in;
+    v3d_profile prof{};
+    const uint64_t* camera_indices = nullptr;
+    uint64_t n_refs = 0;
+};
+
+// dense.rs:674-747 for every (clip, reference camera) of `jobs`, run as one
+// device batch; out, mesh_out and present hold the references clip by clip.
+int32_t clip_batch(v3d_context* ctx, const std::vector<ClipJob>& jobs, int32_t fine_grid,
+                   const v3d_profile& batch_prof, v3d_cancel_fn cancel, void* cancel_user,
+                   v3d_dense_result* out, v3d_mesh_result* mesh_out, int32_t* present) {
     std::lock_guard<std::mutex> lock(ctx->mu);
     cudaSetDevice(ctx->device);
     const auto t_plan = std::chrono::steady_clock::now();
-    Inputs in = load_inputs(frames, n_frames, cameras, n_cameras, sparse_xyz, n_sparse, focal);
+    std::vector<size_t> job_of, first_of(jobs.size() + 1, 0), frame_base(jobs.size() + 1, 0);
+    for (size_t j = 0; j < jobs.size(); ++j) {
+        first_of[j + 1] = first_of[j] + jobs[j].n_refs;
+        frame_base[j + 1] = frame_base[j] + jobs[j].in.n_frames;
+        for (uint64_t i = 0; i < jobs[j].n_refs; ++i) job_of.push_back(j);
+    }
+    const size_t n_refs = first_of.back();
     std::vector<RefPlan> plans(n_refs);
-    std::vector<bool> pres(n_refs);
-    CancelPoll cp{cancel, cancel_user};
-    std::vector<uint8_t> canceled(n_refs, 0);
-    std::vector<uint8_t> pres8(n_refs, 0);
+    std::vector<uint8_t> pres8(n_refs, 0), canceled(n_refs, 0);
     parallel_for(n_refs, [&](size_t i) {
+        const ClipJob& J = jobs[job_of[i]];
         bool p = false;
-        plans[i] = plan_reference_patch(*profile, in, camera_indices[i], fine_grid != 0, p);
+        plans[i] = plan_reference_patch(J.prof, J.in, J.camera_indices[i - first_of[job_of[i]]],
+                                        fine_grid != 0, p);
         pres8[i] = p;
     });
-    for (uint64_t i = 0; i < n_refs; ++i) {
-        const bool p = pres8[i] != 0;
-        pres[i] = p;
-        if (!p) {
+    CancelPoll cp{cancel, cancel_user};
+    for (size_t i = 0; i < n_refs; ++i) {
+        if (!pres8[i]) {
             plans[i].skipped = true;
             continue;
         }
@@ -457,18 +460,30 @@ int32_t reference_patches(v3d_context* ctx, const v3d_frame* frames, uint64_t n_
             canceled[i] = 1;
             plans[i].skipped = true;
         }
+        // frame slots into the batch's concatenated frame list
+        const size_t fb = frame_base[job_of[i]];
+        plans[i].ref_slot += fb;
+        for (size_t& s : plans[i].src_slots) s += fb;
+    }
+    const v3d_frame* frames = jobs.empty() ? nullptr : jobs[0].in.frames;
+    std::vector<v3d_frame> all_frames;
+    if (jobs.size() > 1) {
+        all_frames.reserve(frame_base.back());
+        for (const ClipJob& J : jobs) all_frames.insert(all_frames.end(), J.in.frames, J.in.frames + J.in.n_frames);
+        frames = all_frames.data();
     }
     const double plan_ms = std::chrono::duration<double, std::milli>(
                                std::chrono::steady_clock::now() - t_plan).count();
     std::vector<PassResult> res;
     std::vector<MeshOut> meshes;
-    int32_t st = run_batch(ctx, *profile, frames, n_frames, focal, plans, res,
+    const double focal = jobs.empty() ? 0.0 : jobs[0].in.focal;  // each plan carries its own
+    int32_t st = run_batch(ctx, batch_prof, frames, frame_base.back(), focal, plans, res,
                            mesh_out ? &meshes : nullptr);
     ctx->last_plan_ms = plan_ms;
     if (st < 0) return st;
     if (mesh_out && meshes.size() != n_refs) {
         meshes.assign(n_refs, MeshOut{});
-        for (uint64_t i = 0; i < n_refs; ++i) {
+        for (size_t i = 0; i < n_refs; ++i) {
             v3d_mesh_stats& s = meshes[i].stats;
             s.has_reference_frame = plans[i].have_reference;
             s.reference_frame = plans[i].reference_frame;
@@ -477,13 +492,15 @@ int32_t reference_patches(v3d_context* ctx, const v3d_frame* frames, uint64_t n_
                          V3D_SKIP_REASON_BYTES - 1);
         }
     }
-    for (uint64_t i = 0; i < n_refs; ++i) {
-        present[i] = pres[i] ? 1 : 0;
-        if (!pres[i]) continue;
+    for (size_t i = 0; i < n_refs; ++i) {
+        present[i] = pres8[i] ? 1 : 0;
+        if (!pres8[i]) continue;
         if (canceled[i]) canceled_result(res[i]);
+        const ClipJob& J = jobs[job_of[i]];
         // dense.rs:734: the patch reports its reference frame even when skipped
         res[i].stats.has_reference_frame = 1;
-        res[i].stats.reference_frame = in.cameras[camera_indices[i]].frame_index;
+        res[i].stats.reference_frame =
+            J.in.cameras[J.camera_indices[i - first_of[job_of[i]]]].frame_index;
         fill_pass(&out[i], res[i]);
         if (mesh_out) {
             if (canceled[i] || !res[i].stats.attempted) {
@@ -503,9 +520,69 @@ int32_t reference_patches(v3d_context* ctx, const v3d_frame* frames, uint64_t n_
     return V3D_OK;
 }
 
+void clear_outputs(uint64_t n, v3d_dense_result* out, v3d_mesh_result* mesh_out, int32_t* present) {
+    for (uint64_t i = 0; i < n; ++i) {
+        std::memset(&out[i], 0, sizeof(out[i]));
+        if (mesh_out) std::memset(&mesh_out[i], 0, sizeof(mesh_out[i]));
+        present[i] = 0;
+    }
+}
+
+int32_t reference_patches(v3d_context* ctx, const v3d_frame* frames, uint64_t n_frames,
+                          const v3d_camera* cameras, uint64_t n_cameras, const double* sparse_xyz,
+                          uint64_t n_sparse, double focal, int32_t fine_grid,
+                          const v3d_profile* profile, const uint64_t* camera_indices,
+                          uint64_t n_refs, v3d_cancel_fn cancel, void* cancel_user,
+                          v3d_dense_result* out, v3d_mesh_result* mesh_out, int32_t* present) {
+    if (!out || !present || (n_refs && !camera_indices)) return V3D_ERR_INVALID_ARGUMENT;
+    clear_outputs(n_refs, out, mesh_out, present);
+    if (!ensure_device(ctx)) return V3D_ERR_NO_DEVICE;
+    if (!valid_profile(profile) || !valid_frames(frames, n_frames) ||
+        (n_cameras && !cameras) || (n_sparse && !sparse_xyz))
+        return V3D_ERR_INVALID_ARGUMENT;
+    std::vector<ClipJob> jobs(1);
+    jobs[0].in = load_inputs(frames, n_frames, cameras, n_cameras, sparse_xyz, n_sparse, focal);
+    jobs[0].prof = *profile;
+    jobs[0].camera_indices = camera_indices;
+    jobs[0].n_refs = n_refs;
+    return clip_batch(ctx, jobs, fine_grid, *profile, cancel, cancel_user, out, mesh_out, present);
+}
+
 }  // namespace
 
 extern "C" {
+
+int32_t v3d_reconstruct_clips(v3d_context* ctx, const v3d_clip* clips, uint64_t n_clips,
+                              int32_t fine_grid, const v3d_profile* profile, v3d_cancel_fn cancel,
+                              void* cancel_user, v3d_dense_result* out,
+                              v3d_mesh_result* mesh_out, int32_t* present) {
+    if (!out || !present || (n_clips && !clips)) return V3D_ERR_INVALID_ARGUMENT;
+    uint64_t n_refs = 0;
+    for (uint64_t c = 0; c < n_clips; ++c) {
+        if (clips[c].n_references && !clips[c].camera_indices) return V3D_ERR_INVALID_ARGUMENT;
+        n_refs += clips[c].n_references;
+    }
+    clear_outputs(n_refs, out, mesh_out, present);
+    if (!ensure_device(ctx)) return V3D_ERR_NO_DEVICE;
+    if (!valid_profile(profile)) return V3D_ERR_INVALID_ARGUMENT;
+    std::vector<ClipJob> jobs(n_clips);
+    for (uint64_t c = 0; c < n_clips; ++c) {
+        const v3d_clip& k = clips[c];
+        if (!valid_frames(k.frames, k.n_frames) || (k.n_cameras && !k.cameras) ||
+            (k.n_sparse && !k.sparse_xyz))
+            return V3D_ERR_INVALID_ARGUMENT;
+        ClipJob& J = jobs[c];
+        J.prof = *profile;
+        if (k.depth_hypotheses > 0) J.prof.depth_hypotheses = k.depth_hypotheses;
+        if (k.max_source_views > 0) J.prof.max_source_views = k.max_source_views;
+        if (!valid_profile(&J.prof)) return V3D_ERR_INVALID_ARGUMENT;
+        J.in = load_inputs(k.frames, k.n_frames, k.cameras, k.n_cameras, k.sparse_xyz, k.n_sparse,
+                           k.focal);
+        J.camera_indices = k.camera_indices;
+        J.n_refs = k.n_references;
+    }
+    return clip_batch(ctx, jobs, fine_grid, *profile, cancel, cancel_user, out, mesh_out, present);
+}
 
 int32_t v3d_reconstruct_reference_patches(v3d_context* ctx, const v3d_frame* frames,
                                           uint64_t n_frames, const v3d_camera* cameras,

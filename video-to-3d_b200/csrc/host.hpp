@@ -38,6 +38,8 @@ struct RefPlan {
     std::vector<double> src_min, src_max;
     double search_min = 0, search_max = 0;
     uint32_t width = 0, height = 0, stride = 0, border = 0, nx = 0, ny = 0;
+    int planes = 0;    // depth hypotheses (the profile's, per clip in a multi-clip batch)
+    double focal = 0;  // the clip's focal length
 };
 
 // Page-locked host memory shared by the results of one batch

@@ -236,6 +236,8 @@ RefPlan plan_legacy(const v3d_profile& prof, const v3d_frame* frames, size_t n_f
     p.stride = prof.grid_stride > 0 ? static_cast<uint32_t>(prof.grid_stride)
                                     : reference_grid_stride(width, height, fine_grid);
     p.border = static_cast<uint32_t>(r + 2);
+    p.planes = prof.depth_hypotheses;
+    p.focal = focal;
     p.nx = width > 2 * p.border ? (width - 2 * p.border + p.stride - 1) / p.stride : 0;
     p.ny = height > 2 * p.border ? (height - 2 * p.border + p.stride - 1) / p.stride : 0;
     return p;

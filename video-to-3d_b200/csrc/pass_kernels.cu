@@ -134,7 +134,7 @@ __global__ void k_make_primary_cands(BatchDev b, const uint32_t* __restrict__ si
         c.site = local;
         c.x = x;
         c.y = y;
-        c.depth = hypothesis_depth(sr.plane, b.prof.planes, ref.search_min, ref.search_max);
+        c.depth = hypothesis_depth(sr.plane, ref.planes, ref.search_min, ref.search_max);
         c.pos = unproject_exact(ref.cam, (double)x, (double)y, c.depth, ref.img.width,
                                 ref.img.height, ref.focal);
         c.error = sr.error;

@@ -234,7 +234,11 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
         luma_off[u] = rgba ? cv.take<uint8_t>(px) : raw_off[u];
     }
     const size_t o_refs = cv.take<DevReference>(n_active);
-    const size_t inv_count = n_active * kMaxSources * static_cast<size_t>(prof.depth_hypotheses);
+    // per reference a [kMaxSources][planes] table of source inverse depths
+    std::vector<uint64_t> inv_off(n_active + 1, 0);
+    for (size_t k = 0; k < n_active; ++k)
+        inv_off[k + 1] = inv_off[k] + kMaxSources * static_cast<uint64_t>(plans[active[k]].planes);
+    const size_t inv_count = inv_off[n_active];
     const size_t o_srcinv = cv.take<float>(inv_count);
     const size_t o_siteoff = cv.take<uint64_t>(n_active + 1);
     const size_t o_siteref = cv.take<uint32_t>(cap);
@@ -307,7 +311,9 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
         size_t ru = static_cast<size_t>(dev_of[p.ref_slot]);
         d.img = DevImage{at(luma_off[ru]), frames[p.ref_slot].width, frames[p.ref_slot].height};
         d.rgba = rgba ? reinterpret_cast<const uint8_t*>(at(raw_off[ru])) : nullptr;
-        d.focal = focal;
+        d.focal = p.focal;
+        d.planes = p.planes;
+        d.inv_off = inv_off[k];
         d.search_min = p.search_min;
         d.search_max = p.search_max;
         d.border = p.border;
@@ -324,9 +330,9 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
             s.search_min = p.src_min[j];
             s.search_max = p.src_max[j];
             homography_parts(p.ref_cam, d.img.width, d.img.height, p.src_cams[j], sf.width,
-                             sf.height, focal, s.fwd_A, s.fwd_b);
+                             sf.height, p.focal, s.fwd_A, s.fwd_b);
             homography_parts(p.src_cams[j], sf.width, sf.height, p.ref_cam, d.img.width,
-                             d.img.height, focal, s.bwd_A, s.bwd_b);
+                             d.img.height, p.focal, s.bwd_A, s.bwd_b);
         }
     }
     uint64_t* hoff = reinterpret_cast<uint64_t*>(hrefs + n_active);
@@ -335,15 +341,15 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
     // (dense_legacy.rs:286-293, 908-916) rounded once to f32
     float* hinv = reinterpret_cast<float*>(hoff + n_active + 1);
     std::memset(hinv, 0, sizeof(float) * inv_count);
-    const int n_hyp = prof.depth_hypotheses;
     for (size_t k = 0; k < n_active; ++k) {
         const RefPlan& pl = plans[active[k]];
+        const int n_hyp = pl.planes;
         for (size_t j = 0; j < pl.src_slots.size(); ++j)
             for (int q = 0; q < n_hyp; ++q) {
                 double t = n_hyp == 1 ? 0.0 : static_cast<double>(q) / static_cast<double>(n_hyp - 1);
                 double inv = (1.0 / pl.src_min[j]) * (1.0 - t) + (1.0 / pl.src_max[j]) * t;
                 double depth = 1.0 / inv;
-                hinv[(k * kMaxSources + j) * n_hyp + q] = static_cast<float>(1.0 / depth);
+                hinv[inv_off[k] + j * n_hyp + q] = static_cast<float>(1.0 / depth);
             }
     }
     V3D_CK(cudaMemcpyAsync(at(o_refs), hrefs, sizeof(DevReference) * n_active,
@@ -399,7 +405,8 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
     b.storage = storage;
     b.prof.cost = prof.cost;
     b.prof.radius = prof.patch_radius;
-    b.prof.planes = prof.depth_hypotheses;
+    b.prof.planes = 1;
+    for (size_t k = 0; k < n_active; ++k) b.prof.planes = std::max(b.prof.planes, plans[active[k]].planes);
     b.prof.pad = 0;
     b.prof.min_contrast = prof.min_reference_contrast;
     b.prof.max_error = prof.max_photometric_error;
@@ -558,7 +565,7 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
     ctx->last_units = 0;
     for (size_t k = 0; k < n_active; ++k) {
         const RefPlan& pl = plans[active[k]];
-        ctx->last_units += static_cast<uint64_t>(pl.nx) * pl.ny * prof.depth_hypotheses *
+        ctx->last_units += static_cast<uint64_t>(pl.nx) * pl.ny * pl.planes *
                            pl.src_slots.size();
     }
 
@@ -638,7 +645,7 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
             MeshPatchDev& m = mp[k];
             std::memset(&m, 0, sizeof(m));
             set_cam(m.cam, pl.ref_cam);
-            m.focal = focal;
+            m.focal = pl.focal;
             m.width = frames[pl.ref_slot].width;
             m.height = frames[pl.ref_slot].height;
             m.border = pl.border;
@@ -846,7 +853,7 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
         s.reference_frame = p.reference_frame;
         s.source_views = p.src_slots.size();
         s.sampled_pixels = c.sampled;
-        s.depth_hypotheses = static_cast<uint64_t>(prof.depth_hypotheses);
+        s.depth_hypotheses = static_cast<uint64_t>(p.planes);
         s.accepted_points = n;
         s.surface_completion_proposals = c.proposals;
         s.surface_completed_points = c.completed;

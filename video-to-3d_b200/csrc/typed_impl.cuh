@@ -204,8 +204,8 @@ __global__ void __launch_bounds__(256) k_sweep_site(BatchDev b, const uint32_t* 
     }
     Rank st = rank_empty();
     const int n_src = ref.n_src;
-    for (int k = lane; k < prof.planes; k += 32) {
-        const double depth = hypothesis_depth(k, prof.planes, ref.search_min, ref.search_max);
+    for (int k = lane; k < ref.planes; k += 32) {
+        const double depth = hypothesis_depth(k, ref.planes, ref.search_min, ref.search_max);
         const double inv = ddiv(1.0, depth);
         double errs[kMaxSources];
         int n = 0;
@@ -316,8 +316,8 @@ __global__ void __launch_bounds__(256) k_sweep_tiled(BatchDev b, uint64_t total_
         int j = i / 12, c = i - j * 12;
         hA[i] = c < 9 ? ref.src[j].fwd_A[c] : ref.src[j].fwd_b[c - 9];
     }
-    for (int k = tid; k < prof.planes; k += 256)
-        pinv[k] = (float)ddiv(1.0, hypothesis_depth(k, prof.planes, ref.search_min, ref.search_max));
+    for (int k = tid; k < ref.planes; k += 256)
+        pinv[k] = (float)ddiv(1.0, hypothesis_depth(k, ref.planes, ref.search_min, ref.search_max));
     // slot of tap dx of the window that starts at column 0 (add the window's start)
     int toff[W];
 #pragma unroll
@@ -354,7 +354,7 @@ __global__ void __launch_bounds__(256) k_sweep_tiled(BatchDev b, uint64_t total_
     const bool vr_ok = vr > 0.0 && vr >= minvar_n;
     const float vr_f = (float)vr;
     Rank st = rank_empty();
-    for (int k = 0; k < prof.planes; ++k) {
+    for (int k = 0; k < ref.planes; ++k) {
         const float inv = pinv[k];
         const float zmin = 1.0e-4f * inv;
         for (int j = 0; j < n_src; ++j) {
@@ -515,9 +515,9 @@ __global__ void __launch_bounds__(256) k_reciprocal_exact(BatchDev b, const Cand
         if (ok) {
             double be = kInf;
             int bk = 0x7fffffff;
-            if (ok && lane == 0) atomicAdd(&ctr[cd.ref].recip_evals, (unsigned long long)prof.planes);
-            for (int k = lane; ok && k < prof.planes; k += 32) {
-                double d = hypothesis_depth(k, prof.planes, src.search_min, src.search_max);
+            if (ok && lane == 0) atomicAdd(&ctr[cd.ref].recip_evals, (unsigned long long)ref.planes);
+            for (int k = lane; ok && k < ref.planes; k += 32) {
+                double d = hypothesis_depth(k, ref.planes, src.search_min, src.search_max);
                 double e;
                 const bool eok = patch_error_exact<T>(prof, src.cam, src.img, ref.cam, ref.img,
                                                       ref.focal, sp.x, sp.y, d, e);
@@ -539,7 +539,7 @@ __global__ void __launch_bounds__(256) k_reciprocal_exact(BatchDev b, const Cand
             if (bk == 0x7fffffff) {
                 ok = false;
             } else {
-                double rd = hypothesis_depth(bk, prof.planes, src.search_min, src.search_max);
+                double rd = hypothesis_depth(bk, ref.planes, src.search_min, src.search_max);
                 // reciprocal_depth_agrees (dense_legacy.rs:951-957)
                 double ex = sp.z;
                 bool agree = isfinite(ex) && isfinite(rd) && ex > 0.0 && rd > 0.0;
@@ -816,7 +816,7 @@ __global__ void __launch_bounds__(256) k_recip_prepare(BatchDev b, const Cand* _
         if (ok) {
             res.pos = sp;
             res.valid = kObsPending;
-            if (lane == 0) atomicAdd(&ctr[cd.ref].recip_evals, (unsigned long long)prof.planes);
+            if (lane == 0) atomicAdd(&ctr[cd.ref].recip_evals, (unsigned long long)ref.planes);
         }
         if (lane == 0 && si < ref.n_src) obs[it] = res;
     }
@@ -870,7 +870,7 @@ __global__ void __launch_bounds__(256, 3) k_recip_sweep(BatchDev b, const Cand* 
         }
         const float pvar = warp_sum(dsq);
         __syncwarp();
-        const float* inv_tab = b.src_inv + ((size_t)r * kMaxSources + si) * prof.planes;
+        const float* inv_tab = b.src_inv + ref.inv_off + (size_t)si * ref.planes;
         const T* rimg = static_cast<const T*>(ref.img.data);
         const uint32_t rw = ref.img.width;
         const float wl = (float)(ref.img.width - 1), hl = (float)(ref.img.height - 1);
@@ -878,7 +878,7 @@ __global__ void __launch_bounds__(256, 3) k_recip_sweep(BatchDev b, const Cand* 
         const float minvar = (float)prof.min_variance;
         float be = 3.0e38f;
         int bk = 0x7fffffff;
-        for (int k = lane; k < prof.planes; k += 32) {
+        for (int k = lane; k < ref.planes; k += 32) {
             const float inv = inv_tab[k];
             float H[9];
             plane_h(src.bwd_A, src.bwd_b, inv, H);
@@ -910,7 +910,7 @@ __global__ void __launch_bounds__(256, 3) k_recip_sweep(BatchDev b, const Cand* 
             res.pad = 0;
             res.pos = D3{0, 0, 0};
             if (bk != 0x7fffffff) {
-                const double rd = hypothesis_depth(bk, prof.planes, src.search_min, src.search_max);
+                const double rd = hypothesis_depth(bk, ref.planes, src.search_min, src.search_max);
                 const double ex = sp.z;
                 // reciprocal_depth_agrees (dense_legacy.rs:951-957)
                 bool agree = isfinite(ex) && isfinite(rd) && ex > 0.0 && rd > 0.0;

@@ -62,14 +62,15 @@ struct DevReference {
     double search_min, search_max;
     uint32_t border, stride, nx, ny;
     int32_t n_src;
-    int32_t pad;
+    int32_t planes;    // depth hypotheses of this reference (and of its sources' sweeps)
+    uint64_t inv_off;  // first entry of its [kMaxSources][planes] table in BatchDev::src_inv
     DevSource src[kMaxSources];
 };
 
 struct DevProfile {
     int32_t cost;    // 0 ZSAD, 1 ZNCC
     int32_t radius;
-    int32_t planes;
+    int32_t planes;  // the most depth hypotheses of any reference in the batch
     int32_t pad;
     double min_contrast, max_error, min_margin, margin_saturation, error_scale, min_variance;
 };

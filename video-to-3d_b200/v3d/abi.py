@@ -198,6 +198,15 @@ class RunInfo(C.Structure):
 
 CANCEL_FN = C.CFUNCTYPE(C.c_int32, C.c_void_p)
 
+class Clip(C.Structure):
+    _fields_ = [("frames", C.POINTER(Frame)), ("n_frames", C.c_uint64),
+                ("cameras", C.POINTER(Camera)), ("n_cameras", C.c_uint64),
+                ("sparse_xyz", C.POINTER(C.c_double)), ("n_sparse", C.c_uint64),
+                ("focal", C.c_double), ("camera_indices", C.POINTER(C.c_uint64)),
+                ("n_references", C.c_uint64), ("depth_hypotheses", C.c_int32),
+                ("max_source_views", C.c_int32)]
+
+
 STRUCTS = {
     "v3d_frame": Frame, "v3d_camera": Camera, "v3d_profile": Profile, "v3d_point": Point,
     "v3d_grid_site": GridSite, "v3d_point_attributes": PointAttributes,
@@ -206,4 +215,5 @@ STRUCTS = {
     "v3d_mesh_triangle": MeshTriangle, "v3d_mesh_stats": MeshStats,
     "v3d_mesh_result": MeshResult, "v3d_mesh_dense_input": MeshDenseInput,
     "v3d_site_record": SiteRecord, "v3d_run_info": RunInfo, "v3d_mesh_counts": MeshCounts,
+    "v3d_clip": Clip,
 }

@@ -81,6 +81,10 @@ def library():
         C.c_int32, _P(abi.Profile), _P(C.c_uint64), C.c_uint64, abi.CANCEL_FN, C.c_void_p,
         _P(abi.DenseResult), _P(abi.MeshResult), _P(C.c_int32)]
     L.v3d_reconstruct_reference_patches_meshed.restype = C.c_int32
+    L.v3d_reconstruct_clips.argtypes = [C.c_void_p, _P(abi.Clip), C.c_uint64, C.c_int32,
+                                        _P(abi.Profile), abi.CANCEL_FN, C.c_void_p,
+                                        _P(abi.DenseResult), _P(abi.MeshResult), _P(C.c_int32)]
+    L.v3d_reconstruct_clips.restype = C.c_int32
     L.v3d_last_run_info.argtypes = [C.c_void_p, _P(abi.RunInfo)]
     L.v3d_last_run_info.restype = C.c_int32
     _lib = L
@@ -174,6 +178,52 @@ class Context:
                 self.lib.v3d_dense_result_free(C.byref(outs[i]))
                 self.lib.v3d_mesh_result_free(C.byref(meshes[i]))
                 res.append(None)
+        return res
+
+    def reconstruct_clips(self, clips, profile=None, fine_grid=False, meshed=False,
+                          control=None):
+        """The references of many clips of uneven size in one device batch.
+
+        `clips` is a list of dicts with keys frames, cameras, sparse_points, focal,
+        camera_indices and optionally depth_hypotheses / max_source_views (per-clip
+        overrides of the profile's).  Returns one list per clip with, per camera
+        index, a DenseAnalysis (a (DenseAnalysis, MeshAnalysis) pair when `meshed`)
+        or None where the reference returns None."""
+        prof = profile if profile is not None else profiles.reference()
+        fn, _keep = types.cancel_callback(control)
+        inputs, arr = [], (abi.Clip * max(len(clips), 1))()
+        counts = []
+        for c, clip in enumerate(clips):
+            inp = types.Inputs(clip["frames"], clip["cameras"], clip["sparse_points"])
+            idx = list(clip["camera_indices"])
+            ids = (C.c_uint64 * max(len(idx), 1))(*idx)
+            inputs.append((inp, ids))
+            arr[c] = abi.Clip(inp.frames, inp.n_frames, inp.cameras, inp.n_cameras, inp.sparse,
+                              inp.n_sparse, float(clip["focal"]), ids, len(idx),
+                              int(clip.get("depth_hypotheses", 0)),
+                              int(clip.get("max_source_views", 0)))
+            counts.append(len(idx))
+        n = sum(counts)
+        outs = (abi.DenseResult * max(n, 1))()
+        meshes = (abi.MeshResult * max(n, 1))() if meshed else None
+        present = (C.c_int32 * max(n, 1))()
+        self._check(self.lib.v3d_reconstruct_clips(
+            self.handle, arr, len(clips), int(fine_grid), C.byref(prof), fn, None, outs, meshes,
+            present))
+        flat = []
+        for i in range(n):
+            if present[i]:
+                flat.append((self._dense(outs[i]), self._mesh(meshes[i])) if meshed
+                            else self._dense(outs[i]))
+            else:
+                self.lib.v3d_dense_result_free(C.byref(outs[i]))
+                if meshed:
+                    self.lib.v3d_mesh_result_free(C.byref(meshes[i]))
+                flat.append(None)
+        res, at = [], 0
+        for k in counts:
+            res.append(flat[at:at + k])
+            at += k
         return res
 
     def estimate_depth_points_limited(self, frames, cameras, sparse_points, focal,

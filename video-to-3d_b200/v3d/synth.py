@@ -317,3 +317,27 @@ def heavy_clip(seed=5, width=640, height=360, n_frames=120):
     """8 planes plus 4 boxes, 5 % low-texture regions, noise 0.02."""
     return make_clip(width, height, n_frames, 40.0, 4.0, seed, noise_sigma=0.02,
                      jitter_deg=2.0, extra_planes=4, boxes=4, low_texture_fraction=0.05)
+
+
+def batched_clip_specs(n_clips=32, seed=3, min_frames=24, max_frames=120, min_edge=240,
+                       max_edge=640):
+    """Seeded parameters of the batched uneven clips: long edge uniform in
+    [min_edge, max_edge] at 16:9, min_frames..max_frames frames, 2-12 source views
+    per reference, 32-256 hypotheses, 0-2 extra planes and 0-1 boxes."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for i in range(n_clips):
+        w = int(rng.integers(min_edge, max_edge + 1))
+        h = max(16, int(round(w * 9 / 16)))
+        specs.append(dict(width=w, height=h, n_frames=int(rng.integers(min_frames, max_frames + 1)),
+                          sources=int(rng.integers(2, 13)), planes=int(rng.integers(32, 257)),
+                          extra_planes=int(rng.integers(0, 3)), boxes=int(rng.integers(0, 2)),
+                          seed=seed * 1000 + i))
+    return specs
+
+
+def batched_clip(spec):
+    """The clip of one batched_clip_specs entry (a 40-degree arc like the full clip)."""
+    return make_clip(spec["width"], spec["height"], spec["n_frames"], 40.0, 4.0, spec["seed"],
+                     noise_sigma=0.01, jitter_deg=2.0, extra_planes=spec["extra_planes"],
+                     boxes=spec["boxes"], landmarks_per_camera=200)
