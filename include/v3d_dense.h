@@ -61,7 +61,9 @@ typedef enum v3d_status {
     V3D_ERR_CUDA = -2,
     V3D_ERR_OUT_OF_MEMORY = -3,
     V3D_ERR_NO_DEVICE = -4,
-    V3D_ERR_INTERNAL = -5
+    V3D_ERR_INTERNAL = -5,
+    V3D_ERR_TIMEOUT = -6,            /* v3d_server_wait: the request is not done yet */
+    V3D_ERR_SHUTDOWN = -7            /* the server stopped before running the request */
 } v3d_status;
 
 /* Skip reasons of dense_legacy.rs:157-236 and dense.rs, in the order the
@@ -460,6 +462,62 @@ typedef struct v3d_run_info {
 } v3d_run_info;
 
 int32_t v3d_last_run_info(const v3d_context* ctx, v3d_run_info* out);
+
+/* ---- Serving (no counterpart in the reference, which runs one call at a time) ----
+ *
+ * A device-resident request loop.  Clips (frames, cameras, landmarks) are
+ * registered once: their frames are copied to device memory and stay there.
+ * A request asks for reconstruct_reference_patch (dense.rs:674-747) of one
+ * camera of a registered clip, with its own hypothesis count and source-view
+ * limit.  `slots` worker threads, each with its own CUDA stream and device
+ * buffers, take the queued requests in arrival order, as many as the memory
+ * budget of a slot admits, and run them as one device batch; while one slot's
+ * batch is on the GPU, requests arriving meanwhile form the next batch on
+ * another slot, so their work overlaps on the device.  Every request's result
+ * is computed from its own inputs only, so it is the same alone and in any mix. */
+typedef struct v3d_server v3d_server;
+
+typedef struct v3d_server_config {
+    int32_t device;
+    int32_t slots;                 /* batches in flight at once, 1..8 */
+    uint64_t memory_budget_bytes;  /* device buffers of all slots together (frames excluded); 0: 8 GiB */
+    uint32_t max_batch_requests;   /* requests per batch at most; 0: as many as a slot's budget admits */
+    int32_t meshed;                /* also run the reference-grid triangle gates of every patch */
+    int32_t fine_grid;
+    v3d_profile profile;           /* per-request overrides: hypotheses and source views */
+} v3d_server_config;
+
+/* Per-request timing, measured on the host from submission. */
+typedef struct v3d_request_timing {
+    double queue_ms;               /* submitted -> its batch started */
+    double service_ms;             /* its batch started -> results ready */
+    double total_ms;               /* submitted -> results ready */
+    uint64_t batch_requests;       /* requests in its batch */
+    uint64_t plane_view_units;     /* its grid sites x hypotheses x source views */
+} v3d_request_timing;
+
+int32_t v3d_server_create(const v3d_server_config* config, v3d_server** out);
+/* Waits for the batches on the GPU; queued requests end with V3D_ERR_SHUTDOWN
+ * and results not collected are freed. */
+void v3d_server_destroy(v3d_server* server);
+/* Copies the frames to device memory (one pixel format for all clips of a
+ * server); cameras and landmarks are kept on the host for planning. */
+int32_t v3d_server_add_clip(v3d_server* server, const v3d_frame* frames, uint64_t n_frames,
+                            const v3d_camera* cameras, uint64_t n_cameras,
+                            const double* sparse_xyz, uint64_t n_sparse, double focal,
+                            uint64_t* clip_id);
+/* Queues one reference camera of a registered clip; 0 keeps the server
+ * profile's hypothesis count / source-view limit. */
+int32_t v3d_server_submit(v3d_server* server, uint64_t clip_id, uint64_t camera_index,
+                          int32_t depth_hypotheses, int32_t max_source_views, uint64_t* ticket);
+/* Waits up to timeout_ms (negative: no limit) for a request.  On completion
+ * returns its status, moves its result into *out (and *mesh_out for a meshed
+ * server; may be NULL otherwise), sets *present as
+ * v3d_reconstruct_reference_patches does and fills *timing (may be NULL);
+ * the ticket is then spent.  V3D_ERR_TIMEOUT leaves the request pending. */
+int32_t v3d_server_wait(v3d_server* server, uint64_t ticket, int64_t timeout_ms,
+                        v3d_dense_result* out, v3d_mesh_result* mesh_out, int32_t* present,
+                        v3d_request_timing* timing);
 
 /* Per-site outcome of the depth sweep (dense_legacy.rs:272-362) before the
  * reciprocal check: status 1 = below the contrast gate, 2 = no hypothesis had

@@ -64,24 +64,6 @@ bool valid_frames(const v3d_frame* frames, uint64_t n) {
     return true;
 }
 
-Inputs load_inputs(const v3d_frame* frames, uint64_t n_frames, const v3d_camera* cams,
-                   uint64_t n_cams, const double* sparse, uint64_t n_sparse, double focal) {
-    Inputs in;
-    in.frames = frames;
-    in.n_frames = n_frames;
-    in.cameras.resize(n_cams);
-    for (uint64_t i = 0; i < n_cams; ++i) {
-        in.cameras[i].frame_index = cams[i].frame_index;
-        std::memcpy(in.cameras[i].R, cams[i].rotation, sizeof(in.cameras[i].R));
-        std::memcpy(in.cameras[i].t, cams[i].translation, sizeof(in.cameras[i].t));
-    }
-    in.sparse.resize(n_sparse);
-    for (uint64_t i = 0; i < n_sparse; ++i)
-        in.sparse[i] = {sparse[3 * i], sparse[3 * i + 1], sparse[3 * i + 2]};
-    in.focal = focal;
-    return in;
-}
-
 void fill_pass(v3d_dense_result* out, const PassResult& r) {
     std::memset(out, 0, sizeof(*out));
     out->stats = r.stats;
@@ -214,6 +196,8 @@ const char* v3d_status_text(int32_t status) {
         case V3D_ERR_OUT_OF_MEMORY: return "out of device memory";
         case V3D_ERR_NO_DEVICE: return "no CUDA device";
         case V3D_ERR_INTERNAL: return "internal error";
+        case V3D_ERR_TIMEOUT: return "request not done within the timeout";
+        case V3D_ERR_SHUTDOWN: return "server stopped before the request ran";
     }
     return "unknown status";
 }
@@ -412,21 +396,30 @@ void fill_mesh(v3d_mesh_result* out, const MeshOut& m) {
     }
 }
 
-// One clip of a device batch: its inputs, its profile and the cameras to use
-// as references.  Frame slots of its plans are local to the clip until the
-// batch concatenates the clips' frames.
-struct ClipJob {
-    Inputs in;
-    v3d_profile prof{};
-    const uint64_t* camera_indices = nullptr;
-    uint64_t n_refs = 0;
-};
+}  // namespace
 
-// dense.rs:674-747 for every (clip, reference camera) of `jobs`, run as one
-// device batch; out, mesh_out and present hold the references clip by clip.
-int32_t clip_batch(v3d_context* ctx, const std::vector<ClipJob>& jobs, int32_t fine_grid,
-                   const v3d_profile& batch_prof, v3d_cancel_fn cancel, void* cancel_user,
-                   v3d_dense_result* out, v3d_mesh_result* mesh_out, int32_t* present) {
+Inputs v3d::load_inputs(const v3d_frame* frames, uint64_t n_frames, const v3d_camera* cams,
+                   uint64_t n_cams, const double* sparse, uint64_t n_sparse, double focal) {
+    Inputs in;
+    in.frames = frames;
+    in.n_frames = n_frames;
+    in.cameras.resize(n_cams);
+    for (uint64_t i = 0; i < n_cams; ++i) {
+        in.cameras[i].frame_index = cams[i].frame_index;
+        std::memcpy(in.cameras[i].R, cams[i].rotation, sizeof(in.cameras[i].R));
+        std::memcpy(in.cameras[i].t, cams[i].translation, sizeof(in.cameras[i].t));
+    }
+    in.sparse.resize(n_sparse);
+    for (uint64_t i = 0; i < n_sparse; ++i)
+        in.sparse[i] = {sparse[3 * i], sparse[3 * i + 1], sparse[3 * i + 2]};
+    in.focal = focal;
+    return in;
+}
+
+int32_t v3d::clip_batch(v3d_context* ctx, const std::vector<ClipJob>& jobs, int32_t fine_grid,
+                        const v3d_profile& batch_prof, v3d_cancel_fn cancel, void* cancel_user,
+                        v3d_dense_result* out, v3d_mesh_result* mesh_out, int32_t* present,
+                        std::vector<uint64_t>* units) {
     std::lock_guard<std::mutex> lock(ctx->mu);
     cudaSetDevice(ctx->device);
     const auto t_plan = std::chrono::steady_clock::now();
@@ -472,13 +465,33 @@ int32_t clip_batch(v3d_context* ctx, const std::vector<ClipJob>& jobs, int32_t f
         for (const ClipJob& J : jobs) all_frames.insert(all_frames.end(), J.in.frames, J.in.frames + J.in.n_frames);
         frames = all_frames.data();
     }
+    // device-resident frames (a server's clips), when the jobs carry them
+    std::vector<ResidentFrame> resident;
+    const bool on_device = !jobs.empty() && jobs[0].resident != nullptr;
+    if (on_device) {
+        resident.reserve(frame_base.back());
+        for (const ClipJob& J : jobs) {
+            if (!J.resident) {
+                ctx->last_error = "jobs of one batch must all carry resident frames or none";
+                return V3D_ERR_INVALID_ARGUMENT;
+            }
+            resident.insert(resident.end(), J.resident, J.resident + J.in.n_frames);
+        }
+    }
+    if (units) {
+        units->assign(n_refs, 0);
+        for (size_t i = 0; i < n_refs; ++i)
+            if (!plans[i].skipped)
+                (*units)[i] = static_cast<uint64_t>(plans[i].nx) * plans[i].ny * plans[i].planes *
+                              plans[i].src_slots.size();
+    }
     const double plan_ms = std::chrono::duration<double, std::milli>(
                                std::chrono::steady_clock::now() - t_plan).count();
     std::vector<PassResult> res;
     std::vector<MeshOut> meshes;
     const double focal = jobs.empty() ? 0.0 : jobs[0].in.focal;  // each plan carries its own
     int32_t st = run_batch(ctx, batch_prof, frames, frame_base.back(), focal, plans, res,
-                           mesh_out ? &meshes : nullptr);
+                           mesh_out ? &meshes : nullptr, on_device ? &resident : nullptr);
     ctx->last_plan_ms = plan_ms;
     if (st < 0) return st;
     if (mesh_out && meshes.size() != n_refs) {
@@ -519,6 +532,8 @@ int32_t clip_batch(v3d_context* ctx, const std::vector<ClipJob>& jobs, int32_t f
     }
     return V3D_OK;
 }
+
+namespace {
 
 void clear_outputs(uint64_t n, v3d_dense_result* out, v3d_mesh_result* mesh_out, int32_t* present) {
     for (uint64_t i = 0; i < n; ++i) {

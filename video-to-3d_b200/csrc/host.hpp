@@ -60,6 +60,13 @@ struct Span {
     T& operator[](size_t i) const { return ptr[i]; }
 };
 
+// A frame already in device memory (a server's clip store): the frame as
+// handed in and, for RGBA8, its u8 luma plane (else `luma` is the frame).
+struct ResidentFrame {
+    const void* raw = nullptr;
+    const uint8_t* luma = nullptr;
+};
+
 // One patch's reference-grid triangles (mesh_legacy.rs:40-43).
 struct MeshOut {
     v3d_mesh_stats stats{};
@@ -94,6 +101,22 @@ struct CancelPoll {
         return canceled;
     }
 };
+
+// One clip of a device batch: its inputs, its profile and the cameras to use
+// as references; `resident` (one entry per frame, or null) when its frames
+// already live in device memory.
+struct ClipJob {
+    Inputs in;
+    v3d_profile prof{};
+    const uint64_t* camera_indices = nullptr;
+    uint64_t n_refs = 0;
+    const ResidentFrame* resident = nullptr;
+};
+
+// The caller's cameras and landmarks as planning inputs (api.cpp); `frames`
+// is referenced, not copied.
+Inputs load_inputs(const v3d_frame* frames, uint64_t n_frames, const v3d_camera* cams,
+                   uint64_t n_cams, const double* sparse, uint64_t n_sparse, double focal);
 
 // ---- planning (host_plan.cpp) ----
 uint32_t reference_grid_stride(uint32_t w, uint32_t h, bool fine);
@@ -159,9 +182,21 @@ namespace v3d {
 // `results` (same order).  Returns a v3d_status.
 // With `mesh` set, the reference-grid triangle gates of every patch run on
 // the device after completion and (*mesh)[i] receives plan i's mesh.
+// With `resident` (one entry per frame slot) the frames are read where they
+// lie in device memory and nothing is uploaded; `frames` then supplies sizes
+// and the pixel format only.
 int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* frames,
                   size_t n_frames, double focal, const std::vector<RefPlan>& plans,
-                  std::vector<PassResult>& results, std::vector<MeshOut>* mesh = nullptr);
+                  std::vector<PassResult>& results, std::vector<MeshOut>* mesh = nullptr,
+                  const std::vector<ResidentFrame>* resident = nullptr);
+
+// dense.rs:674-747 for every (clip, reference camera) of `jobs`, run as one
+// device batch (api.cpp); out, mesh_out and present hold the references clip
+// by clip, `units` (optional) each reference's sites x hypotheses x sources.
+int32_t clip_batch(v3d_context* ctx, const std::vector<ClipJob>& jobs, int32_t fine_grid,
+                   const v3d_profile& batch_prof, v3d_cancel_fn cancel, void* cancel_user,
+                   v3d_dense_result* out, v3d_mesh_result* mesh_out, int32_t* present,
+                   std::vector<uint64_t>* units = nullptr);
 
 // The sweep of one planned pass alone, as per-site records (v3d_debug_sweep).
 int32_t run_sweep_records(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* frames,

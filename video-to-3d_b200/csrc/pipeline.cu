@@ -171,7 +171,7 @@ struct Prepared {
 int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* frames,
                 size_t n_frames, double focal, const std::vector<RefPlan>& plans,
                 const std::vector<size_t>& active, bool sweep_only, Prepared& P,
-                bool with_mesh = false) {
+                bool with_mesh = false, const std::vector<ResidentFrame>* resident = nullptr) {
     cudaStream_t stream = static_cast<cudaStream_t>(ctx->stream);
     P.active = active;
 
@@ -186,7 +186,9 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
             used.push_back(slot);
         }
         if (format < 0) format = frames[slot].format;
-        return frames[slot].format == format && frames[slot].data != nullptr;
+        const bool has_data = resident ? (*resident)[slot].raw != nullptr && (*resident)[slot].luma
+                                       : frames[slot].data != nullptr;
+        return frames[slot].format == format && has_data;
     };
     for (size_t a : active) {
         if (!use(plans[a].ref_slot)) {
@@ -227,7 +229,7 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
     // ---- arena layout ----
     Carver cv;
     std::vector<size_t> raw_off(used.size()), luma_off(used.size());
-    for (size_t u = 0; u < used.size(); ++u) {
+    for (size_t u = 0; !resident && u < used.size(); ++u) {
         const v3d_frame& f = frames[used[u]];
         size_t px = static_cast<size_t>(f.width) * f.height;
         raw_off[u] = cv.take<uint8_t>(px * bytes_per_pixel(format));
@@ -286,8 +288,14 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
     char* base = static_cast<char*>(ctx->arena);
     auto at = [&](size_t off) { return base + off; };
 
-    // ---- uploads ----
+    // ---- uploads (none for resident frames) ----
+    std::vector<const void*> raw_ptr(used.size()), luma_ptr(used.size());
     for (size_t u = 0; u < used.size(); ++u) {
+        if (resident) {
+            raw_ptr[u] = (*resident)[used[u]].raw;
+            luma_ptr[u] = (*resident)[used[u]].luma;
+            continue;
+        }
         const v3d_frame& f = frames[used[u]];
         size_t px = static_cast<size_t>(f.width) * f.height;
         V3D_CK(cudaMemcpyAsync(at(raw_off[u]), f.data, px * bytes_per_pixel(format),
@@ -295,6 +303,8 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
         if (rgba)
             V3D_CK(launch_luma(reinterpret_cast<const uint8_t*>(at(raw_off[u])),
                                reinterpret_cast<uint8_t*>(at(luma_off[u])), px, stream));
+        raw_ptr[u] = at(raw_off[u]);
+        luma_ptr[u] = at(luma_off[u]);
     }
     const size_t staging = sizeof(DevReference) * n_active + sizeof(uint64_t) * (n_active + 1) +
                            sizeof(float) * inv_count;
@@ -309,8 +319,8 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
         DevReference& d = hrefs[k];
         set_cam(d.cam, p.ref_cam);
         size_t ru = static_cast<size_t>(dev_of[p.ref_slot]);
-        d.img = DevImage{at(luma_off[ru]), frames[p.ref_slot].width, frames[p.ref_slot].height};
-        d.rgba = rgba ? reinterpret_cast<const uint8_t*>(at(raw_off[ru])) : nullptr;
+        d.img = DevImage{luma_ptr[ru], frames[p.ref_slot].width, frames[p.ref_slot].height};
+        d.rgba = rgba ? static_cast<const uint8_t*>(raw_ptr[ru]) : nullptr;
         d.focal = p.focal;
         d.planes = p.planes;
         d.inv_off = inv_off[k];
@@ -326,7 +336,7 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
             size_t su = static_cast<size_t>(dev_of[p.src_slots[j]]);
             const v3d_frame& sf = frames[p.src_slots[j]];
             set_cam(s.cam, p.src_cams[j]);
-            s.img = DevImage{at(luma_off[su]), sf.width, sf.height};
+            s.img = DevImage{luma_ptr[su], sf.width, sf.height};
             s.search_min = p.src_min[j];
             s.search_max = p.src_max[j];
             homography_parts(p.ref_cam, d.img.width, d.img.height, p.src_cams[j], sf.width,
@@ -507,7 +517,8 @@ __global__ void k_pool_output(const OutPoint* __restrict__ pool, const uint32_t*
 
 int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* frames,
                   size_t n_frames, double focal, const std::vector<RefPlan>& plans,
-                  std::vector<PassResult>& results, std::vector<MeshOut>* mesh) {
+                  std::vector<PassResult>& results, std::vector<MeshOut>* mesh,
+                  const std::vector<ResidentFrame>* resident) {
     cudaStream_t stream = static_cast<cudaStream_t>(ctx->stream);
     results.assign(plans.size(), PassResult{});
     std::vector<size_t> active;
@@ -526,7 +537,7 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
     const clk::time_point t_upload = clk::now();
     Prepared P;
     int32_t pst = prepare(ctx, prof, frames, n_frames, focal, plans, active, false, P,
-                          mesh != nullptr);
+                          mesh != nullptr, resident);
     if (pst != V3D_OK) return pst;
     const size_t n_active = P.n_active;
     const uint64_t total = P.total, cap = P.cap;

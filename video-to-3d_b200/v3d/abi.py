@@ -207,6 +207,20 @@ class Clip(C.Structure):
                 ("max_source_views", C.c_int32)]
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("device", C.c_int32), ("slots", C.c_int32), ("memory_budget_bytes", C.c_uint64),
+                ("max_batch_requests", C.c_uint32), ("meshed", C.c_int32),
+                ("fine_grid", C.c_int32), ("profile", Profile)]
+
+
+class RequestTiming(C.Structure):
+    _fields_ = [("queue_ms", C.c_double), ("service_ms", C.c_double), ("total_ms", C.c_double),
+                ("batch_requests", C.c_uint64), ("plane_view_units", C.c_uint64)]
+
+
+TIMEOUT = -6
+SHUTDOWN = -7
+
 STRUCTS = {
     "v3d_frame": Frame, "v3d_camera": Camera, "v3d_profile": Profile, "v3d_point": Point,
     "v3d_grid_site": GridSite, "v3d_point_attributes": PointAttributes,
@@ -215,5 +229,5 @@ STRUCTS = {
     "v3d_mesh_triangle": MeshTriangle, "v3d_mesh_stats": MeshStats,
     "v3d_mesh_result": MeshResult, "v3d_mesh_dense_input": MeshDenseInput,
     "v3d_site_record": SiteRecord, "v3d_run_info": RunInfo, "v3d_mesh_counts": MeshCounts,
-    "v3d_clip": Clip,
+    "v3d_clip": Clip, "v3d_server_config": ServerConfig, "v3d_request_timing": RequestTiming,
 }

@@ -85,6 +85,20 @@ def library():
                                         _P(abi.Profile), abi.CANCEL_FN, C.c_void_p,
                                         _P(abi.DenseResult), _P(abi.MeshResult), _P(C.c_int32)]
     L.v3d_reconstruct_clips.restype = C.c_int32
+    L.v3d_server_create.argtypes = [_P(abi.ServerConfig), _P(C.c_void_p)]
+    L.v3d_server_create.restype = C.c_int32
+    L.v3d_server_destroy.argtypes = [C.c_void_p]
+    L.v3d_server_destroy.restype = None
+    L.v3d_server_add_clip.argtypes = [C.c_void_p, _P(abi.Frame), C.c_uint64, _P(abi.Camera),
+                                      C.c_uint64, _P(C.c_double), C.c_uint64, C.c_double,
+                                      _P(C.c_uint64)]
+    L.v3d_server_add_clip.restype = C.c_int32
+    L.v3d_server_submit.argtypes = [C.c_void_p, C.c_uint64, C.c_uint64, C.c_int32, C.c_int32,
+                                    _P(C.c_uint64)]
+    L.v3d_server_submit.restype = C.c_int32
+    L.v3d_server_wait.argtypes = [C.c_void_p, C.c_uint64, C.c_int64, _P(abi.DenseResult),
+                                  _P(abi.MeshResult), _P(C.c_int32), _P(abi.RequestTiming)]
+    L.v3d_server_wait.restype = C.c_int32
     L.v3d_last_run_info.argtypes = [C.c_void_p, _P(abi.RunInfo)]
     L.v3d_last_run_info.restype = C.c_int32
     _lib = L
@@ -283,3 +297,87 @@ def has_distributed_landmarks(frames, cameras, sparse_points, focal, control=Non
 
 def grid_stride(width, height, fine_grid):
     return int(library().v3d_grid_stride(int(width), int(height), int(fine_grid)))
+
+
+class Served:
+    """Outcome of one served request: status, result (a DenseAnalysis, a
+    (DenseAnalysis, MeshAnalysis) pair for a meshed server, or None where the
+    reference returns None) and the request's timing."""
+
+    def __init__(self, status, result, timing):
+        self.status = status
+        self.result = result
+        self.timing = timing
+
+
+class Server:
+    """A device-resident request loop on one GPU (v3d_server).
+
+    Clips are registered once (their frames stay in device memory); each request
+    is one reference camera of a clip with optional per-request hypothesis and
+    source-view counts.  `slots` batches run at once, each on its own stream."""
+
+    def __init__(self, device=0, slots=2, memory_budget=0, max_batch_requests=0, meshed=False,
+                 fine_grid=False, profile=None):
+        self.lib = library()
+        self.meshed = bool(meshed)
+        cfg = abi.ServerConfig(int(device), int(slots), int(memory_budget), int(max_batch_requests),
+                               int(self.meshed), int(bool(fine_grid)),
+                               profile if profile is not None else profiles.reference())
+        h = C.c_void_p()
+        st = self.lib.v3d_server_create(C.byref(cfg), C.byref(h))
+        if st < 0:
+            raise V3DError(st, "v3d_server_create failed")
+        self.handle = h
+
+    def close(self):
+        if self.handle:
+            self.lib.v3d_server_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        self.close()
+
+    def add_clip(self, frames, cameras, sparse_points, focal):
+        inp = types.Inputs(frames, cameras, sparse_points)
+        cid = C.c_uint64()
+        st = self.lib.v3d_server_add_clip(self.handle, inp.frames, inp.n_frames, inp.cameras,
+                                          inp.n_cameras, inp.sparse, inp.n_sparse, float(focal),
+                                          C.byref(cid))
+        if st < 0:
+            raise V3DError(st, "v3d_server_add_clip failed")
+        return cid.value
+
+    def submit(self, clip_id, camera_index, depth_hypotheses=0, max_source_views=0):
+        t = C.c_uint64()
+        st = self.lib.v3d_server_submit(self.handle, int(clip_id), int(camera_index),
+                                        int(depth_hypotheses), int(max_source_views), C.byref(t))
+        if st < 0:
+            raise V3DError(st, "v3d_server_submit failed")
+        return t.value
+
+    def wait(self, ticket, timeout_ms=-1):
+        """The request's Served outcome, or None while it is not done within timeout_ms."""
+        out = abi.DenseResult()
+        mesh = abi.MeshResult()
+        present = C.c_int32()
+        timing = abi.RequestTiming()
+        st = self.lib.v3d_server_wait(self.handle, int(ticket), int(timeout_ms), C.byref(out),
+                                      C.byref(mesh) if self.meshed else None, C.byref(present),
+                                      C.byref(timing))
+        if st == abi.TIMEOUT:
+            return None
+        t = {name: getattr(timing, name) for name, _ in abi.RequestTiming._fields_}
+        if st < 0:
+            raise V3DError(st, "request failed")
+        if not present.value:
+            self.lib.v3d_dense_result_free(C.byref(out))
+            if self.meshed:
+                self.lib.v3d_mesh_result_free(C.byref(mesh))
+            return Served(st, None, t)
+        dense = types.dense_from_result(
+            out, st, types.ResultOwner(self.lib.v3d_dense_result_free, out))
+        if self.meshed:
+            m = types.mesh_from_result(mesh, types.ResultOwner(self.lib.v3d_mesh_result_free, mesh))
+            return Served(st, (dense, m), t)
+        return Served(st, dense, t)
