@@ -56,6 +56,16 @@ def parse():
     ap.add_argument("--frames", type=int, default=FRAMES)
     ap.add_argument("--no-cpu-baseline", action="store_true",
                     help="skip the CPU baseline leg (profiling runs)")
+    ap.add_argument("--config", choices=["full", "small", "heavy", "batched", "served"],
+                    default="full",
+                    help="full: the headline line (default); small: 360x202 1+4 views; heavy: "
+                         "bf16 16 views 256 planes 9x9; batched: 32 uneven clips through the "
+                         "server vs one request at a time; served: Poisson arrivals, p50/p99")
+    ap.add_argument("--rates", default="50,200,800", help="served: request rates (req/s)")
+    ap.add_argument("--duration", type=float, default=3.0, help="served: seconds of arrivals")
+    ap.add_argument("--clips", type=int, default=32, help="batched/served: number of clips")
+    ap.add_argument("--budget-gib", type=int, default=32,
+                    help="batched/served: device memory budget of the server's batch slots")
     return ap.parse_args()
 
 
@@ -327,11 +337,215 @@ def run_ours(args, rank, world, local):
         dist.destroy_process_group()
 
 
+# ---- the other configurations: one JSON line each, not the headline ----------
+
+def _render_batched(spec):
+    from v3d import synth
+    c = synth.batched_clip(spec)
+    return (spec, c.width, c.height, c.focal, np.stack([k.rotation for k in c.cameras]),
+            np.stack([k.translation for k in c.cameras]), np.stack(c.images), c.sparse)
+
+
+def batched_clips(n, seed=3):
+    """The seeded uneven clips of the batched and served configurations, rendered
+    in a process pool and cached under the system temp directory."""
+    import concurrent.futures as cf
+    import multiprocessing as mp
+    import pickle
+    from v3d import synth
+    from v3d.types import RegisteredCamera
+    path = os.path.join(tempfile.gettempdir(), "v3d_batched_%d_%d.pkl" % (n, seed))
+    if os.path.exists(path):
+        rendered = pickle.load(open(path, "rb"))
+    else:
+        specs = synth.batched_clip_specs(n_clips=n, seed=seed)
+        with cf.ProcessPoolExecutor(max_workers=min(n, os.cpu_count() or 1),
+                                    mp_context=mp.get_context("spawn")) as ex:
+            rendered = list(ex.map(_render_batched, specs))
+        pickle.dump(rendered, open(path, "wb"))
+    clips = []
+    for spec, w, h, f, R, t, images, sparse in rendered:
+        cams = [RegisteredCamera(i, R[i], t[i]) for i in range(len(R))]
+        clips.append((spec, synth.Clip(w, h, f, cams, list(images), [], sparse)))
+    return clips
+
+
+def _percentile(v, q):
+    return float(np.percentile(np.asarray(v, dtype=np.float64), q)) if v else None
+
+
+def _drive(srv, ids, reqs, arrivals):
+    """Submits reqs at their arrival offsets (seconds) from a thread and collects
+    them in order; returns latency percentiles and throughput."""
+    import queue
+    q = queue.Queue()
+    t0 = time.perf_counter()
+
+    def submit():
+        for i, ((ci, cam, planes, sources), at) in enumerate(zip(reqs, arrivals)):
+            d = t0 + at - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            q.put(srv.submit(ids[ci], cam, planes, sources))
+
+    th = threading.Thread(target=submit)
+    th.start()
+    lat, queue_ms, units, batches = [], [], 0, []
+    for _ in reqs:
+        out = srv.wait(q.get())
+        lat.append(out.timing["total_ms"])
+        queue_ms.append(out.timing["queue_ms"])
+        units += out.timing["plane_view_units"]
+        batches.append(out.timing["batch_requests"])
+    elapsed = time.perf_counter() - t0
+    th.join()
+    return {"requests": len(reqs), "p50_ms": _percentile(lat, 50), "p99_ms": _percentile(lat, 99),
+            "p50_queue_ms": _percentile(queue_ms, 50), "units": units, "seconds": elapsed,
+            "units_per_s": units / elapsed, "mean_batch_requests": float(np.mean(batches))}
+
+
+def _server(form, args, prof):
+    from v3d import dense
+    if form in ("served", "batched"):
+        return dense.Server(slots=2, memory_budget=args.budget_gib << 30, profile=prof)
+    # the plain per-request kernel: one request per batch, one batch at a time
+    return dense.Server(slots=1, memory_budget=args.budget_gib << 30, max_batch_requests=1,
+                        profile=prof)
+
+
+def run_batched(args):
+    """Every frame of every uneven clip as a reference: the batched server
+    (all requests queued at once) against the plain per-request kernel."""
+    from v3d import profiles
+    clips = batched_clips(args.clips)
+    prof = profiles.zncc(RADIUS, PLANES, SOURCES, STRIDE)
+    reqs = [(ci, cam, spec["planes"], spec["sources"])
+            for ci, (spec, c) in enumerate(clips) for cam in range(len(c.cameras))]
+    forms = {}
+    for form in ("batched", "plain"):
+        srv = _server(form, args, prof)
+        ids = [srv.add_clip(c.frames(args.storage), c.cameras, c.sparse, c.focal)
+               for _, c in clips]
+        _drive(srv, ids, reqs[:8], [0.0] * 8)  # warm-up
+        forms[form] = _drive(srv, ids, reqs, [0.0] * len(reqs))
+        srv.close()
+    line = {"metric": METRIC, "unit": UNIT, "config": {
+                "workload": "%d seeded uneven clips (long edge 240-640 px 16:9, 24-120 frames, "
+                            "2-12 source views, 32-256 planes per clip), every frame a "
+                            "reference, 7x7 ZNCC, stride 2, %s images, frames resident in HBM"
+                            % (len(clips), args.storage),
+                "references": len(reqs)},
+            "batched": forms["batched"], "plain_per_request": forms["plain"],
+            "batched_over_plain": forms["batched"]["units_per_s"] / forms["plain"]["units_per_s"]}
+    print(json.dumps(line), flush=True)
+
+
+def run_served(args):
+    """Poisson arrivals of single-reference requests drawn from the uneven clips
+    (random clip and camera, 2-16 source views, 32-256 planes): the serving loop
+    (two overlapping batch slots, continuous admission) against the plain
+    per-request kernel, p50/p99 latency and throughput per rate."""
+    from v3d import profiles
+    clips = batched_clips(args.clips)
+    prof = profiles.zncc(RADIUS, PLANES, SOURCES, STRIDE)
+    rates = [float(r) for r in args.rates.split(",")]
+    plans = {}
+    for rate in rates:
+        rng = np.random.default_rng(int(rate) + 101)
+        n = max(1, int(round(rate * args.duration)))
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, n)).tolist()
+        reqs = []
+        for _ in range(n):
+            ci = int(rng.integers(0, len(clips)))
+            reqs.append((ci, int(rng.integers(0, len(clips[ci][1].cameras))),
+                         int(rng.integers(32, 257)), int(rng.integers(2, 17))))
+        plans[rate] = (reqs, arrivals)
+    out = {}
+    for form in ("served", "plain"):
+        srv = _server(form, args, prof)
+        ids = [srv.add_clip(c.frames(args.storage), c.cameras, c.sparse, c.focal)
+               for _, c in clips]
+        _drive(srv, ids, plans[rates[0]][0][:8], [0.0] * 8)  # warm-up
+        out[form] = {str(int(r)): _drive(srv, ids, *plans[r]) for r in rates}
+        srv.close()
+    line = {"metric": "served p50/p99 latency and " + METRIC, "unit": UNIT, "config": {
+                "workload": "Poisson arrivals over %.1f s of single-reference requests from %d "
+                            "seeded uneven clips (240-640 px, 2-16 source views, 32-256 planes), "
+                            "7x7 ZNCC, stride 2, %s images, frames resident in HBM"
+                            % (args.duration, len(clips), args.storage), "rates": rates},
+            "served": out["served"], "plain_per_request": out["plain"]}
+    print(json.dumps(line), flush=True)
+
+
+def _cost_error(ctx, oracle, clip, frames, prof):
+    """Chosen-hypothesis agreement and cost error of the fast policy against the
+    f64 oracle, over every grid site of the legacy pass's reference."""
+    from v3d import abi, profiles
+    exact = profiles.with_precision(prof, abi.PRECISION_EXACT64)
+    g = ctx.debug_sweep(frames, clip.cameras, clip.sparse, clip.focal, profile=prof)
+    o = oracle.debug_sweep(frames, clip.cameras, clip.sparse, clip.focal, profile=exact)
+    both = (g["status"] >= 3) & (o["status"] >= 3)
+    same = both & (g["plane"] == o["plane"])
+    err = np.abs(g["error"][same] - o["error"][same])
+    return {"sites": int(len(g)), "plane_agreement": float(same.sum() / max(1, both.sum())),
+            "max_cost_error": float(err.max()) if err.size else 0.0,
+            "median_cost_error": float(np.median(err)) if err.size else 0.0}
+
+
+def run_plain_config(args):
+    """Config 1 (small) or 5 (heavy) as a plain clip run, plus the fast policy's
+    cost error against the f64 oracle (for heavy on a 200x112 cut of the same
+    generator and profile, where the oracle finishes in seconds)."""
+    from tests.oracle_ffi import Oracle
+    from v3d import dense, profiles, synth
+    if args.config == "small":
+        clip = synth.plain_small_clip(seed=1)
+        storage = "f32" if args.storage == "f32" else args.storage
+        prof = profiles.zncc(2, 64, 4, 2)
+        refs = [2]
+        check_clip, name = clip, "plain small 360x202, 1 reference + 4 source views, 64 planes, 5x5 ZNCC, stride 2"
+    else:
+        clip = synth.heavy_clip(seed=5, n_frames=args.frames)
+        storage = "bf16" if args.storage == "f32" else args.storage
+        prof = profiles.zncc(4, 256, 16, 2)
+        refs = list(range(len(clip.cameras)))
+        check_clip = synth.make_clip(200, 112, 12, 40.0, 4.0, 5, noise_sigma=0.02, jitter_deg=2.0,
+                                     extra_planes=4, boxes=4, low_texture_fraction=0.05)
+        name = ("heavy 640x360, %d keyframes, 16 source views, 256 planes, 9x9 ZNCC, stride 2, "
+                "8 planes + 4 boxes, 5%% low texture, noise 0.02" % len(clip.cameras))
+    frames = clip.frames(storage)
+    ctx = dense.Context(0)
+    dev, wall = [], []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        ctx.reconstruct_reference_patches_meshed(frames, clip.cameras, clip.sparse, clip.focal,
+                                                 refs, profile=prof)
+        w = time.perf_counter() - t0
+        info = ctx.last_run_info()
+        if i >= args.warmup:
+            dev.append(info["device_ms"] / 1e3)
+            wall.append(w)
+    units = info["plane_view_units"]
+    err = _cost_error(ctx, Oracle(), check_clip, check_clip.frames(storage), prof)
+    line = {"metric": METRIC, "value": units / float(np.mean(dev)), "unit": UNIT,
+            "e2e": units / float(np.mean(wall)), "ms_per_step": float(np.mean(dev)) * 1e3,
+            "steps": args.steps, "warmup": args.warmup, "dtype": storage,
+            "config": {"workload": name + ", %s images" % storage, "units_per_step": units},
+            "cost_error_vs_fp64": err}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
     if args.impl == "reference":
         run_reference(args, rank, world)
+    elif args.config == "batched":
+        run_batched(args)
+    elif args.config == "served":
+        run_served(args)
+    elif args.config in ("small", "heavy"):
+        run_plain_config(args)
     else:
         run_ours(args, rank, world, local)
 
