@@ -677,6 +677,79 @@ __device__ __forceinline__ bool window_cost(const float* pvc, float pm, float pv
     return true;
 }
 
+// The ZNCC window costs of two hypotheses at once, for windows that
+// window_inside admitted: the same operations as window_cost<T, R, 1, false>,
+// each done on both hypotheses by one packed f32x2 instruction (sm_100) with
+// the scalar's rounding, so every component equals the scalar cost bit for
+// bit while the pair costs about half the issue slots.
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
+
+template <class T>
+__device__ __forceinline__ float2 sample_nonneg_pair(const T* __restrict__ p, uint32_t w, float2 u,
+                                                     float2 v) {
+    const float2 shift = f2(8388608.0f, 8388608.0f);  // 2^23, as in sample_nonneg
+    const float2 tu = __fadd2_rd(u, shift), tv = __fadd2_rd(v, shift);
+    const float2 fu = __fadd2_rn(tu, neg2(shift)), fv = __fadd2_rn(tv, neg2(shift));
+    const int sb = __float_as_int(8388608.0f);
+    const uint32_t ixa = (uint32_t)(__float_as_int(tu.x) - sb), ixb = (uint32_t)(__float_as_int(tu.y) - sb);
+    const uint32_t iya = (uint32_t)(__float_as_int(tv.x) - sb), iyb = (uint32_t)(__float_as_int(tv.y) - sb);
+    const float2 tx = __fadd2_rn(u, neg2(fu)), ty = __fadd2_rn(v, neg2(fv));
+    const size_t ra = (size_t)iya * w + ixa, rb = (size_t)iyb * w + ixb;
+    const float2 v00 = f2(pix<T>(p, ra), pix<T>(p, rb));
+    const float2 v10 = f2(pix<T>(p, ra + 1), pix<T>(p, rb + 1));
+    const float2 v01 = f2(pix<T>(p, ra + w), pix<T>(p, rb + w));
+    const float2 v11 = f2(pix<T>(p, ra + w + 1), pix<T>(p, rb + w + 1));
+    const float2 top = __ffma2_rn(__fadd2_rn(v10, neg2(v00)), tx, v00);
+    const float2 bot = __ffma2_rn(__fadd2_rn(v11, neg2(v01)), tx, v01);
+    return __ffma2_rn(__fadd2_rn(bot, neg2(top)), ty, top);
+}
+
+template <class T, int R>
+__device__ __forceinline__ void window_cost_zncc_pair(const float* pvc, float pm, float pvar,
+                                                      const float* Ha, const float* Hb,
+                                                      float minvar, const T* __restrict__ img,
+                                                      uint32_t w, float x, float y, bool& oka,
+                                                      float& ea, bool& okb, float& eb) {
+    constexpr int W = 2 * R + 1;
+    constexpr int N = W * W;
+    const float2 H0 = f2(Ha[0], Hb[0]), H3 = f2(Ha[3], Hb[3]), H6 = f2(Ha[6], Hb[6]);
+    const float2 H1 = f2(Ha[1], Hb[1]), H4 = f2(Ha[4], Hb[4]), H7 = f2(Ha[7], Hb[7]);
+    const float2 H2 = f2(Ha[2], Hb[2]), H5 = f2(Ha[5], Hb[5]), H8 = f2(Ha[8], Hb[8]);
+    const float2 npm = f2(-pm, -pm);
+    float2 ss = f2(0.f, 0.f), sss = f2(0.f, 0.f), sps = f2(0.f, 0.f);
+#pragma unroll 1
+    for (int dy = 0; dy < W; ++dy) {
+        const float Y = y + (float)(dy - R);
+        const float2 Y2 = f2(Y, Y);
+        const float2 hx = __ffma2_rn(H1, Y2, H2), hy = __ffma2_rn(H4, Y2, H5),
+                     hz = __ffma2_rn(H7, Y2, H8);
+        const float* prow = pvc + dy * W;
+#pragma unroll
+        for (int dx = 0; dx < W; ++dx) {
+            const float X = x + (float)(dx - R);
+            const float2 X2 = f2(X, X);
+            const float2 h2 = __ffma2_rn(H6, X2, hz);
+            const float2 iv = f2(__fdividef(1.0f, h2.x), __fdividef(1.0f, h2.y));
+            const float2 u = __fmul2_rn(__ffma2_rn(H0, X2, hx), iv);
+            const float2 v = __fmul2_rn(__ffma2_rn(H3, X2, hy), iv);
+            const float2 s = __fadd2_rn(sample_nonneg_pair<T>(img, w, u, v), npm);
+            ss = __fadd2_rn(ss, s);
+            sss = __ffma2_rn(s, s, sss);
+            sps = __ffma2_rn(f2(prow[dx], prow[dx]), s, sps);
+        }
+    }
+    const float n = (float)N;
+    auto finish = [&](float ssv, float sssv, float spsv, float& cost) {
+        const float vs = sssv - ssv * ssv / n;
+        if (!(pvar > 0.f) || !(vs > 0.f) || pvar / n < minvar || vs / n < minvar) return false;
+        cost = 1.0f - spsv * rsqrtf(pvar * vs);
+        return true;
+    };
+    oka = finish(ss.x, sss.x, sps.x, ea);
+    okb = finish(ss.y, sss.y, sps.y, eb);
+}
+
 template <class T, int R, int COST>
 __global__ void __launch_bounds__(256) k_recip_prepare(BatchDev b, const Cand* __restrict__ cands,
                                                        const uint32_t* __restrict__ count,
@@ -823,7 +896,7 @@ __global__ void __launch_bounds__(256) k_recip_prepare(BatchDev b, const Cand* _
 }
 
 template <class T, int R, int COST>
-__global__ void __launch_bounds__(256, 3) k_recip_sweep(BatchDev b, const Cand* __restrict__ cands,
+__global__ void __launch_bounds__(256, 2) k_recip_sweep(BatchDev b, const Cand* __restrict__ cands,
                                                      const uint32_t* __restrict__ count,
                                                      RecipObs* __restrict__ obs) {
     constexpr int W = 2 * R + 1;
@@ -878,21 +951,48 @@ __global__ void __launch_bounds__(256, 3) k_recip_sweep(BatchDev b, const Cand* 
         const float minvar = (float)prof.min_variance;
         float be = 3.0e38f;
         int bk = 0x7fffffff;
-        for (int k = lane; k < ref.planes; k += 32) {
-            const float inv = inv_tab[k];
-            float H[9];
-            plane_h(src.bwd_A, src.bwd_b, inv, H);
-            const float zmin = 1.0e-4f * inv;
+        // one hypothesis alone, through the scalar paths
+        auto single = [&](int k, const float* H, bool inside) {
+            const float zmin = 1.0e-4f * inv_tab[k];
             float e;
             const bool ok =
-                window_inside<R>(H, zmin, wl, hl, x0, y0)
-                    ? window_cost<T, R, COST, false>(pvc, pm, pvar, H, zmin, wl, hl, minvar, rimg,
-                                                     rw, x0, y0, e)
-                    : window_cost<T, R, COST, true>(pvc, pm, pvar, H, zmin, wl, hl, minvar, rimg,
-                                                    rw, x0, y0, e);
+                inside ? window_cost<T, R, COST, false>(pvc, pm, pvar, H, zmin, wl, hl, minvar,
+                                                        rimg, rw, x0, y0, e)
+                       : window_cost<T, R, COST, true>(pvc, pm, pvar, H, zmin, wl, hl, minvar,
+                                                       rimg, rw, x0, y0, e);
             if (ok && (double)e <= prof.max_error && e < be) {
                 be = e;
                 bk = k;
+            }
+        };
+        // this lane's hypotheses in the order lane, lane + 32, lane + 64, ...,
+        // taken two at a time (k, k + 32) for the packed ZNCC path
+        for (int k = lane; k < ref.planes; k += 64) {
+            const int k2 = k + 32;
+            float Ha[9], Hb[9];
+            plane_h(src.bwd_A, src.bwd_b, inv_tab[k], Ha);
+            const bool ina = window_inside<R>(Ha, 1.0e-4f * inv_tab[k], wl, hl, x0, y0);
+            bool inb = false;
+            if (k2 < ref.planes) {
+                plane_h(src.bwd_A, src.bwd_b, inv_tab[k2], Hb);
+                inb = window_inside<R>(Hb, 1.0e-4f * inv_tab[k2], wl, hl, x0, y0);
+            }
+            if (COST == 1 && ina && inb) {
+                bool oka, okb;
+                float ea, eb;
+                window_cost_zncc_pair<T, R>(pvc, pm, pvar, Ha, Hb, minvar, rimg, rw, x0, y0, oka,
+                                            ea, okb, eb);
+                if (oka && (double)ea <= prof.max_error && ea < be) {
+                    be = ea;
+                    bk = k;
+                }
+                if (okb && (double)eb <= prof.max_error && eb < be) {
+                    be = eb;
+                    bk = k2;
+                }
+            } else {
+                single(k, Ha, ina);
+                if (k2 < ref.planes) single(k2, Hb, inb);
             }
         }
 #pragma unroll
