@@ -13,6 +13,7 @@ namespace typed_detail {
 
 constexpr int kTileX = 32;
 constexpr int kTileY = 8;
+constexpr int kTileThreads = kTileX * kTileY;  // one thread per grid site of a tile
 constexpr double kInf = __builtin_huge_val();
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
@@ -170,6 +171,31 @@ __device__ __forceinline__ float sample_nonneg(const T* __restrict__ p, uint32_t
 
 
 
+// Packed f32x2 forms (sm_100): each component is computed exactly as the
+// scalar form with the same rounding.
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
+
+template <class T>
+__device__ __forceinline__ float2 sample_nonneg_pair(const T* __restrict__ p, uint32_t w, float2 u,
+                                                     float2 v) {
+    const float2 shift = f2(8388608.0f, 8388608.0f);  // 2^23, as in sample_nonneg
+    const float2 tu = __fadd2_rd(u, shift), tv = __fadd2_rd(v, shift);
+    const float2 fu = __fadd2_rn(tu, neg2(shift)), fv = __fadd2_rn(tv, neg2(shift));
+    const int sb = __float_as_int(8388608.0f);
+    const uint32_t ixa = (uint32_t)(__float_as_int(tu.x) - sb), ixb = (uint32_t)(__float_as_int(tu.y) - sb);
+    const uint32_t iya = (uint32_t)(__float_as_int(tv.x) - sb), iyb = (uint32_t)(__float_as_int(tv.y) - sb);
+    const float2 tx = __fadd2_rn(u, neg2(fu)), ty = __fadd2_rn(v, neg2(fv));
+    const size_t ra = (size_t)iya * w + ixa, rb = (size_t)iyb * w + ixb;
+    const float2 v00 = f2(pix<T>(p, ra), pix<T>(p, rb));
+    const float2 v10 = f2(pix<T>(p, ra + 1), pix<T>(p, rb + 1));
+    const float2 v01 = f2(pix<T>(p, ra + w), pix<T>(p, rb + w));
+    const float2 v11 = f2(pix<T>(p, ra + w + 1), pix<T>(p, rb + w + 1));
+    const float2 top = __ffma2_rn(__fadd2_rn(v10, neg2(v00)), tx, v00);
+    const float2 bot = __ffma2_rn(__fadd2_rn(v11, neg2(v01)), tx, v01);
+    return __ffma2_rn(__fadd2_rn(bot, neg2(top)), ty, top);
+}
+
 // ---- sweep, warp per site ----------------------------------------------------
 // Lanes take hypotheses lane, lane+32, ...; each lane keeps the running
 // best/second state, and a warp merge reproduces the reference's sort.
@@ -269,7 +295,7 @@ __global__ void __launch_bounds__(256) k_sweep_site(BatchDev b, const uint32_t* 
 // footprint's x coordinates come from a per-slot table, so the warp step
 // converts no integers.
 template <class T, int R>
-__global__ void __launch_bounds__(256) k_sweep_tiled(BatchDev b, uint64_t total_sites_unused,
+__global__ void __launch_bounds__(kTileThreads) k_sweep_tiled(BatchDev b, uint64_t total_sites_unused,
                                                      SiteRank* __restrict__ rank,
                                                      uint8_t* __restrict__ status,
                                                      RefCounters* __restrict__ ctr) {
@@ -292,17 +318,17 @@ __global__ void __launch_bounds__(256) k_sweep_tiled(BatchDev b, uint64_t total_
     float* refv = reinterpret_cast<float*>(hrs + PY * kTileX);  // [PY][PXp] reference values
     float* samp = refv + np;                 // [PY][PXp] source samples (NaN = invalid)
     float* colx = samp + np;                 // [PXp] footprint x of each slot, NaN = padding
-    float* costs = colx + PXp;               // [max_src][256]
-    float* hA = costs + ms * 256;            // [max_src][12] homography parts
+    float* costs = colx + PXp;               // [max_src][kTileThreads]
+    float* hA = costs + ms * kTileThreads;   // [max_src][12] homography parts
     float* pinv = hA + ms * 12;              // [planes] inverse depths
     const int tid = threadIdx.x;
     const T* rdata = static_cast<const T*>(ref.img.data);
     const int px0 = (int)(ref.border + gx0 * s) - R, py0 = (int)(ref.border + gy0 * s) - R;
-    for (int t = tid; t < PXp; t += 256) {
+    for (int t = tid; t < PXp; t += kTileThreads) {
         const int x = (t % PXs) * s + t / PXs;
         colx[t] = x < PX ? (float)(px0 + x) : __int_as_float(0x7fc00000);
     }
-    for (int i = tid; i < np; i += 256) {
+    for (int i = tid; i < np; i += kTileThreads) {
         const int yy = i / PXp, t = i - yy * PXp;
         const int x = (t % PXs) * s + t / PXs;
         const int X = px0 + x, Y = py0 + yy;
@@ -312,11 +338,11 @@ __global__ void __launch_bounds__(256) k_sweep_tiled(BatchDev b, uint64_t total_
         refv[i] = v;
     }
     const int n_src = ref.n_src;
-    for (int i = tid; i < n_src * 12; i += 256) {
+    for (int i = tid; i < n_src * 12; i += kTileThreads) {
         int j = i / 12, c = i - j * 12;
         hA[i] = c < 9 ? ref.src[j].fwd_A[c] : ref.src[j].fwd_b[c - 9];
     }
-    for (int k = tid; k < ref.planes; k += 256)
+    for (int k = tid; k < ref.planes; k += kTileThreads)
         pinv[k] = (float)ddiv(1.0, hypothesis_depth(k, ref.planes, ref.search_min, ref.search_max));
     // slot of tap dx of the window that starts at column 0 (add the window's start)
     int toff[W];
@@ -371,7 +397,31 @@ __global__ void __launch_bounds__(256) k_sweep_tiled(BatchDev b, uint64_t total_
             for (int yy = ty; yy < PY; yy += kTileY, Y += (float)kTileY) {
                 const float hx = fmaf(A[1], Y, H2), hy = fmaf(A[4], Y, H5), hz = fmaf(A[7], Y, H8);
                 float* row = samp + yy * PXp;
-                for (int t = tx; t < PXp; t += kTileX) {
+                int t = tx;
+                // slots t and t + 32 together with packed f32x2 arithmetic; each
+                // component is the scalar computation of the loop below, bit for bit
+                for (; t + kTileX < PXp; t += 2 * kTileX) {
+                    const float2 X2 = f2(colx[t], colx[t + kTileX]);
+                    const float2 h2 = __ffma2_rn(f2(A[6], A[6]), X2, f2(hz, hz));
+                    const float2 iv = f2(__fdividef(1.0f, h2.x), __fdividef(1.0f, h2.y));
+                    const float2 u = __fmul2_rn(__ffma2_rn(f2(A[0], A[0]), X2, f2(hx, hx)), iv);
+                    const float2 q = __fmul2_rn(__ffma2_rn(f2(A[3], A[3]), X2, f2(hy, hy)), iv);
+                    // padding slots have a NaN x and fail the first test
+                    const bool ia = h2.x > zmin && u.x >= 0.f && q.x >= 0.f && u.x < wl && q.x < hl;
+                    const bool ib = h2.y > zmin && u.y >= 0.f && q.y >= 0.f && u.y < wl && q.y < hl;
+                    float va = __int_as_float(0x7fc00000), vb = va;
+                    if (ia && ib) {
+                        const float2 sv = sample_nonneg_pair<T>(sdata, si.width, u, q);
+                        va = sv.x;
+                        vb = sv.y;
+                    } else {
+                        if (ia) va = sample_nonneg<T>(sdata, si.width, u.x, q.x);
+                        if (ib) vb = sample_nonneg<T>(sdata, si.width, u.y, q.y);
+                    }
+                    row[t] = va;
+                    row[t + kTileX] = vb;
+                }
+                for (; t < PXp; t += kTileX) {
                     const float X = colx[t];
                     const float h2 = fmaf(A[6], X, hz);
                     float v = __int_as_float(0x7fc00000);
@@ -419,7 +469,7 @@ __global__ void __launch_bounds__(256) k_sweep_tiled(BatchDev b, uint64_t total_
                 float cost = __int_as_float(0x7fc00000);
                 if (vs > 0.0 && vs >= minvar_n && vr_ok)
                     cost = 1.0f - (float)cov * rsqrtf(vr_f * (float)vs);
-                costs[j * 256 + tid] = cost;  // NaN when invalid
+                costs[j * kTileThreads + tid] = cost;  // NaN when invalid
             }
         }
         if (sampled) {
@@ -427,23 +477,23 @@ __global__ void __launch_bounds__(256) k_sweep_tiled(BatchDev b, uint64_t total_
             float* col = costs + tid;
             int cnt = 0;
             for (int j = 0; j < n_src; ++j) {
-                const float c = col[j * 256];
-                if ((double)c <= prof.max_error) col[(cnt++) * 256] = c;
+                const float c = col[j * kTileThreads];
+                if ((double)c <= prof.max_error) col[(cnt++) * kTileThreads] = c;
             }
             if (cnt > 0) {
                 for (int i = 1; i < cnt; ++i) {
-                    const float x = col[i * 256];
+                    const float x = col[i * kTileThreads];
                     int m = i - 1;
-                    while (m >= 0 && col[m * 256] > x) {
-                        col[(m + 1) * 256] = col[m * 256];
+                    while (m >= 0 && col[m * kTileThreads] > x) {
+                        col[(m + 1) * kTileThreads] = col[m * kTileThreads];
                         --m;
                     }
-                    col[(m + 1) * 256] = x;
+                    col[(m + 1) * kTileThreads] = x;
                 }
                 Rank c;
                 c.support = cnt;
                 c.plane = k;
-                c.error = (double)col[(cnt / 2) * 256];
+                c.error = (double)col[(cnt / 2) * kTileThreads];
                 c.second = kInf;
                 st = rank_merge(st, c);
             }
@@ -682,29 +732,6 @@ __device__ __forceinline__ bool window_cost(const float* pvc, float pm, float pv
 // each done on both hypotheses by one packed f32x2 instruction (sm_100) with
 // the scalar's rounding, so every component equals the scalar cost bit for
 // bit while the pair costs about half the issue slots.
-__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
-__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
-
-template <class T>
-__device__ __forceinline__ float2 sample_nonneg_pair(const T* __restrict__ p, uint32_t w, float2 u,
-                                                     float2 v) {
-    const float2 shift = f2(8388608.0f, 8388608.0f);  // 2^23, as in sample_nonneg
-    const float2 tu = __fadd2_rd(u, shift), tv = __fadd2_rd(v, shift);
-    const float2 fu = __fadd2_rn(tu, neg2(shift)), fv = __fadd2_rn(tv, neg2(shift));
-    const int sb = __float_as_int(8388608.0f);
-    const uint32_t ixa = (uint32_t)(__float_as_int(tu.x) - sb), ixb = (uint32_t)(__float_as_int(tu.y) - sb);
-    const uint32_t iya = (uint32_t)(__float_as_int(tv.x) - sb), iyb = (uint32_t)(__float_as_int(tv.y) - sb);
-    const float2 tx = __fadd2_rn(u, neg2(fu)), ty = __fadd2_rn(v, neg2(fv));
-    const size_t ra = (size_t)iya * w + ixa, rb = (size_t)iyb * w + ixb;
-    const float2 v00 = f2(pix<T>(p, ra), pix<T>(p, rb));
-    const float2 v10 = f2(pix<T>(p, ra + 1), pix<T>(p, rb + 1));
-    const float2 v01 = f2(pix<T>(p, ra + w), pix<T>(p, rb + w));
-    const float2 v11 = f2(pix<T>(p, ra + w + 1), pix<T>(p, rb + w + 1));
-    const float2 top = __ffma2_rn(__fadd2_rn(v10, neg2(v00)), tx, v00);
-    const float2 bot = __ffma2_rn(__fadd2_rn(v11, neg2(v01)), tx, v01);
-    return __ffma2_rn(__fadd2_rn(bot, neg2(top)), ty, top);
-}
-
 template <class T, int R>
 __device__ __forceinline__ void window_cost_zncc_pair(const float* pvc, float pm, float pvar,
                                                       const float* Ha, const float* Hb,
@@ -1183,13 +1210,13 @@ cudaError_t Typed<T>::sweep_tiled(const BatchDev& b, uint32_t max_nx, uint32_t m
         const int PX = (kTileX - 1) * s + W, PY = (kTileY - 1) * s + W;
         const size_t PXp = (size_t)((PX + s - 1) / s) * s, np = PXp * PY;
         const size_t smem = sizeof(double) * 3 * (size_t)PY * kTileX +
-                            sizeof(float) * (2 * np + PXp + (size_t)b.max_src * (256 + 12) +
+                            sizeof(float) * (2 * np + PXp + (size_t)b.max_src * (kTileThreads + 12) +
                                              (size_t)b.prof.planes);
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);
         if (e != cudaSuccess) return e;
         dim3 grid((max_nx + kTileX - 1) / kTileX, (max_ny + kTileY - 1) / kTileY, b.n_refs);
-        kern<<<grid, 256, smem, st>>>(b, 0, rank, status, ctr);
+        kern<<<grid, kTileThreads, smem, st>>>(b, 0, rank, status, ctr);
         return cudaGetLastError();
     };
     switch (b.prof.radius) {
