@@ -4,7 +4,7 @@
 // device straight into one page-locked block, and every per-reference result
 // of the batch points into it.  The block is reference counted (one count per
 // PassResult copy, per C result and per mesh result); when the last holder
-// lets go it returns to a small process-wide cache instead of being unpinned.
+// lets go it returns to a process-wide cache instead of being unpinned.
 // A fresh block is pinned together with a spare of its size, so a caller that
 // keeps one call's results while it makes the next alternates between two
 // blocks and never pins (or page-faults) again.
@@ -18,12 +18,23 @@
 namespace v3d {
 namespace {
 
-constexpr size_t kBlockAlign = size_t{2} << 20;  // sizes rounded to 2 MiB
-constexpr size_t kCachedBlocks = 4;               // blocks kept for reuse
+// Blocks come in power-of-two sizes from 2 MiB, so results of varying size
+// (one small request after another in a serving loop) share a few classes.
+constexpr size_t kMinBlock = size_t{2} << 20;
+// Bytes of free blocks kept pinned: unpinning waits for the device, so the
+// cache lets go of blocks only beyond this.
+constexpr size_t kCachedBytes = size_t{2} << 30;
+
+size_t size_class(size_t bytes) {
+    size_t c = kMinBlock;
+    while (c < bytes) c <<= 1;
+    return c;
+}
 
 struct BlockCache {
     std::mutex mu;
     std::multimap<size_t, void*> free;  // bytes -> block
+    size_t free_bytes = 0;
 };
 
 // Never destroyed: holders may release blocks during static destruction.
@@ -38,10 +49,13 @@ void recycle(void* p, size_t bytes) {
     {
         std::lock_guard<std::mutex> lock(c.mu);
         c.free.emplace(bytes, p);
-        if (c.free.size() > kCachedBlocks) {
-            // keep the largest blocks; unpin the smallest
-            auto it = c.free.begin();
+        c.free_bytes += bytes;
+        if (c.free_bytes > kCachedBytes && c.free.size() > 1) {
+            // unpin the largest other block: the cap is about bytes
+            auto it = std::prev(c.free.end());
+            if (it->second == p) --it;
             drop = it->second;
+            c.free_bytes -= it->first;
             c.free.erase(it);
         }
     }
@@ -57,18 +71,18 @@ struct BlockRecycler {
 }  // namespace
 
 HostBlock host_block(size_t bytes) {
-    bytes = (bytes + kBlockAlign - 1) / kBlockAlign * kBlockAlign;
-    if (bytes == 0) bytes = kBlockAlign;
+    bytes = size_class(bytes);
     BlockCache& c = cache();
     void* p = nullptr;
     size_t have = 0;
     {
         std::lock_guard<std::mutex> lock(c.mu);
-        // the smallest cached block that fits, unless it wastes more than 4x
+        // the smallest cached block that fits, at most two classes up
         auto it = c.free.lower_bound(bytes);
         if (it != c.free.end() && it->first <= 4 * bytes) {
             p = it->second;
             have = it->first;
+            c.free_bytes -= it->first;
             c.free.erase(it);
         }
     }

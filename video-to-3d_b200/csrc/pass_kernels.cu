@@ -363,18 +363,37 @@ cudaError_t launch_site_ref(const uint64_t* site_off, int32_t n_refs, uint64_t t
     return cudaGetLastError();
 }
 
+namespace {
+// Folds the plane chunks of every pending site in plane order and applies the gates.
+__global__ void k_merge_chunks(DevProfile prof, uint64_t total, int n, const Rank* __restrict__ partial,
+                               SiteRank* __restrict__ rank, uint8_t* __restrict__ status) {
+    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < total;
+         g += (uint64_t)gridDim.x * blockDim.x) {
+        if (status[g] != kSitePending) continue;
+        Rank st = partial[g];
+        for (int c = 1; c < n; ++c) st = rank_merge(st, partial[(uint64_t)c * total + g]);
+        finish_site(st, prof, g, rank, status);
+    }
+}
+}  // namespace
+
 cudaError_t launch_sweep_dispatch(const BatchDev& b, const uint32_t* site_ref, uint64_t total_sites,
                                   uint32_t max_nx, uint32_t max_ny, uint32_t uniform_stride,
                                   bool tiled, SiteRank* rank, uint8_t* status,
-                                  RefCounters* counters, cudaStream_t stream) {
+                                  RefCounters* counters, cudaStream_t stream, SweepChunks chunks) {
     if (!total_sites) return cudaSuccess;
-    return by_storage(b.storage, [&](auto t) {
+    if (!tiled) chunks = SweepChunks{};
+    cudaError_t e = by_storage(b.storage, [&](auto t) {
         using T = decltype(t);
         if (tiled)
             return Typed<T>::sweep_tiled(b, max_nx, max_ny, uniform_stride, rank, status,
-                                         counters, stream);
+                                         counters, stream, total_sites, chunks);
         return Typed<T>::sweep_site(b, site_ref, total_sites, rank, status, counters, stream);
     });
+    if (e != cudaSuccess || chunks.n <= 1) return e;
+    k_merge_chunks<<<grid_for(total_sites, 256), 256, 0, stream>>>(b.prof, total_sites, chunks.n,
+                                                                chunks.partial, rank, status);
+    return cudaGetLastError();
 }
 
 size_t compaction_scratch_bytes(uint64_t n) {

@@ -16,6 +16,7 @@ enum SiteStatus : uint8_t {
     kSiteNoCandidate = 2,  // no hypothesis had a passing source view
     kSiteGateRejected = 3, // photometric or ambiguity gate (dense_legacy.rs:350-362)
     kSiteAccepted = 4,     // goes to the reciprocal check
+    kSitePending = 5,      // swept in plane chunks, waiting for their merge
 };
 
 struct SiteRank {
@@ -116,12 +117,44 @@ cudaError_t launch_luma(const uint8_t* rgba, uint8_t* luma, size_t pixels, cudaS
 cudaError_t launch_site_ref(const uint64_t* site_off, int32_t n_refs, uint64_t total_sites,
                             uint32_t* site_ref, cudaStream_t stream);
 
+// Plane chunking of the tiled sweep: `n` CTAs per tile each sweep a
+// contiguous share of the hypotheses and leave their running rank state in
+// `partial` ([n][sites]); a merge folds the shares in plane order.  The rank
+// merge is associative and commutative over disjoint plane sets, so the
+// result is the one-CTA sweep's.
+struct SweepChunks {
+    int n = 1;
+    Rank* partial = nullptr;
+};
+
+// The gates of one swept site on its final rank state (dense_legacy.rs:332-362).
+__device__ __forceinline__ void finish_site(const Rank& st, const DevProfile& prof, uint64_t g,
+                                            SiteRank* rank, uint8_t* status) {
+    SiteRank out;
+    out.support = st.support;
+    out.plane = st.plane;
+    out.error = st.error;
+    out.margin = isinf(st.second) ? __longlong_as_double(0x7ff0000000000000LL)
+                                  : dsub(st.second, st.error);
+    uint8_t code;
+    if (st.support < 0)
+        code = kSiteNoCandidate;
+    else if (st.error > prof.max_error || out.margin < prof.min_margin)
+        code = kSiteGateRejected;
+    else
+        code = kSiteAccepted;
+    rank[g] = out;
+    status[g] = code;
+}
+
 // `tiled` selects the box-filter ZNCC sweep (fast policy, all references share
-// `uniform_stride`); otherwise the warp-per-site sweep runs.
+// `uniform_stride`, optionally in plane chunks); otherwise the warp-per-site
+// sweep runs.
 cudaError_t launch_sweep_dispatch(const BatchDev& b, const uint32_t* site_ref,
                                   uint64_t total_sites, uint32_t max_nx, uint32_t max_ny,
                                   uint32_t uniform_stride, bool tiled, SiteRank* rank,
-                                  uint8_t* status, RefCounters* counters, cudaStream_t stream);
+                                  uint8_t* status, RefCounters* counters, cudaStream_t stream,
+                                  SweepChunks chunks = SweepChunks{});
 
 // Order-preserving compaction of indices i in [0, n) with flags[i] == value.
 // `scratch` needs compaction_scratch_bytes(n) bytes; *count_dev gets the count.

@@ -136,6 +136,8 @@ struct Prepared {
     uint64_t total = 0, cap = 1;
     uint32_t max_nx = 0, max_ny = 0, stride0 = 0;
     bool tiled = false;
+    int chunks = 1;             // plane chunks of the tiled sweep
+    Rank* d_partial = nullptr;  // [chunks][sites] when chunks > 1
     BatchDev b{};
     uint32_t* d_siteref = nullptr;
     SiteRank* d_rank = nullptr;
@@ -220,6 +222,34 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
     }
     const uint64_t total = site_off[n_active];
     const uint64_t cap = std::max<uint64_t>(total, 1);
+    // the box-filter sweep and, for batches of few tiles, its plane chunks:
+    // enough CTAs for two waves of four per SM, at least 4 hypotheses a chunk
+    {
+        const uint32_t s0 = plans[active[0]].stride;
+        const int w = 2 * prof.patch_radius + 1;
+        P.tiled = prof.precision != V3D_PRECISION_EXACT64 && prof.cost == V3D_COST_ZNCC &&
+                  uniform_stride && s0 >= 1 && s0 <= 4 && static_cast<int>(s0) < w;
+        P.chunks = 1;
+        if (P.tiled) {
+            uint64_t tiles = 0;
+            int min_planes = kMaxPlanes;
+            for (size_t k = 0; k < n_active; ++k) {
+                const RefPlan& p = plans[active[k]];
+                tiles += static_cast<uint64_t>((p.nx + 31) / 32) * ((p.ny + 7) / 8);
+                min_planes = std::min(min_planes, p.planes);
+            }
+            static int sms = 0;
+            if (!sms && cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device) != cudaSuccess) {
+                cudaGetLastError();
+                sms = 148;
+            }
+            const uint64_t target = static_cast<uint64_t>(sms) * 8;
+            if (tiles && tiles < target) {
+                const uint64_t want = (target + tiles - 1) / tiles;
+                P.chunks = static_cast<int>(std::min<uint64_t>({want, 16, static_cast<uint64_t>(std::max(1, min_planes / 4))}));
+            }
+        }
+    }
     P.n_active = n_active;
     P.total = total;
     P.cap = cap;
@@ -246,6 +276,7 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
     const size_t o_siteref = cv.take<uint32_t>(cap);
     const size_t o_rank = cv.take<SiteRank>(cap);
     const size_t o_status = cv.take<uint8_t>(cap);
+    const size_t o_partial = cv.take<Rank>(P.chunks > 1 ? static_cast<uint64_t>(P.chunks) * cap : 1);
     const size_t o_ctr = cv.take<RefCounters>(n_active);
     const uint64_t pc = sweep_only ? 1 : cap;  // pass buffers are not needed for the sweep alone
     const size_t o_scratch = cv.take<uint8_t>(compaction_scratch_bytes(pc));
@@ -369,6 +400,7 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
     V3D_CK(cudaMemcpyAsync(at(o_srcinv), hinv, sizeof(float) * inv_count, cudaMemcpyHostToDevice,
                            stream));
 
+    P.d_partial = P.chunks > 1 ? reinterpret_cast<Rank*>(at(o_partial)) : nullptr;
     auto* d_siteref = P.d_siteref = reinterpret_cast<uint32_t*>(at(o_siteref));
     P.d_rank = reinterpret_cast<SiteRank*>(at(o_rank));
     auto* d_status = P.d_status = reinterpret_cast<uint8_t*>(at(o_status));
@@ -426,11 +458,7 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
     b.prof.min_variance = prof.min_window_variance;
     b.exact = prof.precision == V3D_PRECISION_EXACT64;
 
-    const uint32_t stride0 = plans[active[0]].stride;
-    const int W = 2 * prof.patch_radius + 1;
-    P.stride0 = stride0;
-    P.tiled = !b.exact && prof.cost == V3D_COST_ZNCC && uniform_stride && stride0 >= 1 &&
-              stride0 <= 4 && static_cast<int>(stride0) < W;
+    P.stride0 = plans[active[0]].stride;
     return V3D_OK;
 }
 
@@ -572,6 +600,7 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
     // completion pass propose, compaction (3), gather, reciprocal, fuse,
     // compaction (3), append (2), occupancy
     ctx->last_launches = 1 + 3 + 1 + 1 + 1 + 3 + 2 + 2 + 2 * (1 + 3 + 1 + 1 + 1 + 3 + 2 + 1);
+    if (P.chunks > 1) ctx->last_launches += 1;  // the chunk merge
     ctx->last_sites = total;
     ctx->last_units = 0;
     for (size_t k = 0; k < n_active; ++k) {
@@ -586,7 +615,7 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
     // primary sweep, reciprocal check and fusion
     cudaEventRecord(es[0], stream);
     V3D_CK(launch_sweep_dispatch(b, d_siteref, total, max_nx, max_ny, stride0, tiled, d_rank,
-                                 d_status, d_ctr, stream));
+                                 d_status, d_ctr, stream, SweepChunks{P.chunks, P.d_partial}));
     cudaEventRecord(es[1], stream);
     V3D_CK(launch_compact(d_status, kSiteAccepted, total, d_idx, c_cand, d_scratch, stream));
     V3D_CK(launch_make_primary_cands(b, d_idx, c_cand, cap, d_siteref, d_rank, d_cands, stream));
@@ -912,7 +941,8 @@ int32_t run_sweep_records(v3d_context* ctx, const v3d_profile& prof, const v3d_f
     int32_t pst = prepare(ctx, prof, frames, n_frames, focal, plans, {0}, true, P);
     if (pst != V3D_OK) return pst;
     V3D_CK(launch_sweep_dispatch(P.b, P.d_siteref, P.total, P.max_nx, P.max_ny, P.stride0, P.tiled,
-                                 P.d_rank, P.d_status, P.d_ctr, stream));
+                                 P.d_rank, P.d_status, P.d_ctr, stream,
+                                 SweepChunks{P.chunks, P.d_partial}));
     std::vector<SiteRank> rank(P.total);
     std::vector<uint8_t> status(P.total);
     if (P.total) {

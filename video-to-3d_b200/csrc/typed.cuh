@@ -13,7 +13,8 @@ struct Typed {
                                   cudaStream_t st);
     static cudaError_t sweep_tiled(const BatchDev& b, uint32_t max_nx, uint32_t max_ny,
                                    uint32_t stride, SiteRank* rank, uint8_t* status,
-                                   RefCounters* ctr, cudaStream_t st);
+                                   RefCounters* ctr, cudaStream_t st, uint64_t total_sites,
+                                   SweepChunks chunks);
     static cudaError_t reciprocal(const BatchDev& b, const Cand* cands, const uint32_t* count,
                                   RecipObs* obs, RefCounters* ctr, cudaStream_t st);
     static cudaError_t propose(const BatchDev& b, int pass, uint64_t total,

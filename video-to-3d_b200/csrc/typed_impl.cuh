@@ -295,18 +295,23 @@ __global__ void __launch_bounds__(256) k_sweep_site(BatchDev b, const uint32_t* 
 // footprint's x coordinates come from a per-slot table, so the warp step
 // converts no integers.
 template <class T, int R>
-__global__ void __launch_bounds__(kTileThreads) k_sweep_tiled(BatchDev b, uint64_t total_sites_unused,
+__global__ void __launch_bounds__(kTileThreads) k_sweep_tiled(BatchDev b, uint64_t total_sites,
                                                      SiteRank* __restrict__ rank,
                                                      uint8_t* __restrict__ status,
-                                                     RefCounters* __restrict__ ctr) {
+                                                     RefCounters* __restrict__ ctr, int n_chunks,
+                                                     Rank* __restrict__ partial) {
     constexpr int W = 2 * R + 1;
     constexpr int N = W * W;
     extern __shared__ double smem_d[];
-    const uint32_t r = blockIdx.z;
+    // blockIdx.z = reference x plane chunk; the chunk sweeps planes [k0, k1)
+    const uint32_t r = blockIdx.z / (uint32_t)n_chunks;
+    const int chunk = (int)(blockIdx.z - r * (uint32_t)n_chunks);
     const DevReference& ref = b.refs[r];
     const DevProfile& prof = b.prof;
     const uint32_t gx0 = blockIdx.x * kTileX, gy0 = blockIdx.y * kTileY;
     if (gx0 >= ref.nx || gy0 >= ref.ny) return;
+    const int per_chunk = (ref.planes + n_chunks - 1) / n_chunks;
+    const int k0 = chunk * per_chunk, k1 = min(ref.planes, k0 + per_chunk);
     const int s = (int)ref.stride;
     const int PX = (kTileX - 1) * s + W, PY = (kTileY - 1) * s + W;
     const int PXs = (PX + s - 1) / s, PXp = PXs * s;  // columns per residue, padded row
@@ -370,8 +375,10 @@ __global__ void __launch_bounds__(kTileThreads) k_sweep_tiled(BatchDev b, uint64
             }
         double contrast = (double)mx - (double)mn;
         sampled = contrast >= prof.min_contrast;
-        if (!sampled) status[gsite] = kSiteLowContrast;
-        else atomicAdd(&ctr[r].sampled, 1ull);
+        if (chunk == 0) {  // one chunk records the gate
+            if (!sampled) status[gsite] = kSiteLowContrast;
+            else atomicAdd(&ctr[r].sampled, 1ull);
+        }
     }
     const double n = (double)N;
     const double inv_n = 1.0 / n;
@@ -380,7 +387,7 @@ __global__ void __launch_bounds__(kTileThreads) k_sweep_tiled(BatchDev b, uint64
     const bool vr_ok = vr > 0.0 && vr >= minvar_n;
     const float vr_f = (float)vr;
     Rank st = rank_empty();
-    for (int k = 0; k < ref.planes; ++k) {
+    for (int k = k0; k < k1; ++k) {
         const float inv = pinv[k];
         const float zmin = 1.0e-4f * inv;
         for (int j = 0; j < n_src; ++j) {
@@ -500,20 +507,12 @@ __global__ void __launch_bounds__(kTileThreads) k_sweep_tiled(BatchDev b, uint64
         }
     }
     if (!sampled) return;
-    SiteRank out;
-    out.support = st.support;
-    out.plane = st.plane;
-    out.error = st.error;
-    out.margin = isinf(st.second) ? kInf : dsub(st.second, st.error);
-    uint8_t code;
-    if (st.support < 0)
-        code = kSiteNoCandidate;
-    else if (st.error > prof.max_error || out.margin < prof.min_margin)
-        code = kSiteGateRejected;
-    else
-        code = kSiteAccepted;
-    rank[gsite] = out;
-    status[gsite] = code;
+    if (n_chunks > 1) {
+        partial[(uint64_t)chunk * total_sites + gsite] = st;
+        if (chunk == 0) status[gsite] = kSitePending;
+        return;
+    }
+    finish_site(st, prof, gsite, rank, status);
 }
 
 // ---- reciprocal check, warp per (candidate, source) ----------------------------
@@ -1203,7 +1202,8 @@ cudaError_t Typed<T>::sweep_site(const BatchDev& b, const uint32_t* site_ref, ui
 template <class T>
 cudaError_t Typed<T>::sweep_tiled(const BatchDev& b, uint32_t max_nx, uint32_t max_ny,
                                   uint32_t stride, SiteRank* rank, uint8_t* status,
-                                  RefCounters* ctr, cudaStream_t st) {
+                                  RefCounters* ctr, cudaStream_t st, uint64_t total_sites,
+                                  SweepChunks chunks) {
     using namespace typed_detail;
     auto run = [&](auto kern, int W) -> cudaError_t {
         const int s = (int)stride;
@@ -1215,8 +1215,10 @@ cudaError_t Typed<T>::sweep_tiled(const BatchDev& b, uint32_t max_nx, uint32_t m
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);
         if (e != cudaSuccess) return e;
-        dim3 grid((max_nx + kTileX - 1) / kTileX, (max_ny + kTileY - 1) / kTileY, b.n_refs);
-        kern<<<grid, kTileThreads, smem, st>>>(b, 0, rank, status, ctr);
+        const int n = chunks.n > 1 ? chunks.n : 1;
+        dim3 grid((max_nx + kTileX - 1) / kTileX, (max_ny + kTileY - 1) / kTileY,
+                  (unsigned)b.n_refs * (unsigned)n);
+        kern<<<grid, kTileThreads, smem, st>>>(b, total_sites, rank, status, ctr, n, chunks.partial);
         return cudaGetLastError();
     };
     switch (b.prof.radius) {
