@@ -295,7 +295,7 @@ __global__ void __launch_bounds__(256) k_sweep_site(BatchDev b, const uint32_t* 
 // footprint's x coordinates come from a per-slot table, so the warp step
 // converts no integers.
 template <class T, int R>
-__global__ void __launch_bounds__(kTileThreads) k_sweep_tiled(BatchDev b, uint64_t total_sites,
+__global__ void __launch_bounds__(kTileThreads, 1024 / kTileThreads) k_sweep_tiled(BatchDev b, uint64_t total_sites,
                                                      SiteRank* __restrict__ rank,
                                                      uint8_t* __restrict__ status,
                                                      RefCounters* __restrict__ ctr, int n_chunks,
