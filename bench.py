@@ -308,6 +308,7 @@ def run_ours(args, rank, world, local):
                     "d2h_bytes_per_step": points * 72 + triangles * 32,
                     "ms_per_step": wall_s * 1e3},
             "gpu_launches": infos[-1]["kernel_launches"],
+            "sweep_chunks": infos[-1]["sweep_chunks"],
             "stages_ms": {"sweep": sweep_ms, "reciprocal_primary": recip_ms,
                           "completion": comp_ms, "mesh": mesh_ms, "total": dev_s * 1e3,
                           **host},

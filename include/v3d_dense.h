@@ -459,6 +459,7 @@ typedef struct v3d_run_info {
     double host_block_ms;     /* acquiring the pinned result block (within host_wait_ms) */
     double host_readback_ms;  /* result copies into that block (within host_wait_ms) */
     uint64_t result_bytes;    /* bytes of that block the results occupy */
+    uint64_t sweep_chunks;    /* plane chunks of the box-filtered sweep (1: none) */
 } v3d_run_info;
 
 int32_t v3d_last_run_info(const v3d_context* ctx, v3d_run_info* out);

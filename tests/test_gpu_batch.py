@@ -84,3 +84,24 @@ def test_uneven_clips_exact_policy_matches_the_oracle(oracle):
             assert (g is None) == (w is None)
             if g is not None:
                 _same(g, w)
+
+
+@pytest.mark.gpu
+def test_sweep_chunk_tuning_never_changes_results():
+    """The tiled sweep's plane chunking is tuned on live calls; whatever chunk
+    count a call runs with, its results are the same bit for bit."""
+    clip = synth.make_clip(232, 130, 5, 15.0, 1.2, 31, landmark_cameras=[2],
+                           landmarks_per_camera=400)
+    frames = clip.frames("f32")
+    prof = profiles.zncc(2, 48, 4, 2)
+    ctx = dense.Context(0)
+    outs, chunks = [], []
+    for _ in range(6):
+        outs.append(ctx.reconstruct_reference_patches(frames, clip.cameras, clip.sparse,
+                                                      clip.focal, [2], profile=prof)[0])
+        chunks.append(ctx.last_run_info()["sweep_chunks"])
+    assert len(outs[0].points) > 0
+    for o in outs[1:]:
+        _same(o, outs[0])
+    assert len(set(chunks)) >= 2          # candidates were tried
+    assert chunks[-1] == chunks[-2] > 1   # and one was kept (a small batch chunks)

@@ -245,6 +245,7 @@ int32_t v3d_last_run_info(const v3d_context* ctx, v3d_run_info* out) {
     out->host_block_ms = ctx->last_block_ms;
     out->host_readback_ms = ctx->last_readback_ms;
     out->result_bytes = ctx->last_result_bytes;
+    out->sweep_chunks = ctx->last_chunks;
     return V3D_OK;
 }
 

@@ -118,6 +118,18 @@ struct ClipJob {
 Inputs load_inputs(const v3d_frame* frames, uint64_t n_frames, const v3d_camera* cams,
                    uint64_t n_cams, const double* sparse, uint64_t n_sparse, double focal);
 
+// ---- launch-shape tuning of the tiled sweep (sweep_tuner.cpp) ----
+struct SweepShapeKey {
+    int device, radius, stride, tiles, planes, sources;  // the last three as log2 buckets
+};
+SweepShapeKey sweep_shape_key(int device, int radius, int stride, uint64_t tiles, int planes,
+                              int sources);
+// Plane chunks to run for a batch of this shape: a candidate while the shape
+// is being measured, then the fastest one.
+int sweep_chunks_pick(const SweepShapeKey& key, int heuristic, int max_chunks);
+// Sweep device time of a batch run with `chunks`, over `units` window costs.
+void sweep_chunks_record(const SweepShapeKey& key, int chunks, double sweep_ms, uint64_t units);
+
 // ---- planning (host_plan.cpp) ----
 uint32_t reference_grid_stride(uint32_t w, uint32_t h, bool fine);
 HVec3 camera_center(const HCamera& c);
@@ -174,6 +186,7 @@ struct v3d_context {
     uint64_t last_triangles = 0;
     double last_block_ms = 0, last_readback_ms = 0;
     uint64_t last_result_bytes = 0;
+    uint64_t last_chunks = 1;
 };
 
 namespace v3d {

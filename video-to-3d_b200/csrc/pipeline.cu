@@ -137,6 +137,7 @@ struct Prepared {
     uint32_t max_nx = 0, max_ny = 0, stride0 = 0;
     bool tiled = false;
     int chunks = 1;             // plane chunks of the tiled sweep
+    SweepShapeKey shape{};      // its launch-shape key for the tuner
     Rank* d_partial = nullptr;  // [chunks][sites] when chunks > 1
     BatchDev b{};
     uint32_t* d_siteref = nullptr;
@@ -244,10 +245,16 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
                 sms = 148;
             }
             const uint64_t target = static_cast<uint64_t>(sms) * 8;
-            if (tiles && tiles < target) {
-                const uint64_t want = (target + tiles - 1) / tiles;
-                P.chunks = static_cast<int>(std::min<uint64_t>({want, 16, static_cast<uint64_t>(std::max(1, min_planes / 4))}));
-            }
+            const int max_chunks = std::max(1, std::min(16, min_planes / 4));
+            int heuristic = 1;
+            if (tiles && tiles < target)
+                heuristic = static_cast<int>(std::min<uint64_t>((target + tiles - 1) / tiles, max_chunks));
+            int max_src = 1;
+            for (size_t k = 0; k < n_active; ++k)
+                max_src = std::max<int>(max_src, static_cast<int>(plans[active[k]].src_slots.size()));
+            P.shape = sweep_shape_key(ctx->device, prof.patch_radius, static_cast<int>(s0), tiles,
+                                      min_planes, max_src);
+            P.chunks = sweep_chunks_pick(P.shape, heuristic, max_chunks);
         }
     }
     P.n_active = n_active;
@@ -601,6 +608,7 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
     // compaction (3), append (2), occupancy
     ctx->last_launches = 1 + 3 + 1 + 1 + 1 + 3 + 2 + 2 + 2 * (1 + 3 + 1 + 1 + 1 + 3 + 2 + 1);
     if (P.chunks > 1) ctx->last_launches += 1;  // the chunk merge
+    ctx->last_chunks = static_cast<uint64_t>(P.chunks);
     ctx->last_sites = total;
     ctx->last_units = 0;
     for (size_t k = 0; k < n_active; ++k) {
@@ -735,6 +743,7 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
     V3D_CK(cudaStreamSynchronize(stream));
     cudaEventElapsedTime(&ctx->last_ms, ev0, ev1);
     cudaEventElapsedTime(&ctx->last_sweep_ms, es[0], es[1]);
+    if (P.tiled) sweep_chunks_record(P.shape, P.chunks, ctx->last_sweep_ms, ctx->last_units);
     cudaEventElapsedTime(&ctx->last_recip_ms, es[2], es[3]);
     cudaEventElapsedTime(&ctx->last_completion_ms, es[4], es[5]);
     ctx->last_mesh_ms = 0.f;

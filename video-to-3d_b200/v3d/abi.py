@@ -193,7 +193,8 @@ class RunInfo(C.Structure):
                 ("host_upload_ms", C.c_double), ("host_wait_ms", C.c_double),
                 ("host_assemble_ms", C.c_double), ("mesh_ms", C.c_double),
                 ("triangles", C.c_uint64), ("host_block_ms", C.c_double),
-                ("host_readback_ms", C.c_double), ("result_bytes", C.c_uint64)]
+                ("host_readback_ms", C.c_double), ("result_bytes", C.c_uint64),
+                ("sweep_chunks", C.c_uint64)]
 
 
 CANCEL_FN = C.CFUNCTYPE(C.c_int32, C.c_void_p)
