@@ -40,10 +40,10 @@ UNIT = "samples·planes·views/s"
 WIDTH, HEIGHT, FRAMES = 640, 360, 120
 RADIUS, PLANES, SOURCES, STRIDE = 3, 128, 8, 2
 # DRAM bytes per unit of the depth sweep (k_sweep_tiled), from one ncu capture of
-# the same workload cut to 12 keyframes (677.4 M units; 11.18 MB read + 0.01 MB
+# the same workload cut to 12 keyframes (677.4 M units; 11.12 MB read + 0.03 MB
 # written; profiles/k_sweep_tiled_zncc7x7_640x360_12kf.md).  A clip's frames live
 # in L2, so the sweep's DRAM traffic grows with its units.
-SWEEP_DRAM_BYTES_PER_UNIT = (11.183616e6 + 0.008704e6) / 677.376e6
+SWEEP_DRAM_BYTES_PER_UNIT = (11.121664e6 + 0.025856e6) / 677.376e6
 
 
 def parse():

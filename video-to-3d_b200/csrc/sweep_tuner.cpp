@@ -4,7 +4,8 @@
 // it can be tuned on live calls.  Batches are keyed by their launch shape
 // (window radius, stride, and the power-of-two buckets of their tile count,
 // hypothesis count and source count).  A key's first calls each try one
-// candidate: the occupancy heuristic's chunk count, half of it and twice it.
+// candidate: the occupancy heuristic's chunk count, twice and four times it
+// and half of it.
 // Every try records the sweep's device time per unit of work; once all
 // candidates have run, the key keeps the fastest.
 #include <map>
@@ -59,7 +60,7 @@ int sweep_chunks_pick(const SweepShapeKey& key, int heuristic, int max_chunks) {
     auto it = t.entries.find(k);
     if (it == t.entries.end()) {
         Entry e;
-        for (int c : {heuristic, heuristic / 2, heuristic * 2}) {
+        for (int c : {heuristic, heuristic * 2, heuristic * 4, heuristic / 2}) {
             c = std::max(1, std::min(c, max_chunks));
             bool seen = false;
             for (int d : e.candidates) seen = seen || d == c;
