@@ -327,6 +327,23 @@ def run_ours(args, rank, world, local):
             "points_per_step": points,
             "triangles_per_step": triangles,
         }
+        # the sweep's warped samples against the measured gather ceiling: a CTA
+        # warps its tile's footprint, PX x PY pixels, per (plane, source)
+        px = 31 * STRIDE + 2 * RADIUS + 1
+        py = 7 * STRIDE + 2 * RADIUS + 1
+        nx = (WIDTH - 2 * (RADIUS + 2) + STRIDE - 1) // STRIDE
+        ny = (HEIGHT - 2 * (RADIUS + 2) + STRIDE - 1) // STRIDE
+        tiles = ((nx + 31) // 32) * ((ny + 7) // 8)
+        samples = units * tiles * px * py / float(nx * ny)
+        rate = ctx.measure_gather_rate()
+        line["roofline_gather"] = {
+            "kernel": "k_sweep_tiled", "bound": "gather", "unit": "bilinear samples/s",
+            "achieved": samples / (sweep_ms / 1e3), "peak": rate,
+            "frac": samples / (sweep_ms / 1e3) / rate,
+            "note": "homography-warped f32 bilinear samples the depth sweep computes per second "
+                    "(each shared by the overlapping windows of its tile) against the rate a "
+                    "kernel doing only that step sustains on this GPU (v3d_measure_gather_rate); "
+                    "the rest of the sweep's time goes to its f64 box filters and ranking"}
         if world == 1 and not args.no_cpu_baseline:
             v, info = cpu_baseline(clip, frames, prof, os.cpu_count() or 1)
             line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": info["cores"],

@@ -464,6 +464,13 @@ typedef struct v3d_run_info {
 
 int32_t v3d_last_run_info(const v3d_context* ctx, v3d_run_info* out);
 
+/* Diagnostic with no counterpart in the reference: the rate of homography-
+ * warped f32 bilinear samples this GPU sustains when it does nothing else (the
+ * depth sweep's warp step alone, over CTA-sized footprints that stay in L1 and
+ * L2), for the gather roofline of the sweep.  Allocates and frees a 2 MiB
+ * image; about 0.1 s on a B200. */
+int32_t v3d_measure_gather_rate(v3d_context* ctx, double* samples_per_second);
+
 /* ---- Serving (no counterpart in the reference, which runs one call at a time) ----
  *
  * A device-resident request loop.  Clips (frames, cameras, landmarks) are

@@ -99,6 +99,8 @@ def library():
     L.v3d_server_wait.argtypes = [C.c_void_p, C.c_uint64, C.c_int64, _P(abi.DenseResult),
                                   _P(abi.MeshResult), _P(C.c_int32), _P(abi.RequestTiming)]
     L.v3d_server_wait.restype = C.c_int32
+    L.v3d_measure_gather_rate.argtypes = [C.c_void_p, _P(C.c_double)]
+    L.v3d_measure_gather_rate.restype = C.c_int32
     L.v3d_last_run_info.argtypes = [C.c_void_p, _P(abi.RunInfo)]
     L.v3d_last_run_info.restype = C.c_int32
     _lib = L
@@ -252,6 +254,12 @@ class Context:
             inp.n_sparse, float(focal), int(reference_views), int(fine_grid), C.byref(prof), fn,
             None, C.byref(out), C.byref(omitted)))
         return self._dense(out, st), bool(omitted.value)
+
+    def measure_gather_rate(self):
+        """Warped bilinear samples per second this GPU sustains alone (diagnostic)."""
+        rate = C.c_double()
+        self._check(self.lib.v3d_measure_gather_rate(self.handle, C.byref(rate)))
+        return rate.value
 
     def last_run_info(self):
         """Device time, kernel launches and work units of the last dense call."""
