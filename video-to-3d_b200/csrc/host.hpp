@@ -165,6 +165,7 @@ void skip_result(PassResult& r, int code, const std::string& reason);
 
 struct v3d_context {
     int device = 0;
+    int sm_count = 0;        // multiprocessors of `device`, read on first use
     void* stream = nullptr;  // cudaStream_t
     std::mutex mu;
     std::string last_error;

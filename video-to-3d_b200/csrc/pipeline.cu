@@ -239,12 +239,13 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
                 tiles += static_cast<uint64_t>((p.nx + 31) / 32) * ((p.ny + 7) / 8);
                 min_planes = std::min(min_planes, p.planes);
             }
-            static int sms = 0;
-            if (!sms && cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device) != cudaSuccess) {
+            if (!ctx->sm_count &&
+                cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount,
+                                       ctx->device) != cudaSuccess) {
                 cudaGetLastError();
-                sms = 148;
+                ctx->sm_count = 148;
             }
-            const uint64_t target = static_cast<uint64_t>(sms) * 8;
+            const uint64_t target = static_cast<uint64_t>(ctx->sm_count) * 8;
             const int max_chunks = std::max(1, std::min(16, min_planes / 4));
             int heuristic = 1;
             if (tiles && tiles < target)

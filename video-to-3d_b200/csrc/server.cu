@@ -37,8 +37,9 @@ namespace {
 // Device bytes of one batch per grid site and per reference: the arena of a
 // batch (site records, candidates, 16 reciprocal slots, fused and pooled
 // points, output arrays, mesh lattice and slots) comes to about 1.2 KB per
-// site with the mesh; these bounds round that up.
-constexpr uint64_t kBytesPerSite = 1536;
+// site with the mesh, plus up to 0.4 KB of plane-chunk rank states for
+// batches of few tiles; these bounds round that up.
+constexpr uint64_t kBytesPerSite = 2048;
 constexpr uint64_t kBytesPerReference = 64u << 10;
 constexpr uint64_t kDefaultBudget = 8ull << 30;
 constexpr size_t kPinnedStaging = 16u << 20;
