@@ -313,18 +313,20 @@ __global__ void k_gather_cands(const uint32_t* __restrict__ idx, const uint32_t*
 }
 
 
+// Multiprocessors of the current device when first asked (a thread-safe
+// static: server slots launch from several threads).
 int sm_count() {
-    static int sms = 0;
-    if (!sms) {
-        int dev = 0;
+    static const int sms = [] {
+        int dev = 0, n = 0;
         cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (sms <= 0) sms = 148;
-    }
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) {
+            cudaGetLastError();
+            n = 148;
+        }
+        return n;
+    }();
     return sms;
 }
-
-// Dispatch helpers over (storage type, exactness, radius).
 
 unsigned grid_for(uint64_t cap, int threads) {
     uint64_t blocks = (cap + threads - 1) / threads;

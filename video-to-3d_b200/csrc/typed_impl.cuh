@@ -1166,14 +1166,18 @@ __global__ void __launch_bounds__(128) k_propose(BatchDev b, int pass, uint64_t 
 }
 
 
+// Multiprocessors of the current device when first asked (a thread-safe
+// static: server slots launch from several threads).
 inline int sm_count() {
-    static int sms = 0;
-    if (!sms) {
-        int dev = 0;
+    static const int sms = [] {
+        int dev = 0, n = 0;
         cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (sms <= 0) sms = 148;
-    }
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) {
+            cudaGetLastError();
+            n = 148;
+        }
+        return n;
+    }();
     return sms;
 }
 
