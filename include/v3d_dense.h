@@ -88,6 +88,7 @@ typedef enum v3d_pixel_format {
     V3D_PIXEL_GRAY_BF16 = 3   /* width*height bfloat16 */
 } v3d_pixel_format;
 
+/* A frame holds fewer than 2^32 pixels (width * height). */
 typedef struct v3d_frame {
     uint32_t width;
     uint32_t height;

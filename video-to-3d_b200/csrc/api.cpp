@@ -58,9 +58,13 @@ bool valid_profile(const v3d_profile* p) {
 
 bool valid_frames(const v3d_frame* frames, uint64_t n) {
     if (n && !frames) return false;
-    for (uint64_t i = 0; i < n; ++i)
+    for (uint64_t i = 0; i < n; ++i) {
         if (frames[i].format < V3D_PIXEL_RGBA8 || frames[i].format > V3D_PIXEL_GRAY_BF16)
             return false;
+        // the kernels address pixels with 32-bit offsets
+        if (static_cast<uint64_t>(frames[i].width) * frames[i].height >= (uint64_t{1} << 32))
+            return false;
+    }
     return true;
 }
 

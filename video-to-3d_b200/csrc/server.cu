@@ -282,7 +282,8 @@ int32_t v3d_server_add_clip(v3d_server* s, const v3d_frame* frames, uint64_t n_f
     for (uint64_t i = 0; i < n_frames; ++i) {
         const v3d_frame& f = frames[i];
         if (f.format < V3D_PIXEL_RGBA8 || f.format > V3D_PIXEL_GRAY_BF16 || !f.data ||
-            f.width == 0 || f.height == 0)
+            f.width == 0 || f.height == 0 ||
+            static_cast<uint64_t>(f.width) * f.height >= (uint64_t{1} << 32))  // 32-bit offsets
             return V3D_ERR_INVALID_ARGUMENT;
         if (f.format != frames[0].format) return V3D_ERR_INVALID_ARGUMENT;
     }

@@ -161,9 +161,11 @@ __device__ __forceinline__ float sample_nonneg(const T* __restrict__ p, uint32_t
     const uint32_t ix = (uint32_t)(__float_as_int(tu) - __float_as_int(kShift));
     const uint32_t iy = (uint32_t)(__float_as_int(tv) - __float_as_int(kShift));
     const float tx = u - fu, ty = v - fv;
-    const size_t r0 = (size_t)iy * w + ix;
-    const float v00 = pix<T>(p, r0), v10 = pix<T>(p, r0 + 1);
-    const float v01 = pix<T>(p, r0 + w), v11 = pix<T>(p, r0 + w + 1);
+    // 32-bit element offsets (frames hold fewer than 2^32 pixels): each row's
+    // address is then one wide multiply-add from the image base
+    const uint32_t o0 = iy * w + ix, o1 = o0 + w;
+    const float v00 = pix<T>(p + o0, 0), v10 = pix<T>(p + o0, 1);
+    const float v01 = pix<T>(p + o1, 0), v11 = pix<T>(p + o1, 1);
     const float top = fmaf(v10 - v00, tx, v00);
     const float bot = fmaf(v11 - v01, tx, v01);
     return fmaf(bot - top, ty, top);
@@ -186,11 +188,12 @@ __device__ __forceinline__ float2 sample_nonneg_pair(const T* __restrict__ p, ui
     const uint32_t ixa = (uint32_t)(__float_as_int(tu.x) - sb), ixb = (uint32_t)(__float_as_int(tu.y) - sb);
     const uint32_t iya = (uint32_t)(__float_as_int(tv.x) - sb), iyb = (uint32_t)(__float_as_int(tv.y) - sb);
     const float2 tx = __fadd2_rn(u, neg2(fu)), ty = __fadd2_rn(v, neg2(fv));
-    const size_t ra = (size_t)iya * w + ixa, rb = (size_t)iyb * w + ixb;
-    const float2 v00 = f2(pix<T>(p, ra), pix<T>(p, rb));
-    const float2 v10 = f2(pix<T>(p, ra + 1), pix<T>(p, rb + 1));
-    const float2 v01 = f2(pix<T>(p, ra + w), pix<T>(p, rb + w));
-    const float2 v11 = f2(pix<T>(p, ra + w + 1), pix<T>(p, rb + w + 1));
+    const uint32_t oa = iya * w + ixa, ob = iyb * w + ixb;  // as in sample_nonneg
+    const T *qa0 = p + oa, *qb0 = p + ob, *qa1 = p + (oa + w), *qb1 = p + (ob + w);
+    const float2 v00 = f2(pix<T>(qa0, 0), pix<T>(qb0, 0));
+    const float2 v10 = f2(pix<T>(qa0, 1), pix<T>(qb0, 1));
+    const float2 v01 = f2(pix<T>(qa1, 0), pix<T>(qb1, 0));
+    const float2 v11 = f2(pix<T>(qa1, 1), pix<T>(qb1, 1));
     const float2 top = __ffma2_rn(__fadd2_rn(v10, neg2(v00)), tx, v00);
     const float2 bot = __ffma2_rn(__fadd2_rn(v11, neg2(v01)), tx, v01);
     return __ffma2_rn(__fadd2_rn(bot, neg2(top)), ty, top);
