@@ -463,13 +463,88 @@ cudaError_t launch_occupy(const BatchDev& b, const OutPoint* pool, const uint32_
     return cudaGetLastError();
 }
 
+namespace {
+// First stage of a completion pass (dense_legacy.rs:551-599): every empty site
+// with at least 3 occupied grid neighbours whose depths spread by at most 6 %
+// becomes a seed with its predicted depth (surface_depth_prediction,
+// dense_legacy.rs:739-753) and its neighbours' mean confidence and margin.
+__global__ void k_propose_seed(BatchDev b, int pass, uint64_t total,
+                               const uint32_t* __restrict__ site_ref,
+                               const int32_t* __restrict__ occ, const OutPoint* __restrict__ pool,
+                               uint8_t* __restrict__ prop_status, Cand* __restrict__ prop,
+                               RefCounters* __restrict__ ctr) {
+    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < total;
+         g += (uint64_t)gridDim.x * blockDim.x) {
+        prop_status[g] = kPropNone;
+        const uint32_t r = site_ref[g];
+        const DevReference& ref = b.refs[r];
+        if (ref.n_src == 0 || ref.stride == 0) continue;
+        if (pass > 0 && ctr[r].pass_additions[pass - 1] == 0) continue;
+        if (occ[g] >= 0) continue;
+        const uint32_t local = (uint32_t)(g - b.site_off[r]);
+        const uint32_t gy = local / ref.nx, gx = local - gy * ref.nx;
+        double depths[8], confs[8], margins[8];
+        int n = 0;
+        for (int oy = -1; oy <= 1; ++oy)
+            for (int ox = -1; ox <= 1; ++ox) {
+                if (ox == 0 && oy == 0) continue;
+                int ngx = (int)gx + ox, ngy = (int)gy + oy;
+                if (ngx < 0 || ngy < 0 || ngx >= (int)ref.nx || ngy >= (int)ref.ny) continue;
+                int32_t pi = occ[b.site_off[r] + (uint64_t)ngy * ref.nx + ngx];
+                if (pi < 0) continue;
+                const OutPoint& pt = pool[pi];
+                D3 pos{(double)pt.p.x, (double)pt.p.y, (double)pt.p.z};
+                D3 q;
+                if (!project_exact(ref.cam, pos, ref.img.width, ref.img.height, ref.focal, q))
+                    continue;
+                depths[n] = q.z;
+                confs[n] = (double)pt.p.confidence;
+                margins[n] = (double)pt.a.depth_margin;
+                ++n;
+            }
+        if (n < kMinSurfaceNeighbors) continue;
+        double sorted[8];
+        for (int i = 0; i < n; ++i) sorted[i] = depths[i];
+        const double predicted = median_of(sorted, n);
+        const double mn = sorted[0], mx = sorted[n - 1];
+        if (!isfinite(mn) || !isfinite(mx) || mn <= 0.0 || mx <= 0.0) continue;
+        if (ddiv(dsub(mx, mn), mx) > kMaxSurfaceNeighborSpread) continue;
+        atomicAdd(&ctr[r].proposals, 1ull);
+        double csum = 0.0, msum = 0.0;
+        for (int i = 0; i < n; ++i) csum = dadd(csum, confs[i]);
+        for (int i = 0; i < n; ++i) msum = dadd(msum, margins[i]);
+        Cand cd;
+        cd.ref = r;
+        cd.site = local;
+        cd.x = ref.border + gx * ref.stride;
+        cd.y = ref.border + gy * ref.stride;
+        cd.pos = D3{0, 0, 0};
+        cd.depth = predicted;
+        cd.error = 0.0;
+        cd.margin = ddiv(msum, (double)n);
+        cd.nconf = ddiv(csum, (double)n);
+        cd.support = 0;
+        cd.pad = 0;
+        prop[g] = cd;
+        prop_status[g] = kPropSeed;
+    }
+}
+}  // namespace
+
 cudaError_t launch_propose(const BatchDev& b, int pass, uint64_t total_sites,
                            const uint32_t* site_ref, const int32_t* occ, const OutPoint* pool,
                            uint8_t* prop_status, Cand* prop_cand, RefCounters* counters,
+                           uint32_t* seed_idx, uint32_t* seed_count, void* scratch,
                            cudaStream_t stream) {
     if (!total_sites) return cudaSuccess;
+    k_propose_seed<<<grid_for(total_sites, 256), 256, 0, stream>>>(
+        b, pass, total_sites, site_ref, occ, pool, prop_status, prop_cand, counters);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    e = launch_compact(prop_status, kPropSeed, total_sites, seed_idx, seed_count, scratch, stream);
+    if (e != cudaSuccess) return e;
     return by_storage(b.storage, [&](auto t) {
-        return Typed<decltype(t)>::propose(b, pass, total_sites, site_ref, occ, pool, prop_status,
+        return Typed<decltype(t)>::propose(b, seed_idx, seed_count, total_sites, prop_status,
                                            prop_cand, counters, stream);
     });
 }

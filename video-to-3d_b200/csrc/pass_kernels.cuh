@@ -96,6 +96,7 @@ enum PropStatus : uint8_t {
     kPropTexture = 1,
     kPropCrossView = 2,
     kPropCandidate = 3,
+    kPropSeed = 4,        // passed the neighbour tests, its costs still to come
 };
 
 struct BatchDev {
@@ -187,9 +188,14 @@ cudaError_t launch_occupancy_clear(int32_t* occ, uint64_t total_sites, cudaStrea
 cudaError_t launch_occupy(const BatchDev& b, const OutPoint* pool, const uint32_t* begin,
                           const uint32_t* end, uint64_t cap, int32_t* occ, cudaStream_t stream);
 
+// complete_surface_samples (dense_legacy.rs:542-650) proposals of one pass, in
+// two stages: a thread per site for the neighbour tests, then, over the
+// compacted seeds (seed_idx, *seed_count, `scratch` for the compaction), a
+// thread per seed for the contrast and cross-view costs.
 cudaError_t launch_propose(const BatchDev& b, int pass, uint64_t total_sites,
                            const uint32_t* site_ref, const int32_t* occ, const OutPoint* pool,
                            uint8_t* prop_status, Cand* prop_cand, RefCounters* counters,
+                           uint32_t* seed_idx, uint32_t* seed_count, void* scratch,
                            cudaStream_t stream);
 
 cudaError_t launch_gather_cands(const uint32_t* idx, const uint32_t* count_dev, uint64_t cap,

@@ -607,7 +607,7 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
     // candidates, reciprocal, fuse, append (2), occupancy (2), then per
     // completion pass propose, compaction (3), gather, reciprocal, fuse,
     // compaction (3), append (2), occupancy
-    ctx->last_launches = 1 + 3 + 1 + 1 + 1 + 3 + 2 + 2 + 2 * (1 + 3 + 1 + 1 + 1 + 3 + 2 + 1);
+    ctx->last_launches = 1 + 3 + 1 + 1 + 1 + 3 + 2 + 2 + 2 * (5 + 3 + 1 + 1 + 1 + 3 + 2 + 1);
     if (P.chunks > 1) ctx->last_launches += 1;  // the chunk merge
     ctx->last_chunks = static_cast<uint64_t>(P.chunks);
     ctx->last_sites = total;
@@ -642,7 +642,7 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
     cudaEventRecord(es[4], stream);
     for (int pass = 0; pass < 2; ++pass) {
         V3D_CK(launch_propose(b, pass, total, d_siteref, d_occ, d_pool, d_pstat, d_prop, d_ctr,
-                              stream));
+                              d_idx, P.d_counts + 8, d_scratch, stream));
         V3D_CK(launch_compact(d_pstat, kPropCandidate, total, d_idx, c_cand, d_scratch, stream));
         V3D_CK(launch_gather_cands(d_idx, c_cand, cap, d_prop, d_cands, stream));
         V3D_CK(launch_reciprocal(b, d_cands, c_cand, cap, d_obs, d_ctr, stream));

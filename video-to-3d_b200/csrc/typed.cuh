@@ -17,10 +17,9 @@ struct Typed {
                                    SweepChunks chunks);
     static cudaError_t reciprocal(const BatchDev& b, const Cand* cands, const uint32_t* count,
                                   RecipObs* obs, RefCounters* ctr, cudaStream_t st);
-    static cudaError_t propose(const BatchDev& b, int pass, uint64_t total,
-                               const uint32_t* site_ref, const int32_t* occ,
-                               const OutPoint* pool, uint8_t* prop_status, Cand* prop,
-                               RefCounters* ctr, cudaStream_t st);
+    static cudaError_t propose(const BatchDev& b, const uint32_t* seed_idx,
+                               const uint32_t* seed_count, uint64_t total, uint8_t* prop_status,
+                               Cand* prop, RefCounters* ctr, cudaStream_t st);
 };
 
 extern template struct Typed<uint8_t>;

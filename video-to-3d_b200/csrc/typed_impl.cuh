@@ -1060,55 +1060,30 @@ __global__ void __launch_bounds__(256, 2) k_recip_sweep(BatchDev b, const Cand* 
 }
 
 
-// ---- surface completion proposals (dense_legacy.rs:542-650) ------------------
+// ---- surface completion proposals (dense_legacy.rs:600-650) ------------------
+// Second stage of a completion pass, a thread per seed left by the first stage
+// (the seed Cand holds the site, the predicted depth and the neighbours' mean
+// margin and confidence): the reference window's contrast, then the predicted
+// point's cost in every source view.  Seeds are compacted in site order, so the
+// warps run full.
 template <class T, bool EXACT, int R, int COST>
-__global__ void __launch_bounds__(128) k_propose(BatchDev b, int pass, uint64_t total,
-                                                 const uint32_t* __restrict__ site_ref,
-                                                 const int32_t* __restrict__ occ,
-                                                 const OutPoint* __restrict__ pool,
-                                                 uint8_t* __restrict__ prop_status,
-                                                 Cand* __restrict__ prop, RefCounters* __restrict__ ctr) {
+__global__ void __launch_bounds__(128) k_propose_costs(BatchDev b,
+                                                       const uint32_t* __restrict__ seed_idx,
+                                                       const uint32_t* __restrict__ seed_count,
+                                                       uint8_t* __restrict__ prop_status,
+                                                       Cand* __restrict__ prop,
+                                                       RefCounters* __restrict__ ctr) {
     constexpr int W = 2 * R + 1;
-    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < total;
-         g += (uint64_t)gridDim.x * blockDim.x) {
-        prop_status[g] = kPropNone;
-        const uint32_t r = site_ref[g];
+    const uint32_t count = *seed_count;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count;
+         i += gridDim.x * blockDim.x) {
+        const uint32_t g = seed_idx[i];
+        Cand cd = prop[g];
+        const uint32_t r = cd.ref;
         const DevReference& ref = b.refs[r];
-        if (ref.n_src == 0 || ref.stride == 0) continue;
-        if (pass > 0 && ctr[r].pass_additions[pass - 1] == 0) continue;
-        if (occ[g] >= 0) continue;
-        const uint32_t local = (uint32_t)(g - b.site_off[r]);
-        const uint32_t gy = local / ref.nx, gx = local - gy * ref.nx;
-        const uint32_t x = ref.border + gx * ref.stride, y = ref.border + gy * ref.stride;
-        double depths[8], confs[8], margins[8];
-        int n = 0;
-        for (int oy = -1; oy <= 1; ++oy)
-            for (int ox = -1; ox <= 1; ++ox) {
-                if (ox == 0 && oy == 0) continue;
-                int ngx = (int)gx + ox, ngy = (int)gy + oy;
-                if (ngx < 0 || ngy < 0 || ngx >= (int)ref.nx || ngy >= (int)ref.ny) continue;
-                int32_t pi = occ[b.site_off[r] + (uint64_t)ngy * ref.nx + ngx];
-                if (pi < 0) continue;
-                const OutPoint& pt = pool[pi];
-                D3 pos{(double)pt.p.x, (double)pt.p.y, (double)pt.p.z};
-                D3 q;
-                if (!project_exact(ref.cam, pos, ref.img.width, ref.img.height, ref.focal, q))
-                    continue;
-                depths[n] = q.z;
-                confs[n] = (double)pt.p.confidence;
-                margins[n] = (double)pt.a.depth_margin;
-                ++n;
-            }
-        // surface_depth_prediction (dense_legacy.rs:739-753)
-        if (n < kMinSurfaceNeighbors) continue;
-        double sorted[8];
-        for (int i = 0; i < n; ++i) sorted[i] = depths[i];
-        double predicted = median_of(sorted, n);
-        double mn = sorted[0], mx = sorted[n - 1];
-        if (!isfinite(mn) || !isfinite(mx) || mn <= 0.0 || mx <= 0.0) continue;
-        if (ddiv(dsub(mx, mn), mx) > kMaxSurfaceNeighborSpread) continue;
+        const uint32_t x = cd.x, y = cd.y;
+        const double predicted = cd.depth;
         RefCounters& c = ctr[r];
-        atomicAdd(&c.proposals, 1ull);
         if (patch_contrast_exact<T>(ref.img, (double)x, (double)y, R) < b.prof.min_contrast) {
             atomicAdd(&c.rej_texture, 1ull);
             prop_status[g] = kPropTexture;
@@ -1147,22 +1122,9 @@ __global__ void __launch_bounds__(128) k_propose(BatchDev b, int pass, uint64_t 
             prop_status[g] = kPropCrossView;
             continue;
         }
-        double direct_error = median_of(errs, ne);
-        double csum = 0.0, msum = 0.0;
-        for (int i = 0; i < n; ++i) csum = dadd(csum, confs[i]);
-        for (int i = 0; i < n; ++i) msum = dadd(msum, margins[i]);
-        Cand cd;
-        cd.ref = r;
-        cd.site = local;
-        cd.x = x;
-        cd.y = y;
         cd.pos = ppos;
-        cd.depth = predicted;
-        cd.error = direct_error;
-        cd.margin = ddiv(msum, (double)n);
-        cd.nconf = ddiv(csum, (double)n);
+        cd.error = median_of(errs, ne);
         cd.support = ne;
-        cd.pad = 0;
         prop[g] = cd;
         prop_status[g] = kPropCandidate;
     }
@@ -1261,20 +1223,18 @@ cudaError_t Typed<T>::reciprocal(const BatchDev& b, const Cand* cands, const uin
 }
 
 template <class T>
-cudaError_t Typed<T>::propose(const BatchDev& b, int pass, uint64_t total,
-                              const uint32_t* site_ref, const int32_t* occ, const OutPoint* pool,
-                              uint8_t* prop_status, Cand* prop, RefCounters* ctr,
-                              cudaStream_t st) {
+cudaError_t Typed<T>::propose(const BatchDev& b, const uint32_t* seed_idx,
+                              const uint32_t* seed_count, uint64_t total, uint8_t* prop_status,
+                              Cand* prop, RefCounters* ctr, cudaStream_t st) {
     using namespace typed_detail;
     uint64_t blocks = (total + 127) / 128;
-    if (blocks > (uint64_t)sm_count() * 64) blocks = (uint64_t)sm_count() * 64;
+    if (blocks > (uint64_t)sm_count() * 16) blocks = (uint64_t)sm_count() * 16;
     if (blocks == 0) blocks = 1;
-#define V3D_PROP(E, RR, C)                                                                \
-    if (b.exact == E && b.prof.radius == RR && (E || b.prof.cost == C)) {                  \
-        k_propose<T, E, RR, C><<<(unsigned)blocks, 128, 0, st>>>(b, pass, total, site_ref, \
-                                                                 occ, pool, prop_status,   \
-                                                                 prop, ctr);               \
-        return cudaGetLastError();                                                        \
+#define V3D_PROP(E, RR, C)                                                                  \
+    if (b.exact == E && b.prof.radius == RR && (E || b.prof.cost == C)) {                    \
+        k_propose_costs<T, E, RR, C><<<(unsigned)blocks, 128, 0, st>>>(b, seed_idx, seed_count, \
+                                                                       prop_status, prop, ctr); \
+        return cudaGetLastError();                                                          \
     }
 #define V3D_PROP_R(RR) V3D_PROP(true, RR, 0) V3D_PROP(false, RR, 0) V3D_PROP(false, RR, 1)
     V3D_PROP_R(1) V3D_PROP_R(2) V3D_PROP_R(3) V3D_PROP_R(4)
