@@ -283,6 +283,46 @@ __global__ void __launch_bounds__(256) k_sweep_site(BatchDev b, const uint32_t* 
     status[gw] = code;
 }
 
+// True when every point (X, Y) of the rectangle [xa, xb] x [ya, yb] maps
+// through H, by the per-tap f32 formula of the sweeps (h2 = H6 X + (H7 Y + H8),
+// u = (H0 X + (H1 Y + H2)) / h2, v likewise), to a denominator above zmin and
+// into [0, wl) x [0, hl).  The denominator is affine, so its minimum over the
+// rectangle is at a corner, and a projective map with a positive denominator
+// keeps the rectangle inside the hull of its mapped corners; the margins bound
+// the f32 rounding of any point's evaluation (a few ulp of the magnitudes
+// involved, taken at 2^-20 relative).
+__device__ __forceinline__ bool rect_inside(const float* H, float zmin, float wl, float hl,
+                                            float xa, float xb, float ya, float yb) {
+    const float ax = fmaxf(fabsf(xa), fabsf(xb)), ay = fmaxf(fabsf(ya), fabsf(yb));
+    const float su = fmaf(fabsf(H[0]), ax, fmaf(fabsf(H[1]), ay, fabsf(H[2])));
+    const float sv = fmaf(fabsf(H[3]), ax, fmaf(fabsf(H[4]), ay, fabsf(H[5])));
+    const float sz = fmaf(fabsf(H[6]), ax, fmaf(fabsf(H[7]), ay, fabsf(H[8])));
+    constexpr float kRel = 9.5367431640625e-07f;  // 2^-20
+    float hmin = 3.0e38f, umin = 3.0e38f, vmin = 3.0e38f, umax = -3.0e38f, vmax = -3.0e38f;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const float X = (c & 1) ? xb : xa;
+        const float Y = (c & 2) ? yb : ya;
+        const float h2 = fmaf(H[6], X, fmaf(H[7], Y, H[8]));
+        const float iv = __fdividef(1.0f, h2);
+        const float u = fmaf(H[0], X, fmaf(H[1], Y, H[2])) * iv;
+        const float v = fmaf(H[3], X, fmaf(H[4], Y, H[5])) * iv;
+        hmin = fminf(hmin, h2);
+        umin = fminf(umin, u);
+        umax = fmaxf(umax, u);
+        vmin = fminf(vmin, v);
+        vmax = fmaxf(vmax, v);
+    }
+    if (!(hmin > zmin + kRel * sz) || !(hmin > 0.f)) return false;
+    const float m = 0.015625f + kRel * (fmaxf(su, sv) + fmaxf(wl, hl) * sz) / hmin;
+    // NaN fails every comparison
+    return umin >= m && vmin >= m && umax <= wl - m && vmax <= hl - m;
+}
+
+// Pair-steps of the tiled sweep's warp step per warp: every step of the
+// CTA's warps covers 64 footprint slots each.
+__host__ __device__ constexpr int tiled_steps(int np) { return (np + 2 * kTileThreads - 1) / (2 * kTileThreads); }
+
 // ---- sweep, tiled ZNCC (fast policy) -----------------------------------------
 // A CTA owns a 32x8 block of grid sites.  For every (plane, source) it warps
 // the block's pixel footprint into the source once (f32 homography and f32
@@ -294,9 +334,13 @@ __global__ void __launch_bounds__(256) k_sweep_site(BatchDev b, const uint32_t* 
 //
 // The footprint rows in shared memory keep their columns grouped by x mod
 // stride (column x at slot (x % s) * PXs + x / s), so the stride-s reads of
-// the horizontal box filter fall on consecutive words across the lanes; the
-// footprint's x coordinates come from a per-slot table, so the warp step
-// converts no integers.
+// the horizontal box filter fall on consecutive words across the lanes.  The
+// warp step runs over the flat footprint (slot f = row * PXp + column slot),
+// 64 slots per warp and step with packed f32x2 arithmetic, their coordinates
+// from a per-CTA table, so it converts no integers and leaves no lanes idle at
+// row ends.  When the footprint's image in a source lies inside that image
+// (tested once per plane and source on the rectangle's corners), the step
+// skips the per-sample domain tests.
 template <class T, int R>
 __global__ void __launch_bounds__(kTileThreads, 1024 / kTileThreads) k_sweep_tiled(BatchDev b, uint64_t total_sites,
                                                      SiteRank* __restrict__ rank,
@@ -325,16 +369,36 @@ __global__ void __launch_bounds__(kTileThreads, 1024 / kTileThreads) k_sweep_til
     double* hrs = hss + PY * kTileX;         // [PY][32] row sums of r*s
     float* refv = reinterpret_cast<float*>(hrs + PY * kTileX);  // [PY][PXp] reference values
     float* samp = refv + np;                 // [PY][PXp] source samples (NaN = invalid)
-    float* colx = samp + np;                 // [PXp] footprint x of each slot, NaN = padding
-    float* costs = colx + PXp;               // [max_src][kTileThreads]
+    float* costs = samp + np;                // [max_src][kTileThreads]
     float* hA = costs + ms * kTileThreads;   // [max_src][12] homography parts
     float* pinv = hA + ms * 12;              // [planes] inverse depths
+    uint32_t* inmask = reinterpret_cast<uint32_t*>(pinv + b.prof.planes);  // [planes] inside sources
+    // [steps * kTileY][32] (x_a, x_b, y_a, y_b) of the slots f and f + 32 of each lane step
+    float4* slotxy = reinterpret_cast<float4*>(
+        (reinterpret_cast<uintptr_t>(inmask + b.prof.planes) + 15) & ~(uintptr_t)15);
+    const int n_steps = tiled_steps(np);
     const int tid = threadIdx.x;
     const T* rdata = static_cast<const T*>(ref.img.data);
     const int px0 = (int)(ref.border + gx0 * s) - R, py0 = (int)(ref.border + gy0 * s) - R;
-    for (int t = tid; t < PXp; t += kTileThreads) {
-        const int x = (t % PXs) * s + t / PXs;
-        colx[t] = x < PX ? (float)(px0 + x) : __int_as_float(0x7fc00000);
+    // padding slots (column PX and beyond) and slots past the footprint take
+    // the footprint's last column: their samples are never read, and the
+    // coordinates stay inside the rectangle that the inside test covers
+    auto slot_xy = [&](int f, float& X, float& Y) {
+        int yy = 0, x = PX - 1;
+        if (f < np) {
+            yy = f / PXp;
+            const int t = f - yy * PXp;
+            x = min((t % PXs) * s + t / PXs, PX - 1);
+        }
+        X = (float)(px0 + x);
+        Y = (float)(py0 + yy);
+    };
+    for (int i = tid; i < n_steps * kTileThreads; i += kTileThreads) {
+        const int fa = (i >> 5) * 64 + (i & 31);
+        float4 e;
+        slot_xy(fa, e.x, e.z);
+        slot_xy(fa + 32, e.y, e.w);
+        slotxy[i] = e;
     }
     for (int i = tid; i < np; i += kTileThreads) {
         const int yy = i / PXp, t = i - yy * PXp;
@@ -352,6 +416,22 @@ __global__ void __launch_bounds__(kTileThreads, 1024 / kTileThreads) k_sweep_til
     }
     for (int k = tid; k < ref.planes; k += kTileThreads)
         pinv[k] = (float)ddiv(1.0, hypothesis_depth(k, ref.planes, ref.search_min, ref.search_max));
+    // sources whose image of the footprint rectangle lies inside, per plane of the chunk
+    for (int kk = tid; kk < k1 - k0; kk += kTileThreads) {
+        const float inv = (float)ddiv(1.0, hypothesis_depth(k0 + kk, ref.planes, ref.search_min,
+                                                             ref.search_max));
+        uint32_t m = 0;
+        for (int j = 0; j < n_src; ++j) {
+            const DevSource& sj = ref.src[j];
+            const float H[9] = {sj.fwd_A[0], sj.fwd_A[1], fmaf(inv, sj.fwd_b[0], sj.fwd_A[2]),
+                                sj.fwd_A[3], sj.fwd_A[4], fmaf(inv, sj.fwd_b[1], sj.fwd_A[5]),
+                                sj.fwd_A[6], sj.fwd_A[7], fmaf(inv, sj.fwd_b[2], sj.fwd_A[8])};
+            if (rect_inside(H, 1.0e-4f * inv, (float)(sj.img.width - 1), (float)(sj.img.height - 1),
+                            (float)px0, (float)(px0 + PX - 1), (float)py0, (float)(py0 + PY - 1)))
+                m |= 1u << j;
+        }
+        inmask[kk] = m;
+    }
     // slot of tap dx of the window that starts at column 0 (add the window's start)
     int toff[W];
 #pragma unroll
@@ -401,25 +481,33 @@ __global__ void __launch_bounds__(kTileThreads, 1024 / kTileThreads) k_sweep_til
             const DevImage si = ref.src[j].img;
             const T* sdata = static_cast<const T*>(si.data);
             const float wl = (float)(si.width - 1), hl = (float)(si.height - 1);
-            // warps over rows, lanes over column slots; the homography folded
-            // per row, the reciprocal from the approximate unit
-            float Y = (float)(py0 + ty);
-            for (int yy = ty; yy < PY; yy += kTileY, Y += (float)kTileY) {
-                const float hx = fmaf(A[1], Y, H2), hy = fmaf(A[4], Y, H5), hz = fmaf(A[7], Y, H8);
-                float* row = samp + yy * PXp;
-                int t = tx;
-                // slots t and t + 32 together with packed f32x2 arithmetic; each
-                // component is the scalar computation of the loop below, bit for bit
-                for (; t + kTileX < PXp; t += 2 * kTileX) {
-                    const float2 X2 = f2(colx[t], colx[t + kTileX]);
-                    const float2 h2 = __ffma2_rn(f2(A[6], A[6]), X2, f2(hz, hz));
-                    const float2 iv = f2(__fdividef(1.0f, h2.x), __fdividef(1.0f, h2.y));
-                    const float2 u = __fmul2_rn(__ffma2_rn(f2(A[0], A[0]), X2, f2(hx, hx)), iv);
-                    const float2 q = __fmul2_rn(__ffma2_rn(f2(A[3], A[3]), X2, f2(hy, hy)), iv);
-                    // padding slots have a NaN x and fail the first test
+            // the flat footprint, slots fa and fa + 32 per lane and step; the
+            // reciprocal from the approximate unit; each component of the packed
+            // arithmetic is the scalar computation, bit for bit
+            const bool inside = (inmask[k - k0] >> j) & 1u;
+            const float a0 = A[0], a1 = A[1], a3 = A[3], a4 = A[4], a6 = A[6], a7 = A[7];
+            for (int p = 0; p < n_steps; ++p) {
+                const int ws = p * kTileY + ty;
+                const int fa = ws * 64 + tx;
+                if (fa >= np) break;
+                const int fb = fa + 32;
+                const float4 e = slotxy[ws * 32 + tx];
+                const float2 X2 = f2(e.x, e.y), Y2 = f2(e.z, e.w);
+                const float2 hx = __ffma2_rn(f2(a1, a1), Y2, f2(H2, H2));
+                const float2 hy = __ffma2_rn(f2(a4, a4), Y2, f2(H5, H5));
+                const float2 hz = __ffma2_rn(f2(a7, a7), Y2, f2(H8, H8));
+                const float2 h2 = __ffma2_rn(f2(a6, a6), X2, hz);
+                const float2 iv = f2(__fdividef(1.0f, h2.x), __fdividef(1.0f, h2.y));
+                const float2 u = __fmul2_rn(__ffma2_rn(f2(a0, a0), X2, hx), iv);
+                const float2 q = __fmul2_rn(__ffma2_rn(f2(a3, a3), X2, hy), iv);
+                float va = __int_as_float(0x7fc00000), vb = va;
+                if (inside) {
+                    const float2 sv = sample_nonneg_pair<T>(sdata, si.width, u, q);
+                    va = sv.x;
+                    vb = sv.y;
+                } else {
                     const bool ia = h2.x > zmin && u.x >= 0.f && q.x >= 0.f && u.x < wl && q.x < hl;
                     const bool ib = h2.y > zmin && u.y >= 0.f && q.y >= 0.f && u.y < wl && q.y < hl;
-                    float va = __int_as_float(0x7fc00000), vb = va;
                     if (ia && ib) {
                         const float2 sv = sample_nonneg_pair<T>(sdata, si.width, u, q);
                         va = sv.x;
@@ -428,22 +516,9 @@ __global__ void __launch_bounds__(kTileThreads, 1024 / kTileThreads) k_sweep_til
                         if (ia) va = sample_nonneg<T>(sdata, si.width, u.x, q.x);
                         if (ib) vb = sample_nonneg<T>(sdata, si.width, u.y, q.y);
                     }
-                    row[t] = va;
-                    row[t + kTileX] = vb;
                 }
-                for (; t < PXp; t += kTileX) {
-                    const float X = colx[t];
-                    const float h2 = fmaf(A[6], X, hz);
-                    float v = __int_as_float(0x7fc00000);
-                    if (h2 > zmin) {  // false for padding slots (X is NaN)
-                        const float iv = __fdividef(1.0f, h2);
-                        const float u = fmaf(A[0], X, hx) * iv;
-                        const float q = fmaf(A[3], X, hy) * iv;
-                        if (u >= 0.f && q >= 0.f && u < wl && q < hl)
-                            v = sample_nonneg<T>(sdata, si.width, u, q);
-                    }
-                    row[t] = v;
-                }
+                samp[fa] = va;
+                if (fb < np) samp[fb] = vb;
             }
             __syncthreads();
             // horizontal box filter, one row per warp, the window of lane c at slot c
@@ -1179,8 +1254,9 @@ cudaError_t Typed<T>::sweep_tiled(const BatchDev& b, uint32_t max_nx, uint32_t m
         const int PX = (kTileX - 1) * s + W, PY = (kTileY - 1) * s + W;
         const size_t PXp = (size_t)((PX + s - 1) / s) * s, np = PXp * PY;
         const size_t smem = sizeof(double) * 3 * (size_t)PY * kTileX +
-                            sizeof(float) * (2 * np + PXp + (size_t)b.max_src * (kTileThreads + 12) +
-                                             (size_t)b.prof.planes);
+                            sizeof(float) * (2 * np + (size_t)b.max_src * (kTileThreads + 12) +
+                                             2 * (size_t)b.prof.planes) +
+                            16 + sizeof(float4) * (size_t)tiled_steps((int)np) * kTileThreads;
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);
         if (e != cudaSuccess) return e;
