@@ -40,10 +40,10 @@ UNIT = "samples·planes·views/s"
 WIDTH, HEIGHT, FRAMES = 640, 360, 120
 RADIUS, PLANES, SOURCES, STRIDE = 3, 128, 8, 2
 # DRAM bytes per unit of the depth sweep (k_sweep_tiled), from one ncu capture of
-# the same workload cut to 12 keyframes (677.4 M units; 11.12 MB read + 0.03 MB
+# the same workload cut to 12 keyframes (677.4 M units; 11.15 MB read + 0.01 MB
 # written; profiles/k_sweep_tiled_zncc7x7_640x360_12kf.md).  A clip's frames live
 # in L2, so the sweep's DRAM traffic grows with its units.
-SWEEP_DRAM_BYTES_PER_UNIT = (11.121664e6 + 0.025856e6) / 677.376e6
+SWEEP_DRAM_BYTES_PER_UNIT = (11.151360e6 + 0.008192e6) / 677.376e6
 
 
 def parse():
@@ -307,7 +307,7 @@ def run_ours(args, rank, world, local):
             "e2e": {"value": total_units / wall_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": points * 72 + triangles * 32,
                     "ms_per_step": wall_s * 1e3},
-            "gpu_launches": infos[-1]["kernel_launches"],
+            "gpu_launches": int(sum(i["kernel_launches"] for i in infos)),
             "sweep_chunks": infos[-1]["sweep_chunks"],
             "stages_ms": {"sweep": sweep_ms, "reciprocal_primary": recip_ms,
                           "completion": comp_ms, "mesh": mesh_ms, "total": dev_s * 1e3,

@@ -310,16 +310,18 @@ cudaError_t mesh_batch_enqueue(const MeshScratch& s, uint32_t n_patches, uint64_
         return e;
     if ((e = cudaMemsetAsync(s.winners, 0xFF, sizeof(uint32_t) * total_cells, stream))) return e;
     if (n_points) {
-        k_mb_vertices<<<blocks_for(n_points), 256, 0, stream>>>(s, points, sites, patch_of, local_of,
+        V3D_COUNTED k_mb_vertices<<<blocks_for(n_points), 256, 0, stream>>>(s, points, sites, patch_of, local_of,
                                                                 n_points);
-        k_mb_winners<<<blocks_for(n_points), 256, 0, stream>>>(s, sites, patch_of, n_points);
+        V3D_COUNTED k_mb_winners<<<blocks_for(n_points), 256, 0, stream>>>(s, sites, patch_of, n_points);
     }
-    if (total_slots) k_mb_slots<<<blocks_for(total_slots), 256, 0, stream>>>(s, n_patches, total_slots);
+    if (total_slots) {
+        V3D_COUNTED k_mb_slots<<<blocks_for(total_slots), 256, 0, stream>>>(s, n_patches, total_slots);
+    }
     if ((e = cudaGetLastError())) return e;
     if ((e = launch_compact(s.slot_status, 1, total_slots, s.slot_idx, s.count, s.compact_scratch,
                             stream)))
         return e;
-    k_mb_emit<<<blocks_for(total_slots), 256, 0, stream>>>(s, n_patches, tris, tri_patch);
+    V3D_COUNTED k_mb_emit<<<blocks_for(total_slots), 256, 0, stream>>>(s, n_patches, tris, tri_patch);
     return cudaGetLastError();
 }
 

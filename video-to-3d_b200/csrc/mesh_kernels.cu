@@ -341,13 +341,13 @@ int32_t run_mesh_patch(v3d_context* ctx, const v3d_point* points, const v3d_grid
     cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long) * 4, st);
     if (n) {
         unsigned blocks = (unsigned)std::min<size_t>((n + 255) / 256, 148 * 16);
-        k_mesh_vertices<<<blocks, 256, 0, st>>>(mp, d_pts, d_sites, map.empty() ? nullptr : d_map,
+        V3D_COUNTED k_mesh_vertices<<<blocks, 256, 0, st>>>(mp, d_pts, d_sites, map.empty() ? nullptr : d_map,
                                                 d_grid, d_vtx);
     }
     size_t cells = (size_t)gw * gh;
     if (cells) {
         unsigned blocks = (unsigned)std::min<size_t>((cells + 255) / 256, 148 * 16);
-        k_mesh_extent<<<blocks, 256, 0, st>>>(mp, d_grid, d_ext, d_cnt);
+        V3D_COUNTED k_mesh_extent<<<blocks, 256, 0, st>>>(mp, d_grid, d_ext, d_cnt);
     }
     int ext[4];
     unsigned long long vertices = 0;
@@ -418,7 +418,7 @@ int32_t run_mesh_patch(v3d_context* ctx, const v3d_point* points, const v3d_grid
     {
         size_t items = L.cells + L.hb + L.vb;
         unsigned blocks = (unsigned)std::max<size_t>(1, std::min<size_t>((items + 255) / 256, 148 * 16));
-        k_mesh_triangles<<<blocks, 256, 0, st>>>(mp, L, d_grid, d_vtx, d_slot, d_tri, d_cnt + 1);
+        V3D_COUNTED k_mesh_triangles<<<blocks, 256, 0, st>>>(mp, L, d_grid, d_vtx, d_slot, d_tri, d_cnt + 1);
     }
     std::vector<uint8_t> hs(slots);
     std::vector<v3d_mesh_triangle> ht(slots);

@@ -16,6 +16,9 @@
 #include "typed.cuh"
 
 namespace v3d {
+
+thread_local uint64_t g_kernel_launches = 0;
+
 namespace {
 
 constexpr double kInf = __builtin_huge_val();
@@ -352,7 +355,7 @@ cudaError_t by_storage(int storage, F&& f) {
 
 cudaError_t launch_luma(const uint8_t* rgba, uint8_t* luma, size_t pixels, cudaStream_t stream) {
     if (!pixels) return cudaSuccess;
-    k_luma<<<grid_for(pixels, 256), 256, 0, stream>>>(reinterpret_cast<const uchar4*>(rgba), luma,
+    V3D_COUNTED k_luma<<<grid_for(pixels, 256), 256, 0, stream>>>(reinterpret_cast<const uchar4*>(rgba), luma,
                                                       pixels);
     return cudaGetLastError();
 }
@@ -360,7 +363,7 @@ cudaError_t launch_luma(const uint8_t* rgba, uint8_t* luma, size_t pixels, cudaS
 cudaError_t launch_site_ref(const uint64_t* site_off, int32_t n_refs, uint64_t total_sites,
                             uint32_t* site_ref, cudaStream_t stream) {
     if (!total_sites) return cudaSuccess;
-    k_site_ref<<<grid_for(total_sites, 256), 256, 0, stream>>>(site_off, n_refs, total_sites,
+    V3D_COUNTED k_site_ref<<<grid_for(total_sites, 256), 256, 0, stream>>>(site_off, n_refs, total_sites,
                                                                site_ref);
     return cudaGetLastError();
 }
@@ -393,7 +396,7 @@ cudaError_t launch_sweep_dispatch(const BatchDev& b, const uint32_t* site_ref, u
         return Typed<T>::sweep_site(b, site_ref, total_sites, rank, status, counters, stream);
     });
     if (e != cudaSuccess || chunks.n <= 1) return e;
-    k_merge_chunks<<<grid_for(total_sites, 256), 256, 0, stream>>>(b.prof, total_sites, chunks.n,
+    V3D_COUNTED k_merge_chunks<<<grid_for(total_sites, 256), 256, 0, stream>>>(b.prof, total_sites, chunks.n,
                                                                 chunks.partial, rank, status);
     return cudaGetLastError();
 }
@@ -410,9 +413,9 @@ cudaError_t launch_compact(const uint8_t* flags, uint8_t value, uint64_t n, uint
         return cudaMemsetAsync(count_dev, 0, sizeof(uint32_t), stream);
     }
     uint32_t* bc = static_cast<uint32_t*>(scratch);
-    k_compact_count<<<(unsigned)blocks, kCompactThreads, 0, stream>>>(flags, value, n, bc);
-    k_compact_scan<<<1, 1024, 0, stream>>>(bc, (uint32_t)blocks, count_dev);
-    k_compact_scatter<<<(unsigned)blocks, kCompactThreads, 0, stream>>>(flags, value, n, bc,
+    V3D_COUNTED k_compact_count<<<(unsigned)blocks, kCompactThreads, 0, stream>>>(flags, value, n, bc);
+    V3D_COUNTED k_compact_scan<<<1, 1024, 0, stream>>>(bc, (uint32_t)blocks, count_dev);
+    V3D_COUNTED k_compact_scatter<<<(unsigned)blocks, kCompactThreads, 0, stream>>>(flags, value, n, bc,
                                                                         out_idx);
     return cudaGetLastError();
 }
@@ -421,7 +424,7 @@ cudaError_t launch_make_primary_cands(const BatchDev& b, const uint32_t* site_id
                                       const uint32_t* count_dev, uint64_t cap,
                                       const uint32_t* site_ref, const SiteRank* rank, Cand* cands,
                                       cudaStream_t stream) {
-    k_make_primary_cands<<<grid_for(cap, 256), 256, 0, stream>>>(b, site_idx, count_dev, site_ref,
+    V3D_COUNTED k_make_primary_cands<<<grid_for(cap, 256), 256, 0, stream>>>(b, site_idx, count_dev, site_ref,
                                                                   rank, cands);
     return cudaGetLastError();
 }
@@ -438,7 +441,7 @@ cudaError_t launch_fuse(const BatchDev& b, const Cand* cands, const uint32_t* co
                         uint64_t cap, const RecipObs* obs, bool completion, int pass,
                         OutPoint* out, uint8_t* cand_status, RefCounters* counters,
                         cudaStream_t stream) {
-    k_fuse<<<grid_for(cap, 128), 128, 0, stream>>>(b, cands, count_dev, obs, completion ? 1 : 0,
+    V3D_COUNTED k_fuse<<<grid_for(cap, 128), 128, 0, stream>>>(b, cands, count_dev, obs, completion ? 1 : 0,
                                                    pass, out, cand_status, counters);
     return cudaGetLastError();
 }
@@ -446,20 +449,20 @@ cudaError_t launch_fuse(const BatchDev& b, const Cand* cands, const uint32_t* co
 cudaError_t launch_append(const uint32_t* idx, const uint32_t* count_dev, uint64_t cap,
                           const OutPoint* src, OutPoint* pool, uint32_t* pool_size,
                           uint32_t* segment_end, cudaStream_t stream) {
-    k_append<<<grid_for(cap, 256), 256, 0, stream>>>(idx, count_dev, src, pool, pool_size);
-    k_bump<<<1, 1, 0, stream>>>(pool_size, count_dev, segment_end);
+    V3D_COUNTED k_append<<<grid_for(cap, 256), 256, 0, stream>>>(idx, count_dev, src, pool, pool_size);
+    V3D_COUNTED k_bump<<<1, 1, 0, stream>>>(pool_size, count_dev, segment_end);
     return cudaGetLastError();
 }
 
 cudaError_t launch_occupancy_clear(int32_t* occ, uint64_t total_sites, cudaStream_t stream) {
     if (!total_sites) return cudaSuccess;
-    k_fill<<<grid_for(total_sites, 256), 256, 0, stream>>>(occ, total_sites, -1);
+    V3D_COUNTED k_fill<<<grid_for(total_sites, 256), 256, 0, stream>>>(occ, total_sites, -1);
     return cudaGetLastError();
 }
 
 cudaError_t launch_occupy(const BatchDev& b, const OutPoint* pool, const uint32_t* begin,
                           const uint32_t* end, uint64_t cap, int32_t* occ, cudaStream_t stream) {
-    k_occupy<<<grid_for(cap, 256), 256, 0, stream>>>(b, pool, begin, end, occ);
+    V3D_COUNTED k_occupy<<<grid_for(cap, 256), 256, 0, stream>>>(b, pool, begin, end, occ);
     return cudaGetLastError();
 }
 
@@ -537,7 +540,7 @@ cudaError_t launch_propose(const BatchDev& b, int pass, uint64_t total_sites,
                            uint32_t* seed_idx, uint32_t* seed_count, void* scratch,
                            cudaStream_t stream) {
     if (!total_sites) return cudaSuccess;
-    k_propose_seed<<<grid_for(total_sites, 256), 256, 0, stream>>>(
+    V3D_COUNTED k_propose_seed<<<grid_for(total_sites, 256), 256, 0, stream>>>(
         b, pass, total_sites, site_ref, occ, pool, prop_status, prop_cand, counters);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
@@ -551,7 +554,7 @@ cudaError_t launch_propose(const BatchDev& b, int pass, uint64_t total_sites,
 
 cudaError_t launch_gather_cands(const uint32_t* idx, const uint32_t* count_dev, uint64_t cap,
                                 const Cand* src, Cand* dst, cudaStream_t stream) {
-    k_gather_cands<<<grid_for(cap, 256), 256, 0, stream>>>(idx, count_dev, src, dst);
+    V3D_COUNTED k_gather_cands<<<grid_for(cap, 256), 256, 0, stream>>>(idx, count_dev, src, dst);
     return cudaGetLastError();
 }
 

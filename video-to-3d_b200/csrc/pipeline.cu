@@ -571,6 +571,7 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
         return std::chrono::duration<double, std::milli>(clk::now() - t).count();
     };
     const clk::time_point t_upload = clk::now();
+    const uint64_t launches0 = g_kernel_launches;
     Prepared P;
     int32_t pst = prepare(ctx, prof, frames, n_frames, focal, plans, active, false, P,
                           mesh != nullptr, resident);
@@ -603,12 +604,6 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
     cudaEventCreate(&ev0);
     cudaEventCreate(&ev1);
     cudaEventRecord(ev0, stream);
-    // kernel launches enqueued below: sweep, 2 x 3 compaction kernels,
-    // candidates, reciprocal, fuse, append (2), occupancy (2), then per
-    // completion pass propose, compaction (3), gather, reciprocal, fuse,
-    // compaction (3), append (2), occupancy
-    ctx->last_launches = 1 + 3 + 1 + 1 + 1 + 3 + 2 + 2 + 2 * (5 + 3 + 1 + 1 + 1 + 3 + 2 + 1);
-    if (P.chunks > 1) ctx->last_launches += 1;  // the chunk merge
     ctx->last_chunks = static_cast<uint64_t>(P.chunks);
     ctx->last_sites = total;
     ctx->last_units = 0;
@@ -658,16 +653,15 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
     {
         const unsigned gb = static_cast<unsigned>(std::min<uint64_t>((cap + 255) / 256, 148 * 16));
         V3D_CK(cudaMemsetAsync(P.m_range, 0, sizeof(uint32_t) * 6 * n_active, stream));
-        k_pool_ranges<<<gb, 256, 0, stream>>>(d_pool, c_seg, static_cast<uint32_t>(n_active),
+        V3D_COUNTED k_pool_ranges<<<gb, 256, 0, stream>>>(d_pool, c_seg, static_cast<uint32_t>(n_active),
                                               P.m_range, P.m_range + 3 * n_active);
-        k_ref_bases<<<1, 1024, 0, stream>>>(P.m_range, P.m_range + 3 * n_active,
+        V3D_COUNTED k_ref_bases<<<1, 1024, 0, stream>>>(P.m_range, P.m_range + 3 * n_active,
                                            static_cast<uint32_t>(n_active), P.o_base);
-        k_pool_output<<<gb, 256, 0, stream>>>(d_pool, c_seg, static_cast<uint32_t>(n_active),
+        V3D_COUNTED k_pool_output<<<gb, 256, 0, stream>>>(d_pool, c_seg, static_cast<uint32_t>(n_active),
                                               P.m_range, P.m_range + 3 * n_active, P.o_base,
                                               P.o_pts, P.o_sites, P.o_attrs, P.o_med, P.o_patch,
                                               P.o_local);
         V3D_CK(cudaGetLastError());
-        ctx->last_launches += 3;
     }
     // The result block, acquired on a helper thread while the device works,
     // sized like the last call's results: a caller that still holds those
@@ -719,10 +713,10 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
         V3D_CK(mesh_batch_enqueue(P.mesh, static_cast<uint32_t>(n_active), total, P.total_slots,
                                   P.o_pts, P.o_sites, P.o_patch, P.o_local, n_points, P.m_tris,
                                   P.m_tpatch, stream));
-        ctx->last_launches += 6;
     }
     cudaEventRecord(es[7], stream);
     cudaEventRecord(ev1, stream);
+    ctx->last_launches = g_kernel_launches - launches0;
 
     // ---- read back ----
     ctx->last_upload_ms = ms_since(t_upload);

@@ -1233,7 +1233,7 @@ cudaError_t Typed<T>::sweep_site(const BatchDev& b, const uint32_t* site_ref, ui
     const unsigned blocks = (unsigned)((total * 32 + 255) / 256);
 #define V3D_SITE(E, RR, C)                                                                   \
     if (b.exact == E && b.prof.radius == RR && (E || b.prof.cost == C)) {                     \
-        k_sweep_site<T, E, RR, C><<<blocks, 256, 0, st>>>(b, site_ref, total, rank, status, ctr); \
+        V3D_COUNTED k_sweep_site<T, E, RR, C><<<blocks, 256, 0, st>>>(b, site_ref, total, rank, status, ctr); \
         return cudaGetLastError();                                                           \
     }
 #define V3D_SITE_R(RR) V3D_SITE(true, RR, 0) V3D_SITE(false, RR, 0) V3D_SITE(false, RR, 1)
@@ -1263,7 +1263,7 @@ cudaError_t Typed<T>::sweep_tiled(const BatchDev& b, uint32_t max_nx, uint32_t m
         const int n = chunks.n > 1 ? chunks.n : 1;
         dim3 grid((max_nx + kTileX - 1) / kTileX, (max_ny + kTileY - 1) / kTileY,
                   (unsigned)b.n_refs * (unsigned)n);
-        kern<<<grid, kTileThreads, smem, st>>>(b, total_sites, rank, status, ctr, n, chunks.partial);
+        V3D_COUNTED kern<<<grid, kTileThreads, smem, st>>>(b, total_sites, rank, status, ctr, n, chunks.partial);
         return cudaGetLastError();
     };
     switch (b.prof.radius) {
@@ -1282,14 +1282,14 @@ cudaError_t Typed<T>::reciprocal(const BatchDev& b, const Cand* cands, const uin
     const unsigned blocks = (unsigned)sm_count() * 8;
 #define V3D_REC(RR)                                                                            \
     if (b.prof.radius == RR) {                                                                 \
-        if (b.exact)                                                                           \
-            k_reciprocal_exact<T, RR><<<blocks, 256, 0, st>>>(b, cands, count, obs, ctr);      \
-        else if (b.prof.cost == 1) {                                                           \
-            k_recip_prepare<T, RR, 1><<<blocks, 256, 0, st>>>(b, cands, count, obs, ctr);      \
-            k_recip_sweep<T, RR, 1><<<blocks, 256, 0, st>>>(b, cands, count, obs);             \
+        if (b.exact) {                                                                         \
+            V3D_COUNTED k_reciprocal_exact<T, RR><<<blocks, 256, 0, st>>>(b, cands, count, obs, ctr);      \
+        } else if (b.prof.cost == 1) {                                                         \
+            V3D_COUNTED k_recip_prepare<T, RR, 1><<<blocks, 256, 0, st>>>(b, cands, count, obs, ctr);      \
+            V3D_COUNTED k_recip_sweep<T, RR, 1><<<blocks, 256, 0, st>>>(b, cands, count, obs);             \
         } else {                                                                               \
-            k_recip_prepare<T, RR, 0><<<blocks, 256, 0, st>>>(b, cands, count, obs, ctr);      \
-            k_recip_sweep<T, RR, 0><<<blocks, 256, 0, st>>>(b, cands, count, obs);             \
+            V3D_COUNTED k_recip_prepare<T, RR, 0><<<blocks, 256, 0, st>>>(b, cands, count, obs, ctr);      \
+            V3D_COUNTED k_recip_sweep<T, RR, 0><<<blocks, 256, 0, st>>>(b, cands, count, obs);             \
         }                                                                                      \
         return cudaGetLastError();                                                             \
     }
@@ -1308,7 +1308,7 @@ cudaError_t Typed<T>::propose(const BatchDev& b, const uint32_t* seed_idx,
     if (blocks == 0) blocks = 1;
 #define V3D_PROP(E, RR, C)                                                                  \
     if (b.exact == E && b.prof.radius == RR && (E || b.prof.cost == C)) {                    \
-        k_propose_costs<T, E, RR, C><<<(unsigned)blocks, 128, 0, st>>>(b, seed_idx, seed_count, \
+        V3D_COUNTED k_propose_costs<T, E, RR, C><<<(unsigned)blocks, 128, 0, st>>>(b, seed_idx, seed_count, \
                                                                        prop_status, prop, ctr); \
         return cudaGetLastError();                                                          \
     }

@@ -19,6 +19,11 @@
 
 namespace v3d {
 
+// Kernel launches enqueued by this host thread: every launch site counts
+// itself with V3D_COUNTED, and a call reports the difference across it.
+extern thread_local uint64_t g_kernel_launches;
+#define V3D_COUNTED ++::v3d::g_kernel_launches;
+
 constexpr int kMaxRadius = 4;
 constexpr int kMaxTaps = (2 * kMaxRadius + 1) * (2 * kMaxRadius + 1);
 constexpr int kMaxSources = 16;
