@@ -527,6 +527,10 @@ int32_t v3d_server_submit(v3d_server* server, uint64_t clip_id, uint64_t camera_
 int32_t v3d_server_wait(v3d_server* server, uint64_t ticket, int64_t timeout_ms,
                         v3d_dense_result* out, v3d_mesh_result* mesh_out, int32_t* present,
                         v3d_request_timing* timing);
+/* Copies the description of the most recent failed batch (empty when none
+ * failed) into buf, NUL-terminated and cut to n bytes; returns its full
+ * length.  A failed request's status says that it failed; this says why. */
+uint64_t v3d_server_last_error(v3d_server* server, char* buf, uint64_t n);
 
 /* Per-site outcome of the depth sweep (dense_legacy.rs:272-362) before the
  * reciprocal check: status 1 = below the contrast gate, 2 = no hypothesis had

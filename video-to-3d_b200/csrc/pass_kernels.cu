@@ -431,9 +431,9 @@ cudaError_t launch_make_primary_cands(const BatchDev& b, const uint32_t* site_id
 
 cudaError_t launch_reciprocal(const BatchDev& b, const Cand* cands, const uint32_t* count_dev,
                               uint64_t /*cap*/, RecipObs* obs, RefCounters* counters,
-                              cudaStream_t stream) {
+                              const RecipQueue& queue, cudaStream_t stream) {
     return by_storage(b.storage, [&](auto t) {
-        return Typed<decltype(t)>::reciprocal(b, cands, count_dev, obs, counters, stream);
+        return Typed<decltype(t)>::reciprocal(b, cands, count_dev, obs, counters, queue, stream);
     });
 }
 

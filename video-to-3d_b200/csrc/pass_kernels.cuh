@@ -168,9 +168,21 @@ cudaError_t launch_make_primary_cands(const BatchDev& b, const uint32_t* site_id
                                       const uint32_t* site_ref, const SiteRank* rank, Cand* cands,
                                       cudaStream_t stream);
 
+// Work queue of the fast-policy reciprocal sweep: the prologue flags each
+// (candidate, source) item that passed it (item = candidate * max_src +
+// source; `cap_items` = the candidate capacity * max_src flags), a compaction
+// lists the flagged items in order, and the sweep's warps take the list round
+// robin, so every warp gets the same share of the pairs that need a sweep.
+struct RecipQueue {
+    uint8_t* flags;       // [cap_items]
+    uint32_t* items;      // [cap_items]
+    uint32_t* n_items;    // device count of listed items
+    void* scratch;        // compaction_scratch_bytes(cap_items)
+    uint64_t cap_items;
+};
 cudaError_t launch_reciprocal(const BatchDev& b, const Cand* cands, const uint32_t* count_dev,
                               uint64_t cap, RecipObs* obs, RefCounters* counters,
-                              cudaStream_t stream);
+                              const RecipQueue& queue, cudaStream_t stream);
 
 cudaError_t launch_fuse(const BatchDev& b, const Cand* cands, const uint32_t* count_dev,
                         uint64_t cap, const RecipObs* obs, bool completion, int pass,

@@ -155,6 +155,7 @@ struct Prepared {
     uint8_t* d_pstat = nullptr;
     Cand* d_prop = nullptr;
     uint32_t* d_counts = nullptr;
+    RecipQueue queue{};         // the reciprocal sweep's work queue
     // output: the pool in per-reference order (primaries, then completions)
     v3d_point* o_pts = nullptr;
     v3d_grid_site* o_sites = nullptr;
@@ -287,7 +288,18 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
     const size_t o_partial = cv.take<Rank>(P.chunks > 1 ? static_cast<uint64_t>(P.chunks) * cap : 1);
     const size_t o_ctr = cv.take<RefCounters>(n_active);
     const uint64_t pc = sweep_only ? 1 : cap;  // pass buffers are not needed for the sweep alone
-    const size_t o_scratch = cv.take<uint8_t>(compaction_scratch_bytes(pc));
+    // the reciprocal sweep's work queue: a flag and a list entry per (candidate, source)
+    size_t queue_src = 1;
+    for (size_t k = 0; k < n_active; ++k)
+        queue_src = std::max(queue_src, plans[active[k]].src_slots.size());
+    const uint64_t pq = pc * queue_src;
+    if (pq >= (1ull << 32)) {
+        ctx->last_error = "batch too large: 2^32 or more (grid site, source) pairs";
+        return V3D_ERR_INVALID_ARGUMENT;
+    }
+    const size_t o_scratch = cv.take<uint8_t>(compaction_scratch_bytes(pq));
+    const size_t o_qflags = cv.take<uint8_t>(pq);
+    const size_t o_qitems = cv.take<uint32_t>(pq);
     const size_t o_idx = cv.take<uint32_t>(pc);
     const size_t o_cands = cv.take<Cand>(pc);
     const size_t o_cstat = cv.take<uint8_t>(pc);
@@ -418,12 +430,15 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
     P.d_cands = reinterpret_cast<Cand*>(at(o_cands));
     P.d_cstat = reinterpret_cast<uint8_t*>(at(o_cstat));
     P.d_obs = reinterpret_cast<RecipObs*>(at(o_obs));
+    P.queue = RecipQueue{reinterpret_cast<uint8_t*>(at(o_qflags)),
+                         reinterpret_cast<uint32_t*>(at(o_qitems)), nullptr, P.d_scratch, pq};
     P.d_fused = reinterpret_cast<OutPoint*>(at(o_fused));
     P.d_pool = reinterpret_cast<OutPoint*>(at(o_pool));
     P.d_occ = reinterpret_cast<int32_t*>(at(o_occ));
     P.d_pstat = reinterpret_cast<uint8_t*>(at(o_pstat));
     P.d_prop = reinterpret_cast<Cand*>(at(o_prop));
     auto* d_counts = P.d_counts = reinterpret_cast<uint32_t*>(at(o_counts));
+    P.queue.n_items = P.d_counts + 9;  // [8] completion seeds, [9] reciprocal items
     P.o_pts = reinterpret_cast<v3d_point*>(at(o_opts));
     P.o_sites = reinterpret_cast<v3d_grid_site*>(at(o_osites));
     P.o_attrs = reinterpret_cast<v3d_point_attributes*>(at(o_oattrs));
@@ -624,7 +639,7 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
     V3D_CK(launch_compact(d_status, kSiteAccepted, total, d_idx, c_cand, d_scratch, stream));
     V3D_CK(launch_make_primary_cands(b, d_idx, c_cand, cap, d_siteref, d_rank, d_cands, stream));
     cudaEventRecord(es[2], stream);
-    V3D_CK(launch_reciprocal(b, d_cands, c_cand, cap, d_obs, d_ctr, stream));
+    V3D_CK(launch_reciprocal(b, d_cands, c_cand, cap, d_obs, d_ctr, P.queue, stream));
     cudaEventRecord(es[3], stream);
     V3D_CK(cudaMemsetAsync(d_cstat, 0, cap, stream));
     V3D_CK(launch_fuse(b, d_cands, c_cand, cap, d_obs, false, 0, d_fused, d_cstat, d_ctr, stream));
@@ -640,7 +655,7 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
                               d_idx, P.d_counts + 8, d_scratch, stream));
         V3D_CK(launch_compact(d_pstat, kPropCandidate, total, d_idx, c_cand, d_scratch, stream));
         V3D_CK(launch_gather_cands(d_idx, c_cand, cap, d_prop, d_cands, stream));
-        V3D_CK(launch_reciprocal(b, d_cands, c_cand, cap, d_obs, d_ctr, stream));
+        V3D_CK(launch_reciprocal(b, d_cands, c_cand, cap, d_obs, d_ctr, P.queue, stream));
         V3D_CK(cudaMemsetAsync(d_cstat, 0, cap, stream));
         V3D_CK(launch_fuse(b, d_cands, c_cand, cap, d_obs, true, pass, d_fused, d_cstat, d_ctr,
                            stream));

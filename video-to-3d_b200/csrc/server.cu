@@ -91,6 +91,7 @@ struct v3d_server {
     std::unordered_map<uint64_t, Finished> finished;
     uint64_t next_ticket = 1;
     bool stop = false;
+    std::string last_error;                // of the most recent failed batch
     std::vector<v3d_context*> ctxs;
     std::vector<std::thread> workers;
 };
@@ -143,6 +144,9 @@ void run_batch_of_requests(v3d_server* s, v3d_context* ctx, const std::vector<Re
     const clk::time_point done = clk::now();
     {
         std::lock_guard<std::mutex> lock(s->mu);
+        if (st < 0)
+            s->last_error = ctx->last_error.empty() ? std::string(v3d_status_text(st))
+                                                    : ctx->last_error;
         for (size_t k = 0; k < n; ++k) {
             const Request& r = batch[order[k]];
             Finished f;
@@ -405,6 +409,18 @@ int32_t v3d_server_wait(v3d_server* s, uint64_t ticket, int64_t timeout_ms, v3d_
     *present = f.present;
     if (timing) *timing = f.timing;
     return f.status;
+}
+
+uint64_t v3d_server_last_error(v3d_server* s, char* buf, uint64_t n) {
+    if (!s) return 0;
+    std::lock_guard<std::mutex> lock(s->mu);
+    const std::string& e = s->last_error;
+    if (buf && n) {
+        const uint64_t k = std::min<uint64_t>(e.size(), n - 1);
+        std::memcpy(buf, e.data(), k);
+        buf[k] = '\0';
+    }
+    return e.size();
 }
 
 }  // extern "C"

@@ -16,7 +16,8 @@ struct Typed {
                                    RefCounters* ctr, cudaStream_t st, uint64_t total_sites,
                                    SweepChunks chunks);
     static cudaError_t reciprocal(const BatchDev& b, const Cand* cands, const uint32_t* count,
-                                  RecipObs* obs, RefCounters* ctr, cudaStream_t st);
+                                  RecipObs* obs, RefCounters* ctr, const RecipQueue& queue,
+                                  cudaStream_t st);
     static cudaError_t propose(const BatchDev& b, const uint32_t* seed_idx,
                                const uint32_t* seed_count, uint64_t total, uint8_t* prop_status,
                                Cand* prop, RefCounters* ctr, cudaStream_t st);

@@ -858,7 +858,8 @@ template <class T, int R, int COST>
 __global__ void __launch_bounds__(256) k_recip_prepare(BatchDev b, const Cand* __restrict__ cands,
                                                        const uint32_t* __restrict__ count,
                                                        RecipObs* __restrict__ obs,
-                                                       RefCounters* __restrict__ ctr) {
+                                                       RefCounters* __restrict__ ctr,
+                                                       uint8_t* __restrict__ pending) {
     constexpr int W = 2 * R + 1;
     constexpr int N = W * W;
     const uint32_t lane = lane_id();
@@ -996,12 +997,14 @@ __global__ void __launch_bounds__(256) k_recip_prepare(BatchDev b, const Cand* _
             if (lane == 0) atomicAdd(&ctr[cd.ref].recip_evals, (unsigned long long)ref.planes);
         }
         if (lane == 0 && si < ref.n_src) obs[it] = res;
+        if (lane == 0) pending[item] = ok ? 1 : 0;
     }
 }
 
 template <class T, int R, int COST>
 __global__ void __launch_bounds__(256, 2) k_recip_sweep(BatchDev b, const Cand* __restrict__ cands,
-                                                     const uint32_t* __restrict__ count,
+                                                     const uint32_t* __restrict__ list,
+                                                     const uint32_t* __restrict__ list_count,
                                                      RecipObs* __restrict__ obs) {
     constexpr int W = 2 * R + 1;
     constexpr int N = W * W;
@@ -1009,17 +1012,17 @@ __global__ void __launch_bounds__(256, 2) k_recip_sweep(BatchDev b, const Cand* 
     const uint32_t lane = lane_id(), wid = threadIdx.x >> 5;
     float* pvc = pvc_all[wid];
     const uint32_t ms = (uint32_t)b.max_src;
-    const uint64_t items = (uint64_t)(*count) * ms;
-    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    const uint32_t n_list = *list_count;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
     const DevProfile& prof = b.prof;
-    for (uint64_t item = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; item < items;
-         item += nwarps) {
-        const uint32_t ci = (uint32_t)(item / ms);
-        const int si = (int)(item - (uint64_t)ci * ms);
+    // the pending (candidate, source) items, listed in order by the compaction
+    for (uint32_t li = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; li < n_list; li += nwarps) {
+        const uint32_t item = list[li];
+        const uint32_t ci = item / ms;
+        const int si = (int)(item - ci * ms);
         const uint64_t it = (uint64_t)ci * kMaxSources + si;
         const uint32_t r = cands[ci].ref;
         const DevReference& ref = b.refs[r];
-        if (si >= ref.n_src || obs[it].valid != kObsPending) continue;
         const D3 sp = obs[it].pos;
         const DevSource& src = ref.src[si];
         // the source window as the contrast gate sampled it, centred; taps
@@ -1277,19 +1280,32 @@ cudaError_t Typed<T>::sweep_tiled(const BatchDev& b, uint32_t max_nx, uint32_t m
 
 template <class T>
 cudaError_t Typed<T>::reciprocal(const BatchDev& b, const Cand* cands, const uint32_t* count,
-                                 RecipObs* obs, RefCounters* ctr, cudaStream_t st) {
+                                 RecipObs* obs, RefCounters* ctr, const RecipQueue& q,
+                                 cudaStream_t st) {
     using namespace typed_detail;
     const unsigned blocks = (unsigned)sm_count() * 8;
+    // prologue, then the list of its pending items, then the sweep over the list
+    auto prep_and_list = [&](auto prep) -> cudaError_t {
+        cudaError_t e = cudaMemsetAsync(q.flags, 0, q.cap_items, st);
+        if (e != cudaSuccess) return e;
+        V3D_COUNTED prep<<<blocks, 256, 0, st>>>(b, cands, count, obs, ctr, q.flags);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        return launch_compact(q.flags, 1, q.cap_items, q.items, q.n_items, q.scratch, st);
+    };
 #define V3D_REC(RR)                                                                            \
     if (b.prof.radius == RR) {                                                                 \
         if (b.exact) {                                                                         \
             V3D_COUNTED k_reciprocal_exact<T, RR><<<blocks, 256, 0, st>>>(b, cands, count, obs, ctr);      \
         } else if (b.prof.cost == 1) {                                                         \
-            V3D_COUNTED k_recip_prepare<T, RR, 1><<<blocks, 256, 0, st>>>(b, cands, count, obs, ctr);      \
-            V3D_COUNTED k_recip_sweep<T, RR, 1><<<blocks, 256, 0, st>>>(b, cands, count, obs);             \
+            const cudaError_t e = prep_and_list(k_recip_prepare<T, RR, 1>);                    \
+            if (e != cudaSuccess) return e;                                                    \
+            V3D_COUNTED k_recip_sweep<T, RR, 1><<<blocks, 256, 0, st>>>(b, cands, q.items,     \
+                                                                        q.n_items, obs);       \
         } else {                                                                               \
-            V3D_COUNTED k_recip_prepare<T, RR, 0><<<blocks, 256, 0, st>>>(b, cands, count, obs, ctr);      \
-            V3D_COUNTED k_recip_sweep<T, RR, 0><<<blocks, 256, 0, st>>>(b, cands, count, obs);             \
+            const cudaError_t e = prep_and_list(k_recip_prepare<T, RR, 0>);                    \
+            if (e != cudaSuccess) return e;                                                    \
+            V3D_COUNTED k_recip_sweep<T, RR, 0><<<blocks, 256, 0, st>>>(b, cands, q.items,     \
+                                                                        q.n_items, obs);       \
         }                                                                                      \
         return cudaGetLastError();                                                             \
     }

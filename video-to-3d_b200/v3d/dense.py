@@ -99,6 +99,8 @@ def library():
     L.v3d_server_wait.argtypes = [C.c_void_p, C.c_uint64, C.c_int64, _P(abi.DenseResult),
                                   _P(abi.MeshResult), _P(C.c_int32), _P(abi.RequestTiming)]
     L.v3d_server_wait.restype = C.c_int32
+    L.v3d_server_last_error.argtypes = [C.c_void_p, C.c_char_p, C.c_uint64]
+    L.v3d_server_last_error.restype = C.c_uint64
     L.v3d_measure_gather_rate.argtypes = [C.c_void_p, _P(C.c_double)]
     L.v3d_measure_gather_rate.restype = C.c_int32
     L.v3d_last_run_info.argtypes = [C.c_void_p, _P(abi.RunInfo)]
@@ -377,7 +379,9 @@ class Server:
             return None
         t = {name: getattr(timing, name) for name, _ in abi.RequestTiming._fields_}
         if st < 0:
-            raise V3DError(st, "request failed")
+            buf = C.create_string_buffer(1024)
+            self.lib.v3d_server_last_error(self.handle, buf, len(buf))
+            raise V3DError(st, "request failed: " + buf.value.decode(errors="replace"))
         if not present.value:
             self.lib.v3d_dense_result_free(C.byref(out))
             if self.meshed:
