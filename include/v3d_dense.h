@@ -472,6 +472,47 @@ int32_t v3d_last_run_info(const v3d_context* ctx, v3d_run_info* out);
  * image; about 0.1 s on a B200. */
 int32_t v3d_measure_gather_rate(v3d_context* ctx, double* samples_per_second);
 
+/* ---- cross-reference surface fusion (surface_fusion.rs:356-852) ---------
+ * The first step of surface consolidation after the grid mesh
+ * (consolidate_surface_recording_with_control, surface_fusion.rs:128-231,
+ * called from reconstruction_stages.rs:874): mesh vertices of different
+ * camera-support groups that are mutually nearest within the local and global
+ * edge-scale bounds, with aligned vertex normals, move to their
+ * confidence-weighted mean unless the complete move set would weaken a
+ * triangle incident to a moved vertex. */
+
+/* FusionStats (surface_fusion.rs:17-24). */
+typedef struct v3d_fusion_stats {
+    uint64_t eligible_vertices;
+    uint64_t candidate_pairs;
+    uint64_t rejected_normal_pairs;
+    uint64_t rejected_topology_pairs;
+    uint64_t fused_pairs;
+} v3d_fusion_stats;
+
+/* One accepted pair (FusionOutcome::pairs, surface_fusion.rs:27-32):
+ * first < second, both moved to one position. */
+typedef struct v3d_fusion_pair {
+    uint64_t first, second;
+} v3d_fusion_pair;
+
+/* fuse_mutually_supported_vertices_with_control (surface_fusion.rs:369-549),
+ * replacing that function behind the same inputs and outputs.  points
+ * [n_points] are moved in place; triangles [n_triangles] index into them;
+ * membership [n_points] is each point's camera-support group as
+ * evidence_support_membership (surface_fusion.rs:316-345) assigns it,
+ * negative for none.  pairs needs room for n_points / 2 entries and moved for
+ * n_points; *n_pairs and *n_moved get their counts (moved indices ascending:
+ * FusionOutcome::moved_indices).  cancel (may be NULL) is polled between the
+ * stages; a canceled call returns V3D_OK with zero stats, no pairs and the
+ * points unchanged, the reference's FusionOutcome::default().  Device work
+ * on the context's stream; the call returns when the results are on the host. */
+int32_t v3d_fuse_mutually_supported_vertices(
+    v3d_context* ctx, v3d_point* points, uint64_t n_points,
+    const v3d_mesh_triangle* triangles, uint64_t n_triangles, const int64_t* membership,
+    v3d_cancel_fn cancel, void* cancel_user, v3d_fusion_stats* stats,
+    v3d_fusion_pair* pairs, uint64_t* n_pairs, uint64_t* moved, uint64_t* n_moved);
+
 /* ---- Serving (no counterpart in the reference, which runs one call at a time) ----
  *
  * A device-resident request loop.  Clips (frames, cameras, landmarks) are

@@ -17,7 +17,9 @@
 // The restatement is pinned by re-running every assertion of the reference's
 // own tests for the path (dense_legacy.rs:1261-1514, dense.rs:1089-1562,
 // surface_completion_tests.rs:56-113, mesh_legacy.rs:609-908,
-// mesh.rs:311-380) in oracle/oracle_selftest.cpp.
+// mesh.rs:311-380) in oracle/oracle_selftest.cpp.  Cross-reference surface
+// fusion (surface_fusion.rs:316-852, oracle_fusion.cpp) is pinned the same way
+// by surface_fusion.rs:891-1070 and fusion_prepass_acceptance_tests.rs:31-57.
 #pragma once
 
 #include <cstdint>
@@ -324,5 +326,50 @@ MeshAnalysis reconstruct_dense_mesh_with_control(const std::vector<Point3>& poin
 // Half / bfloat16 decoding (exact).
 double half_to_double(uint16_t h);
 double bf16_to_double(uint16_t b);
+
+// ---- surface_fusion.rs (oracle_fusion.cpp) ----
+// SurfaceEvidenceRegion (reconstruction_evidence.rs), the fields that
+// evidence_support_membership reads.
+struct EvidenceRegion {
+    std::optional<size_t> reference_frame;
+    std::vector<size_t> source_frames;
+    size_t start = 0, count = 0;
+};
+// VertexSurfaceEvidence (surface_fusion.rs:47-52)
+struct VertexEvidence {
+    std::vector<std::optional<Vec3>> normals;
+    std::vector<std::optional<double>> local_scales;
+    std::vector<std::vector<size_t>> incident;
+    std::optional<double> global_edge_scale;
+};
+// FusionMove (surface_fusion.rs:40-45)
+struct FusionMove {
+    size_t first, second;
+    Vec3 position;
+};
+// FusionStats, FusionOutcome (surface_fusion.rs:17-32)
+struct FusionStats {
+    size_t eligible_vertices = 0, candidate_pairs = 0, rejected_normal_pairs = 0,
+           rejected_topology_pairs = 0, fused_pairs = 0;
+};
+struct FusionOutcome {
+    FusionStats stats;
+    std::vector<std::pair<size_t, size_t>> pairs;
+    std::vector<size_t> moved_indices;
+};
+std::pair<std::vector<int64_t>, size_t> evidence_support_membership(
+    const std::vector<EvidenceRegion>& regions, size_t point_count);
+std::optional<VertexEvidence> vertex_surface_evidence(const std::vector<Point3>& points,
+                                                      const std::vector<MeshTriangle>& triangles,
+                                                      Control& control);
+std::pair<std::vector<FusionMove>, size_t> topology_safe_moves(
+    const std::vector<Point3>& points, const std::vector<MeshTriangle>& triangles,
+    const std::vector<std::vector<size_t>>& incident, std::vector<FusionMove> moves,
+    Control& control);
+// membership: support group per point, negative = none
+FusionOutcome fuse_mutually_supported_vertices(std::vector<Point3>& points,
+                                               const std::vector<MeshTriangle>& triangles,
+                                               const std::vector<int64_t>& membership,
+                                               Control& control);
 
 }  // namespace v3do

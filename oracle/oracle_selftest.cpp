@@ -661,6 +661,123 @@ void mesh_tests() {
     }
 }
 
+// ---- surface_fusion.rs:891-1070 and fusion_prepass_acceptance_tests.rs ----
+Point3 fpoint(float x, float y, float z, float c) { return Point3{x, y, z, c, 128, 128, 128}; }
+MeshTriangle ftri(size_t a, size_t b, size_t c) { return MeshTriangle{a, b, c, 0.9f}; }
+
+// surface_fusion.rs:891-915
+void groups_evidence_regions_by_camera_support_instead_of_dense_patch_identity() {
+    std::vector<EvidenceRegion> regions = {
+        {0, {2, 1}, 0, 2}, {0, {1, 2}, 2, 1}, {3, {4}, 3, 1}, {std::nullopt, {}, 4, 1}};
+    auto [membership, groups] = evidence_support_membership(regions, 5);
+    CHECK(groups == 2);
+    CHECK((membership == std::vector<int64_t>{0, 0, 0, 1, -1}));
+}
+
+// surface_fusion.rs:917-940
+void aligns_mutually_nearest_vertices_from_consistent_evidence_groups() {
+    std::vector<Point3> pts = {fpoint(0, 0, 0, 1), fpoint(1, 0, 0, 1), fpoint(0, 1, 0, 1),
+                               fpoint(0, 0, 0.06f, 1), fpoint(1, 0, 0.06f, 1),
+                               fpoint(0, 1, 0.06f, 1)};
+    std::vector<MeshTriangle> tris = {ftri(0, 1, 2), ftri(3, 4, 5)};
+    std::vector<int64_t> mem = {0, 0, 0, 1, 1, 1};
+    Control ctl = never();
+    FusionStats st = fuse_mutually_supported_vertices(pts, tris, mem, ctl).stats;
+    CHECK(st.fused_pairs == 3);
+    CHECK(st.rejected_normal_pairs == 0);
+    CHECK(st.rejected_topology_pairs == 0);
+    for (auto [l, r] : {std::pair<int, int>{0, 3}, {1, 4}, {2, 5}}) {
+        CHECK(std::fabs(pts[l].z - 0.03f) < 1.0e-6f);
+        CHECK(std::fabs(pts[l].z - pts[r].z) < 1.0e-6f);
+    }
+}
+
+// surface_fusion.rs:942-961
+void rejects_nearby_vertices_when_surface_normals_disagree() {
+    std::vector<Point3> pts = {fpoint(0, 0, 0, 1), fpoint(1, 0, 0, 1), fpoint(0, 1, 0, 1),
+                               fpoint(0, 0, 0.05f, 1), fpoint(1, 0, 0.05f, 1),
+                               fpoint(0, 0.05f, 1, 1)};
+    std::vector<MeshTriangle> tris = {ftri(0, 1, 2), ftri(3, 4, 5)};
+    std::vector<int64_t> mem = {0, 0, 0, 1, 1, 1};
+    Control ctl = never();
+    FusionStats st = fuse_mutually_supported_vertices(pts, tris, mem, ctl).stats;
+    CHECK(st.fused_pairs == 0);
+    CHECK(st.rejected_normal_pairs >= 2);
+    CHECK(pts[0].z == 0.0f);
+    CHECK(pts[3].z == 0.05f);
+}
+
+// surface_fusion.rs:963-982
+void rejects_a_seam_move_that_would_weaken_an_accepted_triangle() {
+    std::vector<Point3> pts = {fpoint(0, 0, 0, 1), fpoint(1, 0, 0, 1), fpoint(0.9f, 0.01f, 0, 1),
+                               fpoint(0, 0.12f, 0, 1), fpoint(1, 0.12f, 0, 1),
+                               fpoint(0, 1.12f, 0, 1)};
+    std::vector<MeshTriangle> tris = {ftri(0, 1, 2), ftri(3, 4, 5)};
+    std::vector<int64_t> mem = {0, 0, 0, 1, 1, 1};
+    Control ctl = never();
+    FusionStats st = fuse_mutually_supported_vertices(pts, tris, mem, ctl).stats;
+    CHECK(st.fused_pairs == 0);
+    CHECK(st.rejected_topology_pairs > 0);
+    CHECK(pts[0].y == 0.0f);
+    CHECK(pts[3].y == 0.12f);
+}
+
+// surface_fusion.rs:984-1010
+void validates_the_complete_move_set_against_original_topology() {
+    std::vector<Point3> pts = {fpoint(0, 0, 0, 1), fpoint(1, 0, 0, 1), fpoint(0, 1, 0, 1),
+                               fpoint(0.2f, 0, 0, 1), fpoint(0.8f, 0, 0, 1)};
+    std::vector<MeshTriangle> tris = {ftri(0, 1, 2)};
+    std::vector<std::vector<size_t>> incident = {{0}, {0}, {0}, {}, {}};
+    std::vector<FusionMove> moves = {FusionMove{0, 3, Vec3{0.2, 0, 0}},
+                                     FusionMove{1, 4, Vec3{0.8, 0, 0}}};
+    Control ctl = never();
+    auto [accepted, rejected] = topology_safe_moves(pts, tris, incident, moves, ctl);
+    CHECK(accepted.empty());
+    CHECK(rejected == 2);
+}
+
+// surface_fusion.rs:1012-1027
+void never_fuses_vertices_from_the_same_evidence_group() {
+    std::vector<Point3> pts = {fpoint(0, 0, 0, 1), fpoint(1, 0, 0, 1), fpoint(0, 1, 0, 1)};
+    std::vector<MeshTriangle> tris = {ftri(0, 1, 2)};
+    std::vector<int64_t> mem = {0, 0, 0};
+    Control ctl = never();
+    FusionStats st = fuse_mutually_supported_vertices(pts, tris, mem, ctl).stats;
+    CHECK(st.fused_pairs == 0);
+    CHECK(st.candidate_pairs == 0);
+}
+
+// fusion_prepass_acceptance_tests.rs:31-57 and :59-79 (evidence of 4096
+// repeated triangles; a cancellation after entry yields no partial evidence)
+void controlled_fusion_prepass_preserves_actual_geometry_evidence() {
+    std::vector<Point3> pts = {fpoint(0, 0, 0, 0.9f), fpoint(1, 0, 0, 0.9f), fpoint(0, 1, 0, 0.9f)};
+    std::vector<MeshTriangle> tris(4096, ftri(0, 1, 2));
+    int polls = 0;
+    Control ctl;
+    ctl.poll = [&] {
+        ++polls;
+        return false;
+    };
+    auto ev = vertex_surface_evidence(pts, tris, ctl);
+    CHECK(ev.has_value());
+    if (!ev) return;
+    CHECK(polls > 4);
+    CHECK(ev->global_edge_scale.has_value() && *ev->global_edge_scale == 1.0);
+    bool normals = ev->normals.size() == 3;
+    for (auto& n : ev->normals) normals = normals && n && n->x == 0 && n->y == 0 && n->z == 1;
+    CHECK(normals);
+    std::vector<size_t> all(tris.size());
+    for (size_t i = 0; i < all.size(); ++i) all[i] = i;
+    CHECK((ev->incident == std::vector<std::vector<size_t>>(3, all)));
+    for (int cancel_at : {2, 4}) {
+        int k = 0;
+        Control c2;
+        c2.poll = [&] { return ++k >= cancel_at; };
+        CHECK(!vertex_surface_evidence(pts, tris, c2).has_value());
+        CHECK(k >= cancel_at);
+    }
+}
+
 struct Test {
     const char* name;
     void (*fn)();
@@ -701,6 +818,20 @@ extern "C" int32_t v3do_selftest(char* report, uint64_t capacity, int32_t* check
         {"verified_surface_completion_adds_expected_plane_geometry",
          verified_surface_completion_adds_expected_plane_geometry},
         {"mesh_legacy_and_mesh_tests", mesh_tests},
+        {"groups_evidence_regions_by_camera_support_instead_of_dense_patch_identity",
+         groups_evidence_regions_by_camera_support_instead_of_dense_patch_identity},
+        {"aligns_mutually_nearest_vertices_from_consistent_evidence_groups",
+         aligns_mutually_nearest_vertices_from_consistent_evidence_groups},
+        {"rejects_nearby_vertices_when_surface_normals_disagree",
+         rejects_nearby_vertices_when_surface_normals_disagree},
+        {"rejects_a_seam_move_that_would_weaken_an_accepted_triangle",
+         rejects_a_seam_move_that_would_weaken_an_accepted_triangle},
+        {"validates_the_complete_move_set_against_original_topology",
+         validates_the_complete_move_set_against_original_topology},
+        {"never_fuses_vertices_from_the_same_evidence_group",
+         never_fuses_vertices_from_the_same_evidence_group},
+        {"controlled_fusion_prepass_preserves_actual_geometry_evidence",
+         controlled_fusion_prepass_preserves_actual_geometry_evidence},
     };
     std::string names;
     for (const Test& t : tests) {

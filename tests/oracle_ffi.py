@@ -54,6 +54,19 @@ class Oracle:
                                                      _P(abi.SiteRecord), C.c_uint64,
                                                      _P(C.c_uint64)]
         L.v3do_debug_sweep.restype = C.c_int32
+        L.v3do_fuse_mutually_supported_vertices.argtypes = [
+            C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64, C.c_void_p, abi.CANCEL_FN,
+            C.c_void_p, _P(abi.FusionStats), C.c_void_p, _P(C.c_uint64), C.c_void_p,
+            _P(C.c_uint64)]
+        L.v3do_fuse_mutually_supported_vertices.restype = C.c_int32
+
+    def fuse_mutually_supported_vertices(self, points, triangles, membership, control=None):
+        """surface_fusion.rs:369-549 on the CPU: moves `points` in place."""
+        from v3d import dense
+        st, out = dense._fuse(self.lib.v3do_fuse_mutually_supported_vertices, (), points,
+                              triangles, membership, control)
+        assert st == 0, st
+        return out
 
     def selftest(self):
         buf = C.create_string_buffer(1 << 16)

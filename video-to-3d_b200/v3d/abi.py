@@ -222,7 +222,18 @@ class RequestTiming(C.Structure):
 TIMEOUT = -6
 SHUTDOWN = -7
 
+class FusionStats(C.Structure):
+    _fields_ = [("eligible_vertices", C.c_uint64), ("candidate_pairs", C.c_uint64),
+                ("rejected_normal_pairs", C.c_uint64), ("rejected_topology_pairs", C.c_uint64),
+                ("fused_pairs", C.c_uint64)]
+
+
+class FusionPair(C.Structure):
+    _fields_ = [("first", C.c_uint64), ("second", C.c_uint64)]
+
+
 STRUCTS = {
+    "v3d_fusion_stats": FusionStats, "v3d_fusion_pair": FusionPair,
     "v3d_frame": Frame, "v3d_camera": Camera, "v3d_profile": Profile, "v3d_point": Point,
     "v3d_grid_site": GridSite, "v3d_point_attributes": PointAttributes,
     "v3d_dense_stats": DenseStats, "v3d_reference_attempt": ReferenceAttempt,

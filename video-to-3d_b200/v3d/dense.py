@@ -13,6 +13,8 @@ raises.
 import ctypes as C
 import os
 
+import numpy as np
+
 from . import abi, profiles, types
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -101,6 +103,10 @@ def library():
     L.v3d_server_wait.restype = C.c_int32
     L.v3d_server_last_error.argtypes = [C.c_void_p, C.c_char_p, C.c_uint64]
     L.v3d_server_last_error.restype = C.c_uint64
+    L.v3d_fuse_mutually_supported_vertices.argtypes = [
+        C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64, C.c_void_p, abi.CANCEL_FN,
+        C.c_void_p, _P(abi.FusionStats), C.c_void_p, _P(C.c_uint64), C.c_void_p, _P(C.c_uint64)]
+    L.v3d_fuse_mutually_supported_vertices.restype = C.c_int32
     L.v3d_measure_gather_rate.argtypes = [C.c_void_p, _P(C.c_double)]
     L.v3d_measure_gather_rate.restype = C.c_int32
     L.v3d_last_run_info.argtypes = [C.c_void_p, _P(abi.RunInfo)]
@@ -295,6 +301,57 @@ class Context:
             self.handle, *mi.args(), cams.cameras, cams.n_cameras, int(width), int(height),
             float(focal), fn, None, C.byref(out)))
         return self._mesh(out)
+
+    def fuse_mutually_supported_vertices(self, points, triangles, membership, control=None):
+        """fuse_mutually_supported_vertices_with_control (surface_fusion.rs:369-549)
+        on the device: moves `points` in place and returns a FusionOutcome."""
+        st, out = _fuse(self.lib.v3d_fuse_mutually_supported_vertices, (self.handle,), points,
+                        triangles, membership, control)
+        self._check(st)
+        return out
+
+
+class FusionOutcome:
+    """FusionOutcome (surface_fusion.rs:27-32): stats (a dict of FusionStats),
+    pairs (n x 2 uint64, first < second) and moved_indices (ascending)."""
+
+    def __init__(self, stats, pairs, moved_indices):
+        self.stats = stats
+        self.pairs = pairs
+        self.moved_indices = moved_indices
+
+
+def fusion_arguments(points, triangles, membership):
+    """Checked contiguous arrays for v3d_fuse_mutually_supported_vertices:
+    points (POINT_DTYPE, moved in place, so it must already be contiguous),
+    triangles (TRIANGLE_DTYPE) and membership (int64, negative = no group)."""
+    if not (isinstance(points, np.ndarray) and points.dtype == types.POINT_DTYPE
+            and points.flags.c_contiguous and points.flags.writeable):
+        raise TypeError("points must be a writable contiguous POINT_DTYPE array")
+    tris = np.ascontiguousarray(triangles, dtype=types.TRIANGLE_DTYPE)
+    mem = np.ascontiguousarray(membership, dtype=np.int64)
+    if mem.shape != (len(points),):
+        raise ValueError("membership needs one entry per point")
+    return tris, mem
+
+
+def fusion_outcome(stats, pairs, n_pairs, moved, n_moved):
+    st = {name: int(getattr(stats, name)) for name, _ in abi.FusionStats._fields_}
+    return FusionOutcome(st, pairs[:n_pairs].copy(), moved[:n_moved].copy())
+
+
+def _fuse(lib_fn, head, points, triangles, membership, control):
+    tris, mem = fusion_arguments(points, triangles, membership)
+    n = len(points)
+    fn, _keep = types.cancel_callback(control)
+    stats = abi.FusionStats()
+    pairs = np.zeros((max(n // 2, 1), 2), dtype=np.uint64)
+    moved = np.zeros(max(n, 1), dtype=np.uint64)
+    n_pairs, n_moved = C.c_uint64(), C.c_uint64()
+    st = lib_fn(*head, points.ctypes.data, n, tris.ctypes.data, len(tris), mem.ctypes.data, fn,
+                None, C.byref(stats), pairs.ctypes.data, C.byref(n_pairs), moved.ctypes.data,
+                C.byref(n_moved))
+    return st, fusion_outcome(stats, pairs, n_pairs.value, moved, n_moved.value)
 
 
 def has_distributed_landmarks(frames, cameras, sparse_points, focal, control=None):
