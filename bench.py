@@ -56,11 +56,12 @@ def parse():
     ap.add_argument("--frames", type=int, default=FRAMES)
     ap.add_argument("--no-cpu-baseline", action="store_true",
                     help="skip the CPU baseline leg (profiling runs)")
-    ap.add_argument("--config", choices=["full", "small", "heavy", "batched", "served"],
+    ap.add_argument("--config", choices=["full", "small", "heavy", "batched", "served", "fusion"],
                     default="full",
                     help="full: the headline line (default); small: 360x202 1+4 views; heavy: "
                          "bf16 16 views 256 planes 9x9; batched: 32 uneven clips through the "
-                         "server vs one request at a time; served: Poisson arrivals, p50/p99")
+                         "server vs one request at a time; served: Poisson arrivals, p50/p99; "
+                         "fusion: cross-reference surface fusion of the full clip's patches")
     ap.add_argument("--rates", default="50,200,800", help="served: request rates (req/s)")
     ap.add_argument("--duration", type=float, default=3.0, help="served: seconds of arrivals")
     ap.add_argument("--clips", type=int, default=32, help="batched/served: number of clips")
@@ -553,6 +554,90 @@ def run_plain_config(args):
     print(json.dumps(line), flush=True)
 
 
+def run_fusion(args):
+    """Cross-reference surface fusion (surface_fusion.rs:369-549) on the
+    consolidated output of the full clip: every keyframe's reference patch and
+    grid mesh from this library, one camera-support group per patch.  A step is
+    one v3d_fuse_mutually_supported_vertices call with host buffers."""
+    import torch
+    from v3d import dense, profiles, surface
+    clip = load_clip(2, args.frames)
+    frames = clip.frames(args.storage)
+    prof = profiles.zncc(RADIUS, PLANES, SOURCES, STRIDE)
+    ctx = dense.Context(0)
+    res = ctx.reconstruct_reference_patches_meshed(frames, clip.cameras, clip.sparse, clip.focal,
+                                                   list(range(args.frames)), profile=prof)
+    patches = [r for r in res if r is not None]
+    pts, tris, mem, groups = surface.consolidation_inputs(patches)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    for _ in range(args.warmup):
+        ctx.fuse_mutually_supported_vertices(pts.copy(), tris, mem)
+    dev, wall, outs, launches = [], [], [], 0
+    clocks = Clocks(0)
+    clocks.start()
+    for _ in range(args.steps):
+        p = pts.copy()
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        out = ctx.fuse_mutually_supported_vertices(p, tris, mem)
+        wall.append(time.perf_counter() - t0)
+        info = ctx.last_run_info()
+        dev.append(info["device_ms"] / 1e3)
+        launches += int(info["kernel_launches"])
+        outs.append(out)
+    clk = clocks.stop()
+    n, nt = len(pts), len(tris)
+    dev_s, wall_s = float(np.mean(dev)), float(np.mean(wall))
+    pairs = outs[-1].stats["fused_pairs"]
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    alg = n * (20 + 8) + nt * 32 + pairs * 2 * 20
+    line = {"metric": "mesh vertices fused/s", "value": n / dev_s, "unit": "vertices/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": dev_s * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64",
+            "data": "the library's own dense output of the seeded synthetic clip",
+            "config": {"workload": "cross-reference surface fusion of the consolidated dense "
+                                   "output of the full clip (%d reference patches and their "
+                                   "grid meshes, %d camera-support groups)" % (len(patches), groups),
+                       "points": n, "triangles": nt,
+                       "l2": "flushed between timed steps (256 MiB write)"},
+            "clocks": clk,
+            "e2e": {"value": n / wall_s, "unit": "vertices/s",
+                    "h2d_bytes_per_step": n * (20 + 8) + nt * 32,
+                    "d2h_bytes_per_step": pairs * (16 + 2 * 20) + len(outs[-1].moved_indices) * 4,
+                    "ms_per_step": wall_s * 1e3},
+            "gpu_launches": launches,
+            "outcome": outs[-1].stats,
+            "roofline": {"bound": "hbm", "kernel": "whole fusion call (per-triangle, per-vertex "
+                                                   "and per-cell kernels, sorts, topology rounds)",
+                         "achieved": alg / dev_s / 1e9, "peak": hbm, "unit": "GB/s",
+                         "frac": alg / dev_s / 1e9 / hbm, "traffic": None,
+                         "algorithmic_bytes": alg,
+                         "note": "algorithmic bytes = points, membership and triangles read once "
+                                 "plus the fused points written; the call also sorts incidence "
+                                 "entries, edge lengths and cells and reads three scalars back "
+                                 "to the host between stages"}}
+    if not args.no_cpu_baseline:
+        from tests.oracle_ffi import Oracle
+        k = min(12, len(patches))
+        sp, st, sm, _ = surface.consolidation_inputs(patches[:k])
+        t0 = time.perf_counter()
+        Oracle().fuse_mutually_supported_vertices(sp, st, sm)
+        cpu_s = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": len(sp) / cpu_s, "unit": "vertices/s", "cores": 1,
+                                "kind": "port",
+                                "sample": "the first %d patches (%d points, %d triangles), one "
+                                          "thread" % (k, len(sp), len(st))}
+    print(json.dumps(line), flush=True)
+    ctx.close()
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
@@ -564,6 +649,8 @@ def main():
         run_served(args)
     elif args.config in ("small", "heavy"):
         run_plain_config(args)
+    elif args.config == "fusion":
+        run_fusion(args)
     else:
         run_ours(args, rank, world, local)
 

@@ -590,6 +590,20 @@ extern "C" int32_t v3d_fuse_mutually_supported_vertices(
     V3D_FCK(cudaMemsetAsync(d_ctr, 0, sizeof(unsigned long long) * 4, st));
     V3D_FCK(cudaMemsetAsync(d_vcnt, 0, sizeof(uint32_t) * (n + 1), st));
 
+    // the device span from the first kernel to the last (with the host reads
+    // between the stages) for the run info's device_ms
+    cudaEvent_t ev0, ev1;
+    cudaEventCreate(&ev0);
+    cudaEventCreate(&ev1);
+    struct Events {
+        cudaEvent_t a, b;
+        ~Events() {
+            cudaEventDestroy(a);
+            cudaEventDestroy(b);
+        }
+    } events{ev0, ev1};
+    cudaEventRecord(ev0, st);
+
     // ---- vertex evidence ----
     V3D_COUNTED k_tri_evidence<<<grid_of(nt), 256, 0, st>>>(d_pts, n, d_tris, nt, d_valid, d_len, d_wn);
     V3D_FCK(cudaGetLastError());
@@ -695,6 +709,7 @@ extern "C" int32_t v3d_fuse_mutually_supported_vertices(
     V3D_FCK(launch_compact(d_moved, 1, n, d_movedi, c_moved, d_scratch, st));
     V3D_COUNTED k_pairs_out<<<grid_of(n_moves), 256, 0, st>>>(d_moves, d_acc, c_acc, d_pts, d_pairs, d_ppts);
     V3D_FCK(cudaGetLastError());
+    cudaEventRecord(ev1, st);
     uint32_t cnt[2] = {0, 0};
     V3D_FCK(cudaMemcpyAsync(cnt, c_acc, sizeof(cnt), cudaMemcpyDeviceToHost, st));
     V3D_FCK(cudaStreamSynchronize(st));
@@ -723,5 +738,7 @@ extern "C" int32_t v3d_fuse_mutually_supported_vertices(
     *n_pairs = n_acc;
     *n_moved = n_mv;
     ctx->last_launches = g_kernel_launches - launches0;
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, ev0, ev1) == cudaSuccess) ctx->last_ms = ms;
     return V3D_OK;
 }
