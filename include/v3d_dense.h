@@ -506,7 +506,8 @@ typedef struct v3d_fusion_pair {
  * FusionOutcome::moved_indices).  cancel (may be NULL) is polled between the
  * stages; a canceled call returns V3D_OK with zero stats, no pairs and the
  * points unchanged, the reference's FusionOutcome::default().  Device work
- * on the context's stream; the call returns when the results are on the host. */
+ * on the context's stream; the call returns when the results are on the host.
+ * Takes fewer than 2^30 points and 2^30 triangles (V3D_ERR_INVALID_ARGUMENT). */
 int32_t v3d_fuse_mutually_supported_vertices(
     v3d_context* ctx, v3d_point* points, uint64_t n_points,
     const v3d_mesh_triangle* triangles, uint64_t n_triangles, const int64_t* membership,

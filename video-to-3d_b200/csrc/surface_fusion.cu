@@ -10,9 +10,9 @@
 // vertex's triangles in index order (a stable radix sort of the incidence
 // entries by vertex), the global edge scale is the median of the sorted
 // lengths, and each vertex scans its 27 neighbour cells dz-dy-dx from -1 to 1
-// with every cell's vertices in index order (a stable sort of the eligible
-// vertices by cell), so the nearest-neighbour tie rule sees the candidates in
-// the reference's order.  Moves, pairs and moved indices come out of
+// with every cell's vertices in index order (cells found through a hash table,
+// the eligible vertices sorted stably by their cell's representative), so the
+// nearest-neighbour tie rule sees the candidates in the reference's order.  Moves, pairs and moved indices come out of
 // order-preserving compactions.  The outcome is the reference's bit for bit.
 //
 // The work is HBM- and latency-bound integer/f64 bookkeeping: per triangle
@@ -67,13 +67,27 @@ __device__ __forceinline__ int64_t as_i64(double v) {
 struct Cell {
     int64_t x, y, z;
 };
-__device__ __forceinline__ bool cell_less(const Cell& a, const Cell& b) {
-    if (a.x != b.x) return a.x < b.x;
-    if (a.y != b.y) return a.y < b.y;
-    return a.z < b.z;
+__device__ __forceinline__ bool cell_eq(const Cell& a, const Cell& b) {
+    return a.x == b.x && a.y == b.y && a.z == b.z;
 }
-struct CellLess {
-    __device__ bool operator()(const Cell& a, const Cell& b) const { return cell_less(a, b); }
+__device__ __forceinline__ uint32_t cell_hash(const Cell& c) {
+    uint64_t h = (uint64_t)c.x * 0x9E3779B97F4A7C15ull ^ (uint64_t)c.y * 0xC2B2AE3D27D4EB4Full ^
+                 (uint64_t)c.z * 0x165667B19E3779F9ull;
+    h ^= h >> 29;
+    h *= 0xBF58476D1CE4E5B9ull;
+    h ^= h >> 32;
+    return (uint32_t)h;
+}
+
+// An eligible vertex as the neighbour scan reads it, in cell order.
+struct Member {
+    float x, y, z;
+    uint32_t index;
+    int64_t group;
+    double scale;
+    D3 normal;
+    uint32_t rep;  // eligible position of its cell's representative
+    uint32_t pad;  // 64 bytes
 };
 
 struct Move {
@@ -197,37 +211,62 @@ __global__ void k_gather_cells(const uint32_t* __restrict__ idx, const uint32_t*
         out[k] = cell[idx[k]];
 }
 
-// First entry of each distinct cell in the cell-sorted eligible list.
-__global__ void k_cell_heads(const Cell* __restrict__ sorted, const uint32_t* __restrict__ count,
-                             uint8_t* __restrict__ head) {
+// The cell table: open addressing over `mask + 1` slots, each holding the
+// eligible position k of the first vertex that claimed its cell; every
+// eligible vertex learns its cell's representative, which keys the sort.
+__global__ void k_cell_insert(const Cell* __restrict__ el_cell, const uint32_t* __restrict__ count,
+                              uint32_t* __restrict__ table, uint32_t mask, uint32_t* __restrict__ rep) {
     const uint32_t m = *count;
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) {
-        const Cell c = sorted[k];
-        head[k] = k == 0 || c.x != sorted[k - 1].x || c.y != sorted[k - 1].y || c.z != sorted[k - 1].z;
+        const Cell c = el_cell[k];
+        uint32_t h = cell_hash(c) & mask, r = k;
+        for (uint32_t probe = 0; probe <= mask; ++probe, h = (h + 1) & mask) {
+            const uint32_t prev = atomicCAS(&table[h], kNone, k);
+            if (prev == kNone) break;
+            if (cell_eq(el_cell[prev], c)) {
+                r = prev;
+                break;
+            }
+        }
+        rep[k] = r;
+    }
+}
+
+// Cell-ordered member records and each cell's [begin, end) range, by
+// representative.
+__global__ void k_members(const uint32_t* __restrict__ sorted_rep, const uint32_t* __restrict__ sorted_v,
+                          const uint32_t* __restrict__ count, const v3d_point* __restrict__ pts,
+                          const int64_t* __restrict__ membership, const D3* __restrict__ normal,
+                          const double* __restrict__ scale, Member* __restrict__ members,
+                          uint32_t* __restrict__ begin, uint32_t* __restrict__ end) {
+    const uint32_t m = *count;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < m; j += gridDim.x * blockDim.x) {
+        const uint32_t v = sorted_v[j], r = sorted_rep[j];
+        const v3d_point p = pts[v];
+        members[j] = Member{p.x, p.y, p.z, v, membership[v], scale[v], normal[v], r, 0u};
+        if (j == 0 || sorted_rep[j - 1] != r) begin[r] = j;
+        if (j + 1 == m || sorted_rep[j + 1] != r) end[r] = j + 1;
     }
 }
 
 // The mutually-nearest search (surface_fusion.rs:418-481), a thread per
-// eligible vertex: its 27 neighbour cells in the reference's order, each
-// cell's vertices in index order, the reference's replace rule.
-__global__ void k_nearest(const v3d_point* __restrict__ pts, const int64_t* __restrict__ membership,
-                          const D3* __restrict__ normal, const double* __restrict__ scale,
-                          const uint32_t* __restrict__ el_vertex, const Cell* __restrict__ el_cell,
-                          const uint32_t* __restrict__ n_el_dev, const uint32_t* __restrict__ heads,
-                          const uint32_t* __restrict__ n_cells_dev, double global,
+// eligible vertex in cell order: its 27 neighbour cells in the reference's
+// order (dz, dy, dx from -1 to 1), each cell's vertices in index order, the
+// reference's replace rule.
+__global__ void k_nearest(const Member* __restrict__ members, const Cell* __restrict__ el_cell,
+                          const uint32_t* __restrict__ n_el_dev, const uint32_t* __restrict__ table,
+                          uint32_t mask, const uint32_t* __restrict__ begin,
+                          const uint32_t* __restrict__ end, double global,
                           uint32_t* __restrict__ nearest, double* __restrict__ nearest_d,
                           unsigned long long* __restrict__ counters) {
-    const uint32_t n_el = *n_el_dev, n_cells = *n_cells_dev;
+    const uint32_t n_el = *n_el_dev;
     const double gmax = dmul(global, kMaxGlobalEdgeFraction);
     unsigned long long cand = 0, rejn = 0;
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n_el; k += gridDim.x * blockDim.x) {
-        const uint32_t i = el_vertex[k];
-        const Cell c = el_cell[k];
-        D3 p;
-        position_of(pts[i], p);
-        const int64_t group = membership[i];
-        const D3 nrm = normal[i];
-        const double ls = scale[i];
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n_el; j += gridDim.x * blockDim.x) {
+        const Member me = members[j];
+        const uint32_t i = me.index;
+        const Cell c = el_cell[me.rep];
+        const D3 p{(double)me.x, (double)me.y, (double)me.z};
         uint32_t best = kNone;
         double best_d = 0.0;
         for (int dz = -1; dz <= 1; ++dz)
@@ -236,40 +275,36 @@ __global__ void k_nearest(const v3d_point* __restrict__ pts, const int64_t* __re
                     const Cell q{(int64_t)((uint64_t)c.x + (uint64_t)(int64_t)dx),
                                  (int64_t)((uint64_t)c.y + (uint64_t)(int64_t)dy),
                                  (int64_t)((uint64_t)c.z + (uint64_t)(int64_t)dz)};
-                    // lower bound among the distinct cells
-                    uint32_t lo = 0, hi = n_cells;
-                    while (lo < hi) {
-                        const uint32_t mid = (lo + hi) >> 1;
-                        if (cell_less(el_cell[heads[mid]], q))
-                            lo = mid + 1;
-                        else
-                            hi = mid;
+                    uint32_t r = kNone, h = cell_hash(q) & mask;
+                    for (uint32_t probe = 0; probe <= mask; ++probe, h = (h + 1) & mask) {
+                        const uint32_t s = table[h];
+                        if (s == kNone) break;
+                        if (cell_eq(el_cell[s], q)) {
+                            r = s;
+                            break;
+                        }
                     }
-                    if (lo == n_cells) continue;
-                    const Cell f = el_cell[heads[lo]];
-                    if (f.x != q.x || f.y != q.y || f.z != q.z) continue;
-                    const uint32_t end = lo + 1 < n_cells ? heads[lo + 1] : n_el;
-                    for (uint32_t j = heads[lo]; j < end; ++j) {
-                        const uint32_t o = el_vertex[j];
-                        if (o == i || membership[o] == group) continue;
-                        D3 op;
-                        position_of(pts[o], op);
-                        const double os = scale[o];
-                        const double maxd = fmin(dmul(fmin(ls, os), kMaxLocalEdgeFraction), gmax);
+                    if (r == kNone) continue;
+                    for (uint32_t k = begin[r]; k < end[r]; ++k) {
+                        const Member o = members[k];
+                        if (o.index == i || o.group == me.group) continue;
+                        const D3 op{(double)o.x, (double)o.y, (double)o.z};
+                        const double maxd =
+                            fmin(dmul(fmin(me.scale, o.scale), kMaxLocalEdgeFraction), gmax);
                         const double d = vnorm(vsub(op, p));
                         if (!isfinite(d) || d > maxd) continue;
-                        if (i < o) ++cand;
-                        const double align = fabs(vdot(nrm, normal[o]));
+                        if (i < o.index) ++cand;
+                        const double align = fabs(vdot(me.normal, o.normal));
                         if (align < kMinNormalAlignment) {
-                            if (i < o) ++rejn;
+                            if (i < o.index) ++rejn;
                             continue;
                         }
                         bool replace = best == kNone;
                         if (!replace)
                             replace = d < dsub(best_d, kGeometricEpsilon) ||
-                                      (fabs(dsub(d, best_d)) <= kGeometricEpsilon && o < best);
+                                      (fabs(dsub(d, best_d)) <= kGeometricEpsilon && o.index < best);
                         if (replace) {
-                            best = o;
+                            best = o.index;
                             best_d = d;
                         }
                     }
@@ -471,8 +506,8 @@ extern "C" int32_t v3d_fuse_mutually_supported_vertices(
     std::memset(stats, 0, sizeof(*stats));
     *n_pairs = 0;
     *n_moved = 0;
-    if (n >= 0xFFFFFFFFull || nt >= 0x40000000ull) {
-        ctx->last_error = "surface fusion takes fewer than 2^32 - 1 points and 2^30 triangles";
+    if (n >= 0x40000000ull || nt >= 0x40000000ull) {
+        ctx->last_error = "surface fusion takes fewer than 2^30 points and 2^30 triangles";
         return V3D_ERR_INVALID_ARGUMENT;
     }
     std::lock_guard<std::mutex> lock(ctx->mu);
@@ -487,16 +522,17 @@ extern "C" int32_t v3d_fuse_mutually_supported_vertices(
     while (vbits < 32 && (1ull << vbits) <= n) ++vbits;
 
     // ---- CUB temporary storage sizes ----
-    size_t t_scan = 0, t_pairs = 0, t_keys = 0, t_merge = 0;
+    size_t t_scan = 0, t_pairs = 0, t_keys = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, t_scan, (uint32_t*)nullptr, (uint32_t*)nullptr,
                                   (int)std::max<uint64_t>(nt, n + 1), st);
     cub::DeviceRadixSort::SortPairs(nullptr, t_pairs, (uint32_t*)nullptr, (uint32_t*)nullptr,
-                                    (uint32_t*)nullptr, (uint32_t*)nullptr, (int)ne, 0, vbits, st);
+                                    (uint32_t*)nullptr, (uint32_t*)nullptr,
+                                    (int)std::max<uint64_t>(ne, n), 0, vbits, st);
     cub::DeviceRadixSort::SortKeys(nullptr, t_keys, (double*)nullptr, (double*)nullptr, (int)ne, 0,
                                    64, st);
-    cub::DeviceMergeSort::StableSortPairs(nullptr, t_merge, (Cell*)nullptr, (uint32_t*)nullptr,
-                                          (int)n, CellLess(), st);
-    const size_t t_cub = std::max(std::max(t_scan, t_pairs), std::max(t_keys, t_merge));
+    const size_t t_cub = std::max(std::max(t_scan, t_pairs), t_keys);
+    uint32_t table_slots = 2;  // a power of two above twice the eligible vertices
+    while (table_slots < 2 * n + 2) table_slots <<= 1;
 
     // ---- arena ----
     Carve cv;
@@ -511,7 +547,10 @@ extern "C" int32_t v3d_fuse_mutually_supported_vertices(
                  o_scale = cv.take<double>(n), o_has = cv.take<uint8_t>(n),
                  o_elig = cv.take<uint8_t>(n), o_cell = cv.take<Cell>(n),
                  o_elv = cv.take<uint32_t>(n), o_elc = cv.take<Cell>(n),
-                 o_head = cv.take<uint8_t>(n), o_heads = cv.take<uint32_t>(n),
+                 o_table = cv.take<uint32_t>(table_slots), o_rep = cv.take<uint32_t>(n),
+                 o_rep2 = cv.take<uint32_t>(n), o_elv2 = cv.take<uint32_t>(n),
+                 o_mem_rec = cv.take<Member>(n), o_cbeg = cv.take<uint32_t>(n),
+                 o_cend = cv.take<uint32_t>(n),
                  o_near = cv.take<uint32_t>(n), o_neard = cv.take<double>(n),
                  o_flag = cv.take<uint8_t>(n), o_fused = cv.take<D3>(n),
                  o_first = cv.take<uint32_t>(n), o_moves = cv.take<Move>(n / 2 + 1),
@@ -551,8 +590,13 @@ extern "C" int32_t v3d_fuse_mutually_supported_vertices(
     auto* d_cell = reinterpret_cast<Cell*>(at(o_cell));
     auto* d_elv = reinterpret_cast<uint32_t*>(at(o_elv));
     auto* d_elc = reinterpret_cast<Cell*>(at(o_elc));
-    auto* d_head = reinterpret_cast<uint8_t*>(at(o_head));
-    auto* d_heads = reinterpret_cast<uint32_t*>(at(o_heads));
+    auto* d_table = reinterpret_cast<uint32_t*>(at(o_table));
+    auto* d_rep = reinterpret_cast<uint32_t*>(at(o_rep));
+    auto* d_rep2 = reinterpret_cast<uint32_t*>(at(o_rep2));
+    auto* d_elv2 = reinterpret_cast<uint32_t*>(at(o_elv2));
+    auto* d_members = reinterpret_cast<Member*>(at(o_mem_rec));
+    auto* d_cbeg = reinterpret_cast<uint32_t*>(at(o_cbeg));
+    auto* d_cend = reinterpret_cast<uint32_t*>(at(o_cend));
     auto* d_near = reinterpret_cast<uint32_t*>(at(o_near));
     auto* d_neard = reinterpret_cast<double*>(at(o_neard));
     auto* d_flag = reinterpret_cast<uint8_t*>(at(o_flag));
@@ -574,7 +618,6 @@ extern "C" int32_t v3d_fuse_mutually_supported_vertices(
     size_t cub_bytes = t_cub;
     // counts: [0] eligible, [1] cells, [2] moves, [3] accepted, [4] moved, [5] round flag
     uint32_t* c_el = d_counts + 0;
-    uint32_t* c_cells = d_counts + 1;
     uint32_t* c_moves = d_counts + 2;
     uint32_t* c_acc = d_counts + 3;
     uint32_t* c_moved = d_counts + 4;
@@ -650,20 +693,24 @@ extern "C" int32_t v3d_fuse_mutually_supported_vertices(
     V3D_FCK(cudaMemcpyAsync(&n_el, c_el, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     V3D_FCK(cudaStreamSynchronize(st));
     stats->eligible_vertices = n_el;
+    // cells: a hash table of representatives, the eligible vertices sorted by
+    // representative (stable, so each cell keeps index order), member records
+    V3D_FCK(cudaMemsetAsync(d_table, 0xFF, sizeof(uint32_t) * table_slots, st));
+    V3D_COUNTED k_cell_insert<<<grid_of(n), 256, 0, st>>>(d_elc, c_el, d_table, table_slots - 1, d_rep);
+    V3D_FCK(cudaGetLastError());
     if (n_el) {
         cub_bytes = t_cub;
-        V3D_FCK(cub::DeviceMergeSort::StableSortPairs(d_cub, cub_bytes, d_elc, d_elv, (int)n_el,
-                                                      CellLess(), st));
+        V3D_FCK(cub::DeviceRadixSort::SortPairs(d_cub, cub_bytes, d_rep, d_rep2, d_elv, d_elv2,
+                                                (int)n_el, 0, vbits, st));
     }
-    V3D_COUNTED k_cell_heads<<<grid_of(n), 256, 0, st>>>(d_elc, c_el, d_head);
+    V3D_COUNTED k_members<<<grid_of(n), 256, 0, st>>>(d_rep2, d_elv2, c_el, d_pts, d_mem, d_nrm, d_scale,
+                                                       d_members, d_cbeg, d_cend);
     V3D_FCK(cudaGetLastError());
-    V3D_FCK(launch_compact(d_head, 1, n_el, d_heads, c_cells, d_scratch, st));
 
     // ---- nearest cross-group neighbours, mutual pairs ----
     V3D_FCK(cudaMemsetAsync(d_near, 0xFF, sizeof(uint32_t) * n, st));
-    V3D_COUNTED k_nearest<<<grid_of(n), 256, 0, st>>>(d_pts, d_mem, d_nrm, d_scale, d_elv, d_elc, c_el,
-                                                       d_heads, c_cells, global, d_near, d_neard,
-                                                       d_ctr);
+    V3D_COUNTED k_nearest<<<grid_of(n), 256, 0, st>>>(d_members, d_elc, c_el, d_table, table_slots - 1,
+                                                       d_cbeg, d_cend, global, d_near, d_neard, d_ctr);
     V3D_FCK(cudaGetLastError());
     V3D_COUNTED k_mutual<<<grid_of(n), 256, 0, st>>>(d_pts, n, d_near, d_flag, d_fused);
     V3D_FCK(cudaGetLastError());
