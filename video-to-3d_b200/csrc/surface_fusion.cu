@@ -252,8 +252,10 @@ __global__ void k_members(const uint32_t* __restrict__ sorted_rep, const uint32_
 // The mutually-nearest search (surface_fusion.rs:418-481), a thread per
 // eligible vertex in cell order: its 27 neighbour cells in the reference's
 // order (dz, dy, dx from -1 to 1), each cell's vertices in index order, the
-// reference's replace rule.
-__global__ void k_nearest(const Member* __restrict__ members, const Cell* __restrict__ el_cell,
+// reference's replace rule.  The scan waits on L2 reads (cell table, member
+// records), so the kernel trades registers for resident warps: six blocks of
+// 256 threads per SM.
+__global__ void __launch_bounds__(256, 6) k_nearest(const Member* __restrict__ members, const Cell* __restrict__ el_cell,
                           const uint32_t* __restrict__ n_el_dev, const uint32_t* __restrict__ table,
                           uint32_t mask, const uint32_t* __restrict__ begin,
                           const uint32_t* __restrict__ end, double global,
