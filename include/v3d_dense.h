@@ -472,6 +472,65 @@ int32_t v3d_last_run_info(const v3d_context* ctx, v3d_run_info* out);
  * image; about 0.1 s on a B200. */
 int32_t v3d_measure_gather_rate(v3d_context* ctx, double* samples_per_second);
 
+/* ---- geometric depth-grid verification (colmap_surface.rs:158-314) --------
+ * The alternate dense provider's gate: every reference depth-grid sample is
+ * checked against each of its source views (parallax, visibility, an
+ * independent source depth within 2 %, colour within 105 summed RGB levels),
+ * and the samples any source verified are merged into one reference grid. */
+
+/* One view of external geometric depth (colmap_surface.rs:24-29, 158-173):
+ * its RGBA8 frame, its depth grid of ceil(width / stride) x ceil(height /
+ * stride) f32 samples in row-major order (0 = no depth) and its camera. */
+typedef struct v3d_depth_view {
+    const uint8_t* rgba;
+    const float* depth;
+    uint32_t width, height;
+    v3d_camera camera;
+} v3d_depth_view;
+
+/* VerificationFunnel (colmap_surface.rs:56-66). */
+typedef struct v3d_verification_funnel {
+    uint64_t reference_samples;
+    uint64_t missing_reference_depth;
+    uint64_t insufficient_parallax;
+    uint64_t behind_source;
+    uint64_t outside_source;
+    uint64_t missing_source_depth;
+    uint64_t depth_disagreement;
+    uint64_t color_disagreement;
+    uint64_t accepted;
+} v3d_verification_funnel;
+
+/* VerifiedSample (colmap_surface.rs:277-283): the reference sample's point
+ * (world position from the reference depth, the reference colour, the
+ * strongest agreement of its verifying sources as confidence), its grid site,
+ * and bit j set when the reference's j-th source view verified it. */
+typedef struct v3d_verified_sample {
+    v3d_point point;
+    v3d_grid_site site;
+    uint32_t source_mask;
+} v3d_verified_sample;
+
+/* verify_patch (colmap_surface.rs:175-275) of every reference against each of
+ * its sources, then verified_union (colmap_surface.rs:289-314), for many
+ * references in one device pass.  views [n_views] share one frame size;
+ * reference_views [n_references] and source_views [n_references x 4] index
+ * into views (sources in the grid's order, -1 = none; at most 4 per reference,
+ * as the export accepts).  stride and reference_stride are the grid spacing
+ * and the meshed spacing (a multiple of it).  samples get each reference's
+ * verified samples in grid row-major order, reference after reference;
+ * sample_offsets [n_references + 1] their ranges; capacity is the room in
+ * samples (V3D_ERR_INVALID_ARGUMENT, and nothing written, when the samples
+ * would not fit: n_references * ceil(width / reference_stride) *
+ * ceil(height / reference_stride) always does).  funnel gets the counts summed
+ * over every (reference, source) pair, as the export's diagnostics sum them. */
+int32_t v3d_verify_depth_grids(
+    v3d_context* ctx, const v3d_depth_view* views, uint64_t n_views,
+    const uint32_t* reference_views, uint64_t n_references, const int32_t* source_views,
+    uint32_t stride, uint32_t reference_stride, double focal,
+    v3d_verified_sample* samples, uint64_t capacity, uint64_t* sample_offsets,
+    v3d_verification_funnel* funnel);
+
 /* ---- cross-reference surface fusion (surface_fusion.rs:356-852) ---------
  * The first step of surface consolidation after the grid mesh
  * (consolidate_surface_recording_with_control, surface_fusion.rs:128-231,

@@ -19,7 +19,9 @@
 // surface_completion_tests.rs:56-113, mesh_legacy.rs:609-908,
 // mesh.rs:311-380) in oracle/oracle_selftest.cpp.  Cross-reference surface
 // fusion (surface_fusion.rs:316-852, oracle_fusion.cpp) is pinned the same way
-// by surface_fusion.rs:891-1070 and fusion_prepass_acceptance_tests.rs:31-57.
+// by surface_fusion.rs:891-1070 and fusion_prepass_acceptance_tests.rs:31-57,
+// and the geometric depth-grid verification (colmap_surface.rs:56-314,
+// oracle_colmap.cpp) by colmap_surface.rs:548-759.
 #pragma once
 
 #include <cstdint>
@@ -371,5 +373,50 @@ FusionOutcome fuse_mutually_supported_vertices(std::vector<Point3>& points,
                                                const std::vector<MeshTriangle>& triangles,
                                                const std::vector<int64_t>& membership,
                                                Control& control);
+
+// ---- colmap_surface.rs (oracle_colmap.cpp) ----
+// View (colmap_surface.rs:158-162): a frame, its depth grid and its camera
+struct DepthView {
+    uint32_t width = 0, height = 0;
+    const uint8_t* rgba = nullptr;
+    const float* depth = nullptr;
+    Camera camera;
+};
+// VerificationFunnel (colmap_surface.rs:56-79)
+struct Funnel {
+    size_t reference_samples = 0, missing_reference_depth = 0, insufficient_parallax = 0,
+           behind_source = 0, outside_source = 0, missing_source_depth = 0,
+           depth_disagreement = 0, color_disagreement = 0, accepted = 0;
+    void add(const Funnel& o) {
+        reference_samples += o.reference_samples;
+        missing_reference_depth += o.missing_reference_depth;
+        insufficient_parallax += o.insufficient_parallax;
+        behind_source += o.behind_source;
+        outside_source += o.outside_source;
+        missing_source_depth += o.missing_source_depth;
+        depth_disagreement += o.depth_disagreement;
+        color_disagreement += o.color_disagreement;
+        accepted += o.accepted;
+    }
+};
+// VerifiedSample (colmap_surface.rs:277-283)
+struct VerifiedSample {
+    Point3 point;
+    GridSite site;
+    std::vector<size_t> sources;
+};
+// SurfaceTopology (colmap_surface.rs:114-121)
+struct Topology {
+    size_t islands = 0, small_islands = 0, small_island_triangles = 0,
+           largest_island_triangles = 0, boundary_edges = 0;
+};
+double min_parallax_cos();
+const char* dominant_rejection(const Funnel& f);
+std::vector<std::pair<Point3, GridSite>> verify_patch(const DepthView& ref, const DepthView& src,
+                                                      size_t stride, size_t reference_stride,
+                                                      double focal, Funnel& funnel);
+std::vector<VerifiedSample> verified_union(
+    const std::vector<std::pair<size_t, std::vector<std::pair<Point3, GridSite>>>>& candidates);
+Topology surface_topology(size_t vertex_count, const std::vector<MeshTriangle>& triangles);
 
 }  // namespace v3do

@@ -778,6 +778,97 @@ void controlled_fusion_prepass_preserves_actual_geometry_evidence() {
     }
 }
 
+// ---- colmap_surface.rs:548-759 ----
+// colmap_surface.rs:548-631
+void sources_verifying_one_sample_share_one_vertex() {
+    auto sample = [](uint32_t x, uint32_t y, float c) {
+        return std::make_pair(Point3{(float)x, (float)y, 5.f, c, 1, 2, 3}, GridSite{x, y});
+    };
+    std::vector<std::pair<size_t, std::vector<std::pair<Point3, GridSite>>>> cand = {
+        {7, {sample(0, 0, 0.9f), sample(4, 0, 0.9f), sample(0, 4, 0.9f), sample(4, 4, 0.9f)}},
+        {3, {sample(4, 0, 0.95f), sample(8, 0, 0.95f), sample(4, 4, 0.8f), sample(8, 4, 0.95f)}}};
+    auto u = verified_union(cand);
+    std::vector<std::pair<uint32_t, uint32_t>> sites;
+    for (auto& v : u) sites.emplace_back(v.site.x, v.site.y);
+    CHECK((sites == std::vector<std::pair<uint32_t, uint32_t>>{{0, 0}, {4, 0}, {8, 0}, {0, 4}, {4, 4}, {8, 4}}));
+    std::vector<std::vector<size_t>> srcs;
+    for (auto& v : u) srcs.push_back(v.sources);
+    CHECK((srcs == std::vector<std::vector<size_t>>{{7}, {3, 7}, {3}, {7}, {3, 7}, {3}}));
+    CHECK(u.size() == 6 && u[1].point.confidence == 0.95f && u[4].point.confidence == 0.9f);
+    if (u.size() != 6) return;
+    std::vector<Camera> cams(3);
+    cams[0].frame_index = 0;
+    cams[1].frame_index = 3;
+    cams[2].frame_index = 7;
+    std::vector<Point3> pts;
+    std::vector<GridSite> gs;
+    for (auto& v : u) {
+        Point3 p = v.point;
+        p.x = ((float)v.site.x + 0.5f - 6.f) / 20.f * 5.f;
+        p.y = ((float)v.site.y + 0.5f - 4.f) / 20.f * 5.f;
+        pts.push_back(p);
+        gs.push_back(v.site);
+    }
+    MeshDenseInput d;
+    d.attempted = true;
+    d.reference_frame = 0;
+    d.grid_stride = 4;
+    Control ctl = never();
+    auto m = reconstruct_dense_mesh_with_control(pts, gs, d, cams, 12, 8, 20.0, ctl);
+    CHECK(m.triangles.size() == 4);
+    CHECK(surface_topology(pts.size(), m.triangles).islands == 1);
+}
+
+// colmap_surface.rs:633-730
+void plane_requires_agreeing_depth_color_and_camera_baseline() {
+    std::vector<uint8_t> frame(24 * 16 * 4, 100), other_color(24 * 16 * 4, 200);
+    std::vector<float> map(24, 5.f), wrong(24, 8.f);
+    Camera first, second;
+    second.frame_index = 1;
+    second.t[0] = -1.0;
+    DepthView reference{24, 16, frame.data(), map.data(), first};
+    DepthView source{24, 16, frame.data(), map.data(), second};
+    Funnel f;
+    CHECK(verify_patch(reference, source, 4, 4, 20.0, f).size() == 20);
+    CHECK(f.reference_samples == 24 && f.outside_source == 4 && f.accepted == 20 &&
+          f.missing_reference_depth == 0 && f.insufficient_parallax == 0 && f.behind_source == 0 &&
+          f.missing_source_depth == 0 && f.depth_disagreement == 0 && f.color_disagreement == 0);
+    Funnel g;
+    auto coarse = verify_patch(reference, source, 4, 8, 20.0, g);
+    CHECK(coarse.size() == 4);
+    bool on = true;
+    for (auto& [p, site] : coarse) on = on && site.x % 8 == 0 && site.y % 8 == 0;
+    CHECK(on);
+    DepthView w = source;
+    w.depth = wrong.data();
+    DepthView c = source;
+    c.rgba = other_color.data();
+    DepthView pa = source;
+    pa.camera = first;
+    const std::pair<DepthView, const char*> cases[] = {
+        {w, "depth_disagreement"}, {c, "color_disagreement"}, {pa, "insufficient_parallax"}};
+    for (auto& [view, expected] : cases) {
+        Funnel h;
+        CHECK(verify_patch(reference, view, 4, 4, 20.0, h).empty());
+        CHECK(h.accepted == 0);
+        const char* dom = dominant_rejection(h);
+        CHECK(dom && std::string(dom) == expected);
+    }
+}
+
+// colmap_surface.rs:732-759
+void topology_counts_islands_and_open_boundaries() {
+    auto face = [](size_t a, size_t b, size_t c) { return MeshTriangle{a, b, c, 1.f}; };
+    std::vector<MeshTriangle> tris = {face(0, 1, 2), face(1, 3, 2), face(4, 5, 6), face(5, 7, 6)};
+    Topology t = surface_topology(8, tris);
+    CHECK(t.islands == 2 && t.small_islands == 2 && t.small_island_triangles == 4 &&
+          t.largest_island_triangles == 2 && t.boundary_edges == 8);
+    std::vector<MeshTriangle> large;
+    for (size_t i = 0; i < 32; ++i) large.push_back(face(i, i + 1, i + 2));
+    Topology l = surface_topology(34, large);
+    CHECK(l.islands == 1 && l.small_islands == 0 && l.largest_island_triangles == 32);
+}
+
 struct Test {
     const char* name;
     void (*fn)();
@@ -832,6 +923,10 @@ extern "C" int32_t v3do_selftest(char* report, uint64_t capacity, int32_t* check
          never_fuses_vertices_from_the_same_evidence_group},
         {"controlled_fusion_prepass_preserves_actual_geometry_evidence",
          controlled_fusion_prepass_preserves_actual_geometry_evidence},
+        {"sources_verifying_one_sample_share_one_vertex", sources_verifying_one_sample_share_one_vertex},
+        {"plane_requires_agreeing_depth_color_and_camera_baseline",
+         plane_requires_agreeing_depth_color_and_camera_baseline},
+        {"topology_counts_islands_and_open_boundaries", topology_counts_islands_and_open_boundaries},
     };
     std::string names;
     for (const Test& t : tests) {

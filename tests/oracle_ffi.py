@@ -59,6 +59,10 @@ class Oracle:
             C.c_void_p, _P(abi.FusionStats), C.c_void_p, _P(C.c_uint64), C.c_void_p,
             _P(C.c_uint64)]
         L.v3do_fuse_mutually_supported_vertices.restype = C.c_int32
+        L.v3do_verify_depth_grids.argtypes = [
+            C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint32, C.c_uint32,
+            C.c_double, C.c_void_p, C.c_uint64, C.c_void_p, _P(abi.VerificationFunnel)]
+        L.v3do_verify_depth_grids.restype = C.c_int32
 
     def fuse_mutually_supported_vertices(self, points, triangles, membership, control=None):
         """surface_fusion.rs:369-549 on the CPU: moves `points` in place."""
@@ -67,6 +71,16 @@ class Oracle:
                               triangles, membership, control)
         assert st == 0, st
         return out
+
+    def verify_depth_grids(self, views, reference_views, source_views, stride, reference_stride,
+                           focal):
+        """colmap_surface.rs:175-314 on the CPU: (samples per reference, funnel)."""
+        from v3d import dense
+        st, per_ref, funnel = dense._verify(self.lib.v3do_verify_depth_grids, (), views,
+                                            reference_views, source_views, stride,
+                                            reference_stride, focal)
+        assert st == 0, st
+        return per_ref, funnel
 
     def selftest(self):
         buf = C.create_string_buffer(1 << 16)

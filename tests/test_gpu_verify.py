@@ -1,0 +1,57 @@
+"""Depth-grid verification on the device against the CPU oracle, bit for bit:
+every verified sample (position, colour, confidence, site, verifying sources)
+and every funnel count, on the reference's own test plane and its rejected
+variants, on seeded clips at three grid spacings, on a full-size clip, and on
+the edge cases of no references and references without sources."""
+import numpy as np
+import pytest
+
+from v3d import dense
+
+from tests import depth_grid_scenes
+from tests.oracle_ffi import Oracle
+
+
+def _compare(views, refs, sources, stride, rstride, focal):
+    g, gf = dense.Context(0).verify_depth_grids(views, refs, sources, stride, rstride, focal)
+    o, of = Oracle().verify_depth_grids(views, refs, sources, stride, rstride, focal)
+    assert gf == of
+    assert len(g) == len(o)
+    for a, b in zip(g, o):
+        assert a.tobytes() == b.tobytes()
+    return g, gf
+
+
+@pytest.mark.gpu
+def test_reference_plane_and_its_rejections():
+    frame, other_color, first, second, depth, wrong = depth_grid_scenes.reference_plane()
+    views = [(frame, depth, first), (frame, depth, second), (frame, wrong, second),
+             (other_color, depth, second), (frame, depth, first)]
+    per_ref, funnel = _compare(views, [0], [[1]], 4, 4, 20.0)
+    assert len(per_ref[0]) == 20 and funnel["outside_source"] == 4
+    per_ref, _ = _compare(views, [0], [[1]], 4, 8, 20.0)
+    assert len(per_ref[0]) == 4
+    per_ref, funnel = _compare(views, [0, 0, 0, 0], [[2], [3], [4], [1, 2, 3, 4]], 4, 4, 20.0)
+    assert [len(p) for p in per_ref] == [0, 0, 0, 20]
+    assert (per_ref[3]["source_mask"] == 1).all()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("seed,stride,rstride", [(1, 2, 2), (2, 2, 4), (3, 4, 8), (4, 3, 6)])
+def test_seeded_clips(seed, stride, rstride):
+    views, refs, sources, focal = depth_grid_scenes.clip_views(seed, stride=stride)
+    per_ref, funnel = _compare(views, refs, sources, stride, rstride, focal)
+    assert funnel["accepted"] > 0 and funnel["color_disagreement"] >= 0
+    assert any(((p["source_mask"] & (p["source_mask"] - 1)) > 0).any() for p in per_ref)
+
+
+@pytest.mark.gpu
+def test_full_size_clip_and_edge_cases():
+    views, refs, sources, focal = depth_grid_scenes.clip_views(5, width=640, height=360,
+                                                               frames=12, stride=2)
+    per_ref, funnel = _compare(views, refs, sources, 2, 4, focal)
+    assert funnel["reference_samples"] > 100000
+    per_ref, funnel = _compare(views, [], [], 2, 4, focal)
+    assert per_ref == [] and all(v == 0 for v in funnel.values())
+    per_ref, funnel = _compare(views, [0, 3], [[], [2]], 2, 2, focal)
+    assert len(per_ref[0]) == 0 and len(per_ref[1]) > 0

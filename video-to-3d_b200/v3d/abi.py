@@ -232,7 +232,25 @@ class FusionPair(C.Structure):
     _fields_ = [("first", C.c_uint64), ("second", C.c_uint64)]
 
 
+class DepthView(C.Structure):
+    _fields_ = [("rgba", C.c_void_p), ("depth", C.c_void_p), ("width", C.c_uint32),
+                ("height", C.c_uint32), ("camera", Camera)]
+
+
+class VerificationFunnel(C.Structure):
+    _fields_ = [(name, C.c_uint64) for name in (
+        "reference_samples", "missing_reference_depth", "insufficient_parallax", "behind_source",
+        "outside_source", "missing_source_depth", "depth_disagreement", "color_disagreement",
+        "accepted")]
+
+
+class VerifiedSample(C.Structure):
+    _fields_ = [("point", Point), ("site", GridSite), ("source_mask", C.c_uint32)]
+
+
 STRUCTS = {
+    "v3d_depth_view": DepthView, "v3d_verification_funnel": VerificationFunnel,
+    "v3d_verified_sample": VerifiedSample,
     "v3d_fusion_stats": FusionStats, "v3d_fusion_pair": FusionPair,
     "v3d_frame": Frame, "v3d_camera": Camera, "v3d_profile": Profile, "v3d_point": Point,
     "v3d_grid_site": GridSite, "v3d_point_attributes": PointAttributes,

@@ -107,6 +107,10 @@ def library():
         C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64, C.c_void_p, abi.CANCEL_FN,
         C.c_void_p, _P(abi.FusionStats), C.c_void_p, _P(C.c_uint64), C.c_void_p, _P(C.c_uint64)]
     L.v3d_fuse_mutually_supported_vertices.restype = C.c_int32
+    L.v3d_verify_depth_grids.argtypes = [
+        C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint32,
+        C.c_uint32, C.c_double, C.c_void_p, C.c_uint64, C.c_void_p, _P(abi.VerificationFunnel)]
+    L.v3d_verify_depth_grids.restype = C.c_int32
     L.v3d_measure_gather_rate.argtypes = [C.c_void_p, _P(C.c_double)]
     L.v3d_measure_gather_rate.restype = C.c_int32
     L.v3d_last_run_info.argtypes = [C.c_void_p, _P(abi.RunInfo)]
@@ -302,6 +306,16 @@ class Context:
             float(focal), fn, None, C.byref(out)))
         return self._mesh(out)
 
+    def verify_depth_grids(self, views, reference_views, source_views, stride, reference_stride,
+                           focal):
+        """verify_patch and verified_union (colmap_surface.rs:175-314) for every
+        reference on the device: (samples per reference, funnel dict)."""
+        st, per_ref, funnel = _verify(self.lib.v3d_verify_depth_grids, (self.handle,), views,
+                                      reference_views, source_views, stride, reference_stride,
+                                      focal)
+        self._check(st)
+        return per_ref, funnel
+
     def fuse_mutually_supported_vertices(self, points, triangles, membership, control=None):
         """fuse_mutually_supported_vertices_with_control (surface_fusion.rs:369-549)
         on the device: moves `points` in place and returns a FusionOutcome."""
@@ -352,6 +366,46 @@ def _fuse(lib_fn, head, points, triangles, membership, control):
                 None, C.byref(stats), pairs.ctypes.data, C.byref(n_pairs), moved.ctypes.data,
                 C.byref(n_moved))
     return st, fusion_outcome(stats, pairs, n_pairs.value, moved, n_moved.value)
+
+
+VERIFIED_DTYPE = np.dtype([("x", "<f4"), ("y", "<f4"), ("z", "<f4"), ("confidence", "<f4"),
+                           ("r", "u1"), ("g", "u1"), ("b", "u1"), ("pad", "u1"),
+                           ("site_x", "<u4"), ("site_y", "<u4"), ("source_mask", "<u4")])
+
+
+def _verify(lib_fn, head, views, reference_views, source_views, stride, reference_stride, focal):
+    """Shared by the device entry point and the oracle: views is a list of
+    (rgba uint8 [h, w, 4], depth float32 [rows, cols], camera); source_views one
+    list of at most 4 view indices per reference.  Returns (samples per
+    reference as VERIFIED_DTYPE arrays, funnel dict)."""
+    keep = []
+    arr = (abi.DepthView * max(len(views), 1))()
+    for i, (rgba, depth, cam) in enumerate(views):
+        rgba = np.ascontiguousarray(rgba, dtype=np.uint8)
+        depth = np.ascontiguousarray(depth, dtype=np.float32)
+        keep += [rgba, depth]
+        R = np.asarray(cam.rotation, dtype=np.float64).reshape(9)
+        t = np.asarray(cam.translation, dtype=np.float64).reshape(3)
+        arr[i] = abi.DepthView(rgba.ctypes.data, depth.ctypes.data, rgba.shape[1], rgba.shape[0],
+                               abi.Camera(int(cam.frame_index), (C.c_double * 9)(*R),
+                                          (C.c_double * 3)(*t)))
+    n_ref = len(reference_views)
+    refs = np.ascontiguousarray(reference_views, dtype=np.uint32)
+    src = np.full((max(n_ref, 1), 4), -1, dtype=np.int32)
+    for r, s in enumerate(source_views):
+        if len(s) > 4:
+            raise ValueError("at most 4 source views per reference")
+        src[r, :len(s)] = s
+    h, w = (views[0][0].shape[0], views[0][0].shape[1]) if views else (0, 0)
+    cap = max(n_ref * (-(-w // reference_stride)) * (-(-h // reference_stride)), 1)
+    out = np.zeros(cap, dtype=VERIFIED_DTYPE)
+    offsets = np.zeros(n_ref + 1, dtype=np.uint64)
+    funnel = abi.VerificationFunnel()
+    st = lib_fn(*head, arr, len(views), refs.ctypes.data, n_ref, src.ctypes.data, int(stride),
+                int(reference_stride), float(focal), out.ctypes.data, cap, offsets.ctypes.data,
+                C.byref(funnel))
+    per_ref = [out[int(offsets[r]):int(offsets[r + 1])].copy() for r in range(n_ref)] if st >= 0 else []
+    return st, per_ref, {name: int(getattr(funnel, name)) for name, _ in funnel._fields_}
 
 
 def has_distributed_landmarks(frames, cameras, sparse_points, focal, control=None):
