@@ -56,12 +56,14 @@ def parse():
     ap.add_argument("--frames", type=int, default=FRAMES)
     ap.add_argument("--no-cpu-baseline", action="store_true",
                     help="skip the CPU baseline leg (profiling runs)")
-    ap.add_argument("--config", choices=["full", "small", "heavy", "batched", "served", "fusion"],
+    ap.add_argument("--config", choices=["full", "small", "heavy", "batched", "served", "fusion",
+                                         "verify"],
                     default="full",
                     help="full: the headline line (default); small: 360x202 1+4 views; heavy: "
                          "bf16 16 views 256 planes 9x9; batched: 32 uneven clips through the "
                          "server vs one request at a time; served: Poisson arrivals, p50/p99; "
-                         "fusion: cross-reference surface fusion of the full clip's patches")
+                         "fusion: cross-reference surface fusion of the full clip's patches; "
+                         "verify: geometric depth-grid verification of the full clip")
     ap.add_argument("--rates", default="50,200,800", help="served: request rates (req/s)")
     ap.add_argument("--duration", type=float, default=3.0, help="served: seconds of arrivals")
     ap.add_argument("--clips", type=int, default=32, help="batched/served: number of clips")
@@ -91,19 +93,21 @@ def workload(args):
 
 
 def load_clip(seed, frames):
-    """The seeded clip, cached under the system temp directory between runs."""
+    """The seeded clip (with its true depth maps), cached under the system temp
+    directory between runs."""
     from v3d import synth
-    path = os.path.join(tempfile.gettempdir(), "v3d_clip_%d_%d_%d_%d.npz" %
+    path = os.path.join(tempfile.gettempdir(), "v3d_clip2_%d_%d_%d_%d.npz" %
                         (seed, WIDTH, HEIGHT, frames))
     if os.path.exists(path):
         z = np.load(path)
         from v3d.types import RegisteredCamera
         cams = [RegisteredCamera(i, z["R"][i], z["t"][i]) for i in range(frames)]
-        return synth.Clip(WIDTH, HEIGHT, float(z["focal"]), cams, list(z["images"]), [], z["sparse"])
+        return synth.Clip(WIDTH, HEIGHT, float(z["focal"]), cams, list(z["images"]),
+                          list(z["depths"]), z["sparse"])
     clip = synth.full_clip(seed=seed, width=WIDTH, height=HEIGHT, n_frames=frames)
     np.savez(path, images=np.stack(clip.images), R=np.stack([c.rotation for c in clip.cameras]),
              t=np.stack([c.translation for c in clip.cameras]), sparse=clip.sparse,
-             focal=clip.focal)
+             focal=clip.focal, depths=np.stack(clip.depths).astype(np.float32))
     return clip
 
 
@@ -638,6 +642,104 @@ def run_fusion(args):
     ctx.close()
 
 
+def verify_views(clip, stride=2, seed=5):
+    """External depth for every keyframe: the true depth on the grid with 0.8 %
+    multiplicative noise and 5 % holes, RGBA frames (every third view tinted),
+    each keyframe a reference against its 4 nearest keyframes."""
+    from v3d import synth
+    rng = np.random.default_rng(seed)
+    views = []
+    for k, (img, depth, cam) in enumerate(zip(clip.images, clip.depths, clip.cameras)):
+        rgba = synth.to_rgba8(img).copy()
+        if k % 3 == 1:
+            rgba[..., 0] = np.clip(rgba[..., 0].astype(np.int32) + 70, 0, 255).astype(np.uint8)
+        # the depth as the clip cache stores it (f32), so fresh and cached runs agree
+        g = np.asarray(depth, dtype=np.float32).astype(np.float64)[::stride, ::stride]
+        g = g * (1.0 + rng.normal(0.0, 0.008, g.shape))
+        g[~np.isfinite(g)] = 0.0
+        g[rng.random(g.shape) < 0.05] = 0.0
+        views.append((rgba, g.astype(np.float32), cam))
+    n = len(views)
+    sources = [[s for _, s in sorted((abs(s - r), s) for s in range(n) if s != r)[:4]]
+               for r in range(n)]
+    return views, list(range(n)), sources
+
+
+def run_verify(args):
+    """Geometric depth-grid verification (colmap_surface.rs:175-314) of the full
+    clip: every keyframe's grid (stride 2) checked against its 4 nearest views
+    and merged at spacing 4, one v3d_verify_depth_grids call per step."""
+    import torch
+    from v3d import dense
+    clip = load_clip(2, args.frames)
+    stride, rstride = 2, 4
+    views, refs, sources = verify_views(clip, stride)
+    ctx = dense.Context(0)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    for _ in range(args.warmup):
+        ctx.verify_depth_grids(views, refs, sources, stride, rstride, clip.focal)
+    dev, wall, launches = [], [], 0
+    clocks = Clocks(0)
+    clocks.start()
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        per_ref, funnel = ctx.verify_depth_grids(views, refs, sources, stride, rstride, clip.focal)
+        wall.append(time.perf_counter() - t0)
+        info = ctx.last_run_info()
+        dev.append(info["device_ms"] / 1e3)
+        launches += int(info["kernel_launches"])
+    clk = clocks.stop()
+    checks = funnel["reference_samples"]
+    dev_s, wall_s = float(np.mean(dev)), float(np.mean(wall))
+    n = len(views)
+    frame_bytes = WIDTH * HEIGHT * 4
+    grid_bytes = views[0][1].nbytes
+    samples = sum(len(p) for p in per_ref)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    alg = n * (frame_bytes + grid_bytes) + samples * 32
+    line = {"metric": "depth-grid samples verified per source/s", "value": checks / dev_s,
+            "unit": "sample-source checks/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dev_s * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: the seeded clip's true depth with noise and holes",
+            "config": {"workload": "depth-grid verification of the full clip %dx%d: %d keyframes, "
+                                   "grid stride %d, meshed at %d, each keyframe against its 4 "
+                                   "nearest" % (WIDTH, HEIGHT, n, stride, rstride),
+                       "l2": "flushed between timed steps (256 MiB write)"},
+            "clocks": clk,
+            "e2e": {"value": checks / wall_s, "unit": "sample-source checks/s",
+                    "h2d_bytes_per_step": n * (frame_bytes + grid_bytes),
+                    "d2h_bytes_per_step": samples * 32, "ms_per_step": wall_s * 1e3},
+            "gpu_launches": launches, "funnel": funnel, "verified_samples": samples,
+            "roofline": {"bound": "hbm", "kernel": "k_verify (one thread per reference sample, "
+                                                   "its sources in order)",
+                         "achieved": alg / dev_s / 1e9, "peak": hbm, "unit": "GB/s",
+                         "frac": alg / dev_s / 1e9 / hbm, "traffic": None,
+                         "algorithmic_bytes": alg,
+                         "note": "algorithmic bytes = every frame and depth grid read once plus "
+                                 "the verified samples written; the checks re-read source "
+                                 "frames and grids from L2"}}
+    if not args.no_cpu_baseline:
+        from tests.oracle_ffi import Oracle
+        k = 6
+        t0 = time.perf_counter()
+        _, f = Oracle().verify_depth_grids(views, refs[:k], sources[:k], stride, rstride, clip.focal)
+        cpu_s = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": f["reference_samples"] / cpu_s,
+                                "unit": "sample-source checks/s", "cores": 1, "kind": "port",
+                                "sample": "the first %d references (%d checks), one thread"
+                                          % (k, f["reference_samples"])}
+    print(json.dumps(line), flush=True)
+    ctx.close()
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
@@ -651,6 +753,8 @@ def main():
         run_plain_config(args)
     elif args.config == "fusion":
         run_fusion(args)
+    elif args.config == "verify":
+        run_verify(args)
     else:
         run_ours(args, rank, world, local)
 

@@ -359,8 +359,8 @@ def _fuse(lib_fn, head, points, triangles, membership, control):
     n = len(points)
     fn, _keep = types.cancel_callback(control)
     stats = abi.FusionStats()
-    pairs = np.zeros((max(n // 2, 1), 2), dtype=np.uint64)
-    moved = np.zeros(max(n, 1), dtype=np.uint64)
+    pairs = np.empty((max(n // 2, 1), 2), dtype=np.uint64)
+    moved = np.empty(max(n, 1), dtype=np.uint64)
     n_pairs, n_moved = C.c_uint64(), C.c_uint64()
     st = lib_fn(*head, points.ctypes.data, n, tris.ctypes.data, len(tris), mem.ctypes.data, fn,
                 None, C.byref(stats), pairs.ctypes.data, C.byref(n_pairs), moved.ctypes.data,
@@ -398,13 +398,14 @@ def _verify(lib_fn, head, views, reference_views, source_views, stride, referenc
         src[r, :len(s)] = s
     h, w = (views[0][0].shape[0], views[0][0].shape[1]) if views else (0, 0)
     cap = max(n_ref * (-(-w // reference_stride)) * (-(-h // reference_stride)), 1)
-    out = np.zeros(cap, dtype=VERIFIED_DTYPE)
+    out = np.empty(cap, dtype=VERIFIED_DTYPE)
     offsets = np.zeros(n_ref + 1, dtype=np.uint64)
     funnel = abi.VerificationFunnel()
     st = lib_fn(*head, arr, len(views), refs.ctypes.data, n_ref, src.ctypes.data, int(stride),
                 int(reference_stride), float(focal), out.ctypes.data, cap, offsets.ctypes.data,
                 C.byref(funnel))
-    per_ref = [out[int(offsets[r]):int(offsets[r + 1])].copy() for r in range(n_ref)] if st >= 0 else []
+    # views into one buffer: no copy per reference
+    per_ref = [out[int(offsets[r]):int(offsets[r + 1])] for r in range(n_ref)] if st >= 0 else []
     return st, per_ref, {name: int(getattr(funnel, name)) for name, _ in funnel._fields_}
 
 
