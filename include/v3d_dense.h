@@ -531,6 +531,26 @@ int32_t v3d_verify_depth_grids(
     v3d_verified_sample* samples, uint64_t capacity, uint64_t* sample_offsets,
     v3d_verification_funnel* funnel);
 
+/* SurfaceTopology (colmap_surface.rs:114-121): connected islands of a mesh
+ * (vertices joined by triangle edges; islands counted over the triangles),
+ * those with fewer than 32 triangles and their triangles, the largest
+ * island's triangles, and the edges used by exactly one triangle. */
+typedef struct v3d_surface_topology {
+    uint64_t islands;
+    uint64_t small_islands;
+    uint64_t small_island_triangles;
+    uint64_t largest_island_triangles;
+    uint64_t boundary_edges;
+} v3d_surface_topology;
+
+/* surface_topology (colmap_surface.rs:125-157) on the device, for the export's
+ * diagnostics.  Every index must be below vertex_count (the reference panics
+ * otherwise; here V3D_ERR_INVALID_ARGUMENT); fewer than 2^32 vertices and
+ * 2^30 triangles. */
+int32_t v3d_surface_topology_of(v3d_context* ctx, const v3d_mesh_triangle* triangles,
+                                uint64_t n_triangles, uint64_t vertex_count,
+                                v3d_surface_topology* out);
+
 /* ---- cross-reference surface fusion (surface_fusion.rs:356-852) ---------
  * The first step of surface consolidation after the grid mesh
  * (consolidate_surface_recording_with_control, surface_fusion.rs:128-231,

@@ -268,3 +268,23 @@ extern "C" int32_t v3do_verify_depth_grids(const v3d_depth_view* views, uint64_t
     funnel->accepted = total.accepted;
     return V3D_OK;
 }
+
+extern "C" int32_t v3do_surface_topology_of(const v3d_mesh_triangle* triangles, uint64_t n_triangles,
+                                            uint64_t vertex_count, v3d_surface_topology* out) {
+    if (!out || (n_triangles && !triangles)) return V3D_ERR_INVALID_ARGUMENT;
+    std::vector<MeshTriangle> tris(n_triangles);
+    for (uint64_t t = 0; t < n_triangles; ++t) {
+        if (triangles[t].a >= vertex_count || triangles[t].b >= vertex_count ||
+            triangles[t].c >= vertex_count)
+            return V3D_ERR_INVALID_ARGUMENT;
+        tris[t] = MeshTriangle{(size_t)triangles[t].a, (size_t)triangles[t].b,
+                               (size_t)triangles[t].c, triangles[t].confidence};
+    }
+    const Topology top = surface_topology(vertex_count, tris);
+    out->islands = top.islands;
+    out->small_islands = top.small_islands;
+    out->small_island_triangles = top.small_island_triangles;
+    out->largest_island_triangles = top.largest_island_triangles;
+    out->boundary_edges = top.boundary_edges;
+    return V3D_OK;
+}

@@ -63,6 +63,9 @@ class Oracle:
             C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint32, C.c_uint32,
             C.c_double, C.c_void_p, C.c_uint64, C.c_void_p, _P(abi.VerificationFunnel)]
         L.v3do_verify_depth_grids.restype = C.c_int32
+        L.v3do_surface_topology_of.argtypes = [C.c_void_p, C.c_uint64, C.c_uint64,
+                                               _P(abi.SurfaceTopology)]
+        L.v3do_surface_topology_of.restype = C.c_int32
 
     def fuse_mutually_supported_vertices(self, points, triangles, membership, control=None):
         """surface_fusion.rs:369-549 on the CPU: moves `points` in place."""
@@ -81,6 +84,13 @@ class Oracle:
                                             reference_stride, focal)
         assert st == 0, st
         return per_ref, funnel
+
+    def surface_topology(self, triangles, vertex_count):
+        """colmap_surface.rs:125-157 on the CPU."""
+        from v3d import dense
+        st, out = dense._topology(self.lib.v3do_surface_topology_of, (), triangles, vertex_count)
+        assert st == 0, st
+        return out
 
     def selftest(self):
         buf = C.create_string_buffer(1 << 16)

@@ -2,7 +2,9 @@
 every verified sample (position, colour, confidence, site, verifying sources)
 and every funnel count, on the reference's own test plane and its rejected
 variants, on seeded clips at three grid spacings, on a full-size clip, and on
-the edge cases of no references and references without sources."""
+the edge cases of no references and references without sources.  The mesh
+topology figures of the same module against the oracle on the reference's
+cases, grid meshes, triangle soups and long chains."""
 import numpy as np
 import pytest
 
@@ -55,3 +57,40 @@ def test_full_size_clip_and_edge_cases():
     assert per_ref == [] and all(v == 0 for v in funnel.values())
     per_ref, funnel = _compare(views, [0, 3], [[], [2]], 2, 2, focal)
     assert len(per_ref[0]) == 0 and len(per_ref[1]) > 0
+
+
+def _tris(a, b, c):
+    from v3d import types
+    t = np.zeros(len(a), dtype=types.TRIANGLE_DTYPE)
+    t["a"], t["b"], t["c"], t["confidence"] = a, b, c, 1.0
+    return t
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["reference", "soup", "chain", "grids", "fusion_mesh"])
+def test_surface_topology(case):
+    rng = np.random.default_rng(11)
+    if case == "reference":
+        tris, n = _tris([0, 1, 4, 5], [1, 3, 5, 7], [2, 2, 6, 6]), 8
+    elif case == "soup":  # many small islands, repeated and degenerate triangles
+        n = 200000
+        a = rng.integers(0, n, 150000)
+        tris = _tris(a, np.minimum(a + rng.integers(0, 3, a.size), n - 1),
+                     np.minimum(a + rng.integers(0, 40, a.size), n - 1))
+    elif case == "chain":  # one island whose union order builds long parent chains
+        n = 300001
+        i = np.arange(0, n - 2)[::-1]
+        tris = _tris(i, i + 1, i + 2)
+    elif case == "grids":
+        from tests import fusion_scenes
+        pts, tris, _ = fusion_scenes.layered_grids(3, groups=6, nx=120, ny=90, defects=False)
+        n = len(pts)
+    else:
+        from tests import fusion_scenes
+        pts, tris, _ = fusion_scenes.layered_grids(4, groups=2, nx=30, ny=20)
+        n = len(pts)
+        tris = tris[(tris["a"] < n) & (tris["b"] < n) & (tris["c"] < n)]
+    g = dense.Context(0).surface_topology(tris, n)
+    o = Oracle().surface_topology(tris, n)
+    assert g == o
+    assert g["islands"] >= 1

@@ -46,3 +46,21 @@ def test_oracle_outcome_invariants(seed, stride, rstride):
         assert (samples["source_mask"] > 0).all()
         assert (samples["source_mask"] < (1 << len(sources[r]))).all()
         assert (samples["confidence"] > 0.97).all() and (samples["confidence"] <= 1.0).all()
+
+
+def _tris(rows):
+    from v3d import types
+    t = np.zeros(len(rows), dtype=types.TRIANGLE_DTYPE)
+    for i, (a, b, c) in enumerate(rows):
+        t[i] = (a, b, c, 1.0, 0)
+    return t
+
+
+def test_topology_reference_case_through_the_c_entry_point():
+    # colmap_surface.rs:732-759
+    o = Oracle()
+    top = o.surface_topology(_tris([(0, 1, 2), (1, 3, 2), (4, 5, 6), (5, 7, 6)]), 8)
+    assert top == {"islands": 2, "small_islands": 2, "small_island_triangles": 4,
+                   "largest_island_triangles": 2, "boundary_edges": 8}
+    top = o.surface_topology(_tris([(i, i + 1, i + 2) for i in range(32)]), 34)
+    assert (top["islands"], top["small_islands"], top["largest_island_triangles"]) == (1, 0, 32)

@@ -248,7 +248,14 @@ class VerifiedSample(C.Structure):
     _fields_ = [("point", Point), ("site", GridSite), ("source_mask", C.c_uint32)]
 
 
+class SurfaceTopology(C.Structure):
+    _fields_ = [(name, C.c_uint64) for name in (
+        "islands", "small_islands", "small_island_triangles", "largest_island_triangles",
+        "boundary_edges")]
+
+
 STRUCTS = {
+    "v3d_surface_topology": SurfaceTopology,
     "v3d_depth_view": DepthView, "v3d_verification_funnel": VerificationFunnel,
     "v3d_verified_sample": VerifiedSample,
     "v3d_fusion_stats": FusionStats, "v3d_fusion_pair": FusionPair,

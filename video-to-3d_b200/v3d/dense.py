@@ -111,6 +111,9 @@ def library():
         C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint32,
         C.c_uint32, C.c_double, C.c_void_p, C.c_uint64, C.c_void_p, _P(abi.VerificationFunnel)]
     L.v3d_verify_depth_grids.restype = C.c_int32
+    L.v3d_surface_topology_of.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64,
+                                          _P(abi.SurfaceTopology)]
+    L.v3d_surface_topology_of.restype = C.c_int32
     L.v3d_measure_gather_rate.argtypes = [C.c_void_p, _P(C.c_double)]
     L.v3d_measure_gather_rate.restype = C.c_int32
     L.v3d_last_run_info.argtypes = [C.c_void_p, _P(abi.RunInfo)]
@@ -306,6 +309,15 @@ class Context:
             float(focal), fn, None, C.byref(out)))
         return self._mesh(out)
 
+    def surface_topology(self, triangles, vertex_count):
+        """surface_topology (colmap_surface.rs:125-157) on the device: a dict of
+        islands, small_islands, small_island_triangles, largest_island_triangles
+        and boundary_edges."""
+        st, out = _topology(self.lib.v3d_surface_topology_of, (self.handle,), triangles,
+                            vertex_count)
+        self._check(st)
+        return out
+
     def verify_depth_grids(self, views, reference_views, source_views, stride, reference_stride,
                            focal):
         """verify_patch and verified_union (colmap_surface.rs:175-314) for every
@@ -407,6 +419,13 @@ def _verify(lib_fn, head, views, reference_views, source_views, stride, referenc
     # views into one buffer: no copy per reference
     per_ref = [out[int(offsets[r]):int(offsets[r + 1])] for r in range(n_ref)] if st >= 0 else []
     return st, per_ref, {name: int(getattr(funnel, name)) for name, _ in funnel._fields_}
+
+
+def _topology(lib_fn, head, triangles, vertex_count):
+    tris = np.ascontiguousarray(triangles, dtype=types.TRIANGLE_DTYPE)
+    out = abi.SurfaceTopology()
+    st = lib_fn(*head, tris.ctypes.data, len(tris), int(vertex_count), C.byref(out))
+    return st, {name: int(getattr(out, name)) for name, _ in out._fields_}
 
 
 def has_distributed_landmarks(frames, cameras, sparse_points, focal, control=None):
