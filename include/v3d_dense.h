@@ -397,6 +397,21 @@ typedef struct v3d_clip {
     int32_t max_source_views;
 } v3d_clip;
 
+/* The multi-reference planner's two landmark scans for many clips at once:
+ * reference_candidate_order (dense.rs:620-672: cameras with at least 8
+ * visible landmarks, the most-visible first, the rest farthest-from-it first)
+ * and has_distributed_landmarks (dense.rs:165-213: a majority of cameras see
+ * 2 or more landmarks in 8 of their 4x4 image tiles).  Every (camera,
+ * landmark) projection of every clip runs in one device pass; the orders are
+ * then sorted on the host exactly as the reference sorts them.  clips uses
+ * frames (their sizes), cameras, sparse_xyz and focal of each v3d_clip.
+ * orders needs the sum of the clips' n_cameras entries: clip k's order (camera
+ * indices) starts at the sum of the earlier clips' n_cameras, and
+ * order_counts[k] is its length; distributed[k] is 1 when the clip's
+ * landmarks are distributed. */
+int32_t v3d_plan_clips(v3d_context* ctx, const v3d_clip* clips, uint64_t n_clips,
+                       uint64_t* orders, uint64_t* order_counts, int32_t* distributed);
+
 /* reconstruct_reference_patch (dense.rs:674-747) for the references of many
  * clips of uneven size, as one device batch: every kernel runs once over the
  * references of all clips.  The reference has no multi-clip call; per clip

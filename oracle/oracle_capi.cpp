@@ -334,6 +334,23 @@ int32_t v3do_has_distributed_landmarks(const v3d_frame* frames, uint64_t n_frame
     return has_distributed_landmarks(f, c, s, focal, ctl) ? 1 : 0;
 }
 
+int32_t v3do_reference_candidate_order(const v3d_frame* frames, uint64_t n_frames,
+                                       const v3d_camera* cams, uint64_t n_cams,
+                                       const double* sparse, uint64_t n_sparse, double focal,
+                                       uint64_t* order, uint64_t* n_order) {
+    std::vector<Frame> f(n_frames);
+    for (uint64_t i = 0; i < n_frames; ++i) {
+        f[i].width = frames[i].width;
+        f[i].height = frames[i].height;
+    }
+    auto c = load_cameras(cams, n_cams);
+    auto s = load_sparse(sparse, n_sparse);
+    auto o = reference_candidate_order(f, c, s, focal);
+    for (size_t i = 0; i < o.size(); ++i) order[i] = o[i];
+    *n_order = o.size();
+    return V3D_OK;
+}
+
 uint64_t v3do_grid_stride(uint32_t w, uint32_t h, int32_t fine) { return grid_stride(w, h, fine != 0); }
 
 int32_t v3do_reconstruct_dense_mesh_with_control(

@@ -66,6 +66,8 @@ class Oracle:
         L.v3do_surface_topology_of.argtypes = [C.c_void_p, C.c_uint64, C.c_uint64,
                                                _P(abi.SurfaceTopology)]
         L.v3do_surface_topology_of.restype = C.c_int32
+        L.v3do_reference_candidate_order.argtypes = frames_args + [_P(C.c_uint64), _P(C.c_uint64)]
+        L.v3do_reference_candidate_order.restype = C.c_int32
 
     def fuse_mutually_supported_vertices(self, points, triangles, membership, control=None):
         """surface_fusion.rs:369-549 on the CPU: moves `points` in place."""
@@ -91,6 +93,17 @@ class Oracle:
         st, out = dense._topology(self.lib.v3do_surface_topology_of, (), triangles, vertex_count)
         assert st == 0, st
         return out
+
+    def reference_candidate_order(self, frames, cameras, sparse_points, focal):
+        """dense.rs:620-672 on the CPU: camera indices in planning order."""
+        inp = types.Inputs(frames, cameras, sparse_points)
+        out = (C.c_uint64 * max(len(cameras), 1))()
+        n = C.c_uint64()
+        st = self.lib.v3do_reference_candidate_order(inp.frames, inp.n_frames, inp.cameras,
+                                                     inp.n_cameras, inp.sparse, inp.n_sparse,
+                                                     float(focal), out, C.byref(n))
+        assert st == 0, st
+        return [int(out[i]) for i in range(n.value)]
 
     def selftest(self):
         buf = C.create_string_buffer(1 << 16)

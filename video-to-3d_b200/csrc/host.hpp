@@ -157,6 +157,10 @@ RefPlan plan_reference_patch(const v3d_profile& prof, const Inputs& in, size_t c
                              bool fine_grid, bool& present);
 
 std::vector<size_t> reference_candidate_order(const Inputs& in);
+// dense.rs:627-671 given each camera's visible landmark count (-1 where the
+// camera's frame is missing); shared with the device scan of v3d_plan_clips.
+std::vector<size_t> order_from_visible(const std::vector<HCamera>& cameras,
+                                       const std::vector<int64_t>& visible);
 bool has_distributed_landmarks(const Inputs& in, CancelPoll& cancel);
 
 void skip_result(PassResult& r, int code, const std::string& reason);

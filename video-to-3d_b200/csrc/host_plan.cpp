@@ -292,28 +292,38 @@ RefPlan plan_reference_patch(const v3d_profile& prof, const Inputs& in, size_t c
 
 std::vector<size_t> reference_candidate_order(const Inputs& in) {
     // dense.rs:620-672
-    std::vector<std::pair<size_t, size_t>> cands;
+    std::vector<int64_t> visible(in.cameras.size(), -1);
     for (size_t i = 0; i < in.cameras.size(); ++i) {
         const HCamera& c = in.cameras[i];
         if (c.frame_index >= in.n_frames) continue;
         const v3d_frame& f = in.frames[c.frame_index];
-        size_t visible = 0;
+        int64_t n = 0;
         for (const HVec3& p : in.sparse) {
             HVec3 q;
             if (project_h(c, p, f.width, f.height, in.focal, q) &&
                 in_image_bounds_h(q.x, q.y, f.width, f.height))
-                ++visible;
+                ++n;
         }
-        if (visible >= kMinVisibleSparsePoints) cands.push_back({i, visible});
+        visible[i] = n;
     }
+    return order_from_visible(in.cameras, visible);
+}
+
+std::vector<size_t> order_from_visible(const std::vector<HCamera>& cameras,
+                                       const std::vector<int64_t>& visible) {
+    // dense.rs:627-671, given each camera's visible landmark count
+    std::vector<std::pair<size_t, size_t>> cands;
+    for (size_t i = 0; i < cameras.size(); ++i)
+        if (visible[i] >= static_cast<int64_t>(kMinVisibleSparsePoints))
+            cands.push_back({i, static_cast<size_t>(visible[i])});
     std::stable_sort(cands.begin(), cands.end(), [&](const auto& a, const auto& b) {
         if (a.second != b.second) return a.second > b.second;
-        return in.cameras[a.first].frame_index < in.cameras[b.first].frame_index;
+        return cameras[a.first].frame_index < cameras[b.first].frame_index;
     });
     if (cands.empty()) return {};
-    HVec3 pc = camera_center(in.cameras[cands[0].first]);
+    HVec3 pc = camera_center(cameras[cands[0].first]);
     auto dist2 = [&](size_t i) {
-        HVec3 c = camera_center(in.cameras[i]);
+        HVec3 c = camera_center(cameras[i]);
         double dx = c.x - pc.x, dy = c.y - pc.y, dz = c.z - pc.z;
         return (dx * dx + dy * dy) + dz * dz;
     };
@@ -321,7 +331,7 @@ std::vector<size_t> reference_candidate_order(const Inputs& in) {
         double da = dist2(a.first), db = dist2(b.first);
         if (da != db) return da > db;
         if (a.second != b.second) return a.second > b.second;
-        return in.cameras[a.first].frame_index < in.cameras[b.first].frame_index;
+        return cameras[a.first].frame_index < cameras[b.first].frame_index;
     });
     std::vector<size_t> out;
     for (auto& c : cands) out.push_back(c.first);

@@ -114,6 +114,9 @@ def library():
     L.v3d_surface_topology_of.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64,
                                           _P(abi.SurfaceTopology)]
     L.v3d_surface_topology_of.restype = C.c_int32
+    L.v3d_plan_clips.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64, _P(C.c_uint64),
+                                 _P(C.c_uint64), _P(C.c_int32)]
+    L.v3d_plan_clips.restype = C.c_int32
     L.v3d_measure_gather_rate.argtypes = [C.c_void_p, _P(C.c_double)]
     L.v3d_measure_gather_rate.restype = C.c_int32
     L.v3d_last_run_info.argtypes = [C.c_void_p, _P(abi.RunInfo)]
@@ -308,6 +311,29 @@ class Context:
             self.handle, *mi.args(), cams.cameras, cams.n_cameras, int(width), int(height),
             float(focal), fn, None, C.byref(out)))
         return self._mesh(out)
+
+    def plan_clips(self, clips):
+        """reference_candidate_order (dense.rs:620-672) and has_distributed_landmarks
+        (dense.rs:165-213) of many clips in one device pass.  `clips` is a list of
+        dicts with frames, cameras, sparse_points and focal; returns one (order,
+        distributed) pair per clip."""
+        keep, arr = [], (abi.Clip * max(len(clips), 1))()
+        total = 0
+        for c, clip in enumerate(clips):
+            inp = types.Inputs(clip["frames"], clip["cameras"], clip["sparse_points"])
+            keep.append(inp)
+            arr[c] = abi.Clip(inp.frames, inp.n_frames, inp.cameras, inp.n_cameras, inp.sparse,
+                              inp.n_sparse, float(clip["focal"]), None, 0, 0, 0)
+            total += len(clip["cameras"])
+        orders = (C.c_uint64 * max(total, 1))()
+        counts = (C.c_uint64 * max(len(clips), 1))()
+        flags = (C.c_int32 * max(len(clips), 1))()
+        self._check(self.lib.v3d_plan_clips(self.handle, arr, len(clips), orders, counts, flags))
+        out, base = [], 0
+        for c, clip in enumerate(clips):
+            out.append(([int(orders[base + i]) for i in range(counts[c])], bool(flags[c])))
+            base += len(clip["cameras"])
+        return out
 
     def surface_topology(self, triangles, vertex_count):
         """surface_topology (colmap_surface.rs:125-157) on the device: a dict of
