@@ -61,14 +61,6 @@ __global__ void k_landmark_coverage(const PlanCamera* __restrict__ cams, uint64_
 
 using namespace v3d;
 
-#define V3D_PCK(call)                                                                \
-    do {                                                                             \
-        cudaError_t e_ = (call);                                                     \
-        if (e_ != cudaSuccess) {                                                     \
-            ctx->last_error = std::string(#call) + ": " + cudaGetErrorString(e_);    \
-            return e_ == cudaErrorMemoryAllocation ? V3D_ERR_OUT_OF_MEMORY : V3D_ERR_CUDA; \
-        }                                                                            \
-    } while (0)
 
 extern "C" int32_t v3d_plan_clips(v3d_context* ctx, const v3d_clip* clips, uint64_t n_clips,
                                   uint64_t* orders, uint64_t* order_counts, int32_t* distributed) {
@@ -111,32 +103,25 @@ extern "C" int32_t v3d_plan_clips(v3d_context* ctx, const v3d_clip* clips, uint6
         const size_t o_cams = 0, o_pts = up(sizeof(PlanCamera) * nc),
                      o_vis = up(o_pts + sizeof(D3) * std::max<size_t>(pts.size(), 1)),
                      o_tiles = up(o_vis + sizeof(uint32_t) * nc), need = o_tiles + sizeof(uint32_t) * 16 * nc;
-        if (ctx->arena_bytes < need) {
-            if (ctx->arena) cudaFree(ctx->arena);
-            ctx->arena = nullptr;
-            ctx->arena_bytes = 0;
-            if (cudaMalloc(&ctx->arena, need) != cudaSuccess) {
-                cudaGetLastError();
-                ctx->last_error = "device arena allocation failed";
-                return V3D_ERR_OUT_OF_MEMORY;
-            }
-            ctx->arena_bytes = need;
+        if (!ensure_arena(ctx, need)) {
+            ctx->last_error = "device arena allocation failed";
+            return V3D_ERR_OUT_OF_MEMORY;
         }
         char* base = static_cast<char*>(ctx->arena);
         auto* d_cams = reinterpret_cast<PlanCamera*>(base + o_cams);
         auto* d_pts = reinterpret_cast<D3*>(base + o_pts);
         auto* d_vis = reinterpret_cast<uint32_t*>(base + o_vis);
         auto* d_tiles = reinterpret_cast<uint32_t*>(base + o_tiles);
-        V3D_PCK(cudaMemcpyAsync(d_cams, cams.data(), sizeof(PlanCamera) * nc, cudaMemcpyHostToDevice, st));
+        V3D_CTX_CK(cudaMemcpyAsync(d_cams, cams.data(), sizeof(PlanCamera) * nc, cudaMemcpyHostToDevice, st));
         if (!pts.empty())
-            V3D_PCK(cudaMemcpyAsync(d_pts, pts.data(), sizeof(D3) * pts.size(), cudaMemcpyHostToDevice, st));
+            V3D_CTX_CK(cudaMemcpyAsync(d_pts, pts.data(), sizeof(D3) * pts.size(), cudaMemcpyHostToDevice, st));
         const uint64_t launches0 = g_kernel_launches;
         const unsigned blocks = (unsigned)std::min<uint64_t>(nc, 148ull * 32);
         V3D_COUNTED k_landmark_coverage<<<blocks, 256, 0, st>>>(d_cams, nc, d_pts, d_vis, d_tiles);
-        V3D_PCK(cudaGetLastError());
-        V3D_PCK(cudaMemcpyAsync(visible.data(), d_vis, sizeof(uint32_t) * nc, cudaMemcpyDeviceToHost, st));
-        V3D_PCK(cudaMemcpyAsync(tiles.data(), d_tiles, sizeof(uint32_t) * 16 * nc, cudaMemcpyDeviceToHost, st));
-        V3D_PCK(cudaStreamSynchronize(st));
+        V3D_CTX_CK(cudaGetLastError());
+        V3D_CTX_CK(cudaMemcpyAsync(visible.data(), d_vis, sizeof(uint32_t) * nc, cudaMemcpyDeviceToHost, st));
+        V3D_CTX_CK(cudaMemcpyAsync(tiles.data(), d_tiles, sizeof(uint32_t) * 16 * nc, cudaMemcpyDeviceToHost, st));
+        V3D_CTX_CK(cudaStreamSynchronize(st));
         ctx->last_launches = g_kernel_launches - launches0;
     }
     for (uint64_t k = 0; k < n_clips; ++k) {

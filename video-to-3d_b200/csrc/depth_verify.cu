@@ -217,14 +217,6 @@ struct Carve {
 
 using namespace v3d;
 
-#define V3D_VCK(call)                                                                \
-    do {                                                                             \
-        cudaError_t e_ = (call);                                                     \
-        if (e_ != cudaSuccess) {                                                     \
-            ctx->last_error = std::string(#call) + ": " + cudaGetErrorString(e_);    \
-            return e_ == cudaErrorMemoryAllocation ? V3D_ERR_OUT_OF_MEMORY : V3D_ERR_CUDA; \
-        }                                                                            \
-    } while (0)
 
 extern "C" int32_t v3d_verify_depth_grids(
     v3d_context* ctx, const v3d_depth_view* views, uint64_t n_views, const uint32_t* reference_views,
@@ -270,34 +262,27 @@ extern "C" int32_t v3d_verify_depth_grids(
                  o_perref = cv.take<uint32_t>(n_references), o_funnel = cv.take<unsigned long long>(16),
                  o_count = cv.take<uint32_t>(4),
                  o_scratch = cv.take<uint8_t>(compaction_scratch_bytes(total));
-    if (ctx->arena_bytes < cv.off + 256) {
-        if (ctx->arena) cudaFree(ctx->arena);
-        ctx->arena = nullptr;
-        ctx->arena_bytes = 0;
-        if (cudaMalloc(&ctx->arena, cv.off + 256) != cudaSuccess) {
-            cudaGetLastError();
-            ctx->last_error = "device arena allocation failed";
-            return V3D_ERR_OUT_OF_MEMORY;
-        }
-        ctx->arena_bytes = cv.off + 256;
+    if (!ensure_arena(ctx, cv.off + 256)) {
+        ctx->last_error = "device arena allocation failed";
+        return V3D_ERR_OUT_OF_MEMORY;
     }
     char* base = static_cast<char*>(ctx->arena);
     auto at = [&](size_t o) { return base + o; };
     std::vector<DevView> hv(n_views);
     for (uint64_t v = 0; v < n_views; ++v) {
-        V3D_VCK(cudaMemcpyAsync(at(o_rgba[v]), views[v].rgba, frame_bytes, cudaMemcpyHostToDevice, st));
-        V3D_VCK(cudaMemcpyAsync(at(o_depth[v]), views[v].depth, sizeof(float) * cells,
+        V3D_CTX_CK(cudaMemcpyAsync(at(o_rgba[v]), views[v].rgba, frame_bytes, cudaMemcpyHostToDevice, st));
+        V3D_CTX_CK(cudaMemcpyAsync(at(o_depth[v]), views[v].depth, sizeof(float) * cells,
                                 cudaMemcpyHostToDevice, st));
         hv[v].rgba = reinterpret_cast<const uint8_t*>(at(o_rgba[v]));
         hv[v].depth = reinterpret_cast<const float*>(at(o_depth[v]));
         std::memcpy(hv[v].R, views[v].camera.rotation, sizeof(hv[v].R));
         std::memcpy(hv[v].t, views[v].camera.translation, sizeof(hv[v].t));
     }
-    V3D_VCK(cudaMemcpyAsync(at(o_views), hv.data(), sizeof(DevView) * n_views, cudaMemcpyHostToDevice, st));
+    V3D_CTX_CK(cudaMemcpyAsync(at(o_views), hv.data(), sizeof(DevView) * n_views, cudaMemcpyHostToDevice, st));
     if (n_references) {
-        V3D_VCK(cudaMemcpyAsync(at(o_ref), reference_views, sizeof(uint32_t) * n_references,
+        V3D_CTX_CK(cudaMemcpyAsync(at(o_ref), reference_views, sizeof(uint32_t) * n_references,
                                 cudaMemcpyHostToDevice, st));
-        V3D_VCK(cudaMemcpyAsync(at(o_src), source_views, sizeof(int32_t) * 4 * n_references,
+        V3D_CTX_CK(cudaMemcpyAsync(at(o_src), source_views, sizeof(int32_t) * 4 * n_references,
                                 cudaMemcpyHostToDevice, st));
     }
     auto* d_slot = reinterpret_cast<v3d_verified_sample*>(at(o_slot));
@@ -307,9 +292,9 @@ extern "C" int32_t v3d_verify_depth_grids(
     auto* d_perref = reinterpret_cast<uint32_t*>(at(o_perref));
     auto* d_funnel = reinterpret_cast<unsigned long long*>(at(o_funnel));
     auto* d_count = reinterpret_cast<uint32_t*>(at(o_count));
-    V3D_VCK(cudaMemsetAsync(d_perref, 0, sizeof(uint32_t) * std::max<uint64_t>(n_references, 1), st));
-    V3D_VCK(cudaMemsetAsync(d_funnel, 0, sizeof(unsigned long long) * 16, st));
-    V3D_VCK(cudaMemsetAsync(d_count, 0, sizeof(uint32_t) * 4, st));
+    V3D_CTX_CK(cudaMemsetAsync(d_perref, 0, sizeof(uint32_t) * std::max<uint64_t>(n_references, 1), st));
+    V3D_CTX_CK(cudaMemsetAsync(d_funnel, 0, sizeof(unsigned long long) * 16, st));
+    V3D_CTX_CK(cudaMemsetAsync(d_count, 0, sizeof(uint32_t) * 4, st));
 
     Params p;
     p.views = reinterpret_cast<const DevView*>(at(o_views));
@@ -341,29 +326,29 @@ extern "C" int32_t v3d_verify_depth_grids(
     cudaEventRecord(ev0, st);
     if (total) {
         V3D_COUNTED k_verify<<<grid_of(total), 256, 0, st>>>(p, d_slot, d_kept, d_perref, d_funnel);
-        V3D_VCK(cudaGetLastError());
+        V3D_CTX_CK(cudaGetLastError());
     }
-    V3D_VCK(launch_compact(d_kept, 1, total, d_idx, d_count, at(o_scratch), st));
+    V3D_CTX_CK(launch_compact(d_kept, 1, total, d_idx, d_count, at(o_scratch), st));
     V3D_COUNTED k_gather_samples<<<grid_of(total), 256, 0, st>>>(d_idx, d_count, d_slot, d_out);
-    V3D_VCK(cudaGetLastError());
+    V3D_CTX_CK(cudaGetLastError());
     cudaEventRecord(ev1, st);
     std::vector<uint32_t> per_ref(std::max<uint64_t>(n_references, 1));
     unsigned long long f[16];
     uint32_t n_out = 0;
-    V3D_VCK(cudaMemcpyAsync(per_ref.data(), d_perref, sizeof(uint32_t) * per_ref.size(),
+    V3D_CTX_CK(cudaMemcpyAsync(per_ref.data(), d_perref, sizeof(uint32_t) * per_ref.size(),
                             cudaMemcpyDeviceToHost, st));
-    V3D_VCK(cudaMemcpyAsync(f, d_funnel, sizeof(f), cudaMemcpyDeviceToHost, st));
-    V3D_VCK(cudaMemcpyAsync(&n_out, d_count, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-    V3D_VCK(cudaStreamSynchronize(st));
+    V3D_CTX_CK(cudaMemcpyAsync(f, d_funnel, sizeof(f), cudaMemcpyDeviceToHost, st));
+    V3D_CTX_CK(cudaMemcpyAsync(&n_out, d_count, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    V3D_CTX_CK(cudaStreamSynchronize(st));
     if (n_out > capacity) {
         ctx->last_error = "verified samples exceed the caller's capacity";
         return V3D_ERR_INVALID_ARGUMENT;
     }
     if (n_out) {
         if (!samples) return V3D_ERR_INVALID_ARGUMENT;
-        V3D_VCK(cudaMemcpyAsync(samples, d_out, sizeof(v3d_verified_sample) * n_out,
+        V3D_CTX_CK(cudaMemcpyAsync(samples, d_out, sizeof(v3d_verified_sample) * n_out,
                                 cudaMemcpyDeviceToHost, st));
-        V3D_VCK(cudaStreamSynchronize(st));
+        V3D_CTX_CK(cudaStreamSynchronize(st));
     }
     uint64_t k = 0;
     for (uint64_t r = 0; r < n_references; ++r) {

@@ -156,6 +156,21 @@ void parallel_for(size_t n, const std::function<void(size_t)>& fn);
 RefPlan plan_reference_patch(const v3d_profile& prof, const Inputs& in, size_t camera_index,
                              bool fine_grid, bool& present);
 
+// The context's device arena grown to at least `need` bytes (its contents are
+// not kept); false when the allocation fails.
+bool ensure_arena(v3d_context* ctx, size_t need);
+
+// Returns from an entry point that holds `ctx` when a CUDA call fails, with
+// the failing call and CUDA's text in ctx->last_error.
+#define V3D_CTX_CK(call)                                                             \
+    do {                                                                             \
+        cudaError_t e_ = (call);                                                     \
+        if (e_ != cudaSuccess) {                                                     \
+            ctx->last_error = std::string(#call) + ": " + cudaGetErrorString(e_);    \
+            return e_ == cudaErrorMemoryAllocation ? V3D_ERR_OUT_OF_MEMORY : V3D_ERR_CUDA; \
+        }                                                                            \
+    } while (0)
+
 std::vector<size_t> reference_candidate_order(const Inputs& in);
 // dense.rs:627-671 given each camera's visible landmark count (-1 where the
 // camera's frame is missing); shared with the device scan of v3d_plan_clips.

@@ -117,6 +117,10 @@ struct Seg {
 
 }  // namespace
 
+bool ensure_arena(v3d_context* ctx, size_t need) {
+    return grow(&ctx->arena, &ctx->arena_bytes, need, false);
+}
+
 #define V3D_CK(call)                                              \
     do {                                                          \
         cudaError_t e_ = (call);                                  \

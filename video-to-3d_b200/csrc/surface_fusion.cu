@@ -470,32 +470,11 @@ struct Carve {
     }
 };
 
-bool grow_arena(v3d_context* ctx, size_t need) {
-    if (ctx->arena_bytes >= need) return true;
-    if (ctx->arena) cudaFree(ctx->arena);
-    ctx->arena = nullptr;
-    ctx->arena_bytes = 0;
-    if (cudaMalloc(&ctx->arena, need) != cudaSuccess) {
-        cudaGetLastError();
-        return false;
-    }
-    ctx->arena_bytes = need;
-    return true;
-}
-
 }  // namespace
 }  // namespace v3d
 
 using namespace v3d;
 
-#define V3D_FCK(call)                                                                \
-    do {                                                                             \
-        cudaError_t e_ = (call);                                                     \
-        if (e_ != cudaSuccess) {                                                     \
-            ctx->last_error = std::string(#call) + ": " + cudaGetErrorString(e_);    \
-            return e_ == cudaErrorMemoryAllocation ? V3D_ERR_OUT_OF_MEMORY : V3D_ERR_CUDA; \
-        }                                                                            \
-    } while (0)
 
 extern "C" int32_t v3d_fuse_mutually_supported_vertices(
     v3d_context* ctx, v3d_point* points, uint64_t n, const v3d_mesh_triangle* triangles,
@@ -564,7 +543,7 @@ extern "C" int32_t v3d_fuse_mutually_supported_vertices(
                  o_ctr = cv.take<unsigned long long>(4),
                  o_scratch = cv.take<uint8_t>(compaction_scratch_bytes(std::max(n, nt))),
                  o_cub = cv.take<uint8_t>(t_cub);
-    if (!grow_arena(ctx, cv.off + 256)) {
+    if (!ensure_arena(ctx, cv.off + 256)) {
         ctx->last_error = "device arena allocation failed";
         return V3D_ERR_OUT_OF_MEMORY;
     }
@@ -627,13 +606,13 @@ extern "C" int32_t v3d_fuse_mutually_supported_vertices(
     const uint64_t launches0 = g_kernel_launches;
 
     // ---- upload ----
-    V3D_FCK(cudaMemcpyAsync(d_pts, points, sizeof(v3d_point) * n, cudaMemcpyHostToDevice, st));
-    V3D_FCK(cudaMemcpyAsync(d_tris, triangles, sizeof(v3d_mesh_triangle) * nt,
+    V3D_CTX_CK(cudaMemcpyAsync(d_pts, points, sizeof(v3d_point) * n, cudaMemcpyHostToDevice, st));
+    V3D_CTX_CK(cudaMemcpyAsync(d_tris, triangles, sizeof(v3d_mesh_triangle) * nt,
                             cudaMemcpyHostToDevice, st));
-    V3D_FCK(cudaMemcpyAsync(d_mem, membership, sizeof(int64_t) * n, cudaMemcpyHostToDevice, st));
-    V3D_FCK(cudaMemsetAsync(d_counts, 0, sizeof(uint32_t) * 16, st));
-    V3D_FCK(cudaMemsetAsync(d_ctr, 0, sizeof(unsigned long long) * 4, st));
-    V3D_FCK(cudaMemsetAsync(d_vcnt, 0, sizeof(uint32_t) * (n + 1), st));
+    V3D_CTX_CK(cudaMemcpyAsync(d_mem, membership, sizeof(int64_t) * n, cudaMemcpyHostToDevice, st));
+    V3D_CTX_CK(cudaMemsetAsync(d_counts, 0, sizeof(uint32_t) * 16, st));
+    V3D_CTX_CK(cudaMemsetAsync(d_ctr, 0, sizeof(unsigned long long) * 4, st));
+    V3D_CTX_CK(cudaMemsetAsync(d_vcnt, 0, sizeof(uint32_t) * (n + 1), st));
 
     // the device span from the first kernel to the last (with the host reads
     // between the stages) for the run info's device_ms
@@ -651,35 +630,35 @@ extern "C" int32_t v3d_fuse_mutually_supported_vertices(
 
     // ---- vertex evidence ----
     V3D_COUNTED k_tri_evidence<<<grid_of(nt), 256, 0, st>>>(d_pts, n, d_tris, nt, d_valid, d_len, d_wn);
-    V3D_FCK(cudaGetLastError());
-    V3D_FCK(cub::DeviceScan::ExclusiveSum(d_cub, cub_bytes, d_valid, d_pos, (int)nt, st));
+    V3D_CTX_CK(cudaGetLastError());
+    V3D_CTX_CK(cub::DeviceScan::ExclusiveSum(d_cub, cub_bytes, d_valid, d_pos, (int)nt, st));
     V3D_COUNTED k_incidence<<<grid_of(nt), 256, 0, st>>>(d_tris, nt, d_valid, d_pos, d_len, d_keys,
                                                           d_vals, d_lens, d_vcnt);
-    V3D_FCK(cudaGetLastError());
+    V3D_CTX_CK(cudaGetLastError());
     uint32_t nv_last[2] = {0, 0};
-    V3D_FCK(cudaMemcpyAsync(&nv_last[0], d_pos + (nt - 1), sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-    V3D_FCK(cudaMemcpyAsync(&nv_last[1], d_valid + (nt - 1), sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-    V3D_FCK(cudaStreamSynchronize(st));
+    V3D_CTX_CK(cudaMemcpyAsync(&nv_last[0], d_pos + (nt - 1), sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    V3D_CTX_CK(cudaMemcpyAsync(&nv_last[1], d_valid + (nt - 1), sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    V3D_CTX_CK(cudaStreamSynchronize(st));
     const uint64_t n_valid = (uint64_t)nv_last[0] + nv_last[1];
     const uint64_t n_ent = 3 * n_valid;
     if (canceled()) return V3D_OK;
     if (n_valid == 0) return V3D_OK;  // no edge lengths: no global edge scale
     cub_bytes = t_cub;
-    V3D_FCK(cub::DeviceRadixSort::SortPairs(d_cub, cub_bytes, d_keys, d_keys2, d_vals, d_vals2,
+    V3D_CTX_CK(cub::DeviceRadixSort::SortPairs(d_cub, cub_bytes, d_keys, d_keys2, d_vals, d_vals2,
                                             (int)n_ent, 0, vbits, st));
     cub_bytes = t_cub;
-    V3D_FCK(cub::DeviceScan::ExclusiveSum(d_cub, cub_bytes, d_vcnt, d_voff, (int)(n + 1), st));
+    V3D_CTX_CK(cub::DeviceScan::ExclusiveSum(d_cub, cub_bytes, d_vcnt, d_voff, (int)(n + 1), st));
     V3D_COUNTED k_vertex_evidence<<<grid_of(n), 256, 0, st>>>(n, d_tris, d_voff, d_vals2, d_len, d_wn,
                                                                d_nrm, d_scale, d_has);
-    V3D_FCK(cudaGetLastError());
+    V3D_CTX_CK(cudaGetLastError());
     cub_bytes = t_cub;
-    V3D_FCK(cub::DeviceRadixSort::SortKeys(d_cub, cub_bytes, d_lens, d_lens2, (int)n_ent, 0, 64, st));
+    V3D_CTX_CK(cub::DeviceRadixSort::SortKeys(d_cub, cub_bytes, d_lens, d_lens2, (int)n_ent, 0, 64, st));
     double mid[2] = {0, 0};
     const uint64_t half = n_ent / 2;
-    V3D_FCK(cudaMemcpyAsync(&mid[1], d_lens2 + half, sizeof(double), cudaMemcpyDeviceToHost, st));
+    V3D_CTX_CK(cudaMemcpyAsync(&mid[1], d_lens2 + half, sizeof(double), cudaMemcpyDeviceToHost, st));
     if (n_ent % 2 == 0)
-        V3D_FCK(cudaMemcpyAsync(&mid[0], d_lens2 + half - 1, sizeof(double), cudaMemcpyDeviceToHost, st));
-    V3D_FCK(cudaStreamSynchronize(st));
+        V3D_CTX_CK(cudaMemcpyAsync(&mid[0], d_lens2 + half - 1, sizeof(double), cudaMemcpyDeviceToHost, st));
+    V3D_CTX_CK(cudaStreamSynchronize(st));
     // median (surface_fusion.rs:838-849)
     const double global = n_ent % 2 == 0 ? (mid[0] + mid[1]) * 0.5 : mid[1];
     const double cell_size = std::max(global * kMaxGlobalEdgeFraction, kGeometricEpsilon);
@@ -687,45 +666,45 @@ extern "C" int32_t v3d_fuse_mutually_supported_vertices(
 
     // ---- eligible vertices, sorted by cell ----
     V3D_COUNTED k_eligible<<<grid_of(n), 256, 0, st>>>(d_pts, n, d_mem, d_has, cell_size, d_elig, d_cell);
-    V3D_FCK(cudaGetLastError());
-    V3D_FCK(launch_compact(d_elig, 1, n, d_elv, c_el, d_scratch, st));
+    V3D_CTX_CK(cudaGetLastError());
+    V3D_CTX_CK(launch_compact(d_elig, 1, n, d_elv, c_el, d_scratch, st));
     V3D_COUNTED k_gather_cells<<<grid_of(n), 256, 0, st>>>(d_elv, c_el, d_cell, d_elc);
-    V3D_FCK(cudaGetLastError());
+    V3D_CTX_CK(cudaGetLastError());
     uint32_t n_el = 0;
-    V3D_FCK(cudaMemcpyAsync(&n_el, c_el, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-    V3D_FCK(cudaStreamSynchronize(st));
+    V3D_CTX_CK(cudaMemcpyAsync(&n_el, c_el, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    V3D_CTX_CK(cudaStreamSynchronize(st));
     stats->eligible_vertices = n_el;
     // cells: a hash table of representatives, the eligible vertices sorted by
     // representative (stable, so each cell keeps index order), member records
-    V3D_FCK(cudaMemsetAsync(d_table, 0xFF, sizeof(uint32_t) * table_slots, st));
+    V3D_CTX_CK(cudaMemsetAsync(d_table, 0xFF, sizeof(uint32_t) * table_slots, st));
     V3D_COUNTED k_cell_insert<<<grid_of(n), 256, 0, st>>>(d_elc, c_el, d_table, table_slots - 1, d_rep);
-    V3D_FCK(cudaGetLastError());
+    V3D_CTX_CK(cudaGetLastError());
     if (n_el) {
         cub_bytes = t_cub;
-        V3D_FCK(cub::DeviceRadixSort::SortPairs(d_cub, cub_bytes, d_rep, d_rep2, d_elv, d_elv2,
+        V3D_CTX_CK(cub::DeviceRadixSort::SortPairs(d_cub, cub_bytes, d_rep, d_rep2, d_elv, d_elv2,
                                                 (int)n_el, 0, vbits, st));
     }
     V3D_COUNTED k_members<<<grid_of(n), 256, 0, st>>>(d_rep2, d_elv2, c_el, d_pts, d_mem, d_nrm, d_scale,
                                                        d_members, d_cbeg, d_cend);
-    V3D_FCK(cudaGetLastError());
+    V3D_CTX_CK(cudaGetLastError());
 
     // ---- nearest cross-group neighbours, mutual pairs ----
-    V3D_FCK(cudaMemsetAsync(d_near, 0xFF, sizeof(uint32_t) * n, st));
+    V3D_CTX_CK(cudaMemsetAsync(d_near, 0xFF, sizeof(uint32_t) * n, st));
     V3D_COUNTED k_nearest<<<grid_of(n), 256, 0, st>>>(d_members, d_elc, c_el, d_table, table_slots - 1,
                                                        d_cbeg, d_cend, global, d_near, d_neard, d_ctr);
-    V3D_FCK(cudaGetLastError());
+    V3D_CTX_CK(cudaGetLastError());
     V3D_COUNTED k_mutual<<<grid_of(n), 256, 0, st>>>(d_pts, n, d_near, d_flag, d_fused);
-    V3D_FCK(cudaGetLastError());
-    V3D_FCK(launch_compact(d_flag, 1, n, d_first, c_moves, d_scratch, st));
-    V3D_FCK(cudaMemsetAsync(d_moveof, 0xFF, sizeof(int32_t) * n, st));
+    V3D_CTX_CK(cudaGetLastError());
+    V3D_CTX_CK(launch_compact(d_flag, 1, n, d_first, c_moves, d_scratch, st));
+    V3D_CTX_CK(cudaMemsetAsync(d_moveof, 0xFF, sizeof(int32_t) * n, st));
     V3D_COUNTED k_make_moves<<<grid_of(n / 2 + 1), 256, 0, st>>>(d_first, c_moves, d_near, d_fused,
                                                                   d_moves, d_moveof, d_active);
-    V3D_FCK(cudaGetLastError());
+    V3D_CTX_CK(cudaGetLastError());
     uint32_t n_moves = 0;
     unsigned long long ctr[2] = {0, 0};
-    V3D_FCK(cudaMemcpyAsync(&n_moves, c_moves, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-    V3D_FCK(cudaMemcpyAsync(ctr, d_ctr, sizeof(ctr), cudaMemcpyDeviceToHost, st));
-    V3D_FCK(cudaStreamSynchronize(st));
+    V3D_CTX_CK(cudaMemcpyAsync(&n_moves, c_moves, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    V3D_CTX_CK(cudaMemcpyAsync(ctr, d_ctr, sizeof(ctr), cudaMemcpyDeviceToHost, st));
+    V3D_CTX_CK(cudaStreamSynchronize(st));
     if (canceled()) {
         std::memset(stats, 0, sizeof(*stats));
         return V3D_OK;
@@ -733,48 +712,48 @@ extern "C" int32_t v3d_fuse_mutually_supported_vertices(
 
     // ---- topology gate: rounds until no active move is rejected ----
     for (uint32_t round = 0; n_moves > 0; ++round) {
-        V3D_FCK(cudaMemsetAsync(d_reject, 0, n_moves, st));
-        V3D_FCK(cudaMemsetAsync(c_any, 0, sizeof(uint32_t), st));
+        V3D_CTX_CK(cudaMemsetAsync(d_reject, 0, n_moves, st));
+        V3D_CTX_CK(cudaMemsetAsync(c_any, 0, sizeof(uint32_t), st));
         V3D_COUNTED k_topology_round<<<grid_of(nt), 256, 0, st>>>(d_pts, d_tris, nt, d_valid, d_moves,
                                                                    d_active, d_moveof, d_reject, c_any);
-        V3D_FCK(cudaGetLastError());
+        V3D_CTX_CK(cudaGetLastError());
         uint32_t any = 0;
-        V3D_FCK(cudaMemcpyAsync(&any, c_any, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-        V3D_FCK(cudaStreamSynchronize(st));
+        V3D_CTX_CK(cudaMemcpyAsync(&any, c_any, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        V3D_CTX_CK(cudaStreamSynchronize(st));
         if (canceled()) {
             std::memset(stats, 0, sizeof(*stats));
             return V3D_OK;
         }
         if (!any) break;
         V3D_COUNTED k_apply_rejects<<<grid_of(n_moves), 256, 0, st>>>(d_active, d_reject, c_moves);
-        V3D_FCK(cudaGetLastError());
+        V3D_CTX_CK(cudaGetLastError());
     }
 
     // ---- apply, pairs, moved indices ----
-    V3D_FCK(cudaMemsetAsync(d_moved, 0, n, st));
+    V3D_CTX_CK(cudaMemsetAsync(d_moved, 0, n, st));
     V3D_COUNTED k_apply_moves<<<grid_of(n_moves), 256, 0, st>>>(d_pts, d_moves, d_active, c_moves, d_moved);
-    V3D_FCK(cudaGetLastError());
-    V3D_FCK(launch_compact(d_active, 1, n_moves, d_acc, c_acc, d_scratch, st));
-    V3D_FCK(launch_compact(d_moved, 1, n, d_movedi, c_moved, d_scratch, st));
+    V3D_CTX_CK(cudaGetLastError());
+    V3D_CTX_CK(launch_compact(d_active, 1, n_moves, d_acc, c_acc, d_scratch, st));
+    V3D_CTX_CK(launch_compact(d_moved, 1, n, d_movedi, c_moved, d_scratch, st));
     V3D_COUNTED k_pairs_out<<<grid_of(n_moves), 256, 0, st>>>(d_moves, d_acc, c_acc, d_pts, d_pairs, d_ppts);
-    V3D_FCK(cudaGetLastError());
+    V3D_CTX_CK(cudaGetLastError());
     cudaEventRecord(ev1, st);
     uint32_t cnt[2] = {0, 0};
-    V3D_FCK(cudaMemcpyAsync(cnt, c_acc, sizeof(cnt), cudaMemcpyDeviceToHost, st));
-    V3D_FCK(cudaStreamSynchronize(st));
+    V3D_CTX_CK(cudaMemcpyAsync(cnt, c_acc, sizeof(cnt), cudaMemcpyDeviceToHost, st));
+    V3D_CTX_CK(cudaStreamSynchronize(st));
     const uint32_t n_acc = cnt[0], n_mv = cnt[1];
     std::vector<uint32_t> mv(n_mv);
     std::vector<v3d_point> ppts(2ull * n_acc);
     if (n_acc) {
-        V3D_FCK(cudaMemcpyAsync(pairs, d_pairs, sizeof(v3d_fusion_pair) * n_acc,
+        V3D_CTX_CK(cudaMemcpyAsync(pairs, d_pairs, sizeof(v3d_fusion_pair) * n_acc,
                                 cudaMemcpyDeviceToHost, st));
-        V3D_FCK(cudaMemcpyAsync(ppts.data(), d_ppts, sizeof(v3d_point) * 2 * n_acc,
+        V3D_CTX_CK(cudaMemcpyAsync(ppts.data(), d_ppts, sizeof(v3d_point) * 2 * n_acc,
                                 cudaMemcpyDeviceToHost, st));
     }
     if (n_mv)
-        V3D_FCK(cudaMemcpyAsync(mv.data(), d_movedi, sizeof(uint32_t) * n_mv,
+        V3D_CTX_CK(cudaMemcpyAsync(mv.data(), d_movedi, sizeof(uint32_t) * n_mv,
                                 cudaMemcpyDeviceToHost, st));
-    V3D_FCK(cudaStreamSynchronize(st));
+    V3D_CTX_CK(cudaStreamSynchronize(st));
     for (uint32_t k = 0; k < n_acc; ++k) {
         points[pairs[k].first] = ppts[2ull * k];
         points[pairs[k].second] = ppts[2ull * k + 1];

@@ -152,14 +152,6 @@ unsigned grid_of(uint64_t n) {
 
 using namespace v3d;
 
-#define V3D_TCK(call)                                                                \
-    do {                                                                             \
-        cudaError_t e_ = (call);                                                     \
-        if (e_ != cudaSuccess) {                                                     \
-            ctx->last_error = std::string(#call) + ": " + cudaGetErrorString(e_);    \
-            return e_ == cudaErrorMemoryAllocation ? V3D_ERR_OUT_OF_MEMORY : V3D_ERR_CUDA; \
-        }                                                                            \
-    } while (0)
 
 extern "C" int32_t v3d_surface_topology_of(v3d_context* ctx, const v3d_mesh_triangle* triangles,
                                            uint64_t nt, uint64_t n, v3d_surface_topology* out) {
@@ -189,16 +181,9 @@ extern "C" int32_t v3d_surface_topology_of(v3d_context* ctx, const v3d_mesh_tria
                  o_keys2 = up(o_keys + sizeof(unsigned long long) * nk),
                  o_out = up(o_keys2 + sizeof(unsigned long long) * nk), o_tmp = up(o_out + 64 + 16),
                  need = o_tmp + t_sort + 256;
-    if (ctx->arena_bytes < need) {
-        if (ctx->arena) cudaFree(ctx->arena);
-        ctx->arena = nullptr;
-        ctx->arena_bytes = 0;
-        if (cudaMalloc(&ctx->arena, need) != cudaSuccess) {
-            cudaGetLastError();
-            ctx->last_error = "device arena allocation failed";
-            return V3D_ERR_OUT_OF_MEMORY;
-        }
-        ctx->arena_bytes = need;
+    if (!ensure_arena(ctx, need)) {
+        ctx->last_error = "device arena allocation failed";
+        return V3D_ERR_OUT_OF_MEMORY;
     }
     char* base = static_cast<char*>(ctx->arena);
     auto* d_tris = reinterpret_cast<v3d_mesh_triangle*>(base + o_tris);
@@ -208,10 +193,10 @@ extern "C" int32_t v3d_surface_topology_of(v3d_context* ctx, const v3d_mesh_tria
     auto* d_keys2 = reinterpret_cast<unsigned long long*>(base + o_keys2);
     auto* d_out = reinterpret_cast<unsigned long long*>(base + o_out);
     const uint64_t launches0 = g_kernel_launches;
-    V3D_TCK(cudaMemcpyAsync(d_tris, triangles, sizeof(v3d_mesh_triangle) * nt, cudaMemcpyHostToDevice, st));
-    V3D_TCK(cudaMemsetAsync(d_size, 0, sizeof(unsigned long long) * std::max<uint64_t>(n, 1), st));
+    V3D_CTX_CK(cudaMemcpyAsync(d_tris, triangles, sizeof(v3d_mesh_triangle) * nt, cudaMemcpyHostToDevice, st));
+    V3D_CTX_CK(cudaMemsetAsync(d_size, 0, sizeof(unsigned long long) * std::max<uint64_t>(n, 1), st));
     uint32_t* d_err = reinterpret_cast<uint32_t*>(base + o_out + 64);
-    V3D_TCK(cudaMemsetAsync(d_out, 0, 64 + 16, st));
+    V3D_CTX_CK(cudaMemsetAsync(d_out, 0, 64 + 16, st));
     cudaEvent_t ev0, ev1;
     cudaEventCreate(&ev0);
     cudaEventCreate(&ev1);
@@ -227,17 +212,17 @@ extern "C" int32_t v3d_surface_topology_of(v3d_context* ctx, const v3d_mesh_tria
     V3D_COUNTED k_unite_edges<<<grid_of(nt), 256, 0, st>>>(d_tris, nt, d_parent, d_keys, d_err);
     V3D_COUNTED k_flatten<<<grid_of(n), 256, 0, st>>>(d_parent, n);
     V3D_COUNTED k_island_sizes<<<grid_of(nt), 256, 0, st>>>(d_tris, nt, d_parent, d_size);
-    V3D_TCK(cudaGetLastError());
+    V3D_CTX_CK(cudaGetLastError());
     size_t bytes = t_sort;
-    V3D_TCK(cub::DeviceRadixSort::SortKeys(base + o_tmp, bytes, d_keys, d_keys2, (int)nk, 0, 64, st));
+    V3D_CTX_CK(cub::DeviceRadixSort::SortKeys(base + o_tmp, bytes, d_keys, d_keys2, (int)nk, 0, 64, st));
     V3D_COUNTED k_topology_counts<<<grid_of(std::max(n, nk)), 256, 0, st>>>(d_size, n, d_keys2, nk, d_out);
-    V3D_TCK(cudaGetLastError());
+    V3D_CTX_CK(cudaGetLastError());
     cudaEventRecord(ev1, st);
     unsigned long long h[5];
     uint32_t err = 0;
-    V3D_TCK(cudaMemcpyAsync(h, d_out, sizeof(h), cudaMemcpyDeviceToHost, st));
-    V3D_TCK(cudaMemcpyAsync(&err, d_err, sizeof(err), cudaMemcpyDeviceToHost, st));
-    V3D_TCK(cudaStreamSynchronize(st));
+    V3D_CTX_CK(cudaMemcpyAsync(h, d_out, sizeof(h), cudaMemcpyDeviceToHost, st));
+    V3D_CTX_CK(cudaMemcpyAsync(&err, d_err, sizeof(err), cudaMemcpyDeviceToHost, st));
+    V3D_CTX_CK(cudaStreamSynchronize(st));
     if (err) {
         ctx->last_error = "surface topology: a union did not settle within its retry bound";
         return V3D_ERR_CUDA;
