@@ -94,3 +94,47 @@ def test_surface_topology(case):
     o = Oracle().surface_topology(tris, n)
     assert g == o
     assert g["islands"] >= 1
+
+
+@pytest.mark.gpu
+def test_entry_points_reject_bad_arguments():
+    import ctypes as C
+    from v3d import abi, types
+    ctx = dense.Context(0)
+    lib = ctx.lib
+    # a triangle index at the vertex count
+    t = np.zeros(1, dtype=types.TRIANGLE_DTYPE)
+    t[0] = (0, 1, 3, 1.0, 0)
+    out = abi.SurfaceTopology()
+    assert lib.v3d_surface_topology_of(ctx.handle, t.ctypes.data, 1, 3, C.byref(out)) == abi.ERR_INVALID_ARGUMENT
+    # verified samples beyond the caller's capacity
+    frame, _, first, second, depth, _ = depth_grid_scenes.reference_plane()
+    views = (abi.DepthView * 2)()
+    keep = [np.ascontiguousarray(frame), np.ascontiguousarray(depth)]
+    for i, cam in enumerate([first, second]):
+        views[i] = abi.DepthView(keep[0].ctypes.data, keep[1].ctypes.data, 24, 16,
+                                 abi.Camera(i, (C.c_double * 9)(*np.asarray(cam.rotation).ravel()),
+                                            (C.c_double * 3)(*np.asarray(cam.translation))))
+    refs = np.zeros(1, dtype=np.uint32)
+    src = np.array([1, -1, -1, -1], dtype=np.int32)
+    samples = np.zeros(4, dtype=dense.VERIFIED_DTYPE)
+    offsets = np.zeros(2, dtype=np.uint64)
+    funnel = abi.VerificationFunnel()
+    st = lib.v3d_verify_depth_grids(ctx.handle, views, 2, refs.ctypes.data, 1, src.ctypes.data, 4, 4,
+                                    20.0, samples.ctypes.data, 4, offsets.ctypes.data, C.byref(funnel))
+    assert st == abi.ERR_INVALID_ARGUMENT
+    # a meshed spacing that is not a multiple of the grid spacing, a source past the views
+    for rstride, s0 in [(6, 1), (4, 2)]:
+        src[0] = s0
+        st = lib.v3d_verify_depth_grids(ctx.handle, views, 2, refs.ctypes.data, 1, src.ctypes.data,
+                                        4, rstride, 20.0, samples.ctypes.data, 4,
+                                        offsets.ctypes.data, C.byref(funnel))
+        assert st == abi.ERR_INVALID_ARGUMENT
+    # the context stays usable after the refused calls
+    per_ref, funnel = ctx.verify_depth_grids([(frame, depth, first), (frame, depth, second)], [0],
+                                             [[1]], 4, 4, 20.0)
+    assert len(per_ref[0]) == 20 and funnel["accepted"] == 20
+    # membership of the wrong length
+    pts = np.zeros(3, dtype=types.POINT_DTYPE)
+    with pytest.raises(ValueError):
+        ctx.fuse_mutually_supported_vertices(pts, t, np.zeros(2, dtype=np.int64))
