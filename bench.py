@@ -57,13 +57,14 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true",
                     help="skip the CPU baseline leg (profiling runs)")
     ap.add_argument("--config", choices=["full", "small", "heavy", "batched", "served", "fusion",
-                                         "verify"],
+                                         "verify", "artifact"],
                     default="full",
                     help="full: the headline line (default); small: 360x202 1+4 views; heavy: "
                          "bf16 16 views 256 planes 9x9; batched: 32 uneven clips through the "
                          "server vs one request at a time; served: Poisson arrivals, p50/p99; "
                          "fusion: cross-reference surface fusion of the full clip's patches; "
-                         "verify: geometric depth-grid verification of the full clip")
+                         "verify: geometric depth-grid verification of the full clip; "
+                         "artifact: the full clip's dense evidence as artifact JSON + SHA-256")
     ap.add_argument("--rates", default="50,200,800", help="served: request rates (req/s)")
     ap.add_argument("--duration", type=float, default=3.0, help="served: seconds of arrivals")
     ap.add_argument("--clips", type=int, default=32, help="batched/served: number of clips")
@@ -740,6 +741,94 @@ def run_verify(args):
     ctx.close()
 
 
+def run_artifact(args):
+    """The dense artifact's arrays as serde_json text (DenseStageArtifact::to_json
+    and content_hash, reconstruction_stages.rs:287-380) for the full clip's
+    dense evidence: every keyframe's reference patch from this library,
+    concatenated.  A step is one v3d_encode_dense_evidence call with host
+    buffers: upload, device formatting, the document streamed back and hashed."""
+    import hashlib
+    import torch
+    from v3d import dense, profiles, types
+    clip = load_clip(2, args.frames)
+    frames = clip.frames(args.storage)
+    prof = profiles.zncc(RADIUS, PLANES, SOURCES, STRIDE)
+    ctx = dense.Context(0)
+    res = ctx.reconstruct_reference_patches(frames, clip.cameras, clip.sparse, clip.focal,
+                                            list(range(args.frames)), profile=prof)
+    patches = [r for r in res if r is not None]
+    pts = np.concatenate([r.points for r in patches]).astype(types.POINT_DTYPE)
+    sites = np.concatenate([r.grid_sites for r in patches]).astype(types.SITE_DTYPE)
+    attrs = np.concatenate([r.point_attributes for r in patches]).astype(types.ATTR_DTYPE)
+    prefix = b'{"schema_version":1,"dense":{"stats":{},"points":'
+    suffix = b',"warnings":[]}}'
+    doc_buf = np.zeros(dense.document_bound(len(pts), len(sites), len(attrs), len(prefix),
+                                            len(suffix)), dtype=np.uint8)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    for _ in range(args.warmup):
+        ctx.encode_dense_evidence(pts, sites, attrs, prefix, suffix, out=doc_buf)
+    dev, wall, launches = [], [], 0
+    clocks = Clocks(0)
+    clocks.start()
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        doc, info = ctx.encode_dense_evidence(pts, sites, attrs, prefix, suffix, out=doc_buf)
+        wall.append(time.perf_counter() - t0)
+        run = ctx.last_run_info()
+        dev.append(run["device_ms"] / 1e3)
+        launches += int(run["kernel_launches"])
+    clk = clocks.stop()
+    n = len(pts)
+    dev_s, wall_s = float(np.mean(dev)), float(np.mean(wall))
+    body = info["points_bytes"] + info["grid_sites_bytes"] + info["point_attributes_bytes"]
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    h2d = pts.nbytes + sites.nbytes + attrs.nbytes
+    alg = h2d + body
+    line = {"metric": "dense evidence points serialized/s", "value": n / dev_s,
+            "unit": "points/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": dev_s * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32 (exact shortest f32 decimals)",
+            "data": "synthetic: the seeded clip's dense evidence from this library",
+            "config": {"workload": "DenseEvidence JSON arrays and SHA-256 of the full clip %dx%d, "
+                                   "%d keyframes: %d points, grid sites and attributes, %.1f MB "
+                                   "of text" % (WIDTH, HEIGHT, len(patches), n, body / 1e6),
+                       "l2": "flushed between timed steps (256 MiB write)"},
+            "clocks": clk,
+            "e2e": {"value": n / wall_s, "unit": "points/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": info["document_bytes"], "ms_per_step": wall_s * 1e3},
+            "gpu_launches": launches, "document_bytes": info["document_bytes"],
+            "content_hash": info["content_hash"],
+            "roofline": {"bound": "hbm", "kernel": "k_measure + k_emit (exact shortest f32 "
+                                                   "decimals, text stores)",
+                         "achieved": alg / dev_s / 1e9, "peak": hbm, "unit": "GB/s",
+                         "frac": alg / dev_s / 1e9 / hbm, "traffic": None,
+                         "algorithmic_bytes": alg,
+                         "note": "algorithmic bytes = the evidence arrays read once plus the text "
+                                 "written once; the exact 160-bit digit search makes the "
+                                 "formatting issue-bound, and the end-to-end time is the host "
+                                 "SHA-256 of the streamed document"}}
+    if not args.no_cpu_baseline:
+        from tests.oracle_ffi import Oracle
+        k = 40000
+        t0 = time.perf_counter()
+        odoc, _ = Oracle().encode_dense_evidence(pts[:k], sites[:k], attrs[:k], prefix, suffix)
+        hashlib.sha256(odoc).hexdigest()
+        cpu_s = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": k / cpu_s, "unit": "points/s", "cores": 1, "kind": "port",
+                                "sample": "the first %d points, grid sites and attributes "
+                                          "formatted by the oracle (glibc printf/strtof digit "
+                                          "search) and hashed with hashlib, one thread" % k}
+    print(json.dumps(line), flush=True)
+    ctx.close()
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
@@ -755,6 +844,8 @@ def main():
         run_fusion(args)
     elif args.config == "verify":
         run_verify(args)
+    elif args.config == "artifact":
+        run_artifact(args)
     else:
         run_ours(args, rank, world, local)
 

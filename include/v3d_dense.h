@@ -764,6 +764,73 @@ int32_t v3d_mesh_patch_device_noalloc(
     v3d_mesh_triangle* triangles_dev, uint64_t triangle_capacity,
     v3d_mesh_counts* counts_dev, void* stream);
 
+/* ---- the dense artifact wire format ---------------------------------------
+ * DenseStageArtifact (reconstruction_stages.rs:153-161, 248-256) is stored as
+ * serde_json's compact document of
+ *   {"schema_version":..,"request_hash":..,"cameras_hash":..,"dense":{"stats":{..},
+ *    "points":[..],"grid_sites":[..],"point_attributes":[..],"warnings":[..]}}
+ * and identified by the SHA-256 of those bytes (stage_artifact_document!,
+ * reconstruction_stages.rs:287-420).  The three arrays are nearly all of the
+ * document; they are formatted here on the device.  Point3
+ * (reconstruction/types.rs:68-77) is {"x":f,"y":f,"z":f,"confidence":f,"r":u,
+ * "g":u,"b":u}, DenseGridSite (dense.rs:56-60) {"x":u,"y":u} and
+ * EvidencePointAttributes (reconstruction_evidence.rs:107-115)
+ * {"reciprocal_consistency":f,"depth_margin":f}.  Each f32 is written as the
+ * shortest decimal that reads back to the same f32 (the closest such, ties to
+ * an even last digit) in the notation serde_json uses for f32: plain decimals
+ * for magnitudes from 1e-6 up to below 1e13 ("1.0", "0.000015",
+ * "10000000000.0"), otherwise d.ddde±x without a '+' ("1e-7", "3.4028235e38");
+ * a non-finite f32 is written as null, as serde_json does. */
+
+typedef struct v3d_dense_document {
+    uint64_t document_bytes;         /* prefix + arrays + suffix */
+    uint64_t points_bytes;           /* the text of "[...]" for each array */
+    uint64_t grid_sites_bytes;
+    uint64_t point_attributes_bytes;
+    uint64_t non_finite;             /* floats written as null (check_finite's rejections) */
+    uint8_t sha256[32];              /* ContentHash::of_bytes of the document, raw digest */
+} v3d_dense_document;
+
+/* Upper bound of document_bytes for the given counts and host parts; a
+ * document buffer of this size is always large enough. */
+uint64_t v3d_dense_document_bound(uint64_t n_points, uint64_t n_grid_sites,
+                                  uint64_t n_point_attributes, uint64_t prefix_bytes,
+                                  uint64_t suffix_bytes);
+
+/* DenseStageArtifact::to_json and content_hash (reconstruction_stages.rs:290-
+ * 380) with the arrays formatted on the device:
+ *   document = prefix ‖ points ‖ ,"grid_sites": ‖ sites ‖ ,"point_attributes": ‖ attributes ‖ suffix
+ * where the caller serializes the prefix (everything up to and including
+ * `"points":`) and the suffix (from `,"warnings":` to the end), which are
+ * small.  Any array pointer may be NULL with count 0 ("[]").  The document is
+ * written to `document` (capacity bytes; v3d_dense_document_bound is always
+ * enough; when too small the call returns V3D_ERR_INVALID_ARGUMENT with
+ * out->document_bytes set and nothing written) and hashed with SHA-256 while
+ * it streams back.  out->non_finite counts the nulls; the reference's
+ * to_json_with_cancel refuses such an artifact (NonFinite), to_json writes
+ * null. */
+int32_t v3d_encode_dense_evidence(
+    v3d_context* ctx,
+    const v3d_point* points, uint64_t n_points,
+    const v3d_grid_site* grid_sites, uint64_t n_grid_sites,
+    const v3d_point_attributes* point_attributes, uint64_t n_point_attributes,
+    const char* prefix, uint64_t prefix_bytes, const char* suffix, uint64_t suffix_bytes,
+    char* document, uint64_t capacity, v3d_dense_document* out);
+
+/* The browser transport's packed point buffers (pack_dense_points,
+ * crates/video-to-3d-wasm/src/lib.rs:227-240): values_f32_le gets x, y, z,
+ * confidence of every point as little-endian f32 (16 bytes a point), rgb
+ * three bytes a point.  PackedDenseGridSiteBuffer and
+ * PackedDensePointAttributeBuffer (lib.rs:242-265) are byte for byte the
+ * v3d_grid_site and v3d_point_attributes arrays on a little-endian host and
+ * need no call.  Host only; no device or context. */
+void v3d_pack_dense_points(const v3d_point* points, uint64_t n_points,
+                           uint8_t* values_f32_le, uint8_t* rgb);
+
+/* SHA-256 (FIPS 180-4) of bytes[n] into digest[32], on the host; the hash of
+ * ContentHash::of_bytes (scene_project.rs:463-465). */
+void v3d_sha256(const void* bytes, uint64_t n, uint8_t* digest);
+
 #ifdef __cplusplus
 }
 #endif

@@ -68,6 +68,15 @@ class Oracle:
         L.v3do_surface_topology_of.restype = C.c_int32
         L.v3do_reference_candidate_order.argtypes = frames_args + [_P(C.c_uint64), _P(C.c_uint64)]
         L.v3do_reference_candidate_order.restype = C.c_int32
+        L.v3do_shortest_f32.argtypes = [C.c_float, _P(C.c_uint32), _P(C.c_int32)]
+        L.v3do_shortest_f32.restype = C.c_int32
+        L.v3do_format_f32.argtypes = [C.c_float, C.c_char_p]
+        L.v3do_format_f32.restype = C.c_uint64
+        L.v3do_encode_dense_evidence.argtypes = [
+            C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64, C.c_char_p,
+            C.c_uint64, C.c_char_p, C.c_uint64, C.c_void_p, C.c_uint64, _P(abi.DenseDocument)]
+        L.v3do_encode_dense_evidence.restype = C.c_int32
+        L.v3do_pack_dense_points.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]
 
     def fuse_mutually_supported_vertices(self, points, triangles, membership, control=None):
         """surface_fusion.rs:369-549 on the CPU: moves `points` in place."""
@@ -93,6 +102,40 @@ class Oracle:
         st, out = dense._topology(self.lib.v3do_surface_topology_of, (), triangles, vertex_count)
         assert st == 0, st
         return out
+
+    def format_f32(self, value):
+        """serde_json's text of one f32 (reconstruction_stages.rs:290-294)."""
+        buf = C.create_string_buffer(32)
+        n = self.lib.v3do_format_f32(float(value), buf)
+        return buf.raw[:n].decode()
+
+    def shortest_f32(self, value):
+        """(digits, exponent) of the shortest round-trip decimal, None for 0
+        and non-finite values."""
+        d, k = C.c_uint32(), C.c_int32()
+        if not self.lib.v3do_shortest_f32(float(value), C.byref(d), C.byref(k)):
+            return None
+        return d.value, k.value
+
+    def encode_dense_evidence(self, points, grid_sites, point_attributes, prefix=b"",
+                              suffix=b""):
+        """The DenseEvidence arrays framed like v3d_encode_dense_evidence, on
+        the CPU: (document bytes, info dict; its sha256 is left empty)."""
+        from v3d import dense
+        st, doc, info = dense._encode(self.lib.v3do_encode_dense_evidence, (), points, grid_sites,
+                                      point_attributes, prefix, suffix)
+        assert st == 0, st
+        return doc, info
+
+    def pack_dense_points(self, points):
+        """pack_dense_points (wasm/src/lib.rs:227-240): (values_f32_le, rgb)."""
+        import numpy as np
+        pts = np.ascontiguousarray(points, dtype=types.POINT_DTYPE)
+        values = np.empty(16 * len(pts), dtype=np.uint8)
+        rgb = np.empty(3 * len(pts), dtype=np.uint8)
+        self.lib.v3do_pack_dense_points(pts.ctypes.data, len(pts), values.ctypes.data,
+                                        rgb.ctypes.data)
+        return values.tobytes(), rgb.tobytes()
 
     def reference_candidate_order(self, frames, cameras, sparse_points, focal):
         """dense.rs:620-672 on the CPU: camera indices in planning order."""

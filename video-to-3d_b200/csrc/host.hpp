@@ -42,6 +42,17 @@ struct RefPlan {
     double focal = 0;  // the clip's focal length
 };
 
+// Incremental SHA-256 on the host (sha256.cpp).
+struct Sha256 {
+    uint32_t h[8];
+    uint8_t buf[64];
+    uint64_t length = 0;
+    size_t fill = 0;
+    Sha256();
+    void update(const void* data, size_t n);
+    void finish(uint8_t digest[32]);
+};
+
 // Page-locked host memory shared by the results of one batch
 // (host_block.cpp); the deleter returns it to a process-wide cache.
 using HostBlock = std::shared_ptr<uint8_t>;

@@ -254,7 +254,14 @@ class SurfaceTopology(C.Structure):
         "boundary_edges")]
 
 
+class DenseDocument(C.Structure):
+    _fields_ = [("document_bytes", C.c_uint64), ("points_bytes", C.c_uint64),
+                ("grid_sites_bytes", C.c_uint64), ("point_attributes_bytes", C.c_uint64),
+                ("non_finite", C.c_uint64), ("sha256", C.c_uint8 * 32)]
+
+
 STRUCTS = {
+    "v3d_dense_document": DenseDocument,
     "v3d_surface_topology": SurfaceTopology,
     "v3d_depth_view": DepthView, "v3d_verification_funnel": VerificationFunnel,
     "v3d_verified_sample": VerifiedSample,

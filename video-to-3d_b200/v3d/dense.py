@@ -117,6 +117,17 @@ def library():
     L.v3d_plan_clips.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64, _P(C.c_uint64),
                                  _P(C.c_uint64), _P(C.c_int32)]
     L.v3d_plan_clips.restype = C.c_int32
+    L.v3d_dense_document_bound.argtypes = [C.c_uint64] * 5
+    L.v3d_dense_document_bound.restype = C.c_uint64
+    L.v3d_encode_dense_evidence.argtypes = [
+        C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64,
+        C.c_char_p, C.c_uint64, C.c_char_p, C.c_uint64, C.c_void_p, C.c_uint64,
+        _P(abi.DenseDocument)]
+    L.v3d_encode_dense_evidence.restype = C.c_int32
+    L.v3d_pack_dense_points.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]
+    L.v3d_pack_dense_points.restype = None
+    L.v3d_sha256.argtypes = [C.c_char_p, C.c_uint64, C.c_void_p]
+    L.v3d_sha256.restype = None
     L.v3d_measure_gather_rate.argtypes = [C.c_void_p, _P(C.c_double)]
     L.v3d_measure_gather_rate.restype = C.c_int32
     L.v3d_last_run_info.argtypes = [C.c_void_p, _P(abi.RunInfo)]
@@ -354,6 +365,21 @@ class Context:
         self._check(st)
         return per_ref, funnel
 
+    def encode_dense_evidence(self, points, grid_sites, point_attributes, prefix=b"",
+                              suffix=b"", out=None):
+        """DenseStageArtifact::to_json and content_hash
+        (reconstruction_stages.rs:287-380) with the arrays formatted on the
+        device: returns (document, info) where the document is
+        prefix + the three arrays + suffix and info holds the array lengths,
+        the count of non-finite floats (written as null) and content_hash
+        ("sha256:" + 64 hex digits).  With `out` (a uint8 array of at least
+        document_bound bytes, reused across calls) the document is a
+        memoryview into it; otherwise new bytes."""
+        st, doc, info = _encode(self.lib.v3d_encode_dense_evidence, (self.handle,), points,
+                                grid_sites, point_attributes, prefix, suffix, out)
+        self._check(st)
+        return doc, info
+
     def fuse_mutually_supported_vertices(self, points, triangles, membership, control=None):
         """fuse_mutually_supported_vertices_with_control (surface_fusion.rs:369-549)
         on the device: moves `points` in place and returns a FusionOutcome."""
@@ -445,6 +471,64 @@ def _verify(lib_fn, head, views, reference_views, source_views, stride, referenc
     # views into one buffer: no copy per reference
     per_ref = [out[int(offsets[r]):int(offsets[r + 1])] for r in range(n_ref)] if st >= 0 else []
     return st, per_ref, {name: int(getattr(funnel, name)) for name, _ in funnel._fields_}
+
+
+def document_bound(n_points, n_grid_sites, n_point_attributes, prefix_bytes=0, suffix_bytes=0):
+    """v3d_dense_document_bound: bytes that always hold the document."""
+    return int(library().v3d_dense_document_bound(n_points, n_grid_sites, n_point_attributes,
+                                                  prefix_bytes, suffix_bytes))
+
+
+def _encode(lib_fn, head, points, grid_sites, point_attributes, prefix, suffix, out=None):
+    """Shared by the device entry point and the oracle: points (POINT_DTYPE),
+    grid_sites (SITE_DTYPE) and point_attributes (ATTR_DTYPE), any of them
+    None for an empty array; prefix and suffix bytes; out an optional
+    reusable uint8 buffer."""
+    def arr(a, dt):
+        return np.ascontiguousarray(np.zeros(0, dt) if a is None else a, dtype=dt)
+    pts = arr(points, types.POINT_DTYPE)
+    sites = arr(grid_sites, types.SITE_DTYPE)
+    attrs = arr(point_attributes, types.ATTR_DTYPE)
+    prefix, suffix = bytes(prefix), bytes(suffix)
+    cap = document_bound(len(pts), len(sites), len(attrs), len(prefix), len(suffix))
+    if out is None:
+        buf = np.empty(max(cap, 1), dtype=np.uint8)
+    else:
+        buf = out
+        if not (isinstance(buf, np.ndarray) and buf.dtype == np.uint8 and buf.flags.c_contiguous
+                and buf.flags.writeable and buf.size >= cap):
+            raise ValueError("out must be a writable contiguous uint8 array of %d bytes" % cap)
+    res = abi.DenseDocument()
+    st = lib_fn(*head, pts.ctypes.data, len(pts), sites.ctypes.data, len(sites), attrs.ctypes.data,
+                len(attrs), prefix, len(prefix), suffix, len(suffix), buf.ctypes.data, buf.size,
+                C.byref(res))
+    info = {name: int(getattr(res, name)) for name, _ in res._fields_ if name != "sha256"}
+    digest = bytes(res.sha256)
+    info["content_hash"] = "sha256:" + digest.hex() if any(digest) else None
+    if st != 0:
+        return st, b"", info
+    doc = buf[:res.document_bytes]
+    return st, (doc.tobytes() if out is None else memoryview(doc)), info
+
+
+def pack_dense_points(points):
+    """pack_dense_points (crates/video-to-3d-wasm/src/lib.rs:227-240):
+    (values_f32_le, rgb) byte strings.  Grid sites and point attributes need
+    no packing: SITE_DTYPE and ATTR_DTYPE arrays are already those buffers."""
+    pts = np.ascontiguousarray(points, dtype=types.POINT_DTYPE)
+    values = np.empty(16 * len(pts), dtype=np.uint8)
+    rgb = np.empty(3 * len(pts), dtype=np.uint8)
+    library().v3d_pack_dense_points(pts.ctypes.data, len(pts), values.ctypes.data, rgb.ctypes.data)
+    return values.tobytes(), rgb.tobytes()
+
+
+def content_hash(data):
+    """ContentHash::of_bytes (scene_project.rs:463-465) through the library's
+    host SHA-256."""
+    data = bytes(data)
+    digest = (C.c_uint8 * 32)()
+    library().v3d_sha256(data, len(data), digest)
+    return "sha256:" + bytes(digest).hex()
 
 
 def _topology(lib_fn, head, triangles, vertex_count):
