@@ -57,14 +57,15 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true",
                     help="skip the CPU baseline leg (profiling runs)")
     ap.add_argument("--config", choices=["full", "small", "heavy", "batched", "served", "fusion",
-                                         "verify", "artifact"],
+                                         "verify", "artifact", "colmap"],
                     default="full",
                     help="full: the headline line (default); small: 360x202 1+4 views; heavy: "
                          "bf16 16 views 256 planes 9x9; batched: 32 uneven clips through the "
                          "server vs one request at a time; served: Poisson arrivals, p50/p99; "
                          "fusion: cross-reference surface fusion of the full clip's patches; "
                          "verify: geometric depth-grid verification of the full clip; "
-                         "artifact: the full clip's dense evidence as artifact JSON + SHA-256")
+                         "artifact: the full clip's dense evidence as artifact JSON + SHA-256; "
+                         "colmap: verification, meshing, re-indexing and topology of the full clip")
     ap.add_argument("--rates", default="50,200,800", help="served: request rates (req/s)")
     ap.add_argument("--duration", type=float, default=3.0, help="served: seconds of arrivals")
     ap.add_argument("--clips", type=int, default=32, help="batched/served: number of clips")
@@ -741,6 +742,85 @@ def run_verify(args):
     ctx.close()
 
 
+def run_colmap(args):
+    """The geometric part of the COLMAP export (colmap_surface.rs:380-471) for
+    the full clip: every keyframe's grid (stride 2) verified against its 4
+    nearest views, united, meshed at spacing 4 with the reference-grid gates,
+    re-indexed in first-use order, and the topology of the whole mesh; one
+    v3d_mesh_verified_depth_grids call per step."""
+    import torch
+    from v3d import dense
+    clip = load_clip(2, args.frames)
+    stride, rstride = 2, 4
+    views, refs, sources = verify_views(clip, stride)
+    ctx = dense.Context(0)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    for _ in range(args.warmup):
+        ctx.mesh_verified_depth_grids(views, refs, sources, stride, rstride, clip.focal)
+    dev, wall, launches = [], [], 0
+    clocks = Clocks(0)
+    clocks.start()
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        surf = ctx.mesh_verified_depth_grids(views, refs, sources, stride, rstride, clip.focal)
+        wall.append(time.perf_counter() - t0)
+        info = ctx.last_run_info()
+        dev.append(info["device_ms"] / 1e3)
+        launches += int(info["kernel_launches"])
+    clk = clocks.stop()
+    d = surf.diagnostics
+    checks = d["verification"]["reference_samples"]
+    dev_s, wall_s = float(np.mean(dev)), float(np.mean(wall))
+    n = len(views)
+    frame_bytes = WIDTH * HEIGHT * 4
+    grid_bytes = views[0][1].nbytes
+    out_bytes = len(surf.points) * 28 + len(surf.triangles) * 32
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    alg = n * (frame_bytes + grid_bytes) + out_bytes
+    line = {"metric": "depth-grid samples verified and meshed per source/s", "value": checks / dev_s,
+            "unit": "sample-source checks/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dev_s * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: the seeded clip's true depth with noise and holes",
+            "config": {"workload": "COLMAP export geometry of the full clip %dx%d: %d keyframes, "
+                                   "grid stride %d verified against the 4 nearest, meshed at %d, "
+                                   "re-indexed, topology" % (WIDTH, HEIGHT, n, stride, rstride),
+                       "l2": "flushed between timed steps (256 MiB write)"},
+            "clocks": clk,
+            "e2e": {"value": checks / wall_s, "unit": "sample-source checks/s",
+                    "h2d_bytes_per_step": n * (frame_bytes + grid_bytes),
+                    "d2h_bytes_per_step": out_bytes, "ms_per_step": wall_s * 1e3},
+            "gpu_launches": launches, "diagnostics": d, "points": len(surf.points),
+            "triangles": len(surf.triangles), "regions": len(surf.regions),
+            "roofline": {"bound": "hbm", "kernel": "k_verify (one thread per reference sample), "
+                                                   "then the batched grid mesh",
+                         "achieved": alg / dev_s / 1e9, "peak": hbm, "unit": "GB/s",
+                         "frac": alg / dev_s / 1e9 / hbm, "traffic": None,
+                         "algorithmic_bytes": alg,
+                         "note": "algorithmic bytes = every frame and depth grid read once plus "
+                                 "the exported points and triangles written; verification and "
+                                 "meshing are latency-bound gathers"}}
+    if not args.no_cpu_baseline:
+        from tests.oracle_ffi import Oracle
+        k = 6
+        t0 = time.perf_counter()
+        o = Oracle().mesh_verified_depth_grids(views, refs[:k], sources[:k], stride, rstride,
+                                               clip.focal)
+        cpu_s = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": o.diagnostics["verification"]["reference_samples"] / cpu_s,
+                                "unit": "sample-source checks/s", "cores": 1, "kind": "port",
+                                "sample": "the first %d references, one thread" % k}
+    print(json.dumps(line), flush=True)
+    ctx.close()
+
+
 def run_artifact(args):
     """The dense artifact's arrays as serde_json text (DenseStageArtifact::to_json
     and content_hash, reconstruction_stages.rs:287-380) for the full clip's
@@ -846,6 +926,8 @@ def main():
         run_verify(args)
     elif args.config == "artifact":
         run_artifact(args)
+    elif args.config == "colmap":
+        run_colmap(args)
     else:
         run_ours(args, rank, world, local)
 

@@ -566,6 +566,66 @@ int32_t v3d_surface_topology_of(v3d_context* ctx, const v3d_mesh_triangle* trian
                                 uint64_t n_triangles, uint64_t vertex_count,
                                 v3d_surface_topology* out);
 
+/* MeshingFunnel (colmap_surface.rs:98-109). */
+typedef struct v3d_meshing_funnel {
+    uint64_t depth_views;
+    uint64_t meshed_reference_views;
+    uint64_t candidate_cells;
+    uint64_t rejected_discontinuities;
+    uint64_t rejected_degenerate;
+    uint64_t multiply_verified_samples;
+    uint64_t exported_triangles;
+} v3d_meshing_funnel;
+
+/* One exported SurfaceEvidenceRegion (colmap_surface.rs:448-455): the points
+ * a meshed reference view added, [first_point, first_point + point_count),
+ * and the source frames that verified them (frame_index of the source views,
+ * ascending). */
+typedef struct v3d_verified_surface_region {
+    uint64_t reference_frame;
+    uint64_t first_point;
+    uint64_t point_count;
+    uint64_t source_frames[4];
+    uint32_t n_source_frames;
+    uint32_t reserved;
+} v3d_verified_surface_region;
+
+/* SurfaceDiagnostics (colmap_surface.rs:44-53) and the export's counts. */
+typedef struct v3d_verified_surface {
+    v3d_verification_funnel verification;
+    v3d_meshing_funnel meshing;
+    v3d_surface_topology topology;
+    int32_t dominant_rejection;  /* 1..7: the funnel field after reference_samples, in order; 0 none */
+    int32_t reserved;
+    uint64_t n_points, n_triangles, n_regions;
+} v3d_verified_surface;
+
+/* Capacities that always hold the outputs of v3d_mesh_verified_depth_grids. */
+void v3d_verified_surface_bounds(uint32_t width, uint32_t height, uint32_t reference_stride,
+                                 uint64_t n_references, uint64_t* max_points,
+                                 uint64_t* max_triangles);
+
+/* The geometric part of the COLMAP export (colmap_surface.rs:380-471, up to
+ * the material bake and GLB encoding): for each reference in order, every
+ * source is verified and the results united (as v3d_verify_depth_grids), the
+ * union is meshed with the reference-grid gates at reference_stride (mesh.rs:
+ * 74-220 over one patch, grid border 0, the reference view's camera), and the
+ * vertices the triangles use are appended in the order the triangles first
+ * use them; references that add no triangle are left out.  Then the
+ * topology of the whole mesh and the dominant rejection.  All of it runs on
+ * the device; the host reads counts between the three stages.  Views must
+ * have distinct camera frame indices.  points and sites receive n_points
+ * entries, triangles n_triangles (indices into points), regions n_regions
+ * (at most n_references).  Returns V3D_SKIPPED with the reference's message
+ * in v3d_last_error when no triangle is exported. */
+int32_t v3d_mesh_verified_depth_grids(
+    v3d_context* ctx, const v3d_depth_view* views, uint64_t n_views,
+    const uint32_t* reference_views, uint64_t n_references, const int32_t* source_views,
+    uint32_t stride, uint32_t reference_stride, double focal,
+    v3d_point* points, v3d_grid_site* sites, uint64_t point_capacity,
+    v3d_mesh_triangle* triangles, uint64_t triangle_capacity,
+    v3d_verified_surface_region* regions, v3d_verified_surface* out);
+
 /* ---- cross-reference surface fusion (surface_fusion.rs:356-852) ---------
  * The first step of surface consolidation after the grid mesh
  * (consolidate_surface_recording_with_control, surface_fusion.rs:128-231,

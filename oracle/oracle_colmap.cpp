@@ -288,3 +288,141 @@ extern "C" int32_t v3do_surface_topology_of(const v3d_mesh_triangle* triangles, 
     out->boundary_edges = top.boundary_edges;
     return V3D_OK;
 }
+
+// The geometric part of the COLMAP export (colmap_surface.rs:380-471): per
+// reference, verify every source and unite, mesh the union at the reference
+// spacing with the reference-grid gates (mesh.rs:74-220 with no patches, which
+// is mesh_legacy.rs:150-358 over all points), append the vertices in the order
+// the triangles first use them, record the region; then topology and the
+// dominant rejection.  Material baking and the GLB encoding are not part of it.
+extern "C" int32_t v3do_mesh_verified_depth_grids(
+    const v3d_depth_view* views, uint64_t n_views, const uint32_t* reference_views,
+    uint64_t n_references, const int32_t* source_views, uint32_t stride, uint32_t reference_stride,
+    double focal, v3d_point* points, v3d_grid_site* sites, uint64_t point_capacity,
+    v3d_mesh_triangle* triangles, uint64_t triangle_capacity, v3d_verified_surface_region* regions,
+    v3d_verified_surface* out) {
+    if (!views || !n_views || !out || (n_references && (!reference_views || !source_views)) ||
+        stride == 0 || reference_stride == 0 || reference_stride % stride != 0)
+        return V3D_ERR_INVALID_ARGUMENT;
+    std::memset(out, 0, sizeof(*out));
+    std::vector<DepthView> dv(n_views);
+    std::vector<Camera> cameras(n_views);
+    for (uint64_t i = 0; i < n_views; ++i) {
+        if (views[i].width != views[0].width || views[i].height != views[0].height)
+            return V3D_ERR_INVALID_ARGUMENT;
+        for (uint64_t k = 0; k < i; ++k)
+            if (views[k].camera.frame_index == views[i].camera.frame_index) return V3D_ERR_INVALID_ARGUMENT;
+        dv[i].width = views[i].width;
+        dv[i].height = views[i].height;
+        dv[i].rgba = views[i].rgba;
+        dv[i].depth = views[i].depth;
+        dv[i].camera.frame_index = views[i].camera.frame_index;
+        std::memcpy(dv[i].camera.R, views[i].camera.rotation, sizeof(dv[i].camera.R));
+        std::memcpy(dv[i].camera.t, views[i].camera.translation, sizeof(dv[i].camera.t));
+        cameras[i] = dv[i].camera;
+    }
+    for (uint64_t r = 0; r < n_references; ++r) {
+        if (reference_views[r] >= n_views) return V3D_ERR_INVALID_ARGUMENT;
+        for (int j = 0; j < 4; ++j)
+            if (source_views[4 * r + j] >= (int64_t)n_views) return V3D_ERR_INVALID_ARGUMENT;
+    }
+    Funnel total;
+    v3d_meshing_funnel m{};
+    m.depth_views = n_views;
+    std::vector<Point3> P;
+    std::vector<GridSite> G;
+    std::vector<MeshTriangle> T;
+    std::vector<v3d_verified_surface_region> R;
+    for (uint64_t r = 0; r < n_references; ++r) {
+        const DepthView& ref = dv[reference_views[r]];
+        std::vector<std::pair<size_t, std::vector<std::pair<Point3, GridSite>>>> cand;
+        for (int j = 0; j < 4; ++j) {
+            const int32_t s = source_views[4 * r + j];
+            if (s < 0) continue;
+            Funnel f;
+            auto patch = verify_patch(ref, dv[s], stride, reference_stride, focal, f);
+            total.add(f);
+            cand.emplace_back((size_t)j, std::move(patch));
+        }
+        const std::vector<VerifiedSample> uni = verified_union(cand);
+        for (const VerifiedSample& v : uni) m.multiply_verified_samples += v.sources.size() > 1;
+        const size_t previous = T.size();
+        if (!uni.empty()) {
+            std::vector<Point3> p;
+            std::vector<GridSite> g;
+            for (const VerifiedSample& v : uni) {
+                p.push_back(v.point);
+                g.push_back(v.site);
+            }
+            MeshDenseInput d;
+            d.attempted = true;
+            d.reference_frame = ref.camera.frame_index;
+            d.grid_stride = reference_stride;
+            Control ctl;
+            MeshAnalysis mesh = reconstruct_dense_mesh_with_control(p, g, d, cameras, ref.width, ref.height,
+                                                                    focal, ctl);
+            m.candidate_cells += mesh.stats.candidate_cells;
+            m.rejected_discontinuities += mesh.stats.rejected_discontinuities;
+            m.rejected_degenerate += mesh.stats.rejected_degenerate;
+            const size_t start = P.size();
+            std::vector<int64_t> index(p.size(), -1);
+            std::vector<uint64_t> frames;
+            for (MeshTriangle face : mesh.triangles) {
+                for (size_t* corner : {&face.a, &face.b, &face.c}) {
+                    const size_t i = *corner;
+                    if (index[i] < 0) {
+                        index[i] = (int64_t)P.size();
+                        P.push_back(p[i]);
+                        G.push_back(g[i]);
+                        for (size_t j : uni[i].sources) {
+                            const uint64_t f = dv[source_views[4 * r + j]].camera.frame_index;
+                            if (std::find(frames.begin(), frames.end(), f) == frames.end()) frames.push_back(f);
+                        }
+                    }
+                    *corner = (size_t)index[i];
+                }
+                T.push_back(face);
+            }
+            if (P.size() > start) {
+                std::sort(frames.begin(), frames.end());
+                v3d_verified_surface_region reg{};
+                reg.reference_frame = ref.camera.frame_index;
+                reg.first_point = start;
+                reg.point_count = P.size() - start;
+                reg.n_source_frames = (uint32_t)frames.size();
+                for (size_t k = 0; k < frames.size(); ++k) reg.source_frames[k] = frames[k];
+                R.push_back(reg);
+            }
+        }
+        if (T.size() == previous) continue;
+        ++m.meshed_reference_views;
+    }
+    out->verification = v3d_verification_funnel{
+        total.reference_samples, total.missing_reference_depth, total.insufficient_parallax,
+        total.behind_source,     total.outside_source,          total.missing_source_depth,
+        total.depth_disagreement, total.color_disagreement,     total.accepted};
+    m.exported_triangles = T.size();
+    out->meshing = m;
+    out->n_points = P.size();
+    out->n_triangles = T.size();
+    out->n_regions = R.size();
+    if (T.empty()) return V3D_SKIPPED;  // "COLMAP stereo produced no cross-view verified surface triangles"
+    const Topology top = surface_topology(P.size(), T);
+    out->topology = v3d_surface_topology{top.islands, top.small_islands, top.small_island_triangles,
+                                         top.largest_island_triangles, top.boundary_edges};
+    static const char* const names[] = {"missing_reference_depth", "insufficient_parallax", "behind_source",
+                                        "outside_source",          "missing_source_depth",  "depth_disagreement",
+                                        "color_disagreement"};
+    const char* dom = dominant_rejection(total);
+    for (int k = 0; k < 7; ++k)
+        if (dom && std::strcmp(dom, names[k]) == 0) out->dominant_rejection = k + 1;
+    if (P.size() > point_capacity || T.size() > triangle_capacity || !points || !sites || !triangles || !regions)
+        return V3D_ERR_INVALID_ARGUMENT;
+    for (size_t i = 0; i < P.size(); ++i) {
+        points[i] = v3d_point{P[i].x, P[i].y, P[i].z, P[i].confidence, P[i].r, P[i].g, P[i].b, 0};
+        sites[i] = v3d_grid_site{G[i].x, G[i].y};
+    }
+    for (size_t t = 0; t < T.size(); ++t) triangles[t] = v3d_mesh_triangle{T[t].a, T[t].b, T[t].c, T[t].confidence, 0};
+    std::copy(R.begin(), R.end(), regions);
+    return V3D_OK;
+}

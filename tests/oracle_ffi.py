@@ -68,6 +68,11 @@ class Oracle:
         L.v3do_surface_topology_of.restype = C.c_int32
         L.v3do_reference_candidate_order.argtypes = frames_args + [_P(C.c_uint64), _P(C.c_uint64)]
         L.v3do_reference_candidate_order.restype = C.c_int32
+        L.v3do_mesh_verified_depth_grids.argtypes = [
+            C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint32, C.c_uint32,
+            C.c_double, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64, C.c_void_p,
+            _P(abi.VerifiedSurface)]
+        L.v3do_mesh_verified_depth_grids.restype = C.c_int32
         L.v3do_shortest_f32.argtypes = [C.c_float, _P(C.c_uint32), _P(C.c_int32)]
         L.v3do_shortest_f32.restype = C.c_int32
         L.v3do_format_f32.argtypes = [C.c_float, C.c_char_p]
@@ -102,6 +107,15 @@ class Oracle:
         st, out = dense._topology(self.lib.v3do_surface_topology_of, (), triangles, vertex_count)
         assert st == 0, st
         return out
+
+    def mesh_verified_depth_grids(self, views, reference_views, source_views, stride,
+                                  reference_stride, focal):
+        """colmap_surface.rs:380-471 on the CPU: a VerifiedSurface."""
+        from v3d import dense
+        st, surf = dense._surface(self.lib.v3do_mesh_verified_depth_grids, (), views,
+                                  reference_views, source_views, stride, reference_stride, focal)
+        assert st in (0, 1), st
+        return surf
 
     def format_f32(self, value):
         """serde_json's text of one f32 (reconstruction_stages.rs:290-294)."""

@@ -138,3 +138,65 @@ def test_entry_points_reject_bad_arguments():
     pts = np.zeros(3, dtype=types.POINT_DTYPE)
     with pytest.raises(ValueError):
         ctx.fuse_mutually_supported_vertices(pts, t, np.zeros(2, dtype=np.int64))
+
+
+def _compare_surface(views, refs, sources, stride, rstride, focal):
+    g = dense.Context(0).mesh_verified_depth_grids(views, refs, sources, stride, rstride, focal)
+    o = Oracle().mesh_verified_depth_grids(views, refs, sources, stride, rstride, focal)
+    assert g.status == o.status
+    assert g.diagnostics == o.diagnostics
+    assert g.regions == o.regions
+    assert g.points.tobytes() == o.points.tobytes()
+    assert g.sites.tobytes() == o.sites.tobytes()
+    assert g.triangles.tobytes() == o.triangles.tobytes()
+    return g
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("seed,stride,rstride", [(1, 2, 2), (2, 2, 4), (3, 4, 8), (4, 3, 6)])
+def test_verified_surface_seeded_clips(seed, stride, rstride):
+    views, refs, sources, focal = depth_grid_scenes.clip_views(seed, stride=stride)
+    g = _compare_surface(views, refs, sources, stride, rstride, focal)
+    assert g.status == 0 and len(g.triangles) > 100 and len(g.regions) > 1
+
+
+@pytest.mark.gpu
+def test_verified_surface_full_size_and_edge_cases():
+    views, refs, sources, focal = depth_grid_scenes.clip_views(5, width=640, height=360,
+                                                               frames=12, stride=2)
+    g = _compare_surface(views, refs, sources, 2, 4, focal)
+    assert g.diagnostics["meshing"]["exported_triangles"] > 50000
+    # no references, a reference without sources, references in another order
+    assert _compare_surface(views, [], [], 2, 4, focal).status == 1
+    _compare_surface(views, [0, 3], [[], [2]], 2, 4, focal)
+    _compare_surface(views, [5, 1, 7], [sources[5], sources[1], sources[7]], 2, 4, focal)
+    # the reference plane: all-rejecting sources give no triangle
+    frame, _, first, second, depth, wrong = depth_grid_scenes.reference_plane()
+    assert _compare_surface([(frame, depth, first), (frame, wrong, second)], [0], [[1]], 4, 4,
+                            20.0).status == 1
+    _compare_surface([(frame, depth, first), (frame, depth, second)], [0, 1], [[1], [0]], 4, 4,
+                     20.0)
+
+
+@pytest.mark.gpu
+def test_verified_surface_sparse_references():
+    # references left with fewer than three samples, or none, between meshed ones
+    views, refs, sources, focal = depth_grid_scenes.clip_views(6, stride=2, holes=0.995)
+    dense_views, _, _, _ = depth_grid_scenes.clip_views(6, stride=2)
+    mixed = [dense_views[i] if i % 3 else views[i] for i in range(len(views))]
+    g = _compare_surface(mixed, refs, sources, 2, 4, focal)
+    assert g.status == 0
+
+
+@pytest.mark.gpu
+def test_verified_surface_rejects_duplicate_frames():
+    import ctypes as C
+    from v3d import abi
+    views, refs, sources, focal = depth_grid_scenes.clip_views(1, stride=2)
+    dup = list(views)
+    dup[1] = (views[1][0], views[1][1], views[0][2])
+    ctx = dense.Context(0)
+    st, _ = dense._surface(ctx.lib.v3d_mesh_verified_depth_grids, (ctx.handle,), dup, refs,
+                           sources, 2, 4, focal)
+    assert st == abi.ERR_INVALID_ARGUMENT
+    assert _compare_surface(views, refs, sources, 2, 4, focal).status == 0

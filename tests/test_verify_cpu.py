@@ -4,6 +4,8 @@ seeded clips."""
 import numpy as np
 import pytest
 
+from v3d import types
+
 from tests import depth_grid_scenes
 from tests.oracle_ffi import Oracle
 
@@ -64,3 +66,80 @@ def test_topology_reference_case_through_the_c_entry_point():
                    "largest_island_triangles": 2, "boundary_edges": 8}
     top = o.surface_topology(_tris([(i, i + 1, i + 2) for i in range(32)]), 34)
     assert (top["islands"], top["small_islands"], top["largest_island_triangles"]) == (1, 0, 32)
+
+
+def _recompose(views, refs, sources, stride, rstride, focal):
+    """colmap_surface.rs:380-471 in Python over the oracle's verification
+    and mesh calls: per reference the united samples are meshed as one patch
+    and the vertices appended in the order the triangles first use them."""
+    o = Oracle()
+    per_ref, funnel = o.verify_depth_grids(views, refs, sources, stride, rstride, focal)
+    cams = [cam for _, _, cam in views]
+    h, w = views[0][0].shape[:2]
+    pts, sites, tris, regions = [], [], [], []
+    meshing = {"candidate_cells": 0, "rejected_discontinuities": 0, "rejected_degenerate": 0,
+               "multiply_verified_samples": 0}
+    for r, samples in enumerate(per_ref):
+        meshing["multiply_verified_samples"] += int(
+            sum(bin(int(m)).count("1") > 1 for m in samples["source_mask"]))
+        if len(samples) == 0:
+            continue
+        p = np.zeros(len(samples), dtype=types.POINT_DTYPE)
+        for f in ("x", "y", "z", "confidence", "r", "g", "b"):
+            p[f] = samples[f]
+        g = np.zeros(len(samples), dtype=types.SITE_DTYPE)
+        g["x"], g["y"] = samples["site_x"], samples["site_y"]
+        frame = int(views[refs[r]][2].frame_index)
+        mesh = o.reconstruct_dense_mesh_with_control(
+            p, g, {"attempted": True, "reference_frame": frame, "grid_stride": rstride}, cams, w,
+            h, focal)
+        for k in ("candidate_cells", "rejected_discontinuities", "rejected_degenerate"):
+            meshing[k] += int(mesh.stats[k])
+        start, index, frames = len(pts), {}, set()
+        for t in mesh.triangles:
+            corners = []
+            for i in (int(t["a"]), int(t["b"]), int(t["c"])):
+                if i not in index:
+                    index[i] = len(pts)
+                    pts.append(p[i])
+                    sites.append(g[i])
+                    m = int(samples["source_mask"][i])
+                    frames |= {int(views[sources[r][j]][2].frame_index) for j in range(4) if m >> j & 1}
+                corners.append(index[i])
+            tris.append((*corners, float(t["confidence"])))
+        if len(pts) > start:
+            regions.append({"reference_frame": frame, "first_point": start,
+                            "point_count": len(pts) - start, "source_frames": sorted(frames)})
+    return pts, sites, tris, regions, funnel, meshing
+
+
+@pytest.mark.parametrize("seed,stride,rstride", [(1, 2, 2), (2, 2, 4), (4, 3, 6)])
+def test_oracle_verified_surface_equals_its_recomposition(seed, stride, rstride):
+    views, refs, sources, focal = depth_grid_scenes.clip_views(seed, stride=stride)
+    surf = Oracle().mesh_verified_depth_grids(views, refs, sources, stride, rstride, focal)
+    pts, sites, tris, regions, funnel, meshing = _recompose(views, refs, sources, stride, rstride,
+                                                           focal)
+    assert surf.status == 0 and len(tris) > 0
+    assert surf.diagnostics["verification"] == funnel
+    for k, v in meshing.items():
+        assert surf.diagnostics["meshing"][k] == v, k
+    assert surf.diagnostics["meshing"]["exported_triangles"] == len(tris)
+    assert surf.diagnostics["meshing"]["meshed_reference_views"] == len(regions)
+    assert surf.regions == regions
+    assert np.array(pts, dtype=surf.points.dtype).tobytes() == surf.points.tobytes()
+    assert np.array(sites, dtype=surf.sites.dtype).tobytes() == surf.sites.tobytes()
+    t = surf.triangles
+    assert [(int(a), int(b), int(c), float(f)) for a, b, c, f in
+            zip(t["a"], t["b"], t["c"], t["confidence"])] == tris
+    assert surf.diagnostics["topology"] == Oracle().surface_topology(surf.triangles, len(pts))
+    top = surf.diagnostics["topology"]
+    assert top["islands"] >= len(regions)
+    assert surf.diagnostics["dominant_rejection"] is not None
+
+
+def test_oracle_verified_surface_without_triangles_is_skipped():
+    frame, _, first, second, depth, wrong = depth_grid_scenes.reference_plane()
+    views = [(frame, depth, first), (frame, wrong, second)]
+    surf = Oracle().mesh_verified_depth_grids(views, [0], [[1]], 4, 4, 20.0)
+    assert surf.status == 1 and len(surf.points) == 0
+    assert surf.diagnostics["verification"]["depth_disagreement"] > 0

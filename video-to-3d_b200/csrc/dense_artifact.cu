@@ -661,7 +661,8 @@ extern "C" int32_t v3d_encode_dense_evidence(
         }
         cv_ready.notify_one();
     };
-    std::thread hasher([&] {
+    std::thread hasher;
+    auto hash_document = [&] {
         Sha256 h;
         uint64_t done = 0;
         while (done < total) {
@@ -676,7 +677,13 @@ extern "C" int32_t v3d_encode_dense_evidence(
             done = r;
         }
         h.finish(out->sha256);
-    });
+    };
+    try {
+        hasher = std::thread(hash_document);
+    } catch (const std::exception&) {
+        ctx->last_error = "could not start the hashing thread";
+        return V3D_ERR_INTERNAL;
+    }
     if (prefix_bytes) std::memcpy(document, prefix, prefix_bytes);
     publish(prefix_bytes, false);
     constexpr uint64_t kChunk = 8ull << 20;

@@ -42,6 +42,13 @@ struct RefPlan {
     double focal = 0;  // the clip's focal length
 };
 
+// surface_topology (colmap_surface.rs:125-157) of host triangles whose indices
+// are already checked, with ctx->mu held and the device current
+// (surface_topology.cu).  Uses the arena from its start.
+int32_t surface_topology_locked(v3d_context* ctx, const v3d_mesh_triangle* triangles, uint64_t nt,
+                                uint64_t n, v3d_surface_topology* out, float* device_ms,
+                                uint64_t* launches);
+
 // Incremental SHA-256 on the host (sha256.cpp).
 struct Sha256 {
     uint32_t h[8];

@@ -105,12 +105,22 @@ __global__ void k_flatten(uint32_t* parent, uint64_t n) {
         parent[v] = find_root(parent, (uint32_t)v);
 }
 
-// Triangles per island root (the root of each triangle's first vertex).
+// Triangles per island root (the root of each triangle's first vertex).  The
+// lanes of a warp that share a root add once (neighbouring triangles mostly
+// share one), so a large island does not serialise on one address.
 __global__ void k_island_sizes(const v3d_mesh_triangle* __restrict__ tris, uint64_t nt,
                                const uint32_t* __restrict__ root, unsigned long long* __restrict__ size) {
-    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < nt;
-         t += (uint64_t)gridDim.x * blockDim.x)
-        atomicAdd(&size[root[tris[t].a]], 1ull);
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t first = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    // every lane of a warp takes the same number of turns, so the warp stays whole
+    const uint64_t warp_first = first - (threadIdx.x & 31);
+    for (uint64_t t0 = warp_first; t0 < nt; t0 += stride) {
+        const uint64_t t = t0 + (threadIdx.x & 31);
+        const uint32_t r = t < nt ? root[tris[t].a] : 0xFFFFFFFFu;
+        const unsigned same = __match_any_sync(0xFFFFFFFFu, r);
+        if (r != 0xFFFFFFFFu && (threadIdx.x & 31) == __ffs(same) - 1)
+            atomicAdd(&size[r], (unsigned long long)__popc(same));
+    }
 }
 
 // The island figures over the roots, and the edges that occur once.
@@ -134,11 +144,31 @@ __global__ void k_topology_counts(const unsigned long long* __restrict__ size, u
         const unsigned long long k = sorted[i];
         if ((i == 0 || sorted[i - 1] != k) && (i + 1 == n_keys || sorted[i + 1] != k)) ++boundary;
     }
-    atomicAdd(&out[0], islands);
-    atomicAdd(&out[1], small);
-    atomicAdd(&out[2], small_tris);
-    atomicMax(&out[3], largest);
-    atomicAdd(&out[4], boundary);
+    // one atomic per block and figure: the warps reduce by shuffles, the
+    // block through shared memory
+    unsigned long long v[5] = {islands, small, small_tris, largest, boundary};
+#pragma unroll
+    for (int k = 0; k < 5; ++k)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long w = __shfl_down_sync(0xFFFFFFFFu, v[k], o);
+            v[k] = k == 3 ? max(v[k], w) : v[k] + w;
+        }
+    __shared__ unsigned long long part[5][32];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, warps = (blockDim.x + 31) >> 5;
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < 5; ++k) part[k][warp] = v[k];
+    __syncthreads();
+    if (threadIdx.x < 5) {
+        const int k = threadIdx.x;
+        unsigned long long a = 0;
+        for (int w = 0; w < warps; ++w) a = k == 3 ? max(a, part[k][w]) : a + part[k][w];
+        if (a) {
+            if (k == 3) atomicMax(&out[3], a);
+            else atomicAdd(&out[k], a);
+        }
+    }
 }
 
 unsigned grid_of(uint64_t n) {
@@ -169,6 +199,21 @@ extern "C" int32_t v3d_surface_topology_of(v3d_context* ctx, const v3d_mesh_tria
     if (nt == 0) return V3D_OK;
     std::lock_guard<std::mutex> lock(ctx->mu);
     cudaSetDevice(ctx->device);
+    float ms = 0.f;
+    uint64_t launches = 0;
+    const int32_t status = v3d::surface_topology_locked(ctx, triangles, nt, n, out, &ms, &launches);
+    if (status == V3D_OK) {
+        ctx->last_ms = ms;
+        ctx->last_launches = launches;
+    }
+    return status;
+}
+
+namespace v3d {
+
+int32_t surface_topology_locked(v3d_context* ctx, const v3d_mesh_triangle* triangles, uint64_t nt,
+                                uint64_t n, v3d_surface_topology* out, float* device_ms,
+                                uint64_t* launches) {
     cudaStream_t st = static_cast<cudaStream_t>(ctx->stream);
     const uint64_t nk = 3 * nt;
     size_t t_sort = 0;
@@ -233,7 +278,9 @@ extern "C" int32_t v3d_surface_topology_of(v3d_context* ctx, const v3d_mesh_tria
     out->largest_island_triangles = h[3];
     out->boundary_edges = h[4];
     float ms = 0.f;
-    if (cudaEventElapsedTime(&ms, ev0, ev1) == cudaSuccess) ctx->last_ms = ms;
-    ctx->last_launches = g_kernel_launches - launches0;
+    if (cudaEventElapsedTime(&ms, ev0, ev1) == cudaSuccess) *device_ms = ms;
+    *launches = g_kernel_launches - launches0;
     return V3D_OK;
 }
+
+}  // namespace v3d

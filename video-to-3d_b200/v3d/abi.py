@@ -254,6 +254,25 @@ class SurfaceTopology(C.Structure):
         "boundary_edges")]
 
 
+class MeshingFunnel(C.Structure):
+    _fields_ = [(name, C.c_uint64) for name in (
+        "depth_views", "meshed_reference_views", "candidate_cells", "rejected_discontinuities",
+        "rejected_degenerate", "multiply_verified_samples", "exported_triangles")]
+
+
+class VerifiedSurfaceRegion(C.Structure):
+    _fields_ = [("reference_frame", C.c_uint64), ("first_point", C.c_uint64),
+                ("point_count", C.c_uint64), ("source_frames", C.c_uint64 * 4),
+                ("n_source_frames", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class VerifiedSurface(C.Structure):
+    _fields_ = [("verification", VerificationFunnel), ("meshing", MeshingFunnel),
+                ("topology", SurfaceTopology), ("dominant_rejection", C.c_int32),
+                ("reserved", C.c_int32), ("n_points", C.c_uint64), ("n_triangles", C.c_uint64),
+                ("n_regions", C.c_uint64)]
+
+
 class DenseDocument(C.Structure):
     _fields_ = [("document_bytes", C.c_uint64), ("points_bytes", C.c_uint64),
                 ("grid_sites_bytes", C.c_uint64), ("point_attributes_bytes", C.c_uint64),
@@ -262,6 +281,8 @@ class DenseDocument(C.Structure):
 
 STRUCTS = {
     "v3d_dense_document": DenseDocument,
+    "v3d_meshing_funnel": MeshingFunnel, "v3d_verified_surface_region": VerifiedSurfaceRegion,
+    "v3d_verified_surface": VerifiedSurface,
     "v3d_surface_topology": SurfaceTopology,
     "v3d_depth_view": DepthView, "v3d_verification_funnel": VerificationFunnel,
     "v3d_verified_sample": VerifiedSample,

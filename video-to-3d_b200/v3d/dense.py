@@ -117,6 +117,14 @@ def library():
     L.v3d_plan_clips.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64, _P(C.c_uint64),
                                  _P(C.c_uint64), _P(C.c_int32)]
     L.v3d_plan_clips.restype = C.c_int32
+    L.v3d_verified_surface_bounds.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64,
+                                              _P(C.c_uint64), _P(C.c_uint64)]
+    L.v3d_verified_surface_bounds.restype = None
+    L.v3d_mesh_verified_depth_grids.argtypes = [
+        C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint32,
+        C.c_uint32, C.c_double, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64,
+        C.c_void_p, _P(abi.VerifiedSurface)]
+    L.v3d_mesh_verified_depth_grids.restype = C.c_int32
     L.v3d_dense_document_bound.argtypes = [C.c_uint64] * 5
     L.v3d_dense_document_bound.restype = C.c_uint64
     L.v3d_encode_dense_evidence.argtypes = [
@@ -380,6 +388,17 @@ class Context:
         self._check(st)
         return doc, info
 
+    def mesh_verified_depth_grids(self, views, reference_views, source_views, stride,
+                                  reference_stride, focal):
+        """The geometric part of the COLMAP export (colmap_surface.rs:380-471)
+        on the device: a VerifiedSurface.  A SKIPPED status (no triangle) is
+        returned, not raised, with the diagnostics filled."""
+        st, surf = _surface(self.lib.v3d_mesh_verified_depth_grids, (self.handle,), views,
+                            reference_views, source_views, stride, reference_stride, focal)
+        if st != abi.SKIPPED:
+            self._check(st)
+        return surf
+
     def fuse_mutually_supported_vertices(self, points, triangles, membership, control=None):
         """fuse_mutually_supported_vertices_with_control (surface_fusion.rs:369-549)
         on the device: moves `points` in place and returns a FusionOutcome."""
@@ -437,11 +456,9 @@ VERIFIED_DTYPE = np.dtype([("x", "<f4"), ("y", "<f4"), ("z", "<f4"), ("confidenc
                            ("site_x", "<u4"), ("site_y", "<u4"), ("source_mask", "<u4")])
 
 
-def _verify(lib_fn, head, views, reference_views, source_views, stride, reference_stride, focal):
-    """Shared by the device entry point and the oracle: views is a list of
-    (rgba uint8 [h, w, 4], depth float32 [rows, cols], camera); source_views one
-    list of at most 4 view indices per reference.  Returns (samples per
-    reference as VERIFIED_DTYPE arrays, funnel dict)."""
+def _depth_views(views, reference_views, source_views):
+    """ctypes arrays of v3d_depth_view, references and 4 sources per reference
+    (-1 for none), and the numpy arrays they point into."""
     keep = []
     arr = (abi.DepthView * max(len(views), 1))()
     for i, (rgba, depth, cam) in enumerate(views):
@@ -460,6 +477,65 @@ def _verify(lib_fn, head, views, reference_views, source_views, stride, referenc
         if len(s) > 4:
             raise ValueError("at most 4 source views per reference")
         src[r, :len(s)] = s
+    return arr, keep, refs, src
+
+
+DOMINANT_REJECTIONS = [None, "missing_reference_depth", "insufficient_parallax", "behind_source",
+                       "outside_source", "missing_source_depth", "depth_disagreement",
+                       "color_disagreement"]
+
+
+class VerifiedSurface:
+    """The geometric part of the COLMAP export: points (POINT_DTYPE), sites
+    (SITE_DTYPE), triangles (TRIANGLE_DTYPE, indices into points), regions
+    (dicts of reference_frame, first_point, point_count, source_frames) and
+    diagnostics (verification, meshing, topology, dominant_rejection); status
+    is OK, or SKIPPED when no triangle was exported."""
+
+    def __init__(self, status, points, sites, triangles, regions, diagnostics):
+        self.status = status
+        self.points = points
+        self.sites = sites
+        self.triangles = triangles
+        self.regions = regions
+        self.diagnostics = diagnostics
+
+
+def _surface(lib_fn, head, views, reference_views, source_views, stride, reference_stride, focal):
+    arr, keep, refs, src = _depth_views(views, reference_views, source_views)
+    n_ref = len(reference_views)
+    h, w = (views[0][0].shape[0], views[0][0].shape[1]) if views else (0, 0)
+    mp, mt = C.c_uint64(), C.c_uint64()
+    library().v3d_verified_surface_bounds(w, h, int(reference_stride), n_ref, C.byref(mp), C.byref(mt))
+    pts = np.empty(max(mp.value, 1), dtype=types.POINT_DTYPE)
+    sites = np.empty(max(mp.value, 1), dtype=types.SITE_DTYPE)
+    tris = np.empty(max(mt.value, 1), dtype=types.TRIANGLE_DTYPE)
+    regs = (abi.VerifiedSurfaceRegion * max(n_ref, 1))()
+    out = abi.VerifiedSurface()
+    st = lib_fn(*head, arr, len(views), refs.ctypes.data, n_ref, src.ctypes.data, int(stride),
+                int(reference_stride), float(focal), pts.ctypes.data, sites.ctypes.data, len(pts),
+                tris.ctypes.data, len(tris), regs, C.byref(out))
+    as_dict = lambda s: {name: int(getattr(s, name)) for name, _ in s._fields_}  # noqa: E731
+    diag = {"verification": as_dict(out.verification), "meshing": as_dict(out.meshing),
+            "topology": as_dict(out.topology),
+            "dominant_rejection": DOMINANT_REJECTIONS[out.dominant_rejection]}
+    if st != 0:
+        return st, VerifiedSurface(st, pts[:0], sites[:0], tris[:0], [], diag)
+    regions = [{"reference_frame": int(g.reference_frame), "first_point": int(g.first_point),
+                "point_count": int(g.point_count),
+                "source_frames": [int(g.source_frames[i]) for i in range(g.n_source_frames)]}
+               for g in regs[:out.n_regions]]
+    n, nt = out.n_points, out.n_triangles
+    return st, VerifiedSurface(st, pts[:n], sites[:n], tris[:nt], regions, diag)
+
+
+def _verify(lib_fn, head, views, reference_views, source_views, stride, reference_stride, focal):
+    """Shared by the device entry point and the oracle: views is a list of
+    (rgba uint8 [h, w, 4], depth float32 [rows, cols], camera); source_views one
+    list of at most 4 view indices per reference.  Returns (samples per
+    reference as VERIFIED_DTYPE arrays, funnel dict)."""
+    arr, keep, refs, src = _depth_views(views, reference_views, source_views)
+    n_ref = len(reference_views)
     h, w = (views[0][0].shape[0], views[0][0].shape[1]) if views else (0, 0)
     cap = max(n_ref * (-(-w // reference_stride)) * (-(-h // reference_stride)), 1)
     out = np.empty(cap, dtype=VERIFIED_DTYPE)
