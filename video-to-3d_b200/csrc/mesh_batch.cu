@@ -196,42 +196,90 @@ __global__ void k_mb_vertices(MeshScratch s, const v3d_point* __restrict__ pts,
     }
 }
 
+// Adds one lane's outcome counts to its patch's counters.  Consecutive
+// lanes nearly always share a patch: the warp then reduces its counts and
+// adds once per counter instead of every lane hitting the same addresses.
+// Every lane of the warp must call this.
+__device__ __forceinline__ void add_patch_counts(MeshCounters* counters, uint32_t pi, bool valid,
+                                                 unsigned vertices, unsigned cells, unsigned cands,
+                                                 unsigned acc, unsigned disc, unsigned degen) {
+    const unsigned full = 0xFFFFFFFFu;
+    const uint32_t pi0 = __shfl_sync(full, pi, 0);
+    if (__all_sync(full, !valid || pi == pi0)) {
+        vertices = __reduce_add_sync(full, vertices);
+        cells = __reduce_add_sync(full, cells);
+        cands = __reduce_add_sync(full, cands);
+        acc = __reduce_add_sync(full, acc);
+        disc = __reduce_add_sync(full, disc);
+        degen = __reduce_add_sync(full, degen);
+        if ((threadIdx.x & 31) != 0) return;
+        pi = pi0;
+    } else if (!valid) {
+        return;
+    }
+    MeshCounters& c = counters[pi];
+    if (vertices) atomicAdd(&c.vertices, (unsigned long long)vertices);
+    if (cells) atomicAdd(&c.candidate_cells, (unsigned long long)cells);
+    if (cands) atomicAdd(&c.candidate_triangles, (unsigned long long)cands);
+    if (acc) atomicAdd(&c.accepted, (unsigned long long)acc);
+    if (disc) atomicAdd(&c.discontinuities, (unsigned long long)disc);
+    if (degen) atomicAdd(&c.degenerate, (unsigned long long)degen);
+}
+
 __global__ void k_mb_winners(MeshScratch s, const v3d_grid_site* __restrict__ sites,
                              const uint32_t* __restrict__ patch_of, uint64_t n) {
     const MVtx* vtx = static_cast<const MVtx*>(s.vtx);
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
-         i += (uint64_t)gridDim.x * blockDim.x) {
-        const MVtx v = vtx[i];
-        if (v.local == kNone) continue;
-        const uint32_t pi = patch_of ? patch_of[i] : 0u;
-        const MeshPatchDev& P = s.patches[pi];
-        const v3d_grid_site st = sites[i];
-        const uint64_t cell = P.grid_off + (uint64_t)((st.y - P.border) / P.stride) * P.gw +
-                              (st.x - P.border) / P.stride;
-        if (s.grid_keys[cell] == vkey(v.conf, v.local)) {
-            s.winners[cell] = (uint32_t)i;
-            atomicAdd(&s.counters[pi].vertices, 1ull);
+    const unsigned lane = threadIdx.x & 31;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    // warp-aligned turns, so every lane reaches the counter reduction
+    for (uint64_t i0 = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x - lane; i0 < n; i0 += stride) {
+        const uint64_t i = i0 + lane;
+        uint32_t pi = 0;
+        unsigned won = 0;
+        if (i < n) {
+            const MVtx v = vtx[i];
+            pi = patch_of ? patch_of[i] : 0u;
+            if (v.local != kNone) {
+                const MeshPatchDev& P = s.patches[pi];
+                const v3d_grid_site st = sites[i];
+                const uint64_t cell = P.grid_off + (uint64_t)((st.y - P.border) / P.stride) * P.gw +
+                                      (st.x - P.border) / P.stride;
+                if (s.grid_keys[cell] == vkey(v.conf, v.local)) {
+                    s.winners[cell] = (uint32_t)i;
+                    won = 1;
+                }
+            }
         }
+        add_patch_counts(s.counters, pi, i < n, won, 0, 0, 0, 0, 0);
     }
 }
 
 __global__ void k_mb_slots(MeshScratch s, uint32_t n_patches, uint64_t total_slots) {
-    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < total_slots;
-         g += (uint64_t)gridDim.x * blockDim.x) {
-        s.slot_status[g] = 0;
-        const uint32_t pi = patch_of_slot(s.patches, n_patches, g);
-        const MeshPatchDev& P = s.patches[pi];
-        MeshCounters& c = s.counters[pi];
-        if (P.n_points < 3 || c.vertices < 3) continue;
-        const MVtx *a, *b, *cc;
-        double jump;
-        bool counts_cell;
-        if (!slot_triangle(s, P, g - P.slot_off, a, b, cc, jump, counts_cell)) continue;
-        if (counts_cell) atomicAdd(&c.candidate_cells, 1ull);
-        atomicAdd(&c.candidate_triangles, 1ull);
-        const uint8_t st = gate(P, *a, *b, *cc, jump);
-        s.slot_status[g] = st;
-        atomicAdd(st == 1 ? &c.accepted : (st == 2 ? &c.discontinuities : &c.degenerate), 1ull);
+    const unsigned lane = threadIdx.x & 31;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t g0 = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x - lane; g0 < total_slots; g0 += stride) {
+        const uint64_t g = g0 + lane;
+        uint32_t pi = 0;
+        unsigned cells = 0, cands = 0, acc = 0, disc = 0, degen = 0;
+        if (g < total_slots) {
+            s.slot_status[g] = 0;
+            pi = patch_of_slot(s.patches, n_patches, g);
+            const MeshPatchDev& P = s.patches[pi];
+            const MVtx *a, *b, *cc;
+            double jump;
+            bool counts_cell;
+            if (P.n_points >= 3 && s.counters[pi].vertices >= 3 &&
+                slot_triangle(s, P, g - P.slot_off, a, b, cc, jump, counts_cell)) {
+                cells = counts_cell ? 1u : 0u;
+                cands = 1;
+                const uint8_t st = gate(P, *a, *b, *cc, jump);
+                s.slot_status[g] = st;
+                acc = st == 1;
+                disc = st == 2;
+                degen = st != 1 && st != 2;
+            }
+        }
+        add_patch_counts(s.counters, pi, g < total_slots, 0, cells, cands, acc, disc, degen);
     }
 }
 
