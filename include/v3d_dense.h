@@ -887,6 +887,37 @@ int32_t v3d_encode_dense_evidence(
 void v3d_pack_dense_points(const v3d_point* points, uint64_t n_points,
                            uint8_t* values_f32_le, uint8_t* rgb);
 
+/* TriangleSourceCorners (reconstruction_evidence.rs:124-130). */
+typedef struct v3d_triangle_source {
+    uint64_t triangle;
+    uint64_t corners[3];
+} v3d_triangle_source;
+
+/* DerivedVertexSource (reconstruction_evidence.rs:142-153). */
+typedef struct v3d_derived_vertex_source {
+    uint64_t point_index;
+    uint64_t source_triangle;
+    uint64_t source_corners[3];
+    double barycentric[3];
+} v3d_derived_vertex_source;
+
+/* The browser transport's packed mesh buffers (pack_mesh_triangles,
+ * crates/video-to-3d-wasm/src/lib.rs:269-326): indices_u32_le 12 bytes and
+ * confidence_f32_le 4 bytes a triangle, sources_u32_le 16 bytes a source
+ * record (triangle, a, b, c), derived_u32_le 20 bytes and
+ * derived_barycentric_f64_le 24 bytes a derived record.  Checks in the
+ * reference's order (sources, derived, then triangles); on failure returns
+ * V3D_ERR_INVALID_ARGUMENT and, when error is not NULL, points it at the
+ * reference's message ("failed to serialize reconstruction: ...").  Host
+ * only; no device or context. */
+int32_t v3d_pack_mesh_triangles(const v3d_mesh_triangle* triangles, uint64_t n_triangles,
+                                const v3d_triangle_source* sources, uint64_t n_sources,
+                                const v3d_derived_vertex_source* derived, uint64_t n_derived,
+                                uint64_t point_count, uint8_t* indices_u32_le,
+                                uint8_t* confidence_f32_le, uint8_t* sources_u32_le,
+                                uint8_t* derived_u32_le, uint8_t* derived_barycentric_f64_le,
+                                const char** error);
+
 /* SHA-256 (FIPS 180-4) of bytes[n] into digest[32], on the host; the hash of
  * ContentHash::of_bytes (scene_project.rs:463-465). */
 void v3d_sha256(const void* bytes, uint64_t n, uint8_t* digest);

@@ -256,4 +256,60 @@ void v3do_pack_dense_points(const v3d_point* points, uint64_t n, uint8_t* values
     }
 }
 
+// pack_mesh_triangles (crates/video-to-3d-wasm/src/lib.rs:269-326), byte by
+// byte; returns 0, or 1 + the index of the failing message (0 source range,
+// 1 missing point, 2 point index range).
+int32_t v3do_pack_mesh_triangles(const v3d_mesh_triangle* triangles, uint64_t nt,
+                                 const v3d_triangle_source* sources, uint64_t ns,
+                                 const v3d_derived_vertex_source* derived, uint64_t nd, uint64_t point_count,
+                                 uint8_t* indices, uint8_t* confidence, uint8_t* src, uint8_t* der,
+                                 uint8_t* bary) {
+    auto le32 = [](uint8_t* at, uint64_t v) {
+        for (int q = 0; q < 4; ++q) at[q] = (uint8_t)(v >> (8 * q));
+    };
+    auto le64 = [](uint8_t* at, uint64_t v) {
+        for (int q = 0; q < 8; ++q) at[q] = (uint8_t)(v >> (8 * q));
+    };
+    size_t o = 0;
+    for (uint64_t i = 0; i < ns; ++i) {
+        const uint64_t v[4] = {sources[i].triangle, sources[i].corners[0], sources[i].corners[1],
+                               sources[i].corners[2]};
+        for (uint64_t x : v) {
+            if (x > 0xFFFFFFFFull) return 1;
+            le32(src + o, x);
+            o += 4;
+        }
+    }
+    o = 0;
+    size_t ob = 0;
+    for (uint64_t i = 0; i < nd; ++i) {
+        const uint64_t v[5] = {derived[i].point_index, derived[i].source_triangle, derived[i].source_corners[0],
+                               derived[i].source_corners[1], derived[i].source_corners[2]};
+        for (uint64_t x : v) {
+            if (x > 0xFFFFFFFFull) return 1;
+            le32(der + o, x);
+            o += 4;
+        }
+        for (double w : derived[i].barycentric) {
+            uint64_t b;
+            std::memcpy(&b, &w, 8);
+            le64(bary + ob, b);
+            ob += 8;
+        }
+    }
+    o = 0;
+    for (uint64_t t = 0; t < nt; ++t) {
+        for (uint64_t x : {triangles[t].a, triangles[t].b, triangles[t].c}) {
+            if (x >= point_count) return 2;
+            if (x > 0xFFFFFFFFull) return 3;
+            le32(indices + o, x);
+            o += 4;
+        }
+        uint32_t c;
+        std::memcpy(&c, &triangles[t].confidence, 4);
+        le32(confidence + 4 * t, c);
+    }
+    return 0;
+}
+
 }  // extern "C"

@@ -82,6 +82,9 @@ class Oracle:
             C.c_uint64, C.c_char_p, C.c_uint64, C.c_void_p, C.c_uint64, _P(abi.DenseDocument)]
         L.v3do_encode_dense_evidence.restype = C.c_int32
         L.v3do_pack_dense_points.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]
+        L.v3do_pack_mesh_triangles.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64,
+                                               C.c_void_p, C.c_uint64, C.c_uint64] + [C.c_void_p] * 5
+        L.v3do_pack_mesh_triangles.restype = C.c_int32
 
     def fuse_mutually_supported_vertices(self, points, triangles, membership, control=None):
         """surface_fusion.rs:369-549 on the CPU: moves `points` in place."""
@@ -150,6 +153,23 @@ class Oracle:
         self.lib.v3do_pack_dense_points(pts.ctypes.data, len(pts), values.ctypes.data,
                                         rgb.ctypes.data)
         return values.tobytes(), rgb.tobytes()
+
+    def pack_mesh_triangles(self, triangles, point_count, sources, derived):
+        """pack_mesh_triangles (wasm/src/lib.rs:269-326) on the CPU: (status,
+        buffers dict); status 0, or 1 + the index of the failing message."""
+        import numpy as np
+        from v3d import dense
+        tris = np.ascontiguousarray(triangles, dtype=types.TRIANGLE_DTYPE)
+        src = np.ascontiguousarray(sources, dtype=dense.TRIANGLE_SOURCE_DTYPE)
+        der = np.ascontiguousarray(derived, dtype=dense.DERIVED_VERTEX_DTYPE)
+        bufs = [np.zeros(k * n, np.uint8) for k, n in
+                ((12, len(tris)), (4, len(tris)), (16, len(src)), (20, len(der)), (24, len(der)))]
+        st = self.lib.v3do_pack_mesh_triangles(
+            tris.ctypes.data, len(tris), src.ctypes.data, len(src), der.ctypes.data, len(der),
+            int(point_count), *(b.ctypes.data for b in bufs))
+        names = ["indices_u32_le", "confidence_f32_le", "sources_u32_le", "derived_u32_le",
+                 "derived_barycentric_f64_le"]
+        return st, dict(zip(names, (b.tobytes() for b in bufs)))
 
     def reference_candidate_order(self, frames, cameras, sparse_points, focal):
         """dense.rs:620-672 on the CPU: camera indices in planning order."""

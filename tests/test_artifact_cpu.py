@@ -184,3 +184,58 @@ def test_oracle_document_reads_back():
     empty, info = Oracle().encode_dense_evidence(None, None, None)
     assert empty == b'[],"grid_sites":[],"point_attributes":[]'
     assert (info["points_bytes"], info["grid_sites_bytes"], info["point_attributes_bytes"]) == (2, 2, 2)
+
+
+def _mesh_records(n, seed, points=1000):
+    rng = np.random.default_rng(seed)
+    tris = np.zeros(n, dtype=types.TRIANGLE_DTYPE)
+    for f in ("a", "b", "c"):
+        tris[f] = rng.integers(0, points, n)
+    tris["confidence"] = rng.random(n).astype(np.float32)
+    src = np.zeros(n // 3, dtype=dense.TRIANGLE_SOURCE_DTYPE)
+    src["triangle"] = np.sort(rng.integers(0, n, len(src)))
+    src["corners"] = rng.integers(0, points, (len(src), 3))
+    der = np.zeros(n // 5, dtype=dense.DERIVED_VERTEX_DTYPE)
+    der["point_index"] = points + np.arange(len(der))
+    der["source_triangle"] = rng.integers(0, n, len(der))
+    der["source_corners"] = rng.integers(0, points, (len(der), 3))
+    w = rng.random((len(der), 3))
+    der["barycentric"] = w / w.sum(axis=1, keepdims=True)
+    return tris, src, der
+
+
+def test_pack_mesh_triangles():
+    tris, src, der = _mesh_records(3000, 4)
+    got = dense.pack_mesh_triangles(tris, 1000, src, der)
+    st, want = Oracle().pack_mesh_triangles(tris, 1000, src, der)
+    assert st == 0 and got == want
+    idx = np.stack([tris["a"], tris["b"], tris["c"]], axis=1).astype("<u4").tobytes()
+    assert got["indices_u32_le"] == idx
+    assert got["confidence_f32_le"] == tris["confidence"].astype("<f4").tobytes()
+    assert got["derived_barycentric_f64_le"] == der["barycentric"].astype("<f8").tobytes()
+    assert dense.pack_mesh_triangles(tris[:0], 0) == {
+        k: b"" for k in ("indices_u32_le", "confidence_f32_le", "sources_u32_le", "derived_u32_le",
+                         "derived_barycentric_f64_le")}
+
+
+@pytest.mark.parametrize("case,message", [
+    ("missing", "mesh triangle references a missing dense point"),
+    ("index", "dense point index exceeds browser transport range"),
+    ("source", "triangle source exceeds browser transport range"),
+    ("derived", "triangle source exceeds browser transport range")])
+def test_pack_mesh_triangles_errors(case, message):
+    tris, src, der = _mesh_records(30, 5)
+    count = 1000
+    if case == "missing":
+        tris["b"][7] = 1000
+    elif case == "index":
+        count = 1 << 40
+        tris["c"][3] = 1 << 33
+    elif case == "source":
+        src["corners"][2, 1] = 1 << 32
+    else:
+        der["source_triangle"][1] = 1 << 32
+    with pytest.raises(ValueError, match=message):
+        dense.pack_mesh_triangles(tris, count, src, der)
+    st, _ = Oracle().pack_mesh_triangles(tris, count, src, der)
+    assert st == {"source": 1, "derived": 1, "missing": 2, "index": 3}[case]

@@ -559,6 +559,60 @@ extern "C" void v3d_pack_dense_points(const v3d_point* points, uint64_t n, uint8
     }
 }
 
+extern "C" int32_t v3d_pack_mesh_triangles(const v3d_mesh_triangle* triangles, uint64_t nt,
+                                           const v3d_triangle_source* sources, uint64_t ns,
+                                           const v3d_derived_vertex_source* derived, uint64_t nd,
+                                           uint64_t point_count, uint8_t* indices_u32_le,
+                                           uint8_t* confidence_f32_le, uint8_t* sources_u32_le,
+                                           uint8_t* derived_u32_le, uint8_t* derived_barycentric_f64_le,
+                                           const char** error) {
+    static_assert(__BYTE_ORDER__ == __ORDER_LITTLE_ENDIAN__, "to_le_bytes is the in-memory layout");
+    const char* const source_range =
+        "failed to serialize reconstruction: triangle source exceeds browser transport range";
+    auto fail = [&](const char* why) {
+        if (error) *error = why;
+        return (int32_t)V3D_ERR_INVALID_ARGUMENT;
+    };
+    if (error) *error = nullptr;
+    if ((nt && (!triangles || !indices_u32_le || !confidence_f32_le)) || (ns && (!sources || !sources_u32_le)) ||
+        (nd && (!derived || !derived_u32_le || !derived_barycentric_f64_le)))
+        return V3D_ERR_INVALID_ARGUMENT;
+    auto put_u32 = [](uint8_t* at, uint64_t v) {
+        const uint32_t w = (uint32_t)v;
+        std::memcpy(at, &w, 4);
+    };
+    for (uint64_t i = 0; i < ns; ++i) {
+        const uint64_t v[4] = {sources[i].triangle, sources[i].corners[0], sources[i].corners[1],
+                               sources[i].corners[2]};
+        for (int k = 0; k < 4; ++k) {
+            if (v[k] > 0xFFFFFFFFull) return fail(source_range);
+            put_u32(sources_u32_le + 16 * i + 4 * k, v[k]);
+        }
+    }
+    for (uint64_t i = 0; i < nd; ++i) {
+        const v3d_derived_vertex_source& d = derived[i];
+        const uint64_t v[5] = {d.point_index, d.source_triangle, d.source_corners[0], d.source_corners[1],
+                               d.source_corners[2]};
+        for (int k = 0; k < 5; ++k) {
+            if (v[k] > 0xFFFFFFFFull) return fail(source_range);
+            put_u32(derived_u32_le + 20 * i + 4 * k, v[k]);
+        }
+        std::memcpy(derived_barycentric_f64_le + 24 * i, d.barycentric, 24);
+    }
+    for (uint64_t t = 0; t < nt; ++t) {
+        const uint64_t v[3] = {triangles[t].a, triangles[t].b, triangles[t].c};
+        for (int k = 0; k < 3; ++k) {
+            if (v[k] >= point_count)
+                return fail("failed to serialize reconstruction: mesh triangle references a missing dense point");
+            if (v[k] > 0xFFFFFFFFull)
+                return fail("failed to serialize reconstruction: dense point index exceeds browser transport range");
+            put_u32(indices_u32_le + 12 * t + 4 * k, v[k]);
+        }
+        std::memcpy(confidence_f32_le + 4 * t, &triangles[t].confidence, 4);
+    }
+    return V3D_OK;
+}
+
 extern "C" int32_t v3d_encode_dense_evidence(
     v3d_context* ctx, const v3d_point* points, uint64_t np, const v3d_grid_site* sites, uint64_t ns,
     const v3d_point_attributes* attrs, uint64_t na, const char* prefix, uint64_t prefix_bytes,

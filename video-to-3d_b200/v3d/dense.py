@@ -134,6 +134,10 @@ def library():
     L.v3d_encode_dense_evidence.restype = C.c_int32
     L.v3d_pack_dense_points.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]
     L.v3d_pack_dense_points.restype = None
+    L.v3d_pack_mesh_triangles.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64,
+                                          C.c_void_p, C.c_uint64, C.c_uint64] + [C.c_void_p] * 5 + [
+                                          _P(C.c_char_p)]
+    L.v3d_pack_mesh_triangles.restype = C.c_int32
     L.v3d_sha256.argtypes = [C.c_char_p, C.c_uint64, C.c_void_p]
     L.v3d_sha256.restype = None
     L.v3d_measure_gather_rate.argtypes = [C.c_void_p, _P(C.c_double)]
@@ -596,6 +600,34 @@ def pack_dense_points(points):
     rgb = np.empty(3 * len(pts), dtype=np.uint8)
     library().v3d_pack_dense_points(pts.ctypes.data, len(pts), values.ctypes.data, rgb.ctypes.data)
     return values.tobytes(), rgb.tobytes()
+
+
+TRIANGLE_SOURCE_DTYPE = np.dtype([("triangle", "<u8"), ("corners", "<u8", (3,))])
+DERIVED_VERTEX_DTYPE = np.dtype([("point_index", "<u8"), ("source_triangle", "<u8"),
+                                 ("source_corners", "<u8", (3,)), ("barycentric", "<f8", (3,))])
+
+
+def pack_mesh_triangles(triangles, point_count, sources=None, derived=None):
+    """pack_mesh_triangles (crates/video-to-3d-wasm/src/lib.rs:269-326): a dict
+    of the five little-endian buffers; ValueError with the reference's message
+    when an index does not fit the transport."""
+    tris = np.ascontiguousarray(triangles, dtype=types.TRIANGLE_DTYPE)
+    src = np.ascontiguousarray(np.zeros(0, TRIANGLE_SOURCE_DTYPE) if sources is None else sources,
+                               dtype=TRIANGLE_SOURCE_DTYPE)
+    der = np.ascontiguousarray(np.zeros(0, DERIVED_VERTEX_DTYPE) if derived is None else derived,
+                               dtype=DERIVED_VERTEX_DTYPE)
+    bufs = {"indices_u32_le": np.empty(12 * len(tris), np.uint8),
+            "confidence_f32_le": np.empty(4 * len(tris), np.uint8),
+            "sources_u32_le": np.empty(16 * len(src), np.uint8),
+            "derived_u32_le": np.empty(20 * len(der), np.uint8),
+            "derived_barycentric_f64_le": np.empty(24 * len(der), np.uint8)}
+    err = C.c_char_p()
+    st = library().v3d_pack_mesh_triangles(
+        tris.ctypes.data, len(tris), src.ctypes.data, len(src), der.ctypes.data, len(der),
+        int(point_count), *(b.ctypes.data for b in bufs.values()), C.byref(err))
+    if st != 0:
+        raise ValueError(err.value.decode() if err.value else "invalid arguments")
+    return {k: v.tobytes() for k, v in bufs.items()}
 
 
 def content_hash(data):
