@@ -767,10 +767,13 @@ extern "C" int32_t v3d_mesh_verified_depth_grids(
     V3D_COUNTED k_first_use<<<grid_of(n_tris), 256, 0, st>>>(d_tris, d_tpatch, n_tris, d_moff, d_first);
     V3D_COUNTED k_iota_retained<<<grid_of(n_mesh), 256, 0, st>>>(d_first, n_mesh, d_vals, d_ctr + 1);
     V3D_CTX_CK(cudaGetLastError());
+    // keys below 3 * n_tris; one bit more keeps the unused inputs' all-ones keys last
+    int key_bits = 1;
+    while (key_bits < kFirstUseBits - 1 && (3ull * n_tris) >> key_bits) ++key_bits;
     size_t sb = sort_bytes;
     V3D_CTX_CK(cub::DeviceRadixSort::SortPairs(at(o_sort), sb, d_first,
                                                reinterpret_cast<unsigned long long*>(at(o_keys2)), d_vals, d_vals2,
-                                               (int)n_mesh, 0, kFirstUseBits, st));
+                                               (int)n_mesh, 0, key_bits + 1, st));
     V3D_COUNTED k_place<<<grid_of(n_mesh), 256, 0, st>>>(d_vals2, d_ctr + 1, d_mp, d_ms, d_mpatch, d_mmask, d_newidx,
                                                          d_outp, d_outs, d_msort, d_rfirst, d_rend);
     V3D_COUNTED k_region_masks<<<n_patches, 256, 0, st>>>(d_rfirst, d_rend, d_msort, d_rmask);

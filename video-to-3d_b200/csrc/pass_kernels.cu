@@ -176,29 +176,72 @@ __device__ __forceinline__ void sample_rgb(const DevReference& ref, int32_t stor
     p.r = p.g = p.b = (uint8_t)q;
 }
 
-__global__ void k_fuse(BatchDev b, const Cand* __restrict__ cands, const uint32_t* __restrict__ count,
-                       const RecipObs* __restrict__ obs, int completion, int pass,
-                       OutPoint* __restrict__ out, uint8_t* __restrict__ cand_status,
-                       RefCounters* __restrict__ ctr) {
-    const uint32_t n = *count;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const Cand cd = cands[i];
+// One candidate's contribution to its reference's counters.
+struct FuseCounts {
+    unsigned recip_rejected, consistent, fusion_input, fusion_rejected_obs, fusion_rejected,
+        footprint_rejected, accepted;
+};
+
+// Adds every lane's FuseCounts to its reference's counters: one atomic per
+// counter and warp when the warp's candidates share a reference (candidates
+// are listed reference by reference), one per lane otherwise.  Every lane of
+// the warp calls it.
+__device__ __forceinline__ void add_fuse_counts(RefCounters* ctr, uint32_t r, bool valid, FuseCounts k,
+                                                int completion, int pass) {
+    const unsigned full = 0xFFFFFFFFu;
+    unsigned cand = valid ? 1u : 0u;
+    const uint32_t r0 = __shfl_sync(full, r, 0);
+    if (__all_sync(full, !valid || r == r0)) {
+        cand = __reduce_add_sync(full, cand);
+        k.recip_rejected = __reduce_add_sync(full, k.recip_rejected);
+        k.consistent = __reduce_add_sync(full, k.consistent);
+        k.fusion_input = __reduce_add_sync(full, k.fusion_input);
+        k.fusion_rejected_obs = __reduce_add_sync(full, k.fusion_rejected_obs);
+        k.fusion_rejected = __reduce_add_sync(full, k.fusion_rejected);
+        k.footprint_rejected = __reduce_add_sync(full, k.footprint_rejected);
+        k.accepted = __reduce_add_sync(full, k.accepted);
+        if ((threadIdx.x & 31) != 0) return;
+        r = r0;
+    } else if (!valid) {
+        return;
+    }
+    RefCounters& c = ctr[r];
+    auto add = [](unsigned long long* at, unsigned v) {
+        if (v) atomicAdd(at, (unsigned long long)v);
+    };
+    add(&c.candidates, cand);
+    if (!completion) add(&c.checked, cand);
+    add(completion ? &c.rej_recip : &c.recip_rejected, k.recip_rejected);
+    add(completion ? &c.rej_fusion : &c.fusion_rejected_pts, k.fusion_rejected);
+    if (!completion) {
+        add(&c.consistent, k.consistent);
+        add(&c.fusion_input, k.fusion_input);
+        add(&c.fusion_rejected_obs, k.fusion_rejected_obs);
+        add(&c.primary_points, k.accepted);
+    } else {
+        add(&c.rej_footprint, k.footprint_rejected);
+        add(&c.completed, k.accepted);
+        add(&c.pass_additions[pass], k.accepted);
+    }
+}
+
+// fuse_depth_observations (dense_legacy.rs:859-884) and the point's
+// confidence and attributes for one candidate.
+__device__ __forceinline__ void fuse_one(const BatchDev& b, const Cand& cd, uint32_t i,
+                                         const RecipObs* __restrict__ o, int completion,
+                                         OutPoint* __restrict__ out, uint8_t* __restrict__ cand_status,
+                                         FuseCounts& k) {
+    {
         const DevReference& ref = b.refs[cd.ref];
-        RefCounters& c = ctr[cd.ref];
-        const RecipObs* o = obs + (uint64_t)i * kMaxSources;
-        atomicAdd(&c.candidates, 1ull);
         int nrec = 0;
         for (int s = 0; s < ref.n_src; ++s) nrec += o[s].valid;
-        if (!completion) atomicAdd(&c.checked, 1ull);
         if (nrec == 0) {
-            atomicAdd(completion ? &c.rej_recip : &c.recip_rejected, 1ull);
+            k.recip_rejected = 1;
             cand_status[i] = kCandRecipRejected;
-            continue;
+            return;
         }
-        if (!completion) {
-            atomicAdd(&c.consistent, 1ull);
-            atomicAdd(&c.fusion_input, (unsigned long long)(1 + nrec));
-        }
+        k.consistent = 1;
+        k.fusion_input = (unsigned)(1 + nrec);
         // fuse_depth_observations (dense_legacy.rs:859-884)
         double radius = fmax(dmul(fabs(cd.depth), kMaxFusionRelativePositionError), 1.0e-4);
         D3 sum = cd.pos;
@@ -218,11 +261,11 @@ __global__ void k_fuse(BatchDev b, const Cand* __restrict__ cands, const uint32_
             ++nobs;
         }
         D3 fused{ddiv(sum.x, (double)nobs), ddiv(sum.y, (double)nobs), ddiv(sum.z, (double)nobs)};
-        if (!completion) atomicAdd(&c.fusion_rejected_obs, (unsigned long long)rejected);
+        k.fusion_rejected_obs = (unsigned)rejected;
         if (nobs < kMinFusionObservations) {
-            atomicAdd(completion ? &c.rej_fusion : &c.fusion_rejected_pts, 1ull);
+            k.fusion_rejected = 1;
             cand_status[i] = kCandFusionRejected;
-            continue;
+            return;
         }
         const double S = (double)ref.n_src;
         const double support_conf = ddiv((double)cd.support, S);
@@ -238,16 +281,14 @@ __global__ void k_fuse(BatchDev b, const Cand* __restrict__ cands, const uint32_
                          !(fabs(dsub(fp.y, (double)cd.y)) >= limit);
             }
             if (!inside) {
-                atomicAdd(&c.rej_footprint, 1ull);
+                k.footprint_rejected = 1;
                 cand_status[i] = kCandFootprintRejected;
-                continue;
+                return;
             }
             double conf = dmul(dmul(dmul(dmul(cd.nconf, support_conf), recip_conf), error_conf),
                                kSurfaceCompletionConfidenceScale);
             op.p.confidence = (float)clampd(conf, 0.05, 0.9);
             op.a.depth_margin = (float)clampd(cd.margin, 0.0, 1.0);
-            atomicAdd(&c.completed, 1ull);
-            atomicAdd(&c.pass_additions[pass], 1ull);
         } else {
             double dm = isfinite(cd.margin) ? clampd(ddiv(cd.margin, b.prof.margin_saturation), 0.0, 1.0)
                                             : 1.0;
@@ -255,7 +296,6 @@ __global__ void k_fuse(BatchDev b, const Cand* __restrict__ cands, const uint32_
             double conf = dmul(dmul(dmul(support_conf, recip_conf), error_conf), mc);
             op.p.confidence = (float)clampd(conf, 0.05, 1.0);
             op.a.depth_margin = (float)dm;
-            atomicAdd(&c.primary_points, 1ull);
         }
         op.p.x = (float)fused.x;
         op.p.y = (float)fused.y;
@@ -272,6 +312,27 @@ __global__ void k_fuse(BatchDev b, const Cand* __restrict__ cands, const uint32_
         op.observations = (double)nobs;
         out[i] = op;
         cand_status[i] = kCandAccepted;
+        k.accepted = 1;
+    }
+}
+
+__global__ void k_fuse(BatchDev b, const Cand* __restrict__ cands, const uint32_t* __restrict__ count,
+                       const RecipObs* __restrict__ obs, int completion, int pass,
+                       OutPoint* __restrict__ out, uint8_t* __restrict__ cand_status,
+                       RefCounters* __restrict__ ctr) {
+    const uint32_t n = *count;
+    const unsigned lane = threadIdx.x & 31;
+    // warp-aligned turns, so every lane reaches the counter reduction
+    for (uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x - lane; i0 < n; i0 += gridDim.x * blockDim.x) {
+        const uint32_t i = i0 + lane;
+        FuseCounts k{};
+        uint32_t r = 0;
+        if (i < n) {
+            const Cand cd = cands[i];
+            r = cd.ref;
+            fuse_one(b, cd, i, obs + (uint64_t)i * kMaxSources, completion, out, cand_status, k);
+        }
+        add_fuse_counts(ctr, r, i < n, k, completion, pass);
     }
 }
 

@@ -80,17 +80,18 @@ __global__ void k_init_parent(uint32_t* parent, uint64_t n) {
         parent[v] = (uint32_t)v;
 }
 
-// Unions over every triangle edge and the sorted-edge keys (min << 32 | max).
+// Unions over every triangle edge and the edge keys (min << bits | max, with
+// `bits` enough for any vertex index, so the sort needs only 2 * bits).
 __global__ void k_unite_edges(const v3d_mesh_triangle* __restrict__ tris, uint64_t nt,
                               uint32_t* parent, unsigned long long* __restrict__ keys,
-                              uint32_t* err) {
+                              uint32_t* err, int bits) {
     for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < nt;
          t += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t v[3] = {(uint32_t)tris[t].a, (uint32_t)tris[t].b, (uint32_t)tris[t].c};
         for (int e = 0; e < 3; ++e) {
             const uint32_t a = v[e], b = v[(e + 1) % 3];
             const uint32_t lo = min(a, b), hi = max(a, b);
-            keys[3 * t + e] = ((unsigned long long)lo << 32) | hi;
+            keys[3 * t + e] = ((unsigned long long)lo << bits) | hi;
             unite(parent, a, b, err);
         }
     }
@@ -217,8 +218,10 @@ int32_t surface_topology_locked(v3d_context* ctx, const v3d_mesh_triangle* trian
     cudaStream_t st = static_cast<cudaStream_t>(ctx->stream);
     const uint64_t nk = 3 * nt;
     size_t t_sort = 0;
+    int bits = 1;  // bits of the largest vertex index
+    while (bits < 32 && (n - 1) >> bits) ++bits;
     cub::DeviceRadixSort::SortKeys(nullptr, t_sort, (unsigned long long*)nullptr,
-                                   (unsigned long long*)nullptr, (int)nk, 0, 64, st);
+                                   (unsigned long long*)nullptr, (int)nk, 0, 2 * bits, st);
     auto up = [](size_t x) { return (x + 255) & ~size_t(255); };
     const size_t o_tris = 0, o_parent = up(o_tris + sizeof(v3d_mesh_triangle) * nt),
                  o_size = up(o_parent + sizeof(uint32_t) * n),
@@ -254,12 +257,12 @@ int32_t surface_topology_locked(v3d_context* ctx, const v3d_mesh_triangle* trian
     } events{ev0, ev1};
     cudaEventRecord(ev0, st);
     V3D_COUNTED k_init_parent<<<grid_of(n), 256, 0, st>>>(d_parent, n);
-    V3D_COUNTED k_unite_edges<<<grid_of(nt), 256, 0, st>>>(d_tris, nt, d_parent, d_keys, d_err);
+    V3D_COUNTED k_unite_edges<<<grid_of(nt), 256, 0, st>>>(d_tris, nt, d_parent, d_keys, d_err, bits);
     V3D_COUNTED k_flatten<<<grid_of(n), 256, 0, st>>>(d_parent, n);
     V3D_COUNTED k_island_sizes<<<grid_of(nt), 256, 0, st>>>(d_tris, nt, d_parent, d_size);
     V3D_CTX_CK(cudaGetLastError());
     size_t bytes = t_sort;
-    V3D_CTX_CK(cub::DeviceRadixSort::SortKeys(base + o_tmp, bytes, d_keys, d_keys2, (int)nk, 0, 64, st));
+    V3D_CTX_CK(cub::DeviceRadixSort::SortKeys(base + o_tmp, bytes, d_keys, d_keys2, (int)nk, 0, 2 * bits, st));
     V3D_COUNTED k_topology_counts<<<grid_of(std::max(n, nk)), 256, 0, st>>>(d_size, n, d_keys2, nk, d_out);
     V3D_CTX_CK(cudaGetLastError());
     cudaEventRecord(ev1, st);
