@@ -95,7 +95,7 @@ struct Params {
 // One reference grid sample against each of its sources (verify_patch), the
 // union of the verdicts (verified_union).
 __global__ void k_verify(Params p, v3d_verified_sample* __restrict__ slot, uint8_t* __restrict__ kept,
-                         uint32_t* __restrict__ per_ref, unsigned long long* __restrict__ funnel) {
+                         unsigned long long* __restrict__ funnel) {
     const uint64_t cells = (uint64_t)p.cols * p.rows, total = cells * p.n_refs;
     uint32_t cnt[kOutcomes + 1] = {};  // [kOutcomes] = reference samples
     for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < total;
@@ -180,7 +180,6 @@ __global__ void k_verify(Params p, v3d_verified_sample* __restrict__ slot, uint8
         out.source_mask = mask;
         slot[g] = out;
         kept[g] = 1;
-        atomicAdd(&per_ref[r], 1u);
     }
     // the warp's counts, then one atomic per counter
 #pragma unroll
@@ -190,6 +189,26 @@ __global__ void k_verify(Params p, v3d_verified_sample* __restrict__ slot, uint8
         for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
         if ((threadIdx.x & 31) == 0 && v) atomicAdd(&funnel[k], (unsigned long long)v);
     }
+}
+
+// Samples per reference from the compacted slot list: slots are numbered
+// reference by reference, so a reference's samples are the run between two
+// lower bounds of the sorted list.
+__global__ void k_ref_counts(const uint32_t* __restrict__ idx, const uint32_t* __restrict__ count,
+                             uint64_t cells, uint32_t n_refs, uint32_t* __restrict__ per_ref) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n_refs) return;
+    const uint32_t n = *count;
+    auto lower = [&](uint64_t key) {
+        uint32_t lo = 0, hi = n;
+        while (lo < hi) {
+            const uint32_t mid = lo + (hi - lo) / 2;
+            if (idx[mid] < key) lo = mid + 1;
+            else hi = mid;
+        }
+        return lo;
+    };
+    per_ref[r] = lower((uint64_t)(r + 1) * cells) - lower((uint64_t)r * cells);
 }
 
 __global__ void k_gather_samples(const uint32_t* __restrict__ idx, const uint32_t* __restrict__ count,
@@ -454,10 +473,15 @@ int32_t verify_enqueue(v3d_context* ctx, char* base, const VerifyArgs& a, const 
     p.min_cos = std::cos(0.5 * (3.141592653589793 / 180.0));  // 0.5_f64.to_radians().cos()
     cudaEventRecord(first_kernel, st);
     if (a.total) {
-        V3D_COUNTED k_verify<<<grid_of(a.total), 256, 0, st>>>(p, d_slot, d_kept, d_perref, d_funnel);
+        V3D_COUNTED k_verify<<<grid_of(a.total), 256, 0, st>>>(p, d_slot, d_kept, d_funnel);
         V3D_CTX_CK(cudaGetLastError());
     }
     V3D_CTX_CK(launch_compact(d_kept, 1, a.total, d_idx, d_count, at(L.o_scratch), st));
+    if (a.n_refs) {
+        V3D_COUNTED k_ref_counts<<<(unsigned)((a.n_refs + 255) / 256), 256, 0, st>>>(d_idx, d_count, a.cells,
+                                                                                   (uint32_t)a.n_refs, d_perref);
+        V3D_CTX_CK(cudaGetLastError());
+    }
     V3D_COUNTED k_gather_samples<<<grid_of(a.total), 256, 0, st>>>(d_idx, d_count, d_slot, d_out);
     V3D_CTX_CK(cudaGetLastError());
     return V3D_OK;
