@@ -314,8 +314,24 @@ __global__ void __launch_bounds__(256, 6) k_nearest(const Member* __restrict__ m
         nearest[i] = best;
         nearest_d[i] = best_d;
     }
-    if (cand) atomicAdd(&counters[0], cand);
-    if (rejn) atomicAdd(&counters[1], rejn);
+    // one atomic per block and counter (per-thread atomics on two addresses
+    // serialise in L2)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        cand += __shfl_down_sync(0xFFFFFFFFu, cand, o);
+        rejn += __shfl_down_sync(0xFFFFFFFFu, rejn, o);
+    }
+    __shared__ unsigned long long part[2][8];
+    if ((threadIdx.x & 31) == 0) {
+        part[0][threadIdx.x >> 5] = cand;
+        part[1][threadIdx.x >> 5] = rejn;
+    }
+    __syncthreads();
+    if (threadIdx.x < 2) {
+        unsigned long long a = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) a += part[threadIdx.x][w];
+        if (a) atomicAdd(&counters[threadIdx.x], a);
+    }
 }
 
 // Mutually nearest pairs and their confidence-weighted positions
