@@ -77,3 +77,25 @@ def test_context_without_device_fails_loudly():
     with pytest.raises(dense.V3DError) as e:
         dense.Context(0)
     assert e.value.status == abi.ERR_NO_DEVICE
+
+
+def test_record_dtypes_match_the_header():
+    from v3d import types
+    dtypes = {"v3d_point": types.POINT_DTYPE, "v3d_grid_site": types.SITE_DTYPE,
+              "v3d_point_attributes": types.ATTR_DTYPE, "v3d_mesh_triangle": types.TRIANGLE_DTYPE,
+              "v3d_verified_sample": dense.VERIFIED_DTYPE,
+              "v3d_triangle_source": dense.TRIANGLE_SOURCE_DTYPE,
+              "v3d_derived_vertex_source": dense.DERIVED_VERTEX_DTYPE}
+    src = ['#include <stdio.h>', '#include "%s"' % HEADER, "int main(void){"]
+    for cname in dtypes:
+        src.append('printf("%s %%zu\\n", sizeof(%s));' % (cname, cname))
+    src.append("return 0;}")
+    with tempfile.TemporaryDirectory() as d:
+        c = os.path.join(d, "sizes.c")
+        exe = os.path.join(d, "sizes")
+        open(c, "w").write("\n".join(src))
+        subprocess.run(["gcc", "-std=c99", c, "-o", exe], check=True)
+        out = subprocess.run([exe], check=True, capture_output=True, text=True).stdout
+    sizes = dict(line.split() for line in out.strip().splitlines())
+    for cname, dt in dtypes.items():
+        assert int(sizes[cname]) == dt.itemsize, cname

@@ -521,16 +521,6 @@ __global__ void __launch_bounds__(kThreads) k_emit(Arrays in, const Dec* __restr
     }
 }
 
-struct Carve {
-    size_t off = 0;
-    template <class T>
-    size_t take(uint64_t count) {
-        const size_t at = (off + 255) & ~size_t(255);
-        off = at + sizeof(T) * std::max<uint64_t>(count, 1);
-        return at;
-    }
-};
-
 constexpr uint64_t kGlueBytes = 1 + 16 + 22 + 1;
 constexpr uint64_t kMaxPoint = 123, kMaxSite = 32, kMaxAttr = 78;  // comma included
 

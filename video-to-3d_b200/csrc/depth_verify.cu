@@ -219,22 +219,6 @@ __global__ void k_gather_samples(const uint32_t* __restrict__ idx, const uint32_
         out[k] = slot[idx[k]];
 }
 
-unsigned grid_of(uint64_t n) {
-    uint64_t b = (n + 255) / 256;
-    if (b > 148ull * 16) b = 148ull * 16;
-    return (unsigned)std::max<uint64_t>(b, 1);
-}
-
-struct Carve {
-    size_t off = 0;
-    template <class T>
-    size_t take(uint64_t count) {
-        const size_t at = (off + 255) & ~size_t(255);
-        off = at + sizeof(T) * std::max<uint64_t>(count, 1);
-        return at;
-    }
-};
-
 // ---- the export's meshing of verified samples (colmap_surface.rs:380-471) ----
 
 constexpr unsigned long long kUnused = ~0ull;  // first use of an input no triangle names

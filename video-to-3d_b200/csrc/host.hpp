@@ -49,6 +49,26 @@ int32_t surface_topology_locked(v3d_context* ctx, const v3d_mesh_triangle* trian
                                 uint64_t n, v3d_surface_topology* out, float* device_ms,
                                 uint64_t* launches);
 
+// Offsets of device buffers carved one after another from the context's
+// arena, each 256-byte aligned (at least one element each).
+struct Carve {
+    size_t off = 0;
+    template <class T>
+    size_t take(uint64_t count) {
+        const size_t at = (off + 255) & ~size_t(255);
+        off = at + sizeof(T) * (count > 1 ? count : 1);
+        return at;
+    }
+};
+
+// Blocks of 256 threads for a grid-stride loop over n items: at most 16 per
+// SM of a 148-SM B200, at least one.
+inline unsigned grid_of(uint64_t n) {
+    uint64_t b = (n + 255) / 256;
+    if (b > 148ull * 16) b = 148ull * 16;
+    return (unsigned)(b ? b : 1);
+}
+
 // Incremental SHA-256 on the host (sha256.cpp).
 struct Sha256 {
     uint32_t h[8];

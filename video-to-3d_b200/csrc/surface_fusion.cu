@@ -468,24 +468,8 @@ __global__ void k_pairs_out(const Move* __restrict__ moves, const uint32_t* __re
     }
 }
 
-unsigned grid_of(uint64_t n) {
-    uint64_t b = (n + 255) / 256;
-    if (b > 148ull * 16) b = 148ull * 16;
-    return (unsigned)std::max<uint64_t>(b, 1);
-}
-
 // A bump allocator over the context's arena, regrown (and the carve redone)
 // when a call needs more than it holds.
-struct Carve {
-    size_t off = 0;
-    template <class T>
-    size_t take(uint64_t count) {
-        const size_t at = (off + 255) & ~size_t(255);
-        off = at + sizeof(T) * std::max<uint64_t>(count, 1);
-        return at;
-    }
-};
-
 }  // namespace
 }  // namespace v3d
 

@@ -172,12 +172,6 @@ __global__ void k_topology_counts(const unsigned long long* __restrict__ size, u
     }
 }
 
-unsigned grid_of(uint64_t n) {
-    uint64_t b = (n + 255) / 256;
-    if (b > 148ull * 16) b = 148ull * 16;
-    return (unsigned)std::max<uint64_t>(b, 1);
-}
-
 }  // namespace
 }  // namespace v3d
 
