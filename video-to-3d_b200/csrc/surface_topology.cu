@@ -80,7 +80,7 @@ __global__ void k_init_parent(uint32_t* parent, uint64_t n) {
         parent[v] = (uint32_t)v;
 }
 
-// Unions over every triangle edge and the edge keys (min << bits | max, with
+// Unions over two edges of every triangle and the keys of all three (min << bits | max, with
 // `bits` enough for any vertex index, so the sort needs only 2 * bits).
 __global__ void k_unite_edges(const v3d_mesh_triangle* __restrict__ tris, uint64_t nt,
                               uint32_t* parent, unsigned long long* __restrict__ keys,
@@ -92,7 +92,7 @@ __global__ void k_unite_edges(const v3d_mesh_triangle* __restrict__ tris, uint64
             const uint32_t a = v[e], b = v[(e + 1) % 3];
             const uint32_t lo = min(a, b), hi = max(a, b);
             keys[3 * t + e] = ((unsigned long long)lo << bits) | hi;
-            unite(parent, a, b, err);
+            if (e < 2) unite(parent, a, b, err);  // two edges already join all three corners
         }
     }
 }
