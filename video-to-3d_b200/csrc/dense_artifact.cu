@@ -133,10 +133,28 @@ __device__ int cmp_dec_bin(uint32_t d, int k, uint32_t X, int c) {
     return cmp(A, B);
 }
 
-// floor(X * 2^c / 10^k) (< 2^31 for the scales used here) and whether the
-// quotient is exact.
-__device__ uint32_t floor_scaled(uint32_t X, int c, int k, bool* exact) {
+// floor(X * 2^c / 10^k) (< 2^31 for the scales used here), whether the
+// quotient is exact, and, when not, where the fraction lies against one half
+// (1 below, 2 exactly, 3 above).  The double estimate is off by less than
+// 4e-7 here (ldexp is exact, exp10 within an ulp, the product within half an
+// ulp, quotients below 1.1e9), so a fraction at least kMargin from 0, 1/2 and
+// 1 decides all three; only the rare quotients near those use the exact
+// comparisons.
+constexpr double kMargin = 1.0 / 65536.0;
+
+__device__ uint32_t floor_scaled(uint32_t X, int c, int k, bool* exact, int* half) {
     const double approx = ldexp((double)X, c) * exp10((double)-k);
+    if (approx >= 4.0e9) {  // a scale one decade too fine: saturate, the caller moves k
+        *exact = false;
+        *half = 1;
+        return 0xFFFFFFFFu;
+    }
+    const double whole = floor(approx), frac = approx - whole;
+    if (frac > kMargin && frac < 1.0 - kMargin && fabs(frac - 0.5) > kMargin) {
+        *exact = false;
+        *half = frac < 0.5 ? 1 : 3;
+        return (uint32_t)whole;
+    }
     uint32_t q = (uint32_t)approx;  // within one of the floor
     int t = cmp_dec_bin(q, k, X, c);
     for (int i = 0; i < 4 && t > 0; ++i) t = cmp_dec_bin(--q, k, X, c);
@@ -147,6 +165,11 @@ __device__ uint32_t floor_scaled(uint32_t X, int c, int k, bool* exact) {
         t = t1;
     }
     *exact = t == 0;
+    *half = 0;
+    if (!*exact) {
+        const int th = cmp_dec_bin(2u * q + 1u, k, X, c + 1);  // (2q + 1) 10^k against 2 X 2^c
+        *half = th > 0 ? 1 : (th == 0 ? 2 : 3);
+    }
     return q;
 }
 
@@ -190,22 +213,22 @@ __device__ Dec decimal_of(float f) {
     // halves at the bottom of a binade (not below the smallest normal)
     const uint32_t mv = 4u * m, mp = mv + 2u, mm = mv - ((ieee_m != 0u || ieee_e <= 1u) ? 2u : 1u);
     const int c = e2 - 2;
-    int K = (int)floor(log10((double)__uint_as_float(mag)));
-    if (cmp_dec_bin(1u, K, m, e2) > 0) --K;
-    else if (cmp_dec_bin(1u, K + 1, m, e2) <= 0) ++K;
-    const int k9 = K - 8;  // 10^8 <= v / 10^k9 < 10^9
+    // k9 such that 10^8 <= v / 10^k9 < 10^9: the estimate from log10 is
+    // corrected by the exact quotient's range
+    int k9 = (int)floor(log10((double)__uint_as_float(mag))) - 8;
     bool ev, el, eu;
-    const uint32_t qv = floor_scaled(mv, c, k9, &ev);
-    const uint32_t ql = floor_scaled(mm, c, k9, &el);
-    const uint32_t qu = floor_scaled(mp, c, k9, &eu);
+    int frac, unused;
+    uint32_t qv = floor_scaled(mv, c, k9, &ev, &frac);
+    for (int i = 0; i < 2 && (qv < 100000000u || qv >= 1000000000u); ++i) {
+        k9 += qv < 100000000u ? -1 : 1;
+        qv = floor_scaled(mv, c, k9, &ev, &frac);
+    }
+    const uint32_t ql = floor_scaled(mm, c, k9, &el, &unused);
+    const uint32_t qu = floor_scaled(mp, c, k9, &eu, &unused);
     const uint32_t lo = (el && even) ? ql : ql + 1u;
     const uint32_t hi = (eu && !even) ? qu - 1u : qu;
     // v / 10^k9 - qv: 0 exact, 1 below one half, 2 one half, 3 above
-    int frac = 0;
-    if (!ev) {
-        const int th = cmp_dec_bin(2u * qv + 1u, k9, mv, c + 1);
-        frac = th > 0 ? 1 : (th == 0 ? 2 : 3);
-    }
+    if (ev) frac = 0;
     uint32_t p = 1u;
     int s = 0;
     while (s < 9) {
