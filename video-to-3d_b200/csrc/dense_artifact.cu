@@ -439,23 +439,27 @@ __global__ void __launch_bounds__(kThreads) k_measure(Arrays in, Dec* __restrict
     if (nonfinite) atomicAdd(&summary->non_finite, (unsigned long long)nonfinite);
 }
 
-// Exclusive scan of the block totals by one block; base[b] is block b's first
-// body byte.
+// Exclusive scan of the block totals by one block, 8 consecutive totals a
+// thread; base[b] is block b's first body byte.
 __global__ void __launch_bounds__(512) k_block_bases(const unsigned long long* __restrict__ totals,
-                                                      uint64_t n, unsigned long long* __restrict__ base,
-                                                      Summary* __restrict__ summary) {
+                                                     uint64_t n, unsigned long long* __restrict__ base,
+                                                     Summary* __restrict__ summary) {
+    constexpr int kItems = 8, kTile = 512 * kItems;
     using Scan = cub::BlockScan<unsigned long long, 512>;
     __shared__ typename Scan::TempStorage scan;
     __shared__ unsigned long long carry;
     if (threadIdx.x == 0) carry = 0;
     __syncthreads();
-    for (uint64_t b0 = 0; b0 < n; b0 += 512) {
-        const uint64_t b = b0 + threadIdx.x;
-        const unsigned long long v = b < n ? totals[b] : 0ull;
-        unsigned long long ex, sum;
+    for (uint64_t b0 = 0; b0 < n; b0 += kTile) {
+        const uint64_t first = b0 + (uint64_t)threadIdx.x * kItems;
+        unsigned long long v[kItems], ex[kItems], sum;
+#pragma unroll
+        for (int k = 0; k < kItems; ++k) v[k] = first + k < n ? totals[first + k] : 0ull;
         Scan(scan).ExclusiveSum(v, ex, sum);
         const unsigned long long c = carry;
-        if (b < n) base[b] = c + ex;
+#pragma unroll
+        for (int k = 0; k < kItems; ++k)
+            if (first + k < n) base[first + k] = c + ex[k];
         __syncthreads();
         if (threadIdx.x == 0) carry = c + sum;
         __syncthreads();
