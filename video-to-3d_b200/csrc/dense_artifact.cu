@@ -142,8 +142,8 @@ __device__ int cmp_dec_bin(uint32_t d, int k, uint32_t X, int c) {
 // comparisons.
 constexpr double kMargin = 1.0 / 65536.0;
 
-__device__ uint32_t floor_scaled(uint32_t X, int c, int k, bool* exact, int* half) {
-    const double approx = ldexp((double)X, c) * exp10((double)-k);
+__device__ uint32_t floor_scaled(uint32_t X, int c, int k, double scale, bool* exact, int* half) {
+    const double approx = (double)X * scale;  // scale = 2^c 10^-k
     if (approx >= 4.0e9) {  // a scale one decade too fine: saturate, the caller moves k
         *exact = false;
         *half = 1;
@@ -213,18 +213,22 @@ __device__ Dec decimal_of(float f) {
     // halves at the bottom of a binade (not below the smallest normal)
     const uint32_t mv = 4u * m, mp = mv + 2u, mm = mv - ((ieee_m != 0u || ieee_e <= 1u) ? 2u : 1u);
     const int c = e2 - 2;
-    // k9 such that 10^8 <= v / 10^k9 < 10^9: the estimate from log10 is
-    // corrected by the exact quotient's range
-    int k9 = (int)floor(log10((double)__uint_as_float(mag))) - 8;
+    // k9 such that 10^8 <= v / 10^k9 < 10^9: floor(E log10 2) for v in
+    // [2^E, 2^(E+1)) is off by at most one, which the exact quotient's range
+    // corrects
+    const int E = e2 + 31 - __clz(m);
+    int k9 = (int)floor((double)E * 0.30102999566398120) - 8;
     bool ev, el, eu;
     int frac, unused;
-    uint32_t qv = floor_scaled(mv, c, k9, &ev, &frac);
+    double scale = ldexp(exp10((double)-k9), c);  // one scale for the value and both bounds
+    uint32_t qv = floor_scaled(mv, c, k9, scale, &ev, &frac);
     for (int i = 0; i < 2 && (qv < 100000000u || qv >= 1000000000u); ++i) {
         k9 += qv < 100000000u ? -1 : 1;
-        qv = floor_scaled(mv, c, k9, &ev, &frac);
+        scale = ldexp(exp10((double)-k9), c);
+        qv = floor_scaled(mv, c, k9, scale, &ev, &frac);
     }
-    const uint32_t ql = floor_scaled(mm, c, k9, &el, &unused);
-    const uint32_t qu = floor_scaled(mp, c, k9, &eu, &unused);
+    const uint32_t ql = floor_scaled(mm, c, k9, scale, &el, &unused);
+    const uint32_t qu = floor_scaled(mp, c, k9, scale, &eu, &unused);
     const uint32_t lo = (el && even) ? ql : ql + 1u;
     const uint32_t hi = (eu && !even) ? qu - 1u : qu;
     // v / 10^k9 - qv: 0 exact, 1 below one half, 2 one half, 3 above
