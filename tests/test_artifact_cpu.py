@@ -239,3 +239,17 @@ def test_pack_mesh_triangles_errors(case, message):
         dense.pack_mesh_triangles(tris, count, src, der)
     st, _ = Oracle().pack_mesh_triangles(tris, count, src, der)
     assert st == {"source": 1, "derived": 1, "missing": 2, "index": 3}[case]
+
+
+def test_reused_buffer_is_checked_before_any_call():
+    pts, sites, attrs = _evidence(50, 3)
+    fn = Oracle().lib.v3do_encode_dense_evidence
+    bound = dense.document_bound(50, 50, 50)
+    for bad in (np.zeros(bound - 1, np.uint8), np.zeros(bound, np.int8),
+                np.zeros((2, bound), np.uint8)[:, ::2]):
+        with pytest.raises(ValueError):
+            dense._encode(fn, (), pts, sites, attrs, b"", b"", bad)
+    buf = np.zeros(bound, np.uint8)
+    st, view, info = dense._encode(fn, (), pts, sites, attrs, b"", b"", buf)
+    assert st == 0 and isinstance(view, memoryview) and len(view) == info["document_bytes"]
+    assert bytes(view) == Oracle().encode_dense_evidence(pts, sites, attrs)[0]
