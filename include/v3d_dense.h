@@ -17,6 +17,15 @@
  *   v3d_grid_stride                         dense.rs:215-218
  *   v3d_reconstruct_dense_mesh_samples      mesh_legacy.rs:150-358
  *   v3d_reconstruct_dense_mesh_with_control mesh.rs:74-220
+ *   v3d_plan_clips                          dense.rs:165-213, 620-672 (many clips)
+ *   v3d_fuse_mutually_supported_vertices    surface_fusion.rs:369-549
+ *   v3d_verify_depth_grids                  colmap_surface.rs:175-314, 394-420
+ *   v3d_mesh_verified_depth_grids           colmap_surface.rs:380-471
+ *   v3d_surface_topology_of                 colmap_surface.rs:125-157
+ *   v3d_encode_dense_evidence               reconstruction_stages.rs:287-380
+ *   v3d_pack_dense_points, v3d_pack_mesh_triangles
+ *                                           crates/video-to-3d-wasm/src/lib.rs:227-326
+ *   v3d_sha256                              scene_project.rs:463-465
  *
  * Data contract (mirrors the Rust types bit for bit where a layout exists):
  *   FrameInput  (reconstruction/types.rs:17-21)  -> v3d_frame (RGBA8, tightly packed)
