@@ -143,3 +143,22 @@ def test_oracle_verified_surface_without_triangles_is_skipped():
     surf = Oracle().mesh_verified_depth_grids(views, [0], [[1]], 4, 4, 20.0)
     assert surf.status == 1 and len(surf.points) == 0
     assert surf.diagnostics["verification"]["depth_disagreement"] > 0
+
+
+def test_verified_surface_bounds_hold_the_oracle_outputs():
+    import ctypes as C
+    from v3d import dense
+    lib = dense.library()
+    mp, mt = C.c_uint64(), C.c_uint64()
+    lib.v3d_verified_surface_bounds(640, 360, 4, 3, C.byref(mp), C.byref(mt))
+    gw, gh = 160, 90
+    slots = 2 * (gw + 1) * (gh + 1) + (gw - 2) * gh + gw * (gh - 2)
+    assert (mp.value, mt.value) == (3 * gw * gh, 3 * slots)
+    lib.v3d_verified_surface_bounds(641, 361, 4, 1, C.byref(mp), C.byref(mt))
+    assert mp.value == 161 * 91
+    for seed, stride, rstride in [(1, 2, 2), (3, 4, 8)]:
+        views, refs, sources, focal = depth_grid_scenes.clip_views(seed, stride=stride)
+        surf = Oracle().mesh_verified_depth_grids(views, refs, sources, stride, rstride, focal)
+        h, w = views[0][0].shape[:2]
+        lib.v3d_verified_surface_bounds(w, h, rstride, len(refs), C.byref(mp), C.byref(mt))
+        assert 0 < len(surf.points) <= mp.value and 0 < len(surf.triangles) <= mt.value
