@@ -96,3 +96,20 @@ def test_large_evidence_and_a_short_buffer():
     for _ in range(2):
         view, info2 = ctx.encode_dense_evidence(pts, sites, attrs, PREFIX, SUFFIX, out=buf)
         assert view == doc and info2 == info
+
+
+@pytest.mark.gpu
+def test_encode_refuses_inconsistent_arguments():
+    pts, sites, attrs = _evidence(10, 9)
+    ctx = dense.Context(0)
+    out = abi.DenseDocument()
+    buf = np.zeros(dense.document_bound(10, 10, 10, 8, 0), dtype=np.uint8)
+    # a prefix length without a prefix, a count without its array
+    assert ctx.lib.v3d_encode_dense_evidence(
+        ctx.handle, pts.ctypes.data, 10, sites.ctypes.data, 10, attrs.ctypes.data, 10, None, 8,
+        None, 0, buf.ctypes.data, len(buf), C.byref(out)) == abi.ERR_INVALID_ARGUMENT
+    assert ctx.lib.v3d_encode_dense_evidence(
+        ctx.handle, None, 10, sites.ctypes.data, 10, attrs.ctypes.data, 10, None, 0, None, 0,
+        buf.ctypes.data, len(buf), C.byref(out)) == abi.ERR_INVALID_ARGUMENT
+    doc, _ = ctx.encode_dense_evidence(pts, sites, attrs)
+    assert doc == Oracle().encode_dense_evidence(pts, sites, attrs)[0]

@@ -200,3 +200,25 @@ def test_verified_surface_rejects_duplicate_frames():
                            sources, 2, 4, focal)
     assert st == abi.ERR_INVALID_ARGUMENT
     assert _compare_surface(views, refs, sources, 2, 4, focal).status == 0
+
+
+@pytest.mark.gpu
+def test_verified_surface_refuses_short_capacities():
+    import ctypes as C
+    from v3d import abi, types
+    views, refs, sources, focal = depth_grid_scenes.clip_views(2, stride=2)
+    ctx = dense.Context(0)
+    arr, keep, r, src = dense._depth_views(views, refs, sources)
+    pts = np.zeros(10, dtype=types.POINT_DTYPE)
+    sites = np.zeros(10, dtype=types.SITE_DTYPE)
+    tris = np.zeros(10, dtype=types.TRIANGLE_DTYPE)
+    regs = (abi.VerifiedSurfaceRegion * len(refs))()
+    out = abi.VerifiedSurface()
+    st = ctx.lib.v3d_mesh_verified_depth_grids(
+        ctx.handle, arr, len(views), r.ctypes.data, len(refs), src.ctypes.data, 2, 4, float(focal),
+        pts.ctypes.data, sites.ctypes.data, len(pts), tris.ctypes.data, len(tris), regs,
+        C.byref(out))
+    assert st == abi.ERR_INVALID_ARGUMENT
+    full = _compare_surface(views, refs, sources, 2, 4, focal)
+    # the refused call reports the sizes it needed
+    assert (out.n_points, out.n_triangles) == (len(full.points), len(full.triangles))
