@@ -206,16 +206,48 @@ struct Fused {
 };
 Fused fuse_depth_observations(Vec3 primary, const std::vector<Vec3>& reciprocal,
                               double reference_depth);
+// `gap`, when given, receives the smallest distance of a cost-based decision of
+// the call to the point where it would go the other way (see ExplainRecord).
 std::optional<double> estimate_single_view_depth(const Profile& prof, const Camera& ref_cam,
                                                  const Camera& src_cam, const Plane& ref_img,
                                                  const Plane& src_img, double x, double y,
                                                  double search_min, double search_max,
-                                                 double focal);
+                                                 double focal, double* gap = nullptr);
 std::vector<Vec3> reciprocal_depth_observations(const Profile& prof, Vec3 position,
                                                 const Camera& ref_cam, const Frame& ref_frame,
                                                 const Plane& ref_luma,
                                                 const std::vector<SourceView>& sources,
-                                                double focal);
+                                                double focal, double* gap = nullptr);
+
+// Parity diagnostic (no counterpart in the reference): for every sampled
+// primary grid site and every completion proposal of a pass, how close its
+// cost-based decisions came to going the other way.  A device policy that
+// computes window costs with a bounded error can only decide differently
+// where one of these gaps is within twice that bound, so the parity tests
+// attribute every differing output site to a gap, to a moved hypothesis or to
+// a differing neighbour.
+//  * sweep_gap: primary sites: min(|best cost - photometric gate|,
+//    |margin - ambiguity gate|), or for sites without a candidate the smallest
+//    |cost - photometric gate| of any window; completion proposals: the
+//    smallest |direct cost - photometric gate| over the sources.
+//  * recip_gap: over the reciprocal check of every source: |direct cost -
+//    photometric gate|, and in the single-view sweep the distance between the
+//    best and second-best passing costs (a near tie moves the arg-min) and
+//    |best cost - photometric gate| (or, with no passing hypothesis, the
+//    smallest |cost - photometric gate|).
+struct ExplainRecord {
+    uint32_t x, y;
+    int32_t stage;    // 0 primary sweep, 1 and 2 the completion passes
+    int32_t outcome;  // primary: sweep status 2..4, 5 reciprocal rejected, 6 fusion rejected,
+                      // 7 kept; completion: 0 kept, 1 texture, 2 cross view, 3 reciprocal,
+                      // 4 fusion, 5 footprint
+    int32_t plane;
+    int32_t support;
+    double error;   // primary: the best candidate's cost; completion: the median direct cost
+    double margin;  // primary: the ambiguity margin (infinite without a comparable second)
+    double sweep_gap;
+    double recip_gap;
+};
 struct CompletionStats {
     size_t proposals = 0, accepted = 0, rejected_texture = 0, rejected_cross_view = 0,
            rejected_reciprocal = 0, rejected_fusion = 0, rejected_footprint = 0;
@@ -232,7 +264,8 @@ CompletionStats complete_surface_samples(const Profile& prof, const Camera& ref_
                                          std::vector<Attr>& attrs, std::vector<double>& errors,
                                          std::vector<double>& supports, uint32_t width,
                                          uint32_t height, uint32_t border, size_t stride,
-                                         double focal, Control& control);
+                                         double focal, Control& control,
+                                         std::vector<ExplainRecord>* explain = nullptr);
 
 // dense_legacy.rs:149-470
 LegacyAnalysis estimate_depth_points_with_control(const Profile& prof,
@@ -250,14 +283,19 @@ struct RowBand {
 };
 
 // `sweep_records`, when given, receives the per-site sweep outcome in raster
-// order and the pass stops after the sweep (a parity diagnostic).
+// order and the pass stops after the sweep (a parity diagnostic); `explain`
+// receives the ExplainRecords of the primary sites in raster order, then of
+// each completion pass's proposals.  Sites are independent, so the grid is
+// swept by OpenMP threads and reduced in raster order; the cancellation
+// callback is polled once per grid row, in row order, before the rows run.
 LegacyAnalysis estimate_depth_points_ptr(const Profile& prof,
                                          const std::vector<const Frame*>& frames,
                                          const std::vector<Camera>& cameras,
                                          const std::vector<Vec3>& sparse, double focal,
                                          bool fine_grid, Control& control,
                                          std::vector<v3d_site_record>* sweep_records = nullptr,
-                                         const RowBand* band = nullptr);
+                                         const RowBand* band = nullptr,
+                                         std::vector<ExplainRecord>* explain = nullptr);
 
 // ---- dense.rs ----
 size_t grid_stride(uint32_t width, uint32_t height, bool fine_grid);
@@ -274,7 +312,8 @@ std::optional<LegacyAnalysis> reconstruct_reference_patch(const Profile& prof,
                                                           const std::vector<Vec3>& sparse,
                                                           double focal, size_t camera_index,
                                                           bool fine_grid, Control& control,
-                                                          const RowBand* band = nullptr);
+                                                          const RowBand* band = nullptr,
+                                                          std::vector<ExplainRecord>* explain = nullptr);
 AttemptStats reference_attempt_stats(size_t reference_frame, const LegacyStats& stats,
                                      size_t accepted_points, bool accepted);
 std::vector<AttemptStats> merge_fallback_attempts(std::vector<AttemptStats> attempts,
@@ -286,6 +325,34 @@ std::pair<DenseAnalysis, bool> estimate_depth_points_limited(const Profile& prof
                                                              const std::vector<Vec3>& sparse,
                                                              double focal, size_t reference_views,
                                                              bool fine_grid, Control& control);
+
+// ---- the working-set budget (dense.rs:15-28, 354-605) ----
+struct WorkingSet {  // DenseWorkingSetEstimate
+    uint64_t frame_bytes = 0, retry_frame_bytes = 0, remapped_frame_bytes = 0,
+             luminance_bytes = 0, sparse_pipeline_bytes = 0, dense_sample_bytes = 0,
+             topology_bytes = 0, mesh_builder_bytes = 0, surface_fusion_bytes = 0,
+             retained_candidate_bytes = 0, packed_output_bytes = 0, total_bytes = 0;
+};
+// estimate_working_set (dense.rs:423-605); a frame's bytes are its storage as
+// handed in (the reference's RGBA frames: width x height x 4).
+WorkingSet estimate_working_set(const std::vector<Frame>& frames, uint64_t max_features,
+                                uint32_t descriptor_radius, uint64_t reference_views,
+                                bool fine_grid);
+struct BudgetedAnalysis {
+    DenseAnalysis analysis;
+    WorkingSet estimate;          // stats.working_set_estimate
+    uint64_t budget_bytes = 0;    // stats.working_set_budget_bytes
+    uint64_t full_bytes = 0;      // stats.full_working_set_bytes
+    bool fine_grid = false;       // the plan that ran
+    uint64_t reference_views = 0; // 0: the budget skip
+};
+// estimate_depth_points_with_budget_and_control (dense.rs:355-420)
+BudgetedAnalysis estimate_depth_points_with_budget(const Profile& prof,
+                                                   const std::vector<Frame>& frames,
+                                                   const std::vector<Camera>& cameras,
+                                                   const std::vector<Vec3>& sparse, double focal,
+                                                   uint64_t budget, uint64_t max_features,
+                                                   uint32_t descriptor_radius, Control& control);
 
 // ---- mesh_legacy.rs / mesh.rs ----
 struct MeshTriangle {

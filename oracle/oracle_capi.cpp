@@ -483,4 +483,101 @@ int32_t v3do_debug_sweep(const v3d_frame* frames, uint64_t n_frames, const v3d_c
     return V3D_OK;
 }
 
+// The remapped pass of one reference camera (as v3do_reconstruct_reference_patches
+// runs it), or with camera_index == UINT64_MAX the legacy single call (as
+// v3do_estimate_depth_points_with_control runs it), together with its
+// ExplainRecords (oracle.hpp): primary sites in raster order, then each
+// completion pass's proposals.  *records is malloc'd; free it with v3do_free.
+// Returns V3D_SKIPPED (and no result) where the pass does not run.
+int32_t v3do_explain_reference_patch(const v3d_frame* frames, uint64_t n_frames,
+                                     const v3d_camera* cams, uint64_t n_cams,
+                                     const double* sparse, uint64_t n_sparse, double focal,
+                                     int32_t fine_grid, const v3d_profile* profile,
+                                     uint64_t camera_index, v3d_dense_result* out,
+                                     ExplainRecord** records, uint64_t* n_records) {
+    static_assert(sizeof(ExplainRecord) == 56, "ExplainRecord layout");
+    *records = nullptr;
+    *n_records = 0;
+    std::memset(out, 0, sizeof(*out));
+    auto f = load_frames(frames, n_frames);
+    auto c = load_cameras(cams, n_cams);
+    auto s = load_sparse(sparse, n_sparse);
+    Control ctl;
+    std::vector<ExplainRecord> rec;
+    try {
+        std::optional<LegacyAnalysis> a;
+        if (camera_index == UINT64_MAX) {
+            std::vector<const Frame*> ptrs;
+            for (const Frame& x : f) ptrs.push_back(&x);
+            a = estimate_depth_points_ptr(Profile::from_c(*profile), ptrs, c, s, focal,
+                                          fine_grid != 0, ctl, nullptr, nullptr, &rec);
+            if (!a->stats.attempted) return V3D_SKIPPED;
+        } else {
+            a = reconstruct_reference_patch(Profile::from_c(*profile), f, c, s, focal,
+                                            camera_index, fine_grid != 0, ctl, nullptr, &rec);
+        }
+        if (!a) return V3D_SKIPPED;
+        fill_legacy(out, *a);
+    } catch (const std::invalid_argument&) {
+        return V3D_ERR_INVALID_ARGUMENT;
+    }
+    *records = dup(rec);
+    *n_records = rec.size();
+    return V3D_OK;
+}
+
+void v3do_free(void* p) { std::free(p); }
+
+// estimate_working_set (dense.rs:423-605), twelve u64 fields in
+// DenseWorkingSetEstimate order.
+int32_t v3do_estimate_working_set(const v3d_frame* frames, uint64_t n_frames,
+                                  uint64_t max_features, uint32_t descriptor_radius,
+                                  uint64_t reference_views, int32_t fine_grid, uint64_t* out) {
+    auto f = load_frames(frames, n_frames);
+    WorkingSet w = estimate_working_set(f, max_features, descriptor_radius, reference_views,
+                                        fine_grid != 0);
+    const uint64_t v[12] = {w.frame_bytes, w.retry_frame_bytes, w.remapped_frame_bytes,
+                            w.luminance_bytes, w.sparse_pipeline_bytes, w.dense_sample_bytes,
+                            w.topology_bytes, w.mesh_builder_bytes, w.surface_fusion_bytes,
+                            w.retained_candidate_bytes, w.packed_output_bytes, w.total_bytes};
+    std::memcpy(out, v, sizeof(v));
+    return V3D_OK;
+}
+
+// estimate_depth_points_with_budget_and_control (dense.rs:355-420): the result,
+// and in plan[0..16) the estimate (12 fields), the budget, the full plan's
+// bytes, the fine-grid flag and the plan's reference views (0: budget skip).
+int32_t v3do_estimate_depth_points_with_budget(const v3d_frame* frames, uint64_t n_frames,
+                                               const v3d_camera* cams, uint64_t n_cams,
+                                               const double* sparse, uint64_t n_sparse,
+                                               double focal, uint64_t budget,
+                                               uint64_t max_features, uint32_t descriptor_radius,
+                                               const v3d_profile* profile, v3d_cancel_fn cancel,
+                                               void* user, v3d_dense_result* out,
+                                               uint64_t* plan) {
+    try {
+        auto f = load_frames(frames, n_frames);
+        auto c = load_cameras(cams, n_cams);
+        auto s = load_sparse(sparse, n_sparse);
+        Control ctl = make_control(cancel, user);
+        BudgetedAnalysis b = estimate_depth_points_with_budget(
+            Profile::from_c(*profile), f, c, s, focal, budget, max_features, descriptor_radius,
+            ctl);
+        const WorkingSet& w = b.estimate;
+        const uint64_t v[16] = {w.frame_bytes, w.retry_frame_bytes, w.remapped_frame_bytes,
+                                w.luminance_bytes, w.sparse_pipeline_bytes, w.dense_sample_bytes,
+                                w.topology_bytes, w.mesh_builder_bytes, w.surface_fusion_bytes,
+                                w.retained_candidate_bytes, w.packed_output_bytes, w.total_bytes,
+                                b.budget_bytes, b.full_bytes, b.fine_grid ? 1u : 0u,
+                                b.reference_views};
+        std::memcpy(plan, v, sizeof(v));
+        fill_dense(out, b.analysis);
+        if (b.reference_views == 0) out->stats.skip_code = V3D_SKIP_WORKING_SET_BUDGET;
+        return b.analysis.stats.attempted ? V3D_OK : V3D_SKIPPED;
+    } catch (const std::invalid_argument&) {
+        std::memset(out, 0, sizeof(*out));
+        return V3D_ERR_INVALID_ARGUMENT;
+    }
+}
+
 }  // extern "C"

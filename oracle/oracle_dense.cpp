@@ -382,23 +382,33 @@ std::optional<double> estimate_single_view_depth(const Profile& prof, const Came
                                                  const Camera& src_cam, const Plane& ref_img,
                                                  const Plane& src_img, double x, double y,
                                                  double search_min, double search_max,
-                                                 double focal) {
+                                                 double focal, double* gap) {
     // dense_legacy.rs:887-949: ref_cam/ref_img are the source view being checked.
     if (patch_contrast(ref_img, x, y, prof.patch_radius) < prof.min_reference_contrast)
         return std::nullopt;
     bool have = false;
     double best_depth = 0, best_error = 0;
+    double second = kInf, nearest = kInf;  // decision gaps (ExplainRecord)
     for (int k = 0; k < prof.depth_hypotheses; ++k) {
         double depth = hypothesis_depth(k, prof.depth_hypotheses, search_min, search_max);
         auto e = patch_error(prof, ref_cam, src_cam, ref_img, src_img, x, y, depth, focal);
-        if (!e || !(*e <= prof.max_photometric_error)) continue;
+        if (!e) continue;
+        nearest = std::fmin(nearest, std::fabs(*e - prof.max_photometric_error));
+        if (!(*e <= prof.max_photometric_error)) continue;
         // sort by (error asc, depth asc), take the first
         if (!have || *e < best_error || (*e == best_error && depth < best_depth)) {
+            if (have) second = std::fmin(second, best_error);
             have = true;
             best_error = *e;
             best_depth = depth;
+        } else {
+            second = std::fmin(second, *e);
         }
     }
+    if (gap)
+        *gap = have ? std::fmin(second - best_error,
+                                std::fabs(best_error - prof.max_photometric_error))
+                    : nearest;
     if (!have) return std::nullopt;
     return best_depth;
 }
@@ -407,26 +417,33 @@ std::vector<Vec3> reciprocal_depth_observations(const Profile& prof, Vec3 positi
                                                 const Camera& ref_cam, const Frame& ref_frame,
                                                 const Plane& ref_luma,
                                                 const std::vector<SourceView>& sources,
-                                                double focal) {
+                                                double focal, double* gap) {
     // dense_legacy.rs:777-857
     std::vector<Vec3> out;
+    double g = kInf;
     auto rp = project(ref_cam, position, ref_frame.width, ref_frame.height, focal);
-    if (!rp) return out;
-    for (const SourceView& s : sources) {
-        auto direct = patch_error(prof, ref_cam, *s.camera, ref_luma, s.luma, rp->x, rp->y, rp->z,
-                                  focal);
-        if (!direct) continue;
-        if (*direct > prof.max_photometric_error) continue;
-        auto sp = project(*s.camera, position, s.frame->width, s.frame->height, focal);
-        if (!sp) continue;
-        auto rd = estimate_single_view_depth(prof, *s.camera, ref_cam, s.luma, ref_luma, sp->x,
-                                             sp->y, s.search_min_depth, s.search_max_depth,
-                                             focal);
-        if (!rd) continue;
-        if (!reciprocal_depth_agrees(sp->z, *rd)) continue;
-        Vec3 pos = unproject(*s.camera, sp->x, sp->y, *rd, s.frame->width, s.frame->height, focal);
-        if (finite3(pos)) out.push_back(pos);
+    if (rp) {
+        for (const SourceView& s : sources) {
+            auto direct = patch_error(prof, ref_cam, *s.camera, ref_luma, s.luma, rp->x, rp->y,
+                                      rp->z, focal);
+            if (!direct) continue;
+            g = std::fmin(g, std::fabs(*direct - prof.max_photometric_error));
+            if (*direct > prof.max_photometric_error) continue;
+            auto sp = project(*s.camera, position, s.frame->width, s.frame->height, focal);
+            if (!sp) continue;
+            double sg = kInf;
+            auto rd = estimate_single_view_depth(prof, *s.camera, ref_cam, s.luma, ref_luma,
+                                                 sp->x, sp->y, s.search_min_depth,
+                                                 s.search_max_depth, focal, gap ? &sg : nullptr);
+            g = std::fmin(g, sg);
+            if (!rd) continue;
+            if (!reciprocal_depth_agrees(sp->z, *rd)) continue;
+            Vec3 pos =
+                unproject(*s.camera, sp->x, sp->y, *rd, s.frame->width, s.frame->height, focal);
+            if (finite3(pos)) out.push_back(pos);
+        }
     }
+    if (gap) *gap = g;
     return out;
 }
 
@@ -438,12 +455,29 @@ CompletionStats complete_surface_samples(const Profile& prof, const Camera& ref_
                                          std::vector<Attr>& attrs, std::vector<double>& errors,
                                          std::vector<double>& supports, uint32_t width,
                                          uint32_t height, uint32_t border, size_t stride,
-                                         double focal, Control& control) {
+                                         double focal, Control& control,
+                                         std::vector<ExplainRecord>* explain) {
     // dense_legacy.rs:519-737
     CompletionStats stats;
     if (stride == 0 || sources.empty()) return stats;
     const double S = static_cast<double>(sources.size());
     const int64_t st = static_cast<int64_t>(stride);
+    struct Addition {
+        Point3 p;
+        GridSite s;
+        Attr a;
+        double error, support;
+    };
+    // kind: -1 no proposal, 0 kept, 1 texture, 2 cross view, 3 reciprocal, 4 fusion,
+    // 5 footprint (the order of the rejection counters)
+    struct Outcome {
+        int kind = -1;
+        int support = 0;
+        double sweep_gap = kInf, recip_gap = kInf;
+        Addition add{};
+    };
+    std::vector<uint32_t> cols;
+    for (uint32_t x = border; x < width - border; x += stride) cols.push_back(x);
     for (size_t pass = 0; pass < kSurfaceCompletionPasses; ++pass) {
         // occupied: BTreeMap<(x,y), index>; later entries overwrite earlier ones.
         // A dense lookup over the pixel raster is equivalent.
@@ -456,108 +490,134 @@ CompletionStats complete_surface_samples(const Profile& prof, const Camera& ref_
             if (x < 0 || y < 0 || x >= width || y >= height) return -1;
             return occ[static_cast<size_t>(y) * width + x];
         };
-        struct Addition {
-            Point3 p;
-            GridSite s;
-            Attr a;
-            double error, support;
-        };
-        std::vector<Addition> additions;
+        // The reference polls once per row before its sites (dense_legacy.rs:551)
+        // and a cancel returns the counters of the rows before it; the rows are
+        // polled here in order first, and only those rows run.
+        std::vector<uint32_t> rows;
+        bool canceled = false;
         for (uint32_t y = border; y < height - border; y += stride) {
-            if (control.is_canceled()) return stats;
-            for (uint32_t x = border; x < width - border; x += stride) {
-                if (lookup(x, y) >= 0) continue;
-                std::vector<double> nd, nc, nm;
-                for (int64_t oy = -1; oy <= 1; ++oy)
-                    for (int64_t ox = -1; ox <= 1; ++ox) {
-                        if (ox == 0 && oy == 0) continue;
-                        int64_t nx = static_cast<int64_t>(x) + ox * st;
-                        int64_t ny = static_cast<int64_t>(y) + oy * st;
-                        if (nx < 0 || ny < 0) continue;
-                        int64_t pi = lookup(nx, ny);
-                        if (pi < 0 || static_cast<size_t>(pi) >= points.size()) continue;
-                        const Point3& pt = points[pi];
-                        Vec3 pos{static_cast<double>(pt.x), static_cast<double>(pt.y),
-                                 static_cast<double>(pt.z)};
-                        auto pr = project(ref_cam, pos, width, height, focal);
-                        if (!pr) continue;
-                        nd.push_back(pr->z);
-                        nc.push_back(static_cast<double>(pt.confidence));
-                        nm.push_back(static_cast<size_t>(pi) < attrs.size()
-                                         ? static_cast<double>(attrs[pi].depth_margin)
-                                         : 0.0);
-                    }
-                auto predicted = surface_depth_prediction(nd);
-                if (!predicted) continue;
-                stats.proposals++;
-                if (patch_contrast(ref_luma, x, y, prof.patch_radius) <
-                    prof.min_reference_contrast) {
-                    stats.rejected_texture++;
-                    continue;
-                }
-                Vec3 ppos = unproject(ref_cam, x, y, *predicted, width, height, focal);
-                std::vector<double> de;
-                for (const SourceView& s : sources) {
-                    auto e = patch_error(prof, ref_cam, *s.camera, ref_luma, s.luma, x, y,
-                                         *predicted, focal);
-                    if (!e) continue;
-                    if (*e <= prof.max_photometric_error) de.push_back(*e);
-                }
-                if (de.empty()) {
-                    stats.rejected_cross_view++;
-                    continue;
-                }
-                sort_f64(de);
-                double direct_error = quantile(de, 0.5);
-                auto recip = reciprocal_depth_observations(prof, ppos, ref_cam, ref_frame,
-                                                           ref_luma, sources, focal);
-                if (recip.empty()) {
-                    stats.rejected_reciprocal++;
-                    continue;
-                }
-                Fused fused = fuse_depth_observations(ppos, recip, *predicted);
-                if (fused.observations < kMinFusionObservations) {
-                    stats.rejected_fusion++;
-                    continue;
-                }
-                auto fp = project(ref_cam, fused.position, width, height, focal);
-                if (!fp) {
-                    stats.rejected_footprint++;
-                    continue;
-                }
-                double limit = static_cast<double>(stride) * 0.5;
-                if (std::fabs(fp->x - x) >= limit || std::fabs(fp->y - y) >= limit) {
-                    stats.rejected_footprint++;
-                    continue;
-                }
-                double csum = 0.0;
-                for (double c : nc) csum += c;
-                double neighbor_confidence = csum / static_cast<double>(nc.size());
-                double support_confidence = static_cast<double>(de.size()) / S;
-                double reciprocal_confidence =
-                    clampd(static_cast<double>(fused.observations - 1) / S, 0.0, 1.0);
-                double error_confidence = 1.0 / (1.0 + direct_error / prof.error_confidence_scale);
-                float confidence = static_cast<float>(
-                    clampd(neighbor_confidence * support_confidence * reciprocal_confidence *
-                               error_confidence * kSurfaceCompletionConfidenceScale,
-                           0.05, 0.9));
-                double msum = 0.0;
-                for (double m : nm) msum += m;
-                double depth_margin = msum / static_cast<double>(nm.size());
-                Addition add_;
-                sample_rgb(ref_frame, x, y, add_.p.r, add_.p.g, add_.p.b);
-                add_.p.x = static_cast<float>(fused.position.x);
-                add_.p.y = static_cast<float>(fused.position.y);
-                add_.p.z = static_cast<float>(fused.position.z);
-                add_.p.confidence = confidence;
-                add_.s = {x, y};
-                add_.a.reciprocal_consistency = static_cast<float>(reciprocal_confidence);
-                add_.a.depth_margin = static_cast<float>(clampd(depth_margin, 0.0, 1.0));
-                add_.error = direct_error;
-                add_.support = static_cast<double>(de.size());
-                additions.push_back(add_);
+            if (control.is_canceled()) {
+                canceled = true;
+                break;
             }
+            rows.push_back(y);
         }
+        const size_t nsites = rows.size() * cols.size();
+        std::vector<Outcome> outs(nsites);
+        // every proposal reads only the state before the pass
+#pragma omp parallel for schedule(dynamic, 16)
+        for (int64_t i = 0; i < static_cast<int64_t>(nsites); ++i) {
+            const uint32_t y = rows[i / cols.size()], x = cols[i % cols.size()];
+            Outcome& o = outs[i];
+            if (lookup(x, y) >= 0) continue;
+            std::vector<double> nd, nc, nm;
+            for (int64_t oy = -1; oy <= 1; ++oy)
+                for (int64_t ox = -1; ox <= 1; ++ox) {
+                    if (ox == 0 && oy == 0) continue;
+                    int64_t nx = static_cast<int64_t>(x) + ox * st;
+                    int64_t ny = static_cast<int64_t>(y) + oy * st;
+                    if (nx < 0 || ny < 0) continue;
+                    int64_t pi = lookup(nx, ny);
+                    if (pi < 0 || static_cast<size_t>(pi) >= points.size()) continue;
+                    const Point3& pt = points[pi];
+                    Vec3 pos{static_cast<double>(pt.x), static_cast<double>(pt.y),
+                             static_cast<double>(pt.z)};
+                    auto pr = project(ref_cam, pos, width, height, focal);
+                    if (!pr) continue;
+                    nd.push_back(pr->z);
+                    nc.push_back(static_cast<double>(pt.confidence));
+                    nm.push_back(static_cast<size_t>(pi) < attrs.size()
+                                     ? static_cast<double>(attrs[pi].depth_margin)
+                                     : 0.0);
+                }
+            auto predicted = surface_depth_prediction(nd);
+            if (!predicted) continue;
+            if (patch_contrast(ref_luma, x, y, prof.patch_radius) < prof.min_reference_contrast) {
+                o.kind = 1;
+                continue;
+            }
+            Vec3 ppos = unproject(ref_cam, x, y, *predicted, width, height, focal);
+            std::vector<double> de;
+            for (const SourceView& s : sources) {
+                auto e = patch_error(prof, ref_cam, *s.camera, ref_luma, s.luma, x, y,
+                                     *predicted, focal);
+                if (!e) continue;
+                o.sweep_gap = std::fmin(o.sweep_gap, std::fabs(*e - prof.max_photometric_error));
+                if (*e <= prof.max_photometric_error) de.push_back(*e);
+            }
+            o.support = static_cast<int>(de.size());
+            if (de.empty()) {
+                o.kind = 2;
+                continue;
+            }
+            sort_f64(de);
+            double direct_error = quantile(de, 0.5);
+            auto recip = reciprocal_depth_observations(prof, ppos, ref_cam, ref_frame, ref_luma,
+                                                       sources, focal,
+                                                       explain ? &o.recip_gap : nullptr);
+            if (recip.empty()) {
+                o.kind = 3;
+                continue;
+            }
+            Fused fused = fuse_depth_observations(ppos, recip, *predicted);
+            if (fused.observations < kMinFusionObservations) {
+                o.kind = 4;
+                continue;
+            }
+            auto fp = project(ref_cam, fused.position, width, height, focal);
+            double limit = static_cast<double>(stride) * 0.5;
+            if (!fp || std::fabs(fp->x - x) >= limit || std::fabs(fp->y - y) >= limit) {
+                o.kind = 5;
+                continue;
+            }
+            double csum = 0.0;
+            for (double c : nc) csum += c;
+            double neighbor_confidence = csum / static_cast<double>(nc.size());
+            double support_confidence = static_cast<double>(de.size()) / S;
+            double reciprocal_confidence =
+                clampd(static_cast<double>(fused.observations - 1) / S, 0.0, 1.0);
+            double error_confidence = 1.0 / (1.0 + direct_error / prof.error_confidence_scale);
+            float confidence = static_cast<float>(
+                clampd(neighbor_confidence * support_confidence * reciprocal_confidence *
+                           error_confidence * kSurfaceCompletionConfidenceScale,
+                       0.05, 0.9));
+            double msum = 0.0;
+            for (double m : nm) msum += m;
+            double depth_margin = msum / static_cast<double>(nm.size());
+            Addition& add_ = o.add;
+            sample_rgb(ref_frame, x, y, add_.p.r, add_.p.g, add_.p.b);
+            add_.p.x = static_cast<float>(fused.position.x);
+            add_.p.y = static_cast<float>(fused.position.y);
+            add_.p.z = static_cast<float>(fused.position.z);
+            add_.p.confidence = confidence;
+            add_.s = {x, y};
+            add_.a.reciprocal_consistency = static_cast<float>(reciprocal_confidence);
+            add_.a.depth_margin = static_cast<float>(clampd(depth_margin, 0.0, 1.0));
+            add_.error = direct_error;
+            add_.support = static_cast<double>(de.size());
+            o.kind = 0;
+        }
+        // the counters and additions in raster order
+        std::vector<Addition> additions;
+        for (size_t i = 0; i < nsites; ++i) {
+            const Outcome& o = outs[i];
+            if (o.kind < 0) continue;
+            stats.proposals++;
+            switch (o.kind) {
+                case 0: additions.push_back(o.add); break;
+                case 1: stats.rejected_texture++; break;
+                case 2: stats.rejected_cross_view++; break;
+                case 3: stats.rejected_reciprocal++; break;
+                case 4: stats.rejected_fusion++; break;
+                default: stats.rejected_footprint++; break;
+            }
+            if (explain)
+                explain->push_back({cols[i % cols.size()], rows[i / cols.size()],
+                                    static_cast<int32_t>(pass + 1), o.kind, -1, o.support,
+                                    o.kind == 0 ? o.add.error : 0.0, 0.0, o.sweep_gap,
+                                    o.recip_gap});
+        }
+        if (canceled) return stats;
         if (additions.empty()) break;
         stats.accepted += additions.size();
         for (const Addition& a : additions) {
@@ -600,7 +660,8 @@ LegacyAnalysis estimate_depth_points_ptr(const Profile& prof,
                                          const std::vector<Vec3>& sparse, double focal,
                                          bool fine_grid, Control& control,
                                          std::vector<v3d_site_record>* sweep_records,
-                                         const RowBand* band) {
+                                         const RowBand* band,
+                                         std::vector<ExplainRecord>* explain) {
     // dense_legacy.rs:149-470
     if (frames.empty()) return skipped(V3D_SKIP_NO_FRAMES, "no sampled frames are available");
     if (cameras.size() < 2)
@@ -705,8 +766,6 @@ LegacyAnalysis estimate_depth_points_ptr(const Profile& prof,
     std::vector<double> errors, supports, fusion_counts;
     size_t sampled = 0, rchecked = 0, rrejected = 0, rconsistent = 0, finput = 0, frejobs = 0,
            frejpts = 0;
-    std::vector<Candidate> cands;
-    std::vector<double> source_errors;
     auto record = [&](uint32_t x, uint32_t y, int status, const Candidate* c, double margin) {
         if (!sweep_records) return;
         v3d_site_record r{};
@@ -719,18 +778,46 @@ LegacyAnalysis estimate_depth_points_ptr(const Profile& prof,
         r.margin = c ? margin : 0.0;
         sweep_records->push_back(r);
     };
-    uint32_t row = 0;
-    for (uint32_t y = border; y < height - border; y += stride, ++row) {
-        if (band && (row < band->begin || row >= band->end)) continue;
-        if (control.is_canceled()) return skipped(V3D_SKIP_CANCELED, "dense reconstruction canceled");
-        for (uint32_t x = border; x < width - border; x += stride) {
-            if (band) band->units += static_cast<uint64_t>(prof.depth_hypotheses) * sources.size();
-            if (patch_contrast(ref_luma, x, y, prof.patch_radius) < prof.min_reference_contrast) {
-                record(x, y, 1, nullptr, 0.0);
+    // The reference polls once per grid row before its sites (dense_legacy.rs:273)
+    // and a cancel discards the pass; the rows are polled here in order first.
+    std::vector<uint32_t> rows, cols;
+    {
+        uint32_t row = 0;
+        for (uint32_t y = border; y < height - border; y += stride, ++row) {
+            if (band && (row < band->begin || row >= band->end)) continue;
+            if (control.is_canceled())
+                return skipped(V3D_SKIP_CANCELED, "dense reconstruction canceled");
+            rows.push_back(y);
+        }
+        for (uint32_t x = border; x < width - border; x += stride) cols.push_back(x);
+    }
+    const size_t nsites = rows.size() * cols.size();
+    if (band)
+        band->units += static_cast<uint64_t>(nsites) * prof.depth_hypotheses * sources.size();
+    // Each site's sweep, reciprocal check and fusion depend only on the inputs,
+    // so the sites run in parallel; the counters, records and points are then
+    // reduced in raster order.
+    struct SiteOutcome {
+        int status = 1;  // 1 low contrast, 2 no candidate, 3 gate rejected, 4 accepted
+        Candidate best{};
+        double margin = 0.0;
+        double sweep_gap = kInf, recip_gap = kInf;
+        size_t n_recip = 0;
+        Fused fused{};
+    };
+    std::vector<SiteOutcome> outs(nsites);
+#pragma omp parallel
+    {
+        std::vector<Candidate> cands;
+        std::vector<double> source_errors;
+#pragma omp for schedule(dynamic, 8)
+        for (int64_t i = 0; i < static_cast<int64_t>(nsites); ++i) {
+            const uint32_t y = rows[i / cols.size()], x = cols[i % cols.size()];
+            SiteOutcome& o = outs[i];
+            if (patch_contrast(ref_luma, x, y, prof.patch_radius) < prof.min_reference_contrast)
                 continue;
-            }
-            ++sampled;
             cands.clear();
+            double nearest = kInf;
             for (int k = 0; k < prof.depth_hypotheses; ++k) {
                 double depth = hypothesis_depth(k, prof.depth_hypotheses, search_min, search_max);
                 Vec3 position = unproject(*reference, x, y, depth, width, height, focal);
@@ -739,78 +826,122 @@ LegacyAnalysis estimate_depth_points_ptr(const Profile& prof,
                     auto e = patch_error(prof, *reference, *s.camera, ref_luma, s.luma, x, y,
                                          depth, focal);
                     if (!e) continue;
+                    nearest = std::fmin(nearest, std::fabs(*e - prof.max_photometric_error));
                     if (*e <= prof.max_photometric_error) source_errors.push_back(*e);
                 }
                 if (source_errors.empty()) continue;
                 sort_f64(source_errors);
-                cands.push_back({depth, position, source_errors.size(), quantile(source_errors, 0.5), k});
+                cands.push_back({depth, position, source_errors.size(),
+                                 quantile(source_errors, 0.5), k});
             }
-            std::stable_sort(cands.begin(), cands.end(), [](const Candidate& a, const Candidate& b) {
-                if (a.support != b.support) return a.support > b.support;
-                if (a.error != b.error) return a.error < b.error;
-                return a.depth < b.depth;
-            });
+            std::stable_sort(cands.begin(), cands.end(),
+                             [](const Candidate& a, const Candidate& b) {
+                                 if (a.support != b.support) return a.support > b.support;
+                                 if (a.error != b.error) return a.error < b.error;
+                                 return a.depth < b.depth;
+                             });
             if (cands.empty()) {
-                record(x, y, 2, nullptr, 0.0);
+                o.status = 2;
+                o.sweep_gap = nearest;
                 continue;
             }
-            const Candidate best = cands[0];
+            o.best = cands[0];
             double margin = kInf;
-            for (size_t i = 1; i < cands.size(); ++i)
-                if (cands[i].support == best.support) {
-                    margin = cands[i].error - best.error;
+            for (size_t j = 1; j < cands.size(); ++j)
+                if (cands[j].support == o.best.support) {
+                    margin = cands[j].error - o.best.error;
                     break;
                 }
-            if (best.error > prof.max_photometric_error || margin < prof.min_ambiguity_margin) {
-                record(x, y, 3, &best, margin);
+            o.margin = margin;
+            o.sweep_gap = std::fmin(std::fabs(o.best.error - prof.max_photometric_error),
+                                    std::fabs(margin - prof.min_ambiguity_margin));
+            if (o.best.error > prof.max_photometric_error || margin < prof.min_ambiguity_margin) {
+                o.status = 3;
                 continue;
             }
-            record(x, y, 4, &best, margin);
+            o.status = 4;
             if (sweep_records) continue;
-            ++rchecked;
-            auto recip = reciprocal_depth_observations(prof, best.position, *reference, ref_frame,
-                                                       ref_luma, sources, focal);
-            if (recip.empty()) {
-                ++rrejected;
-                continue;
-            }
-            ++rconsistent;
-            finput += 1 + recip.size();
-            Fused fused = fuse_depth_observations(best.position, recip, best.depth);
-            frejobs += fused.rejected_observations;
-            if (fused.observations < kMinFusionObservations) {
-                ++frejpts;
-                continue;
-            }
-            fusion_counts.push_back(static_cast<double>(fused.observations));
-            double support_confidence = static_cast<double>(best.support) / S;
-            double reciprocal_confidence =
-                clampd(static_cast<double>(fused.observations - 1) / S, 0.0, 1.0);
-            double error_confidence = 1.0 / (1.0 + best.error / prof.error_confidence_scale);
-            double depth_margin = depth_margin_score(margin, prof.depth_margin_saturation);
-            double margin_confidence = std::fmax(depth_margin, 0.2);
-            float confidence = static_cast<float>(clampd(
-                support_confidence * reciprocal_confidence * error_confidence * margin_confidence,
-                0.05, 1.0));
-            Point3 p;
-            sample_rgb(ref_frame, x, y, p.r, p.g, p.b);
-            p.x = static_cast<float>(fused.position.x);
-            p.y = static_cast<float>(fused.position.y);
-            p.z = static_cast<float>(fused.position.z);
-            p.confidence = confidence;
-            out.points.push_back(p);
-            out.grid_sites.push_back({x, y});
-            out.point_attributes.push_back({static_cast<float>(reciprocal_confidence),
-                                            static_cast<float>(depth_margin)});
-            errors.push_back(best.error);
-            supports.push_back(static_cast<double>(best.support));
+            auto recip = reciprocal_depth_observations(prof, o.best.position, *reference,
+                                                       ref_frame, ref_luma, sources, focal,
+                                                       explain ? &o.recip_gap : nullptr);
+            o.n_recip = recip.size();
+            if (!recip.empty()) o.fused = fuse_depth_observations(o.best.position, recip, o.best.depth);
         }
+    }
+    auto note = [&](uint32_t x, uint32_t y, int outcome, const SiteOutcome& o) {
+        if (!explain) return;
+        const bool c = o.status >= 3;
+        explain->push_back({x, y, 0, outcome, c ? o.best.plane : -1,
+                            c ? static_cast<int32_t>(o.best.support) : 0, c ? o.best.error : 0.0,
+                            c ? o.margin : 0.0, o.sweep_gap, o.recip_gap});
+    };
+    for (size_t i = 0; i < nsites; ++i) {
+        const uint32_t y = rows[i / cols.size()], x = cols[i % cols.size()];
+        const SiteOutcome& o = outs[i];
+        if (o.status == 1) {
+            record(x, y, 1, nullptr, 0.0);
+            continue;
+        }
+        ++sampled;
+        if (o.status == 2) {
+            record(x, y, 2, nullptr, 0.0);
+            note(x, y, 2, o);
+            continue;
+        }
+        const Candidate& best = o.best;
+        const double margin = o.margin;
+        if (o.status == 3) {
+            record(x, y, 3, &best, margin);
+            note(x, y, 3, o);
+            continue;
+        }
+        record(x, y, 4, &best, margin);
+        if (sweep_records) continue;
+        ++rchecked;
+        if (o.n_recip == 0) {
+            ++rrejected;
+            note(x, y, 5, o);
+            continue;
+        }
+        ++rconsistent;
+        finput += 1 + o.n_recip;
+        const Fused& fused = o.fused;
+        frejobs += fused.rejected_observations;
+        if (fused.observations < kMinFusionObservations) {
+            ++frejpts;
+            note(x, y, 6, o);
+            continue;
+        }
+        note(x, y, 7, o);
+        fusion_counts.push_back(static_cast<double>(fused.observations));
+        double support_confidence = static_cast<double>(best.support) / S;
+        double reciprocal_confidence =
+            clampd(static_cast<double>(fused.observations - 1) / S, 0.0, 1.0);
+        double error_confidence = 1.0 / (1.0 + best.error / prof.error_confidence_scale);
+        double depth_margin = depth_margin_score(margin, prof.depth_margin_saturation);
+        double margin_confidence = std::fmax(depth_margin, 0.2);
+        float confidence = static_cast<float>(clampd(
+            support_confidence * reciprocal_confidence * error_confidence * margin_confidence,
+            0.05, 1.0));
+        Point3 p;
+        sample_rgb(ref_frame, x, y, p.r, p.g, p.b);
+        p.x = static_cast<float>(fused.position.x);
+        p.y = static_cast<float>(fused.position.y);
+        p.z = static_cast<float>(fused.position.z);
+        p.confidence = confidence;
+        out.points.push_back(p);
+        out.grid_sites.push_back({x, y});
+        out.point_attributes.push_back({static_cast<float>(reciprocal_confidence),
+                                        static_cast<float>(depth_margin)});
+        errors.push_back(best.error);
+        supports.push_back(static_cast<double>(best.support));
     }
 
     if (sweep_records || band) return out;
     CompletionStats cs = complete_surface_samples(
         prof, *reference, ref_frame, ref_luma, sources, out.points, out.grid_sites,
-        out.point_attributes, errors, supports, width, height, border, stride, focal, control);
+        out.point_attributes, errors, supports, width, height, border, stride, focal, control,
+        explain);
 
     LegacyStats& st = out.stats;
     st.attempted = true;

@@ -220,7 +220,8 @@ std::optional<LegacyAnalysis> reconstruct_reference_patch(const Profile& prof,
                                                           const std::vector<Vec3>& sparse,
                                                           double focal, size_t camera_index,
                                                           bool fine_grid, Control& control,
-                                                          const RowBand* band) {
+                                                          const RowBand* band,
+                                                          std::vector<ExplainRecord>* explain) {
     // dense.rs:674-747
     if (camera_index >= cameras.size()) return std::nullopt;
     const Camera& rc = cameras[camera_index];
@@ -250,7 +251,7 @@ std::optional<LegacyAnalysis> reconstruct_reference_patch(const Profile& prof,
         rcams.push_back(m);
     }
     LegacyAnalysis a = estimate_depth_points_ptr(prof, rframes, rcams, visible, focal, fine_grid,
-                                                 control, nullptr, band);
+                                                 control, nullptr, band, explain);
     a.stats.reference_frame = rc.frame_index;
     std::vector<size_t> mapped;
     for (size_t r : a.stats.source_frames)
@@ -383,6 +384,207 @@ std::pair<DenseAnalysis, bool> estimate_depth_points_limited(const Profile& prof
         return {std::move(fb), false};
     }
     return {combine_patches(std::move(patches), std::move(attempts)), omitted};
+}
+
+
+// ---- the working-set budget (dense.rs:354-605) -------------------------------
+//
+// Pure size arithmetic over Rust type sizes.  Every size below is the
+// x86-64 layout rustc gives the named type (repr(Rust): fields reordered by
+// alignment, no niche in usize/f64/u8, so Option<T> adds an aligned tag).
+
+namespace {
+
+uint64_t sat_add(uint64_t a, uint64_t b) { return a + b < a ? UINT64_MAX : a + b; }
+uint64_t sat_mul(uint64_t a, uint64_t b) {
+    uint64_t r;
+    return __builtin_mul_overflow(a, b, &r) ? UINT64_MAX : r;
+}
+
+constexpr uint64_t kUsize = 8, kF64 = 8, kF32 = 4, kU32 = 4, kI32 = 4, kI64 = 8, kI16 = 2,
+                   kBool = 1, kU8 = 1;
+constexpr uint64_t kVec = 24;                    // Vec<T>: pointer, capacity, length
+constexpr uint64_t kVector3 = 24;                // nalgebra Vector3<f64>
+constexpr uint64_t kPoint3 = 20;                 // reconstruction/types.rs:69: 4 x f32 + 3 x u8
+constexpr uint64_t kGridSite = 8;                // DenseGridSite {u32, u32}
+constexpr uint64_t kAttrs = 8;                   // EvidencePointAttributes {f32, f32}
+constexpr uint64_t kMeshTriangle = 32;           // mesh_legacy.rs:18: 3 x usize + f32
+constexpr uint64_t kOptUsize = 16, kOptF64 = 16, kOptVector3 = 32, kOptUsizeF64 = 24;
+constexpr uint64_t kOptOrigin = 1;               // Option<EvidenceOrigin>: 4-variant enum, niche
+constexpr uint64_t kOptTriangleGeometry = 128;   // surface_merge.rs:1137: 120 B + tag
+constexpr uint64_t kImageRemoval = 24;           // surface_merge_stitch.rs:67
+constexpr uint64_t kProjectedTriangle = 72;      // [(Vector2<f64>, f64); 3]
+constexpr uint64_t kTriangleSourceCorners = 32;  // reconstruction_evidence.rs:125
+constexpr uint64_t kKeptTriangle = 112;          // ([Vector3<f64>; 3], usize, [usize; 3], usize)
+constexpr uint64_t kHalfEdge = 16;               // surface_merge_stitch.rs:78: 4 x u32
+constexpr uint64_t kOptSeam = 32;                // [u32; 6] + u8 = 28 B, plus an aligned tag
+constexpr uint64_t kEdgeUse = 8;                 // {u32, u32}
+constexpr uint64_t kMaxScaleSamples = 4096;      // surface_merge.rs:99
+constexpr uint64_t kMaxSeamVertices = 6;         // surface_merge_stitch.rs:51
+constexpr uint64_t kMaxSeamsPerVertex = 16;      // surface_merge_stitch.rs:54
+constexpr uint64_t kMaxReferenceViews = 3;       // dense.rs:8
+constexpr uint64_t kMaxSourceViewsPerReference = 4;  // dense.rs:11
+constexpr uint64_t kDenseGridBorder = 3;         // dense.rs:12
+
+constexpr uint64_t entry(uint64_t payload) { return payload + 4 * kUsize + 32; }
+
+uint64_t grid_axis_samples(uint64_t extent, uint64_t stride) {
+    // dense.rs:615-618
+    uint64_t usable = extent > 2 * kDenseGridBorder ? extent - 2 * kDenseGridBorder : 0;
+    return sat_add(usable, stride ? stride - 1 : 0) / stride;
+}
+
+uint64_t stitch_working_set(uint64_t vertices, uint64_t triangles) {
+    // surface_merge_stitch.rs:128-152
+    const uint64_t per_vertex = kBool;
+    const uint64_t per_triangle = 3 * kHalfEdge + kOptSeam + kMaxSeamVertices * 8 + 3 * kU32 +
+                                  kMeshTriangle + 3 * entry(8 + kEdgeUse) + kUsize +
+                                  entry(32 + kVec);
+    const uint64_t scratch =
+        2 * kMaxSeamsPerVertex * (entry(kUsize) + kMaxSeamVertices * (entry(kUsize) + 2 * 32));
+    return sat_add(sat_add(sat_mul(vertices, per_vertex), sat_mul(triangles, per_triangle)),
+                   scratch);
+}
+
+uint64_t merge_working_set(uint64_t vertices, uint64_t triangles) {
+    // surface_merge.rs:1080-1121
+    const uint64_t per_vertex = 3 * kUsize + kBool + kOptOrigin + 2 * 16 + entry(16) +
+                                2 * entry(2 * kUsize) + entry(kUsize + 24);
+    const uint64_t per_triangle = kUsize + kOptUsize + kBool + kOptTriangleGeometry + 2 * kUsize +
+                                  kImageRemoval + kProjectedTriangle + kUsize + 24 + 2 * kUsize +
+                                  entry(24 + kVec) + entry(32 + kVec) + entry(2 * kUsize) + 32 +
+                                  kTriangleSourceCorners;
+    const uint64_t ownership = sat_add(
+        sat_mul(triangles, 3 * kF64 + kKeptTriangle + entry(kUsize)), kMaxScaleSamples * kF64);
+    return sat_add(sat_add(sat_mul(vertices, per_vertex), sat_mul(triangles, per_triangle)),
+                   std::max(ownership, stitch_working_set(vertices, triangles)));
+}
+
+}  // namespace
+
+WorkingSet estimate_working_set(const std::vector<Frame>& frames, uint64_t max_features,
+                                uint32_t descriptor_radius, uint64_t reference_views,
+                                bool fine_grid) {
+    // dense.rs:423-605
+    WorkingSet w;
+    uint64_t luminance_pixels = 0, largest = 0;
+    for (const Frame& f : frames) {
+        const uint64_t px = sat_mul(f.width, f.height);
+        w.frame_bytes = sat_add(w.frame_bytes, f.bytes.size());
+        luminance_pixels = sat_add(luminance_pixels, px);
+        largest = std::max(largest, px);
+    }
+    uint64_t per_reference = 0;
+    if (!frames.empty()) {
+        const uint64_t stride = grid_stride(frames[0].width, frames[0].height, fine_grid);
+        per_reference = sat_mul(grid_axis_samples(frames[0].width, stride),
+                                grid_axis_samples(frames[0].height, stride));
+    }
+    const uint64_t samples = sat_mul(per_reference, reference_views);
+    const uint64_t triangles = sat_mul(samples, 8);
+    w.retry_frame_bytes = w.frame_bytes;
+    w.remapped_frame_bytes = w.frame_bytes;
+    w.luminance_bytes =
+        sat_add(luminance_pixels, sat_mul(largest, 1 + kMaxSourceViewsPerReference));
+    const uint64_t side = sat_add(sat_mul(descriptor_radius, 2), 1);
+    const uint64_t descriptor_bytes = sat_mul(sat_mul(side, side), kI16);
+    const uint64_t n = frames.size();
+    const uint64_t features = sat_mul(n, max_features);
+    const uint64_t matches = sat_mul(n ? n - 1 : 0, max_features);
+    const uint64_t observations = sat_mul(matches, 2);
+    const uint64_t feature_record = 3 * kU32 + kVec;
+    w.sparse_pipeline_bytes = sat_add(
+        sat_add(sat_add(sat_add(sat_add(sat_mul(features, sat_add(feature_record, descriptor_bytes)),
+                                        sat_mul(matches, 3 * kUsize)),
+                                sat_mul(matches, kVec)),
+                        sat_mul(observations, 2 * kUsize)),
+                sat_mul(observations, entry(3 * kUsize))),
+        sat_mul(matches, kPoint3 + kUsize + kF32 + kVector3 + 2 * kF64 + 4 * kUsize));
+    const uint64_t retained_sample = kPoint3 + kGridSite + kAttrs + 2 * kF64 + 3 * kUsize;
+    w.dense_sample_bytes = sat_mul(sat_mul(samples, retained_sample), 2);
+    w.topology_bytes = sat_mul(triangles, kMeshTriangle);
+    w.mesh_builder_bytes = sat_add(
+        sat_add(sat_add(sat_mul(samples, entry(2 * kI32 + kUsize + 6 * kF64 + kF32)),
+                        sat_mul(sat_mul(samples, 4), entry(2 * kI32))),
+                sat_mul(triangles, entry(3 * kUsize))),
+        sat_mul(triangles, kMeshTriangle));
+    const uint64_t per_vertex_fusion = kOptUsize + kVector3 + kF64 + kUsize + kVec + kOptVector3 +
+                                       kOptF64 + kOptUsizeF64 + kOptUsize + 2 * kBool + 3 * kI64 +
+                                       kVec + 4 * kUsize + kUsize + 2 * kUsize + kVector3;
+    const uint64_t per_triangle_fusion = 6 * kUsize + 3 * kF64 + kBool + kUsize;
+    w.surface_fusion_bytes = std::max(sat_add(sat_mul(samples, per_vertex_fusion),
+                                              sat_mul(triangles, per_triangle_fusion)),
+                                      merge_working_set(samples, triangles));
+    const uint64_t retained = sat_mul(per_reference, kMaxReferenceViews);
+    w.retained_candidate_bytes = sat_add(sat_mul(retained, kPoint3 + kGridSite + kAttrs),
+                                         sat_mul(sat_mul(retained, 8), kMeshTriangle));
+    w.packed_output_bytes = sat_add(sat_mul(samples, 6 * kF32 + 3 * kU8 + 2 * kU32),
+                                    sat_mul(triangles, 4 * kU32));
+    uint64_t t = 0;
+    for (uint64_t v : {w.frame_bytes, w.retry_frame_bytes, w.remapped_frame_bytes,
+                       w.luminance_bytes, w.sparse_pipeline_bytes, w.dense_sample_bytes,
+                       w.topology_bytes, w.mesh_builder_bytes, w.surface_fusion_bytes,
+                       w.retained_candidate_bytes, w.packed_output_bytes})
+        t = sat_add(t, v);
+    w.total_bytes = t;
+    return w;
+}
+
+BudgetedAnalysis estimate_depth_points_with_budget(const Profile& prof,
+                                                   const std::vector<Frame>& frames,
+                                                   const std::vector<Camera>& cameras,
+                                                   const std::vector<Vec3>& sparse, double focal,
+                                                   uint64_t budget, uint64_t max_features,
+                                                   uint32_t descriptor_radius, Control& control) {
+    // dense.rs:355-420
+    BudgetedAnalysis out;
+    out.budget_bytes = budget;
+    auto estimate = [&](uint64_t views, bool fine) {
+        return estimate_working_set(frames, max_features, descriptor_radius, views, fine);
+    };
+    const bool finer = !frames.empty() && grid_stride(frames[0].width, frames[0].height, true) <
+                                              grid_stride(frames[0].width, frames[0].height, false);
+    std::optional<WorkingSet> fine_estimate;
+    if (finer && has_distributed_landmarks(frames, cameras, sparse, focal, control)) {
+        WorkingSet f = estimate(kMaxReferenceViews, true);
+        if (f.total_bytes <= budget) fine_estimate = f;
+    }
+    const bool fine_grid = fine_estimate.has_value();
+    const WorkingSet full = fine_estimate ? *fine_estimate : estimate(kMaxReferenceViews, false);
+    out.full_bytes = full.total_bytes;
+    uint64_t views = 0;
+    WorkingSet plan;
+    if (full.total_bytes <= budget) {
+        views = kMaxReferenceViews;
+        plan = full;
+    } else {
+        for (uint64_t v = kMaxReferenceViews - 1; v >= 1; --v) {
+            WorkingSet l = estimate(v, false);
+            if (l.total_bytes <= budget) {
+                views = v;
+                plan = l;
+                break;
+            }
+        }
+    }
+    if (views == 0) {
+        const WorkingSet single = estimate(1, false);
+        out.estimate = single;
+        out.analysis.stats.skip_reason =
+            "estimated dense working set of " + std::to_string(single.total_bytes) +
+            " bytes exceeds the configured " + std::to_string(budget) +
+            " byte budget even for one reference view";
+        return out;
+    }
+    auto [analysis, omitted] =
+        estimate_depth_points_limited(prof, frames, cameras, sparse, focal, views, fine_grid,
+                                      control);
+    out.analysis = std::move(analysis);
+    out.estimate = plan;
+    out.fine_grid = fine_grid;
+    out.reference_views = views;
+    if (views < kMaxReferenceViews && omitted) out.analysis.stats.reference_view_limit = views;
+    return out;
 }
 
 }  // namespace v3do

@@ -7,12 +7,20 @@ as ``v3d.dense`` and return the same result objects.
 import ctypes as C
 import os
 
+import numpy as np
+
 from v3d import abi, types
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 LIB = os.path.join(ROOT, "oracle", "_build", "liboracle_v3d.so")
 
 _P = C.POINTER
+
+# ExplainRecord (oracle/oracle.hpp)
+EXPLAIN_DTYPE = np.dtype([("x", "<u4"), ("y", "<u4"), ("stage", "<i4"), ("outcome", "<i4"),
+                          ("plane", "<i4"), ("support", "<i4"), ("error", "<f8"),
+                          ("margin", "<f8"), ("sweep_gap", "<f8"),
+                          ("recip_gap", "<f8")])
 
 
 class Oracle:
@@ -223,6 +231,81 @@ class Oracle:
             res.append(types.dense_from_result(outs[i]) if present[i] else None)
             self.lib.v3do_dense_result_free(C.byref(outs[i]))
         return res
+
+    def explain_reference_patch(self, frames, cameras, sparse_points, focal, camera_index,
+                                profile, fine_grid=False):
+        """The remapped pass of one reference (camera_index None: the legacy
+        single call) and its decision records (ExplainRecord in
+        oracle/oracle.hpp): primary sites in raster order, then the completion
+        proposals of each pass.  None where the pass does not run."""
+        L = self.lib
+        if not getattr(self, "_explain_bound", False):
+            L.v3do_explain_reference_patch.argtypes = [
+                _P(abi.Frame), C.c_uint64, _P(abi.Camera), C.c_uint64, _P(C.c_double), C.c_uint64,
+                C.c_double, C.c_int32, _P(abi.Profile), C.c_uint64, _P(abi.DenseResult),
+                _P(C.c_void_p), _P(C.c_uint64)]
+            L.v3do_explain_reference_patch.restype = C.c_int32
+            L.v3do_free.argtypes = [C.c_void_p]
+            self._explain_bound = True
+        inp = types.Inputs(frames, cameras, sparse_points)
+        out = abi.DenseResult()
+        recs, n = C.c_void_p(), C.c_uint64()
+        st = L.v3do_explain_reference_patch(
+            inp.frames, inp.n_frames, inp.cameras, inp.n_cameras, inp.sparse, inp.n_sparse,
+            float(focal), int(fine_grid), C.byref(profile),
+            (1 << 64) - 1 if camera_index is None else int(camera_index), C.byref(out),
+            C.byref(recs), C.byref(n))
+        if st < 0:
+            raise ValueError("oracle rejected the inputs (status %d)" % st)
+        if st == abi.SKIPPED:
+            return None, np.zeros(0, EXPLAIN_DTYPE)
+        res = types.dense_from_result(out)
+        L.v3do_dense_result_free(C.byref(out))
+        rec = np.zeros(n.value, EXPLAIN_DTYPE)
+        if n.value:
+            C.memmove(rec.ctypes.data, recs, n.value * EXPLAIN_DTYPE.itemsize)
+        L.v3do_free(recs)
+        return res, rec
+
+    def estimate_working_set(self, frames, max_features, descriptor_radius, reference_views,
+                             fine_grid):
+        L = self.lib
+        L.v3do_estimate_working_set.argtypes = [_P(abi.Frame), C.c_uint64, C.c_uint64,
+                                                C.c_uint32, C.c_uint64, C.c_int32,
+                                                _P(C.c_uint64)]
+        L.v3do_estimate_working_set.restype = C.c_int32
+        inp = types.Inputs(frames, [], [])
+        out = (C.c_uint64 * 12)()
+        L.v3do_estimate_working_set(inp.frames, inp.n_frames, int(max_features),
+                                    int(descriptor_radius), int(reference_views), int(fine_grid),
+                                    out)
+        return dict(zip(abi.WORKING_SET_FIELDS, [int(v) for v in out]))
+
+    def estimate_depth_points_with_budget_and_control(self, frames, cameras, sparse_points, focal,
+                                                      working_set_budget_bytes, max_features,
+                                                      descriptor_radius, profile, control=None):
+        L = self.lib
+        L.v3do_estimate_depth_points_with_budget.argtypes = [
+            _P(abi.Frame), C.c_uint64, _P(abi.Camera), C.c_uint64, _P(C.c_double), C.c_uint64,
+            C.c_double, C.c_uint64, C.c_uint64, C.c_uint32, _P(abi.Profile), abi.CANCEL_FN,
+            C.c_void_p, _P(abi.DenseResult), _P(C.c_uint64)]
+        L.v3do_estimate_depth_points_with_budget.restype = C.c_int32
+        inp = types.Inputs(frames, cameras, sparse_points)
+        fn, _keep = types.cancel_callback(control)
+        out = abi.DenseResult()
+        plan = (C.c_uint64 * 16)()
+        st = L.v3do_estimate_depth_points_with_budget(
+            inp.frames, inp.n_frames, inp.cameras, inp.n_cameras, inp.sparse, inp.n_sparse,
+            float(focal), int(working_set_budget_bytes), int(max_features),
+            int(descriptor_radius), C.byref(profile), fn, None, C.byref(out), plan)
+        if st < 0:
+            raise ValueError("oracle rejected the inputs (status %d)" % st)
+        res = types.dense_from_result(out)
+        L.v3do_dense_result_free(C.byref(out))
+        v = [int(x) for x in plan]
+        return res, {"working_set_estimate": dict(zip(abi.WORKING_SET_FIELDS, v[:12])),
+                     "working_set_budget_bytes": v[12], "full_working_set_bytes": v[13],
+                     "fine_grid": bool(v[14]), "reference_views": v[15]}
 
     def estimate_depth_points_limited(self, frames, cameras, sparse_points, focal,
                                       reference_views, fine_grid, profile, control=None):
