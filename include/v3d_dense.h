@@ -13,6 +13,9 @@
  *   v3d_estimate_depth_points_with_control  dense_legacy.rs:149-470
  *   v3d_reconstruct_reference_patches       dense.rs:674-747 (one call per camera, batched)
  *   v3d_estimate_depth_points_limited       dense.rs:250-330
+ *   v3d_estimate_depth_points_with_budget_and_control
+ *                                           dense.rs:355-420
+ *   v3d_estimate_working_set                dense.rs:423-605
  *   v3d_has_distributed_landmarks           dense.rs:165-213
  *   v3d_grid_stride                         dense.rs:215-218
  *   v3d_reconstruct_dense_mesh_samples      mesh_legacy.rs:150-358
@@ -87,7 +90,8 @@ typedef enum v3d_skip_code {
     V3D_SKIP_NO_DEPTH_ENVELOPE = 6,      /* dense_legacy.rs:197-199 */
     V3D_SKIP_REFERENCE_FRAME_MISSING = 7,/* dense_legacy.rs:206 */
     V3D_SKIP_NO_SOURCE_VIEW = 8,         /* dense_legacy.rs:233-235 */
-    V3D_SKIP_CANCELED = 9                /* dense_legacy.rs:274 */
+    V3D_SKIP_CANCELED = 9,               /* dense_legacy.rs:274 */
+    V3D_SKIP_WORKING_SET_BUDGET = 10     /* dense.rs:385-402; the reason carries the sizes */
 } v3d_skip_code;
 
 typedef enum v3d_pixel_format {
@@ -450,6 +454,70 @@ int32_t v3d_estimate_depth_points_limited(
     v3d_cancel_fn cancel, void* cancel_user,
     v3d_dense_result* out, int32_t* omitted_references);
 
+/* ---- the working-set budget (dense.rs:354-605) ----------------------------
+ * Pure host arithmetic: no context, no device. */
+
+/* DenseWorkingSetEstimate (dense.rs:15-28). */
+typedef struct v3d_working_set_estimate {
+    uint64_t frame_bytes;
+    uint64_t retry_frame_bytes;
+    uint64_t remapped_frame_bytes;
+    uint64_t luminance_bytes;
+    uint64_t sparse_pipeline_bytes;
+    uint64_t dense_sample_bytes;
+    uint64_t topology_bytes;
+    uint64_t mesh_builder_bytes;
+    uint64_t surface_fusion_bytes;  /* peak of surface fusion and the connected-surface merge */
+    uint64_t retained_candidate_bytes;
+    uint64_t packed_output_bytes;
+    uint64_t total_bytes;
+} v3d_working_set_estimate;
+
+/* The budget fields of DenseStats (dense.rs:133-136) and the plan that ran. */
+typedef struct v3d_dense_budget {
+    v3d_working_set_estimate working_set_estimate;
+    uint64_t working_set_budget_bytes;
+    uint64_t full_working_set_bytes;
+    int32_t fine_grid;         /* the grid the plan ran on */
+    int32_t pad0;
+    uint64_t reference_views;  /* the plan's reference-view limit; 0 when the budget skipped */
+} v3d_dense_budget;
+
+/* estimate_working_set (dense.rs:423-605): the conservative bytes the Rust
+ * process holds at the dense stage's peak with at most `reference_views`
+ * reference patches, from the frames, the sparse-stage options (max_features,
+ * descriptor_radius) and the grid.  Sizes are those of the x86-64 Rust
+ * layouts of the containers the reference charges.  A frame counts its bytes
+ * as handed in (the reference's RGBA frames: width x height x 4).
+ * Saturating, like the reference. */
+int32_t v3d_estimate_working_set(
+    const v3d_frame* frames, uint64_t n_frames,
+    uint64_t max_features, uint32_t descriptor_radius,
+    uint64_t reference_views, int32_t fine_grid,
+    v3d_working_set_estimate* out);
+
+/* estimate_depth_points_with_budget_and_control (dense.rs:355-420): picks the
+ * fine grid (when finer spacing exists, the landmarks are distributed and the
+ * three-view fine plan fits), else the most reference views (3, 2, 1) whose
+ * estimate fits `working_set_budget_bytes`, runs
+ * v3d_estimate_depth_points_limited with that plan and reports the plan in
+ * *budget.  When not even one view fits, returns V3D_SKIPPED with skip code
+ * V3D_SKIP_WORKING_SET_BUDGET and the reference's message ("estimated dense
+ * working set of N bytes exceeds the configured B byte budget even for one
+ * reference view").  stats.reference_view_limit is set when the plan kept
+ * fewer than 3 views and a further reference candidate remained.  The cancel
+ * callback is sticky across the landmark test and the pass. */
+int32_t v3d_estimate_depth_points_with_budget_and_control(
+    v3d_context* ctx,
+    const v3d_frame* frames, uint64_t n_frames,
+    const v3d_camera* cameras, uint64_t n_cameras,
+    const double* sparse_xyz, uint64_t n_sparse,
+    double focal, uint64_t working_set_budget_bytes,
+    uint64_t max_features, uint32_t descriptor_radius,
+    const v3d_profile* profile,
+    v3d_cancel_fn cancel, void* cancel_user,
+    v3d_dense_result* out, v3d_dense_budget* budget);
+
 /* has_distributed_landmarks (dense.rs:165-213), polling `cancel` once per
  * 256-landmark chunk like the reference. */
 int32_t v3d_has_distributed_landmarks(
@@ -476,7 +544,9 @@ typedef struct v3d_run_info {
     uint64_t reciprocal_plane_evaluations; /* single-view hypotheses evaluated, all passes */
     uint64_t candidates;      /* primary + completion candidates checked */
     double host_plan_ms;      /* host planning of every reference */
-    double host_upload_ms;    /* staging and enqueueing uploads and kernels */
+    double host_enqueue_ms;   /* staging uploads, enqueueing every kernel, and (in the
+                               * _meshed call) the mid-batch read of the per-reference
+                               * point counts that size the mesh stage */
     double host_wait_ms;      /* waiting for the device, read-back included */
     double host_assemble_ms;  /* splitting the point pool per reference, medians */
     double mesh_ms;           /* device mesh stage of the _meshed call */
@@ -485,16 +555,12 @@ typedef struct v3d_run_info {
     double host_readback_ms;  /* result copies into that block (within host_wait_ms) */
     uint64_t result_bytes;    /* bytes of that block the results occupy */
     uint64_t sweep_chunks;    /* plane chunks of the box-filtered sweep (1: none) */
+    double recip_sweep_ms;    /* the single-view reciprocal sweep kernel, all its launches
+                               * (primary candidates and both completion passes) */
+    double recip_prepare_ms;  /* the reciprocal prologue and its pair list, all launches */
 } v3d_run_info;
 
 int32_t v3d_last_run_info(const v3d_context* ctx, v3d_run_info* out);
-
-/* Diagnostic with no counterpart in the reference: the rate of homography-
- * warped f32 bilinear samples this GPU sustains when it does nothing else (the
- * depth sweep's warp step alone, over CTA-sized footprints that stay in L1 and
- * L2), for the gather roofline of the sweep.  Allocates and frees a 2 MiB
- * image; about 0.1 s on a B200. */
-int32_t v3d_measure_gather_rate(v3d_context* ctx, double* samples_per_second);
 
 /* ---- geometric depth-grid verification (colmap_surface.rs:158-314) --------
  * The alternate dense provider's gate: every reference depth-grid sample is
@@ -811,7 +877,9 @@ typedef struct v3d_mesh_counts {
  * rejected with V3D_ERR_INVALID_ARGUMENT before anything is enqueued (about
  * 1280x720 at grid stride 2 fits).  The first call on a device looks up the
  * array's device address (cudaGetSymbolAddress) with that device current, so
- * make it before any stream capture.  Every call shares the array and leaves
+ * make it before any stream capture; the address is kept for the life of the
+ * process, so the device must not be reset (cudaDeviceReset) nor its primary
+ * context replaced after that first call.  Every call shares the array and leaves
  * the last call's contents there; the call clears what must start at zero.
  * Calls that overlap on the GPU (other streams, other host threads) race on
  * the array: order them on one stream.

@@ -190,11 +190,12 @@ class RunInfo(C.Structure):
                 ("sweep_ms", C.c_double), ("reciprocal_ms", C.c_double),
                 ("completion_ms", C.c_double), ("reciprocal_plane_evaluations", C.c_uint64),
                 ("candidates", C.c_uint64), ("host_plan_ms", C.c_double),
-                ("host_upload_ms", C.c_double), ("host_wait_ms", C.c_double),
+                ("host_enqueue_ms", C.c_double), ("host_wait_ms", C.c_double),
                 ("host_assemble_ms", C.c_double), ("mesh_ms", C.c_double),
                 ("triangles", C.c_uint64), ("host_block_ms", C.c_double),
                 ("host_readback_ms", C.c_double), ("result_bytes", C.c_uint64),
-                ("sweep_chunks", C.c_uint64)]
+                ("sweep_chunks", C.c_uint64), ("recip_sweep_ms", C.c_double),
+                ("recip_prepare_ms", C.c_double)]
 
 
 CANCEL_FN = C.CFUNCTYPE(C.c_int32, C.c_void_p)
@@ -279,7 +280,26 @@ class DenseDocument(C.Structure):
                 ("non_finite", C.c_uint64), ("sha256", C.c_uint8 * 32)]
 
 
+WORKING_SET_FIELDS = ("frame_bytes", "retry_frame_bytes", "remapped_frame_bytes",
+                      "luminance_bytes", "sparse_pipeline_bytes", "dense_sample_bytes",
+                      "topology_bytes", "mesh_builder_bytes", "surface_fusion_bytes",
+                      "retained_candidate_bytes", "packed_output_bytes", "total_bytes")
+
+
+class WorkingSetEstimate(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in WORKING_SET_FIELDS]
+
+
+class DenseBudget(C.Structure):
+    _fields_ = [("working_set_estimate", WorkingSetEstimate),
+                ("working_set_budget_bytes", C.c_uint64), ("full_working_set_bytes", C.c_uint64),
+                ("fine_grid", C.c_int32), ("pad0", C.c_int32), ("reference_views", C.c_uint64)]
+
+
+SKIP_WORKING_SET_BUDGET = 10
+
 STRUCTS = {
+    "v3d_working_set_estimate": WorkingSetEstimate, "v3d_dense_budget": DenseBudget,
     "v3d_dense_document": DenseDocument,
     "v3d_meshing_funnel": MeshingFunnel, "v3d_verified_surface_region": VerifiedSurfaceRegion,
     "v3d_verified_surface": VerifiedSurface,

@@ -65,6 +65,13 @@ def library():
         C.c_uint64, C.c_int32, _P(abi.Profile), abi.CANCEL_FN, C.c_void_p, _P(abi.DenseResult),
         _P(C.c_int32)]
     L.v3d_estimate_depth_points_limited.restype = C.c_int32
+    L.v3d_estimate_depth_points_with_budget_and_control.argtypes = [C.c_void_p] + frames_args + [
+        C.c_uint64, C.c_uint64, C.c_uint32, _P(abi.Profile), abi.CANCEL_FN, C.c_void_p,
+        _P(abi.DenseResult), _P(abi.DenseBudget)]
+    L.v3d_estimate_depth_points_with_budget_and_control.restype = C.c_int32
+    L.v3d_estimate_working_set.argtypes = [_P(abi.Frame), C.c_uint64, C.c_uint64, C.c_uint32,
+                                           C.c_uint64, C.c_int32, _P(abi.WorkingSetEstimate)]
+    L.v3d_estimate_working_set.restype = C.c_int32
     L.v3d_has_distributed_landmarks.argtypes = frames_args + [abi.CANCEL_FN, C.c_void_p]
     L.v3d_has_distributed_landmarks.restype = C.c_int32
     L.v3d_dense_result_free.argtypes = [_P(abi.DenseResult)]
@@ -140,8 +147,6 @@ def library():
     L.v3d_pack_mesh_triangles.restype = C.c_int32
     L.v3d_sha256.argtypes = [C.c_char_p, C.c_uint64, C.c_void_p]
     L.v3d_sha256.restype = None
-    L.v3d_measure_gather_rate.argtypes = [C.c_void_p, _P(C.c_double)]
-    L.v3d_measure_gather_rate.restype = C.c_int32
     L.v3d_last_run_info.argtypes = [C.c_void_p, _P(abi.RunInfo)]
     L.v3d_last_run_info.restype = C.c_int32
     _lib = L
@@ -296,11 +301,23 @@ class Context:
             None, C.byref(out), C.byref(omitted)))
         return self._dense(out, st), bool(omitted.value)
 
-    def measure_gather_rate(self):
-        """Warped bilinear samples per second this GPU sustains alone (diagnostic)."""
-        rate = C.c_double()
-        self._check(self.lib.v3d_measure_gather_rate(self.handle, C.byref(rate)))
-        return rate.value
+    def estimate_depth_points_with_budget_and_control(self, frames, cameras, sparse_points, focal,
+                                                      working_set_budget_bytes, max_features,
+                                                      descriptor_radius, profile=None,
+                                                      control=None):
+        """dense.rs:355-420: the budget plan, then the limited pass.  Returns the
+        analysis and the plan: {"working_set_estimate": {...}, "working_set_budget_bytes",
+        "full_working_set_bytes", "fine_grid", "reference_views"}."""
+        prof = profile if profile is not None else profiles.reference()
+        inp = types.Inputs(frames, cameras, sparse_points)
+        fn, _keep = types.cancel_callback(control)
+        out = abi.DenseResult()
+        plan = abi.DenseBudget()
+        st = self._check(self.lib.v3d_estimate_depth_points_with_budget_and_control(
+            self.handle, inp.frames, inp.n_frames, inp.cameras, inp.n_cameras, inp.sparse,
+            inp.n_sparse, float(focal), int(working_set_budget_bytes), int(max_features),
+            int(descriptor_radius), C.byref(prof), fn, None, C.byref(out), C.byref(plan)))
+        return self._dense(out, st), budget_plan(plan)
 
     def last_run_info(self):
         """Device time, kernel launches and work units of the last dense call."""
@@ -644,6 +661,26 @@ def _topology(lib_fn, head, triangles, vertex_count):
     out = abi.SurfaceTopology()
     st = lib_fn(*head, tris.ctypes.data, len(tris), int(vertex_count), C.byref(out))
     return st, {name: int(getattr(out, name)) for name, _ in out._fields_}
+
+
+def budget_plan(plan):
+    est = plan.working_set_estimate
+    return {"working_set_estimate": {n: int(getattr(est, n)) for n in abi.WORKING_SET_FIELDS},
+            "working_set_budget_bytes": int(plan.working_set_budget_bytes),
+            "full_working_set_bytes": int(plan.full_working_set_bytes),
+            "fine_grid": bool(plan.fine_grid), "reference_views": int(plan.reference_views)}
+
+
+def estimate_working_set(frames, max_features, descriptor_radius, reference_views, fine_grid):
+    """dense.rs:423-605 on the host (no device needed)."""
+    inp = types.Inputs(frames, [], [])
+    out = abi.WorkingSetEstimate()
+    st = library().v3d_estimate_working_set(inp.frames, inp.n_frames, int(max_features),
+                                            int(descriptor_radius), int(reference_views),
+                                            int(fine_grid), C.byref(out))
+    if st != abi.OK:
+        raise V3DError(st)
+    return {n: int(getattr(out, n)) for n in abi.WORKING_SET_FIELDS}
 
 
 def has_distributed_landmarks(frames, cameras, sparse_points, focal, control=None):
