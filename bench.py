@@ -36,14 +36,20 @@ sys.path.insert(0, ROOT)
 import numpy as np  # noqa: E402
 
 METRIC = "plane-sweep samples·planes·views/s"
+# The fast policy's stated cost tolerance against the f64 oracle (tests/attribution.py)
+from tests.attribution import COST_TOLERANCE  # noqa: E402
 UNIT = "samples·planes·views/s"
 WIDTH, HEIGHT, FRAMES = 640, 360, 120
 RADIUS, PLANES, SOURCES, STRIDE = 3, 128, 8, 2
-# DRAM bytes per unit of the depth sweep (k_sweep_tiled), from one ncu capture of
-# the same workload cut to 12 keyframes (677.4 M units; 11.15 MB read + 0.01 MB
-# written; profiles/k_sweep_tiled_zncc7x7_640x360_12kf.md).  A clip's frames live
-# in L2, so the sweep's DRAM traffic grows with its units.
+# DRAM bytes per launch unit of the two large kernels, from ncu captures of the
+# same workload cut to 12 keyframes (profiles/k_sweep_tiled_zncc7x7_640x360_12kf.md,
+# profiles/k_recip_sweep_zncc7x7_640x360_12kf.md): the depth sweep read 11.15 MB
+# and wrote 0.01 MB for 677.4 M window evaluations; the reciprocal sweep read
+# 193.4 MB and wrote 70.1 MB for the pairs of 1 reciprocal launch.  A clip's frames
+# live in L2, so DRAM traffic grows with the work.
 SWEEP_DRAM_BYTES_PER_UNIT = (11.151360e6 + 0.008192e6) / 677.376e6
+ARITH = {"f32": "f32", "f16": "f16 storage, f32 arithmetic",
+         "bf16": "bf16 storage, f32 arithmetic"}
 
 
 def parse():
@@ -92,6 +98,84 @@ def workload(args):
             "storage": args.storage, "cost": "1-ZNCC",
             "l2": "flushed between timed steps (256 MiB write)",
             "parallelism": "weak: one clip per GPU, no collective on the data path"}
+
+
+def kernel_rooflines(info, units, b, sweep_ms, recip_sweep_ms, recip_prep_ms, hbm, peak_note):
+    """Per-kernel roofline objects of a step: each kernel's time summed over all of
+    its launches in the step (CUDA events on the library's stream) and the bytes it
+    must read, counted as unique texels:
+      k_sweep_tiled   per (tile, hypothesis, source) the source texels under the
+                      warped footprint of the tile's windows, (PX+1)(PY+1) of them
+                      (PX = 31*stride + W, PY = 7*stride + W), plus the reference
+                      footprint PX*PY once per tile;
+      k_recip_sweep   per (pending pair, hypothesis) the reference texels under the
+                      warped window, (W+1)^2;
+      k_recip_prepare per (candidate, source) the reference and source texels of the
+                      direct cost and the source window of the contrast gate,
+                      3 (W+1)^2.
+    All three are bound by SM instruction issue with their gathers served from L1
+    and L2 (the profiles under profiles/ give issue-active and L1 figures), so the
+    fraction of the HBM roofline is the share of memory bandwidth the kernel's
+    compulsory reads would need at its achieved rate."""
+    W = 2 * RADIUS + 1
+    PX, PY = 31 * STRIDE + W, 7 * STRIDE + W
+    nx = (WIDTH - 2 * (RADIUS + 2) + STRIDE - 1) // STRIDE
+    ny = (HEIGHT - 2 * (RADIUS + 2) + STRIDE - 1) // STRIDE
+    sites = nx * ny
+    tiles = ((nx + 31) // 32) * ((ny + 7) // 8)
+    refs = units / float(sites * PLANES * SOURCES)
+    sweep_bytes = refs * tiles * (PLANES * SOURCES * (PX + 1) * (PY + 1) + PX * PY) * b
+    recip_bytes = info["reciprocal_plane_evaluations"] * (W + 1) ** 2 * b
+    prep_bytes = info["candidates"] * SOURCES * 3 * (W + 1) ** 2 * b
+    out = {}
+    for name, ms, alg, traffic, what in (
+            ("k_sweep_tiled", sweep_ms, sweep_bytes, units * SWEEP_DRAM_BYTES_PER_UNIT,
+             "depth sweep, box-filtered ZNCC over 32x8-site tiles (plane-chunk merge included)"),
+            ("k_recip_sweep", recip_sweep_ms, recip_bytes, None,
+             "single-view reciprocal sweep, warp per pending pair, all three launches"),
+            ("k_recip_prepare", recip_prep_ms, prep_bytes, None,
+             "reciprocal prologue (direct cost, source contrast) and its pair list")):
+        achieved = alg / (ms / 1e3) / 1e9 if ms > 0 else 0.0
+        out[name] = {"bound": "hbm", "kernel": name, "what": what, "achieved": achieved,
+                     "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
+                     "algorithmic_bytes": alg, "ms_per_step": ms,
+                     "note": "achieved = unique texel bytes the kernel must read per step / its "
+                             "summed CUDA-event time; peak " + peak_note + "; the kernel is "
+                             "bound by instruction issue, its gathers hit L1/L2"}
+    return out
+
+
+def cost_error_vs_fp64(ctx, clip, frames, prof):
+    """The fast policy against the f64 oracle on one reference pass: hypothesis
+    agreement, cost error of the chosen hypotheses, and the attribution of every
+    differing site (tests/attribution.py).  The oracle is the checker here, not
+    the thing timed."""
+    from tests.attribution import attribute
+    from tests.oracle_ffi import Oracle
+    from v3d import abi, profiles
+    exact = profiles.with_precision(prof, abi.PRECISION_EXACT64)
+    o, rec = Oracle().explain_reference_patch(frames, clip.cameras, clip.sparse, clip.focal,
+                                              None, exact)
+    gs = ctx.debug_sweep(frames, clip.cameras, clip.sparse, clip.focal, profile=prof)
+    g = ctx.estimate_depth_points_with_control(frames, clip.cameras, clip.sparse, clip.focal,
+                                               profile=prof)
+    r = attribute(g, gs, o, rec, prof, 2 * COST_TOLERANCE)
+    return {"sites": r["sites"], "sampled": r["sampled"],
+            "plane_agreement": 1.0 - r["moved_fraction"],
+            "max_cost_error": r["max_cost_error"], "median_cost_error": r["median_cost_error"],
+            "cost_tolerance": COST_TOLERANCE, "gate_flips_in_band": r["gate_band"],
+            "reciprocal_argmin_moves": r["recip_moved"],
+            "points": len(g.points), "points_bit_identical": r["points_equal_bits"],
+            "points_compared": r["points_compared"], "unexplained": len(r["unexplained"])}
+
+
+def headline_cut(seed=21):
+    """The full clip's generator and camera spacing at 320x180 with 9 keyframes
+    (the middle one the reference, its 8 neighbours the sources): small enough for
+    the f64 oracle, with the headline's window, hypotheses and source count."""
+    from v3d import synth
+    return synth.make_clip(320, 180, 9, 2.7, 4.0, seed, noise_sigma=0.01, jitter_deg=2.0,
+                           landmark_cameras=[4], landmarks_per_camera=400)
 
 
 def load_clip(seed, frames):
@@ -279,8 +363,10 @@ def run_ours(args, rank, world, local):
     else:
         total_units = float(units)
     host = {k: float(np.mean([i[k] for i in infos]))
-            for k in ("host_plan_ms", "host_upload_ms", "host_wait_ms", "host_block_ms",
+            for k in ("host_plan_ms", "host_enqueue_ms", "host_wait_ms", "host_block_ms",
                       "host_readback_ms", "host_assemble_ms")}
+    recip_sweep_ms = float(np.mean([i["recip_sweep_ms"] for i in infos]))
+    recip_prep_ms = float(np.mean([i["recip_prepare_ms"] for i in infos]))
     sweep_ms = float(np.mean([i["sweep_ms"] for i in infos]))
     recip_ms = float(np.mean([i["reciprocal_ms"] for i in infos]))
     comp_ms = float(np.mean([i["completion_ms"] for i in infos]))
@@ -292,23 +378,19 @@ def run_ours(args, rank, world, local):
             peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
         except OSError:
             pass
-        hbm = peaks.get("hbm_gbs", 6650.0)
-        # the dominant stage and its algorithmic bytes per launch
+        hbm = peaks.get("hbm_gbs")
+        peak_note = "of measured (MEASURED_PEAKS.json hbm_gbs)"
+        if hbm is None:
+            hbm, peak_note = 6650.0, "of fallback (6.65 TB/s; MEASURED_PEAKS.json absent)"
         b = {"f32": 4, "f16": 2, "bf16": 2}[args.storage]
-        taps = (2 * RADIUS + 1) ** 2
-        stages = {"sweep": sweep_ms, "reciprocal": recip_ms}
-        dominant = max(stages, key=stages.get)
-        if dominant == "sweep":
-            alg_bytes = units * 4 * taps * b
-            kernel = "k_sweep_tiled (depth sweep, box-filtered ZNCC)"
-        else:
-            alg_bytes = infos[-1]["reciprocal_plane_evaluations"] * 4 * taps * b
-            kernel = "k_reciprocal (single-view reciprocal sweep)"
-        achieved = alg_bytes / (stages[dominant] / 1e3) / 1e9
+        kern = kernel_rooflines(infos[-1], units, b, sweep_ms, recip_sweep_ms, recip_prep_ms,
+                                hbm, peak_note)
+        order = sorted(kern, key=lambda k: kern[k]["ms_per_step"], reverse=True)
         line = {
             "metric": METRIC, "value": total_units / dev_s, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_s * 1e3,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": ARITH[args.storage],
             "data": "synthetic (seeded value-noise planes, ray-cast)", "config": workload(args),
             "clocks": clk,
             "e2e": {"value": total_units / wall_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
@@ -318,43 +400,22 @@ def run_ours(args, rank, world, local):
             "sweep_chunks": infos[-1]["sweep_chunks"],
             "stages_ms": {"sweep": sweep_ms, "reciprocal_primary": recip_ms,
                           "completion": comp_ms, "mesh": mesh_ms, "total": dev_s * 1e3,
-                          **host},
-            "roofline": {"bound": "hbm", "kernel": kernel, "achieved": achieved, "peak": hbm,
-                         "unit": "GB/s", "frac": achieved / hbm,
-                         "traffic": units * SWEEP_DRAM_BYTES_PER_UNIT if dominant == "sweep"
-                         else None,
-                         "algorithmic_bytes": alg_bytes,
-                         "note": "achieved = bilinear-footprint bytes 4*W^2*b per window "
-                                 "evaluation / kernel time, against the measured HBM copy peak "
-                                 "(of measured); the box filter shares each bilinear sample "
-                                 "among overlapping windows and the gathers are served by L1/L2, "
-                                 "so traffic (ncu DRAM bytes per launch, scaled by units from a "
-                                 "12-keyframe capture) is far below the algorithmic bytes and the "
-                                 "kernel is bound by SM instruction issue, not HBM"},
+                          "k_recip_sweep_all_launches": recip_sweep_ms,
+                          "k_recip_prepare_all_launches": recip_prep_ms, **host},
+            "roofline": kern[order[0]],
+            "roofline_runner_up": kern[order[1]],
             "points_per_step": points,
             "triangles_per_step": triangles,
         }
-        # the sweep's warped samples against the measured gather ceiling: a CTA
-        # warps its tile's footprint, PX x PY pixels, per (plane, source)
-        px = 31 * STRIDE + 2 * RADIUS + 1
-        py = 7 * STRIDE + 2 * RADIUS + 1
-        nx = (WIDTH - 2 * (RADIUS + 2) + STRIDE - 1) // STRIDE
-        ny = (HEIGHT - 2 * (RADIUS + 2) + STRIDE - 1) // STRIDE
-        tiles = ((nx + 31) // 32) * ((ny + 7) // 8)
-        samples = units * tiles * px * py / float(nx * ny)
-        rate = ctx.measure_gather_rate()
-        line["roofline_gather"] = {
-            "kernel": "k_sweep_tiled", "bound": "gather", "unit": "bilinear samples/s",
-            "achieved": samples / (sweep_ms / 1e3), "peak": rate,
-            "frac": samples / (sweep_ms / 1e3) / rate,
-            "note": "homography-warped f32 bilinear samples the depth sweep computes per second "
-                    "(each shared by the overlapping windows of its tile) against the rate a "
-                    "kernel doing only that step sustains on this GPU (v3d_measure_gather_rate); "
-                    "the rest of the sweep's time goes to its f64 box filters and ranking"}
         if world == 1 and not args.no_cpu_baseline:
             v, info = cpu_baseline(clip, frames, prof, os.cpu_count() or 1)
             line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": info["cores"],
                                     "kind": "port", "sample": info["sample"]}
+            cut = headline_cut()
+            err = cost_error_vs_fp64(ctx, cut, cut.frames(args.storage), prof)
+            err["sample"] = ("the headline generator at 320x180, 9 keyframes, the middle one "
+                             "the reference against the other 8, same profile and storage")
+            line["cost_error_vs_fp64"] = err
         print(json.dumps(line), flush=True)
     ctx.close()
     if dist:

@@ -241,7 +241,7 @@ int32_t v3d_last_run_info(const v3d_context* ctx, v3d_run_info* out) {
     out->reciprocal_plane_evaluations = ctx->last_recip_evals;
     out->candidates = ctx->last_candidates;
     out->host_plan_ms = ctx->last_plan_ms;
-    out->host_upload_ms = ctx->last_upload_ms;
+    out->host_enqueue_ms = ctx->last_enqueue_ms;
     out->host_wait_ms = ctx->last_wait_ms;
     out->host_assemble_ms = ctx->last_assemble_ms;
     out->mesh_ms = ctx->last_mesh_ms;
@@ -250,6 +250,8 @@ int32_t v3d_last_run_info(const v3d_context* ctx, v3d_run_info* out) {
     out->host_readback_ms = ctx->last_readback_ms;
     out->result_bytes = ctx->last_result_bytes;
     out->sweep_chunks = ctx->last_chunks;
+    out->recip_sweep_ms = ctx->last_recip_sweep_ms;
+    out->recip_prepare_ms = ctx->last_recip_prepare_ms;
     return V3D_OK;
 }
 

@@ -618,8 +618,9 @@ extern "C" int32_t v3d_mesh_verified_depth_grids(
     const uint32_t gh = (a.height + reference_stride - 1) / reference_stride;
     const uint64_t cells_patch = (uint64_t)gw * gh, slots_patch = mesh_slots(gw, gh);
     const uint64_t ncap = n_references * cells_patch, total_cells = ncap, total_slots = n_references * slots_patch;
-    if (ncap >= 0xFFFFFFFFull || 3 * total_slots >= (1ull << 34)) {
-        ctx->last_error = "the verified surface takes fewer than 2^32 samples and 2^33 triangle slots a call";
+    // the radix sorts take int item counts: samples (and so n_mesh <= ncap) stay below 2^31
+    if (ncap >= 0x7FFFFFFFull || 3 * total_slots >= (1ull << 34)) {
+        ctx->last_error = "the verified surface takes fewer than 2^31 samples and 2^33 triangle slots a call";
         return V3D_ERR_INVALID_ARGUMENT;
     }
     std::lock_guard<std::mutex> lock(ctx->mu);

@@ -238,8 +238,9 @@ struct v3d_context {
     uint64_t last_sites = 0;
     uint64_t last_units = 0;
     float last_sweep_ms = 0.f, last_recip_ms = 0.f, last_completion_ms = 0.f;
+    float last_recip_sweep_ms = 0.f, last_recip_prepare_ms = 0.f;
     uint64_t last_recip_evals = 0, last_candidates = 0;
-    double last_plan_ms = 0, last_upload_ms = 0, last_wait_ms = 0, last_assemble_ms = 0;
+    double last_plan_ms = 0, last_enqueue_ms = 0, last_wait_ms = 0, last_assemble_ms = 0;
     float last_mesh_ms = 0.f;
     uint64_t last_triangles = 0;
     double last_block_ms = 0, last_readback_ms = 0;

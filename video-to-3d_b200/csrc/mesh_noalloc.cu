@@ -39,6 +39,8 @@ cudaError_t scratch_address(void** out) {
     return cudaSuccess;
 }
 
+__global__ void k_put_patch(MeshPatchDev* dst, MeshPatchDev patch) { *dst = patch; }
+
 }  // namespace
 }  // namespace v3d
 
@@ -54,9 +56,10 @@ extern "C" int32_t v3d_mesh_patch_device_noalloc(
         !std::isfinite(focal) || focal <= 0.0 || n_points > 0xFFFFFFFFull)
         return V3D_ERR_INVALID_ARGUMENT;
     const uint32_t stride = static_cast<uint32_t>(grid_stride);
-    const uint32_t gw = width > 2 * grid_border ? (width - 2 * grid_border + stride - 1) / stride : 0;
-    const uint32_t gh =
-        height > 2 * grid_border ? (height - 2 * grid_border + stride - 1) / stride : 0;
+    // the border arithmetic in 64 bits: 2 * grid_border does not wrap
+    const uint64_t border2 = 2ull * grid_border;
+    const uint32_t gw = width > border2 ? (uint32_t)((width - border2 + stride - 1) / stride) : 0;
+    const uint32_t gh = height > border2 ? (uint32_t)((height - border2 + stride - 1) / stride) : 0;
     const uint64_t cells = static_cast<uint64_t>(gw) * gh;
     const uint64_t slots = mesh_slots(gw, gh);
     if (triangle_capacity < slots || (slots && !triangles_dev)) return V3D_ERR_INVALID_ARGUMENT;
@@ -82,9 +85,10 @@ extern "C" int32_t v3d_mesh_patch_device_noalloc(
     patch.slot_off = 0;
     patch.n_points = n_points;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    // a pageable source: the copy has read `patch` when the call returns
-    if (cudaMemcpyAsync(s.patches, &patch, sizeof(patch), cudaMemcpyHostToDevice, st) != cudaSuccess)
-        return V3D_ERR_CUDA;
+    // the descriptor travels as a kernel argument (copied at launch), not as a
+    // copy from this stack frame
+    k_put_patch<<<1, 1, 0, st>>>(s.patches, patch);
+    if (cudaGetLastError() != cudaSuccess) return V3D_ERR_CUDA;
     if (mesh_batch_enqueue(s, 1, cells, slots, points_dev, sites_dev, nullptr, nullptr, n_points,
                            triangles_dev, nullptr, st) != cudaSuccess)
         return V3D_ERR_CUDA;

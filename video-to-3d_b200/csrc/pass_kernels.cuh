@@ -179,6 +179,10 @@ struct RecipQueue {
     uint32_t* n_items;    // device count of listed items
     void* scratch;        // compaction_scratch_bytes(cap_items)
     uint64_t cap_items;
+    // optional timing marks, recorded on the stream before the prologue, before
+    // the single-view sweep and after it (the exact policy's one kernel counts as
+    // the sweep)
+    cudaEvent_t t_prepare = nullptr, t_sweep = nullptr, t_end = nullptr;
 };
 cudaError_t launch_reciprocal(const BatchDev& b, const Cand* cands, const uint32_t* count_dev,
                               uint64_t cap, RecipObs* obs, RefCounters* counters,

@@ -635,6 +635,17 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
     // stage events: sweep | primary reciprocal | completion passes
     cudaEvent_t es[8];
     for (auto& e : es) cudaEventCreate(&e);
+    // the reciprocal check's kernels, per launch (primary, completion 1, 2)
+    cudaEvent_t er[3][3];
+    for (auto& row : er)
+        for (auto& e : row) cudaEventCreate(&e);
+    auto timed_queue = [&](int i) {
+        RecipQueue q = P.queue;
+        q.t_prepare = er[i][0];
+        q.t_sweep = er[i][1];
+        q.t_end = er[i][2];
+        return q;
+    };
     // primary sweep, reciprocal check and fusion
     cudaEventRecord(es[0], stream);
     V3D_CK(launch_sweep_dispatch(b, d_siteref, total, max_nx, max_ny, stride0, tiled, d_rank,
@@ -643,7 +654,7 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
     V3D_CK(launch_compact(d_status, kSiteAccepted, total, d_idx, c_cand, d_scratch, stream));
     V3D_CK(launch_make_primary_cands(b, d_idx, c_cand, cap, d_siteref, d_rank, d_cands, stream));
     cudaEventRecord(es[2], stream);
-    V3D_CK(launch_reciprocal(b, d_cands, c_cand, cap, d_obs, d_ctr, P.queue, stream));
+    V3D_CK(launch_reciprocal(b, d_cands, c_cand, cap, d_obs, d_ctr, timed_queue(0), stream));
     cudaEventRecord(es[3], stream);
     V3D_CK(cudaMemsetAsync(d_cstat, 0, cap, stream));
     V3D_CK(launch_fuse(b, d_cands, c_cand, cap, d_obs, false, 0, d_fused, d_cstat, d_ctr, stream));
@@ -659,7 +670,8 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
                               d_idx, P.d_counts + 8, d_scratch, stream));
         V3D_CK(launch_compact(d_pstat, kPropCandidate, total, d_idx, c_cand, d_scratch, stream));
         V3D_CK(launch_gather_cands(d_idx, c_cand, cap, d_prop, d_cands, stream));
-        V3D_CK(launch_reciprocal(b, d_cands, c_cand, cap, d_obs, d_ctr, P.queue, stream));
+        V3D_CK(launch_reciprocal(b, d_cands, c_cand, cap, d_obs, d_ctr, timed_queue(pass + 1),
+                                 stream));
         V3D_CK(cudaMemsetAsync(d_cstat, 0, cap, stream));
         V3D_CK(launch_fuse(b, d_cands, c_cand, cap, d_obs, true, pass, d_fused, d_cstat, d_ctr,
                            stream));
@@ -738,7 +750,7 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
     ctx->last_launches = g_kernel_launches - launches0;
 
     // ---- read back ----
-    ctx->last_upload_ms = ms_since(t_upload);
+    ctx->last_enqueue_ms = ms_since(t_upload);
     const clk::time_point t_wait = clk::now();
     std::vector<RefCounters> ctr(n_active);
     std::vector<uint32_t> base(n_active + 1);
@@ -759,12 +771,22 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
     cudaEventElapsedTime(&ctx->last_sweep_ms, es[0], es[1]);
     if (P.tiled) sweep_chunks_record(P.shape, P.chunks, ctx->last_sweep_ms, ctx->last_units);
     cudaEventElapsedTime(&ctx->last_recip_ms, es[2], es[3]);
+    ctx->last_recip_sweep_ms = ctx->last_recip_prepare_ms = 0.f;
+    for (auto& row : er) {
+        float a = 0.f, c = 0.f;
+        cudaEventElapsedTime(&a, row[0], row[1]);
+        cudaEventElapsedTime(&c, row[1], row[2]);
+        ctx->last_recip_prepare_ms += a;
+        ctx->last_recip_sweep_ms += c;
+    }
     cudaEventElapsedTime(&ctx->last_completion_ms, es[4], es[5]);
     ctx->last_mesh_ms = 0.f;
     if (mesh) cudaEventElapsedTime(&ctx->last_mesh_ms, es[6], es[7]);
     cudaEventDestroy(ev0);
     cudaEventDestroy(ev1);
     for (auto& e : es) cudaEventDestroy(e);
+    for (auto& row : er)
+        for (auto& e : row) cudaEventDestroy(e);
     ctx->last_recip_evals = 0;
     ctx->last_candidates = 0;
     for (const RefCounters& c : ctr) {

@@ -487,8 +487,9 @@ extern "C" int32_t v3d_fuse_mutually_supported_vertices(
     std::memset(stats, 0, sizeof(*stats));
     *n_pairs = 0;
     *n_moved = 0;
-    if (n >= 0x40000000ull || nt >= 0x40000000ull) {
-        ctx->last_error = "surface fusion takes fewer than 2^30 points and 2^30 triangles";
+    // the sorts take int item counts, and a triangle has three incidence entries
+    if (n >= 0x40000000ull || nt > 0x7FFFFFFFull / 3) {
+        ctx->last_error = "surface fusion takes fewer than 2^30 points and 715,827,882 triangles";
         return V3D_ERR_INVALID_ARGUMENT;
     }
     std::lock_guard<std::mutex> lock(ctx->mu);

@@ -1284,6 +1284,10 @@ cudaError_t Typed<T>::reciprocal(const BatchDev& b, const Cand* cands, const uin
                                  cudaStream_t st) {
     using namespace typed_detail;
     const unsigned blocks = (unsigned)sm_count() * 8;
+    auto mark = [&](cudaEvent_t e) {
+        if (e) cudaEventRecord(e, st);
+    };
+    mark(q.t_prepare);
     // prologue, then the list of its pending items, then the sweep over the list
     auto prep_and_list = [&](auto prep) -> cudaError_t {
         cudaError_t e = cudaMemsetAsync(q.flags, 0, q.cap_items, st);
@@ -1295,18 +1299,22 @@ cudaError_t Typed<T>::reciprocal(const BatchDev& b, const Cand* cands, const uin
 #define V3D_REC(RR)                                                                            \
     if (b.prof.radius == RR) {                                                                 \
         if (b.exact) {                                                                         \
+            mark(q.t_sweep);                                                                   \
             V3D_COUNTED k_reciprocal_exact<T, RR><<<blocks, 256, 0, st>>>(b, cands, count, obs, ctr);      \
         } else if (b.prof.cost == 1) {                                                         \
             const cudaError_t e = prep_and_list(k_recip_prepare<T, RR, 1>);                    \
             if (e != cudaSuccess) return e;                                                    \
+            mark(q.t_sweep);                                                                   \
             V3D_COUNTED k_recip_sweep<T, RR, 1><<<blocks, 256, 0, st>>>(b, cands, q.items,     \
                                                                         q.n_items, obs);       \
         } else {                                                                               \
             const cudaError_t e = prep_and_list(k_recip_prepare<T, RR, 0>);                    \
             if (e != cudaSuccess) return e;                                                    \
+            mark(q.t_sweep);                                                                   \
             V3D_COUNTED k_recip_sweep<T, RR, 0><<<blocks, 256, 0, st>>>(b, cands, q.items,     \
                                                                         q.n_items, obs);       \
         }                                                                                      \
+        mark(q.t_end);                                                                         \
         return cudaGetLastError();                                                             \
     }
     V3D_REC(1) V3D_REC(2) V3D_REC(3) V3D_REC(4)
