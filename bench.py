@@ -59,11 +59,14 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--storage", choices=["f32", "f16", "bf16"], default="f32")
+    ap.add_argument("--precision", choices=["fast32", "sums32"], default="fast32",
+                    help="fast32: f32 taps, the depth sweep's box sums in f64 (default); "
+                         "sums32: those sums in f32 as well")
     ap.add_argument("--frames", type=int, default=FRAMES)
     ap.add_argument("--no-cpu-baseline", action="store_true",
                     help="skip the CPU baseline leg (profiling runs)")
     ap.add_argument("--config", choices=["full", "small", "heavy", "batched", "served", "fusion",
-                                         "verify", "artifact", "colmap"],
+                                         "verify", "artifact", "colmap", "refprofile"],
                     default="full",
                     help="full: the headline line (default); small: 360x202 1+4 views; heavy: "
                          "bf16 16 views 256 planes 9x9; batched: 32 uneven clips through the "
@@ -71,7 +74,9 @@ def parse():
                          "fusion: cross-reference surface fusion of the full clip's patches; "
                          "verify: geometric depth-grid verification of the full clip; "
                          "artifact: the full clip's dense evidence as artifact JSON + SHA-256; "
-                         "colmap: verification, meshing, re-indexing and topology of the full clip")
+                         "colmap: verification, meshing, re-indexing and topology of the full "
+                         "clip; refprofile: the full clip in the reference's own profile (RGBA, "
+                         "3x3 ZSAD, 24 planes, 4 views, exact f64)")
     ap.add_argument("--rates", default="50,200,800", help="served: request rates (req/s)")
     ap.add_argument("--duration", type=float, default=3.0, help="served: seconds of arrivals")
     ap.add_argument("--clips", type=int, default=32, help="batched/served: number of clips")
@@ -95,7 +100,7 @@ def workload(args):
                                        2 * RADIUS + 1, 2 * RADIUS + 1, STRIDE, args.storage),
             "width": WIDTH, "height": HEIGHT, "keyframes": args.frames, "source_views": SOURCES,
             "planes": PLANES, "window": 2 * RADIUS + 1, "grid_stride": STRIDE,
-            "storage": args.storage, "cost": "1-ZNCC",
+            "storage": args.storage, "cost": "1-ZNCC", "precision": args.precision,
             "l2": "flushed between timed steps (256 MiB write)",
             "parallelism": "weak: one clip per GPU, no collective on the data path"}
 
@@ -167,6 +172,14 @@ def cost_error_vs_fp64(ctx, clip, frames, prof):
             "reciprocal_argmin_moves": r["recip_moved"],
             "points": len(g.points), "points_bit_identical": r["points_equal_bits"],
             "points_compared": r["points_compared"], "unexplained": len(r["unexplained"])}
+
+
+def headline_profile(args, radius=RADIUS, planes=PLANES, sources=SOURCES):
+    """The benchmark's ZNCC profile under the chosen arithmetic policy."""
+    from v3d import abi, profiles
+    return profiles.zncc(radius, planes, sources, STRIDE,
+                         precision={"fast32": abi.PRECISION_FAST32,
+                                    "sums32": abi.PRECISION_FAST32_SUMS32}[args.precision])
 
 
 def headline_cut(seed=21):
@@ -277,7 +290,7 @@ def run_reference(args, rank, world):
     from v3d import profiles
     clip = load_clip(2, args.frames)
     frames = clip.frames(args.storage)
-    prof = profiles.zncc(RADIUS, PLANES, SOURCES, STRIDE)
+    prof = headline_profile(args)
     threads = os.cpu_count() or 1
     vals = []
     for i in range(args.warmup + args.steps):
@@ -319,7 +332,7 @@ def run_ours(args, rank, world, local):
         pinned.append((t, FrameInput(t.numpy().view(fi.pixels.dtype), bf16=fi.bf16)))
     frames = [p[1] for p in pinned]
     h2d = sum(f.pixels.nbytes for f in frames)
-    prof = profiles.zncc(RADIUS, PLANES, SOURCES, STRIDE)
+    prof = headline_profile(args)
     ctx = dense.Context(local)
     refs = list(range(args.frames))
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
@@ -504,7 +517,7 @@ def run_batched(args):
     (all requests queued at once) against the plain per-request kernel."""
     from v3d import profiles
     clips = batched_clips(args.clips)
-    prof = profiles.zncc(RADIUS, PLANES, SOURCES, STRIDE)
+    prof = headline_profile(args)
     reqs = [(ci, cam, spec["planes"], spec["sources"])
             for ci, (spec, c) in enumerate(clips) for cam in range(len(c.cameras))]
     forms = {}
@@ -523,7 +536,24 @@ def run_batched(args):
                 "references": len(reqs)},
             "batched": forms["batched"], "plain_per_request": forms["plain"],
             "batched_over_plain": forms["batched"]["units_per_s"] / forms["plain"]["units_per_s"]}
+    if not args.no_cpu_baseline:
+        line["cost_error_vs_fp64"] = uneven_clip_cost_error(args, clips)
     print(json.dumps(line), flush=True)
+
+
+def uneven_clip_cost_error(args, clips):
+    """The fast policy against the f64 oracle on the smallest of the uneven clips,
+    with its own hypothesis and source counts (the legacy pass's reference)."""
+    from v3d import dense
+    spec, clip = min(clips, key=lambda sc: sc[1].width * len(sc[1].cameras))
+    prof = headline_profile(args, RADIUS, spec["planes"], spec["sources"])
+    ctx = dense.Context(0)
+    err = cost_error_vs_fp64(ctx, clip, clip.frames(args.storage), prof)
+    ctx.close()
+    err["sample"] = ("uneven clip %dx%d, %d frames, %d planes, %d sources: the legacy pass's "
+                     "reference" % (clip.width, clip.height, len(clip.cameras), spec["planes"],
+                                    spec["sources"]))
+    return err
 
 
 def run_served(args):
@@ -533,7 +563,7 @@ def run_served(args):
     per-request kernel, p50/p99 latency and throughput per rate."""
     from v3d import profiles
     clips = batched_clips(args.clips)
-    prof = profiles.zncc(RADIUS, PLANES, SOURCES, STRIDE)
+    prof = headline_profile(args)
     rates = [float(r) for r in args.rates.split(",")]
     plans = {}
     for rate in rates:
@@ -560,65 +590,163 @@ def run_served(args):
                             "7x7 ZNCC, stride 2, %s images, frames resident in HBM"
                             % (args.duration, len(clips), args.storage), "rates": rates},
             "served": out["served"], "plain_per_request": out["plain"]}
+    if not args.no_cpu_baseline:
+        line["cost_error_vs_fp64"] = uneven_clip_cost_error(args, clips)
     print(json.dumps(line), flush=True)
-
-
-def _cost_error(ctx, oracle, clip, frames, prof):
-    """Chosen-hypothesis agreement and cost error of the fast policy against the
-    f64 oracle, over every grid site of the legacy pass's reference."""
-    from v3d import abi, profiles
-    exact = profiles.with_precision(prof, abi.PRECISION_EXACT64)
-    g = ctx.debug_sweep(frames, clip.cameras, clip.sparse, clip.focal, profile=prof)
-    o = oracle.debug_sweep(frames, clip.cameras, clip.sparse, clip.focal, profile=exact)
-    both = (g["status"] >= 3) & (o["status"] >= 3)
-    same = both & (g["plane"] == o["plane"])
-    err = np.abs(g["error"][same] - o["error"][same])
-    return {"sites": int(len(g)), "plane_agreement": float(same.sum() / max(1, both.sum())),
-            "max_cost_error": float(err.max()) if err.size else 0.0,
-            "median_cost_error": float(np.median(err)) if err.size else 0.0}
 
 
 def run_plain_config(args):
     """Config 1 (small) or 5 (heavy) as a plain clip run, plus the fast policy's
-    cost error against the f64 oracle (for heavy on a 200x112 cut of the same
-    generator and profile, where the oracle finishes in seconds)."""
-    from tests.oracle_ffi import Oracle
-    from v3d import dense, profiles, synth
+    cost error against the f64 oracle (heavy: on a 224x126 cut of the same
+    generator and keyframe spacing, 16 sources for the middle keyframe, where
+    the oracle finishes in seconds)."""
+    import torch
+    from v3d import dense, synth
     if args.config == "small":
         clip = synth.plain_small_clip(seed=1)
-        storage = "f32" if args.storage == "f32" else args.storage
-        prof = profiles.zncc(2, 64, 4, 2)
+        storage = args.storage
+        prof = headline_profile(args, 2, 64, 4)
         refs = [2]
-        check_clip, name = clip, "plain small 360x202, 1 reference + 4 source views, 64 planes, 5x5 ZNCC, stride 2"
+        check_clip, name = clip, ("plain small 360x202, 1 reference + 4 source views, 64 planes, "
+                                  "5x5 ZNCC, stride 2")
     else:
         clip = synth.heavy_clip(seed=5, n_frames=args.frames)
         storage = "bf16" if args.storage == "f32" else args.storage
-        prof = profiles.zncc(4, 256, 16, 2)
+        prof = headline_profile(args, 4, 256, 16)
         refs = list(range(len(clip.cameras)))
-        check_clip = synth.make_clip(200, 112, 12, 40.0, 4.0, 5, noise_sigma=0.02, jitter_deg=2.0,
-                                     extra_planes=4, boxes=4, low_texture_fraction=0.05)
+        check_clip = synth.make_clip(224, 126, 17, 5.4, 4.0, 25, noise_sigma=0.02,
+                                     jitter_deg=2.0, extra_planes=4, boxes=4,
+                                     low_texture_fraction=0.05, landmark_cameras=[8],
+                                     landmarks_per_camera=400)
         name = ("heavy 640x360, %d keyframes, 16 source views, 256 planes, 9x9 ZNCC, stride 2, "
                 "8 planes + 4 boxes, 5%% low texture, noise 0.02" % len(clip.cameras))
     frames = clip.frames(storage)
     ctx = dense.Context(0)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     dev, wall = [], []
+    clocks = Clocks(0)
     for i in range(args.warmup + args.steps):
+        if i == args.warmup:
+            clocks.start()
+        flush.zero_()
+        torch.cuda.synchronize()
         t0 = time.perf_counter()
-        ctx.reconstruct_reference_patches_meshed(frames, clip.cameras, clip.sparse, clip.focal,
-                                                 refs, profile=prof)
+        res = ctx.reconstruct_reference_patches_meshed(frames, clip.cameras, clip.sparse,
+                                                       clip.focal, refs, profile=prof)
         w = time.perf_counter() - t0
         info = ctx.last_run_info()
         if i >= args.warmup:
             dev.append(info["device_ms"] / 1e3)
             wall.append(w)
+    clk = clocks.stop()
     units = info["plane_view_units"]
-    err = _cost_error(ctx, Oracle(), check_clip, check_clip.frames(storage), prof)
-    line = {"metric": METRIC, "value": units / float(np.mean(dev)), "unit": UNIT,
-            "e2e": units / float(np.mean(wall)), "ms_per_step": float(np.mean(dev)) * 1e3,
-            "steps": args.steps, "warmup": args.warmup, "dtype": storage,
-            "config": {"workload": name + ", %s images" % storage, "units_per_step": units},
-            "cost_error_vs_fp64": err}
+    points = sum(len(r[0].points) for r in res if r is not None)
+    triangles = sum(len(r[1].triangles) for r in res if r is not None)
+    line = {"metric": METRIC, "value": units / float(np.mean(dev)), "unit": UNIT, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.mean(dev)) * 1e3,
+            "higher_is_better": True, "vs_baseline": None, "dtype": ARITH[storage],
+            "data": "synthetic (seeded value-noise planes, ray-cast)",
+            "config": {"workload": name + ", %s images" % storage, "units_per_step": units,
+                       "precision": args.precision,
+                       "l2": "flushed between timed steps (256 MiB write)"},
+            "clocks": clk,
+            "e2e": {"value": units / float(np.mean(wall)), "unit": UNIT,
+                    "h2d_bytes_per_step": sum(f.pixels.nbytes for f in frames),
+                    "d2h_bytes_per_step": points * 72 + triangles * 32,
+                    "ms_per_step": float(np.mean(wall)) * 1e3},
+            "gpu_launches": int(info["kernel_launches"]),
+            "stages_ms": {"sweep": info["sweep_ms"], "k_recip_sweep_all_launches":
+                          info["recip_sweep_ms"], "k_recip_prepare_all_launches":
+                          info["recip_prepare_ms"], "mesh": info["mesh_ms"]}}
+    if not args.no_cpu_baseline:
+        err = cost_error_vs_fp64(ctx, check_clip, check_clip.frames(storage), prof)
+        err["sample"] = ("the same clip's reference" if args.config == "small" else
+                         "224x126 cut of the heavy generator, 17 keyframes at the clip's spacing, "
+                         "the middle one against the other 16")
+        line["cost_error_vs_fp64"] = err
     print(json.dumps(line), flush=True)
+
+
+def run_refprofile(args):
+    """The full clip in the reference's own profile (dense_legacy.rs:6-21): RGBA8
+    frames, u8 luma, 3x3 ZSAD, 24 hypotheses, at most 4 sources, the reference's
+    grid stride (7 at 640x360), exact f64 taps; every keyframe a reference, with
+    completion and the grid-mesh gates, bit-identical to the oracle (checked on
+    three references).  Timed beside the oracle port on all host threads."""
+    import torch
+    from tests.oracle_ffi import Oracle
+    from v3d import dense, profiles
+    clip = load_clip(2, args.frames)
+    frames = [pinned_frame(f) for f in clip.frames("rgba8")]
+    prof = profiles.reference()
+    refs = list(range(args.frames))
+    ctx = dense.Context(0)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    dev, wall = [], []
+    clocks = Clocks(0)
+    for i in range(args.warmup + args.steps):
+        if i == args.warmup:
+            clocks.start()
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = ctx.reconstruct_reference_patches_meshed(frames, clip.cameras, clip.sparse,
+                                                       clip.focal, refs, profile=prof)
+        w = time.perf_counter() - t0
+        info = ctx.last_run_info()
+        if i >= args.warmup:
+            dev.append(info["device_ms"] / 1e3)
+            wall.append(w)
+    clk = clocks.stop()
+    units = info["plane_view_units"]
+    points = sum(len(r[0].points) for r in res if r is not None)
+    triangles = sum(len(r[1].triangles) for r in res if r is not None)
+    line = {"metric": METRIC, "value": units / float(np.mean(dev)), "unit": UNIT, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.mean(dev)) * 1e3,
+            "higher_is_better": True, "vs_baseline": None, "dtype": "f64 (u8 luma)",
+            "data": "synthetic (seeded value-noise planes, ray-cast), RGBA8",
+            "config": {"workload": "full native clip %dx%d, %d keyframes, the reference profile: "
+                                   "3x3 ZSAD, 24 planes, 4 views, grid stride 7, exact f64, "
+                                   "completion and grid-mesh gates" % (WIDTH, HEIGHT, args.frames),
+                       "units_per_step": units, "l2": "flushed between timed steps (256 MiB write)"},
+            "clocks": clk,
+            "e2e": {"value": units / float(np.mean(wall)), "unit": UNIT,
+                    "h2d_bytes_per_step": sum(f.pixels.nbytes for f in frames),
+                    "d2h_bytes_per_step": points * 72 + triangles * 32,
+                    "ms_per_step": float(np.mean(wall)) * 1e3},
+            "gpu_launches": int(info["kernel_launches"]),
+            "stages_ms": {"sweep": info["sweep_ms"], "reciprocal_all_launches":
+                          info["recip_sweep_ms"] + info["recip_prepare_ms"],
+                          "mesh": info["mesh_ms"]}}
+    if not args.no_cpu_baseline:
+        o = Oracle()
+        check = [0, args.frames // 2, args.frames - 1]
+        g = ctx.reconstruct_reference_patches(frames, clip.cameras, clip.sparse, clip.focal,
+                                              check, profile=prof)
+        t0 = time.perf_counter()
+        threads = os.cpu_count() or 1
+        sample = list(range(min(args.frames, max(threads, 8))))
+        o.reconstruct_reference_patches(frames, clip.cameras, clip.sparse, clip.focal, sample,
+                                        prof, threads=threads)
+        cpu_s = time.perf_counter() - t0
+        ob = o.reconstruct_reference_patches(frames, clip.cameras, clip.sparse, clip.focal,
+                                             check, prof, threads=3)
+        same = all((a is None and b is None) or (a is not None and b is not None and
+                                                 a.points.tobytes() == b.points.tobytes() and
+                                                 dict(a.stats) == dict(b.stats))
+                   for a, b in zip(g, ob))
+        line["bitwise_vs_oracle"] = {"references": check, "identical": bool(same)}
+        line["cpu_baseline"] = {"value": units * len(sample) / args.frames / cpu_s, "unit": UNIT,
+                                "cores": threads, "kind": "port",
+                                "sample": "the first %d references, whole passes with completion, "
+                                          "OpenMP over references" % len(sample)}
+    ctx.close()
+    print(json.dumps(line), flush=True)
+
+
+def pinned_frame(f):
+    from v3d.types import FrameInput
+    return FrameInput(pinned(f.pixels), bf16=f.bf16)
 
 
 def run_fusion(args):
@@ -630,7 +758,7 @@ def run_fusion(args):
     from v3d import dense, profiles, surface
     clip = load_clip(2, args.frames)
     frames = clip.frames(args.storage)
-    prof = profiles.zncc(RADIUS, PLANES, SOURCES, STRIDE)
+    prof = headline_profile(args)
     ctx = dense.Context(0)
     res = ctx.reconstruct_reference_patches_meshed(frames, clip.cameras, clip.sparse, clip.focal,
                                                    list(range(args.frames)), profile=prof)
@@ -911,7 +1039,7 @@ def run_artifact(args):
     from v3d import dense, profiles, types
     clip = load_clip(2, args.frames)
     frames = clip.frames(args.storage)
-    prof = profiles.zncc(RADIUS, PLANES, SOURCES, STRIDE)
+    prof = headline_profile(args)
     ctx = dense.Context(0)
     res = ctx.reconstruct_reference_patches(frames, clip.cameras, clip.sparse, clip.focal,
                                             list(range(args.frames)), profile=prof)
@@ -1008,6 +1136,8 @@ def main():
         run_artifact(args)
     elif args.config == "colmap":
         run_colmap(args)
+    elif args.config == "refprofile":
+        run_refprofile(args)
     else:
         run_ours(args, rank, world, local)
 

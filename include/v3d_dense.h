@@ -123,7 +123,11 @@ typedef enum v3d_cost {
 
 typedef enum v3d_precision {
     V3D_PRECISION_EXACT64 = 0,/* every tap in f64 with the reference's unproject/project formulas */
-    V3D_PRECISION_FAST32 = 1  /* per-plane homographies composed in f64, taps and sums in f32 */
+    V3D_PRECISION_FAST32 = 1, /* per-plane homographies composed in f64, taps in f32; the
+                               * box-filtered depth sweep forms its window sums in f64, every
+                               * other window cost sums in f32 */
+    V3D_PRECISION_FAST32_SUMS32 = 2 /* FAST32 with the box-filtered sweep's window sums in
+                                     * f32 too, on values shifted by the tile's centre texel */
 } v3d_precision;
 
 /* Hot-path constants.  v3d_profile_reference() fills dense_legacy.rs:6-21;

@@ -487,13 +487,16 @@ int32_t v3do_debug_sweep(const v3d_frame* frames, uint64_t n_frames, const v3d_c
 // runs it), or with camera_index == UINT64_MAX the legacy single call (as
 // v3do_estimate_depth_points_with_control runs it), together with its
 // ExplainRecords (oracle.hpp): primary sites in raster order, then each
-// completion pass's proposals.  *records is malloc'd; free it with v3do_free.
-// Returns V3D_SKIPPED (and no result) where the pass does not run.
+// completion pass's proposals.  row_end > row_begin restricts the pass to
+// those grid rows (primaries only, no completion, as the CPU-baseline bands
+// run).  *records is malloc'd; free it with v3do_free.  Returns V3D_SKIPPED
+// (and no result) where the pass does not run.
 int32_t v3do_explain_reference_patch(const v3d_frame* frames, uint64_t n_frames,
                                      const v3d_camera* cams, uint64_t n_cams,
                                      const double* sparse, uint64_t n_sparse, double focal,
                                      int32_t fine_grid, const v3d_profile* profile,
-                                     uint64_t camera_index, v3d_dense_result* out,
+                                     uint64_t camera_index, uint32_t row_begin,
+                                     uint32_t row_end, v3d_dense_result* out,
                                      ExplainRecord** records, uint64_t* n_records) {
     static_assert(sizeof(ExplainRecord) == 56, "ExplainRecord layout");
     *records = nullptr;
@@ -504,17 +507,21 @@ int32_t v3do_explain_reference_patch(const v3d_frame* frames, uint64_t n_frames,
     auto s = load_sparse(sparse, n_sparse);
     Control ctl;
     std::vector<ExplainRecord> rec;
+    RowBand band;
+    band.begin = row_begin;
+    band.end = row_end;
+    const RowBand* bp = row_end > row_begin ? &band : nullptr;
     try {
         std::optional<LegacyAnalysis> a;
         if (camera_index == UINT64_MAX) {
             std::vector<const Frame*> ptrs;
             for (const Frame& x : f) ptrs.push_back(&x);
             a = estimate_depth_points_ptr(Profile::from_c(*profile), ptrs, c, s, focal,
-                                          fine_grid != 0, ctl, nullptr, nullptr, &rec);
-            if (!a->stats.attempted) return V3D_SKIPPED;
+                                          fine_grid != 0, ctl, nullptr, bp, &rec);
+            if (!bp && !a->stats.attempted) return V3D_SKIPPED;
         } else {
             a = reconstruct_reference_patch(Profile::from_c(*profile), f, c, s, focal,
-                                            camera_index, fine_grid != 0, ctl, nullptr, &rec);
+                                            camera_index, fine_grid != 0, ctl, bp, &rec);
         }
         if (!a) return V3D_SKIPPED;
         fill_legacy(out, *a);

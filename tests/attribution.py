@@ -42,12 +42,18 @@ def _key(x, y):
     return (int(x), int(y))
 
 
-def attribute(g, g_sweep, o, o_rec, prof, band):
+def attribute(g, g_sweep, o, o_rec, prof, band, rows=None):
     """g / o: the device and oracle analyses of one pass (points in the
     reference's order: primaries, then completions); g_sweep: the device's
     per-site sweep records; o_rec: the oracle's decision records of the same
-    pass.  Returns a report; ``report["unexplained"]`` lists the sites no rule
-    covers."""
+    pass.  rows=(a, b): the oracle ran grid rows a..b-1 only (primaries, no
+    completion); the device's full pass is compared on those rows.  Returns a
+    report; ``report["unexplained"]`` lists the sites no rule covers."""
+    y_lo, y_hi = 0, 1 << 62
+    if rows is not None:
+        border, stride = int(g.stats["grid_border"]), int(g.stats["grid_stride"])
+        y_lo, y_hi = border + rows[0] * stride, border + rows[1] * stride
+        g_sweep = g_sweep[(g_sweep["y"] >= y_lo) & (g_sweep["y"] < y_hi)]
     thr_e, thr_m = prof.max_photometric_error, prof.min_ambiguity_margin
     prim = o_rec[o_rec["stage"] == 0]
     comp = o_rec[o_rec["stage"] > 0]
@@ -99,17 +105,21 @@ def attribute(g, g_sweep, o, o_rec, prof, band):
         rep["median_cost_error"] = float(np.median(errs))
     # ---- points --------------------------------------------------------------
     n_gp = g.stats["accepted_points"]
-    n_op = o.stats["accepted_points"]
+    n_op = o.stats["accepted_points"] if rows is None else len(o.points)
 
     def table(a, lo, hi):
         t = {}
         for i in range(lo, hi):
             s = a.grid_sites[i]
-            t[_key(s["x"], s["y"])] = i
+            if y_lo <= int(s["y"]) < y_hi:
+                t[_key(s["x"], s["y"])] = i
         return t
 
     gpt, opt = table(g, 0, n_gp), table(o, 0, n_op)
-    gct, oct_ = table(g, n_gp, len(g.points)), table(o, n_op, len(o.points))
+    if rows is None:
+        gct, oct_ = table(g, n_gp, len(g.points)), table(o, n_op, len(o.points))
+    else:
+        gct, oct_ = {}, {}  # the band ran no completion
 
     def differs(i, j):
         gp = np.array([g.points[i][c] for c in "xyz"], np.float64)

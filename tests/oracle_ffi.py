@@ -233,17 +233,18 @@ class Oracle:
         return res
 
     def explain_reference_patch(self, frames, cameras, sparse_points, focal, camera_index,
-                                profile, fine_grid=False):
+                                profile, fine_grid=False, rows=None):
         """The remapped pass of one reference (camera_index None: the legacy
         single call) and its decision records (ExplainRecord in
         oracle/oracle.hpp): primary sites in raster order, then the completion
-        proposals of each pass.  None where the pass does not run."""
+        proposals of each pass.  None where the pass does not run.  rows=(a, b):
+        only grid rows a..b-1, primaries only (no completion)."""
         L = self.lib
         if not getattr(self, "_explain_bound", False):
             L.v3do_explain_reference_patch.argtypes = [
                 _P(abi.Frame), C.c_uint64, _P(abi.Camera), C.c_uint64, _P(C.c_double), C.c_uint64,
-                C.c_double, C.c_int32, _P(abi.Profile), C.c_uint64, _P(abi.DenseResult),
-                _P(C.c_void_p), _P(C.c_uint64)]
+                C.c_double, C.c_int32, _P(abi.Profile), C.c_uint64, C.c_uint32, C.c_uint32,
+                _P(abi.DenseResult), _P(C.c_void_p), _P(C.c_uint64)]
             L.v3do_explain_reference_patch.restype = C.c_int32
             L.v3do_free.argtypes = [C.c_void_p]
             self._explain_bound = True
@@ -253,7 +254,8 @@ class Oracle:
         st = L.v3do_explain_reference_patch(
             inp.frames, inp.n_frames, inp.cameras, inp.n_cameras, inp.sparse, inp.n_sparse,
             float(focal), int(fine_grid), C.byref(profile),
-            (1 << 64) - 1 if camera_index is None else int(camera_index), C.byref(out),
+            (1 << 64) - 1 if camera_index is None else int(camera_index),
+            rows[0] if rows else 0, rows[1] if rows else 0, C.byref(out),
             C.byref(recs), C.byref(n))
         if st < 0:
             raise ValueError("oracle rejected the inputs (status %d)" % st)

@@ -239,3 +239,29 @@ def test_fast_points(ctx, oracle, prof_of, storage):
     op = np.stack([o.points[[ok[k] for k in common]][c] for c in "xyz"], -1).astype(np.float64)
     rel = np.linalg.norm(gp - op, axis=1) / np.linalg.norm(op, axis=1)
     assert (rel <= FAST_TOL).mean() >= 0.995, (rel <= FAST_TOL).mean()
+
+
+# ---- the reference profile at the configurations' frame sizes ---------------
+
+@pytest.mark.parametrize("size", ["360x202", "640x360"])
+def test_reference_profile_at_config_sizes(ctx, oracle, size):
+    """The reference's own profile (3x3 ZSAD on u8 luma, 24 hypotheses, at most
+    4 sources, grid_stride(): 4 at 360x202, 7 at 640x360; dense_legacy.rs:6-21,
+    dense.rs:215-218) on RGBA frames of the small configuration's generator at
+    its size and at the full clip's size: bit-identical to the oracle,
+    statistics included."""
+    w, h = map(int, size.split("x"))
+    clip, refs = synth.plain_small_clip(seed=1, width=w, height=h), [0, 2, 4]
+    frames = clip.frames("rgba8")
+    prof = profiles.reference()
+    g = ctx.reconstruct_reference_patches(frames, clip.cameras, clip.sparse, clip.focal, refs,
+                                          profile=prof)
+    o = oracle.reconstruct_reference_patches(frames, clip.cameras, clip.sparse, clip.focal, refs,
+                                             prof, threads=3)
+    for a, b in zip(g, o):
+        assert (a is None) == (b is None)
+        if a is not None:
+            assert_same_analysis(a, b)
+            check_reference_assertions(a)
+    assert g[0] is not None and len(g[0].points) > 200
+    assert g[0].stats["grid_stride"] == (4 if size == "360x202" else 7)

@@ -52,7 +52,8 @@ bool valid_profile(const v3d_profile* p) {
            p->patch_radius <= V3D_MAX_PATCH_RADIUS && p->depth_hypotheses >= 2 &&
            p->depth_hypotheses <= V3D_MAX_DEPTH_HYPOTHESES && p->max_source_views >= 1 &&
            p->max_source_views <= V3D_MAX_SOURCE_VIEWS && p->grid_stride >= 0 &&
-           (p->precision == V3D_PRECISION_EXACT64 || p->precision == V3D_PRECISION_FAST32) &&
+           (p->precision == V3D_PRECISION_EXACT64 || p->precision == V3D_PRECISION_FAST32 ||
+            p->precision == V3D_PRECISION_FAST32_SUMS32) &&
            p->error_confidence_scale > 0 && p->depth_margin_saturation > 0;
 }
 

@@ -108,6 +108,7 @@ struct BatchDev {
     int32_t storage;            // StorageFormat
     DevProfile prof;
     bool exact;
+    bool sums32;                // the box-filtered sweep's window sums in f32
 };
 
 // Launch wrappers (pass_kernels.cu).  All run on `stream`; none synchronises.

@@ -484,6 +484,7 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
     b.prof.error_scale = prof.error_confidence_scale;
     b.prof.min_variance = prof.min_window_variance;
     b.exact = prof.precision == V3D_PRECISION_EXACT64;
+    b.sums32 = prof.precision == V3D_PRECISION_FAST32_SUMS32;
 
     P.stride0 = plans[active[0]].stride;
     return V3D_OK;

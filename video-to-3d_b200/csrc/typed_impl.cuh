@@ -329,8 +329,11 @@ __host__ __device__ constexpr int tiled_steps(int np) { return (np + 2 * kTileTh
 // bilinear), then forms the window sums of s, s^2 and r*s with separable box
 // filters, so overlapping windows (stride < window) share every bilinear
 // sample.  Products and sums are formed in f64: s^2 - (sum s)^2/n cancels
-// badly in f32 on low-variance windows.  Invalid taps are NaN and poison
-// their windows, which reproduces the reference's all-taps-valid rule.
+// badly in f32 on low-variance windows (Acc = double; with Acc = float, the
+// FAST32_SUMS32 policy, the sums are f32 on values shifted by the tile's
+// centre reference texel, which keeps the shifted values near the windows'
+// means).  Invalid taps are NaN and poison their windows, which reproduces
+// the reference's all-taps-valid rule.
 //
 // The footprint rows in shared memory keep their columns grouped by x mod
 // stride (column x at slot (x % s) * PXs + x / s), so the stride-s reads of
@@ -341,7 +344,7 @@ __host__ __device__ constexpr int tiled_steps(int np) { return (np + 2 * kTileTh
 // row ends.  When the footprint's image in a source lies inside that image
 // (tested once per plane and source on the rectangle's corners), the step
 // skips the per-sample domain tests.
-template <class T, int R>
+template <class T, int R, class Acc>
 __global__ void __launch_bounds__(kTileThreads, 1024 / kTileThreads) k_sweep_tiled(BatchDev b, uint64_t total_sites,
                                                      SiteRank* __restrict__ rank,
                                                      uint8_t* __restrict__ status,
@@ -364,9 +367,9 @@ __global__ void __launch_bounds__(kTileThreads, 1024 / kTileThreads) k_sweep_til
     const int PXs = (PX + s - 1) / s, PXp = PXs * s;  // columns per residue, padded row
     const int np = PY * PXp;
     const int ms = b.max_src;
-    double* hs = smem_d;                     // [PY][32] row sums of s
-    double* hss = hs + PY * kTileX;          // [PY][32] row sums of s^2
-    double* hrs = hss + PY * kTileX;         // [PY][32] row sums of r*s
+    Acc* hs = reinterpret_cast<Acc*>(smem_d);  // [PY][32] row sums of s
+    Acc* hss = hs + PY * kTileX;               // [PY][32] row sums of s^2
+    Acc* hrs = hss + PY * kTileX;              // [PY][32] row sums of r*s
     float* refv = reinterpret_cast<float*>(hrs + PY * kTileX);  // [PY][PXp] reference values
     float* samp = refv + np;                 // [PY][PXp] source samples (NaN = invalid)
     float* costs = samp + np;                // [max_src][kTileThreads]
@@ -469,6 +472,18 @@ __global__ void __launch_bounds__(kTileThreads, 1024 / kTileThreads) k_sweep_til
     const double minvar_n = prof.min_variance * n;
     const bool vr_ok = vr > 0.0 && vr >= minvar_n;
     const float vr_f = (float)vr;
+    // f32 sums: every value shifted by the centre texel of the tile's middle
+    // active site (cov and var are shift-invariant; the site is inside the
+    // grid, so the texel is a pixel of the image); f64 sums: no shift
+    constexpr bool kF32 = sizeof(Acc) == 4;
+    float shift = 0.f;
+    if (kF32) {
+        const int cx = R + (int)min(kTileX / 2u, ref.nx - gx0 - 1) * s;
+        const int cy = R + (int)min(kTileY / 2u, ref.ny - gy0 - 1) * s;
+        shift = refv[cy * PXp + (cx % s) * PXs + cx / s];
+    }
+    const float sr_shift = (float)(sr - n * (double)shift);
+    const float inv_nf = 1.0f / (float)N, minvar_nf = (float)minvar_n;
     Rank st = rank_empty();
     for (int k = k0; k < k1; ++k) {
         const float inv = pinv[k];
@@ -525,35 +540,64 @@ __global__ void __launch_bounds__(kTileThreads, 1024 / kTileThreads) k_sweep_til
             for (int yy = ty; yy < PY; yy += kTileY) {
                 const float* sp = samp + yy * PXp + tx;
                 const float* rp = refv + yy * PXp + tx;
-                double a = 0.0, bb = 0.0, c = 0.0;
-#pragma unroll
-                for (int dx = 0; dx < W; ++dx) {
-                    const double v = (double)sp[toff[dx]];
-                    a += v;
-                    bb = fma(v, v, bb);
-                    c = fma((double)rp[toff[dx]], v, c);
-                }
                 const int i = yy * kTileX + tx;
-                hs[i] = a;
-                hss[i] = bb;
-                hrs[i] = c;
+                if (kF32) {
+                    // (sum s, sum s^2) as one packed FMA a tap: (s, s) * (1, s) + acc
+                    float2 ab = f2(0.f, 0.f);
+                    float c = 0.f;
+#pragma unroll
+                    for (int dx = 0; dx < W; ++dx) {
+                        const float v = sp[toff[dx]] - shift;
+                        ab = __ffma2_rn(f2(v, v), f2(1.0f, v), ab);
+                        c = fmaf(rp[toff[dx]] - shift, v, c);
+                    }
+                    hs[i] = (Acc)ab.x;
+                    hss[i] = (Acc)ab.y;
+                    hrs[i] = (Acc)c;
+                } else {
+                    double a = 0.0, bb = 0.0, c = 0.0;
+#pragma unroll
+                    for (int dx = 0; dx < W; ++dx) {
+                        const double v = (double)sp[toff[dx]];
+                        a += v;
+                        bb = fma(v, v, bb);
+                        c = fma((double)rp[toff[dx]], v, c);
+                    }
+                    hs[i] = (Acc)a;
+                    hss[i] = (Acc)bb;
+                    hrs[i] = (Acc)c;
+                }
             }
             __syncthreads();
             if (sampled) {
-                double a = 0.0, bb = 0.0, c = 0.0;
-#pragma unroll
-                for (int dy = 0; dy < W; ++dy) {
-                    const int i = (ty * s + dy) * kTileX + tx;
-                    a += hs[i];
-                    bb += hss[i];
-                    c += hrs[i];
-                }
-                // the cancelling differences in f64, the ratio in f32
-                const double vs = bb - a * a * inv_n;
-                const double cov = c - sr * a * inv_n;
                 float cost = __int_as_float(0x7fc00000);
-                if (vs > 0.0 && vs >= minvar_n && vr_ok)
-                    cost = 1.0f - (float)cov * rsqrtf(vr_f * (float)vs);
+                if (kF32) {
+                    float a = 0.f, bb = 0.f, c = 0.f;
+#pragma unroll
+                    for (int dy = 0; dy < W; ++dy) {
+                        const int i = (ty * s + dy) * kTileX + tx;
+                        a += (float)hs[i];
+                        bb += (float)hss[i];
+                        c += (float)hrs[i];
+                    }
+                    const float vs = bb - a * a * inv_nf;
+                    const float cov = c - sr_shift * a * inv_nf;
+                    if (vs > 0.f && vs >= minvar_nf && vr_ok) cost = 1.0f - cov * rsqrtf(vr_f * vs);
+                } else {
+                    double a = 0.0, bb = 0.0, c = 0.0;
+#pragma unroll
+                    for (int dy = 0; dy < W; ++dy) {
+                        const int i = (ty * s + dy) * kTileX + tx;
+                        a += (double)hs[i];
+                        bb += (double)hss[i];
+                        c += (double)hrs[i];
+                    }
+                    // the cancelling differences in f64, the ratio in f32
+                    const double vs = bb - a * a * inv_n;
+                    const double cov = c - sr * a * inv_n;
+                    if (vs > 0.0 && vs >= minvar_n && vr_ok)
+                        cost = 1.0f - (float)cov * rsqrtf(vr_f * (float)vs);
+                }
                 costs[j * kTileThreads + tid] = cost;  // NaN when invalid
             }
         }
@@ -747,18 +791,74 @@ __device__ __forceinline__ bool window_inside(const float* H, float zmin, float 
     return umin >= m && vmin >= m && umax <= wl - m && vmax <= hl - m;
 }
 
+// Bilinear samplers of the reference image for the single-view sweep, both
+// with the floor, fraction and texels of sample_nonneg:
+//  * ImageSampler reads the image in global memory;
+//  * BandSampler reads a staged box of it in shared memory (a warp's band,
+//    rows of kBandPitch texels starting at image texel (x0, y0)).  The floor is
+//    the same round-down add with the box origin folded into the shift:
+//    u + (2^23 - x0) rounded down is 2^23 - x0 + floor(u) exactly, whose low
+//    mantissa bits are floor(u) - x0, the band column; the fraction u - floor(u)
+//    and the texel values are the image's, so the two samplers agree bit for bit.
+constexpr int kBandPitch = 64;  // texels per staged band row
+constexpr int kBandRows = 20;   // staged band rows
+
+template <class T>
+struct ImageSampler {
+    const T* __restrict__ img;
+    uint32_t w;
+    __device__ __forceinline__ float operator()(float u, float v) const {
+        return sample_nonneg<T>(img, w, u, v);
+    }
+    __device__ __forceinline__ float2 pair(float2 u, float2 v) const {
+        return sample_nonneg_pair<T>(img, w, u, v);
+    }
+};
+
+struct BandSampler {
+    const float* band;
+    float sx, sy;  // 2^23 - x0, 2^23 - y0
+    __device__ __forceinline__ float operator()(float u, float v) const {
+        const int sb = __float_as_int(8388608.0f);
+        const float tu = __fadd_rd(u, sx), tv = __fadd_rd(v, sy);
+        const float fu = tu - sx, fv = tv - sy;
+        const int o = (__float_as_int(tv) - sb) * kBandPitch + (__float_as_int(tu) - sb);
+        const float tx = u - fu, ty = v - fv;
+        const float v00 = band[o], v10 = band[o + 1];
+        const float v01 = band[o + kBandPitch], v11 = band[o + kBandPitch + 1];
+        const float top = fmaf(v10 - v00, tx, v00);
+        const float bot = fmaf(v11 - v01, tx, v01);
+        return fmaf(bot - top, ty, top);
+    }
+    __device__ __forceinline__ float2 pair(float2 u, float2 v) const {
+        const int sb = __float_as_int(8388608.0f);
+        const float2 s2x = f2(sx, sx), s2y = f2(sy, sy);
+        const float2 tu = __fadd2_rd(u, s2x), tv = __fadd2_rd(v, s2y);
+        const float2 fu = __fadd2_rn(tu, neg2(s2x)), fv = __fadd2_rn(tv, neg2(s2y));
+        const int oa = (__float_as_int(tv.x) - sb) * kBandPitch + (__float_as_int(tu.x) - sb);
+        const int ob = (__float_as_int(tv.y) - sb) * kBandPitch + (__float_as_int(tu.y) - sb);
+        const float2 tx = __fadd2_rn(u, neg2(fu)), ty = __fadd2_rn(v, neg2(fv));
+        const float2 v00 = f2(band[oa], band[ob]);
+        const float2 v10 = f2(band[oa + 1], band[ob + 1]);
+        const float2 v01 = f2(band[oa + kBandPitch], band[ob + kBandPitch]);
+        const float2 v11 = f2(band[oa + kBandPitch + 1], band[ob + kBandPitch + 1]);
+        const float2 top = __ffma2_rn(__fadd2_rn(v10, neg2(v00)), tx, v00);
+        const float2 bot = __ffma2_rn(__fadd2_rn(v11, neg2(v01)), tx, v01);
+        return __ffma2_rn(__fadd2_rn(bot, neg2(top)), ty, top);
+    }
+};
+
 // Window cost against the window centred on its mean pm (pvc, squared
 // deviation pvar), sampling the image through H at taps (x + dx, y + dy);
 // the samples are shifted by pm too before their sums, as in the direct cost.  CHECK runs the
 // per-tap domain tests; without it the caller has established the domain
-// with window_inside.  The window rows run as a rolled loop with the taps of
-// a row unrolled: a fully unrolled 7x7 or 9x9 body outgrows the instruction
-// cache.
-template <class T, int R, int COST, bool CHECK>
+// (window_inside, or the band box of every hypothesis).  The window rows run
+// as a rolled loop with the taps of a row unrolled: a fully unrolled 7x7 or
+// 9x9 body outgrows the instruction cache.
+template <int R, int COST, bool CHECK, class S>
 __device__ __forceinline__ bool window_cost(const float* pvc, float pm, float pvar, const float* H,
                                             float zmin, float wl, float hl, float minvar,
-                                            const T* __restrict__ img, uint32_t w, float x,
-                                            float y, float& cost) {
+                                            const S& smp_of, float x, float y, float& cost) {
     constexpr int W = 2 * R + 1;
     constexpr int N = W * W;
     float sv[COST == 1 ? 1 : N];
@@ -777,7 +877,7 @@ __device__ __forceinline__ bool window_cost(const float* pvc, float pm, float pv
             const float u = fmaf(H[0], X, hx) * iv;
             const float v = fmaf(H[3], X, hy) * iv;
             if (CHECK && !(u >= 0.f && v >= 0.f && u < wl && v < hl)) return false;
-            const float smp = sample_nonneg<T>(img, w, u, v);
+            const float smp = smp_of(u, v);
             if (COST == 1) {
                 const float s = smp - pm;
                 ss += s;
@@ -804,17 +904,17 @@ __device__ __forceinline__ bool window_cost(const float* pvc, float pm, float pv
     return true;
 }
 
-// The ZNCC window costs of two hypotheses at once, for windows that
-// window_inside admitted: the same operations as window_cost<T, R, 1, false>,
+// The ZNCC window costs of two hypotheses at once, for windows whose domain
+// the caller established: the same operations as window_cost<R, 1, false>,
 // each done on both hypotheses by one packed f32x2 instruction (sm_100) with
 // the scalar's rounding, so every component equals the scalar cost bit for
 // bit while the pair costs about half the issue slots.
-template <class T, int R>
+template <int R, class S>
 __device__ __forceinline__ void window_cost_zncc_pair(const float* pvc, float pm, float pvar,
                                                       const float* Ha, const float* Hb,
-                                                      float minvar, const T* __restrict__ img,
-                                                      uint32_t w, float x, float y, bool& oka,
-                                                      float& ea, bool& okb, float& eb) {
+                                                      float minvar, const S& smp_of, float x,
+                                                      float y, bool& oka, float& ea, bool& okb,
+                                                      float& eb) {
     constexpr int W = 2 * R + 1;
     constexpr int N = W * W;
     const float2 H0 = f2(Ha[0], Hb[0]), H3 = f2(Ha[3], Hb[3]), H6 = f2(Ha[6], Hb[6]);
@@ -837,7 +937,7 @@ __device__ __forceinline__ void window_cost_zncc_pair(const float* pvc, float pm
             const float2 iv = f2(__fdividef(1.0f, h2.x), __fdividef(1.0f, h2.y));
             const float2 u = __fmul2_rn(__ffma2_rn(H0, X2, hx), iv);
             const float2 v = __fmul2_rn(__ffma2_rn(H3, X2, hy), iv);
-            const float2 s = __fadd2_rn(sample_nonneg_pair<T>(img, w, u, v), npm);
+            const float2 s = __fadd2_rn(smp_of.pair(u, v), npm);
             ss = __fadd2_rn(ss, s);
             sss = __ffma2_rn(s, s, sss);
             sps = __ffma2_rn(f2(prow[dx], prow[dx]), s, sps);
@@ -852,6 +952,60 @@ __device__ __forceinline__ void window_cost_zncc_pair(const float* pvc, float pm
     };
     oka = finish(ss.x, sss.x, sps.x, ea);
     okb = finish(ss.y, sss.y, sps.y, eb);
+}
+
+// The band of the reference that a pair's single-view sweep reads: the box of
+// texels under every tap of every hypothesis.  For one hypothesis the window's
+// image is the convex quadrilateral of its mapped corners (a projective map
+// with a positive denominator); along the hypotheses each tap moves
+// monotonically (u = (p + inv b0) / (q + inv b2) is monotone in inv), and the
+// denominator minus the depth floor is affine in (X, Y, inv); so the corners
+// at the first and last inverse depth bound everything.  The margin bounds the
+// f32 rounding of any tap at any hypothesis (window_inside's, maximised over
+// the two ends: the homography's magnitudes are largest, and the denominator
+// smallest, at an end).  False when that box leaves the bilinear domain or
+// exceeds kBandPitch x kBandRows texels; the caller then tests hypothesis by
+// hypothesis.
+template <int R>
+__device__ __forceinline__ bool band_box(const float* A, const float* bv, float inv_a, float inv_b,
+                                         float wl, float hl, float x, float y, int& bx0, int& by0,
+                                         int& cols, int& rows) {
+    constexpr float kRel = 9.5367431640625e-07f;  // 2^-20
+    float umin = 3.0e38f, vmin = 3.0e38f, umax = -3.0e38f, vmax = -3.0e38f, m = 0.f;
+    const float ax = fabsf(x) + (float)R, ay = fabsf(y) + (float)R;
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+        float H[9];
+        const float inv = e ? inv_b : inv_a;
+        plane_h(A, bv, inv, H);
+        const float su = fmaf(fabsf(H[0]), ax, fmaf(fabsf(H[1]), ay, fabsf(H[2])));
+        const float sv = fmaf(fabsf(H[3]), ax, fmaf(fabsf(H[4]), ay, fabsf(H[5])));
+        const float sz = fmaf(fabsf(H[6]), ax, fmaf(fabsf(H[7]), ay, fabsf(H[8])));
+        float hmin = 3.0e38f;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const float X = x + ((c & 1) ? (float)R : -(float)R);
+            const float Y = y + ((c & 2) ? (float)R : -(float)R);
+            const float h2 = fmaf(H[6], X, fmaf(H[7], Y, H[8]));
+            const float iv = __fdividef(1.0f, h2);
+            const float u = fmaf(H[0], X, fmaf(H[1], Y, H[2])) * iv;
+            const float v = fmaf(H[3], X, fmaf(H[4], Y, H[5])) * iv;
+            hmin = fminf(hmin, h2);
+            umin = fminf(umin, u);
+            umax = fmaxf(umax, u);
+            vmin = fminf(vmin, v);
+            vmax = fmaxf(vmax, v);
+        }
+        if (!(hmin > 1.0e-4f * inv + kRel * sz) || !(hmin > 0.f)) return false;
+        m = fmaxf(m, 0.015625f + kRel * (fmaxf(su, sv) + fmaxf(wl, hl) * sz) / hmin);
+    }
+    // NaN fails every comparison
+    if (!(umin >= m && vmin >= m && umax <= wl - m && vmax <= hl - m)) return false;
+    bx0 = (int)floorf(umin - m);
+    by0 = (int)floorf(vmin - m);
+    cols = (int)floorf(umax + m) + 2 - bx0;
+    rows = (int)floorf(vmax + m) + 2 - by0;
+    return cols <= kBandPitch && rows <= kBandRows;
 }
 
 template <class T, int R, int COST>
@@ -1009,8 +1163,11 @@ __global__ void __launch_bounds__(256, 2) k_recip_sweep(BatchDev b, const Cand* 
     constexpr int W = 2 * R + 1;
     constexpr int N = W * W;
     __shared__ float pvc_all[8][N];
+    // the warps' bands, with a guard row before the first and after the last
+    __shared__ float band_all[(8 * kBandRows + 2) * kBandPitch];
     const uint32_t lane = lane_id(), wid = threadIdx.x >> 5;
     float* pvc = pvc_all[wid];
+    float* band = band_all + (1 + wid * kBandRows) * kBandPitch;
     const uint32_t ms = (uint32_t)b.max_src;
     const uint32_t n_list = *list_count;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -1049,7 +1206,6 @@ __global__ void __launch_bounds__(256, 2) k_recip_sweep(BatchDev b, const Cand* 
             if (t < N) pvc[t] = d;
         }
         const float pvar = warp_sum(dsq);
-        __syncwarp();
         const float* inv_tab = b.src_inv + ref.inv_off + (size_t)si * ref.planes;
         const T* rimg = static_cast<const T*>(ref.img.data);
         const uint32_t rw = ref.img.width;
@@ -1058,48 +1214,86 @@ __global__ void __launch_bounds__(256, 2) k_recip_sweep(BatchDev b, const Cand* 
         const float minvar = (float)prof.min_variance;
         float be = 3.0e38f;
         int bk = 0x7fffffff;
-        // one hypothesis alone, through the scalar paths
-        auto single = [&](int k, const float* H, bool inside) {
-            const float zmin = 1.0e-4f * inv_tab[k];
-            float e;
-            const bool ok =
-                inside ? window_cost<T, R, COST, false>(pvc, pm, pvar, H, zmin, wl, hl, minvar,
-                                                        rimg, rw, x0, y0, e)
-                       : window_cost<T, R, COST, true>(pvc, pm, pvar, H, zmin, wl, hl, minvar,
-                                                       rimg, rw, x0, y0, e);
+        auto take = [&](bool ok, float e, int k) {
             if (ok && (double)e <= prof.max_error && e < be) {
                 be = e;
                 bk = k;
             }
         };
-        // this lane's hypotheses in the order lane, lane + 32, lane + 64, ...,
-        // taken two at a time (k, k + 32) for the packed ZNCC path
-        for (int k = lane; k < ref.planes; k += 64) {
-            const int k2 = k + 32;
-            float Ha[9], Hb[9];
-            plane_h(src.bwd_A, src.bwd_b, inv_tab[k], Ha);
-            const bool ina = window_inside<R>(Ha, 1.0e-4f * inv_tab[k], wl, hl, x0, y0);
-            bool inb = false;
-            if (k2 < ref.planes) {
-                plane_h(src.bwd_A, src.bwd_b, inv_tab[k2], Hb);
-                inb = window_inside<R>(Hb, 1.0e-4f * inv_tab[k2], wl, hl, x0, y0);
+        // every hypothesis's window inside one staged box of the reference
+        int bx0 = 0, by0 = 0, cols = 0, rows = 0;
+        const bool banded = band_box<R>(src.bwd_A, src.bwd_b, inv_tab[0], inv_tab[ref.planes - 1],
+                                        wl, hl, x0, y0, bx0, by0, cols, rows);
+        if (banded) {
+            for (int rr = 0; rr < rows; ++rr) {
+                const T* row = rimg + (size_t)(by0 + rr) * rw + bx0;
+                for (int c = lane; c < cols; c += 32) band[rr * kBandPitch + c] = pix<T>(row, c);
             }
-            if (COST == 1 && ina && inb) {
-                bool oka, okb;
-                float ea, eb;
-                window_cost_zncc_pair<T, R>(pvc, pm, pvar, Ha, Hb, minvar, rimg, rw, x0, y0, oka,
-                                            ea, okb, eb);
-                if (oka && (double)ea <= prof.max_error && ea < be) {
-                    be = ea;
-                    bk = k;
+        }
+        __syncwarp();
+        if (banded) {
+            const BandSampler smp{band, 8388608.0f - (float)bx0, 8388608.0f - (float)by0};
+            // this lane's hypotheses in the order lane, lane + 32, lane + 64, ...,
+            // two at a time (k, k + 32) on the packed ZNCC path
+            for (int k = lane; k < ref.planes; k += 64) {
+                const int k2 = k + 32;
+                float Ha[9], Hb[9];
+                plane_h(src.bwd_A, src.bwd_b, inv_tab[k], Ha);
+                if (COST == 1 && k2 < ref.planes) {
+                    plane_h(src.bwd_A, src.bwd_b, inv_tab[k2], Hb);
+                    bool oka, okb;
+                    float ea, eb;
+                    window_cost_zncc_pair<R>(pvc, pm, pvar, Ha, Hb, minvar, smp, x0, y0, oka, ea,
+                                             okb, eb);
+                    take(oka, ea, k);
+                    take(okb, eb, k2);
+                } else {
+                    float e;
+                    bool ok = window_cost<R, COST, false>(pvc, pm, pvar, Ha, 0.f, wl, hl, minvar,
+                                                          smp, x0, y0, e);
+                    take(ok, e, k);
+                    if (k2 < ref.planes) {
+                        plane_h(src.bwd_A, src.bwd_b, inv_tab[k2], Hb);
+                        ok = window_cost<R, COST, false>(pvc, pm, pvar, Hb, 0.f, wl, hl, minvar,
+                                                         smp, x0, y0, e);
+                        take(ok, e, k2);
+                    }
                 }
-                if (okb && (double)eb <= prof.max_error && eb < be) {
-                    be = eb;
-                    bk = k2;
+            }
+        } else {
+            const ImageSampler<T> smp{rimg, rw};
+            // one hypothesis alone, through the scalar paths
+            auto single = [&](int k, const float* H, bool inside) {
+                const float zmin = 1.0e-4f * inv_tab[k];
+                float e;
+                const bool ok =
+                    inside ? window_cost<R, COST, false>(pvc, pm, pvar, H, zmin, wl, hl, minvar,
+                                                         smp, x0, y0, e)
+                           : window_cost<R, COST, true>(pvc, pm, pvar, H, zmin, wl, hl, minvar,
+                                                        smp, x0, y0, e);
+                take(ok, e, k);
+            };
+            for (int k = lane; k < ref.planes; k += 64) {
+                const int k2 = k + 32;
+                float Ha[9], Hb[9];
+                plane_h(src.bwd_A, src.bwd_b, inv_tab[k], Ha);
+                const bool ina = window_inside<R>(Ha, 1.0e-4f * inv_tab[k], wl, hl, x0, y0);
+                bool inb = false;
+                if (k2 < ref.planes) {
+                    plane_h(src.bwd_A, src.bwd_b, inv_tab[k2], Hb);
+                    inb = window_inside<R>(Hb, 1.0e-4f * inv_tab[k2], wl, hl, x0, y0);
                 }
-            } else {
-                single(k, Ha, ina);
-                if (k2 < ref.planes) single(k2, Hb, inb);
+                if (COST == 1 && ina && inb) {
+                    bool oka, okb;
+                    float ea, eb;
+                    window_cost_zncc_pair<R>(pvc, pm, pvar, Ha, Hb, minvar, smp, x0, y0, oka, ea,
+                                             okb, eb);
+                    take(oka, ea, k);
+                    take(okb, eb, k2);
+                } else {
+                    single(k, Ha, ina);
+                    if (k2 < ref.planes) single(k2, Hb, inb);
+                }
             }
         }
 #pragma unroll
@@ -1256,7 +1450,7 @@ cudaError_t Typed<T>::sweep_tiled(const BatchDev& b, uint32_t max_nx, uint32_t m
         const int s = (int)stride;
         const int PX = (kTileX - 1) * s + W, PY = (kTileY - 1) * s + W;
         const size_t PXp = (size_t)((PX + s - 1) / s) * s, np = PXp * PY;
-        const size_t smem = sizeof(double) * 3 * (size_t)PY * kTileX +
+        const size_t smem = (b.sums32 ? sizeof(float) : sizeof(double)) * 3 * (size_t)PY * kTileX +
                             sizeof(float) * (2 * np + (size_t)b.max_src * (kTileThreads + 12) +
                                              2 * (size_t)b.prof.planes) +
                             16 + sizeof(float4) * (size_t)tiled_steps((int)np) * kTileThreads;
@@ -1269,11 +1463,15 @@ cudaError_t Typed<T>::sweep_tiled(const BatchDev& b, uint32_t max_nx, uint32_t m
         V3D_COUNTED kern<<<grid, kTileThreads, smem, st>>>(b, total_sites, rank, status, ctr, n, chunks.partial);
         return cudaGetLastError();
     };
-    switch (b.prof.radius) {
-        case 1: return run(k_sweep_tiled<T, 1>, 3);
-        case 2: return run(k_sweep_tiled<T, 2>, 5);
-        case 3: return run(k_sweep_tiled<T, 3>, 7);
-        case 4: return run(k_sweep_tiled<T, 4>, 9);
+    switch (b.prof.radius * 2 + (b.sums32 ? 1 : 0)) {
+        case 2: return run(k_sweep_tiled<T, 1, double>, 3);
+        case 4: return run(k_sweep_tiled<T, 2, double>, 5);
+        case 6: return run(k_sweep_tiled<T, 3, double>, 7);
+        case 8: return run(k_sweep_tiled<T, 4, double>, 9);
+        case 3: return run(k_sweep_tiled<T, 1, float>, 3);
+        case 5: return run(k_sweep_tiled<T, 2, float>, 5);
+        case 7: return run(k_sweep_tiled<T, 3, float>, 7);
+        case 9: return run(k_sweep_tiled<T, 4, float>, 9);
     }
     return cudaErrorInvalidValue;
 }

@@ -32,6 +32,7 @@ COST_ZSAD = 0
 COST_ZNCC = 1
 PRECISION_EXACT64 = 0
 PRECISION_FAST32 = 1
+PRECISION_FAST32_SUMS32 = 2
 
 
 class Frame(C.Structure):
