@@ -562,6 +562,8 @@ typedef struct v3d_run_info {
     double recip_sweep_ms;    /* the single-view reciprocal sweep kernel, all its launches
                                * (primary candidates and both completion passes) */
     double recip_prepare_ms;  /* the reciprocal prologue and its pair list, all launches */
+    uint64_t sweep_tile_x;    /* tile width of the box-filtered sweep: 32 (32x8 sites) or 16
+                               * (16x16); 0 when the sweep ran a warp per site */
 } v3d_run_info;
 
 int32_t v3d_last_run_info(const v3d_context* ctx, v3d_run_info* out);

@@ -88,20 +88,23 @@ def test_uneven_clips_exact_policy_matches_the_oracle(oracle):
 
 @pytest.mark.gpu
 def test_sweep_chunk_tuning_never_changes_results():
-    """The tiled sweep's plane chunking is tuned on live calls; whatever chunk
-    count a call runs with, its results are the same bit for bit."""
+    """The tiled sweep's tile shape (32x8 or 16x16) and plane chunking are tuned
+    on live calls; whatever plan a call runs with, its results are the same bit
+    for bit."""
     clip = synth.make_clip(232, 130, 5, 15.0, 1.2, 31, landmark_cameras=[2],
                            landmarks_per_camera=400)
     frames = clip.frames("f32")
     prof = profiles.zncc(2, 48, 4, 2)
     ctx = dense.Context(0)
-    outs, chunks = [], []
-    for _ in range(6):
+    outs, plans = [], []
+    for _ in range(8):
         outs.append(ctx.reconstruct_reference_patches(frames, clip.cameras, clip.sparse,
                                                       clip.focal, [2], profile=prof)[0])
-        chunks.append(ctx.last_run_info()["sweep_chunks"])
+        info = ctx.last_run_info()
+        plans.append((info["sweep_tile_x"], info["sweep_chunks"]))
     assert len(outs[0].points) > 0
     for o in outs[1:]:
         _same(o, outs[0])
-    assert len(set(chunks)) >= 2          # candidates were tried
-    assert chunks[-1] == chunks[-2] > 1   # and one was kept (a small batch chunks)
+    assert {t for t, _ in plans} == {16, 32}     # both tiles were tried
+    assert len({c for _, c in plans}) >= 2       # and several chunk counts
+    assert plans[-1] == plans[-2] and plans[-1][1] > 1  # one plan was kept

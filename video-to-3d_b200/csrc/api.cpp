@@ -251,6 +251,7 @@ int32_t v3d_last_run_info(const v3d_context* ctx, v3d_run_info* out) {
     out->host_readback_ms = ctx->last_readback_ms;
     out->result_bytes = ctx->last_result_bytes;
     out->sweep_chunks = ctx->last_chunks;
+    out->sweep_tile_x = ctx->last_tile_x;
     out->recip_sweep_ms = ctx->last_recip_sweep_ms;
     out->recip_prepare_ms = ctx->last_recip_prepare_ms;
     return V3D_OK;

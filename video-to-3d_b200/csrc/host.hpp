@@ -162,11 +162,18 @@ struct SweepShapeKey {
 };
 SweepShapeKey sweep_shape_key(int device, int radius, int stride, uint64_t tiles, int planes,
                               int sources);
-// Plane chunks to run for a batch of this shape: a candidate while the shape
-// is being measured, then the fastest one.
-int sweep_chunks_pick(const SweepShapeKey& key, int heuristic, int max_chunks);
-// Sweep device time of a batch run with `chunks`, over `units` window costs.
-void sweep_chunks_record(const SweepShapeKey& key, int chunks, double sweep_ms, uint64_t units);
+// How the tiled sweep runs: the tile (32x8 or 16x16 sites) and its plane chunks.
+struct SweepPlan {
+    int tile_x = 32;
+    int chunks = 1;
+};
+// The plan for a batch of this shape: a candidate while the shape is being
+// measured, then the fastest one.  heuristic32 / heuristic16 are the
+// occupancy heuristic's chunk counts for the two tiles.
+SweepPlan sweep_plan_pick(const SweepShapeKey& key, int heuristic32, int heuristic16,
+                          int max_chunks);
+// Sweep device time of a batch run with `plan`, over `units` window costs.
+void sweep_plan_record(const SweepShapeKey& key, SweepPlan plan, double sweep_ms, uint64_t units);
 
 // ---- planning (host_plan.cpp) ----
 uint32_t reference_grid_stride(uint32_t w, uint32_t h, bool fine);
@@ -246,6 +253,7 @@ struct v3d_context {
     double last_block_ms = 0, last_readback_ms = 0;
     uint64_t last_result_bytes = 0;
     uint64_t last_chunks = 1;
+    uint64_t last_tile_x = 32;
 };
 
 namespace v3d {

@@ -127,6 +127,7 @@ cudaError_t launch_site_ref(const uint64_t* site_off, int32_t n_refs, uint64_t t
 struct SweepChunks {
     int n = 1;
     Rank* partial = nullptr;
+    int tile_x = 32;  // tile width: 32 (32x8 sites) or 16 (16x16)
 };
 
 // The gates of one swept site on its final rank state (dense_legacy.rs:332-362).

@@ -141,6 +141,7 @@ struct Prepared {
     uint32_t max_nx = 0, max_ny = 0, stride0 = 0;
     bool tiled = false;
     int chunks = 1;             // plane chunks of the tiled sweep
+    int tile_x = 32;            // its tile: 32x8 or 16x16 sites
     SweepShapeKey shape{};      // its launch-shape key for the tuner
     Rank* d_partial = nullptr;  // [chunks][sites] when chunks > 1
     BatchDev b{};
@@ -236,12 +237,14 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
         P.tiled = prof.precision != V3D_PRECISION_EXACT64 && prof.cost == V3D_COST_ZNCC &&
                   uniform_stride && s0 >= 1 && s0 <= 4 && static_cast<int>(s0) < w;
         P.chunks = 1;
+        P.tile_x = 32;
         if (P.tiled) {
-            uint64_t tiles = 0;
+            uint64_t tiles = 0, tiles16 = 0;
             int min_planes = kMaxPlanes;
             for (size_t k = 0; k < n_active; ++k) {
                 const RefPlan& p = plans[active[k]];
                 tiles += static_cast<uint64_t>((p.nx + 31) / 32) * ((p.ny + 7) / 8);
+                tiles16 += static_cast<uint64_t>((p.nx + 15) / 16) * ((p.ny + 15) / 16);
                 min_planes = std::min(min_planes, p.planes);
             }
             if (!ctx->sm_count &&
@@ -252,15 +255,20 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
             }
             const uint64_t target = static_cast<uint64_t>(ctx->sm_count) * 8;
             const int max_chunks = std::max(1, std::min(16, min_planes / 4));
-            int heuristic = 1;
-            if (tiles && tiles < target)
-                heuristic = static_cast<int>(std::min<uint64_t>((target + tiles - 1) / tiles, max_chunks));
+            auto heuristic = [&](uint64_t n) {
+                return n && n < target
+                           ? static_cast<int>(std::min<uint64_t>((target + n - 1) / n, max_chunks))
+                           : 1;
+            };
             int max_src = 1;
             for (size_t k = 0; k < n_active; ++k)
                 max_src = std::max<int>(max_src, static_cast<int>(plans[active[k]].src_slots.size()));
             P.shape = sweep_shape_key(ctx->device, prof.patch_radius, static_cast<int>(s0), tiles,
                                       min_planes, max_src);
-            P.chunks = sweep_chunks_pick(P.shape, heuristic, max_chunks);
+            const SweepPlan plan =
+                sweep_plan_pick(P.shape, heuristic(tiles), heuristic(tiles16), max_chunks);
+            P.chunks = plan.chunks;
+            P.tile_x = plan.tile_x;
         }
     }
     P.n_active = n_active;
@@ -625,6 +633,7 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
     cudaEventCreate(&ev1);
     cudaEventRecord(ev0, stream);
     ctx->last_chunks = static_cast<uint64_t>(P.chunks);
+    ctx->last_tile_x = static_cast<uint64_t>(P.tiled ? P.tile_x : 0);
     ctx->last_sites = total;
     ctx->last_units = 0;
     for (size_t k = 0; k < n_active; ++k) {
@@ -650,7 +659,8 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
     // primary sweep, reciprocal check and fusion
     cudaEventRecord(es[0], stream);
     V3D_CK(launch_sweep_dispatch(b, d_siteref, total, max_nx, max_ny, stride0, tiled, d_rank,
-                                 d_status, d_ctr, stream, SweepChunks{P.chunks, P.d_partial}));
+                                 d_status, d_ctr, stream,
+                                 SweepChunks{P.chunks, P.d_partial, P.tile_x}));
     cudaEventRecord(es[1], stream);
     V3D_CK(launch_compact(d_status, kSiteAccepted, total, d_idx, c_cand, d_scratch, stream));
     V3D_CK(launch_make_primary_cands(b, d_idx, c_cand, cap, d_siteref, d_rank, d_cands, stream));
@@ -770,7 +780,9 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
     V3D_CK(cudaStreamSynchronize(stream));
     cudaEventElapsedTime(&ctx->last_ms, ev0, ev1);
     cudaEventElapsedTime(&ctx->last_sweep_ms, es[0], es[1]);
-    if (P.tiled) sweep_chunks_record(P.shape, P.chunks, ctx->last_sweep_ms, ctx->last_units);
+    if (P.tiled)
+        sweep_plan_record(P.shape, SweepPlan{P.tile_x, P.chunks}, ctx->last_sweep_ms,
+                          ctx->last_units);
     cudaEventElapsedTime(&ctx->last_recip_ms, es[2], es[3]);
     ctx->last_recip_sweep_ms = ctx->last_recip_prepare_ms = 0.f;
     for (auto& row : er) {
@@ -988,7 +1000,7 @@ int32_t run_sweep_records(v3d_context* ctx, const v3d_profile& prof, const v3d_f
     if (pst != V3D_OK) return pst;
     V3D_CK(launch_sweep_dispatch(P.b, P.d_siteref, P.total, P.max_nx, P.max_ny, P.stride0, P.tiled,
                                  P.d_rank, P.d_status, P.d_ctr, stream,
-                                 SweepChunks{P.chunks, P.d_partial}));
+                                 SweepChunks{P.chunks, P.d_partial, P.tile_x}));
     std::vector<SiteRank> rank(P.total);
     std::vector<uint8_t> status(P.total);
     if (P.total) {

@@ -11,9 +11,10 @@
 namespace v3d {
 namespace typed_detail {
 
-constexpr int kTileX = 32;
-constexpr int kTileY = 8;
-constexpr int kTileThreads = kTileX * kTileY;  // one thread per grid site of a tile
+// The tiled sweep's CTA: one thread per grid site of a TX x TY tile (32x8 or
+// 16x16), eight warps.
+constexpr int kTileThreads = 256;
+constexpr int kTileWarps = kTileThreads / 32;
 constexpr double kInf = __builtin_huge_val();
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
@@ -324,7 +325,9 @@ __device__ __forceinline__ bool rect_inside(const float* H, float zmin, float wl
 __host__ __device__ constexpr int tiled_steps(int np) { return (np + 2 * kTileThreads - 1) / (2 * kTileThreads); }
 
 // ---- sweep, tiled ZNCC (fast policy) -----------------------------------------
-// A CTA owns a 32x8 block of grid sites.  For every (plane, source) it warps
+// A CTA owns a TX x TY block of grid sites (32x8 or 16x16, the tuner's pick;
+// the f64 window sums are formed tap by tap in the same order whatever the
+// tile, so the shape never changes a result).  For every (plane, source) it warps
 // the block's pixel footprint into the source once (f32 homography and f32
 // bilinear), then forms the window sums of s, s^2 and r*s with separable box
 // filters, so overlapping windows (stride < window) share every bilinear
@@ -344,7 +347,7 @@ __host__ __device__ constexpr int tiled_steps(int np) { return (np + 2 * kTileTh
 // row ends.  When the footprint's image in a source lies inside that image
 // (tested once per plane and source on the rectangle's corners), the step
 // skips the per-sample domain tests.
-template <class T, int R, class Acc>
+template <class T, int R, class Acc, int TX>
 __global__ void __launch_bounds__(kTileThreads, 1024 / kTileThreads) k_sweep_tiled(BatchDev b, uint64_t total_sites,
                                                      SiteRank* __restrict__ rank,
                                                      uint8_t* __restrict__ status,
@@ -352,25 +355,26 @@ __global__ void __launch_bounds__(kTileThreads, 1024 / kTileThreads) k_sweep_til
                                                      Rank* __restrict__ partial) {
     constexpr int W = 2 * R + 1;
     constexpr int N = W * W;
+    constexpr int TY = kTileThreads / TX;
     extern __shared__ double smem_d[];
     // blockIdx.z = reference x plane chunk; the chunk sweeps planes [k0, k1)
     const uint32_t r = blockIdx.z / (uint32_t)n_chunks;
     const int chunk = (int)(blockIdx.z - r * (uint32_t)n_chunks);
     const DevReference& ref = b.refs[r];
     const DevProfile& prof = b.prof;
-    const uint32_t gx0 = blockIdx.x * kTileX, gy0 = blockIdx.y * kTileY;
+    const uint32_t gx0 = blockIdx.x * TX, gy0 = blockIdx.y * TY;
     if (gx0 >= ref.nx || gy0 >= ref.ny) return;
     const int per_chunk = (ref.planes + n_chunks - 1) / n_chunks;
     const int k0 = chunk * per_chunk, k1 = min(ref.planes, k0 + per_chunk);
     const int s = (int)ref.stride;
-    const int PX = (kTileX - 1) * s + W, PY = (kTileY - 1) * s + W;
+    const int PX = (TX - 1) * s + W, PY = (TY - 1) * s + W;
     const int PXs = (PX + s - 1) / s, PXp = PXs * s;  // columns per residue, padded row
     const int np = PY * PXp;
     const int ms = b.max_src;
-    Acc* hs = reinterpret_cast<Acc*>(smem_d);  // [PY][32] row sums of s
-    Acc* hss = hs + PY * kTileX;               // [PY][32] row sums of s^2
-    Acc* hrs = hss + PY * kTileX;              // [PY][32] row sums of r*s
-    float* refv = reinterpret_cast<float*>(hrs + PY * kTileX);  // [PY][PXp] reference values
+    Acc* hs = reinterpret_cast<Acc*>(smem_d);  // [PY][TX] row sums of s
+    Acc* hss = hs + PY * TX;                   // [PY][TX] row sums of s^2
+    Acc* hrs = hss + PY * TX;                  // [PY][TX] row sums of r*s
+    float* refv = reinterpret_cast<float*>(hrs + PY * TX);  // [PY][PXp] reference values
     float* samp = refv + np;                 // [PY][PXp] source samples (NaN = invalid)
     float* costs = samp + np;                // [max_src][kTileThreads]
     float* hA = costs + ms * kTileThreads;   // [max_src][12] homography parts
@@ -441,7 +445,8 @@ __global__ void __launch_bounds__(kTileThreads, 1024 / kTileThreads) k_sweep_til
     for (int dx = 0; dx < W; ++dx) toff[dx] = (dx % s) * PXs + dx / s;
     __syncthreads();
 
-    const int tx = tid & 31, ty = tid >> 5;
+    const int tx = tid % TX, ty = tid / TX;         // this thread's site in the tile
+    const int lane = tid & 31, wid = tid >> 5;      // its place in the flat warp step
     const uint32_t gx = gx0 + tx, gy = gy0 + ty;
     const bool active = gx < ref.nx && gy < ref.ny;
     const uint64_t gsite = b.site_off[r] + (uint64_t)gy * ref.nx + gx;
@@ -478,8 +483,8 @@ __global__ void __launch_bounds__(kTileThreads, 1024 / kTileThreads) k_sweep_til
     constexpr bool kF32 = sizeof(Acc) == 4;
     float shift = 0.f;
     if (kF32) {
-        const int cx = R + (int)min(kTileX / 2u, ref.nx - gx0 - 1) * s;
-        const int cy = R + (int)min(kTileY / 2u, ref.ny - gy0 - 1) * s;
+        const int cx = R + (int)min((uint32_t)TX / 2u, ref.nx - gx0 - 1) * s;
+        const int cy = R + (int)min((uint32_t)TY / 2u, ref.ny - gy0 - 1) * s;
         shift = refv[cy * PXp + (cx % s) * PXs + cx / s];
     }
     const float sr_shift = (float)(sr - n * (double)shift);
@@ -502,11 +507,11 @@ __global__ void __launch_bounds__(kTileThreads, 1024 / kTileThreads) k_sweep_til
             const bool inside = (inmask[k - k0] >> j) & 1u;
             const float a0 = A[0], a1 = A[1], a3 = A[3], a4 = A[4], a6 = A[6], a7 = A[7];
             for (int p = 0; p < n_steps; ++p) {
-                const int ws = p * kTileY + ty;
-                const int fa = ws * 64 + tx;
+                const int ws = p * kTileWarps + wid;
+                const int fa = ws * 64 + lane;
                 if (fa >= np) break;
                 const int fb = fa + 32;
-                const float4 e = slotxy[ws * 32 + tx];
+                const float4 e = slotxy[ws * 32 + lane];
                 const float2 X2 = f2(e.x, e.y), Y2 = f2(e.z, e.w);
                 const float2 hx = __ffma2_rn(f2(a1, a1), Y2, f2(H2, H2));
                 const float2 hy = __ffma2_rn(f2(a4, a4), Y2, f2(H5, H5));
@@ -536,11 +541,12 @@ __global__ void __launch_bounds__(kTileThreads, 1024 / kTileThreads) k_sweep_til
                 if (fb < np) samp[fb] = vb;
             }
             __syncthreads();
-            // horizontal box filter, one row per warp, the window of lane c at slot c
-            for (int yy = ty; yy < PY; yy += kTileY) {
-                const float* sp = samp + yy * PXp + tx;
-                const float* rp = refv + yy * PXp + tx;
-                const int i = yy * kTileX + tx;
+            // horizontal box filter: the window of column c of row yy at slot c,
+            // TX windows a row (a warp takes one row of 32, or two rows of 16)
+            for (int i = tid; i < PY * TX; i += kTileThreads) {
+                const int yy = i / TX, c = i % TX;
+                const float* sp = samp + yy * PXp + c;
+                const float* rp = refv + yy * PXp + c;
                 if (kF32) {
                     // (sum s, sum s^2) as one packed FMA a tap: (s, s) * (1, s) + acc
                     float2 ab = f2(0.f, 0.f);
@@ -575,7 +581,7 @@ __global__ void __launch_bounds__(kTileThreads, 1024 / kTileThreads) k_sweep_til
                     float a = 0.f, bb = 0.f, c = 0.f;
 #pragma unroll
                     for (int dy = 0; dy < W; ++dy) {
-                        const int i = (ty * s + dy) * kTileX + tx;
+                        const int i = (ty * s + dy) * TX + tx;
                         a += (float)hs[i];
                         bb += (float)hss[i];
                         c += (float)hrs[i];
@@ -587,7 +593,7 @@ __global__ void __launch_bounds__(kTileThreads, 1024 / kTileThreads) k_sweep_til
                     double a = 0.0, bb = 0.0, c = 0.0;
 #pragma unroll
                     for (int dy = 0; dy < W; ++dy) {
-                        const int i = (ty * s + dy) * kTileX + tx;
+                        const int i = (ty * s + dy) * TX + tx;
                         a += (double)hs[i];
                         bb += (double)hss[i];
                         c += (double)hrs[i];
@@ -1446,11 +1452,12 @@ cudaError_t Typed<T>::sweep_tiled(const BatchDev& b, uint32_t max_nx, uint32_t m
                                   RefCounters* ctr, cudaStream_t st, uint64_t total_sites,
                                   SweepChunks chunks) {
     using namespace typed_detail;
+    const int TX = chunks.tile_x == 16 ? 16 : 32, TY = kTileThreads / TX;
     auto run = [&](auto kern, int W) -> cudaError_t {
         const int s = (int)stride;
-        const int PX = (kTileX - 1) * s + W, PY = (kTileY - 1) * s + W;
+        const int PX = (TX - 1) * s + W, PY = (TY - 1) * s + W;
         const size_t PXp = (size_t)((PX + s - 1) / s) * s, np = PXp * PY;
-        const size_t smem = (b.sums32 ? sizeof(float) : sizeof(double)) * 3 * (size_t)PY * kTileX +
+        const size_t smem = (b.sums32 ? sizeof(float) : sizeof(double)) * 3 * (size_t)PY * TX +
                             sizeof(float) * (2 * np + (size_t)b.max_src * (kTileThreads + 12) +
                                              2 * (size_t)b.prof.planes) +
                             16 + sizeof(float4) * (size_t)tiled_steps((int)np) * kTileThreads;
@@ -1458,22 +1465,26 @@ cudaError_t Typed<T>::sweep_tiled(const BatchDev& b, uint32_t max_nx, uint32_t m
                                              (int)smem);
         if (e != cudaSuccess) return e;
         const int n = chunks.n > 1 ? chunks.n : 1;
-        dim3 grid((max_nx + kTileX - 1) / kTileX, (max_ny + kTileY - 1) / kTileY,
-                  (unsigned)b.n_refs * (unsigned)n);
+        dim3 grid((max_nx + TX - 1) / TX, (max_ny + TY - 1) / TY, (unsigned)b.n_refs * (unsigned)n);
         V3D_COUNTED kern<<<grid, kTileThreads, smem, st>>>(b, total_sites, rank, status, ctr, n, chunks.partial);
         return cudaGetLastError();
     };
-    switch (b.prof.radius * 2 + (b.sums32 ? 1 : 0)) {
-        case 2: return run(k_sweep_tiled<T, 1, double>, 3);
-        case 4: return run(k_sweep_tiled<T, 2, double>, 5);
-        case 6: return run(k_sweep_tiled<T, 3, double>, 7);
-        case 8: return run(k_sweep_tiled<T, 4, double>, 9);
-        case 3: return run(k_sweep_tiled<T, 1, float>, 3);
-        case 5: return run(k_sweep_tiled<T, 2, float>, 5);
-        case 7: return run(k_sweep_tiled<T, 3, float>, 7);
-        case 9: return run(k_sweep_tiled<T, 4, float>, 9);
-    }
-    return cudaErrorInvalidValue;
+    auto by_acc = [&](auto tx_tag) -> cudaError_t {
+        constexpr int X = decltype(tx_tag)::value;
+        switch (b.prof.radius * 2 + (b.sums32 ? 1 : 0)) {
+            case 2: return run(k_sweep_tiled<T, 1, double, X>, 3);
+            case 4: return run(k_sweep_tiled<T, 2, double, X>, 5);
+            case 6: return run(k_sweep_tiled<T, 3, double, X>, 7);
+            case 8: return run(k_sweep_tiled<T, 4, double, X>, 9);
+            case 3: return run(k_sweep_tiled<T, 1, float, X>, 3);
+            case 5: return run(k_sweep_tiled<T, 2, float, X>, 5);
+            case 7: return run(k_sweep_tiled<T, 3, float, X>, 7);
+            case 9: return run(k_sweep_tiled<T, 4, float, X>, 9);
+        }
+        return cudaErrorInvalidValue;
+    };
+    return TX == 16 ? by_acc(std::integral_constant<int, 16>{})
+                    : by_acc(std::integral_constant<int, 32>{});
 }
 
 template <class T>
