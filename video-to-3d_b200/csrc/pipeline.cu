@@ -10,6 +10,8 @@
 //   per cand    candidates, 16 reciprocal slots, fused output, status
 //   pool        accepted points: primaries, then completion pass 1, then pass 2,
 //               each segment in (reference, raster) order
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <cub/block/block_scan.cuh>
@@ -38,6 +40,52 @@ struct Carver {
         return at;
     }
 };
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (the library
+// links no driver library); null when the driver does not offer it.
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            return static_cast<PFN_cuTensorMapEncodeTiled_v12000>(nullptr);
+        }
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }();
+    return fn;
+}
+
+// A 2-D descriptor of a w x h plane of `storage` texels with a box_x x box_y
+// box: false where TMA cannot address the plane (base or row pitch not a
+// multiple of 16 bytes) or the encoder refuses it.
+bool encode_plane_map(CUtensorMap* m, const void* base, uint32_t w, uint32_t h, int storage,
+                      uint32_t box_x, uint32_t box_y) {
+    const PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
+    if (!encode) return false;
+    CUtensorMapDataType type;
+    uint32_t bpp;
+    switch (storage) {
+        case kU8: type = CU_TENSOR_MAP_DATA_TYPE_UINT8; bpp = 1; break;
+        case kF32: type = CU_TENSOR_MAP_DATA_TYPE_FLOAT32; bpp = 4; break;
+        case kF16: type = CU_TENSOR_MAP_DATA_TYPE_FLOAT16; bpp = 2; break;
+        case kBF16: type = CU_TENSOR_MAP_DATA_TYPE_BFLOAT16; bpp = 2; break;
+        default: return false;
+    }
+    if (reinterpret_cast<uintptr_t>(base) % 16 || (uint64_t(w) * bpp) % 16 ||
+        (uint64_t(box_x) * bpp) % 16 || box_x == 0 || box_x > 256 || box_y == 0 || box_y > 256)
+        return false;
+    const cuuint64_t dims[2] = {w, h};
+    const cuuint64_t pitch[1] = {uint64_t(w) * bpp};
+    const cuuint32_t box[2] = {box_x, box_y};
+    const cuuint32_t step[2] = {1, 1};
+    return encode(m, type, 2, const_cast<void*>(base), dims, pitch, box, step,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
 
 int storage_of(int format) {
     switch (format) {
@@ -142,6 +190,8 @@ struct Prepared {
     bool tiled = false;
     int chunks = 1;             // plane chunks of the tiled sweep
     int tile_x = 32;            // its tile: 32x8 or 16x16 sites
+    int tma_box_x = 0;          // > 0: reference footprints staged by TMA, boxes this wide
+    uint32_t* d_error = nullptr;  // bounded waits that gave up
     SweepShapeKey shape{};      // its launch-shape key for the tuner
     Rank* d_partial = nullptr;  // [chunks][sites] when chunks > 1
     BatchDev b{};
@@ -269,6 +319,21 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
                 sweep_plan_pick(P.shape, heuristic(tiles), heuristic(tiles16), max_chunks);
             P.chunks = plan.chunks;
             P.tile_x = plan.tile_x;
+            // the reference footprint by TMA: a box from the 16-byte boundary at or
+            // left of the footprint, staged in the sweep's sample buffer and the
+            // cost columns after it (the homography parts that follow them are
+            // written while the copy is in flight)
+            const int s = static_cast<int>(s0), ty = 256 / P.tile_x;
+            const int px = (P.tile_x - 1) * s + w, py = (ty - 1) * s + w;
+            const int pxp = (px + s - 1) / s * s;
+            const int box_x = (px + 15 + 15) / 16 * 16;
+            const size_t staged =
+                static_cast<size_t>(box_x) * py * (storage == kF32 ? 4 : storage == kU8 ? 1 : 2) +
+                128;
+            const size_t room = sizeof(float) * (static_cast<size_t>(py) * pxp +
+                                                 static_cast<size_t>(max_src) * 256);
+            if (box_x <= 256 && py <= 256 && staged <= room && tensor_map_encoder())
+                P.tma_box_x = box_x;
         }
     }
     P.n_active = n_active;
@@ -299,6 +364,8 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
     const size_t o_status = cv.take<uint8_t>(cap);
     const size_t o_partial = cv.take<Rank>(P.chunks > 1 ? static_cast<uint64_t>(P.chunks) * cap : 1);
     const size_t o_ctr = cv.take<RefCounters>(n_active);
+    const size_t o_tmaps = cv.take<CUtensorMap>(P.tma_box_x ? used.size() : 1);
+    const size_t o_err = cv.take<uint32_t>(1);
     const uint64_t pc = sweep_only ? 1 : cap;  // pass buffers are not needed for the sweep alone
     // the reciprocal sweep's work queue: a flag and a list entry per (candidate, source)
     size_t queue_src = 1;
@@ -369,6 +436,22 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
         raw_ptr[u] = at(raw_off[u]);
         luma_ptr[u] = at(luma_off[u]);
     }
+    // TMA descriptors of the sampled planes (the depth sweep's reference footprints)
+    std::vector<const void*> tmap_ptr(used.size(), nullptr);
+    if (P.tma_box_x) {
+        const int py = (256 / P.tile_x - 1) * static_cast<int>(plans[active[0]].stride) +
+                       2 * prof.patch_radius + 1;
+        std::vector<CUtensorMap> maps(used.size());
+        for (size_t u = 0; u < used.size(); ++u) {
+            const v3d_frame& f = frames[used[u]];
+            if (encode_plane_map(&maps[u], luma_ptr[u], f.width, f.height, storage,
+                                 static_cast<uint32_t>(P.tma_box_x), static_cast<uint32_t>(py)))
+                tmap_ptr[u] = at(o_tmaps + u * sizeof(CUtensorMap));
+        }
+        // pageable source: the copy has read `maps` when the call returns
+        V3D_CK(cudaMemcpyAsync(at(o_tmaps), maps.data(), sizeof(CUtensorMap) * maps.size(),
+                               cudaMemcpyHostToDevice, stream));
+    }
     const size_t staging = sizeof(DevReference) * n_active + sizeof(uint64_t) * (n_active + 1) +
                            sizeof(float) * inv_count;
     if (!grow(&ctx->pinned, &ctx->pinned_bytes, staging, true)) {
@@ -382,7 +465,8 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
         DevReference& d = hrefs[k];
         set_cam(d.cam, p.ref_cam);
         size_t ru = static_cast<size_t>(dev_of[p.ref_slot]);
-        d.img = DevImage{luma_ptr[ru], frames[p.ref_slot].width, frames[p.ref_slot].height};
+        d.img = DevImage{luma_ptr[ru], frames[p.ref_slot].width, frames[p.ref_slot].height,
+                         tmap_ptr[ru]};
         d.rgba = rgba ? static_cast<const uint8_t*>(raw_ptr[ru]) : nullptr;
         d.focal = p.focal;
         d.planes = p.planes;
@@ -468,6 +552,8 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
     V3D_CK(cudaMemsetAsync(d_status, 0, cap, stream));
     V3D_CK(cudaMemsetAsync(d_ctr, 0, sizeof(RefCounters) * n_active, stream));
     V3D_CK(cudaMemsetAsync(d_counts, 0, sizeof(uint32_t) * 16, stream));
+    P.d_error = reinterpret_cast<uint32_t*>(at(o_err));
+    V3D_CK(cudaMemsetAsync(P.d_error, 0, sizeof(uint32_t), stream));
     V3D_CK(launch_site_ref(reinterpret_cast<const uint64_t*>(at(o_siteoff)),
                            static_cast<int32_t>(n_active), total, d_siteref, stream));
 
@@ -493,6 +579,8 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
     b.prof.min_variance = prof.min_window_variance;
     b.exact = prof.precision == V3D_PRECISION_EXACT64;
     b.sums32 = prof.precision == V3D_PRECISION_FAST32_SUMS32;
+    b.tma_box_x = P.tma_box_x;
+    b.error = P.d_error;
 
     P.stride0 = plans[active[0]].stride;
     return V3D_OK;
@@ -766,7 +854,9 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
     std::vector<RefCounters> ctr(n_active);
     std::vector<uint32_t> base(n_active + 1);
     std::vector<MeshCounters> mcount(mesh ? n_active : 0);
-    uint32_t n_tris = 0;
+    uint32_t n_tris = 0, wait_error = 0;
+    V3D_CK(cudaMemcpyAsync(&wait_error, P.d_error, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                           stream));
     V3D_CK(cudaMemcpyAsync(ctr.data(), d_ctr, sizeof(RefCounters) * n_active,
                            cudaMemcpyDeviceToHost, stream));
     V3D_CK(cudaMemcpyAsync(base.data(), P.o_base, sizeof(uint32_t) * (n_active + 1),
@@ -778,6 +868,10 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
                                cudaMemcpyDeviceToHost, stream));
     }
     V3D_CK(cudaStreamSynchronize(stream));
+    if (wait_error) {
+        ctx->last_error = "a TMA copy of the depth sweep did not complete within its wait";
+        return V3D_ERR_CUDA;
+    }
     cudaEventElapsedTime(&ctx->last_ms, ev0, ev1);
     cudaEventElapsedTime(&ctx->last_sweep_ms, es[0], es[1]);
     if (P.tiled)
@@ -1003,12 +1097,19 @@ int32_t run_sweep_records(v3d_context* ctx, const v3d_profile& prof, const v3d_f
                                  SweepChunks{P.chunks, P.d_partial, P.tile_x}));
     std::vector<SiteRank> rank(P.total);
     std::vector<uint8_t> status(P.total);
+    uint32_t wait_error = 0;
+    V3D_CK(cudaMemcpyAsync(&wait_error, P.d_error, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                           stream));
     if (P.total) {
         V3D_CK(cudaMemcpyAsync(rank.data(), P.d_rank, sizeof(SiteRank) * P.total,
                                cudaMemcpyDeviceToHost, stream));
         V3D_CK(cudaMemcpyAsync(status.data(), P.d_status, P.total, cudaMemcpyDeviceToHost, stream));
     }
     V3D_CK(cudaStreamSynchronize(stream));
+    if (wait_error) {
+        ctx->last_error = "a TMA copy of the depth sweep did not complete within its wait";
+        return V3D_ERR_CUDA;
+    }
     out.resize(P.total);
     for (uint64_t i = 0; i < P.total; ++i) {
         v3d_site_record& r = out[i];

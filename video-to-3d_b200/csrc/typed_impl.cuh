@@ -19,6 +19,40 @@ constexpr double kInf = __builtin_huge_val();
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
 
+// ---- TMA (cp.async.bulk.tensor) into this CTA's shared memory ---------------
+// One mbarrier tracks the copy's bytes; the descriptor lives in global memory
+// and covers only this GPU's frames; no multicast.
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const void* tmap, int x, int y, uint64_t* bar,
+                                            uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                 :: "r"(smem_addr(bar)), "r"(bytes) : "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3}], [%4];"
+        :: "r"(smem_addr(dst)), "l"(reinterpret_cast<uint64_t>(tmap)), "r"(x), "r"(y),
+           "r"(smem_addr(bar))
+        : "memory");
+}
+
+// Waits for phase `parity` of the mbarrier for at most about `cycles` SM
+// clocks; false when it gave up.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long long cycles) {
+    const long long t0 = clock64();
+    for (;;) {
+        uint32_t done;
+        asm volatile(
+            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; "
+            "selp.u32 %0, 1, 0, p; }"
+            : "=r"(done) : "r"(smem_addr(bar)), "r"(parity) : "memory");
+        if (done) return true;
+        if (clock64() - t0 > cycles) return false;
+    }
+}
+
 __device__ __forceinline__ void site_xy(const DevReference& ref, uint32_t local, uint32_t& x,
                                         uint32_t& y) {
     uint32_t gy = local / ref.nx, gx = local - gy * ref.nx;
@@ -407,13 +441,41 @@ __global__ void __launch_bounds__(kTileThreads, 1024 / kTileThreads) k_sweep_til
         slot_xy(fa + 32, e.y, e.w);
         slotxy[i] = e;
     }
+    // The reference footprint with its window halos: by one TMA box when the
+    // frame has a descriptor (the box starts at the 16-byte boundary at or left
+    // of the footprint and lands in the sample and cost buffers, unused until
+    // the first warp step), else by plain loads; then spread into the
+    // x-mod-stride layout.
+    __shared__ uint64_t tma_bar;
+    __shared__ int tma_ok;
+    const T* staged = nullptr;
+    int xa = 0;
+    if (b.tma_box_x > 0 && ref.img.tmap != nullptr) {
+        xa = px0 & ~(16 / (int)sizeof(T) - 1);
+        T* stage = reinterpret_cast<T*>((reinterpret_cast<uintptr_t>(samp) + 127) & ~(uintptr_t)127);
+        if (tid == 0) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_addr(&tma_bar))
+                         : "memory");
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            tma_load_2d(stage, ref.img.tmap, xa, py0, &tma_bar,
+                        (uint32_t)((size_t)b.tma_box_x * PY * sizeof(T)));
+            // about a second at B200 clocks: a copy that has not landed by then never will
+            tma_ok = mbar_wait(&tma_bar, 0, 2000000000LL) ? 1 : 0;
+            if (!tma_ok) atomicOr(b.error, 1u);
+        }
+        __syncthreads();
+        if (!tma_ok) return;  // the host reports the error word
+        staged = stage;
+    }
     for (int i = tid; i < np; i += kTileThreads) {
         const int yy = i / PXp, t = i - yy * PXp;
         const int x = (t % PXs) * s + t / PXs;
         const int X = px0 + x, Y = py0 + yy;
         float v = __int_as_float(0x7fc00000);
         if (x < PX && X >= 0 && Y >= 0 && X < (int)ref.img.width && Y < (int)ref.img.height)
-            v = pix<T>(rdata, (size_t)Y * ref.img.width + X);
+            v = staged ? pix<T>(staged, (size_t)yy * b.tma_box_x + (X - xa))
+                       : pix<T>(rdata, (size_t)Y * ref.img.width + X);
         refv[i] = v;
     }
     const int n_src = ref.n_src;

@@ -47,6 +47,9 @@ struct DevCamera {
 struct DevImage {
     const void* data;  // device pointer, tightly packed rows
     uint32_t width, height;
+    // a 2-D TMA descriptor (CUtensorMap in device memory) of `data` whose box is
+    // the depth sweep's staged reference footprint, or nullptr
+    const void* tmap = nullptr;
 };
 
 struct DevSource {
