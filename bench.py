@@ -17,7 +17,8 @@ v3d_reconstruct_reference_patches_meshed over all 120 references.
 A unit is one window cost between a grid site and one source view at one
 hypothesis (every grid site counts; the contrast gate is reported apart).
 With --gpus N each rank runs its own clip (seed + rank): weak scaling, no
-collective on the data path.  `--impl reference` times the CPU restatement of
+collective on the data path; with --sharded the ranks split one clip's
+references round-robin (strong scaling) and rank 0 gathers the results.  `--impl reference` times the CPU restatement of
 the reference pass on a bounded band of grid rows with all host threads.
 """
 import argparse
@@ -63,6 +64,9 @@ def parse():
                     help="fast32: f32 taps, the depth sweep's box sums in f64 (default); "
                          "sums32: those sums in f32 as well")
     ap.add_argument("--frames", type=int, default=FRAMES)
+    ap.add_argument("--sharded", action="store_true",
+                    help="with --gpus N: one clip, its references round-robin over the ranks "
+                         "(v3d.sharding; strong scaling) instead of one clip per rank")
     ap.add_argument("--no-cpu-baseline", action="store_true",
                     help="skip the CPU baseline leg (profiling runs)")
     ap.add_argument("--config", choices=["full", "small", "heavy", "batched", "served", "fusion",
@@ -102,7 +106,10 @@ def workload(args):
             "planes": PLANES, "window": 2 * RADIUS + 1, "grid_stride": STRIDE,
             "storage": args.storage, "cost": "1-ZNCC", "precision": args.precision,
             "l2": "flushed between timed steps (256 MiB write)",
-            "parallelism": "weak: one clip per GPU, no collective on the data path"}
+            "parallelism": ("strong: one clip, its references round-robin over the GPUs, results "
+                            "gathered on rank 0 (host objects), no collective on the data path"
+                            if args.sharded else
+                            "weak: one clip per GPU, no collective on the data path")}
 
 
 def kernel_rooflines(info, units, b, sweep_ms, recip_sweep_ms, recip_prep_ms, hbm, peak_note):
@@ -338,7 +345,7 @@ def run_ours(args, rank, world, local):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     from v3d import dense, profiles
     from v3d.types import FrameInput
-    clip = load_clip(2 + rank, args.frames)
+    clip = load_clip(2 if args.sharded else 2 + rank, args.frames)
     # frames in pinned host memory, as a caller hands them over
     pinned = []
     for fi in clip.frames(args.storage):
@@ -352,7 +359,12 @@ def run_ours(args, rank, world, local):
     h2d = sum(f.pixels.nbytes for f in frames)
     prof = headline_profile(args)
     ctx = dense.Context(local)
-    refs = list(range(args.frames))
+    all_refs = list(range(args.frames))
+    if args.sharded:
+        from v3d import sharding
+        refs = sharding.references_of_rank(all_refs, rank, world)
+    else:
+        refs = all_refs
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
     def step():
@@ -403,6 +415,16 @@ def run_ours(args, rank, world, local):
     recip_ms = float(np.mean([i["reciprocal_ms"] for i in infos]))
     comp_ms = float(np.mean([i["completion_ms"] for i in infos]))
     mesh_ms = float(np.mean([i["mesh_ms"] for i in infos]))
+    gathered = None
+    if args.sharded and dist:
+        # after the timed steps: every rank's host results on rank 0, in reference order
+        from v3d import sharding
+        full = sharding.reconstruct_reference_patches_sharded(
+            lambda idx: ctx.reconstruct_reference_patches(frames, clip.cameras, clip.sparse,
+                                                          clip.focal, idx, profile=prof),
+            all_refs)
+        if rank == 0:
+            gathered = sum(1 for r in full if r is not None)
     line = None
     if rank == 0:
         peaks = {}
@@ -421,7 +443,7 @@ def run_ours(args, rank, world, local):
         line = {
             "metric": METRIC, "value": total_units / dev_s, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_s * 1e3,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "higher_is_better": True, "scaling": "strong" if args.sharded else "weak", "vs_baseline": None,
             "dtype": ARITH[args.storage],
             "data": "synthetic (seeded value-noise planes, ray-cast)", "config": workload(args),
             "clocks": clk,
@@ -439,6 +461,8 @@ def run_ours(args, rank, world, local):
             "points_per_step": points,
             "triangles_per_step": triangles,
         }
+        if gathered is not None:
+            line["sharded_references_gathered"] = gathered
         if world == 1 and not args.no_cpu_baseline:
             v, info = cpu_baseline(clip, frames, prof, os.cpu_count() or 1)
             line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": info["cores"],
