@@ -104,8 +104,11 @@ def attribute(g, g_sweep, o, o_rec, prof, band, rows=None):
         rep["max_cost_error"] = float(np.max(errs))
         rep["median_cost_error"] = float(np.median(errs))
     # ---- points --------------------------------------------------------------
-    n_gp = g.stats["accepted_points"]
-    n_op = o.stats["accepted_points"] if rows is None else len(o.points)
+    # accepted_points counts the completed points too (dense_legacy.rs sets it after
+    # completion); the primaries come first
+    n_gp = g.stats["accepted_points"] - g.stats["surface_completed_points"]
+    n_op = (o.stats["accepted_points"] - o.stats["surface_completed_points"] if rows is None
+            else len(o.points))
 
     def table(a, lo, hi):
         t = {}

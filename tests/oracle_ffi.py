@@ -302,7 +302,7 @@ class Oracle:
             int(descriptor_radius), C.byref(profile), fn, None, C.byref(out), plan)
         if st < 0:
             raise ValueError("oracle rejected the inputs (status %d)" % st)
-        res = types.dense_from_result(out)
+        res = types.dense_from_result(out, st)
         L.v3do_dense_result_free(C.byref(out))
         v = [int(x) for x in plan]
         return res, {"working_set_estimate": dict(zip(abi.WORKING_SET_FIELDS, v[:12])),

@@ -458,6 +458,9 @@ __global__ void __launch_bounds__(kTileThreads, 1024 / kTileThreads) k_sweep_til
                          : "memory");
             asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            // the descriptors live in the batch arena, rewritten by every call
+            asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;"
+                         :: "l"(reinterpret_cast<uint64_t>(ref.img.tmap)) : "memory");
             tma_load_2d(stage, ref.img.tmap, xa, py0, &tma_bar,
                         (uint32_t)((size_t)b.tma_box_x * PY * sizeof(T)));
             // about a second at B200 clocks: a copy that has not landed by then never will
