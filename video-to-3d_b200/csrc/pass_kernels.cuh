@@ -187,6 +187,10 @@ struct RecipQueue {
     // the single-view sweep and after it (the exact policy's one kernel counts as
     // the sweep)
     cudaEvent_t t_prepare = nullptr, t_sweep = nullptr, t_end = nullptr;
+    // pairs whose band does not fit the banded sweep's stage, for the
+    // per-hypothesis sweep: [cap_items] entries and their device count
+    uint32_t* fallback = nullptr;
+    uint32_t* n_fallback = nullptr;
 };
 cudaError_t launch_reciprocal(const BatchDev& b, const Cand* cands, const uint32_t* count_dev,
                               uint64_t cap, RecipObs* obs, RefCounters* counters,

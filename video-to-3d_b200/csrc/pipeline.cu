@@ -379,6 +379,7 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
     const size_t o_scratch = cv.take<uint8_t>(compaction_scratch_bytes(pq));
     const size_t o_qflags = cv.take<uint8_t>(pq);
     const size_t o_qitems = cv.take<uint32_t>(pq);
+    const size_t o_qfall = cv.take<uint32_t>(pq);
     const size_t o_idx = cv.take<uint32_t>(pc);
     const size_t o_cands = cv.take<Cand>(pc);
     const size_t o_cstat = cv.take<uint8_t>(pc);
@@ -535,6 +536,8 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
     P.d_prop = reinterpret_cast<Cand*>(at(o_prop));
     auto* d_counts = P.d_counts = reinterpret_cast<uint32_t*>(at(o_counts));
     P.queue.n_items = P.d_counts + 9;  // [8] completion seeds, [9] reciprocal items
+    P.queue.fallback = reinterpret_cast<uint32_t*>(at(o_qfall));
+    P.queue.n_fallback = P.d_counts + 10;  // [10] pairs for the per-hypothesis sweep
     P.o_pts = reinterpret_cast<v3d_point*>(at(o_opts));
     P.o_sites = reinterpret_cast<v3d_grid_site*>(at(o_osites));
     P.o_attrs = reinterpret_cast<v3d_point_attributes*>(at(o_oattrs));

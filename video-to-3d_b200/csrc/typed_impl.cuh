@@ -1226,11 +1226,22 @@ __global__ void __launch_bounds__(256) k_recip_prepare(BatchDev b, const Cand* _
     }
 }
 
-template <class T, int R, int COST>
-__global__ void __launch_bounds__(256, 2) k_recip_sweep(BatchDev b, const Cand* __restrict__ cands,
-                                                     const uint32_t* __restrict__ list,
-                                                     const uint32_t* __restrict__ list_count,
-                                                     RecipObs* __restrict__ obs) {
+// MODE kRecipBanded takes the pairs whose band fits the stage and appends the
+// others to `fallback`; kRecipPerHypothesis takes a list with the per-hypothesis
+// domain tests only.  The banded kernel needs fewer registers and runs three
+// blocks per SM.
+constexpr int kRecipBanded = 1, kRecipPerHypothesis = 2;
+
+template <int MODE>
+struct RecipBounds {
+    static constexpr int kBlocks = MODE == kRecipBanded ? 3 : 2;
+};
+
+template <class T, int R, int COST, int MODE>
+__global__ void __launch_bounds__(256, RecipBounds<MODE>::kBlocks) k_recip_sweep(
+    BatchDev b, const Cand* __restrict__ cands, const uint32_t* __restrict__ list,
+    const uint32_t* __restrict__ list_count, RecipObs* __restrict__ obs,
+    uint32_t* __restrict__ fallback, uint32_t* __restrict__ n_fallback) {
     constexpr int W = 2 * R + 1;
     constexpr int N = W * W;
     __shared__ float pvc_all[8][N];
@@ -1293,8 +1304,16 @@ __global__ void __launch_bounds__(256, 2) k_recip_sweep(BatchDev b, const Cand* 
         };
         // every hypothesis's window inside one staged box of the reference
         int bx0 = 0, by0 = 0, cols = 0, rows = 0;
-        const bool banded = band_box<R>(src.bwd_A, src.bwd_b, inv_tab[0], inv_tab[ref.planes - 1],
-                                        wl, hl, x0, y0, bx0, by0, cols, rows);
+        const bool banded =
+            MODE == kRecipBanded && band_box<R>(src.bwd_A, src.bwd_b, inv_tab[0],
+                                                inv_tab[ref.planes - 1], wl, hl, x0, y0, bx0,
+                                                by0, cols, rows);
+        if (MODE == kRecipBanded && !banded) {
+            // the per-hypothesis kernel takes this pair
+            if (lane == 0) fallback[atomicAdd(n_fallback, 1u)] = item;
+            __syncwarp();
+            continue;
+        }
         if (banded) {
             for (int rr = 0; rr < rows; ++rr) {
                 const T* row = rimg + (size_t)(by0 + rr) * rw + bx0;
@@ -1558,6 +1577,12 @@ cudaError_t Typed<T>::reciprocal(const BatchDev& b, const Cand* cands, const uin
                                  cudaStream_t st) {
     using namespace typed_detail;
     const unsigned blocks = (unsigned)sm_count() * 8;
+    const unsigned rblocks3 = (unsigned)sm_count() * 12;  // the banded sweep, 3 blocks an SM
+#define V3D_CK_RET(x)                                \
+    do {                                             \
+        const cudaError_t e_ = (x);                  \
+        if (e_ != cudaSuccess) return e_;            \
+    } while (0)
     auto mark = [&](cudaEvent_t e) {
         if (e) cudaEventRecord(e, st);
     };
@@ -1579,20 +1604,27 @@ cudaError_t Typed<T>::reciprocal(const BatchDev& b, const Cand* cands, const uin
             const cudaError_t e = prep_and_list(k_recip_prepare<T, RR, 1>);                    \
             if (e != cudaSuccess) return e;                                                    \
             mark(q.t_sweep);                                                                   \
-            V3D_COUNTED k_recip_sweep<T, RR, 1><<<blocks, 256, 0, st>>>(b, cands, q.items,     \
-                                                                        q.n_items, obs);       \
+            V3D_CK_RET(cudaMemsetAsync(q.n_fallback, 0, sizeof(uint32_t), st));               \
+            V3D_COUNTED k_recip_sweep<T, RR, 1, kRecipBanded><<<rblocks3, 256, 0, st>>>(        \
+                b, cands, q.items, q.n_items, obs, q.fallback, q.n_fallback);                 \
+            V3D_COUNTED k_recip_sweep<T, RR, 1, kRecipPerHypothesis><<<blocks, 256, 0, st>>>(   \
+                b, cands, q.fallback, q.n_fallback, obs, nullptr, nullptr);                    \
         } else {                                                                               \
             const cudaError_t e = prep_and_list(k_recip_prepare<T, RR, 0>);                    \
             if (e != cudaSuccess) return e;                                                    \
             mark(q.t_sweep);                                                                   \
-            V3D_COUNTED k_recip_sweep<T, RR, 0><<<blocks, 256, 0, st>>>(b, cands, q.items,     \
-                                                                        q.n_items, obs);       \
+            V3D_CK_RET(cudaMemsetAsync(q.n_fallback, 0, sizeof(uint32_t), st));               \
+            V3D_COUNTED k_recip_sweep<T, RR, 0, kRecipBanded><<<rblocks3, 256, 0, st>>>(        \
+                b, cands, q.items, q.n_items, obs, q.fallback, q.n_fallback);                 \
+            V3D_COUNTED k_recip_sweep<T, RR, 0, kRecipPerHypothesis><<<blocks, 256, 0, st>>>(   \
+                b, cands, q.fallback, q.n_fallback, obs, nullptr, nullptr);                    \
         }                                                                                      \
         mark(q.t_end);                                                                         \
         return cudaGetLastError();                                                             \
     }
     V3D_REC(1) V3D_REC(2) V3D_REC(3) V3D_REC(4)
 #undef V3D_REC
+#undef V3D_CK_RET
     return cudaErrorInvalidValue;
 }
 
