@@ -10,8 +10,6 @@
 //   per cand    candidates, 16 reciprocal slots, fused output, status
 //   pool        accepted points: primaries, then completion pass 1, then pass 2,
 //               each segment in (reference, raster) order
-#include <cuda.h>
-#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <cub/block/block_scan.cuh>
@@ -40,52 +38,6 @@ struct Carver {
         return at;
     }
 };
-
-// cuTensorMapEncodeTiled through the runtime's driver entry point (the library
-// links no driver library); null when the driver does not offer it.
-PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
-    static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
-        void* p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) !=
-                cudaSuccess ||
-            q != cudaDriverEntryPointSuccess) {
-            cudaGetLastError();
-            return static_cast<PFN_cuTensorMapEncodeTiled_v12000>(nullptr);
-        }
-        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-    }();
-    return fn;
-}
-
-// A 2-D descriptor of a w x h plane of `storage` texels with a box_x x box_y
-// box: false where TMA cannot address the plane (base or row pitch not a
-// multiple of 16 bytes) or the encoder refuses it.
-bool encode_plane_map(CUtensorMap* m, const void* base, uint32_t w, uint32_t h, int storage,
-                      uint32_t box_x, uint32_t box_y) {
-    const PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
-    if (!encode) return false;
-    CUtensorMapDataType type;
-    uint32_t bpp;
-    switch (storage) {
-        case kU8: type = CU_TENSOR_MAP_DATA_TYPE_UINT8; bpp = 1; break;
-        case kF32: type = CU_TENSOR_MAP_DATA_TYPE_FLOAT32; bpp = 4; break;
-        case kF16: type = CU_TENSOR_MAP_DATA_TYPE_FLOAT16; bpp = 2; break;
-        case kBF16: type = CU_TENSOR_MAP_DATA_TYPE_BFLOAT16; bpp = 2; break;
-        default: return false;
-    }
-    if (reinterpret_cast<uintptr_t>(base) % 16 || (uint64_t(w) * bpp) % 16 ||
-        (uint64_t(box_x) * bpp) % 16 || box_x == 0 || box_x > 256 || box_y == 0 || box_y > 256)
-        return false;
-    const cuuint64_t dims[2] = {w, h};
-    const cuuint64_t pitch[1] = {uint64_t(w) * bpp};
-    const cuuint32_t box[2] = {box_x, box_y};
-    const cuuint32_t step[2] = {1, 1};
-    return encode(m, type, 2, const_cast<void*>(base), dims, pitch, box, step,
-                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                  CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
-}
 
 int storage_of(int format) {
     switch (format) {
@@ -190,7 +142,7 @@ struct Prepared {
     bool tiled = false;
     int chunks = 1;             // plane chunks of the tiled sweep
     int tile_x = 32;            // its tile: 32x8 or 16x16 sites
-    int tma_box_x = 0;          // > 0: reference footprints staged by TMA, boxes this wide
+    int tma_box_x = 0;          // > 0: reference footprint rows staged by TMA bulk copies, this wide
     uint32_t* d_error = nullptr;  // bounded waits that gave up
     SweepShapeKey shape{};      // its launch-shape key for the tuner
     Rank* d_partial = nullptr;  // [chunks][sites] when chunks > 1
@@ -319,10 +271,10 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
                 sweep_plan_pick(P.shape, heuristic(tiles), heuristic(tiles16), max_chunks);
             P.chunks = plan.chunks;
             P.tile_x = plan.tile_x;
-            // the reference footprint by TMA: a box from the 16-byte boundary at or
-            // left of the footprint, staged in the sweep's sample buffer and the
-            // cost columns after it (the homography parts that follow them are
-            // written while the copy is in flight)
+            // the reference footprint by TMA bulk row copies: rows from the 16-byte
+            // boundary at or left of the footprint, staged in the sweep's sample
+            // buffer and the cost columns after it (the homography parts that
+            // follow them are written while the copies are in flight)
             const int s = static_cast<int>(s0), ty = 256 / P.tile_x;
             const int px = (P.tile_x - 1) * s + w, py = (ty - 1) * s + w;
             const int pxp = (px + s - 1) / s * s;
@@ -332,8 +284,7 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
                 128;
             const size_t room = sizeof(float) * (static_cast<size_t>(py) * pxp +
                                                  static_cast<size_t>(max_src) * 256);
-            if (box_x <= 256 && py <= 256 && staged <= room && tensor_map_encoder())
-                P.tma_box_x = box_x;
+            if (staged <= room) P.tma_box_x = box_x;
         }
     }
     P.n_active = n_active;
@@ -364,7 +315,6 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
     const size_t o_status = cv.take<uint8_t>(cap);
     const size_t o_partial = cv.take<Rank>(P.chunks > 1 ? static_cast<uint64_t>(P.chunks) * cap : 1);
     const size_t o_ctr = cv.take<RefCounters>(n_active);
-    const size_t o_tmaps = cv.take<CUtensorMap>(P.tma_box_x ? used.size() : 1);
     const size_t o_err = cv.take<uint32_t>(1);
     const uint64_t pc = sweep_only ? 1 : cap;  // pass buffers are not needed for the sweep alone
     // the reciprocal sweep's work queue: a flag and a list entry per (candidate, source)
@@ -437,21 +387,13 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
         raw_ptr[u] = at(raw_off[u]);
         luma_ptr[u] = at(luma_off[u]);
     }
-    // TMA descriptors of the sampled planes (the depth sweep's reference footprints)
-    std::vector<const void*> tmap_ptr(used.size(), nullptr);
-    if (P.tma_box_x) {
-        const int py = (256 / P.tile_x - 1) * static_cast<int>(plans[active[0]].stride) +
-                       2 * prof.patch_radius + 1;
-        std::vector<CUtensorMap> maps(used.size());
-        for (size_t u = 0; u < used.size(); ++u) {
-            const v3d_frame& f = frames[used[u]];
-            if (encode_plane_map(&maps[u], luma_ptr[u], f.width, f.height, storage,
-                                 static_cast<uint32_t>(P.tma_box_x), static_cast<uint32_t>(py)))
-                tmap_ptr[u] = at(o_tmaps + u * sizeof(CUtensorMap));
-        }
-        // pageable source: the copy has read `maps` when the call returns
-        V3D_CK(cudaMemcpyAsync(at(o_tmaps), maps.data(), sizeof(CUtensorMap) * maps.size(),
-                               cudaMemcpyHostToDevice, stream));
+    // planes whose rows bulk asynchronous copies can move: base and row pitch
+    // multiples of 16 bytes
+    std::vector<int32_t> bulk_rows(used.size(), 0);
+    for (size_t u = 0; u < used.size(); ++u) {
+        const uint64_t pitch = uint64_t(frames[used[u]].width) *
+                               (storage == kF32 ? 4 : storage == kU8 ? 1 : 2);
+        bulk_rows[u] = reinterpret_cast<uintptr_t>(luma_ptr[u]) % 16 == 0 && pitch % 16 == 0;
     }
     const size_t staging = sizeof(DevReference) * n_active + sizeof(uint64_t) * (n_active + 1) +
                            sizeof(float) * inv_count;
@@ -467,7 +409,7 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
         set_cam(d.cam, p.ref_cam);
         size_t ru = static_cast<size_t>(dev_of[p.ref_slot]);
         d.img = DevImage{luma_ptr[ru], frames[p.ref_slot].width, frames[p.ref_slot].height,
-                         tmap_ptr[ru]};
+                         bulk_rows[ru]};
         d.rgba = rgba ? static_cast<const uint8_t*>(raw_ptr[ru]) : nullptr;
         d.focal = p.focal;
         d.planes = p.planes;

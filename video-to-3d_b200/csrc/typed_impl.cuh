@@ -19,22 +19,20 @@ constexpr double kInf = __builtin_huge_val();
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
 
-// ---- TMA (cp.async.bulk.tensor) into this CTA's shared memory ---------------
-// One mbarrier tracks the copy's bytes; the descriptor lives in global memory
-// and covers only this GPU's frames; no multicast.
+// ---- TMA bulk copies (cp.async.bulk) into this CTA's shared memory ----------
+// One mbarrier tracks the copies' bytes; every source is this GPU's own frame
+// memory; no multicast.
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
-__device__ __forceinline__ void tma_load_2d(void* dst, const void* tmap, int x, int y, uint64_t* bar,
-                                            uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
-                 :: "r"(smem_addr(bar)), "r"(bytes) : "memory");
+// One row of bytes from global memory into this CTA's shared memory, counted
+// on the mbarrier; both addresses 16-byte aligned, the size a multiple of 16.
+__device__ __forceinline__ void bulk_row_g2s(void* dst, const void* src, uint32_t bytes,
+                                             uint64_t* bar) {
     asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
-        " [%0], [%1, {%2, %3}], [%4];"
-        :: "r"(smem_addr(dst)), "l"(reinterpret_cast<uint64_t>(tmap)), "r"(x), "r"(y),
-           "r"(smem_addr(bar))
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+        :: "r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar))
         : "memory");
 }
 
@@ -441,29 +439,36 @@ __global__ void __launch_bounds__(kTileThreads, 1024 / kTileThreads) k_sweep_til
         slot_xy(fa + 32, e.y, e.w);
         slotxy[i] = e;
     }
-    // The reference footprint with its window halos: by one TMA box when the
-    // frame has a descriptor (the box starts at the 16-byte boundary at or left
-    // of the footprint and lands in the sample and cost buffers, unused until
-    // the first warp step), else by plain loads; then spread into the
-    // x-mod-stride layout.
+    // The reference footprint with its window halos: its rows by TMA bulk copies
+    // when the frame allows them (each row from the 16-byte boundary at or left
+    // of the footprint, clamped to the image, into the sample and cost buffers,
+    // unused until the first warp step), else by plain loads; then spread into
+    // the x-mod-stride layout.
     __shared__ uint64_t tma_bar;
     __shared__ int tma_ok;
     const T* staged = nullptr;
     int xa = 0;
-    if (b.tma_box_x > 0 && ref.img.tmap != nullptr) {
+    if (b.tma_box_x > 0 && ref.img.bulk_rows) {
         xa = px0 & ~(16 / (int)sizeof(T) - 1);
         T* stage = reinterpret_cast<T*>((reinterpret_cast<uintptr_t>(samp) + 127) & ~(uintptr_t)127);
+        // px0 and py0 lie inside the image (a tile exists only with a site inside)
+        const int cols = min(b.tma_box_x, (int)ref.img.width - xa);
+        const int rows = min(PY, (int)ref.img.height - py0);
+        const uint32_t row_bytes = (uint32_t)(cols * sizeof(T));
         if (tid == 0) {
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_addr(&tma_bar))
                          : "memory");
             asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            // the descriptors live in the batch arena, rewritten by every call
-            asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;"
-                         :: "l"(reinterpret_cast<uint64_t>(ref.img.tmap)) : "memory");
-            tma_load_2d(stage, ref.img.tmap, xa, py0, &tma_bar,
-                        (uint32_t)((size_t)b.tma_box_x * PY * sizeof(T)));
-            // about a second at B200 clocks: a copy that has not landed by then never will
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                         :: "r"(smem_addr(&tma_bar)), "r"(row_bytes * (uint32_t)rows) : "memory");
+        }
+        __syncthreads();
+        if (tid < 32)
+            for (int r = tid; r < rows; r += 32)
+                bulk_row_g2s(stage + (size_t)r * b.tma_box_x,
+                             rdata + (size_t)(py0 + r) * ref.img.width + xa, row_bytes, &tma_bar);
+        if (tid == 0) {
+            // about a second at B200 clocks: copies that have not landed by then never will
             tma_ok = mbar_wait(&tma_bar, 0, 2000000000LL) ? 1 : 0;
             if (!tma_ok) atomicOr(b.error, 1u);
         }

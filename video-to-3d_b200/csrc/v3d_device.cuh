@@ -47,9 +47,10 @@ struct DevCamera {
 struct DevImage {
     const void* data;  // device pointer, tightly packed rows
     uint32_t width, height;
-    // a 2-D TMA descriptor (CUtensorMap in device memory) of `data` whose box is
-    // the depth sweep's staged reference footprint, or nullptr
-    const void* tmap = nullptr;
+    // 1 when the base and the row pitch are multiples of 16 bytes, so rows can
+    // move by bulk asynchronous copies (cp.async.bulk)
+    int32_t bulk_rows = 0;
+    int32_t pad_ = 0;
 };
 
 struct DevSource {
