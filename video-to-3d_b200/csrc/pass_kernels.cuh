@@ -109,9 +109,6 @@ struct BatchDev {
     DevProfile prof;
     bool exact;
     bool sums32;                // the box-filtered sweep's window sums in f32
-    int32_t tma_box_x;          // > 0: the sweep stages reference footprint rows by TMA bulk
-                                // copies, rows this many texels apart
-    uint32_t* error;            // device word: nonzero when a bounded wait gave up
 };
 
 // Launch wrappers (pass_kernels.cu).  All run on `stream`; none synchronises.

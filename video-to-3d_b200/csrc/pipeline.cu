@@ -142,8 +142,6 @@ struct Prepared {
     bool tiled = false;
     int chunks = 1;             // plane chunks of the tiled sweep
     int tile_x = 32;            // its tile: 32x8 or 16x16 sites
-    int tma_box_x = 0;          // > 0: reference footprint rows staged by TMA bulk copies, this wide
-    uint32_t* d_error = nullptr;  // bounded waits that gave up
     SweepShapeKey shape{};      // its launch-shape key for the tuner
     Rank* d_partial = nullptr;  // [chunks][sites] when chunks > 1
     BatchDev b{};
@@ -271,20 +269,6 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
                 sweep_plan_pick(P.shape, heuristic(tiles), heuristic(tiles16), max_chunks);
             P.chunks = plan.chunks;
             P.tile_x = plan.tile_x;
-            // the reference footprint by TMA bulk row copies: rows from the 16-byte
-            // boundary at or left of the footprint, staged in the sweep's sample
-            // buffer and the cost columns after it (the homography parts that
-            // follow them are written while the copies are in flight)
-            const int s = static_cast<int>(s0), ty = 256 / P.tile_x;
-            const int px = (P.tile_x - 1) * s + w, py = (ty - 1) * s + w;
-            const int pxp = (px + s - 1) / s * s;
-            const int box_x = (px + 15 + 15) / 16 * 16;
-            const size_t staged =
-                static_cast<size_t>(box_x) * py * (storage == kF32 ? 4 : storage == kU8 ? 1 : 2) +
-                128;
-            const size_t room = sizeof(float) * (static_cast<size_t>(py) * pxp +
-                                                 static_cast<size_t>(max_src) * 256);
-            if (staged <= room) P.tma_box_x = box_x;
         }
     }
     P.n_active = n_active;
@@ -315,7 +299,6 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
     const size_t o_status = cv.take<uint8_t>(cap);
     const size_t o_partial = cv.take<Rank>(P.chunks > 1 ? static_cast<uint64_t>(P.chunks) * cap : 1);
     const size_t o_ctr = cv.take<RefCounters>(n_active);
-    const size_t o_err = cv.take<uint32_t>(1);
     const uint64_t pc = sweep_only ? 1 : cap;  // pass buffers are not needed for the sweep alone
     // the reciprocal sweep's work queue: a flag and a list entry per (candidate, source)
     size_t queue_src = 1;
@@ -387,14 +370,6 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
         raw_ptr[u] = at(raw_off[u]);
         luma_ptr[u] = at(luma_off[u]);
     }
-    // planes whose rows bulk asynchronous copies can move: base and row pitch
-    // multiples of 16 bytes
-    std::vector<int32_t> bulk_rows(used.size(), 0);
-    for (size_t u = 0; u < used.size(); ++u) {
-        const uint64_t pitch = uint64_t(frames[used[u]].width) *
-                               (storage == kF32 ? 4 : storage == kU8 ? 1 : 2);
-        bulk_rows[u] = reinterpret_cast<uintptr_t>(luma_ptr[u]) % 16 == 0 && pitch % 16 == 0;
-    }
     const size_t staging = sizeof(DevReference) * n_active + sizeof(uint64_t) * (n_active + 1) +
                            sizeof(float) * inv_count;
     if (!grow(&ctx->pinned, &ctx->pinned_bytes, staging, true)) {
@@ -408,8 +383,7 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
         DevReference& d = hrefs[k];
         set_cam(d.cam, p.ref_cam);
         size_t ru = static_cast<size_t>(dev_of[p.ref_slot]);
-        d.img = DevImage{luma_ptr[ru], frames[p.ref_slot].width, frames[p.ref_slot].height,
-                         bulk_rows[ru]};
+        d.img = DevImage{luma_ptr[ru], frames[p.ref_slot].width, frames[p.ref_slot].height};
         d.rgba = rgba ? static_cast<const uint8_t*>(raw_ptr[ru]) : nullptr;
         d.focal = p.focal;
         d.planes = p.planes;
@@ -497,8 +471,6 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
     V3D_CK(cudaMemsetAsync(d_status, 0, cap, stream));
     V3D_CK(cudaMemsetAsync(d_ctr, 0, sizeof(RefCounters) * n_active, stream));
     V3D_CK(cudaMemsetAsync(d_counts, 0, sizeof(uint32_t) * 16, stream));
-    P.d_error = reinterpret_cast<uint32_t*>(at(o_err));
-    V3D_CK(cudaMemsetAsync(P.d_error, 0, sizeof(uint32_t), stream));
     V3D_CK(launch_site_ref(reinterpret_cast<const uint64_t*>(at(o_siteoff)),
                            static_cast<int32_t>(n_active), total, d_siteref, stream));
 
@@ -524,8 +496,6 @@ int32_t prepare(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fram
     b.prof.min_variance = prof.min_window_variance;
     b.exact = prof.precision == V3D_PRECISION_EXACT64;
     b.sums32 = prof.precision == V3D_PRECISION_FAST32_SUMS32;
-    b.tma_box_x = P.tma_box_x;
-    b.error = P.d_error;
 
     P.stride0 = plans[active[0]].stride;
     return V3D_OK;
@@ -799,9 +769,7 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
     std::vector<RefCounters> ctr(n_active);
     std::vector<uint32_t> base(n_active + 1);
     std::vector<MeshCounters> mcount(mesh ? n_active : 0);
-    uint32_t n_tris = 0, wait_error = 0;
-    V3D_CK(cudaMemcpyAsync(&wait_error, P.d_error, sizeof(uint32_t), cudaMemcpyDeviceToHost,
-                           stream));
+    uint32_t n_tris = 0;
     V3D_CK(cudaMemcpyAsync(ctr.data(), d_ctr, sizeof(RefCounters) * n_active,
                            cudaMemcpyDeviceToHost, stream));
     V3D_CK(cudaMemcpyAsync(base.data(), P.o_base, sizeof(uint32_t) * (n_active + 1),
@@ -813,10 +781,6 @@ int32_t run_batch(v3d_context* ctx, const v3d_profile& prof, const v3d_frame* fr
                                cudaMemcpyDeviceToHost, stream));
     }
     V3D_CK(cudaStreamSynchronize(stream));
-    if (wait_error) {
-        ctx->last_error = "a TMA copy of the depth sweep did not complete within its wait";
-        return V3D_ERR_CUDA;
-    }
     cudaEventElapsedTime(&ctx->last_ms, ev0, ev1);
     cudaEventElapsedTime(&ctx->last_sweep_ms, es[0], es[1]);
     if (P.tiled)
@@ -1042,19 +1006,12 @@ int32_t run_sweep_records(v3d_context* ctx, const v3d_profile& prof, const v3d_f
                                  SweepChunks{P.chunks, P.d_partial, P.tile_x}));
     std::vector<SiteRank> rank(P.total);
     std::vector<uint8_t> status(P.total);
-    uint32_t wait_error = 0;
-    V3D_CK(cudaMemcpyAsync(&wait_error, P.d_error, sizeof(uint32_t), cudaMemcpyDeviceToHost,
-                           stream));
     if (P.total) {
         V3D_CK(cudaMemcpyAsync(rank.data(), P.d_rank, sizeof(SiteRank) * P.total,
                                cudaMemcpyDeviceToHost, stream));
         V3D_CK(cudaMemcpyAsync(status.data(), P.d_status, P.total, cudaMemcpyDeviceToHost, stream));
     }
     V3D_CK(cudaStreamSynchronize(stream));
-    if (wait_error) {
-        ctx->last_error = "a TMA copy of the depth sweep did not complete within its wait";
-        return V3D_ERR_CUDA;
-    }
     out.resize(P.total);
     for (uint64_t i = 0; i < P.total; ++i) {
         v3d_site_record& r = out[i];

@@ -19,38 +19,6 @@ constexpr double kInf = __builtin_huge_val();
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
 
-// ---- TMA bulk copies (cp.async.bulk) into this CTA's shared memory ----------
-// One mbarrier tracks the copies' bytes; every source is this GPU's own frame
-// memory; no multicast.
-__device__ __forceinline__ uint32_t smem_addr(const void* p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-// One row of bytes from global memory into this CTA's shared memory, counted
-// on the mbarrier; both addresses 16-byte aligned, the size a multiple of 16.
-__device__ __forceinline__ void bulk_row_g2s(void* dst, const void* src, uint32_t bytes,
-                                             uint64_t* bar) {
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-        :: "r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar))
-        : "memory");
-}
-
-// Waits for phase `parity` of the mbarrier for at most about `cycles` SM
-// clocks; false when it gave up.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long long cycles) {
-    const long long t0 = clock64();
-    for (;;) {
-        uint32_t done;
-        asm volatile(
-            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; "
-            "selp.u32 %0, 1, 0, p; }"
-            : "=r"(done) : "r"(smem_addr(bar)), "r"(parity) : "memory");
-        if (done) return true;
-        if (clock64() - t0 > cycles) return false;
-    }
-}
-
 __device__ __forceinline__ void site_xy(const DevReference& ref, uint32_t local, uint32_t& x,
                                         uint32_t& y) {
     uint32_t gy = local / ref.nx, gx = local - gy * ref.nx;
@@ -439,51 +407,13 @@ __global__ void __launch_bounds__(kTileThreads, 1024 / kTileThreads) k_sweep_til
         slot_xy(fa + 32, e.y, e.w);
         slotxy[i] = e;
     }
-    // The reference footprint with its window halos: its rows by TMA bulk copies
-    // when the frame allows them (each row from the 16-byte boundary at or left
-    // of the footprint, clamped to the image, into the sample and cost buffers,
-    // unused until the first warp step), else by plain loads; then spread into
-    // the x-mod-stride layout.
-    __shared__ uint64_t tma_bar;
-    __shared__ int tma_ok;
-    const T* staged = nullptr;
-    int xa = 0;
-    if (b.tma_box_x > 0 && ref.img.bulk_rows) {
-        xa = px0 & ~(16 / (int)sizeof(T) - 1);
-        T* stage = reinterpret_cast<T*>((reinterpret_cast<uintptr_t>(samp) + 127) & ~(uintptr_t)127);
-        // px0 and py0 lie inside the image (a tile exists only with a site inside)
-        const int cols = min(b.tma_box_x, (int)ref.img.width - xa);
-        const int rows = min(PY, (int)ref.img.height - py0);
-        const uint32_t row_bytes = (uint32_t)(cols * sizeof(T));
-        if (tid == 0) {
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_addr(&tma_bar))
-                         : "memory");
-            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
-                         :: "r"(smem_addr(&tma_bar)), "r"(row_bytes * (uint32_t)rows) : "memory");
-        }
-        __syncthreads();
-        if (tid < 32)
-            for (int r = tid; r < rows; r += 32)
-                bulk_row_g2s(stage + (size_t)r * b.tma_box_x,
-                             rdata + (size_t)(py0 + r) * ref.img.width + xa, row_bytes, &tma_bar);
-        if (tid == 0) {
-            // about a second at B200 clocks: copies that have not landed by then never will
-            tma_ok = mbar_wait(&tma_bar, 0, 2000000000LL) ? 1 : 0;
-            if (!tma_ok) atomicOr(b.error, 1u);
-        }
-        __syncthreads();
-        if (!tma_ok) return;  // the host reports the error word
-        staged = stage;
-    }
     for (int i = tid; i < np; i += kTileThreads) {
         const int yy = i / PXp, t = i - yy * PXp;
         const int x = (t % PXs) * s + t / PXs;
         const int X = px0 + x, Y = py0 + yy;
         float v = __int_as_float(0x7fc00000);
         if (x < PX && X >= 0 && Y >= 0 && X < (int)ref.img.width && Y < (int)ref.img.height)
-            v = staged ? pix<T>(staged, (size_t)yy * b.tma_box_x + (X - xa))
-                       : pix<T>(rdata, (size_t)Y * ref.img.width + X);
+            v = pix<T>(rdata, (size_t)Y * ref.img.width + X);
         refv[i] = v;
     }
     const int n_src = ref.n_src;

@@ -47,10 +47,6 @@ struct DevCamera {
 struct DevImage {
     const void* data;  // device pointer, tightly packed rows
     uint32_t width, height;
-    // 1 when the base and the row pitch are multiples of 16 bytes, so rows can
-    // move by bulk asynchronous copies (cp.async.bulk)
-    int32_t bulk_rows = 0;
-    int32_t pad_ = 0;
 };
 
 struct DevSource {
