@@ -223,7 +223,7 @@ def load_clip(seed, frames):
     """The seeded clip (with its true depth maps), cached under the system temp
     directory between runs."""
     from v3d import synth
-    path = os.path.join(tempfile.gettempdir(), "v3d_clip2_%d_%d_%d_%d.npz" %
+    path = os.path.join(tempfile.gettempdir(), "v3d_clip3_%d_%d_%d_%d.npz" %
                         (seed, WIDTH, HEIGHT, frames))
     if os.path.exists(path):
         z = np.load(path)
@@ -231,7 +231,9 @@ def load_clip(seed, frames):
         cams = [RegisteredCamera(i, z["R"][i], z["t"][i]) for i in range(frames)]
         return synth.Clip(WIDTH, HEIGHT, float(z["focal"]), cams, list(z["images"]),
                           list(z["depths"]), z["sparse"])
-    clip = synth.full_clip(seed=seed, width=WIDTH, height=HEIGHT, n_frames=frames)
+    # fewer keyframes than the clip's 120 keep its spacing (40 degrees over 119 steps)
+    clip = synth.full_clip(seed=seed, width=WIDTH, height=HEIGHT, n_frames=frames,
+                           arc_deg=40.0 * (frames - 1) / (FRAMES - 1))
     np.savez(path, images=np.stack(clip.images), R=np.stack([c.rotation for c in clip.cameras]),
              t=np.stack([c.translation for c in clip.cameras]), sparse=clip.sparse,
              focal=clip.focal, depths=np.stack(clip.depths).astype(np.float32))

@@ -62,7 +62,8 @@ def attribute(g, g_sweep, o, o_rec, prof, band, rows=None):
     rep = {"band": band, "sites": len(g_sweep), "sampled": 0, "moved": 0, "second_moved": 0,
            "gate_band": 0, "gate_band_over_1e-5": 0, "recip_moved": 0,
            "recip_moved_over_1e-5": 0, "completion_cascade": 0, "completion_band": 0,
-           "points_compared": 0, "points_equal_bits": 0, "max_cost_error": 0.0,
+           "points_compared": 0, "points_equal_bits": 0, "positions_equal_bits": 0,
+           "max_cost_error": 0.0,
            "median_cost_error": 0.0, "max_confidence_delta": 0.0, "unexplained": []}
     unexplained = rep["unexplained"]
     # ---- sweep -------------------------------------------------------------
@@ -131,6 +132,8 @@ def attribute(g, g_sweep, o, o_rec, prof, band, rows=None):
         rep["points_compared"] += 1
         if g.points[i].tobytes() == o.points[j].tobytes():
             rep["points_equal_bits"] += 1
+        if all(g.points[i][c].tobytes() == o.points[j][c].tobytes() for c in "xyz"):
+            rep["positions_equal_bits"] += 1
         rep["max_confidence_delta"] = max(rep["max_confidence_delta"],
                                           abs(float(g.points[i]["confidence"]) -
                                               float(o.points[j]["confidence"])))

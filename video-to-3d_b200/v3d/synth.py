@@ -307,9 +307,9 @@ def plain_small_clip(seed=1, width=360, height=202):
                      landmark_cameras=[2], landmarks_per_camera=600)
 
 
-def full_clip(seed=2, width=640, height=360, n_frames=120, jitter_deg=2.0, **kw):
+def full_clip(seed=2, width=640, height=360, n_frames=120, jitter_deg=2.0, arc_deg=40.0, **kw):
     """120 keyframes on a 40° arc around the scene centre, ±2° jitter."""
-    return make_clip(width, height, n_frames, 40.0, 4.0, seed, noise_sigma=0.01,
+    return make_clip(width, height, n_frames, arc_deg, 4.0, seed, noise_sigma=0.01,
                      jitter_deg=jitter_deg, **kw)
 
 
