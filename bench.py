@@ -145,7 +145,7 @@ def kernel_rooflines(info, units, b, sweep_ms, recip_sweep_ms, recip_prep_ms, hb
     out = {}
     for name, ms, alg, traffic, what in (
             ("k_sweep_tiled", sweep_ms, sweep_bytes, units * SWEEP_DRAM_BYTES_PER_UNIT,
-             "depth sweep, box-filtered ZNCC over 32x8-site tiles (plane-chunk merge included)"),
+             "depth sweep, box-filtered ZNCC over 32x8- or 16x16-site tiles (plane-chunk merge included)"),
             ("k_recip_sweep", recip_sweep_ms, recip_bytes, None,
              "single-view reciprocal sweep, warp per pending pair, all three launches"),
             ("k_recip_prepare", recip_prep_ms, prep_bytes, None,

@@ -5,6 +5,10 @@
 // parallel; pass_kernels.cu dispatches to them.
 #pragma once
 
+#include <map>
+#include <mutex>
+#include <utility>
+
 #include "pass_kernels.cuh"
 #include "typed.cuh"
 
@@ -801,7 +805,8 @@ __device__ __forceinline__ bool window_inside(const float* H, float zmin, float 
 // with the floor, fraction and texels of sample_nonneg:
 //  * ImageSampler reads the image in global memory;
 //  * BandSampler reads a staged box of it in shared memory (a warp's band,
-//    rows of kBandPitch texels starting at image texel (x0, y0)).  The floor is
+//    rows of kBandPitch entries starting at image texel (x0, y0); entry c of a
+//    row holds texels c and c + 1, so a bilinear tap is two 8-byte loads).  The floor is
 //    the same round-down add with the box origin folded into the shift:
 //    u + (2^23 - x0) rounded down is 2^23 - x0 + floor(u) exactly, whose low
 //    mantissa bits are floor(u) - x0, the band column; the fraction u - floor(u)
@@ -822,7 +827,7 @@ struct ImageSampler {
 };
 
 struct BandSampler {
-    const float* band;
+    const float2* band;
     float sx, sy;  // 2^23 - x0, 2^23 - y0
     __device__ __forceinline__ float operator()(float u, float v) const {
         const int sb = __float_as_int(8388608.0f);
@@ -830,8 +835,8 @@ struct BandSampler {
         const float fu = tu - sx, fv = tv - sy;
         const int o = (__float_as_int(tv) - sb) * kBandPitch + (__float_as_int(tu) - sb);
         const float tx = u - fu, ty = v - fv;
-        const float v00 = band[o], v10 = band[o + 1];
-        const float v01 = band[o + kBandPitch], v11 = band[o + kBandPitch + 1];
+        const float2 t0 = band[o], t1 = band[o + kBandPitch];
+        const float v00 = t0.x, v10 = t0.y, v01 = t1.x, v11 = t1.y;
         const float top = fmaf(v10 - v00, tx, v00);
         const float bot = fmaf(v11 - v01, tx, v01);
         return fmaf(bot - top, ty, top);
@@ -844,10 +849,10 @@ struct BandSampler {
         const int oa = (__float_as_int(tv.x) - sb) * kBandPitch + (__float_as_int(tu.x) - sb);
         const int ob = (__float_as_int(tv.y) - sb) * kBandPitch + (__float_as_int(tu.y) - sb);
         const float2 tx = __fadd2_rn(u, neg2(fu)), ty = __fadd2_rn(v, neg2(fv));
-        const float2 v00 = f2(band[oa], band[ob]);
-        const float2 v10 = f2(band[oa + 1], band[ob + 1]);
-        const float2 v01 = f2(band[oa + kBandPitch], band[ob + kBandPitch]);
-        const float2 v11 = f2(band[oa + kBandPitch + 1], band[ob + kBandPitch + 1]);
+        const float2 a0 = band[oa], a1 = band[oa + kBandPitch];
+        const float2 b0 = band[ob], b1 = band[ob + kBandPitch];
+        const float2 v00 = f2(a0.x, b0.x), v10 = f2(a0.y, b0.y);
+        const float2 v01 = f2(a1.x, b1.x), v11 = f2(a1.y, b1.y);
         const float2 top = __ffma2_rn(__fadd2_rn(v10, neg2(v00)), tx, v00);
         const float2 bot = __ffma2_rn(__fadd2_rn(v11, neg2(v01)), tx, v01);
         return __ffma2_rn(__fadd2_rn(bot, neg2(top)), ty, top);
@@ -1167,24 +1172,30 @@ __global__ void __launch_bounds__(256) k_recip_prepare(BatchDev b, const Cand* _
 // blocks per SM.
 constexpr int kRecipBanded = 1, kRecipPerHypothesis = 2;
 
+// The banded kernel runs 4 warps a block (their bands of texel pairs fill the
+// static shared memory), the per-hypothesis one 8.
 template <int MODE>
 struct RecipBounds {
-    static constexpr int kBlocks = MODE == kRecipBanded ? 3 : 2;
+    static constexpr int kWarps = MODE == kRecipBanded ? 4 : 8;
+    static constexpr int kThreads = 32 * kWarps;
+    static constexpr int kBlocks = MODE == kRecipBanded ? 4 : 2;
 };
 
 template <class T, int R, int COST, int MODE>
-__global__ void __launch_bounds__(256, RecipBounds<MODE>::kBlocks) k_recip_sweep(
+__global__ void __launch_bounds__(RecipBounds<MODE>::kThreads, RecipBounds<MODE>::kBlocks) k_recip_sweep(
     BatchDev b, const Cand* __restrict__ cands, const uint32_t* __restrict__ list,
     const uint32_t* __restrict__ list_count, RecipObs* __restrict__ obs,
     uint32_t* __restrict__ fallback, uint32_t* __restrict__ n_fallback) {
     constexpr int W = 2 * R + 1;
     constexpr int N = W * W;
-    __shared__ float pvc_all[8][N];
-    // the warps' bands, with a guard row before the first and after the last
-    __shared__ float band_all[(8 * kBandRows + 2) * kBandPitch];
+    constexpr int kWarps = RecipBounds<MODE>::kWarps;
+    __shared__ float pvc_all[kWarps][N];
+    // the warps' bands of texel pairs (banded kernel only), with a guard row
+    // before the first and after the last
+    __shared__ float2 band_all[MODE == kRecipBanded ? (kWarps * kBandRows + 2) * kBandPitch : 1];
     const uint32_t lane = lane_id(), wid = threadIdx.x >> 5;
     float* pvc = pvc_all[wid];
-    float* band = band_all + (1 + wid * kBandRows) * kBandPitch;
+    float2* band = band_all + (MODE == kRecipBanded ? (1 + wid * kBandRows) * kBandPitch : 0);
     const uint32_t ms = (uint32_t)b.max_src;
     const uint32_t n_list = *list_count;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -1250,9 +1261,12 @@ __global__ void __launch_bounds__(256, RecipBounds<MODE>::kBlocks) k_recip_sweep
             continue;
         }
         if (banded) {
+            // entry c: texels c and c + 1 of the row; the last column is read only
+            // as a right neighbour
             for (int rr = 0; rr < rows; ++rr) {
                 const T* row = rimg + (size_t)(by0 + rr) * rw + bx0;
-                for (int c = lane; c < cols; c += 32) band[rr * kBandPitch + c] = pix<T>(row, c);
+                for (int c = lane; c < cols - 1; c += 32)
+                    band[rr * kBandPitch + c] = f2(pix<T>(row, c), pix<T>(row, c + 1));
             }
         }
         __syncwarp();
@@ -1428,6 +1442,24 @@ __global__ void __launch_bounds__(128) k_propose_costs(BatchDev b,
 }
 
 
+// Raises a kernel's dynamic shared memory limit on the current device to at
+// least `bytes`, never lowering it: the server's slots launch the same kernel
+// from several threads with different sizes, and a limit lowered by one
+// thread between another's setting and launch would refuse that launch.
+inline cudaError_t raise_dynamic_smem_limit(const void* kern, size_t bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<int, const void*>, size_t> limit;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lock(mu);
+    size_t& have = limit[{dev, kern}];
+    if (bytes <= have) return cudaSuccess;
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) have = bytes;
+    return e;
+}
+
 // Multiprocessors of the current device when first asked (a thread-safe
 // static: server slots launch from several threads).
 inline int sm_count() {
@@ -1480,8 +1512,7 @@ cudaError_t Typed<T>::sweep_tiled(const BatchDev& b, uint32_t max_nx, uint32_t m
                             sizeof(float) * (2 * np + (size_t)b.max_src * (kTileThreads + 12) +
                                              2 * (size_t)b.prof.planes) +
                             16 + sizeof(float4) * (size_t)tiled_steps((int)np) * kTileThreads;
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem);
+        cudaError_t e = raise_dynamic_smem_limit(reinterpret_cast<const void*>(kern), smem);
         if (e != cudaSuccess) return e;
         const int n = chunks.n > 1 ? chunks.n : 1;
         dim3 grid((max_nx + TX - 1) / TX, (max_ny + TY - 1) / TY, (unsigned)b.n_refs * (unsigned)n);
@@ -1512,7 +1543,7 @@ cudaError_t Typed<T>::reciprocal(const BatchDev& b, const Cand* cands, const uin
                                  cudaStream_t st) {
     using namespace typed_detail;
     const unsigned blocks = (unsigned)sm_count() * 8;
-    const unsigned rblocks3 = (unsigned)sm_count() * 12;  // the banded sweep, 3 blocks an SM
+    const unsigned rblocks3 = (unsigned)sm_count() * 16;  // the banded sweep: 4 blocks of 4 warps an SM
 #define V3D_CK_RET(x)                                \
     do {                                             \
         const cudaError_t e_ = (x);                  \
@@ -1540,7 +1571,7 @@ cudaError_t Typed<T>::reciprocal(const BatchDev& b, const Cand* cands, const uin
             if (e != cudaSuccess) return e;                                                    \
             mark(q.t_sweep);                                                                   \
             V3D_CK_RET(cudaMemsetAsync(q.n_fallback, 0, sizeof(uint32_t), st));               \
-            V3D_COUNTED k_recip_sweep<T, RR, 1, kRecipBanded><<<rblocks3, 256, 0, st>>>(        \
+            V3D_COUNTED k_recip_sweep<T, RR, 1, kRecipBanded><<<rblocks3, 128, 0, st>>>(        \
                 b, cands, q.items, q.n_items, obs, q.fallback, q.n_fallback);                 \
             V3D_COUNTED k_recip_sweep<T, RR, 1, kRecipPerHypothesis><<<blocks, 256, 0, st>>>(   \
                 b, cands, q.fallback, q.n_fallback, obs, nullptr, nullptr);                    \
@@ -1549,7 +1580,7 @@ cudaError_t Typed<T>::reciprocal(const BatchDev& b, const Cand* cands, const uin
             if (e != cudaSuccess) return e;                                                    \
             mark(q.t_sweep);                                                                   \
             V3D_CK_RET(cudaMemsetAsync(q.n_fallback, 0, sizeof(uint32_t), st));               \
-            V3D_COUNTED k_recip_sweep<T, RR, 0, kRecipBanded><<<rblocks3, 256, 0, st>>>(        \
+            V3D_COUNTED k_recip_sweep<T, RR, 0, kRecipBanded><<<rblocks3, 128, 0, st>>>(        \
                 b, cands, q.items, q.n_items, obs, q.fallback, q.n_fallback);                 \
             V3D_COUNTED k_recip_sweep<T, RR, 0, kRecipPerHypothesis><<<blocks, 256, 0, st>>>(   \
                 b, cands, q.fallback, q.n_fallback, obs, nullptr, nullptr);                    \
