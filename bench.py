@@ -70,7 +70,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true",
                     help="skip the CPU baseline leg (profiling runs)")
     ap.add_argument("--config", choices=["full", "small", "heavy", "batched", "served", "fusion",
-                                         "verify", "artifact", "colmap", "refprofile"],
+                                         "verify", "artifact", "colmap", "refprofile", "merge"],
                     default="full",
                     help="full: the headline line (default); small: 360x202 1+4 views; heavy: "
                          "bf16 16 views 256 planes 9x9; batched: 32 uneven clips through the "
@@ -920,6 +920,115 @@ def run_fusion(args):
     ctx.close()
 
 
+def merge_inputs(clip, patches, ctx):
+    """The consolidated output of `patches` fused on the device, with one
+    reference camera per support group (its patch's reference frame) and every
+    point's origin GeometricMultiView: the merge's inputs (surface_fusion.rs:
+    145-214)."""
+    from v3d import abi, surface
+    pts, tris, mem, groups = surface.consolidation_inputs(patches)
+    fused = np.ascontiguousarray(pts.copy())
+    out = ctx.fuse_mutually_supported_vertices(fused, tris, mem)
+    cams = [None] * groups
+    base = 0
+    for d, _ in patches:
+        n = len(d.points)
+        if n:
+            cams[int(mem[base])] = clip.cameras[int(d.stats["reference_frame"])]
+        base += n
+    origins = np.full(len(fused), abi.ORIGIN_GEOMETRIC, dtype=np.int32)
+    return fused, tris, mem, out.pairs, cams, origins, groups
+
+
+def run_merge(args):
+    """The connected-surface merge (surface_merge.rs:312-1078) on the fused
+    consolidated output of the full clip.  A step is one
+    v3d_merge_fused_patches_owned call with host buffers: the device judges
+    every candidate triangle against its linked owners' footprints, the host
+    runs the ordered stages (decisions, 3D fallback, stitching, clips,
+    conforming split)."""
+    from v3d import dense
+    clip = load_clip(2, args.frames)
+    frames = clip.frames(args.storage)
+    prof = headline_profile(args)
+    ctx = dense.Context(0)
+    res = ctx.reconstruct_reference_patches_meshed(frames, clip.cameras, clip.sparse, clip.focal,
+                                                   list(range(args.frames)), profile=prof)
+    patches = [r for r in res if r is not None]
+    pts, tris, mem, pairs, cams, origins, groups = merge_inputs(clip, patches, ctx)
+    pts, tris, mem, origins = pinned(pts), pinned(tris), pinned(mem), pinned(origins)
+
+    def step():
+        t0 = time.perf_counter()
+        try:
+            out = ctx.merge_fused_patches_owned(pts, tris, mem, pairs, cams, origins)
+        except dense.MergeRejected as e:
+            out = e
+        return time.perf_counter() - t0, out, ctx.last_run_info()
+    for _ in range(args.warmup):
+        step()
+    walls, devs, launches, out = [], [], 0, None
+    clocks = Clocks(0)
+    clocks.start()
+    for _ in range(args.steps):
+        w, out, info = step()
+        walls.append(w)
+        devs.append(info["device_ms"] / 1e3)
+        launches += int(info["kernel_launches"])
+    clk = clocks.stop()
+    nt = len(tris)
+    wall_s, dev_s = float(np.mean(walls)), float(np.mean(devs))
+    outcome = ({"rejected": str(out)} if isinstance(out, Exception) else
+               {k: (float(v) if isinstance(v, float) else int(v)) for k, v in out.stats.items()})
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    alg = nt * 72
+    line = {"metric": "mesh triangles merged/s", "value": nt / wall_s, "unit": "triangles/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": wall_s * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64",
+            "data": "the library's own dense output of the seeded synthetic clip, fused",
+            "config": {"workload": "connected-surface merge of the fused consolidated output of "
+                                   "the full clip (%d reference patches, %d support groups, "
+                                   "%d fusion pairs)" % (len(patches), groups, len(pairs)),
+                       "points": len(pts), "triangles": nt,
+                       "timing": "whole call (device kernels and the ordered host stages)"},
+            "clocks": clk,
+            "e2e": {"value": nt / wall_s, "unit": "triangles/s",
+                    "h2d_bytes_per_step": len(pts) * (20 + 8 + 4) + nt * 32,
+                    "d2h_bytes_per_step": 0, "ms_per_step": wall_s * 1e3},
+            "device_ms_per_step": dev_s * 1e3,
+            "gpu_launches": launches,
+            "outcome": outcome,
+            "roofline": {"bound": "hbm", "kernel": "k_ownership + k_ratios (all launches)",
+                         "achieved": alg / max(dev_s, 1e-9) / 1e9, "peak": hbm, "unit": "GB/s",
+                         "frac": alg / max(dev_s, 1e-9) / 1e9 / hbm, "traffic": None,
+                         "algorithmic_bytes": alg,
+                         "note": "algorithmic bytes = every triangle's 72-byte world corners "
+                                 "read once; the kernels are f64-issue bound (polygon clipping) "
+                                 "and the call is bound by the ordered host stages"}}
+    if not args.no_cpu_baseline:
+        from tests.oracle_ffi import Oracle
+        k = min(12, len(patches))
+        sp, st, sm, sprs, scams, sorg, _ = merge_inputs(clip, patches[:k], ctx)
+        t0 = time.perf_counter()
+        try:
+            Oracle().merge_fused_patches_owned(sp, st, sm, sprs, scams, sorg)
+        except dense.MergeRejected:
+            pass
+        cpu_s = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": len(st) / cpu_s, "unit": "triangles/s", "cores": 1,
+                                "kind": "port",
+                                "sample": "the first %d patches (%d points, %d triangles) fused "
+                                          "on the device, merged by the oracle, one thread"
+                                          % (k, len(sp), len(st))}
+    print(json.dumps(line), flush=True)
+    ctx.close()
+
 def pinned(a):
     """A copy of numpy array `a` in page-locked host memory, as a caller hands
     its inputs over (the end-to-end figures copy from pinned memory)."""
@@ -1213,6 +1322,8 @@ def main():
         run_plain_config(args)
     elif args.config == "fusion":
         run_fusion(args)
+    elif args.config == "merge":
+        run_merge(args)
     elif args.config == "verify":
         run_verify(args)
     elif args.config == "artifact":

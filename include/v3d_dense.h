@@ -22,6 +22,8 @@
  *   v3d_reconstruct_dense_mesh_with_control mesh.rs:74-220
  *   v3d_plan_clips                          dense.rs:165-213, 620-672 (many clips)
  *   v3d_fuse_mutually_supported_vertices    surface_fusion.rs:369-549
+ *   v3d_merge_fused_patches_owned           surface_merge.rs:312-353 (with
+ *                                           surface_merge_clip.rs, surface_merge_stitch.rs)
  *   v3d_verify_depth_grids                  colmap_surface.rs:175-314, 394-420
  *   v3d_mesh_verified_depth_grids           colmap_surface.rs:380-471
  *   v3d_surface_topology_of                 colmap_surface.rs:125-157
@@ -75,7 +77,8 @@ typedef enum v3d_status {
     V3D_ERR_NO_DEVICE = -4,
     V3D_ERR_INTERNAL = -5,
     V3D_ERR_TIMEOUT = -6,            /* v3d_server_wait: the request is not done yet */
-    V3D_ERR_SHUTDOWN = -7            /* the server stopped before running the request */
+    V3D_ERR_SHUTDOWN = -7,           /* the server stopped before running the request */
+    V3D_REJECTED = 2                 /* the reference returns Err(message): v3d_last_error */
 } v3d_status;
 
 /* Skip reasons of dense_legacy.rs:157-236 and dense.rs, in the order the
@@ -749,6 +752,92 @@ int32_t v3d_fuse_mutually_supported_vertices(
     v3d_cancel_fn cancel, void* cancel_user, v3d_fusion_stats* stats,
     v3d_fusion_pair* pairs, uint64_t* n_pairs, uint64_t* moved, uint64_t* n_moved);
 
+/* ---- connected-surface merge (surface_merge.rs, surface_merge_clip.rs,
+ * surface_merge_stitch.rs) ----------------------------------------------------
+ * The second step of surface consolidation, after fusion
+ * (surface_fusion.rs:206-214): fusion-accepted pairs become shared vertices,
+ * lower-priority triangles owned by a linked higher-priority patch in that
+ * patch's reference image are removed (a 3D coverage test where no image can
+ * judge), trimmed seams are stitched over existing vertices, partially owned
+ * overlap triangles are clipped against their owner with derived vertices,
+ * and edges carrying a derived vertex are split. */
+
+/* ReferenceCamera (surface_merge.rs:103-106), one per camera-support group. */
+typedef struct v3d_reference_camera {
+    int32_t present;          /* 0: None */
+    int32_t pad_;
+    double rotation[9];       /* row-major; x_cam = rotation * x + translation */
+    double translation[3];
+} v3d_reference_camera;
+
+/* EvidenceOrigin (reconstruction_evidence.rs:74-79), per point. */
+enum {
+    V3D_ORIGIN_NONE = -1,
+    V3D_ORIGIN_GEOMETRIC_MULTI_VIEW = 0,
+    V3D_ORIGIN_REVALIDATED_COMPLETION = 1,
+    V3D_ORIGIN_LEARNED_MULTI_VIEW = 2,
+    V3D_ORIGIN_GENERATIVE_COMPLETION = 3
+};
+
+/* DerivedVertexSource (reconstruction_evidence.rs:144-153). */
+typedef struct v3d_derived_vertex_source {
+    uint64_t point_index;
+    uint64_t source_triangle;
+    uint64_t source_corners[3];
+    double barycentric[3];
+} v3d_derived_vertex_source;
+
+/* TriangleSourceCorners (reconstruction_evidence.rs:125-130). */
+typedef struct v3d_triangle_source {
+    uint64_t triangle;
+    uint64_t corners[3];
+} v3d_triangle_source;
+
+/* MergeStats (surface_merge.rs:131-202), its scalar fields; the vectors are
+ * in v3d_merge_result. */
+typedef struct v3d_merge_stats {
+    uint64_t fused_pairs, shared_vertices, cross_reference_triangles,
+        removed_duplicate_triangles, remaining_overlap_triangles, provenance_separated_pairs,
+        trimmed_seam_triangles;
+    double trimmed_seam_area_share;
+    uint64_t stitched_seam_triangles, patch_components, meshed_patches, max_postings_per_query,
+        posting_bound_hits, clipping_budget_exhausted, clipped_overlap_triangles, clip_pieces,
+        derived_vertices, unclipped_overlap_triangles, conformed_triangles, conformance_failures;
+} v3d_merge_stats;
+
+/* OwnedMerge (surface_merge.rs:276-283), owned by the library. */
+typedef struct v3d_merge_result {
+    v3d_merge_stats stats;
+    v3d_point* points;                       /* the input points, then the derived ones */
+    uint64_t n_points;
+    v3d_mesh_triangle* triangles;
+    uint64_t n_triangles;
+    v3d_derived_vertex_source* derived_vertices;
+    uint64_t n_derived_vertices;
+    v3d_fusion_pair* uncalibrated_patch_pairs; /* (owner group, candidate group) */
+    uint64_t n_uncalibrated_patch_pairs;
+    uint64_t* retained_by_group;
+    uint64_t n_retained_by_group;
+    v3d_triangle_source* triangle_sources;
+    uint64_t n_triangle_sources;
+} v3d_merge_result;
+
+/* merge_fused_patches_owned_with_control (surface_merge.rs:312-353).
+ * membership [n_points]: camera-support group per point, negative for none;
+ * pairs: fusion's accepted pairs in its order; cameras [n_cameras]: the
+ * reference camera of each group (indexed by group); origins [n_origins]:
+ * each point's evidence origin (a shorter array leaves the rest absent, as a
+ * shorter slice does).  V3D_OK with *out set, or V3D_REJECTED with the
+ * reference's Err message in v3d_last_error ("reconstruction canceled"
+ * when cancel fired, or the conformance rejection) and *out NULL. */
+int32_t v3d_merge_fused_patches_owned(
+    v3d_context* ctx, const v3d_point* points, uint64_t n_points,
+    const v3d_mesh_triangle* triangles, uint64_t n_triangles, const int64_t* membership,
+    const v3d_fusion_pair* pairs, uint64_t n_pairs, const v3d_reference_camera* cameras,
+    uint64_t n_cameras, const int32_t* origins, uint64_t n_origins, v3d_cancel_fn cancel,
+    void* cancel_user, v3d_merge_result** out);
+void v3d_merge_result_free(v3d_merge_result* result);
+
 /* ---- Serving (no counterpart in the reference, which runs one call at a time) ----
  *
  * A device-resident request loop.  Clips (frames, cameras, landmarks) are
@@ -969,20 +1058,6 @@ int32_t v3d_encode_dense_evidence(
  * need no call.  Host only; no device or context. */
 void v3d_pack_dense_points(const v3d_point* points, uint64_t n_points,
                            uint8_t* values_f32_le, uint8_t* rgb);
-
-/* TriangleSourceCorners (reconstruction_evidence.rs:124-130). */
-typedef struct v3d_triangle_source {
-    uint64_t triangle;
-    uint64_t corners[3];
-} v3d_triangle_source;
-
-/* DerivedVertexSource (reconstruction_evidence.rs:142-153). */
-typedef struct v3d_derived_vertex_source {
-    uint64_t point_index;
-    uint64_t source_triangle;
-    uint64_t source_corners[3];
-    double barycentric[3];
-} v3d_derived_vertex_source;
 
 /* The browser transport's packed mesh buffers (pack_mesh_triangles,
  * crates/video-to-3d-wasm/src/lib.rs:269-326): indices_u32_le 12 bytes and

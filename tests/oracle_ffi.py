@@ -51,6 +51,19 @@ class Oracle:
         L.v3do_mesh_result_free.argtypes = [_P(abi.MeshResult)]
         L.v3do_selftest.argtypes = [C.c_char_p, C.c_uint64, _P(C.c_int32)]
         L.v3do_selftest.restype = C.c_int32
+        L.v3do_merge_fused_patches_owned.argtypes = [
+            C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p, C.c_uint64,
+            C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64, abi.CANCEL_FN, C.c_void_p,
+            _P(_P(abi.MergeResult))]
+        L.v3do_merge_fused_patches_owned.restype = C.c_int32
+        L.v3do_merge_result_free.argtypes = [_P(abi.MergeResult)]
+        L.v3do_merge_result_free.restype = None
+        L.v3do_merge_last_error.restype = C.c_char_p
+        L.v3do_merge_selftest.argtypes = [C.c_char_p, C.c_uint64]
+        L.v3do_merge_selftest.restype = C.c_int32
+        L.v3do_merge_diagnostic.argtypes = [_P(abi.MergeResult), C.c_uint64, C.c_char_p,
+                                            C.c_uint64]
+        L.v3do_merge_diagnostic.restype = C.c_uint64
         L.v3do_patch_error.argtypes = [_P(abi.Profile), _P(abi.Camera), _P(abi.Camera),
                                        _P(abi.Frame), _P(abi.Frame), C.c_double, C.c_double,
                                        C.c_double, C.c_double, _P(C.c_double)]
@@ -195,6 +208,23 @@ class Oracle:
         checks = C.c_int32()
         failures = self.lib.v3do_selftest(buf, len(buf), C.byref(checks))
         return failures, checks.value, buf.value.decode()
+
+    def merge_selftest(self):
+        """The reference's surface-merge tests on the oracle: (checks, failure)."""
+        buf = C.create_string_buffer(1 << 12)
+        n = self.lib.v3do_merge_selftest(buf, len(buf))
+        return n, buf.value.decode()
+
+    def merge_fused_patches_owned(self, points, triangles, membership, pairs, cameras,
+                                  origins=None, control=None):
+        """surface_merge.rs:312-353 on the CPU: a MergeOutcome (MergeRejected on Err)."""
+        from v3d import dense
+        st, out = dense._merge(self.lib.v3do_merge_fused_patches_owned, (),
+                               self.lib.v3do_merge_result_free,
+                               lambda: self.lib.v3do_merge_last_error().decode(), points,
+                               triangles, membership, pairs, cameras, origins, control)
+        assert st == 0, st
+        return out
 
     def max_threads(self):
         return self.lib.v3do_max_threads()

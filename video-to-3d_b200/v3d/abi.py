@@ -297,9 +297,54 @@ class DenseBudget(C.Structure):
                 ("fine_grid", C.c_int32), ("pad0", C.c_int32), ("reference_views", C.c_uint64)]
 
 
+
+class ReferenceCamera(C.Structure):
+    _fields_ = [("present", C.c_int32), ("pad_", C.c_int32), ("rotation", C.c_double * 9),
+                ("translation", C.c_double * 3)]
+
+
+class DerivedVertexSource(C.Structure):
+    _fields_ = [("point_index", C.c_uint64), ("source_triangle", C.c_uint64),
+                ("source_corners", C.c_uint64 * 3), ("barycentric", C.c_double * 3)]
+
+
+class TriangleSource(C.Structure):
+    _fields_ = [("triangle", C.c_uint64), ("corners", C.c_uint64 * 3)]
+
+
+MERGE_STAT_FIELDS = (
+    "fused_pairs", "shared_vertices", "cross_reference_triangles",
+    "removed_duplicate_triangles", "remaining_overlap_triangles", "provenance_separated_pairs",
+    "trimmed_seam_triangles", "trimmed_seam_area_share", "stitched_seam_triangles",
+    "patch_components", "meshed_patches", "max_postings_per_query", "posting_bound_hits",
+    "clipping_budget_exhausted", "clipped_overlap_triangles", "clip_pieces", "derived_vertices",
+    "unclipped_overlap_triangles", "conformed_triangles", "conformance_failures")
+
+
+class MergeStats(C.Structure):
+    _fields_ = [(f, C.c_double if f == "trimmed_seam_area_share" else C.c_uint64)
+                for f in MERGE_STAT_FIELDS]
+
+
+class MergeResult(C.Structure):
+    _fields_ = [("stats", MergeStats),
+                ("points", C.c_void_p), ("n_points", C.c_uint64),
+                ("triangles", C.c_void_p), ("n_triangles", C.c_uint64),
+                ("derived_vertices", C.c_void_p), ("n_derived_vertices", C.c_uint64),
+                ("uncalibrated_patch_pairs", C.c_void_p), ("n_uncalibrated_patch_pairs", C.c_uint64),
+                ("retained_by_group", C.c_void_p), ("n_retained_by_group", C.c_uint64),
+                ("triangle_sources", C.c_void_p), ("n_triangle_sources", C.c_uint64)]
+
+
+REJECTED = 2
+ORIGIN_NONE, ORIGIN_GEOMETRIC, ORIGIN_REVALIDATED, ORIGIN_LEARNED, ORIGIN_GENERATIVE = -1, 0, 1, 2, 3
+
 SKIP_WORKING_SET_BUDGET = 10
 
 STRUCTS = {
+    "v3d_reference_camera": ReferenceCamera, "v3d_derived_vertex_source": DerivedVertexSource,
+    "v3d_triangle_source": TriangleSource, "v3d_merge_stats": MergeStats,
+    "v3d_merge_result": MergeResult,
     "v3d_working_set_estimate": WorkingSetEstimate, "v3d_dense_budget": DenseBudget,
     "v3d_dense_document": DenseDocument,
     "v3d_meshing_funnel": MeshingFunnel, "v3d_verified_surface_region": VerifiedSurfaceRegion,

@@ -114,6 +114,13 @@ def library():
         C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64, C.c_void_p, abi.CANCEL_FN,
         C.c_void_p, _P(abi.FusionStats), C.c_void_p, _P(C.c_uint64), C.c_void_p, _P(C.c_uint64)]
     L.v3d_fuse_mutually_supported_vertices.restype = C.c_int32
+    L.v3d_merge_fused_patches_owned.argtypes = [
+        C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p,
+        C.c_uint64, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64, abi.CANCEL_FN, C.c_void_p,
+        _P(_P(abi.MergeResult))]
+    L.v3d_merge_fused_patches_owned.restype = C.c_int32
+    L.v3d_merge_result_free.argtypes = [_P(abi.MergeResult)]
+    L.v3d_merge_result_free.restype = None
     L.v3d_verify_depth_grids.argtypes = [
         C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint32,
         C.c_uint32, C.c_double, C.c_void_p, C.c_uint64, C.c_void_p, _P(abi.VerificationFunnel)]
@@ -420,6 +427,18 @@ class Context:
             self._check(st)
         return surf
 
+    def merge_fused_patches_owned(self, points, triangles, membership, pairs, cameras,
+                                  origins=None, control=None):
+        """merge_fused_patches_owned_with_control (surface_merge.rs:312-353) on
+        the device: a MergeOutcome, or MergeRejected with the reference's
+        message."""
+        st, out = _merge(self.lib.v3d_merge_fused_patches_owned, (self.handle,),
+                         self.lib.v3d_merge_result_free,
+                         lambda: self.lib.v3d_last_error(self.handle).decode(), points, triangles,
+                         membership, pairs, cameras, origins, control)
+        self._check(st)
+        return out
+
     def fuse_mutually_supported_vertices(self, points, triangles, membership, control=None):
         """fuse_mutually_supported_vertices_with_control (surface_fusion.rs:369-549)
         on the device: moves `points` in place and returns a FusionOutcome."""
@@ -470,6 +489,79 @@ def _fuse(lib_fn, head, points, triangles, membership, control):
                 None, C.byref(stats), pairs.ctypes.data, C.byref(n_pairs), moved.ctypes.data,
                 C.byref(n_moved))
     return st, fusion_outcome(stats, pairs, n_pairs.value, moved, n_moved.value)
+
+
+DERIVED_DTYPE = np.dtype([("point_index", "<u8"), ("source_triangle", "<u8"),
+                          ("source_corners", "<u8", (3,)), ("barycentric", "<f8", (3,))])
+SOURCE_DTYPE = np.dtype([("triangle", "<u8"), ("corners", "<u8", (3,))])
+
+
+class MergeOutcome:
+    """OwnedMerge (surface_merge.rs:276-283): points (POINT_DTYPE, the input
+    points then the derived ones), triangles (TRIANGLE_DTYPE), derived_vertices
+    (DERIVED_DTYPE), and MergeStats as `stats` (a dict of the scalar fields)
+    with uncalibrated_patch_pairs (n x 2), retained_by_group and
+    triangle_sources (SOURCE_DTYPE)."""
+
+    def __init__(self, r):
+        def arr(ptr, n, dtype):
+            if n == 0:
+                return np.empty(0, dtype=dtype)
+            buf = (C.c_char * (n * dtype.itemsize)).from_address(ptr)
+            return np.frombuffer(buf, dtype=dtype, count=n).copy()
+        self.stats = {f: getattr(r.stats, f) for f in abi.MERGE_STAT_FIELDS}
+        self.points = arr(r.points, r.n_points, types.POINT_DTYPE)
+        self.triangles = arr(r.triangles, r.n_triangles, types.TRIANGLE_DTYPE)
+        self.derived_vertices = arr(r.derived_vertices, r.n_derived_vertices, DERIVED_DTYPE)
+        self.uncalibrated_patch_pairs = arr(r.uncalibrated_patch_pairs,
+                                            2 * r.n_uncalibrated_patch_pairs,
+                                            np.dtype("<u8")).reshape(-1, 2)
+        self.retained_by_group = arr(r.retained_by_group, r.n_retained_by_group, np.dtype("<u8"))
+        self.triangle_sources = arr(r.triangle_sources, r.n_triangle_sources, SOURCE_DTYPE)
+
+
+class MergeRejected(Exception):
+    """The reference's Err(message) of merge_fused_patches_owned_with_control."""
+
+
+def merge_arguments(points, triangles, membership, pairs, cameras, origins):
+    """Contiguous arrays for v3d_merge_fused_patches_owned.  cameras: one entry
+    per support group, None or an object with `rotation` (3x3) and
+    `translation` (3); origins: None (an empty slice) or one origin per point
+    (abi.ORIGIN_*, abi.ORIGIN_NONE for none)."""
+    pts = np.ascontiguousarray(points, dtype=types.POINT_DTYPE)
+    tris = np.ascontiguousarray(triangles, dtype=types.TRIANGLE_DTYPE)
+    mem = np.ascontiguousarray(membership, dtype=np.int64)
+    if len(mem) != len(pts):
+        raise ValueError("membership needs one entry per point")
+    prs = np.ascontiguousarray(np.asarray(pairs, dtype=np.uint64).reshape(-1, 2))
+    cams = (abi.ReferenceCamera * max(len(cameras), 1))()
+    for i, cam in enumerate(cameras):
+        if cam is not None:
+            R = np.asarray(cam.rotation, dtype=np.float64).reshape(9)
+            t = np.asarray(cam.translation, dtype=np.float64).reshape(3)
+            cams[i] = abi.ReferenceCamera(1, 0, (C.c_double * 9)(*R), (C.c_double * 3)(*t))
+    org = np.ascontiguousarray(np.zeros(0) if origins is None else origins, dtype=np.int32)
+    return pts, tris, mem, prs, cams, len(cameras), org
+
+
+def _merge(lib_fn, head, free_fn, error_fn, points, triangles, membership, pairs, cameras,
+           origins, control):
+    pts, tris, mem, prs, cams, n_cams, org = merge_arguments(points, triangles, membership,
+                                                             pairs, cameras, origins)
+    fn, _keep = types.cancel_callback(control)
+    out = C.POINTER(abi.MergeResult)()
+    st = lib_fn(*head, pts.ctypes.data, len(pts), tris.ctypes.data, len(tris), mem.ctypes.data,
+                prs.ctypes.data, len(prs), cams, n_cams, org.ctypes.data, len(org), fn, None,
+                C.byref(out))
+    if st == abi.REJECTED:
+        raise MergeRejected(error_fn())
+    if st != 0:
+        return st, None
+    try:
+        return st, MergeOutcome(out.contents)
+    finally:
+        free_fn(out)
 
 
 VERIFIED_DTYPE = np.dtype([("x", "<f4"), ("y", "<f4"), ("z", "<f4"), ("confidence", "<f4"),
