@@ -970,11 +970,13 @@ def run_merge(args):
     walls, devs, launches, out = [], [], 0, None
     clocks = Clocks(0)
     clocks.start()
+    stage_ms = np.zeros(12)
     for _ in range(args.steps):
         w, out, info = step()
         walls.append(w)
         devs.append(info["device_ms"] / 1e3)
         launches += int(info["kernel_launches"])
+        stage_ms += np.asarray(info["merge_stage_ms"]) / args.steps
     clk = clocks.stop()
     nt = len(tris)
     wall_s, dev_s = float(np.mean(walls)), float(np.mean(devs))
@@ -1002,6 +1004,10 @@ def run_merge(args):
                     "h2d_bytes_per_step": len(pts) * (20 + 8 + 4) + nt * 32,
                     "d2h_bytes_per_step": 0, "ms_per_step": wall_s * 1e3},
             "device_ms_per_step": dev_s * 1e3,
+            "stages_ms": dict(zip(("setup", "device_lookups", "decisions", "footprints",
+                                   "stitch", "clips", "conform", "assembly", "scale_samples",
+                                   "stitch_edges", "stitch_seams", "stitch_greedy"),
+                                  [round(float(v), 2) for v in stage_ms])),
             "gpu_launches": launches,
             "outcome": outcome,
             "roofline": {"bound": "hbm", "kernel": "k_ownership + k_ratios (all launches)",

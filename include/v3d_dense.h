@@ -567,6 +567,16 @@ typedef struct v3d_run_info {
     double recip_prepare_ms;  /* the reciprocal prologue and its pair list, all launches */
     uint64_t sweep_tile_x;    /* tile width of the box-filtered sweep: 32 (32x8 sites) or 16
                                * (16x16); 0 when the sweep ran a warp per site */
+    /* the last v3d_merge_fused_patches_owned call, wall milliseconds by stage:
+     * [0] components, pairs, re-index, geometry and the device upload;
+     * [1] the device lookups (job lists, launches, transfers);
+     * [2] the per-candidate decisions and the 3D fallback;
+     * [3] footprints (projection, grid, upload) and the kept-triangle grid;
+     * [4] seam stitching; [5] overlap clips; [6] the edge-conforming split;
+     * [7] assembly and topology; within them: [8] the depth-scale samples
+     * (of [1]), [9] stitching's retained edges, [10] its seams, [11] its
+     * greedy pass (of [4]) */
+    double merge_stage_ms[12];
 } v3d_run_info;
 
 int32_t v3d_last_run_info(const v3d_context* ctx, v3d_run_info* out);

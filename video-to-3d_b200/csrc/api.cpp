@@ -252,6 +252,7 @@ int32_t v3d_last_run_info(const v3d_context* ctx, v3d_run_info* out) {
     out->result_bytes = ctx->last_result_bytes;
     out->sweep_chunks = ctx->last_chunks;
     out->sweep_tile_x = ctx->last_tile_x;
+    for (int i = 0; i < 12; ++i) out->merge_stage_ms[i] = ctx->last_merge_stage_ms[i];
     out->recip_sweep_ms = ctx->last_recip_sweep_ms;
     out->recip_prepare_ms = ctx->last_recip_prepare_ms;
     return V3D_OK;

@@ -254,6 +254,7 @@ struct v3d_context {
     uint64_t last_result_bytes = 0;
     uint64_t last_chunks = 1;
     uint64_t last_tile_x = 32;
+    double last_merge_stage_ms[12] = {};
 };
 
 namespace v3d {

@@ -24,6 +24,7 @@
 // bit for bit: the same triangles, points, lineage and statistics.
 #include <algorithm>
 #include <array>
+#include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <functional>
@@ -32,7 +33,10 @@
 #include <optional>
 #include <set>
 #include <string>
+#include <atomic>
+#include <thread>
 #include <unordered_map>
+#include <unordered_set>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -83,6 +87,8 @@ struct DevFootprint {
     uint32_t item_off;     // into the item array: bucketed items, then unindexed ones
     uint32_t n_bucketed;
     uint32_t n_unindexed;
+    uint32_t omit_off;     // into the omitted-component array
+    uint32_t n_omit;
 };
 
 struct DevStore {
@@ -94,6 +100,30 @@ struct DevStore {
     const mg::GridBucket* buckets;
     const uint32_t* items;
     const int32_t* cluster;         // per component (vertex index): linked cluster or -1
+    const uint32_t* omitted;        // components of each footprint's unprojectable kept triangles
+};
+
+// A patch's candidates and its linked owners (one lookup per pair).
+struct Cand {
+    uint32_t triangle, own_comp;
+};
+struct OwnerRef {
+    uint32_t slot;
+    uint32_t pad_;
+    double scale;
+};
+struct PairOut {
+    double share, surface;
+    uint32_t used;
+    uint32_t status;
+};
+// A candidate's fold over its owners (surface_merge.rs:654-706).
+struct CandOut {
+    double share, surface, scale;  // the best-owning judged owner (share 0: none)
+    uint32_t slot;                 // its footprint, or 0xffffffff
+    uint32_t max_used;             // most postings of the lookups the fold recorded
+    uint32_t bound_hits;           // lookups of those cut off at the posting bound
+    uint32_t flags;                // 1: cut off (kept unjudged); 2: judged by every owner
 };
 
 // One lookup: a candidate triangle against one owner footprint.
@@ -226,15 +256,18 @@ __device__ bool project_candidate(const DevFootprint& f, const double* w, PT& c)
 }
 
 // Footprint::ownership_tallied (surface_merge.rs:1520-1578) for one
-// (candidate, owner) job: thread per job.
-__global__ void __launch_bounds__(128) k_ownership(DevStore s, const Job* jobs, uint32_t n_jobs,
-                                                    JobOut* out) {
-    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= n_jobs) return;
-    const Job job = jobs[j];
-    const DevFootprint f = s.fps[job.footprint];
-    JobOut o{0.0, 0.0, 0u, 0u, kJudged};
-    const double* w = s.corners + (size_t)job.triangle * 9;
+// (candidate, owner) pair: thread per pair, pair j = candidate j / n_owners,
+// owner j % n_owners.
+__global__ void __launch_bounds__(128) k_ownership(DevStore s, const Cand* cands, uint32_t n_cand,
+                                                    const OwnerRef* owners, uint32_t n_owners,
+                                                    PairOut* out) {
+    const uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= (uint64_t)n_cand * n_owners) return;
+    const Cand cd = cands[j / n_owners];
+    const OwnerRef ow = owners[j % n_owners];
+    const DevFootprint f = s.fps[ow.slot];
+    PairOut o{0.0, 0.0, 0u, kJudged};
+    const double* w = s.corners + (size_t)cd.triangle * 9;
     PT cand;
     if (!project_candidate(f, w, cand)) {
         o.status = kUnprojectable;
@@ -257,7 +290,7 @@ __global__ void __launch_bounds__(128) k_ownership(DevStore s, const Job* jobs, 
     double image = 0.0, surface = 0.0;
     for (uint32_t k = 0; k < n; ++k) {
         const uint32_t idx = found[k];
-        if (!linked(s, job.own_comp, s.fp_comp[f.tri_off + idx])) continue;
+        if (!linked(s, cd.own_comp, s.fp_comp[f.tri_off + idx])) continue;
         const PT kept = load_pt(s.fp_tri + (size_t)(f.tri_off + idx) * 9);
         Poly<8> poly;
         if (!mg::clip_to_triangle(cand, kept, poly)) continue;
@@ -269,8 +302,8 @@ __global__ void __launch_bounds__(128) k_ownership(DevStore s, const Job* jobs, 
                 agrees = false;
                 break;
             }
-            const double cd = mg::dvd(1.0, ic), kd = mg::dvd(job.scale, ik);
-            agrees = fabs(mg::sub(cd, kd)) <= mg::mul(kMaxRelativeDepthDisagreement, kd);
+            const double cdd = mg::dvd(1.0, ic), kd = mg::dvd(ow.scale, ik);
+            agrees = fabs(mg::sub(cdd, kd)) <= mg::mul(kMaxRelativeDepthDisagreement, kd);
         }
         if (agrees) {
             image = mg::add(image, mg::poly_area(poly));
@@ -280,6 +313,46 @@ __global__ void __launch_bounds__(128) k_ownership(DevStore s, const Job* jobs, 
     o.share = fmin(mg::dvd(image, total), 1.0);
     o.surface = surface;
     out[j] = o;
+}
+
+// The fold over a candidate's owners in owner order (surface_merge.rs:654-706):
+// the lookups it records (up to and including a cut-off one), the best share
+// by strict improvement, and whether every owner judged it (a judged owner
+// below the removal share leaves it unjudged when a kept triangle it could not
+// project belongs to a linked component).
+__global__ void __launch_bounds__(128) k_fold(DevStore s, const Cand* cands, uint32_t n_cand,
+                                               const OwnerRef* owners, uint32_t n_owners,
+                                               const PairOut* pairs, CandOut* out) {
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n_cand) return;
+    const Cand cd = cands[c];
+    CandOut o{0.0, 0.0, 1.0, 0xffffffffu, 0u, 0u, 0u};
+    uint32_t judged = 0;
+    for (uint32_t k = 0; k < n_owners; ++k) {
+        const PairOut p = pairs[(size_t)c * n_owners + k];
+        if (p.status == kUnprojectable) continue;
+        o.max_used = max(o.max_used, p.used);
+        if (p.status == kPostingBound) {
+            o.bound_hits += 1;
+            o.flags |= 1u;
+            break;
+        }
+        if (p.status == kTooManyCells) continue;
+        const DevFootprint f = s.fps[owners[k].slot];
+        bool unjudged = false;
+        if (p.share < kMinImageOwnershipShare)
+            for (uint32_t q = 0; q < f.n_omit && !unjudged; ++q)
+                unjudged = linked(s, cd.own_comp, s.omitted[f.omit_off + q]);
+        if (!unjudged) judged += 1;
+        if (p.share > o.share) {
+            o.share = p.share;
+            o.surface = p.surface;
+            o.scale = owners[k].scale;
+            o.slot = owners[k].slot;
+        }
+    }
+    if (judged == n_owners) o.flags |= 2u;
+    out[c] = o;
 }
 
 // Footprint::depth_ratios_tallied (surface_merge.rs:1475-1510): the anchored
@@ -345,6 +418,11 @@ __global__ void __launch_bounds__(128) k_ratios(DevStore s, const Job* jobs, uin
 namespace v3d {
 namespace merge {
 namespace {
+
+using Clock = std::chrono::steady_clock;
+double ms_since(Clock::time_point t0) {
+    return std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
+}
 
 bool total_less(double a, double b) {
     int64_t l, r;
@@ -819,7 +897,7 @@ struct ClipState {
     uint64_t base;
     std::vector<Derived> derived;
     std::unordered_map<std::pair<EdgeKey, EdgeKey>, uint64_t, CrossHash> crossings;
-    std::map<EdgeKey, std::vector<std::pair<double, uint64_t>>> carriers;
+    std::unordered_map<EdgeKey, std::vector<std::pair<double, uint64_t>>, PairHash> carriers;
     std::unordered_map<uint64_t, std::vector<EdgeKey>> vertex_carriers;
     void record(EdgeKey edge, double parameter, uint64_t vertex) {
         if (edge.first == vertex || edge.second == vertex) return;
@@ -930,9 +1008,35 @@ bool strictly_inside(const V2 tri[3], V2 p, double tolerance) {
     return true;
 }
 
-// clip_overlap (surface_merge_clip.rs:294-759); false: kept whole
-bool clip_overlap(const Inputs& in, ClipState& state, const ClipJob& job, Tally& tally,
-                  std::vector<std::array<uint64_t, 3>>& out) {
+struct ClipNode {
+    V2 pos;
+    bool vertex;
+    uint64_t id;
+    EdgeKey subject, owner;  // crossing: the ids as on each segment (not sorted)
+    double owner_t;
+    uint32_t owner_triangle;
+};
+struct ClipSeg {
+    size_t nodes[2];
+    uint64_t ids[2];
+    double depths[2];
+    std::vector<std::pair<double, size_t>> inside;
+};
+// The geometric half of one clip: its arrangement, faces and kept pieces,
+// which read the inputs only, so clips are planned concurrently.
+struct ClipPlan {
+    uint32_t footprint;
+    bool flipped;
+    std::vector<ClipNode> nodes;
+    std::vector<ClipSeg> segs;
+    std::vector<std::array<size_t, 3>> kept;
+    std::unordered_map<uint64_t, double> owner_depth;
+};
+
+// clip_overlap (surface_merge_clip.rs:294-694) up to the area balance; false:
+// kept whole
+bool plan_clip(const Inputs& in, const ClipJob& job, Tally& tally, ClipPlan& plan) {
+    plan.footprint = job.footprint;
     const Footprint& f = (*in.footprints)[job.footprint];
     const v3d_mesh_triangle tri = (*in.triangles)[job.triangle];
     if (!(*in.has_geometry)[job.triangle]) return false;
@@ -989,21 +1093,15 @@ bool clip_overlap(const Inputs& in, ClipState& state, const ClipJob& job, Tally&
     const double tolerance = extent * kRelativeTolerance;
     const double subject_area = std::fabs(signed_) * 0.5;
 
-    struct Node {
-        V2 pos;
-        bool vertex;
-        uint64_t id;
-        EdgeKey subject, owner;  // crossing: the ids as on each segment (not sorted)
-        double owner_t;
-        uint32_t owner_triangle;
-    };
-    std::vector<Node> nodes;
+    auto& nodes = plan.nodes;
+    nodes.clear();
     std::unordered_map<uint64_t, size_t> by_id;
     for (int i = 0; i < 3; ++i) {
         by_id[sid[i]] = nodes.size();
-        nodes.push_back(Node{spos[i], true, sid[i], {}, {}, 0.0, 0});
+        nodes.push_back(ClipNode{spos[i], true, sid[i], {}, {}, 0.0, 0});
     }
-    std::unordered_map<uint64_t, double> owner_depth;
+    auto& owner_depth = plan.owner_depth;
+    owner_depth.clear();
     for (const auto& o : owned)
         for (int k = 0; k < 3; ++k) {
             const uint64_t id = f.vert[o.first][k];
@@ -1017,21 +1115,16 @@ bool clip_overlap(const Inputs& in, ClipState& state, const ClipJob& job, Tally&
                     break;
                 }
             if (node == SIZE_MAX) {
-                nodes.push_back(Node{pos, true, id, {}, {}, 0.0, 0});
+                nodes.push_back(ClipNode{pos, true, id, {}, {}, 0.0, 0});
                 node = nodes.size() - 1;
             }
             by_id[id] = node;
         }
-    struct Seg {
-        size_t nodes[2];
-        uint64_t ids[2];
-        double depths[2];
-        std::vector<std::pair<double, size_t>> inside;
-    };
-    std::vector<Seg> segs;
+    auto& segs = plan.segs;
+    segs.clear();
     for (int e = 0; e < 3; ++e) {
         const int n = (e + 1) % 3;
-        segs.push_back(Seg{{(size_t)e, (size_t)n}, {sid[e], sid[n]}, {sdepth[e], sdepth[n]}, {}});
+        segs.push_back(ClipSeg{{(size_t)e, (size_t)n}, {sid[e], sid[n]}, {sdepth[e], sdepth[n]}, {}});
     }
     struct OE {
         uint64_t a, b;
@@ -1048,14 +1141,14 @@ bool clip_overlap(const Inputs& in, ClipState& state, const ClipJob& job, Tally&
     for (const auto& kv : owner_edges) {
         const size_t na = by_id.at(kv.second.a), nb = by_id.at(kv.second.b);
         if (na == nb) continue;
-        segs.push_back(Seg{{na, nb}, {kv.second.a, kv.second.b},
+        segs.push_back(ClipSeg{{na, nb}, {kv.second.a, kv.second.b},
                            {owner_depth.at(kv.second.a), owner_depth.at(kv.second.b)}, {}});
         owner_triangle_of.push_back(kv.second.index);
     }
     std::set<size_t> owner_nodes;
     for (const auto& kv : by_id)
         if (kv.second > 2) owner_nodes.insert(kv.second);
-    auto on_segment = [&](Seg& sg, size_t node) {
+    auto on_segment = [&](ClipSeg& sg, size_t node) {
         const V2 a = nodes[sg.nodes[0]].pos, b = nodes[sg.nodes[1]].pos;
         const double length = mg::norm2(b - a);
         const V2 p = nodes[node].pos;
@@ -1084,7 +1177,7 @@ bool clip_overlap(const Inputs& in, ClipState& state, const ClipJob& job, Tally&
             const double st = dp / (dp - dq), ot = da / (da - db);
             if (nodes.size() >= kMaxClipNodes) return false;
             const size_t node = nodes.size();
-            nodes.push_back(Node{pp + (qp - pp) * st, false, 0, {segs[e].ids[0], segs[e].ids[1]},
+            nodes.push_back(ClipNode{pp + (qp - pp) * st, false, 0, {segs[e].ids[0], segs[e].ids[1]},
                                  {segs[sg].ids[0], segs[sg].ids[1]}, ot,
                                  owner_triangle_of[sg - owner_first]});
             segs[e].inside.push_back({st, node});
@@ -1094,7 +1187,7 @@ bool clip_overlap(const Inputs& in, ClipState& state, const ClipJob& job, Tally&
 
     std::set<std::pair<size_t, size_t>> edges;
     for (size_t index = 0; index < segs.size(); ++index) {
-        Seg& sg = segs[index];
+        ClipSeg& sg = segs[index];
         std::stable_sort(sg.inside.begin(), sg.inside.end(),
                          [](const auto& x, const auto& y) { return total_less(x.first, y.first); });
         std::vector<size_t> chain{sg.nodes[0]};
@@ -1182,7 +1275,8 @@ bool clip_overlap(const Inputs& in, ClipState& state, const ClipJob& job, Tally&
         }
     }
     if (outer != 1) return false;
-    std::vector<std::array<size_t, 3>> kept;
+    auto& kept = plan.kept;
+    kept.clear();
     double kept_area = 0.0, removed_area = 0.0;
     std::vector<std::array<uint32_t, 3>> ears;
     for (const auto& face : faces) {
@@ -1219,7 +1313,21 @@ bool clip_overlap(const Inputs& in, ClipState& state, const ClipJob& job, Tally&
     if (std::fabs((kept_area + removed_area) - subject_area) > balance ||
         std::fabs(removed_area - owned_area) > balance)
         return false;
+    plan.flipped = flipped;
+    return true;
+}
 
+// clip_overlap (surface_merge_clip.rs:696-759): the planned clip's vertex ids,
+// its derived vertices and edge records committed to `state`; false (state
+// unchanged) when a new crossing would join corners of different origins
+bool commit_clip(const Inputs& in, ClipState& state, const ClipPlan& plan,
+                 std::vector<std::array<uint64_t, 3>>& out) {
+    const Footprint& f = (*in.footprints)[plan.footprint];
+    const auto& nodes = plan.nodes;
+    const auto& segs = plan.segs;
+    const auto& kept = plan.kept;
+    const auto& owner_depth = plan.owner_depth;
+    const bool flipped = plan.flipped;
     std::set<size_t> used_nodes;
     for (const auto& k : kept) used_nodes.insert(k.begin(), k.end());
     std::unordered_map<size_t, uint64_t> ids;
@@ -1231,7 +1339,7 @@ bool clip_overlap(const Inputs& in, ClipState& state, const ClipJob& job, Tally&
     std::vector<Fresh> fresh;
     uint64_t next_index = state.base + state.derived.size();
     for (size_t node : used_nodes) {
-        const Node& nd = nodes[node];
+        const ClipNode& nd = nodes[node];
         uint64_t id;
         if (nd.vertex) {
             id = nd.id;
@@ -1277,7 +1385,7 @@ bool clip_overlap(const Inputs& in, ClipState& state, const ClipJob& job, Tally&
         state.crossings[fr.crossing] = fr.id;
         state.derived.push_back(fr.point);
     }
-    for (const Seg& sg : segs) {
+    for (const ClipSeg& sg : segs) {
         const EdgeKey edge = ekey(sg.ids[0], sg.ids[1]);
         const bool forward = edge.first == sg.ids[0];
         for (const auto& e : sg.inside) {
@@ -1303,10 +1411,16 @@ namespace v3d {
 namespace merge {
 namespace {
 
-// conform_edges (surface_merge_clip.rs:775-879); false when canceled
+// conform_edges (surface_merge_clip.rs:775-879); false when canceled.  Every
+// triangle's split reads the edge records only, so slots are split
+// concurrently and the extra pieces appended in slot order afterwards.
 template <class Pos, class Cancel>
 bool conform_edges(const ClipState& state, std::vector<v3d_mesh_triangle>& tris, Pos position,
                    Cancel canceled, std::vector<uint64_t>& split, uint64_t& failures) {
+    const size_t n = tris.size();
+    // the reference polls once every 256 slots; none of them may cancel
+    for (size_t slot = 0; slot < n; slot += 256)
+        if (canceled()) return false;
     auto parameter_on = [&](const EdgeKey& edge, uint64_t v, double& t) -> bool {
         if (v == edge.first) {
             t = 0.0;
@@ -1325,83 +1439,110 @@ bool conform_edges(const ClipState& state, std::vector<v3d_mesh_triangle>& tris,
             }
         return false;
     };
+    // vertices an edge record can involve: carrier edge endpoints and recorded vertices
+    std::unordered_set<uint64_t> touched;
+    for (const auto& kv : state.carriers) {
+        touched.insert(kv.first.first);
+        touched.insert(kv.first.second);
+    }
+    for (const auto& kv : state.vertex_carriers) touched.insert(kv.first);
+    const V2 frame[3] = {V2{0.0, 0.0}, V2{1.0, 0.0}, V2{0.0, 1.0}};
+    struct Part {
+        std::vector<std::pair<uint64_t, std::vector<v3d_mesh_triangle>>> pieces;  // (slot, pieces)
+        uint64_t failures = 0;
+    };
+    const size_t n_threads = std::max<size_t>(1, std::min<size_t>(std::thread::hardware_concurrency(), 16));
+    const size_t chunk = (n + n_threads - 1) / n_threads;
+    std::vector<Part> parts(n_threads);
+    auto work = [&](size_t k) {
+        Part& part = parts[k];
+        std::vector<std::pair<uint64_t, V2>> boundary;
+        std::vector<EdgeKey> carriers;
+        std::vector<std::pair<double, uint64_t>> between;
+        std::vector<std::array<uint32_t, 3>> ears;
+        const size_t lo = k * chunk, hi = std::min(n, lo + chunk);
+        for (size_t slot = lo; slot < hi; ++slot) {
+            const v3d_mesh_triangle t = tris[slot];
+            const uint64_t corners[3] = {t.a, t.b, t.c};
+            // no record can apply to an edge none of whose endpoints is touched
+            if (!touched.count(t.a) && !touched.count(t.b) && !touched.count(t.c)) continue;
+            boundary.clear();
+            bool inserted = false;
+            for (int e = 0; e < 3; ++e) {
+                const uint64_t u = corners[e], v = corners[(e + 1) % 3];
+                boundary.push_back({u, frame[e]});
+                carriers.assign(1, ekey(u, v));
+                for (uint64_t endpoint : {u, v}) {
+                    auto it = state.vertex_carriers.find(endpoint);
+                    if (it != state.vertex_carriers.end())
+                        carriers.insert(carriers.end(), it->second.begin(), it->second.end());
+                }
+                const EdgeKey* carrier = nullptr;
+                double tu = 0.0, tv = 0.0;
+                for (const auto& c : carriers)
+                    if (state.carriers.count(c) && parameter_on(c, u, tu) && parameter_on(c, v, tv)) {
+                        carrier = &c;
+                        break;
+                    }
+                if (!carrier) continue;
+                if (std::fabs(tv - tu) <= mg::kF64Eps) continue;
+                between.clear();
+                for (const auto& en : state.carriers.at(*carrier)) {
+                    if (en.second == u || en.second == v) continue;
+                    const double rel = (en.first - tu) / (tv - tu);
+                    if (rel > 1.0e-9 && rel < 1.0 - 1.0e-9) between.push_back({rel, en.second});
+                }
+                std::stable_sort(between.begin(), between.end(),
+                                 [](const auto& x, const auto& y) { return total_less(x.first, y.first); });
+                between.erase(std::unique(between.begin(), between.end(),
+                                          [](const auto& x, const auto& y) { return x.second == y.second; }),
+                              between.end());
+                const V2 start = frame[e], end = frame[(e + 1) % 3];
+                for (const auto& b : between) {
+                    boundary.push_back({b.second, start + (end - start) * b.first});
+                    inserted = true;
+                }
+            }
+            if (!inserted) continue;
+            Poly2 poly;
+            for (const auto& b : boundary) poly.push_back(b.second);
+            if (!ear_clip(poly, 1.0e-12, ears)) {
+                part.failures += 1;
+                continue;
+            }
+            bool degenerate = false;
+            for (const auto& ear : ears) {
+                const V3 a = position(boundary[ear[0]].first), b = position(boundary[ear[1]].first),
+                         c = position(boundary[ear[2]].first);
+                if (mg::norm3(mg::cross3(b - a, c - a)) <= mg::kF64Eps) {
+                    degenerate = true;
+                    break;
+                }
+            }
+            if (degenerate) {
+                part.failures += 1;
+                continue;
+            }
+            std::vector<v3d_mesh_triangle> pieces;
+            for (const auto& ear : ears)
+                pieces.push_back(v3d_mesh_triangle{boundary[ear[0]].first, boundary[ear[1]].first,
+                                                   boundary[ear[2]].first, t.confidence, 0});
+            part.pieces.push_back({slot, std::move(pieces)});
+        }
+    };
+    std::vector<std::thread> pool;
+    for (size_t k = 0; k < n_threads; ++k) pool.emplace_back(work, k);
+    for (auto& th : pool) th.join();
     split.clear();
     failures = 0;
     std::vector<v3d_mesh_triangle> appended;
-    const V2 frame[3] = {V2{0.0, 0.0}, V2{1.0, 0.0}, V2{0.0, 1.0}};
-    const size_t n = tris.size();
-    std::vector<std::pair<uint64_t, V2>> boundary;
-    std::vector<EdgeKey> carriers;
-    std::vector<std::pair<double, uint64_t>> between;
-    std::vector<std::array<uint32_t, 3>> ears;
-    for (size_t slot = 0; slot < n; ++slot) {
-        if (slot % 256 == 0 && canceled()) return false;
-        const v3d_mesh_triangle t = tris[slot];
-        const uint64_t corners[3] = {t.a, t.b, t.c};
-        boundary.clear();
-        bool inserted = false;
-        for (int e = 0; e < 3; ++e) {
-            const uint64_t u = corners[e], v = corners[(e + 1) % 3];
-            boundary.push_back({u, frame[e]});
-            carriers.assign(1, ekey(u, v));
-            for (uint64_t endpoint : {u, v}) {
-                auto it = state.vertex_carriers.find(endpoint);
-                if (it != state.vertex_carriers.end())
-                    carriers.insert(carriers.end(), it->second.begin(), it->second.end());
-            }
-            const EdgeKey* carrier = nullptr;
-            double tu = 0.0, tv = 0.0;
-            for (const auto& c : carriers)
-                if (state.carriers.count(c) && parameter_on(c, u, tu) && parameter_on(c, v, tv)) {
-                    carrier = &c;
-                    break;
-                }
-            if (!carrier) continue;
-            if (std::fabs(tv - tu) <= mg::kF64Eps) continue;
-            between.clear();
-            for (const auto& en : state.carriers.at(*carrier)) {
-                if (en.second == u || en.second == v) continue;
-                const double rel = (en.first - tu) / (tv - tu);
-                if (rel > 1.0e-9 && rel < 1.0 - 1.0e-9) between.push_back({rel, en.second});
-            }
-            std::stable_sort(between.begin(), between.end(),
-                             [](const auto& x, const auto& y) { return total_less(x.first, y.first); });
-            between.erase(std::unique(between.begin(), between.end(),
-                                      [](const auto& x, const auto& y) { return x.second == y.second; }),
-                          between.end());
-            const V2 start = frame[e], end = frame[(e + 1) % 3];
-            for (const auto& b : between) {
-                boundary.push_back({b.second, start + (end - start) * b.first});
-                inserted = true;
-            }
+    for (const Part& part : parts) {
+        failures += part.failures;
+        for (const auto& sp : part.pieces) {
+            tris[sp.first] = sp.second[0];
+            appended.insert(appended.end(), sp.second.begin() + 1, sp.second.end());
+            split.push_back(sp.first);
         }
-        if (!inserted) continue;
-        Poly2 poly;
-        for (const auto& b : boundary) poly.push_back(b.second);
-        if (!ear_clip(poly, 1.0e-12, ears)) {
-            failures += 1;
-            continue;
-        }
-        bool degenerate = false;
-        for (const auto& ear : ears) {
-            const V3 a = position(boundary[ear[0]].first), b = position(boundary[ear[1]].first),
-                     c = position(boundary[ear[2]].first);
-            if (mg::norm3(mg::cross3(b - a, c - a)) <= mg::kF64Eps) {
-                degenerate = true;
-                break;
-            }
-        }
-        if (degenerate) {
-            failures += 1;
-            continue;
-        }
-        for (size_t k = 0; k < ears.size(); ++k) {
-            const v3d_mesh_triangle p{boundary[ears[k][0]].first, boundary[ears[k][1]].first,
-                                      boundary[ears[k][2]].first, t.confidence};
-            if (k == 0) tris[slot] = p;
-            else appended.push_back(p);
-        }
-        split.push_back(slot);
     }
     tris.insert(tris.end(), appended.begin(), appended.end());
     return true;
@@ -1502,9 +1643,11 @@ struct StitchInputs {
     const Grid3* kept_grid;
     const std::vector<uint32_t>* all_kept;
     double tolerance, cell;
+    double* stage_ms;  // [0] retained edges, [1] seams, [2] the greedy pass
 };
 
 std::vector<v3d_mesh_triangle> stitch_trimmed_seams(const StitchInputs& si, Tally& tally) {
+    auto t0 = Clock::now();
     const Inputs& in = *si.in;
     const auto& tris = *in.triangles;
     const auto& removals = *si.removals;
@@ -1546,44 +1689,93 @@ std::vector<v3d_mesh_triangle> stitch_trimmed_seams(const StitchInputs& si, Tall
         uint8_t len;
         bool ok;
     };
+    si.stage_ms[0] += ms_since(t0);
+    t0 = Clock::now();
     std::vector<Seam> seams(removals.size());
     std::vector<std::pair<uint32_t, uint32_t>> seams_by_vertex;
-    std::vector<uint32_t> found;
-    for (size_t slot = 0; slot < removals.size(); ++slot) {
+    // each removal's seam is independent of the others: threads over removals,
+    // the lookups' tallies folded after (max and sum are order-free)
+    auto seam_of = [&](size_t slot, std::vector<uint32_t>& found, Tally& t) {
         const Removal& r = removals[slot];
         Seam& seam = seams[slot];
         seam.ok = false;
         seam.len = 0;
-        if (r.footprint >= fps.size() || !has_geometry[r.triangle]) continue;
+        if (r.footprint >= fps.size() || !has_geometry[r.triangle]) return;
         const Footprint& f = fps[r.footprint];
         PT projected;
-        if (!f.project_candidate(geometry[r.triangle], projected)) continue;
+        if (!f.project_candidate(geometry[r.triangle], projected)) return;
         const int64_t lower = patch_of[r.triangle];
         const v3d_mesh_triangle& removed = tris[r.triangle];
-        std::set<uint64_t> stitchable;
+        // the stitchable vertices, ascending (a BTreeSet in the reference)
+        uint64_t st[kMaxSeamVertices + 1];
+        size_t n_st = 0;
+        bool too_many = false;
+        auto insert = [&](uint64_t v) {
+            for (size_t i = 0; i < n_st; ++i)
+                if (st[i] == v) return;
+            if (n_st == kMaxSeamVertices) {
+                too_many = true;
+                return;
+            }
+            size_t j = n_st++;
+            while (j > 0 && st[j - 1] > v) {
+                st[j] = st[j - 1];
+                --j;
+            }
+            st[j] = v;
+        };
+        auto has = [&](uint64_t v) {
+            for (size_t i = 0; i < n_st; ++i)
+                if (st[i] == v) return true;
+            return false;
+        };
         for (uint64_t v : {removed.a, removed.b, removed.c})
-            if (on_boundary[v] && in.group(v) >= 0) stitchable.insert(v);
+            if (on_boundary[v] && in.group(v) >= 0) insert(v);
         size_t used;
         const Limit q = f.lookup(projected, found, used);
-        tally.record(used, q);
-        if (q != Limit::None) continue;
+        t.record(used, q);
+        if (q != Limit::None) return;
         for (uint32_t kept : found) {
+            if (too_many) break;
             if (!in.linked(r.triangle, f.comp[kept])) continue;
             for (uint32_t vertex : f.vert[kept]) {
-                if (!on_boundary[vertex] || in.group(vertex) < 0 || in.group(vertex) == lower ||
-                    stitchable.count(vertex))
+                if (!on_boundary[vertex] || in.group(vertex) < 0 || in.group(vertex) == lower || has(vertex))
                     continue;
                 double ix, iy, iz;
                 if (mg::project(f.cam, in.position(vertex), ix, iy, iz) && contains(projected, V2{ix, iy}))
-                    stitchable.insert(vertex);
+                    insert(vertex);
+                if (too_many) break;
             }
         }
-        if (stitchable.size() > kMaxSeamVertices) continue;
+        // more than MAX_SEAM_VERTICES: no seam (the reference fails closed)
+        if (too_many) return;
         seam.ok = true;
-        for (uint64_t v : stitchable) seam.v[seam.len++] = (uint32_t)v;
-        for (uint8_t i = 0; i < seam.len; ++i) seams_by_vertex.push_back({seam.v[i], (uint32_t)slot});
+        for (size_t i = 0; i < n_st; ++i) seam.v[seam.len++] = (uint32_t)st[i];
+    };
+    {
+        const size_t n_threads =
+            std::max<size_t>(1, std::min<size_t>(std::thread::hardware_concurrency(), 16));
+        const size_t chunk = (removals.size() + n_threads - 1) / n_threads;
+        std::vector<Tally> tallies(n_threads);
+        std::vector<std::thread> pool;
+        for (size_t k = 0; k < n_threads; ++k)
+            pool.emplace_back([&, k] {
+                std::vector<uint32_t> found;
+                const size_t lo = k * chunk, hi = std::min(removals.size(), lo + chunk);
+                for (size_t slot = lo; slot < hi; ++slot) seam_of(slot, found, tallies[k]);
+            });
+        for (auto& th : pool) th.join();
+        for (const Tally& t : tallies) {
+            tally.max_postings = std::max(tally.max_postings, t.max_postings);
+            tally.bound_hits += t.bound_hits;
+        }
     }
+    for (size_t slot = 0; slot < removals.size(); ++slot)
+        for (uint8_t i = 0; i < seams[slot].len; ++i)
+            seams_by_vertex.push_back({seams[slot].v[i], (uint32_t)slot});
     std::sort(seams_by_vertex.begin(), seams_by_vertex.end());
+    si.stage_ms[1] += ms_since(t0);
+    t0 = Clock::now();
     auto seams_of = [&](uint64_t vertex, std::vector<uint32_t>& out) {
         auto it = std::partition_point(seams_by_vertex.begin(), seams_by_vertex.end(),
                                        [&](const auto& e) { return e.first < vertex; });
@@ -1748,6 +1940,7 @@ std::vector<v3d_mesh_triangle> stitch_trimmed_seams(const StitchInputs& si, Tall
             break;
         }
     }
+    si.stage_ms[2] += ms_since(t0);
     return output;
 }
 
@@ -1800,7 +1993,12 @@ struct Device {
     v3d_context* ctx;
     cudaStream_t st;
     DevBuf<double> corners, fp_tri, ratios;
-    DevBuf<uint32_t> fp_comp, fp_vert, items, anchors;
+    DevBuf<uint32_t> fp_comp, fp_vert, items, anchors, omitted;
+    DevBuf<Cand> cands;
+    DevBuf<OwnerRef> owner_refs;
+    DevBuf<PairOut> pair_outs;
+    DevBuf<CandOut> cand_outs;
+    size_t n_omitted = 0;
     DevBuf<mg::GridBucket> buckets;
     DevBuf<DevFootprint> fps;
     DevBuf<int32_t> cluster;
@@ -1810,6 +2008,7 @@ struct Device {
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     float kernel_ms = 0.f;
     uint64_t launches = 0;
+    double stage_ms[12] = {};
 
     ~Device() {
         corners.release(st);
@@ -1819,6 +2018,11 @@ struct Device {
         fp_vert.release(st);
         items.release(st);
         anchors.release(st);
+        omitted.release(st);
+        cands.release(st);
+        owner_refs.release(st);
+        pair_outs.release(st);
+        cand_outs.release(st);
         buckets.release(st);
         fps.release(st);
         cluster.release(st);
@@ -1828,13 +2032,15 @@ struct Device {
         if (e1) cudaEventDestroy(e1);
     }
     DevStore store() const {
-        return DevStore{corners.p, fps.p, fp_tri.p, fp_comp.p, fp_vert.p, buckets.p, items.p, cluster.p};
+        return DevStore{corners.p, fps.p, fp_tri.p, fp_comp.p, fp_vert.p, buckets.p, items.p, cluster.p,
+                        omitted.p};
     }
     cudaError_t add_footprint(const Footprint& f, size_t capacity_tri, size_t n_groups) {
         cudaError_t e;
         if ((e = fp_tri.ensure(capacity_tri * 9, st)) || (e = fp_comp.ensure(capacity_tri, st)) ||
             (e = fp_vert.ensure(capacity_tri * 3, st)) || (e = items.ensure(capacity_tri, st)) ||
-            (e = buckets.ensure(capacity_tri, st)) || (e = fps.ensure(n_groups, st)))
+            (e = buckets.ensure(capacity_tri, st)) || (e = fps.ensure(n_groups, st)) ||
+            (e = omitted.ensure(capacity_tri, st)))
             return e;
         DevFootprint d{};
         d.cam = f.cam;
@@ -1847,6 +2053,10 @@ struct Device {
         d.item_off = (uint32_t)n_items;
         d.n_bucketed = f.n_bucketed;
         d.n_unindexed = (uint32_t)(f.items.size() - f.n_bucketed);
+        d.omit_off = (uint32_t)n_omitted;
+        d.n_omit = (uint32_t)f.omitted.size();
+        std::vector<uint32_t> omit_comp(f.omitted.size());
+        for (size_t i = 0; i < f.omitted.size(); ++i) omit_comp[i] = f.omitted[i].first;
         static_assert(sizeof(PT) == 9 * sizeof(double), "PT is nine doubles");
         const size_t k = f.tri.size();
         if ((e = cudaMemcpyAsync(fp_tri.p + n_tri * 9, f.tri.data(), sizeof(PT) * k,
@@ -1857,6 +2067,8 @@ struct Device {
                                  sizeof(mg::GridBucket) * f.buckets.size(), cudaMemcpyHostToDevice, st)) ||
             (e = cudaMemcpyAsync(items.p + n_items, f.items.data(), 4 * f.items.size(),
                                  cudaMemcpyHostToDevice, st)) ||
+            (e = cudaMemcpyAsync(omitted.p + n_omitted, omit_comp.data(), 4 * omit_comp.size(),
+                                 cudaMemcpyHostToDevice, st)) ||
             (e = cudaMemcpyAsync(fps.p + n_fps, &d, sizeof d, cudaMemcpyHostToDevice, st)))
             return e;
         // the host copies must outlive the transfers: wait here (one footprint a patch)
@@ -1864,6 +2076,7 @@ struct Device {
         n_tri += k;
         n_buckets += f.buckets.size();
         n_items += f.items.size();
+        n_omitted += f.omitted.size();
         n_fps += 1;
         return cudaSuccess;
     }
@@ -1923,6 +2136,7 @@ int32_t merge_impl(v3d_context* ctx, Device& dev, const v3d_point* points, uint6
     completed = false;
     stats = Stats();
     derived_out.clear();
+    auto t_stage = Clock::now();
     auto group = [&](uint64_t v) -> int64_t { return v < n_points && membership[v] >= 0 ? membership[v] : -1; };
     const size_t nt = tris.size();
     for (const auto& t : tris)
@@ -2110,16 +2324,30 @@ int32_t merge_impl(v3d_context* ctx, Device& dev, const v3d_point* points, uint6
     for (size_t i = 0; i < nt; ++i)
         if (patch_of[i] >= 0) members_of[(size_t)patch_of[i]].push_back((uint32_t)i);
     std::vector<uint8_t> has_footprint(n_groups, 0);
+    // vertex -> triangles (re-indexed corners), to find each patch's anchored triangles
+    std::vector<uint32_t> inc_off(n_points + 1, 0), inc_tri;
+    {
+        for (size_t i = 0; i < nt; ++i)
+            for (uint64_t v : {tris[i].a, tris[i].b, tris[i].c}) inc_off[v + 1] += 1;
+        for (size_t v = 0; v < n_points; ++v) inc_off[v + 1] += inc_off[v];
+        inc_tri.resize(inc_off[n_points]);
+        std::vector<uint32_t> fill(inc_off.begin(), inc_off.end() - 1);
+        for (size_t i = 0; i < nt; ++i)
+            for (uint64_t v : {tris[i].a, tris[i].b, tris[i].c}) inc_tri[fill[v]++] = (uint32_t)i;
+    }
+    std::vector<uint32_t> anchored;
     std::vector<Job> jobs;
     std::vector<JobOut> outs;
     std::vector<uint32_t> nearby;
     std::vector<double> ratio_buf;
+    dev.stage_ms[0] += ms_since(t_stage);
 
     for (size_t pr = 0; pr < order.size(); ++pr) {
         const size_t patch = order[pr];
         if (control.is_canceled()) return V3D_OK;
         const std::vector<uint32_t>& members = members_of[patch];
         if (pr > 0) {
+            t_stage = Clock::now();
             struct Owner {
                 uint32_t slot;
                 double scale;
@@ -2131,6 +2359,7 @@ int32_t merge_impl(v3d_context* ctx, Device& dev, const v3d_point* points, uint6
                 if (linked_patches.count({std::min(fp, patch), std::max(fp, patch)})) owner_slots.push_back(slot);
             }
             // relative depth scale of each owner pair: median of the anchored samples
+            const auto t_scale = Clock::now();
             if (!owner_slots.empty()) {
                 std::vector<uint32_t> anchors_all;
                 jobs.clear();
@@ -2142,15 +2371,21 @@ int32_t merge_impl(v3d_context* ctx, Device& dev, const v3d_point* points, uint6
                     if (it != scale_anchors.end())
                         anchors_all.insert(anchors_all.end(), it->second.begin(), it->second.end());
                     const uint32_t n_a = (uint32_t)anchors_all.size() - a_off;
-                    const uint32_t* ab = anchors_all.data() + a_off;
-                    auto is_anchor = [&](uint64_t v) { return std::binary_search(ab, ab + n_a, (uint32_t)v); };
                     first_job[k] = jobs.size();
-                    for (uint32_t m : members) {
-                        if (!has_geometry[m]) continue;
-                        const auto& t = tris[m];
-                        if (!(is_anchor(t.a) || is_anchor(t.b) || is_anchor(t.c))) continue;
-                        jobs.push_back(Job{m, owner_slots[k], comp_of_tri[m], a_off, n_a, 0, 0, 0.0});
+                    // this patch's triangles at an anchor vertex, ascending (the members the
+                    // reference's scan over the patch finds anchored)
+                    anchored.clear();
+                    for (uint32_t q = a_off; q < a_off + n_a; ++q) {
+                        const uint32_t v = anchors_all[q];
+                        for (uint32_t e = inc_off[v]; e < inc_off[v + 1]; ++e) {
+                            const uint32_t t = inc_tri[e];
+                            if ((size_t)patch_of[t] == patch && has_geometry[t]) anchored.push_back(t);
+                        }
                     }
+                    std::sort(anchored.begin(), anchored.end());
+                    anchored.erase(std::unique(anchored.begin(), anchored.end()), anchored.end());
+                    for (uint32_t m : anchored)
+                        jobs.push_back(Job{m, owner_slots[k], comp_of_tri[m], a_off, n_a, 0, 0, 0.0});
                 }
                 first_job[owner_slots.size()] = jobs.size();
                 std::vector<double> scales(owner_slots.size(), 1.0);
@@ -2211,26 +2446,67 @@ int32_t merge_impl(v3d_context* ctx, Device& dev, const v3d_point* points, uint6
                     owners.push_back({owner_slots[k], scales[k]});
                 }
             }
+            dev.stage_ms[8] += ms_since(t_scale);
             bool imageless_owner = false;
             for (size_t r = 0; r < pr && !imageless_owner; ++r) {
                 const size_t o = order[r];
                 if (linked_patches.count({std::min(o, patch), std::max(o, patch)}) && !has_footprint[o])
                     imageless_owner = true;
             }
-            // every candidate against every linked owner on the device
-            jobs.clear();
+            // every candidate against every linked owner on the device, and each
+            // candidate's fold over its owners
             std::vector<uint32_t> cand;
             for (uint32_t m : members)
                 if (has_geometry[m]) cand.push_back(m);
-            if (!owners.empty()) {
-                for (uint32_t m : cand)
-                    for (const Owner& o : owners)
-                        jobs.push_back(Job{m, o.slot, comp_of_tri[m], 0, 0, 0, 0, o.scale});
-                const DevStore s = dev.store();
-                V3D_CTX_CK(dev.run(jobs, outs, [&](uint32_t n) {
-                    k_ownership<<<(n + 127) / 128, 128, 0, dev.st>>>(s, dev.jobs.p, n, dev.outs.p);
-                }));
+            std::vector<CandOut> folds(cand.size());
+            std::vector<PairOut> pair_host;  // read only for candidates the 3D test takes
+            const uint32_t n_own = (uint32_t)owners.size();
+            if (n_own && !cand.empty()) {
+                std::vector<Cand> cands(cand.size());
+                for (size_t i = 0; i < cand.size(); ++i) cands[i] = Cand{cand[i], comp_of_tri[cand[i]]};
+                std::vector<OwnerRef> refs(n_own);
+                for (uint32_t k = 0; k < n_own; ++k) refs[k] = OwnerRef{owners[k].slot, 0, owners[k].scale};
+                const size_t n_pairs = cands.size() * n_own;
+                V3D_CTX_CK(dev.cands.ensure(cands.size(), dev.st));
+                V3D_CTX_CK(dev.owner_refs.ensure(n_own, dev.st));
+                V3D_CTX_CK(dev.pair_outs.ensure(n_pairs, dev.st));
+                V3D_CTX_CK(dev.cand_outs.ensure(cands.size(), dev.st));
+                V3D_CTX_CK(cudaMemcpyAsync(dev.cands.p, cands.data(), sizeof(Cand) * cands.size(),
+                                           cudaMemcpyHostToDevice, dev.st));
+                V3D_CTX_CK(cudaMemcpyAsync(dev.owner_refs.p, refs.data(), sizeof(OwnerRef) * n_own,
+                                           cudaMemcpyHostToDevice, dev.st));
+                const DevStore st = dev.store();
+                cudaEventRecord(dev.e0, dev.st);
+                k_ownership<<<(unsigned)((n_pairs + 127) / 128), 128, 0, dev.st>>>(
+                    st, dev.cands.p, (uint32_t)cands.size(), dev.owner_refs.p, n_own, dev.pair_outs.p);
+                k_fold<<<(unsigned)((cands.size() + 127) / 128), 128, 0, dev.st>>>(
+                    st, dev.cands.p, (uint32_t)cands.size(), dev.owner_refs.p, n_own, dev.pair_outs.p,
+                    dev.cand_outs.p);
+                cudaEventRecord(dev.e1, dev.st);
+                dev.launches += 2;
+                ::v3d::g_kernel_launches += 2;
+                V3D_CTX_CK(cudaGetLastError());
+                V3D_CTX_CK(cudaMemcpyAsync(folds.data(), dev.cand_outs.p, sizeof(CandOut) * folds.size(),
+                                           cudaMemcpyDeviceToHost, dev.st));
+                V3D_CTX_CK(cudaStreamSynchronize(dev.st));
+                float ms = 0.f;
+                if (cudaEventElapsedTime(&ms, dev.e0, dev.e1) == cudaSuccess) dev.kernel_ms += ms;
+                bool any_3d = false;
+                for (const CandOut& f : folds)
+                    if (!(f.flags & 1u) && !(f.share >= kMinImageOwnershipShare) &&
+                        !((f.flags & 2u) && !imageless_owner))
+                        any_3d = true;
+                if (any_3d) {
+                    pair_host.resize(n_pairs);
+                    V3D_CTX_CK(cudaMemcpyAsync(pair_host.data(), dev.pair_outs.p, sizeof(PairOut) * n_pairs,
+                                               cudaMemcpyDeviceToHost, dev.st));
+                    V3D_CTX_CK(cudaStreamSynchronize(dev.st));
+                }
+            } else {
+                for (CandOut& f : folds) f = CandOut{0.0, 0.0, 1.0, 0xffffffffu, 0u, 0u, n_own == 0 ? 2u : 0u};
             }
+            dev.stage_ms[1] += ms_since(t_stage);
+            t_stage = Clock::now();
             std::set<size_t> judged_patches;
             std::map<size_t, std::vector<uint32_t>> unjudged_triangles;
             std::vector<const Geometry*> surfaces;
@@ -2238,39 +2514,15 @@ int32_t merge_impl(v3d_context* ctx, Device& dev, const v3d_point* points, uint6
                 if (control.is_canceled()) return V3D_OK;
                 const uint32_t index = cand[ci];
                 const Geometry& candidate = geometry[index];
-                judged_patches.clear();
-                unjudged_triangles.clear();
-                double best_share = 0.0, best_surface = 0.0, best_scale = 1.0;
-                uint32_t best_slot = UINT32_MAX;
-                bool cut_off = false;
-                for (size_t k = 0; k < owners.size(); ++k) {
-                    const JobOut& o = outs[ci * owners.size() + k];
-                    if (o.status == kUnprojectable) continue;
-                    if (o.status == kPostingBound) {
-                        tally.record(o.used, Limit::Postings);
-                        cut_off = true;
-                        break;
-                    }
-                    if (o.status == kTooManyCells) {
-                        tally.record(o.used, Limit::Cells);
-                        continue;
-                    }
-                    tally.record(o.used, Limit::None);
-                    const Footprint& f = footprints[owners[k].slot];
-                    std::vector<uint32_t> unjudged;
-                    if (o.share < kMinImageOwnershipShare)
-                        for (const auto& om : f.omitted)
-                            if (components_linked(index, om.first)) unjudged.push_back(om.second);
-                    if (unjudged.empty()) judged_patches.insert(f.patch);
-                    else unjudged_triangles[f.patch] = std::move(unjudged);
-                    if (o.share > best_share) {
-                        best_share = o.share;
-                        best_surface = o.surface;
-                        best_slot = owners[k].slot;
-                        best_scale = owners[k].scale;
-                    }
+                const CandOut& fo = folds[ci];
+                // the lookups this candidate's owners recorded
+                if (n_own) {
+                    tally.max_postings = std::max<size_t>(tally.max_postings, fo.max_used);
+                    tally.bound_hits += fo.bound_hits;
                 }
-                if (cut_off) continue;
+                if (fo.flags & 1u) continue;  // cut off at the posting bound: kept unjudged
+                const double best_share = fo.share, best_surface = fo.surface, best_scale = fo.scale;
+                const uint32_t best_slot = fo.slot;
                 if (best_share >= kMinImageOwnershipShare) {
                     keep[index] = 0;
                     removed_dup += 1;
@@ -2281,12 +2533,26 @@ int32_t merge_impl(v3d_context* ctx, Device& dev, const v3d_point* points, uint6
                     }
                     continue;
                 }
-                if (judged_patches.size() == owners.size() && !imageless_owner) {
+                if ((fo.flags & 2u) && !imageless_owner) {
                     if (best_share > kOwnershipEpsilon) {
                         remaining_overlap += 1;
                         clip_jobs.push_back({index, best_slot, best_scale});
                     }
                     continue;
+                }
+                // which owners judged it, and the kept triangles the others could not project
+                judged_patches.clear();
+                unjudged_triangles.clear();
+                for (uint32_t k = 0; k < n_own; ++k) {
+                    const PairOut& o = pair_host[ci * n_own + k];
+                    if (o.status != kJudged) continue;
+                    const Footprint& f = footprints[owners[k].slot];
+                    std::vector<uint32_t> unjudged;
+                    if (o.share < kMinImageOwnershipShare)
+                        for (const auto& om : f.omitted)
+                            if (components_linked(index, om.first)) unjudged.push_back(om.second);
+                    if (unjudged.empty()) judged_patches.insert(f.patch);
+                    else unjudged_triangles[f.patch] = std::move(unjudged);
                 }
                 // the 3D test (surface_merge.rs:737-795)
                 double lo[3], hi[3];
@@ -2329,6 +2595,8 @@ int32_t merge_impl(v3d_context* ctx, Device& dev, const v3d_point* points, uint6
                 }
             }
         }
+        if (pr > 0) dev.stage_ms[2] += ms_since(t_stage);
+        t_stage = Clock::now();
         if (patch < n_cams && cams[patch].present) {
             Footprint f;
             f.patch = patch;
@@ -2361,20 +2629,59 @@ int32_t merge_impl(v3d_context* ctx, Device& dev, const v3d_point* points, uint6
             geometry[m].aabb(tolerance, lo, hi);
             kept_grid.insert(m, lo, hi);
         }
+        dev.stage_ms[3] += ms_since(t_stage);
     }
     // seams, clips, assembly (surface_merge.rs:848-1077)
-    StitchInputs si{&in, &keep, &patch_of, &removals, &kept_grid, &all_kept, tolerance, cell};
+    StitchInputs si{&in, &keep, &patch_of, &removals, &kept_grid, &all_kept, tolerance, cell, dev.stage_ms + 9};
+    t_stage = Clock::now();
     std::vector<v3d_mesh_triangle> stitches = stitch_trimmed_seams(si, tally);
+    dev.stage_ms[4] += ms_since(t_stage);
+    t_stage = Clock::now();
     ClipState clip_state;
     clip_state.base = n_points;
     std::vector<std::pair<uint32_t, std::vector<std::array<uint64_t, 3>>>> clipped;
     uint64_t clip_failures = 0;
     std::vector<std::array<uint64_t, 3>> pieces;
-    for (const ClipJob& job : clip_jobs) {
-        if (control.is_canceled()) return V3D_OK;
-        if (clip_overlap(in, clip_state, job, tally, pieces)) clipped.push_back({job.triangle, pieces});
-        else clip_failures += 1;
+    {
+        // plan the clips concurrently (pure geometry), commit them in job order;
+        // batches bound the plans held at once
+        constexpr size_t kBatch = 8192;
+        const size_t n_threads =
+            std::max<size_t>(1, std::min<size_t>(std::thread::hardware_concurrency(), 16));
+        std::vector<ClipPlan> plans;
+        std::vector<uint8_t> planned;
+        std::vector<Tally> tallies(n_threads);
+        for (size_t b0 = 0; b0 < clip_jobs.size(); b0 += kBatch) {
+            const size_t b1 = std::min(clip_jobs.size(), b0 + kBatch);
+            plans.assign(b1 - b0, ClipPlan());
+            planned.assign(b1 - b0, 0);
+            std::atomic<size_t> next{b0};
+            std::vector<std::thread> pool;
+            for (size_t k = 0; k < n_threads; ++k)
+                pool.emplace_back([&, k] {
+                    for (;;) {
+                        const size_t j = next.fetch_add(16);
+                        if (j >= b1) break;
+                        for (size_t i = j; i < std::min(j + 16, b1); ++i)
+                            planned[i - b0] = plan_clip(in, clip_jobs[i], tallies[k], plans[i - b0]) ? 1 : 0;
+                    }
+                });
+            for (auto& th : pool) th.join();
+            for (size_t i = b0; i < b1; ++i) {
+                if (control.is_canceled()) return V3D_OK;
+                if (planned[i - b0] && commit_clip(in, clip_state, plans[i - b0], pieces))
+                    clipped.push_back({clip_jobs[i].triangle, pieces});
+                else
+                    clip_failures += 1;
+            }
+        }
+        for (const Tally& t : tallies) {
+            tally.max_postings = std::max(tally.max_postings, t.max_postings);
+            tally.bound_hits += t.bound_hits;
+        }
     }
+    dev.stage_ms[5] += ms_since(t_stage);
+    t_stage = Clock::now();
     for (const auto& c : clipped) keep[c.first] = 0;
     stats.retained_by_group.assign(n_groups, 0);
     for (size_t i = 0; i < nt; ++i)
@@ -2383,16 +2690,19 @@ int32_t merge_impl(v3d_context* ctx, Device& dev, const v3d_point* points, uint6
         if (patch_of[c.first] >= 0) stats.retained_by_group[(size_t)patch_of[c.first]] += c.second.size();
     uint64_t shared_vertices = 0;
     {
-        std::unordered_map<uint64_t, std::pair<int64_t, bool>> owner;
-        owner.reserve(nt);
+        // per vertex: the patch of the first retained triangle using it, and
+        // whether a retained triangle of another patch uses it too
+        const int64_t kUnseen = INT64_MIN;
+        std::vector<int64_t> first_patch(n_points, kUnseen);
+        std::vector<uint8_t> shared(n_points, 0);
         for (size_t i = 0; i < nt; ++i) {
             if (!keep[i]) continue;
             for (uint64_t v : {tris[i].a, tris[i].b, tris[i].c}) {
-                auto it = owner.emplace(v, std::make_pair(patch_of[i], false)).first;
-                if (it->second.first != patch_of[i]) it->second.second = true;
+                if (first_patch[v] == kUnseen) first_patch[v] = patch_of[i];
+                else if (first_patch[v] != patch_of[i]) shared[v] = 1;
             }
         }
-        for (const auto& kv : owner) shared_vertices += kv.second.second ? 1 : 0;
+        for (size_t v = 0; v < n_points; ++v) shared_vertices += shared[v];
     }
     std::vector<float> clipped_confidence;
     for (const auto& c : clipped) clipped_confidence.push_back(tris[c.first].confidence);
@@ -2420,6 +2730,8 @@ int32_t merge_impl(v3d_context* ctx, Device& dev, const v3d_point* points, uint6
             tris.push_back(v3d_mesh_triangle{p[0], p[1], p[2], clipped_confidence[c], 0});
     }
     uint64_t conformed = 0, conformance_failures = 0;
+    dev.stage_ms[7] += ms_since(t_stage);
+    t_stage = Clock::now();
     if (!clip_state.carriers.empty()) {
         auto derived_position = [&](uint64_t v) {
             if (v < n_points) return position(v);
@@ -2439,6 +2751,8 @@ int32_t merge_impl(v3d_context* ctx, Device& dev, const v3d_point* points, uint6
                                            }),
                             stats.sources.end());
     }
+    dev.stage_ms[6] += ms_since(t_stage);
+    t_stage = Clock::now();
     auto group_all = [&](uint64_t v) -> int64_t {
         if (v < n_points) return group(v);
         const uint64_t d = v - n_points;
@@ -2498,6 +2812,7 @@ int32_t merge_impl(v3d_context* ctx, Device& dev, const v3d_point* points, uint6
     o.conformance_failures = conformance_failures;
     derived_out = std::move(clip_state.derived);
     completed = true;
+    dev.stage_ms[7] += ms_since(t_stage);
     return V3D_OK;
 }
 
@@ -2560,6 +2875,7 @@ extern "C" int32_t v3d_merge_fused_patches_owned(
     }
     ctx->last_ms = dev.kernel_ms;
     ctx->last_launches = g_kernel_launches - launches0;
+    for (int i = 0; i < 12; ++i) ctx->last_merge_stage_ms[i] = dev.stage_ms[i];
     if (control.is_canceled()) {
         ctx->last_error = "reconstruction canceled";
         return V3D_REJECTED;

@@ -196,7 +196,8 @@ class RunInfo(C.Structure):
                 ("triangles", C.c_uint64), ("host_block_ms", C.c_double),
                 ("host_readback_ms", C.c_double), ("result_bytes", C.c_uint64),
                 ("sweep_chunks", C.c_uint64), ("recip_sweep_ms", C.c_double),
-                ("recip_prepare_ms", C.c_double), ("sweep_tile_x", C.c_uint64)]
+                ("recip_prepare_ms", C.c_double), ("sweep_tile_x", C.c_uint64),
+                ("merge_stage_ms", C.c_double * 12)]
 
 
 CANCEL_FN = C.CFUNCTYPE(C.c_int32, C.c_void_p)

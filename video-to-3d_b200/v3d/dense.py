@@ -330,7 +330,8 @@ class Context:
         """Device time, kernel launches and work units of the last dense call."""
         info = abi.RunInfo()
         self._check(self.lib.v3d_last_run_info(self.handle, C.byref(info)))
-        return {name: getattr(info, name) for name, _ in abi.RunInfo._fields_}
+        return {name: (list(getattr(info, name)) if name == "merge_stage_ms" else getattr(info, name))
+                for name, _ in abi.RunInfo._fields_}
 
     def debug_sweep(self, frames, cameras, sparse_points, focal, fine_grid=False, profile=None):
         """Per-site sweep records (status, plane, support, error, margin) in raster order."""
