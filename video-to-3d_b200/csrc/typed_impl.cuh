@@ -183,6 +183,14 @@ __device__ __forceinline__ float sample_nonneg(const T* __restrict__ p, uint32_t
 __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
 __device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
 
+// The approximate reciprocal of the special-function unit, as __fdividef(1, x)
+// computes it for the normal, positive denominators the sweeps pass.
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 template <class T>
 __device__ __forceinline__ float2 sample_nonneg_pair(const T* __restrict__ p, uint32_t w, float2 u,
                                                      float2 v) {
@@ -309,7 +317,7 @@ __device__ __forceinline__ bool rect_inside(const float* H, float zmin, float wl
         const float X = (c & 1) ? xb : xa;
         const float Y = (c & 2) ? yb : ya;
         const float h2 = fmaf(H[6], X, fmaf(H[7], Y, H[8]));
-        const float iv = __fdividef(1.0f, h2);
+        const float iv = rcp_approx(h2);
         const float u = fmaf(H[0], X, fmaf(H[1], Y, H[2])) * iv;
         const float v = fmaf(H[3], X, fmaf(H[4], Y, H[5])) * iv;
         hmin = fminf(hmin, h2);
@@ -521,7 +529,7 @@ __global__ void __launch_bounds__(kTileThreads, 1024 / kTileThreads) k_sweep_til
                 const float2 hy = __ffma2_rn(f2(a4, a4), Y2, f2(H5, H5));
                 const float2 hz = __ffma2_rn(f2(a7, a7), Y2, f2(H8, H8));
                 const float2 h2 = __ffma2_rn(f2(a6, a6), X2, hz);
-                const float2 iv = f2(__fdividef(1.0f, h2.x), __fdividef(1.0f, h2.y));
+                const float2 iv = f2(rcp_approx(h2.x), rcp_approx(h2.y));
                 const float2 u = __fmul2_rn(__ffma2_rn(f2(a0, a0), X2, hx), iv);
                 const float2 q = __fmul2_rn(__ffma2_rn(f2(a3, a3), X2, hy), iv);
                 float va = __int_as_float(0x7fc00000), vb = va;
@@ -786,7 +794,7 @@ __device__ __forceinline__ bool window_inside(const float* H, float zmin, float 
         const float X = x + ((c & 1) ? (float)R : -(float)R);
         const float Y = y + ((c & 2) ? (float)R : -(float)R);
         const float h2 = fmaf(H[6], X, fmaf(H[7], Y, H[8]));
-        const float iv = __fdividef(1.0f, h2);
+        const float iv = rcp_approx(h2);
         const float u = fmaf(H[0], X, fmaf(H[1], Y, H[2])) * iv;
         const float v = fmaf(H[3], X, fmaf(H[4], Y, H[5])) * iv;
         hmin = fminf(hmin, h2);
@@ -806,13 +814,27 @@ __device__ __forceinline__ bool window_inside(const float* H, float zmin, float 
 //  * ImageSampler reads the image in global memory;
 //  * BandSampler reads a staged box of it in shared memory (a warp's band,
 //    rows of kBandPitch entries starting at image texel (x0, y0); entry c of a
-//    row holds texels c and c + 1, so a bilinear tap is two 8-byte loads).  The floor is
-//    the same round-down add with the box origin folded into the shift:
-//    u + (2^23 - x0) rounded down is 2^23 - x0 + floor(u) exactly, whose low
-//    mantissa bits are floor(u) - x0, the band column; the fraction u - floor(u)
-//    and the texel values are the image's, so the two samplers agree bit for bit.
-constexpr int kBandPitch = 64;  // texels per staged band row
+//    row holds texel c and the difference texel c+1 - texel c, the f32
+//    subtraction the bilinear step makes, so a tap reads four words and
+//    starts its interpolation with an FMA).  The floor is the same round-down
+//    add with the box origin folded into the shift: u + (2^23 - x0) rounded
+//    down is 2^23 - x0 + floor(u) exactly, whose bits are 2^23's plus
+//    floor(u) - x0, the band column; so the entry's 32-bit shared address is
+//    one shift-add of each coordinate's bits onto a per-band constant (the
+//    2^23 bits folded in, modulo 2^32).  The fraction u - floor(u) and the
+//    texel values are the image's, so the two samplers agree bit for bit.
+constexpr int kBandPitch = 64;  // entries per staged band row
 constexpr int kBandRows = 20;   // staged band rows
+constexpr int kBandRowShift = 9;  // log2 of a row's bytes (kBandPitch 8-byte entries)
+static_assert(8 * kBandPitch == (1 << kBandRowShift), "band row bytes");
+
+// Shared-memory loads at a 32-bit shared address.
+__device__ __forceinline__ float lds_f32(uint32_t a) {
+    float x;
+    asm volatile("ld.shared.f32 %0, [%1];" : "=f"(x) : "r"(a));
+    return x;
+}
+
 
 template <class T>
 struct ImageSampler {
@@ -827,34 +849,42 @@ struct ImageSampler {
 };
 
 struct BandSampler {
-    const float2* band;
-    float sx, sy;  // 2^23 - x0, 2^23 - y0
+    uint32_t cbase;  // shared address of the band minus (8 + 8 kBandPitch) x bits(2^23), mod 2^32
+    float sx, sy;    // 2^23 - x0, 2^23 - y0
+    __device__ BandSampler(const float2* band, float sx_, float sy_) : sx(sx_), sy(sy_) {
+        const uint32_t sb = (uint32_t)__float_as_int(8388608.0f);
+        cbase = (uint32_t)__cvta_generic_to_shared(band) - (8u + 8u * kBandPitch) * sb;
+    }
+    // shared address of the entry under (tu, tv), the rounded-down shifted coordinates
+    __device__ __forceinline__ uint32_t entry(float tu, float tv) const {
+        return cbase + ((uint32_t)__float_as_int(tv) << kBandRowShift) +
+               ((uint32_t)__float_as_int(tu) << 3);
+    }
     __device__ __forceinline__ float operator()(float u, float v) const {
-        const int sb = __float_as_int(8388608.0f);
         const float tu = __fadd_rd(u, sx), tv = __fadd_rd(v, sy);
         const float fu = tu - sx, fv = tv - sy;
-        const int o = (__float_as_int(tv) - sb) * kBandPitch + (__float_as_int(tu) - sb);
+        const uint32_t a = entry(tu, tv);
         const float tx = u - fu, ty = v - fv;
-        const float2 t0 = band[o], t1 = band[o + kBandPitch];
-        const float v00 = t0.x, v10 = t0.y, v01 = t1.x, v11 = t1.y;
-        const float top = fmaf(v10 - v00, tx, v00);
-        const float bot = fmaf(v11 - v01, tx, v01);
+        constexpr uint32_t kRow = 1u << kBandRowShift;
+        const float v00 = lds_f32(a), d0 = lds_f32(a + 4);
+        const float v01 = lds_f32(a + kRow), d1 = lds_f32(a + kRow + 4);
+        const float top = fmaf(d0, tx, v00);
+        const float bot = fmaf(d1, tx, v01);
         return fmaf(bot - top, ty, top);
     }
+    // two taps at once; the loads land in the halves of the packed operands
     __device__ __forceinline__ float2 pair(float2 u, float2 v) const {
-        const int sb = __float_as_int(8388608.0f);
         const float2 s2x = f2(sx, sx), s2y = f2(sy, sy);
         const float2 tu = __fadd2_rd(u, s2x), tv = __fadd2_rd(v, s2y);
         const float2 fu = __fadd2_rn(tu, neg2(s2x)), fv = __fadd2_rn(tv, neg2(s2y));
-        const int oa = (__float_as_int(tv.x) - sb) * kBandPitch + (__float_as_int(tu.x) - sb);
-        const int ob = (__float_as_int(tv.y) - sb) * kBandPitch + (__float_as_int(tu.y) - sb);
+        const uint32_t aa = entry(tu.x, tv.x), ab = entry(tu.y, tv.y);
         const float2 tx = __fadd2_rn(u, neg2(fu)), ty = __fadd2_rn(v, neg2(fv));
-        const float2 a0 = band[oa], a1 = band[oa + kBandPitch];
-        const float2 b0 = band[ob], b1 = band[ob + kBandPitch];
-        const float2 v00 = f2(a0.x, b0.x), v10 = f2(a0.y, b0.y);
-        const float2 v01 = f2(a1.x, b1.x), v11 = f2(a1.y, b1.y);
-        const float2 top = __ffma2_rn(__fadd2_rn(v10, neg2(v00)), tx, v00);
-        const float2 bot = __ffma2_rn(__fadd2_rn(v11, neg2(v01)), tx, v01);
+        constexpr uint32_t kRow = 1u << kBandRowShift;
+        const float2 v00 = f2(lds_f32(aa), lds_f32(ab)), d0 = f2(lds_f32(aa + 4), lds_f32(ab + 4));
+        const float2 v01 = f2(lds_f32(aa + kRow), lds_f32(ab + kRow));
+        const float2 d1 = f2(lds_f32(aa + kRow + 4), lds_f32(ab + kRow + 4));
+        const float2 top = __ffma2_rn(d0, tx, v00);
+        const float2 bot = __ffma2_rn(d1, tx, v01);
         return __ffma2_rn(__fadd2_rn(bot, neg2(top)), ty, top);
     }
 };
@@ -884,7 +914,7 @@ __device__ __forceinline__ bool window_cost(const float* pvc, float pm, float pv
             const float X = x + (float)(dx - R);
             const float h2 = fmaf(H[6], X, hz);
             if (CHECK && !(h2 > zmin)) return false;
-            const float iv = __fdividef(1.0f, h2);
+            const float iv = rcp_approx(h2);
             const float u = fmaf(H[0], X, hx) * iv;
             const float v = fmaf(H[3], X, hy) * iv;
             if (CHECK && !(u >= 0.f && v >= 0.f && u < wl && v < hl)) return false;
@@ -945,7 +975,7 @@ __device__ __forceinline__ void window_cost_zncc_pair(const float* pvc, float pm
             const float X = x + (float)(dx - R);
             const float2 X2 = f2(X, X);
             const float2 h2 = __ffma2_rn(H6, X2, hz);
-            const float2 iv = f2(__fdividef(1.0f, h2.x), __fdividef(1.0f, h2.y));
+            const float2 iv = f2(rcp_approx(h2.x), rcp_approx(h2.y));
             const float2 u = __fmul2_rn(__ffma2_rn(H0, X2, hx), iv);
             const float2 v = __fmul2_rn(__ffma2_rn(H3, X2, hy), iv);
             const float2 s = __fadd2_rn(smp_of.pair(u, v), npm);
@@ -998,7 +1028,7 @@ __device__ __forceinline__ bool band_box(const float* A, const float* bv, float 
             const float X = x + ((c & 1) ? (float)R : -(float)R);
             const float Y = y + ((c & 2) ? (float)R : -(float)R);
             const float h2 = fmaf(H[6], X, fmaf(H[7], Y, H[8]));
-            const float iv = __fdividef(1.0f, h2);
+            const float iv = rcp_approx(h2);
             const float u = fmaf(H[0], X, fmaf(H[1], Y, H[2])) * iv;
             const float v = fmaf(H[3], X, fmaf(H[4], Y, H[5])) * iv;
             hmin = fminf(hmin, h2);
@@ -1261,12 +1291,14 @@ __global__ void __launch_bounds__(RecipBounds<MODE>::kThreads, RecipBounds<MODE>
             continue;
         }
         if (banded) {
-            // entry c: texels c and c + 1 of the row; the last column is read only
-            // as a right neighbour
+            // entry c: texel c of the row and texel c + 1 minus texel c; the last
+            // column is read only as a right neighbour
             for (int rr = 0; rr < rows; ++rr) {
                 const T* row = rimg + (size_t)(by0 + rr) * rw + bx0;
-                for (int c = lane; c < cols - 1; c += 32)
-                    band[rr * kBandPitch + c] = f2(pix<T>(row, c), pix<T>(row, c + 1));
+                for (int c = lane; c < cols - 1; c += 32) {
+                    const float t0 = pix<T>(row, c), t1 = pix<T>(row, c + 1);
+                    band[rr * kBandPitch + c] = f2(t0, t1 - t0);
+                }
             }
         }
         __syncwarp();
