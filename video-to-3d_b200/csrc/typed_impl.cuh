@@ -392,9 +392,10 @@ __global__ void __launch_bounds__(kTileThreads, 1024 / kTileThreads) k_sweep_til
     float* hA = costs + ms * kTileThreads;   // [max_src][12] homography parts
     float* pinv = hA + ms * 12;              // [planes] inverse depths
     uint32_t* inmask = reinterpret_cast<uint32_t*>(pinv + b.prof.planes);  // [planes] inside sources
+    int* rowmap = reinterpret_cast<int*>(inmask + b.prof.planes);  // [PY] horizontal pass rows
     // [steps * kTileY][32] (x_a, x_b, y_a, y_b) of the slots f and f + 32 of each lane step
     float4* slotxy = reinterpret_cast<float4*>(
-        (reinterpret_cast<uintptr_t>(inmask + b.prof.planes) + 15) & ~(uintptr_t)15);
+        (reinterpret_cast<uintptr_t>(rowmap + PY) + 15) & ~(uintptr_t)15);
     const int n_steps = tiled_steps(np);
     const int tid = threadIdx.x;
     const T* rdata = static_cast<const T*>(ref.img.data);
@@ -450,6 +451,26 @@ __global__ void __launch_bounds__(kTileThreads, 1024 / kTileThreads) k_sweep_til
                 m |= 1u << j;
         }
         inmask[kk] = m;
+    }
+    // The horizontal pass of a 16-wide tile gives a warp's half-warps two rows;
+    // rows pd apart, pd x PXp = 16 (mod 32) words, fall on the two halves of the
+    // banks.  Rows pair up in blocks of 2 pd (the rows of a last partial block
+    // in order); the row sums land at their own rows either way.
+    if (TX == 16) {
+        int pd = 0;
+        for (int d = 1; d < 32 && !pd; ++d)
+            if ((d * PXp) % 32 == 16) pd = d;
+        for (int q = tid; q < PY; q += kTileThreads) {
+            int row = q;
+            if (pd) {
+                const int blk = 2 * pd, bq = q / blk;
+                if ((bq + 1) * blk <= PY) {
+                    const int w = q - bq * blk;
+                    row = bq * blk + (w >> 1) + (w & 1) * pd;
+                }
+            }
+            rowmap[q] = row;
+        }
     }
     // slot of tap dx of the window that starts at column 0 (add the window's start)
     int toff[W];
@@ -556,7 +577,9 @@ __global__ void __launch_bounds__(kTileThreads, 1024 / kTileThreads) k_sweep_til
             // horizontal box filter: the window of column c of row yy at slot c,
             // TX windows a row (a warp takes one row of 32, or two rows of 16)
             for (int i = tid; i < PY * TX; i += kTileThreads) {
-                const int yy = i / TX, c = i % TX;
+                const int c = i % TX;
+                const int yy = TX == 16 ? rowmap[i / TX] : i / TX;
+                const int o = yy * TX + c;
                 const float* sp = samp + yy * PXp + c;
                 const float* rp = refv + yy * PXp + c;
                 if (kF32) {
@@ -569,9 +592,9 @@ __global__ void __launch_bounds__(kTileThreads, 1024 / kTileThreads) k_sweep_til
                         ab = __ffma2_rn(f2(v, v), f2(1.0f, v), ab);
                         c = fmaf(rp[toff[dx]] - shift, v, c);
                     }
-                    hs[i] = (Acc)ab.x;
-                    hss[i] = (Acc)ab.y;
-                    hrs[i] = (Acc)c;
+                    hs[o] = (Acc)ab.x;
+                    hss[o] = (Acc)ab.y;
+                    hrs[o] = (Acc)c;
                 } else {
                     double a = 0.0, bb = 0.0, c = 0.0;
 #pragma unroll
@@ -581,9 +604,9 @@ __global__ void __launch_bounds__(kTileThreads, 1024 / kTileThreads) k_sweep_til
                         bb = fma(v, v, bb);
                         c = fma((double)rp[toff[dx]], v, c);
                     }
-                    hs[i] = (Acc)a;
-                    hss[i] = (Acc)bb;
-                    hrs[i] = (Acc)c;
+                    hs[o] = (Acc)a;
+                    hss[o] = (Acc)bb;
+                    hrs[o] = (Acc)c;
                 }
             }
             __syncthreads();
@@ -949,9 +972,10 @@ __device__ __forceinline__ bool window_cost(const float* pvc, float pm, float pv
 // the caller established: the same operations as window_cost<R, 1, false>,
 // each done on both hypotheses by one packed f32x2 instruction (sm_100) with
 // the scalar's rounding, so every component equals the scalar cost bit for
-// bit while the pair costs about half the issue slots.
+// bit while the pair costs about half the issue slots.  pvc2 holds the
+// centred window with each value twice, so a tap loads its packed operand.
 template <int R, class S>
-__device__ __forceinline__ void window_cost_zncc_pair(const float* pvc, float pm, float pvar,
+__device__ __forceinline__ void window_cost_zncc_pair(const float2* pvc2, float pm, float pvar,
                                                       const float* Ha, const float* Hb,
                                                       float minvar, const S& smp_of, float x,
                                                       float y, bool& oka, float& ea, bool& okb,
@@ -969,7 +993,7 @@ __device__ __forceinline__ void window_cost_zncc_pair(const float* pvc, float pm
         const float2 Y2 = f2(Y, Y);
         const float2 hx = __ffma2_rn(H1, Y2, H2), hy = __ffma2_rn(H4, Y2, H5),
                      hz = __ffma2_rn(H7, Y2, H8);
-        const float* prow = pvc + dy * W;
+        const float2* prow = pvc2 + dy * W;
 #pragma unroll
         for (int dx = 0; dx < W; ++dx) {
             const float X = x + (float)(dx - R);
@@ -981,7 +1005,7 @@ __device__ __forceinline__ void window_cost_zncc_pair(const float* pvc, float pm
             const float2 s = __fadd2_rn(smp_of.pair(u, v), npm);
             ss = __fadd2_rn(ss, s);
             sss = __ffma2_rn(s, s, sss);
-            sps = __ffma2_rn(f2(prow[dx], prow[dx]), s, sps);
+            sps = __ffma2_rn(prow[dx], s, sps);
         }
     }
     const float n = (float)N;
@@ -1220,11 +1244,13 @@ __global__ void __launch_bounds__(RecipBounds<MODE>::kThreads, RecipBounds<MODE>
     constexpr int N = W * W;
     constexpr int kWarps = RecipBounds<MODE>::kWarps;
     __shared__ float pvc_all[kWarps][N];
+    __shared__ float2 pvc2_all[kWarps][N];  // the same values twice, a packed operand each
     // the warps' bands of texel pairs (banded kernel only), with a guard row
     // before the first and after the last
     __shared__ float2 band_all[MODE == kRecipBanded ? (kWarps * kBandRows + 2) * kBandPitch : 1];
     const uint32_t lane = lane_id(), wid = threadIdx.x >> 5;
     float* pvc = pvc_all[wid];
+    float2* pvc2 = pvc2_all[wid];
     float2* band = band_all + (MODE == kRecipBanded ? (1 + wid * kBandRows) * kBandPitch : 0);
     const uint32_t ms = (uint32_t)b.max_src;
     const uint32_t n_list = *list_count;
@@ -1261,7 +1287,10 @@ __global__ void __launch_bounds__(RecipBounds<MODE>::kThreads, RecipBounds<MODE>
             const int t = lane + 32 * h;
             const float d = t < N ? p[h] - pm : 0.f;
             dsq += d * d;
-            if (t < N) pvc[t] = d;
+            if (t < N) {
+                pvc[t] = d;
+                pvc2[t] = f2(d, d);
+            }
         }
         const float pvar = warp_sum(dsq);
         const float* inv_tab = b.src_inv + ref.inv_off + (size_t)si * ref.planes;
@@ -1314,7 +1343,7 @@ __global__ void __launch_bounds__(RecipBounds<MODE>::kThreads, RecipBounds<MODE>
                     plane_h(src.bwd_A, src.bwd_b, inv_tab[k2], Hb);
                     bool oka, okb;
                     float ea, eb;
-                    window_cost_zncc_pair<R>(pvc, pm, pvar, Ha, Hb, minvar, smp, x0, y0, oka, ea,
+                    window_cost_zncc_pair<R>(pvc2, pm, pvar, Ha, Hb, minvar, smp, x0, y0, oka, ea,
                                              okb, eb);
                     take(oka, ea, k);
                     take(okb, eb, k2);
@@ -1357,7 +1386,7 @@ __global__ void __launch_bounds__(RecipBounds<MODE>::kThreads, RecipBounds<MODE>
                 if (COST == 1 && ina && inb) {
                     bool oka, okb;
                     float ea, eb;
-                    window_cost_zncc_pair<R>(pvc, pm, pvar, Ha, Hb, minvar, smp, x0, y0, oka, ea,
+                    window_cost_zncc_pair<R>(pvc2, pm, pvar, Ha, Hb, minvar, smp, x0, y0, oka, ea,
                                              okb, eb);
                     take(oka, ea, k);
                     take(okb, eb, k2);
@@ -1542,7 +1571,7 @@ cudaError_t Typed<T>::sweep_tiled(const BatchDev& b, uint32_t max_nx, uint32_t m
         const size_t PXp = (size_t)((PX + s - 1) / s) * s, np = PXp * PY;
         const size_t smem = (b.sums32 ? sizeof(float) : sizeof(double)) * 3 * (size_t)PY * TX +
                             sizeof(float) * (2 * np + (size_t)b.max_src * (kTileThreads + 12) +
-                                             2 * (size_t)b.prof.planes) +
+                                             2 * (size_t)b.prof.planes + PY) +
                             16 + sizeof(float4) * (size_t)tiled_steps((int)np) * kTileThreads;
         cudaError_t e = raise_dynamic_smem_limit(reinterpret_cast<const void*>(kern), smem);
         if (e != cudaSuccess) return e;
