@@ -774,11 +774,11 @@ __global__ void __launch_bounds__(256) k_reciprocal_exact(BatchDev b, const Cand
 // Same contract as k_reciprocal_exact for the fast policy, split in two
 // kernels so that the single-view sweep, where the time goes, is not sized
 // by the registers of the exact-f64 prologue:
-//  * k_recip_prepare, one warp per (candidate, source): the direct cost and
-//    the exact-f64 source contrast, lane-parallel over the window taps with
-//    warp reductions (max/min are order-free, so the contrast gate stays
-//    exact).  A pair that passes parks its source pixel in its RecipObs slot
-//    with valid = kObsPending;
+//  * k_recip_prepare, one warp per candidate: its reference window once, then
+//    per source the direct cost and the exact-f64 source contrast,
+//    lane-parallel over the window taps with warp reductions (max/min are
+//    order-free, so the contrast gate stays exact).  A pair that passes parks
+//    its source pixel in its RecipObs slot with valid = kObsPending;
 //  * k_recip_sweep, one warp per pending pair, lanes over hypotheses:
 //    re-samples the source window (the same f64 taps, so the same f32
 //    values), sweeps every hypothesis and writes the final RecipObs.
@@ -1074,7 +1074,7 @@ __device__ __forceinline__ bool band_box(const float* A, const float* bv, float 
 }
 
 template <class T, int R, int COST>
-__global__ void __launch_bounds__(256) k_recip_prepare(BatchDev b, const Cand* __restrict__ cands,
+__global__ void __launch_bounds__(256, 3) k_recip_prepare(BatchDev b, const Cand* __restrict__ cands,
                                                        const uint32_t* __restrict__ count,
                                                        RecipObs* __restrict__ obs,
                                                        RefCounters* __restrict__ ctr,
@@ -1083,38 +1083,26 @@ __global__ void __launch_bounds__(256) k_recip_prepare(BatchDev b, const Cand* _
     constexpr int N = W * W;
     const uint32_t lane = lane_id();
     const uint32_t ms = (uint32_t)b.max_src;
-    const uint64_t items = (uint64_t)(*count) * ms;
-    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    const uint32_t n_cands = *count;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
     const DevProfile& prof = b.prof;
-    for (uint64_t item = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; item < items;
-         item += nwarps) {
-        const uint32_t ci = (uint32_t)(item / ms);
-        const int si = (int)(item - (uint64_t)ci * ms);
-        const uint64_t it = (uint64_t)ci * kMaxSources + si;
+    const float n = (float)N;
+    // a warp per candidate: the reference window (its re-projection, taps, mean
+    // and squared deviation) once, then its sources in order
+    for (uint32_t ci = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; ci < n_cands; ci += nwarps) {
         const Cand cd = cands[ci];
         const DevReference& ref = b.refs[cd.ref];
-        RecipObs res;
-        res.valid = 0;
-        res.pad = 0;
-        res.pos = D3{0, 0, 0};
-        bool ok = si < ref.n_src;
-        const DevSource& src = ref.src[ok ? si : 0];
-        D3 rp, sp;
-        if (ok) ok = project_exact(ref.cam, cd.pos, ref.img.width, ref.img.height, ref.focal, rp);
-        // direct cost of the reference window at (rp.x, rp.y), depth rp.z; lanes over taps
-        if (ok) {
-            const double inv = ddiv(1.0, rp.z);
-            float H[9];
-            plane_h(src.fwd_A, src.fwd_b, (float)inv, H);
-            const float zmin = zmin_of(inv);
+        D3 rp;
+        bool rok = project_exact(ref.cam, cd.pos, ref.img.width, ref.img.height, ref.focal, rp);
+        // the reference window at (rp.x, rp.y); taps beyond N are exact zeros in every sum
+        float dr[kTapRounds], vr = 0.f;
+        if (rok) {
             const T* rdata = static_cast<const T*>(ref.img.data);
-            const T* sdata = static_cast<const T*>(src.img.data);
-            float rv[kTapRounds], sv2[kTapRounds];
+            float rv[kTapRounds];
             bool tv = true;
 #pragma unroll
             for (int h = 0; h < kTapRounds; ++h) {
                 rv[h] = 0.f;
-                sv2[h] = 0.f;
                 const int t = lane + 32 * h;
                 if (t >= N) continue;
                 const float X = (float)rp.x + (float)(t % W - R);
@@ -1124,99 +1112,171 @@ __global__ void __launch_bounds__(256) k_recip_prepare(BatchDev b, const Cand* _
                     continue;
                 }
                 rv[h] = sample_fast<T>(rdata, ref.img.width, X, Y);
-                const float h2 = fmaf(H[6], X, fmaf(H[7], Y, H[8]));
-                if (!(h2 > zmin)) {
-                    tv = false;
-                    continue;
-                }
-                const float iv = __frcp_rn(h2);
-                const float u = fmaf(H[0], X, fmaf(H[1], Y, H[2])) * iv;
-                const float v = fmaf(H[3], X, fmaf(H[4], Y, H[5])) * iv;
-                if (!in_bounds_fast(u, v, src.img.width, src.img.height)) {
-                    tv = false;
-                    continue;
-                }
-                sv2[h] = sample_fast<T>(sdata, src.img.width, u, v);
             }
-            ok = __all_sync(0xffffffffu, tv);
-            if (ok) {
-                // taps beyond N contribute exact zeros to every sum
-                const float n = (float)N;
-                float sr = 0.f, ssv = 0.f;
+            rok = __all_sync(0xffffffffu, tv);
+            if (rok) {
+                float sr = 0.f;
 #pragma unroll
-                for (int h = 0; h < kTapRounds; ++h) {
-                    sr += rv[h];
-                    ssv += sv2[h];
-                }
+                for (int h = 0; h < kTapRounds; ++h) sr += rv[h];
                 const float mr = warp_sum(sr) / n;
-                const float mss = warp_sum(ssv) / n;
-                float dr[kTapRounds], ds[kTapRounds];
+                float r2 = 0.f;
 #pragma unroll
                 for (int h = 0; h < kTapRounds; ++h) {
-                    const bool in = lane + 32 * h < N;
-                    dr[h] = in ? rv[h] - mr : 0.f;
-                    ds[h] = in ? sv2[h] - mss : 0.f;
+                    dr[h] = lane + 32 * h < N ? rv[h] - mr : 0.f;
+                    r2 += dr[h] * dr[h];
                 }
-                float cost;
-                if (COST == 1) {
-                    float c = 0.f, r2 = 0.f, s2 = 0.f;
-#pragma unroll
-                    for (int h = 0; h < kTapRounds; ++h) {
-                        c += dr[h] * ds[h];
-                        r2 += dr[h] * dr[h];
-                        s2 += ds[h] * ds[h];
-                    }
-                    const float cov = warp_sum(c);
-                    const float vr = warp_sum(r2);
-                    const float vs = warp_sum(s2);
-                    if (!(vr > 0.f) || !(vs > 0.f) || vr / n < (float)prof.min_variance ||
-                        vs / n < (float)prof.min_variance)
-                        ok = false;
-                    cost = 1.0f - cov * rsqrtf(vr * vs);
-                } else {
-                    float a = 0.f;
-#pragma unroll
-                    for (int h = 0; h < kTapRounds; ++h) a += fabsf(dr[h] - ds[h]);
-                    cost = warp_sum(a) / n;
-                }
-                ok = ok && !((double)cost > prof.max_error);
+                if (COST == 1) vr = warp_sum(r2);
             }
         }
-        if (ok) ok = project_exact(src.cam, cd.pos, src.img.width, src.img.height, ref.focal, sp);
-        // exact patch_contrast of the source window at (sp.x, sp.y), lanes over taps
-        if (ok) {
-            double mn = kInf, mx = -kInf;
-            bool inb = true;
-#pragma unroll
-            for (int h = 0; h < kTapRounds; ++h) {
-                const int t = lane + 32 * h;
-                if (t >= N) continue;
-                double v;
-                if (!sample_exact<T>(src.img, dadd(sp.x, (double)(t % W - R)),
-                                     dadd(sp.y, (double)(t / W - R)), v)) {
-                    inb = false;
-                    continue;
-                }
-                mn = fmin(mn, v);
-                mx = fmax(mx, v);
-            }
-            ok = __all_sync(0xffffffffu, inb);
+        const double inv = rok ? ddiv(1.0, rp.z) : 0.0;
+        const float zmin = zmin_of(inv);
+        unsigned long long evals = 0;
+        for (uint32_t si = 0; si < ms; ++si) {
+            const uint64_t item = (uint64_t)ci * ms + si;
+            const uint64_t it = (uint64_t)ci * kMaxSources + si;
+            RecipObs res;
+            res.valid = 0;
+            res.pad = 0;
+            res.pos = D3{0, 0, 0};
+            bool ok = rok && (int)si < ref.n_src;
+            const DevSource& src = ref.src[(int)si < ref.n_src ? si : 0];
+            D3 sp;
+            // direct cost of the reference window at depth rp.z in this source; lanes over taps
             if (ok) {
+                float H[9];
+                plane_h(src.fwd_A, src.fwd_b, (float)inv, H);
+                const T* sdata = static_cast<const T*>(src.img.data);
+                float sv2[kTapRounds];
+                bool tv = true;
 #pragma unroll
-                for (int o = 16; o > 0; o >>= 1) {
-                    mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
-                    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+                for (int h = 0; h < kTapRounds; ++h) {
+                    sv2[h] = 0.f;
+                    const int t = lane + 32 * h;
+                    if (t >= N) continue;
+                    const float X = (float)rp.x + (float)(t % W - R);
+                    const float Y = (float)rp.y + (float)(t / W - R);
+                    const float h2 = fmaf(H[6], X, fmaf(H[7], Y, H[8]));
+                    if (!(h2 > zmin)) {
+                        tv = false;
+                        continue;
+                    }
+                    const float iv = __frcp_rn(h2);
+                    const float u = fmaf(H[0], X, fmaf(H[1], Y, H[2])) * iv;
+                    const float v = fmaf(H[3], X, fmaf(H[4], Y, H[5])) * iv;
+                    if (!in_bounds_fast(u, v, src.img.width, src.img.height)) {
+                        tv = false;
+                        continue;
+                    }
+                    sv2[h] = sample_fast<T>(sdata, src.img.width, u, v);
                 }
-                ok = !(dsub(mx, mn) < prof.min_contrast);
+                ok = __all_sync(0xffffffffu, tv);
+                if (ok) {
+                    float ssv = 0.f;
+#pragma unroll
+                    for (int h = 0; h < kTapRounds; ++h) ssv += sv2[h];
+                    const float mss = warp_sum(ssv) / n;
+                    float ds[kTapRounds];
+#pragma unroll
+                    for (int h = 0; h < kTapRounds; ++h) ds[h] = lane + 32 * h < N ? sv2[h] - mss : 0.f;
+                    float cost;
+                    if (COST == 1) {
+                        float c = 0.f, s2 = 0.f;
+#pragma unroll
+                        for (int h = 0; h < kTapRounds; ++h) {
+                            c += dr[h] * ds[h];
+                            s2 += ds[h] * ds[h];
+                        }
+                        const float cov = warp_sum(c);
+                        const float vs = warp_sum(s2);
+                        if (!(vr > 0.f) || !(vs > 0.f) || vr / n < (float)prof.min_variance ||
+                            vs / n < (float)prof.min_variance)
+                            ok = false;
+                        cost = 1.0f - cov * rsqrtf(vr * vs);
+                    } else {
+                        float a = 0.f;
+#pragma unroll
+                        for (int h = 0; h < kTapRounds; ++h) a += fabsf(dr[h] - ds[h]);
+                        cost = warp_sum(a) / n;
+                    }
+                    ok = ok && !((double)cost > prof.max_error);
+                }
             }
+            if (ok) ok = project_exact(src.cam, cd.pos, src.img.width, src.img.height, ref.focal, sp);
+            // patch_contrast of the source window at (sp.x, sp.y), lanes over taps:
+            // first in f32 on the exact texels and fractions of the f64 taps, whose
+            // error is below M 2^-19 (M the largest texel magnitude read); the
+            // exact f64 contrast decides when that leaves the gate open
+            if (ok) {
+                const T* sdata = static_cast<const T*>(src.img.data);
+                const uint32_t sw = src.img.width;
+                float mnf = 3.0e38f, mxf = -3.0e38f, mag = 0.f;
+                bool inb = true;
+#pragma unroll
+                for (int h = 0; h < kTapRounds; ++h) {
+                    const int t = lane + 32 * h;
+                    if (t >= N) continue;
+                    const double x = dadd(sp.x, (double)(t % W - R)), y = dadd(sp.y, (double)(t / W - R));
+                    if (!in_bilinear_bounds(x, y, sw, src.img.height)) {
+                        inb = false;
+                        continue;
+                    }
+                    const uint32_t x0 = (uint32_t)floor(x), y0 = (uint32_t)floor(y);
+                    const float tx = (float)dsub(x, (double)x0), ty = (float)dsub(y, (double)y0);
+                    const size_t r0 = (size_t)y0 * sw + x0;
+                    const float v00 = pix<T>(sdata, r0), v10 = pix<T>(sdata, r0 + 1);
+                    const float v01 = pix<T>(sdata, r0 + sw), v11 = pix<T>(sdata, r0 + sw + 1);
+                    const float top = fmaf(v10 - v00, tx, v00);
+                    const float bot = fmaf(v11 - v01, tx, v01);
+                    const float v = fmaf(bot - top, ty, top);
+                    mnf = fminf(mnf, v);
+                    mxf = fmaxf(mxf, v);
+                    mag = fmaxf(mag, fmaxf(fmaxf(fabsf(v00), fabsf(v10)), fmaxf(fabsf(v01), fabsf(v11))));
+                }
+                ok = __all_sync(0xffffffffu, inb);
+                if (ok) {
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) {
+                        mnf = fminf(mnf, __shfl_xor_sync(0xffffffffu, mnf, o));
+                        mxf = fmaxf(mxf, __shfl_xor_sync(0xffffffffu, mxf, o));
+                        mag = fmaxf(mag, __shfl_xor_sync(0xffffffffu, mag, o));
+                    }
+                    const double c = (double)mxf - (double)mnf;
+                    const double eps = (double)mag * 1.52587890625e-05;  // 2^-16: 8 x the bound
+                    if (c >= prof.min_contrast + eps) {
+                        ok = true;
+                    } else if (c < prof.min_contrast - eps) {
+                        ok = false;
+                    } else {
+                        // exact patch_contrast near the gate
+                        double mn = kInf, mx = -kInf;
+#pragma unroll
+                        for (int h = 0; h < kTapRounds; ++h) {
+                            const int t = lane + 32 * h;
+                            if (t >= N) continue;
+                            double v = 0.0;
+                            sample_exact<T>(src.img, dadd(sp.x, (double)(t % W - R)),
+                                            dadd(sp.y, (double)(t / W - R)), v);
+                            mn = fmin(mn, v);
+                            mx = fmax(mx, v);
+                        }
+#pragma unroll
+                        for (int o = 16; o > 0; o >>= 1) {
+                            mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+                            mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+                        }
+                        ok = !(dsub(mx, mn) < prof.min_contrast);
+                    }
+                }
+            }
+            if (ok) {
+                res.pos = sp;
+                res.valid = kObsPending;
+                evals += (unsigned long long)ref.planes;
+            }
+            if (lane == 0 && (int)si < ref.n_src) obs[it] = res;
+            if (lane == 0) pending[item] = ok ? 1 : 0;
         }
-        if (ok) {
-            res.pos = sp;
-            res.valid = kObsPending;
-            if (lane == 0) atomicAdd(&ctr[cd.ref].recip_evals, (unsigned long long)ref.planes);
-        }
-        if (lane == 0 && si < ref.n_src) obs[it] = res;
-        if (lane == 0) pending[item] = ok ? 1 : 0;
+        if (lane == 0 && evals) atomicAdd(&ctr[cd.ref].recip_evals, evals);
     }
 }
 
