@@ -359,7 +359,7 @@ __host__ __device__ constexpr int tiled_steps(int np) { return (np + 2 * kTileTh
 // row ends.  When the footprint's image in a source lies inside that image
 // (tested once per plane and source on the rectangle's corners), the step
 // skips the per-sample domain tests.
-template <class T, int R, class Acc, int TX>
+template <class T, int R, class Acc, int TX, int S>
 __global__ void __launch_bounds__(kTileThreads, 1024 / kTileThreads) k_sweep_tiled(BatchDev b, uint64_t total_sites,
                                                      SiteRank* __restrict__ rank,
                                                      uint8_t* __restrict__ status,
@@ -378,7 +378,10 @@ __global__ void __launch_bounds__(kTileThreads, 1024 / kTileThreads) k_sweep_til
     if (gx0 >= ref.nx || gy0 >= ref.ny) return;
     const int per_chunk = (ref.planes + n_chunks - 1) / n_chunks;
     const int k0 = chunk * per_chunk, k1 = min(ref.planes, k0 + per_chunk);
-    const int s = (int)ref.stride;
+    // S, when not 0, is the batch's grid stride at compile time (the tiled sweep
+    // runs batches of one stride), so the footprint's shape and every tap
+    // offset of the box filters fold into constants
+    const int s = S ? S : (int)ref.stride;
     const int PX = (TX - 1) * s + W, PY = (TY - 1) * s + W;
     const int PXs = (PX + s - 1) / s, PXp = PXs * s;  // columns per residue, padded row
     const int np = PY * PXp;
@@ -1640,17 +1643,19 @@ cudaError_t Typed<T>::sweep_tiled(const BatchDev& b, uint32_t max_nx, uint32_t m
         V3D_COUNTED kern<<<grid, kTileThreads, smem, st>>>(b, total_sites, rank, status, ctr, n, chunks.partial);
         return cudaGetLastError();
     };
+    // stride 2 (every ZNCC configuration of the benchmarks) has its own instantiation
+    auto pick = [&](auto k2, auto k0, int W) { return stride == 2 ? run(k2, W) : run(k0, W); };
     auto by_acc = [&](auto tx_tag) -> cudaError_t {
         constexpr int X = decltype(tx_tag)::value;
         switch (b.prof.radius * 2 + (b.sums32 ? 1 : 0)) {
-            case 2: return run(k_sweep_tiled<T, 1, double, X>, 3);
-            case 4: return run(k_sweep_tiled<T, 2, double, X>, 5);
-            case 6: return run(k_sweep_tiled<T, 3, double, X>, 7);
-            case 8: return run(k_sweep_tiled<T, 4, double, X>, 9);
-            case 3: return run(k_sweep_tiled<T, 1, float, X>, 3);
-            case 5: return run(k_sweep_tiled<T, 2, float, X>, 5);
-            case 7: return run(k_sweep_tiled<T, 3, float, X>, 7);
-            case 9: return run(k_sweep_tiled<T, 4, float, X>, 9);
+            case 2: return pick(k_sweep_tiled<T, 1, double, X, 2>, k_sweep_tiled<T, 1, double, X, 0>, 3);
+            case 4: return pick(k_sweep_tiled<T, 2, double, X, 2>, k_sweep_tiled<T, 2, double, X, 0>, 5);
+            case 6: return pick(k_sweep_tiled<T, 3, double, X, 2>, k_sweep_tiled<T, 3, double, X, 0>, 7);
+            case 8: return pick(k_sweep_tiled<T, 4, double, X, 2>, k_sweep_tiled<T, 4, double, X, 0>, 9);
+            case 3: return pick(k_sweep_tiled<T, 1, float, X, 2>, k_sweep_tiled<T, 1, float, X, 0>, 3);
+            case 5: return pick(k_sweep_tiled<T, 2, float, X, 2>, k_sweep_tiled<T, 2, float, X, 0>, 5);
+            case 7: return pick(k_sweep_tiled<T, 3, float, X, 2>, k_sweep_tiled<T, 3, float, X, 0>, 7);
+            case 9: return pick(k_sweep_tiled<T, 4, float, X, 2>, k_sweep_tiled<T, 4, float, X, 0>, 9);
         }
         return cudaErrorInvalidValue;
     };
