@@ -1384,13 +1384,19 @@ __global__ void __launch_bounds__(RecipBounds<MODE>::kThreads, RecipBounds<MODE>
         }
         if (banded) {
             // entry c: texel c of the row and texel c + 1 minus texel c; the last
-            // column is read only as a right neighbour
-            for (int rr = 0; rr < rows; ++rr) {
-                const T* row = rimg + (size_t)(by0 + rr) * rw + bx0;
-                for (int c = lane; c < cols - 1; c += 32) {
-                    const float t0 = pix<T>(row, c), t1 = pix<T>(row, c + 1);
-                    band[rr * kBandPitch + c] = f2(t0, t1 - t0);
-                }
+            // column is read only as a right neighbour.  The lanes run over the
+            // flat rows x (cols - 1) entries; the row of entry e is
+            // floor((e + 1/2) / (cols - 1)), exact in f32 since e < 2^11 and the
+            // fraction lies at least 1/128 from an integer
+            const int c1 = cols - 1;
+            const float inv_c1 = 1.0f / (float)c1;
+            const T* base = rimg + (size_t)by0 * rw + bx0;
+            for (int e = lane; e < rows * c1; e += 32) {
+                const int rr = (int)(((float)e + 0.5f) * inv_c1);
+                const int c = e - rr * c1;
+                const T* row = base + (size_t)rr * rw;
+                const float t0 = pix<T>(row, c), t1 = pix<T>(row, c + 1);
+                band[rr * kBandPitch + c] = f2(t0, t1 - t0);
             }
         }
         __syncwarp();
