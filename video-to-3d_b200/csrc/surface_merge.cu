@@ -1805,139 +1805,240 @@ std::vector<v3d_mesh_triangle> stitch_trimmed_seams(const StitchInputs& si, Tall
     };
     auto length = [&](uint64_t a, uint64_t b) { return mg::norm3(in.position(a) - in.position(b)); };
     Grid3 stitch_grid(si.cell);
-    std::vector<uint32_t> slots_v, cover_v, nearby;
-    auto check = [&](const uint64_t corners[3], uint32_t slot, uint32_t adjacent, double lo[3],
-                     double hi[3]) -> bool {
+    // A stitch check (surface_merge_stitch.rs:253-297) in the reference's order
+    // reads edge usage, then only inputs of this pass (geometry, the seams'
+    // cover, the kept triangles), then the stitches made so far.  The part that
+    // reads only inputs is evaluated for every boundary edge concurrently (in
+    // candidate order, up to the first candidate it passes); the ordered pass
+    // then replays each check: usage, the recorded outcome and lookup tally, and
+    // for a recorded pass the lookup among earlier stitches, whose overlap adds
+    // onto the recorded sum in the same order.  Stitches only add usage and
+    // overlap, so the outcome and the tallies are the reference's.
+    struct Static {
+        uint8_t stage = 0;  // 0 failed before the kept-triangle lookup, 1 failed at or after it, 2 passed
+        Limit q = Limit::None;
+        size_t used = 0;
+        uint32_t footprint = 0;
+        double area = 0.0, overlap = 0.0;
+        double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+        Poly2 polygon;
+    };
+    struct Scratch {
+        std::vector<uint32_t> cover_v, nearby;
+    };
+    auto check_static = [&](const uint64_t corners[3], uint32_t slot, uint32_t adjacent, Scratch& sc,
+                            Static& st) {
         const uint64_t a = corners[0], b = corners[1], c = corners[2];
-        const uint64_t es[3][2] = {{a, b}, {b, c}, {c, a}};
-        for (const auto& e : es) {
-            uint32_t count, from;
-            if (usage((uint32_t)e[0], (uint32_t)e[1], count, from) &&
-                !(count < 2 && from != (uint32_t)e[0]))
-                return false;
-        }
         const V3 cs[3] = {in.position(a), in.position(b), in.position(c)};
         Geometry surface;
-        if (!make_geometry(cs, surface)) return false;
+        if (!make_geometry(cs, surface)) return;
         const Removal& r = removals[slot];
         const Footprint& f = fps[r.footprint];
         const int64_t lower = patch_of[r.triangle];
         PT projected;
-        if (!mg::project_triangle(f.cam, surface.c, projected)) return false;
+        if (!mg::project_triangle(f.cam, surface.c, projected)) return;
         double area = mg::signed_image_area(projected);
-        if (!has_geometry[adjacent]) return false;
+        if (!has_geometry[adjacent]) return;
         PT adj;
-        if (!mg::project_triangle(f.cam, geometry[adjacent].c, adj)) return false;
+        if (!mg::project_triangle(f.cam, geometry[adjacent].c, adj)) return;
         const double adjacent_area = mg::signed_image_area(adj);
         if (std::fabs(area) <= mg::kF64Eps * mg::kF64Eps ||
             mg::signum(adjacent_area) != mg::signum(area))
-            return false;
+            return;
         area = std::fabs(area);
         for (int i = 0; i < 3; ++i)
             if (in.group(corners[i]) != lower) projected.z[i] *= r.scale;
+        auto& cover_v = sc.cover_v;
         cover_v.clear();
         for (int i = 0; i < 3; ++i) seams_of(corners[i], cover_v);
         std::sort(cover_v.begin(), cover_v.end());
         cover_v.erase(std::unique(cover_v.begin(), cover_v.end()), cover_v.end());
         std::vector<PT> cover;
-        for (uint32_t s : cover_v) {
-            if (!seams[s].ok || removals[s].footprint != r.footprint || patch_of[removals[s].triangle] != lower)
+        for (uint32_t s2 : cover_v) {
+            if (!seams[s2].ok || removals[s2].footprint != r.footprint || patch_of[removals[s2].triangle] != lower)
                 continue;
-            const Removal& rs = removals[s];
+            const Removal& rs = removals[s2];
             if (rs.footprint >= fps.size() || !has_geometry[rs.triangle]) continue;
-            PT p;
-            if (fps[rs.footprint].project_candidate(geometry[rs.triangle], p)) cover.push_back(p);
+            PT pp;
+            if (fps[rs.footprint].project_candidate(geometry[rs.triangle], pp)) cover.push_back(pp);
         }
         double unobserved;
-        if (!unobserved_area(projected, cover, unobserved)) return false;
-        if (unobserved > kMaxUnobservedStitchShare * area) return false;
-        const Poly2 polygon{projected.p(0), projected.p(1), projected.p(2)};
-        surface.aabb(si.tolerance, lo, hi);
+        if (!unobserved_area(projected, cover, unobserved)) return;
+        if (unobserved > kMaxUnobservedStitchShare * area) return;
+        st.polygon = Poly2{projected.p(0), projected.p(1), projected.p(2)};
+        surface.aabb(si.tolerance, st.lo, st.hi);
+        auto& nearby = sc.nearby;
         nearby.clear();
         Budget budget;
-        Limit q = si.kept_grid->query(lo, hi, kMaxGridCells, budget, nearby);
+        Limit q = si.kept_grid->query(st.lo, st.hi, kMaxGridCells, budget, nearby);
         if (q == Limit::Cells) q = budget.take(si.all_kept->data(), si.all_kept->size(), nearby);
-        tally.record(budget.used, q);
-        if (q != Limit::None) return false;
+        st.stage = 1;
+        st.used = budget.used;
+        st.q = q;
+        if (q != Limit::None) return;
         std::sort(nearby.begin(), nearby.end());
         double overlap = 0.0;
         for (uint32_t other : nearby) {
             if (!has_geometry[other]) continue;
-            PT p;
-            if (!mg::project_triangle(f.cam, geometry[other].c, p)) return false;
-            overlap += intersection_area(polygon, p);
+            PT pp;
+            if (!mg::project_triangle(f.cam, geometry[other].c, pp)) return;
+            overlap += intersection_area(st.polygon, pp);
         }
-        nearby.clear();
-        Budget budget2;
-        q = stitch_grid.query(lo, hi, kMaxGridCells, budget2, nearby);
-        tally.record(budget2.used, q);
-        if (q != Limit::None) return false;
-        std::sort(nearby.begin(), nearby.end());
-        for (uint32_t other : nearby) {
-            const v3d_mesh_triangle& o = output[other];
-            const V3 oc[3] = {in.position(o.a), in.position(o.b), in.position(o.c)};
-            PT p;
-            if (!mg::project_triangle(f.cam, oc, p)) return false;
-            overlap += intersection_area(polygon, p);
-        }
-        return overlap <= kMaxStitchOverlapShare * area;
+        st.stage = 2;
+        st.footprint = (uint32_t)r.footprint;
+        st.area = area;
+        st.overlap = overlap;
     };
     struct Cand {
         double perimeter;
         std::array<uint64_t, 4> c;
     };
-    std::vector<Cand> candidates;
-    for (uint32_t edge_index : boundary) {
-        if (output.size() >= removals.size()) break;
-        const HalfEdge edge = retained[edge_index];
-        const uint32_t adjacent = edge.triangle;
-        const uint64_t from = edge.from;
-        const uint64_t to = edge.from == edge.low ? edge.high : edge.low;
-        if (in.group(from) != in.group(to)) continue;
-        slots_v.clear();
-        seams_of(from, slots_v);
-        seams_of(to, slots_v);
-        std::sort(slots_v.begin(), slots_v.end());
-        slots_v.erase(std::unique(slots_v.begin(), slots_v.end()), slots_v.end());
-        std::set<uint64_t> seen;
-        candidates.clear();
-        for (uint32_t slot : slots_v) {
-            if (!seams[slot].ok) continue;
-            const int64_t lower = patch_of[removals[slot].triangle];
-            const bool edge_is_lower = in.group(from) == lower;
-            for (uint8_t i = 0; i < seams[slot].len; ++i) {
-                const uint64_t vertex = seams[slot].v[i];
-                if (vertex == from || vertex == to || (in.group(vertex) == lower) == edge_is_lower)
+    // the boundary edges' candidates in the reference's order, and the static
+    // checks up to the first pass, per thread over contiguous edge ranges
+    struct Part {
+        std::vector<uint32_t> start;  // per edge of the range: first candidate (+1 end entry)
+        std::vector<uint8_t> stitchable;
+        std::vector<Cand> cands;
+        std::vector<Static> checked;  // per candidate; stage 255 = not evaluated
+    };
+    const size_t n_edges = boundary.size();
+    const size_t n_threads = std::max<size_t>(1, std::min<size_t>(std::thread::hardware_concurrency(), 16));
+    const size_t chunk = (n_edges + n_threads - 1) / n_threads;
+    std::vector<Part> parts(n_threads);
+    auto build = [&](size_t k) {
+        Part& part = parts[k];
+        const size_t lo = std::min(n_edges, k * chunk), hi = std::min(n_edges, lo + chunk);
+        Scratch sc;
+        std::vector<uint32_t> slots;
+        std::vector<Cand> candidates;
+        part.start.reserve(hi - lo + 1);
+        for (size_t ei = lo; ei < hi; ++ei) {
+            part.start.push_back((uint32_t)part.cands.size());
+            const HalfEdge edge = retained[boundary[ei]];
+            const uint64_t from = edge.from;
+            const uint64_t to = edge.from == edge.low ? edge.high : edge.low;
+            if (in.group(from) != in.group(to)) {
+                part.stitchable.push_back(0);
+                continue;
+            }
+            part.stitchable.push_back(1);
+            slots.clear();
+            seams_of(from, slots);
+            seams_of(to, slots);
+            std::sort(slots.begin(), slots.end());
+            slots.erase(std::unique(slots.begin(), slots.end()), slots.end());
+            std::set<uint64_t> seen;
+            candidates.clear();
+            for (uint32_t slot : slots) {
+                if (!seams[slot].ok) continue;
+                const int64_t lower = patch_of[removals[slot].triangle];
+                const bool edge_is_lower = in.group(from) == lower;
+                for (uint8_t i = 0; i < seams[slot].len; ++i) {
+                    const uint64_t vertex = seams[slot].v[i];
+                    if (vertex == from || vertex == to || (in.group(vertex) == lower) == edge_is_lower)
+                        continue;
+                    if (!seen.insert(vertex).second) continue;
+                    const double perimeter = (length(from, to) + length(to, vertex)) + length(vertex, from);
+                    candidates.push_back({perimeter, {to, from, vertex, slot}});
+                }
+            }
+            std::stable_sort(candidates.begin(), candidates.end(), [](const Cand& l, const Cand& r) {
+                if (total_less(l.perimeter, r.perimeter)) return true;
+                if (total_less(r.perimeter, l.perimeter)) return false;
+                return l.c < r.c;
+            });
+            bool passed = false;
+            for (const Cand& cd : candidates) {
+                part.cands.push_back(cd);
+                part.checked.emplace_back();
+                Static& st = part.checked.back();
+                if (passed) {
+                    st.stage = 255;
                     continue;
-                if (!seen.insert(vertex).second) continue;
-                const double perimeter = (length(from, to) + length(to, vertex)) + length(vertex, from);
-                candidates.push_back({perimeter, {to, from, vertex, slot}});
+                }
+                const uint64_t corners[3] = {cd.c[0], cd.c[1], cd.c[2]};
+                check_static(corners, (uint32_t)cd.c[3], edge.triangle, sc, st);
+                passed = st.stage == 2;
             }
         }
-        std::stable_sort(candidates.begin(), candidates.end(), [](const Cand& l, const Cand& r) {
-            if (total_less(l.perimeter, r.perimeter)) return true;
-            if (total_less(r.perimeter, l.perimeter)) return false;
-            return l.c < r.c;
-        });
-        for (const Cand& cd : candidates) {
-            const uint64_t corners[3] = {cd.c[0], cd.c[1], cd.c[2]};
-            double lo[3], hi[3];
-            if (!check(corners, (uint32_t)cd.c[3], adjacent, lo, hi)) continue;
-            const uint64_t es[3][2] = {{corners[0], corners[1]}, {corners[1], corners[2]},
-                                       {corners[2], corners[0]}};
-            for (const auto& e : es) {
-                uint32_t count, from_;
-                const uint32_t f0 = (uint32_t)e[0], t0 = (uint32_t)e[1];
-                const bool had = usage(f0, t0, count, from_);
-                const uint32_t lo32 = std::min(f0, t0), hi32 = std::max(f0, t0);
-                stitched[((uint64_t)lo32 << 32) | hi32] = had ? std::make_pair(count + 1, from_)
-                                                              : std::make_pair(1u, f0);
+        part.start.push_back((uint32_t)part.cands.size());
+    };
+    {
+        std::vector<std::thread> pool;
+        for (size_t k = 1; k < n_threads; ++k) pool.emplace_back(build, k);
+        build(0);
+        for (auto& th : pool) th.join();
+    }
+    Scratch sc;
+    std::vector<uint32_t> nearby;
+    bool full = false;
+    for (size_t k = 0; k < n_threads && !full; ++k) {
+        Part& part = parts[k];
+        const size_t lo = std::min(n_edges, k * chunk), hi = std::min(n_edges, lo + chunk);
+        for (size_t ei = lo; ei < hi; ++ei) {
+            if (output.size() >= removals.size()) {
+                full = true;
+                break;
             }
-            stitch_grid.insert((uint32_t)output.size(), lo, hi);
-            output.push_back(v3d_mesh_triangle{corners[0], corners[1], corners[2],
-                                               std::fmin(tris[adjacent].confidence,
-                                                         tris[removals[cd.c[3]].triangle].confidence)});
-            break;
+            const size_t e = ei - lo;
+            if (!part.stitchable[e]) continue;
+            const uint32_t adjacent = retained[boundary[ei]].triangle;
+            for (uint32_t j = part.start[e]; j < part.start[e + 1]; ++j) {
+                const Cand& cd = part.cands[j];
+                const uint64_t corners[3] = {cd.c[0], cd.c[1], cd.c[2]};
+                const uint64_t es[3][2] = {{corners[0], corners[1]}, {corners[1], corners[2]},
+                                           {corners[2], corners[0]}};
+                bool ok = true;
+                for (const auto& ed : es) {
+                    uint32_t count, from_;
+                    if (usage((uint32_t)ed[0], (uint32_t)ed[1], count, from_) &&
+                        !(count < 2 && from_ != (uint32_t)ed[0])) {
+                        ok = false;
+                        break;
+                    }
+                }
+                if (!ok) continue;
+                Static& st = part.checked[j];
+                if (st.stage == 255) {
+                    st = Static{};
+                    check_static(corners, (uint32_t)cd.c[3], adjacent, sc, st);
+                }
+                if (st.stage == 0) continue;
+                tally.record(st.used, st.q);
+                if (st.stage == 1) continue;
+                nearby.clear();
+                Budget budget2;
+                const Limit q = stitch_grid.query(st.lo, st.hi, kMaxGridCells, budget2, nearby);
+                tally.record(budget2.used, q);
+                if (q != Limit::None) continue;
+                std::sort(nearby.begin(), nearby.end());
+                const Footprint& f = fps[st.footprint];
+                double overlap = st.overlap;
+                for (uint32_t other : nearby) {
+                    const v3d_mesh_triangle& o = output[other];
+                    const V3 oc[3] = {in.position(o.a), in.position(o.b), in.position(o.c)};
+                    PT pp;
+                    if (!mg::project_triangle(f.cam, oc, pp)) {
+                        ok = false;
+                        break;
+                    }
+                    overlap += intersection_area(st.polygon, pp);
+                }
+                if (!ok || !(overlap <= kMaxStitchOverlapShare * st.area)) continue;
+                for (const auto& ed : es) {
+                    uint32_t count, from_;
+                    const uint32_t f0 = (uint32_t)ed[0], t1 = (uint32_t)ed[1];
+                    const bool had = usage(f0, t1, count, from_);
+                    const uint32_t lo32 = std::min(f0, t1), hi32 = std::max(f0, t1);
+                    stitched[((uint64_t)lo32 << 32) | hi32] = had ? std::make_pair(count + 1, from_)
+                                                                  : std::make_pair(1u, f0);
+                }
+                stitch_grid.insert((uint32_t)output.size(), st.lo, st.hi);
+                output.push_back(v3d_mesh_triangle{corners[0], corners[1], corners[2],
+                                                   std::fmin(tris[adjacent].confidence,
+                                                             tris[removals[cd.c[3]].triangle].confidence)});
+                break;
+            }
         }
     }
     si.stage_ms[2] += ms_since(t0);
