@@ -525,6 +525,16 @@ __global__ void __launch_bounds__(kTileThreads, 1024 / kTileThreads) k_sweep_til
     }
     const float sr_shift = (float)(sr - n * (double)shift);
     const float inv_nf = 1.0f / (float)N, minvar_nf = (float)minvar_n;
+    // the reference taps of this thread's first horizontal window, the same
+    // for every plane and source (the stride-2 instantiation has the registers)
+    float rreg[W];
+    if (S) {
+        const int i = tid < PY * TX ? tid : 0;
+        const int yy = TX == 16 ? rowmap[i / TX] : i / TX;
+        const float* rp = refv + yy * PXp + i % TX;
+#pragma unroll
+        for (int dx = 0; dx < W; ++dx) rreg[dx] = rp[toff[dx]];
+    }
     Rank st = rank_empty();
     for (int k = k0; k < k1; ++k) {
         const float inv = pinv[k];
@@ -579,7 +589,8 @@ __global__ void __launch_bounds__(kTileThreads, 1024 / kTileThreads) k_sweep_til
             __syncthreads();
             // horizontal box filter: the window of column c of row yy at slot c,
             // TX windows a row (a warp takes one row of 32, or two rows of 16)
-            for (int i = tid; i < PY * TX; i += kTileThreads) {
+            // (a thread's first window takes its reference taps from registers)
+            auto hwindow = [&](int i, const float* rtap) {
                 const int c = i % TX;
                 const int yy = TX == 16 ? rowmap[i / TX] : i / TX;
                 const int o = yy * TX + c;
@@ -593,7 +604,7 @@ __global__ void __launch_bounds__(kTileThreads, 1024 / kTileThreads) k_sweep_til
                     for (int dx = 0; dx < W; ++dx) {
                         const float v = sp[toff[dx]] - shift;
                         ab = __ffma2_rn(f2(v, v), f2(1.0f, v), ab);
-                        c = fmaf(rp[toff[dx]] - shift, v, c);
+                        c = fmaf((rtap ? rtap[dx] : rp[toff[dx]]) - shift, v, c);
                     }
                     hs[o] = (Acc)ab.x;
                     hss[o] = (Acc)ab.y;
@@ -605,13 +616,15 @@ __global__ void __launch_bounds__(kTileThreads, 1024 / kTileThreads) k_sweep_til
                         const double v = (double)sp[toff[dx]];
                         a += v;
                         bb = fma(v, v, bb);
-                        c = fma((double)rp[toff[dx]], v, c);
+                        c = fma((double)(rtap ? rtap[dx] : rp[toff[dx]]), v, c);
                     }
                     hs[o] = (Acc)a;
                     hss[o] = (Acc)bb;
                     hrs[o] = (Acc)c;
                 }
-            }
+            };
+            if (tid < PY * TX) hwindow(tid, S ? rreg : nullptr);
+            for (int i = tid + kTileThreads; i < PY * TX; i += kTileThreads) hwindow(i, nullptr);
             __syncthreads();
             if (sampled) {
                 float cost = __int_as_float(0x7fc00000);
