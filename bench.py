@@ -42,13 +42,13 @@ from tests.attribution import COST_TOLERANCE  # noqa: E402
 UNIT = "samples·planes·views/s"
 WIDTH, HEIGHT, FRAMES = 640, 360, 120
 RADIUS, PLANES, SOURCES, STRIDE = 3, 128, 8, 2
-# DRAM bytes per launch unit of the two large kernels, from ncu captures of the
-# same workload cut to 12 keyframes (profiles/k_sweep_tiled_zncc7x7_640x360_12kf.md,
-# profiles/k_recip_sweep_zncc7x7_640x360_12kf.md): the depth sweep read 11.15 MB
-# and wrote 0.01 MB for 677.4 M window evaluations; the reciprocal sweep read
-# 193.4 MB and wrote 70.1 MB for the pairs of 1 reciprocal launch.  A clip's frames
-# live in L2, so DRAM traffic grows with the work.
-SWEEP_DRAM_BYTES_PER_UNIT = (11.151360e6 + 0.008192e6) / 677.376e6
+# DRAM bytes per launch unit of the depth sweep, from the ncu capture of the same
+# workload cut to 12 keyframes (profiles/k_sweep_tiled_zncc7x7_640x360_12kf.md):
+# 12.59 MB read and 4.96 MB written (the plane chunks' partial rank states) for
+# 677.4 M window evaluations.  A clip's frames live in L2, so DRAM traffic grows
+# with the work; the reciprocal sweep's (86.2 MB read, 10.3 MB written by its
+# captured launch) is in its profile.
+SWEEP_DRAM_BYTES_PER_UNIT = (12.587776e6 + 4.957696e6) / 677.376e6
 ARITH = {"f32": "f32", "f16": "f16 storage, f32 arithmetic",
          "bf16": "bf16 storage, f32 arithmetic"}
 
@@ -121,31 +121,40 @@ def kernel_rooflines(info, units, b, sweep_ms, recip_sweep_ms, recip_prep_ms, hb
     must read, counted as unique texels:
       k_sweep_tiled   per (tile, hypothesis, source) the source texels under the
                       warped footprint of the tile's windows, (PX+1)(PY+1) of them
-                      (PX = 31*stride + W, PY = 7*stride + W), plus the reference
-                      footprint PX*PY once per tile;
+                      (PX = (TX-1)*stride + W, PY = (TY-1)*stride + W for the TX x TY
+                      tile the sweep ran), plus the reference footprint PX*PY once
+                      per tile;
       k_recip_sweep   per (pending pair, hypothesis) the reference texels under the
                       warped window, (W+1)^2;
       k_recip_prepare per (candidate, source) the reference and source texels of the
                       direct cost and the source window of the contrast gate,
                       3 (W+1)^2.
-    All three are bound by SM instruction issue with their gathers served from L1
-    and L2 (the profiles under profiles/ give issue-active and L1 figures), so the
-    fraction of the HBM roofline is the share of memory bandwidth the kernel's
-    compulsory reads would need at its achieved rate."""
+    None of them is bound by HBM (their reads are served from L1, L2 and shared
+    memory; the profiles under profiles/ give the binding units), so the fraction
+    of the HBM roofline is the share of memory bandwidth the kernel's compulsory
+    reads would need at its achieved rate."""
     W = 2 * RADIUS + 1
-    PX, PY = 31 * STRIDE + W, 7 * STRIDE + W
+    TX = int(info.get("sweep_tile_x", 32)) or 32
+    TY = 256 // TX
+    PX, PY = (TX - 1) * STRIDE + W, (TY - 1) * STRIDE + W
     nx = (WIDTH - 2 * (RADIUS + 2) + STRIDE - 1) // STRIDE
     ny = (HEIGHT - 2 * (RADIUS + 2) + STRIDE - 1) // STRIDE
     sites = nx * ny
-    tiles = ((nx + 31) // 32) * ((ny + 7) // 8)
+    tiles = ((nx + TX - 1) // TX) * ((ny + TY - 1) // TY)
     refs = units / float(sites * PLANES * SOURCES)
     sweep_bytes = refs * tiles * (PLANES * SOURCES * (PX + 1) * (PY + 1) + PX * PY) * b
     recip_bytes = info["reciprocal_plane_evaluations"] * (W + 1) ** 2 * b
     prep_bytes = info["candidates"] * SOURCES * 3 * (W + 1) ** 2 * b
     out = {}
+    bound = {"k_sweep_tiled": "the shared-memory data path of its f64 box filters (83 % of the L1 "
+                              "wavefront peak in profiles/k_sweep_tiled_zncc7x7_640x360_12kf.md)",
+             "k_recip_sweep": "instruction issue and the FMA pipe, its texels staged in shared memory "
+                              "(profiles/k_recip_sweep_zncc7x7_640x360_12kf.md)",
+             "k_recip_prepare": "latency: f64 projections and warp reductions per candidate"}
     for name, ms, alg, traffic, what in (
             ("k_sweep_tiled", sweep_ms, sweep_bytes, units * SWEEP_DRAM_BYTES_PER_UNIT,
-             "depth sweep, box-filtered ZNCC over 32x8- or 16x16-site tiles (plane-chunk merge included)"),
+             "depth sweep, box-filtered ZNCC over %dx%d-site tiles (plane-chunk merge included)"
+             % (TX, TY)),
             ("k_recip_sweep", recip_sweep_ms, recip_bytes, None,
              "single-view reciprocal sweep, warp per pending pair, all three launches"),
             ("k_recip_prepare", recip_prep_ms, prep_bytes, None,
@@ -156,7 +165,7 @@ def kernel_rooflines(info, units, b, sweep_ms, recip_sweep_ms, recip_prep_ms, hb
                      "algorithmic_bytes": alg, "ms_per_step": ms,
                      "note": "achieved = unique texel bytes the kernel must read per step / its "
                              "summed CUDA-event time; peak " + peak_note + "; the kernel is "
-                             "bound by instruction issue, its gathers hit L1/L2"}
+                             "bound by " + bound[name]}
     return out
 
 
