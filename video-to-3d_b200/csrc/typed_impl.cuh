@@ -552,7 +552,36 @@ __global__ void __launch_bounds__(kTileThreads, 1024 / kTileThreads) k_sweep_til
             // arithmetic is the scalar computation, bit for bit
             const bool inside = (inmask[k - k0] >> j) & 1u;
             const float a0 = A[0], a1 = A[1], a3 = A[3], a4 = A[4], a6 = A[6], a7 = A[7];
-            for (int p = 0; p < n_steps; ++p) {
+            // inside the source: two pair-steps at a time, both steps' gathers
+            // issued before either step's stores (every slot of the table has
+            // coordinates inside the footprint rectangle, so a step past the
+            // footprint samples harmlessly and only its stores are skipped)
+            int p0 = 0;
+            if (inside) {
+                auto step = [&](int ws) {
+                    const float4 e = slotxy[ws * 32 + lane];
+                    const float2 X2 = f2(e.x, e.y), Y2 = f2(e.z, e.w);
+                    const float2 hx = __ffma2_rn(f2(a1, a1), Y2, f2(H2, H2));
+                    const float2 hy = __ffma2_rn(f2(a4, a4), Y2, f2(H5, H5));
+                    const float2 hz = __ffma2_rn(f2(a7, a7), Y2, f2(H8, H8));
+                    const float2 h2 = __ffma2_rn(f2(a6, a6), X2, hz);
+                    const float2 iv = f2(rcp_approx(h2.x), rcp_approx(h2.y));
+                    const float2 u = __fmul2_rn(__ffma2_rn(f2(a0, a0), X2, hx), iv);
+                    const float2 q = __fmul2_rn(__ffma2_rn(f2(a3, a3), X2, hy), iv);
+                    return sample_nonneg_pair<T>(sdata, si.width, u, q);
+                };
+                for (; p0 + 1 < n_steps; p0 += 2) {
+                    const int ws0 = p0 * kTileWarps + wid, ws1 = ws0 + kTileWarps;
+                    const int fa0 = ws0 * 64 + lane, fa1 = ws1 * 64 + lane;
+                    if (fa0 >= np) break;
+                    const float2 s0 = step(ws0), s1 = step(ws1);
+                    samp[fa0] = s0.x;
+                    if (fa0 + 32 < np) samp[fa0 + 32] = s0.y;
+                    if (fa1 < np) samp[fa1] = s1.x;
+                    if (fa1 + 32 < np) samp[fa1 + 32] = s1.y;
+                }
+            }
+            for (int p = p0; p < n_steps; ++p) {
                 const int ws = p * kTileWarps + wid;
                 const int fa = ws * 64 + lane;
                 if (fa >= np) break;
