@@ -820,10 +820,12 @@ __global__ void __launch_bounds__(256) k_reciprocal_exact(BatchDev b, const Cand
 // kernels so that the single-view sweep, where the time goes, is not sized
 // by the registers of the exact-f64 prologue:
 //  * k_recip_prepare, one warp per candidate: its reference window once, then
-//    per source the direct cost and the exact-f64 source contrast,
-//    lane-parallel over the window taps with warp reductions (max/min are
-//    order-free, so the contrast gate stays exact).  A pair that passes parks
-//    its source pixel in its RecipObs slot with valid = kObsPending;
+//    per source the direct cost and the source contrast gate (f32 on the
+//    exact f64 taps' texels and fractions, the exact f64 contrast where the
+//    f32 one lies near the gate), lane-parallel over the window taps with warp
+//    reductions (max/min are order-free, so the gate's decision is the exact
+//    one).  A pair that passes parks its source pixel in its RecipObs slot
+//    with valid = kObsPending;
 //  * k_recip_sweep, one warp per pending pair, lanes over hypotheses:
 //    re-samples the source window (the same f64 taps, so the same f32
 //    values), sweeps every hypothesis and writes the final RecipObs.
@@ -1691,7 +1693,7 @@ cudaError_t Typed<T>::sweep_tiled(const BatchDev& b, uint32_t max_nx, uint32_t m
         V3D_COUNTED kern<<<grid, kTileThreads, smem, st>>>(b, total_sites, rank, status, ctr, n, chunks.partial);
         return cudaGetLastError();
     };
-    // stride 2 (every ZNCC configuration of the benchmarks) has its own instantiation
+    // grid stride 2, the ZNCC profiles' usual stride, has its own instantiation
     auto pick = [&](auto k2, auto k0, int W) { return stride == 2 ? run(k2, W) : run(k0, W); };
     auto by_acc = [&](auto tx_tag) -> cudaError_t {
         constexpr int X = decltype(tx_tag)::value;
