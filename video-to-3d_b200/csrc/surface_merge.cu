@@ -2215,6 +2215,20 @@ namespace v3d {
 namespace merge {
 namespace {
 
+// fn(lo, hi) over [0, n) in contiguous ranges on up to 16 host threads (the
+// callers write disjoint elements, so the result does not depend on the split)
+template <class F>
+void parallel_ranges(size_t n, F&& fn) {
+    const size_t n_threads = std::max<size_t>(
+        1, std::min<size_t>({(size_t)std::thread::hardware_concurrency(), 16, (n + 65535) / 65536}));
+    const size_t chunk = (n + n_threads - 1) / n_threads;
+    std::vector<std::thread> pool;
+    for (size_t k = 1; k < n_threads; ++k)
+        pool.emplace_back([&, k] { fn(std::min(n, k * chunk), std::min(n, (k + 1) * chunk)); });
+    fn(0, std::min(n, chunk));
+    for (auto& th : pool) th.join();
+}
+
 size_t uf_find(std::vector<size_t>& parent, size_t i) {
     size_t r = i;
     while (parent[r] != r) r = parent[r];
@@ -2345,10 +2359,12 @@ int32_t merge_impl(v3d_context* ctx, Device& dev, const v3d_point* points, uint6
     auto position = [&](uint64_t v) { return V3{(double)points[v].x, (double)points[v].y, (double)points[v].z}; };
     std::vector<Geometry> geometry(nt);
     std::vector<uint8_t> has_geometry(nt, 0);
-    for (size_t i = 0; i < nt; ++i) {
-        const V3 c[3] = {position(tris[i].a), position(tris[i].b), position(tris[i].c)};
-        has_geometry[i] = make_geometry(c, geometry[i]) ? 1 : 0;
-    }
+    parallel_ranges(nt, [&](size_t lo, size_t hi) {
+        for (size_t i = lo; i < hi; ++i) {
+            const V3 c[3] = {position(tris[i].a), position(tris[i].b), position(tris[i].c)};
+            has_geometry[i] = make_geometry(c, geometry[i]) ? 1 : 0;
+        }
+    });
     double median_edge;
     {
         std::vector<double> edges;
@@ -2405,13 +2421,15 @@ int32_t merge_impl(v3d_context* ctx, Device& dev, const v3d_point* points, uint6
     // device inputs: every triangle's world corners and the clusters
     {
         std::vector<double> corners(nt * 9, 0.0);
-        for (size_t i = 0; i < nt; ++i)
-            if (has_geometry[i])
-                for (int k = 0; k < 3; ++k) {
-                    corners[i * 9 + 3 * k] = geometry[i].c[k].x;
-                    corners[i * 9 + 3 * k + 1] = geometry[i].c[k].y;
-                    corners[i * 9 + 3 * k + 2] = geometry[i].c[k].z;
-                }
+        parallel_ranges(nt, [&](size_t lo, size_t hi) {
+            for (size_t i = lo; i < hi; ++i)
+                if (has_geometry[i])
+                    for (int k = 0; k < 3; ++k) {
+                        corners[i * 9 + 3 * k] = geometry[i].c[k].x;
+                        corners[i * 9 + 3 * k + 1] = geometry[i].c[k].y;
+                        corners[i * 9 + 3 * k + 2] = geometry[i].c[k].z;
+                    }
+        });
         V3D_CTX_CK(dev.corners.ensure(nt * 9, dev.st));
         V3D_CTX_CK(dev.cluster.ensure(n_points, dev.st));
         V3D_CTX_CK(cudaMemcpyAsync(dev.corners.p, corners.data(), 8 * corners.size(),

@@ -1719,7 +1719,9 @@ cudaError_t Typed<T>::reciprocal(const BatchDev& b, const Cand* cands, const uin
                                  cudaStream_t st) {
     using namespace typed_detail;
     const unsigned blocks = (unsigned)sm_count() * 8;
-    const unsigned rblocks3 = (unsigned)sm_count() * 16;  // the banded sweep: 4 blocks of 4 warps an SM
+    // the banded sweep: four waves of its resident blocks (a whole number of
+    // waves, so the grid-stride loop leaves no partial last wave)
+    const unsigned rblocks3 = (unsigned)sm_count() * 4 * RecipBounds<kRecipBanded>::kBlocks;
 #define V3D_CK_RET(x)                                \
     do {                                             \
         const cudaError_t e_ = (x);                  \
@@ -1733,7 +1735,8 @@ cudaError_t Typed<T>::reciprocal(const BatchDev& b, const Cand* cands, const uin
     auto prep_and_list = [&](auto prep) -> cudaError_t {
         cudaError_t e = cudaMemsetAsync(q.flags, 0, q.cap_items, st);
         if (e != cudaSuccess) return e;
-        V3D_COUNTED prep<<<blocks, 256, 0, st>>>(b, cands, count, obs, ctr, q.flags);
+        // three waves of the prologue's three resident blocks an SM
+        V3D_COUNTED prep<<<(unsigned)sm_count() * 9, 256, 0, st>>>(b, cands, count, obs, ctr, q.flags);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         return launch_compact(q.flags, 1, q.cap_items, q.items, q.n_items, q.scratch, st);
     };
