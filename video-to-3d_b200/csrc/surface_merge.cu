@@ -155,6 +155,121 @@ __device__ __forceinline__ PT load_pt(const double* p) {
     return t;
 }
 
+// A warp's lookup scratch: the postings of one query, then per posting (in
+// ascending order) what the query's loop adds.
+constexpr int kLookupWarps = 4;  // warps per block of the lookup kernels
+struct WarpPostings {
+    uint32_t idx[kMaxPostings];
+    double a[kMaxPostings], b[kMaxPostings];
+    uint8_t ok[kMaxPostings];
+    uint32_t n;
+};
+
+// The candidate's postings on one footprint grid (LevelGrid::query_bounded), by
+// the warp's lanes: w.idx[0, n) ascending (the reference's BTreeSet order), or a
+// QueryLimit status.  Every lane returns the same status, n and used.  The
+// reference takes postings cell by cell until one does not fit the budget; the
+// counts only grow, so that happens exactly when the query's total exceeds it,
+// and the order the lanes gather them in does not matter before the sort.
+__device__ uint8_t warp_grid_lookup(const DevStore& s, const DevFootprint& f, const PT& c,
+                                    WarpPostings& w, uint32_t lane, uint32_t& n, uint32_t& used) {
+    double lo[2] = {INFINITY, INFINITY}, hi[2] = {-INFINITY, -INFINITY};
+    for (int i = 0; i < 3; ++i) {
+        lo[0] = fmin(lo[0], c.x[i]);
+        hi[0] = fmax(hi[0], c.x[i]);
+        lo[1] = fmin(lo[1], c.y[i]);
+        hi[1] = fmax(hi[1], c.y[i]);
+    }
+    n = 0;
+    used = 0;
+    for (int level = 0; level < f.levels; ++level) {
+        uint64_t count = 1;
+        for (int a = 0; a < 2; ++a) {
+            int64_t first, last;
+            if (!mg::axis_range(f.cell, level, lo[a], hi[a], first, last)) return kTooManyCells;
+            first = mg::sat_sub(first, mg::kMaxAnchorCellSpan);
+            if (last < first) return kTooManyCells;
+            const uint64_t span = (uint64_t)last - (uint64_t)first;
+            if (span == UINT64_MAX) return kTooManyCells;
+            const uint64_t cells = span + 1;
+            count = (count != 0 && cells > UINT64_MAX / count) ? UINT64_MAX : count * cells;
+        }
+        if (count > kMaxImageGridCells) return kTooManyCells;
+    }
+    const mg::GridBucket* b = s.buckets + f.bucket_off;
+    // the bucket of cell (level, x, y): its first item and count
+    auto bucket = [&](int level, int64_t x, int64_t y, uint32_t& start) -> uint32_t {
+        uint32_t l = 0, h = f.n_buckets;
+        while (l < h) {
+            const uint32_t mid = (l + h) >> 1;
+            if (mg::bucket_less(b[mid], level, x, y)) l = mid + 1;
+            else h = mid;
+        }
+        if (l < f.n_buckets && b[l].level == level && b[l].x == x && b[l].y == y) {
+            start = b[l].start;
+            return (l + 1 < f.n_buckets ? b[l + 1].start : f.n_bucketed) - b[l].start;
+        }
+        return 0;
+    };
+    // each cell of each level's (first..last)^2 range, lanes over cells; pass 0
+    // counts, pass 1 gathers
+    for (int pass = 0; pass < 2; ++pass) {
+        uint32_t mine = 0;
+        for (int level = 0; level < f.levels; ++level) {
+            int64_t x0, x1, y0, y1;
+            mg::axis_range(f.cell, level, lo[0], hi[0], x0, x1);
+            mg::axis_range(f.cell, level, lo[1], hi[1], y0, y1);
+            x0 = mg::sat_sub(x0, mg::kMaxAnchorCellSpan);
+            y0 = mg::sat_sub(y0, mg::kMaxAnchorCellSpan);
+            const uint32_t nx = (uint32_t)(x1 - x0 + 1), ncell = nx * (uint32_t)(y1 - y0 + 1);
+            for (uint32_t q = lane; q < ncell; q += 32) {
+                uint32_t start = 0;
+                const uint32_t k = bucket(level, x0 + (int64_t)(q % nx), y0 + (int64_t)(q / nx), start);
+                if (!k) continue;
+                if (pass == 0) {
+                    mine += k;
+                } else {
+                    const uint32_t at = atomicAdd(&w.n, k);
+                    for (uint32_t i = 0; i < k; ++i) w.idx[at + i] = s.items[f.item_off + start + i];
+                }
+            }
+        }
+        if (pass == 1) break;
+        for (int o = 16; o > 0; o >>= 1) mine += __shfl_xor_sync(0xffffffffu, mine, o);
+        const uint64_t total = (uint64_t)mine + f.n_unindexed;
+        if (total > kMaxPostings) {
+            used = kMaxPostings;
+            return kPostingBound;
+        }
+        n = used = (uint32_t)total;
+        for (uint32_t i = lane; i < f.n_unindexed; i += 32)
+            w.idx[i] = s.items[f.item_off + f.n_bucketed + i];
+        if (lane == 0) w.n = f.n_unindexed;
+        __syncwarp();
+    }
+    __syncwarp();
+    // ascending: a bitonic sort over the next power of two, padded with the largest key
+    uint32_t N = 1;
+    while (N < n) N <<= 1;
+    for (uint32_t i = n + lane; i < N; i += 32) w.idx[i] = 0xffffffffu;
+    __syncwarp();
+    for (uint32_t k = 2; k <= N; k <<= 1)
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            for (uint32_t i = lane; i < N; i += 32) {
+                const uint32_t l = i ^ j;
+                if (l > i) {
+                    const uint32_t x = w.idx[i], y = w.idx[l];
+                    if ((x > y) == ((i & k) == 0)) {
+                        w.idx[i] = y;
+                        w.idx[l] = x;
+                    }
+                }
+            }
+            __syncwarp();
+        }
+    return kJudged;
+}
+
 // The candidate's postings on one footprint grid, ascending (the reference's
 // BTreeSet), or a QueryLimit status (LevelGrid::query_bounded).
 __device__ uint8_t grid_lookup(const DevStore& s, const DevFootprint& f, const PT& c,
@@ -360,55 +475,67 @@ __global__ void __launch_bounds__(128) k_fold(DevStore s, const Cand* cands, uin
 // false counts them; WRITE true stores the first (out_limit - out_off) of them
 // at ratios[out_off...].
 template <bool WRITE>
-__global__ void __launch_bounds__(128) k_ratios(DevStore s, const Job* jobs, uint32_t n_jobs,
-                                                 const uint32_t* anchors, JobOut* out,
-                                                 double* ratios) {
-    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(32 * kLookupWarps) k_ratios(DevStore s, const Job* jobs, uint32_t n_jobs,
+                                                               const uint32_t* anchors, JobOut* out,
+                                                               double* ratios) {
+    __shared__ WarpPostings scratch[kLookupWarps];
+    const uint32_t lane = threadIdx.x & 31u;
+    WarpPostings& w = scratch[threadIdx.x >> 5];
+    const uint32_t j = blockIdx.x * kLookupWarps + (threadIdx.x >> 5);
     if (j >= n_jobs) return;
     const Job job = jobs[j];
     if (WRITE && job.out_off >= job.out_limit) return;
     const DevFootprint f = s.fps[job.footprint];
-    const double* w = s.corners + (size_t)job.triangle * 9;
+    const double* wc = s.corners + (size_t)job.triangle * 9;
     PT cand;
     JobOut o{0.0, 0.0, 0u, 0u, kJudged};
-    if (!project_candidate(f, w, cand)) {
+    if (!project_candidate(f, wc, cand)) {
         o.status = kUnprojectable;
-        if (!WRITE) out[j] = o;
+        if (!WRITE && lane == 0) out[j] = o;
         return;
     }
-    uint32_t found[kMaxPostings];
     uint32_t n, used;
-    o.status = grid_lookup(s, f, cand, found, n, used);
+    o.status = warp_grid_lookup(s, f, cand, w, lane, n, used);
     o.used = used;
     if (o.status != kJudged) {
-        if (!WRITE) out[j] = o;
+        if (!WRITE && lane == 0) out[j] = o;
         return;
     }
-    const uint32_t limit = WRITE ? job.out_limit - job.out_off : 0xffffffffu;
-    uint32_t count = 0;
-    for (uint32_t k = 0; k < n && count < limit; ++k) {
-        const uint32_t idx = found[k];
-        const uint32_t t = f.tri_off + idx;
-        if (!linked(s, job.own_comp, s.fp_comp[t])) continue;
-        if (!anchored(anchors + job.anchors_off, job.n_anchors, s.fp_vert + (size_t)t * 3)) continue;
-        const PT kept = load_pt(s.fp_tri + (size_t)t * 9);
-        Poly<8> poly;
-        if (!mg::clip_to_triangle(cand, kept, poly)) continue;
-        if (!(mg::poly_area(poly) > 0.0)) continue;
-        V2 sum{0.0, 0.0};
-        for (int v = 0; v < poly.n; ++v) sum = sum + poly.v[v];
-        const V2 centroid = sum / (double)poly.n;
-        double owner, own;
-        if (mg::inverse_depth(kept, centroid, owner) && mg::inverse_depth(cand, centroid, own)) {
-            const double ratio = mg::dvd(owner, own);
-            if (fabs(mg::sub(ratio, 1.0)) <= kMaxRelativeScaleSample) {
-                if (WRITE) ratios[job.out_off + count] = ratio;
-                ++count;
+    // each posting's sample in parallel, then the first `limit` in ascending order
+    for (uint32_t k = lane; k < n; k += 32) {
+        const uint32_t t = f.tri_off + w.idx[k];
+        bool ok = false;
+        double ratio = 0.0;
+        if (linked(s, job.own_comp, s.fp_comp[t]) &&
+            anchored(anchors + job.anchors_off, job.n_anchors, s.fp_vert + (size_t)t * 3)) {
+            const PT kept = load_pt(s.fp_tri + (size_t)t * 9);
+            Poly<8> poly;
+            if (mg::clip_to_triangle(cand, kept, poly) && mg::poly_area(poly) > 0.0) {
+                V2 sum{0.0, 0.0};
+                for (int v = 0; v < poly.n; ++v) sum = sum + poly.v[v];
+                const V2 centroid = sum / (double)poly.n;
+                double owner, own;
+                if (mg::inverse_depth(kept, centroid, owner) && mg::inverse_depth(cand, centroid, own)) {
+                    ratio = mg::dvd(owner, own);
+                    ok = fabs(mg::sub(ratio, 1.0)) <= kMaxRelativeScaleSample;
+                }
             }
         }
+        w.ok[k] = ok ? 1 : 0;
+        w.a[k] = ratio;
     }
-    o.count = count;
-    if (!WRITE) out[j] = o;
+    __syncwarp();
+    if (lane == 0) {
+        const uint32_t limit = WRITE ? job.out_limit - job.out_off : 0xffffffffu;
+        uint32_t count = 0;
+        for (uint32_t k = 0; k < n && count < limit; ++k)
+            if (w.ok[k]) {
+                if (WRITE) ratios[job.out_off + count] = w.a[k];
+                ++count;
+            }
+        o.count = count;
+        if (!WRITE) out[j] = o;
+    }
 }
 
 }  // namespace merge
@@ -2516,7 +2643,7 @@ int32_t merge_impl(v3d_context* ctx, Device& dev, const v3d_point* points, uint6
                     const DevStore s = dev.store();
                     const uint32_t* anchors_d = dev.anchors.p;
                     V3D_CTX_CK(dev.run(jobs, outs, [&](uint32_t n) {
-                        k_ratios<false><<<(n + 127) / 128, 128, 0, dev.st>>>(s, dev.jobs.p, n, anchors_d,
+                        k_ratios<false><<<(n + kLookupWarps - 1) / kLookupWarps, 32 * kLookupWarps, 0, dev.st>>>(s, dev.jobs.p, n, anchors_d,
                                                                              dev.outs.p, nullptr);
                     }));
                     // members are taken in order until 4096 samples (surface_merge.rs:630-647)
@@ -2544,7 +2671,7 @@ int32_t merge_impl(v3d_context* ctx, Device& dev, const v3d_point* points, uint6
                         std::vector<JobOut> unused;
                         double* ratios_d = dev.ratios.p;
                         V3D_CTX_CK(dev.run(writes, unused, [&](uint32_t n) {
-                            k_ratios<true><<<(n + 127) / 128, 128, 0, dev.st>>>(s, dev.jobs.p, n, anchors_d,
+                            k_ratios<true><<<(n + kLookupWarps - 1) / kLookupWarps, 32 * kLookupWarps, 0, dev.st>>>(s, dev.jobs.p, n, anchors_d,
                                                                                 dev.outs.p, ratios_d);
                         }));
                         ratio_buf.resize(owner_slots.size() * kMaxScaleSamples);
