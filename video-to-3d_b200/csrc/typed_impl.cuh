@@ -360,7 +360,7 @@ __host__ __device__ constexpr int tiled_steps(int np) { return (np + 2 * kTileTh
 // (tested once per plane and source on the rectangle's corners), the step
 // skips the per-sample domain tests.
 template <class T, int R, class Acc, int TX, int S>
-__global__ void __launch_bounds__(kTileThreads, 1024 / kTileThreads) k_sweep_tiled(BatchDev b, uint64_t total_sites,
+__global__ void __launch_bounds__(kTileThreads, (S && R >= 4) ? 3 : 1024 / kTileThreads) k_sweep_tiled(BatchDev b, uint64_t total_sites,
                                                      SiteRank* __restrict__ rank,
                                                      uint8_t* __restrict__ status,
                                                      RefCounters* __restrict__ ctr, int n_chunks,
@@ -525,15 +525,19 @@ __global__ void __launch_bounds__(kTileThreads, 1024 / kTileThreads) k_sweep_til
     }
     const float sr_shift = (float)(sr - n * (double)shift);
     const float inv_nf = 1.0f / (float)N, minvar_nf = (float)minvar_n;
-    // the reference taps of this thread's first horizontal window, the same
-    // for every plane and source (the stride-2 instantiation has the registers)
-    float rreg[W];
-    if (S) {
-        const int i = tid < PY * TX ? tid : 0;
+    // the reference taps of this thread's first horizontal windows, the same
+    // for every plane and source: the stride-2 instantiation keeps one window's
+    // in registers at four blocks an SM, and for 9x9 windows three blocks an SM
+    // with three windows' taps (its measured best)
+    constexpr int kRegWindows = S ? (R >= 4 ? 3 : 1) : 0;
+    float rreg[(kRegWindows ? kRegWindows : 1) * W];
+#pragma unroll
+    for (int w = 0; w < kRegWindows; ++w) {
+        const int i0 = tid + w * kTileThreads, i = i0 < PY * TX ? i0 : 0;
         const int yy = TX == 16 ? rowmap[i / TX] : i / TX;
         const float* rp = refv + yy * PXp + i % TX;
 #pragma unroll
-        for (int dx = 0; dx < W; ++dx) rreg[dx] = rp[toff[dx]];
+        for (int dx = 0; dx < W; ++dx) rreg[w * W + dx] = rp[toff[dx]];
     }
     Rank st = rank_empty();
     for (int k = k0; k < k1; ++k) {
@@ -557,7 +561,7 @@ __global__ void __launch_bounds__(kTileThreads, 1024 / kTileThreads) k_sweep_til
             // coordinates inside the footprint rectangle, so a step past the
             // footprint samples harmlessly and only its stores are skipped)
             int p0 = 0;
-            if (inside) {
+            if (inside && R < 4) {
                 auto step = [&](int ws) {
                     const float4 e = slotxy[ws * 32 + lane];
                     const float2 X2 = f2(e.x, e.y), Y2 = f2(e.z, e.w);
@@ -652,8 +656,10 @@ __global__ void __launch_bounds__(kTileThreads, 1024 / kTileThreads) k_sweep_til
                     hrs[o] = (Acc)c;
                 }
             };
-            if (tid < PY * TX) hwindow(tid, S ? rreg : nullptr);
-            for (int i = tid + kTileThreads; i < PY * TX; i += kTileThreads) hwindow(i, nullptr);
+#pragma unroll
+            for (int w = 0; w < kRegWindows; ++w)
+                if (tid + w * kTileThreads < PY * TX) hwindow(tid + w * kTileThreads, rreg + w * W);
+            for (int i = tid + kRegWindows * kTileThreads; i < PY * TX; i += kTileThreads) hwindow(i, nullptr);
             __syncthreads();
             if (sampled) {
                 float cost = __int_as_float(0x7fc00000);
