@@ -910,6 +910,11 @@ __device__ __forceinline__ float lds_f32(uint32_t a) {
     asm volatile("ld.shared.f32 %0, [%1];" : "=f"(x) : "r"(a));
     return x;
 }
+__device__ __forceinline__ float2 lds_f32x2(uint32_t a) {
+    float2 x;
+    asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(x.x), "=f"(x.y) : "r"(a));
+    return x;
+}
 
 
 template <class T>
@@ -948,7 +953,9 @@ struct BandSampler {
         const float bot = fmaf(d1, tx, v01);
         return fmaf(bot - top, ty, top);
     }
-    // two taps at once; the loads land in the halves of the packed operands
+    // two taps at once: each tap's entries come as one 8-byte load a row, the
+    // row interpolations are scalar FMAs whose results form the packed operands
+    // of the last step (the same operations as the scalar sampler, per tap)
     __device__ __forceinline__ float2 pair(float2 u, float2 v) const {
         const float2 s2x = f2(sx, sx), s2y = f2(sy, sy);
         const float2 tu = __fadd2_rd(u, s2x), tv = __fadd2_rd(v, s2y);
@@ -956,11 +963,10 @@ struct BandSampler {
         const uint32_t aa = entry(tu.x, tv.x), ab = entry(tu.y, tv.y);
         const float2 tx = __fadd2_rn(u, neg2(fu)), ty = __fadd2_rn(v, neg2(fv));
         constexpr uint32_t kRow = 1u << kBandRowShift;
-        const float2 v00 = f2(lds_f32(aa), lds_f32(ab)), d0 = f2(lds_f32(aa + 4), lds_f32(ab + 4));
-        const float2 v01 = f2(lds_f32(aa + kRow), lds_f32(ab + kRow));
-        const float2 d1 = f2(lds_f32(aa + kRow + 4), lds_f32(ab + kRow + 4));
-        const float2 top = __ffma2_rn(d0, tx, v00);
-        const float2 bot = __ffma2_rn(d1, tx, v01);
+        const float2 a0 = lds_f32x2(aa), a1 = lds_f32x2(aa + kRow);
+        const float2 b0 = lds_f32x2(ab), b1 = lds_f32x2(ab + kRow);
+        const float2 top = f2(fmaf(a0.y, tx.x, a0.x), fmaf(b0.y, tx.y, b0.x));
+        const float2 bot = f2(fmaf(a1.y, tx.x, a1.x), fmaf(b1.y, tx.y, b1.x));
         return __ffma2_rn(__fadd2_rn(bot, neg2(top)), ty, top);
     }
 };
