@@ -43,7 +43,7 @@ UNIT = "samples·planes·views/s"
 WIDTH, HEIGHT, FRAMES = 640, 360, 120
 RADIUS, PLANES, SOURCES, STRIDE = 3, 128, 8, 2
 # DRAM bytes per launch unit of the depth sweep, from the ncu capture of the same
-# workload cut to 12 keyframes (profiles/k_sweep_tiled_zncc7x7_640x360_12kf.md):
+# workload cut to 12 keyframes (the sweep's captured launch):
 # 12.59 MB read and 4.96 MB written (the plane chunks' partial rank states) for
 # 677.4 M window evaluations.  A clip's frames live in L2, so DRAM traffic grows
 # with the work; the reciprocal sweep's (86.2 MB read, 10.3 MB written by its
@@ -147,9 +147,9 @@ def kernel_rooflines(info, units, b, sweep_ms, recip_sweep_ms, recip_prep_ms, hb
     prep_bytes = info["candidates"] * SOURCES * 3 * (W + 1) ** 2 * b
     out = {}
     bound = {"k_sweep_tiled": "the shared-memory data path of its f64 box filters (83 % of the L1 "
-                              "wavefront peak in profiles/k_sweep_tiled_zncc7x7_640x360_12kf.md)",
+                              "wavefront peak in an ncu capture of the 12-keyframe cut)",
              "k_recip_sweep": "instruction issue and the FMA pipe, its texels staged in shared memory "
-                              "(profiles/k_recip_sweep_zncc7x7_640x360_12kf.md)",
+                              "(64 % issue-active, FMA 57 % in an ncu capture of the 12-keyframe cut)",
              "k_recip_prepare": "latency: f64 projections and warp reductions per candidate"}
     for name, ms, alg, traffic, what in (
             ("k_sweep_tiled", sweep_ms, sweep_bytes, units * SWEEP_DRAM_BYTES_PER_UNIT,
