@@ -83,3 +83,28 @@ def test_sweep_row_pairing_is_a_permutation_with_disjoint_banks():
                     banks_a = {(a * pxp + c) % 32 for c in range(16)}
                     banks_b = {(b * pxp + c) % 32 for c in range(16)}
                     assert not banks_a & banks_b
+
+
+def test_contrast_gate_f32_error_bound():
+    """k_recip_prepare decides the source contrast gate in f32 on the exact
+    texels and fractions of the f64 taps whenever the f32 contrast lies more
+    than M 2^-16 from the gate (M the largest texel magnitude read); the f32
+    bilinear is within M 2^-20 of the f64 one, so the decision is the exact
+    one.  Restated here with f32 products and sums rounded separately (a wider
+    error than the kernel's FMAs) over texels of every storage scale."""
+    rng = np.random.default_rng(7)
+    for scale in (1.0, 255.0, 1e-3, 1e4):
+        t = (rng.random((200000, 4)) * scale).astype(np.float32)
+        frac = rng.random((200000, 2))
+        tx, ty = frac[:, 0].astype(np.float32), frac[:, 1].astype(np.float32)
+        v00, v10, v01, v11 = (t[:, i] for i in range(4))
+        top = (v10 - v00) * tx + v00
+        bot = (v11 - v01) * tx + v01
+        f32 = ((bot - top) * ty + top).astype(np.float64)
+        d = t.astype(np.float64)
+        fx, fy = frac[:, 0], frac[:, 1]
+        top64 = d[:, 0] * (1.0 - fx) + d[:, 1] * fx
+        bot64 = d[:, 2] * (1.0 - fx) + d[:, 3] * fx
+        f64 = top64 * (1.0 - fy) + bot64 * fy
+        mag = np.abs(t).max(axis=1).astype(np.float64)
+        assert np.all(np.abs(f32 - f64) <= mag * 2.0 ** -20), scale
