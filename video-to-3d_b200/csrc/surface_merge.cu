@@ -156,11 +156,11 @@ __device__ __forceinline__ PT load_pt(const double* p) {
 }
 
 // A warp's lookup scratch: the postings of one query, then per posting (in
-// ascending order) what the query's loop adds.
-constexpr int kLookupWarps = 4;  // warps per block of the lookup kernels
+// ascending order) its sample and whether the query's loop takes it.
+constexpr int kLookupWarps = 4;  // warps per block of the warp-per-lookup kernel
 struct WarpPostings {
     uint32_t idx[kMaxPostings];
-    double a[kMaxPostings], b[kMaxPostings];
+    double a[kMaxPostings];
     uint8_t ok[kMaxPostings];
     uint32_t n;
 };
